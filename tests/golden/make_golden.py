@@ -1,0 +1,84 @@
+"""Extracts the reference's frozen reghdfe fixtures into tests/golden/.
+
+The reference (leoliu0/fereg) pins its OLS path against reghdfe 6.13.1 run at tol(1e-14)
+(crates/fereg-core/tests/data/ols_data.csv + ols_s*.json, generated there by
+gen_ols_fixtures.do). This script copies the data columns and the parts of each fixture the
+tests here compare (b, V, dof_table, sample, resid, d, groupvar, scalars), and records each
+fixture's model specification as restated from the reference's harness
+(crates/fereg-core/tests/ols.rs:803-827).
+
+Run once in a container that has the reference mounted:
+    python tests/golden/make_golden.py /path/to/reference
+The outputs are committed; the GPU box never reads the reference.
+"""
+
+import csv
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+IDYEAR = [["id"], ["year"]]
+X3 = ["x1", "x2", "x3"]
+X2 = ["x1", "x2"]
+
+
+def fx(name, x, absorb, **kw):
+    spec = dict(name=name, y="y", x=x, absorb=absorb, vce=[], robust=False, weight=None,
+                weight_kind=None, singletons=True, noconstant=False, firstpair=False)
+    spec.update(kw)
+    return spec
+
+
+# tests/ols.rs:803-827 (s16 uses slopes, which this path does not cover).
+SPECS = [
+    fx("s01_unadj", X3, IDYEAR),
+    fx("s02_robust_3fe", X3, [["id"], ["year"], ["firm"]], robust=True),
+    fx("s03_cluster_eq_fe", X2, IDYEAR, vce=["id"]),
+    fx("s04_fe_nested_in_cluster", X3, IDYEAR, vce=["region"]),
+    fx("s05_twoway_psd", X3, [["firm"], ["year"]], vce=["c1", "c2"]),
+    fx("s06_aw_cluster", X3, IDYEAR, vce=["firm"], weight="w", weight_kind="aweight"),
+    fx("s07_fw_robust", X3, IDYEAR, robust=True, weight="fw", weight_kind="fweight"),
+    fx("s08_pw", X3, [["id"], ["year"], ["firm"]], weight="w", weight_kind="pweight"),
+    fx("s09_absorbed_collinear", ["x1", "x2", "xa", "xc"], IDYEAR, status=[0, 0, 2, 3]),
+    fx("s10_interaction", X2, [["id"], ["firm", "year"]]),
+    fx("s11_noabsorb_cluster", X3, [], vce=["firm"]),
+    fx("s12_noconstant", X2, IDYEAR, noconstant=True),
+    fx("s13_keepsing_twoway", X2, IDYEAR, singletons=False, vce=["id", "year"]),
+    fx("s14_groupvar", X2, [["id"], ["firm"], ["year"]]),
+    fx("s15_firstpair_cluster", X2, [["id"], ["year"], ["firm"]], vce=["firm"], firstpair=True),
+    fx("s17_y_absorbed", X2, IDYEAR, y="y2"),
+    fx("s18_fw_twoway", X3, [["firm"], ["year"]], vce=["c1", "c2"], weight="fw", weight_kind="fweight"),
+]
+
+COLUMNS = ["id", "year", "firm", "region", "c1", "c2", "x1", "x2", "x3", "x4", "xa", "xc", "w", "fw", "y", "y2"]
+
+
+def main(ref):
+    data_dir = os.path.join(ref, "crates", "fereg-core", "tests", "data")
+    with open(os.path.join(data_dir, "ols_data.csv")) as f:
+        rows = list(csv.DictReader(f))
+    with open(os.path.join(HERE, "ols_data.csv"), "w", newline="") as f:
+        w = csv.writer(f)
+        w.writerow(COLUMNS)
+        for r in rows:
+            w.writerow([r[c] for c in COLUMNS])
+    out = []
+    for spec in SPECS:
+        with open(os.path.join(data_dir, f"ols_{spec['name']}.json")) as f:
+            j = json.load(f)
+        tag = spec["name"][1:3]
+        fix = dict(spec=spec, cmdline=j["cmdline"], colnames=j["colnames"], b=j["b"], V=j["V"],
+                   dof_table=j["dof_table"], sample=j["sample"], scalars=j["scalars"])
+        for key in (f"r{tag}", f"d{tag}", f"gv{tag}"):
+            if key in j:
+                fix[key[: -2]] = j[key]
+        out.append(fix)
+    with open(os.path.join(HERE, "ols_fixtures.json"), "w") as f:
+        json.dump(out, f)
+    print(f"wrote {len(out)} fixtures, {len(rows)} rows")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
