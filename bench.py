@@ -1,0 +1,377 @@
+"""Benchmark of the B200 fixed-effects solve on the 1e7-observation 3-FE OLS panel.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config c2|c1]
+
+One step is one call of the solve on the workload: the n x R block [y, x1..x10] (R = 11)
+residualized against indiv + firm + year (Absorber::residualize, the FE solve of the OLS call). `value` times the step with the block already resident in
+HBM; `e2e` times the same call through the C ABI with the block in pinned host memory (the
+host-to-device copy of the inputs and the device-to-host copy of the residualized block inside
+the timed region). Inputs (880 MB) exceed the 126 MB L2, so no flush runs between steps.
+
+Multi-GPU (torchrun): independent replicas, one per GPU (a single solve does not shard at this
+size); the step time is the max over ranks and `value` is seconds per call of the whole job.
+
+`--impl reference` times the reference's algorithm on the host cores: the CPU oracle (a C++
+restatement of the reference solver; the reference's Rust crate cannot be built here), with all
+host threads, on the same workload, metric and unit.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # OLS y ~ x1..x10 | indiv + firm + year, n = 1e6 indiv x 10 years, firm = row mod 1e5.
+    "c2": dict(n_ind=1_000_000, years=10, n_firm=100_000, k=10, seed=10**7 * 100 + 43),
+    # OLS y ~ x1 | indiv + year, n = 1e4 indiv x 10 years.
+    "c1": dict(n_ind=10_000, years=10, n_firm=0, k=1, seed=10**5 * 100 + 42),
+}
+TOL = 1e-8
+
+
+def make_data(cfg):
+    """Synthetic panel with the configuration's shapes and value distributions (seeded)."""
+    n_ind, years, n_firm, k = cfg["n_ind"], cfg["years"], cfg["n_firm"], cfg["k"]
+    n = n_ind * years
+    rng = np.random.default_rng(cfg["seed"])
+    i = np.arange(n)
+    ind = (i // years).astype(np.uint32)
+    year = (i % years).astype(np.uint32)
+    alpha = rng.standard_normal(n_ind)
+    gamma = rng.normal(0.0, np.sqrt(0.5), years)
+    rows = np.empty((n, 1 + k))
+    y = alpha[ind] + gamma[year] + rng.standard_normal(n)
+    codes, g = [ind], [n_ind]
+    if n_firm:
+        firm = (i % n_firm).astype(np.uint32)
+        psi = rng.standard_normal(n_firm)
+        y += psi[firm]
+        codes.append(firm)
+        g.append(n_firm)
+        for j in range(k):
+            x = 0.3 * psi[firm] + np.sqrt(1 - 0.09) * rng.standard_normal(n)
+            rows[:, 1 + j] = x
+            y += x / (j + 1)
+    else:
+        for j in range(k):
+            x = rng.standard_normal(n)
+            rows[:, 1 + j] = x
+            y += 1.0 * x
+    codes.append(year)
+    g.append(years)
+    rows[:, 0] = y
+    return codes, g, rows
+
+
+def ols_from_residualized(zr):
+    """OLS coefficients and iid variance from the residualized block (FP64 on the device)."""
+    import torch
+
+    X = zr[:, 1:]
+    y = zr[:, 0]
+    G = X.T @ X
+    b = torch.linalg.solve(G, X.T @ y)
+    e = y - X @ b
+    return b, e @ e, G
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel, workload):
+    """Per-launch DRAM bytes of `kernel` on `workload` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        with open(path) as f:
+            for ln in f:
+                parts = ln.split()
+                if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, world, local, pg
+
+
+def max_over_ranks(x, pg, device):
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def run_reference(args, cfg_name, cfg, rank, world):
+    """The reference's algorithm on the host cores (the CPU oracle), same metric and unit."""
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    codes, g, rows = make_data(cfg)
+    threads = oracle.max_threads()
+    ab = oracle.Absorber(codes, g)
+    times = []
+    for it in range(args.warmup + args.steps):
+        z = rows.copy()
+        t0 = time.perf_counter()
+        ab.residualize(z, tol=TOL)
+        t1 = time.perf_counter()
+        if it >= args.warmup:
+            times.append(t1 - t0)
+    v = float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(cfg_name, cfg), "n": len(rows), "R": rows.shape[1]},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": "full workload per step (C++ FP64 restatement of the reference solver, OpenMP)"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "sec/call (1e7-obs 3-FE OLS)"
+
+
+def workload_name(cfg_name, cfg):
+    if cfg_name == "c2":
+        return "OLS y~x1..x10 | indiv(1e6)+firm(1e5, row mod 1e5)+year(10), n=1e7, iid SEs"
+    return "OLS y~x1 | indiv(1e4)+year(10), n=1e5, iid SEs"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=list(CONFIGS))
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32r"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing (profiling runs)")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    cfg = CONFIGS[args.config]
+    rank, world, local, pg = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, args.config, cfg, rank, world)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    import torch
+
+    import fereg_b200 as fb
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    prec = fb.PREC_F64 if args.precision == "f64" else fb.PREC_F32_REFINED
+    codes, g, rows = make_data(cfg)
+    n, R = rows.shape
+    t0 = time.perf_counter()
+    ab = fb.Absorber(codes, g)
+    prepare_s = time.perf_counter() - t0
+    pi = ab.row_order()
+    rows = np.ascontiguousarray(rows[pi])  # the caller hands rows in the absorber's row order
+    stream = torch.cuda.ExternalStream(ab.stream(), device=device)
+    src = torch.from_numpy(rows).to(device)
+    work = torch.empty_like(src)
+
+    def step_device():
+        work.copy_(src)  # fresh inputs each step (outside the timed events)
+        torch.cuda.synchronize(device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        info = ab.residualize_device(work.data_ptr(), R, tol=TOL, precision=prec)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, info, None
+
+    for _ in range(args.warmup):
+        step_device()
+    barrier(pg)
+    torch.cuda.synchronize(device)
+    ab.set_profiling(True)
+    l0 = ab.launches()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            dt, info, b = step_device()
+            times.append(dt)
+    torch.cuda.synchronize(device)
+    barrier(pg)
+    launches = ab.launches() - l0
+    phases = ab.phase_times()
+    ab.set_profiling(False)
+    step_s = max_over_ranks(float(np.mean(times)), pg, device)
+    value = step_s / world
+
+    # e2e: the same call through the C ABI with the block in pinned host memory
+    pinned = torch.empty((n, R), dtype=torch.float64, pin_memory=True)
+    host = pinned.numpy()
+
+    def step_e2e():
+        np.copyto(host, rows)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ab.residualize(host, tol=TOL, precision=prec)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    e2e_s = None
+    if not args.no_e2e:
+        for _ in range(2):
+            step_e2e()
+        barrier(pg)
+        e2e_times = [step_e2e() for _ in range(max(3, args.steps // 2))]
+        e2e_s = max_over_ranks(float(np.mean(e2e_times)), pg, device) / world
+
+    # roofline of the dominant kernel (largest share of the timed phases)
+    hbm, peak_kind = peaks()
+    M, nb, g1 = ab.ncells, ab.nb, ab.g1
+    algo = {
+        "residualize": 2 * n * R * 8 + M * nb * 4 + g1 * R * 8 + g1 * 8,
+        "rhs_seg": n * R * 8 + g1 * R * 8 + (g1 + 1) * 4,
+    }
+    dom = max(algo, key=lambda k: phases[k][0])
+    ms, cnt = phases[dom]
+    achieved = algo[dom] / (ms / cnt / 1e3) / 1e9 if cnt else None
+    kern = {"residualize": "k_residualize", "rhs_seg": "k_rhs_seg"}[dom]
+    traffic = traffic_from_profiles(kern, args.config)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+
+        oab = oracle.Absorber(codes, g)
+        ts = []
+        for _ in range(3):
+            z = rows.copy()
+            t1 = time.perf_counter()
+            oab.residualize(z, tol=TOL)
+            ts.append(time.perf_counter() - t1)
+        cpu = {"value": float(np.mean(ts)), "unit": "s", "cores": oracle.max_threads(), "kind": "port",
+               "sample": "full workload, 3 calls (C++ FP64 restatement of the reference solver, OpenMP)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == fb.PREC_F64 else "f32+f64", "data": "synthetic",
+            "config": {"workload": workload_name(args.config, cfg), "n": n, "R": R, "cells": M, "m": ab.m,
+                       "g1": g1, "iterations": info["iterations"], "tol": TOL,
+                       "precision": args.precision, "l2": "inputs (880 MB) larger than L2, no flush",
+                       "parallelism": f"replicas x{world}", "prepare_s": prepare_s},
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm if achieved else None, "traffic": traffic,
+                         "peak_kind": peak_kind, "algorithmic_bytes": algo[dom]},
+            "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": n * R * 8, "d2h_bytes_per_step": n * R * 8},
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    ab.close()
+    if pg is not None:
+        barrier(pg)
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,228 @@
+"""fereg_b200 — B200-native fixed-effects solve behind the reference's `Absorber` boundary.
+
+The compute runs in libfereg_b200.so (hand-written sm_100a CUDA) through the C ABI declared in
+include/fereg_b200.h. This module is the Python host mirror of that ABI, used by the tests and
+the benchmark. There is no CPU fallback: loading fails loudly when the library is missing, and
+every call fails with the library's error when no CUDA device is present.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfereg_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "fereg_b200.h")
+
+PREC_F64 = 0
+PREC_F32_REFINED = 1
+
+_lib = None
+
+P = C.c_void_p
+u32p = C.POINTER(C.c_uint32)
+u64p = C.POINTER(C.c_uint64)
+f64p = C.POINTER(C.c_double)
+u8p = C.POINTER(C.c_uint8)
+
+
+class FeregError(RuntimeError):
+    """A nonzero return code of the C ABI (the reference's RfError::rc)."""
+
+    def __init__(self, rc, msg):
+        super().__init__(f"rc={rc}: {msg}")
+        self.rc = rc
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_uint64), ("escalated", C.c_int32), ("exact", C.c_int32)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m fereg_b200.build`")
+        _lib = C.CDLL(LIB_PATH)
+        _setup(_lib)
+    return _lib
+
+
+def _setup(L):
+    L.fereg_last_error.restype = C.c_char_p
+    L.fereg_absorber_create.argtypes = [C.POINTER(u32p), u32p, C.c_int, f64p, C.c_size_t, P, C.POINTER(P)]
+    L.fereg_absorber_destroy.argtypes = [P]
+    L.fereg_absorber_n.argtypes = [P]
+    L.fereg_absorber_n.restype = C.c_size_t
+    L.fereg_absorber_coefs_len.argtypes = [P]
+    L.fereg_absorber_coefs_len.restype = C.c_size_t
+    L.fereg_absorber_row_order.argtypes = [P, u32p]
+    L.fereg_absorber_weights.argtypes = [P, f64p, C.POINTER(C.c_int)]
+    L.fereg_absorber_set_weights.argtypes = [P, f64p]
+    L.fereg_absorber_residualize.argtypes = [P, f64p, C.c_size_t, C.c_double, C.c_size_t, C.c_int, f64p, f64p,
+                                             C.POINTER(SolveInfo)]
+    L.fereg_absorber_residualize_ex.argtypes = [P, P, C.c_int, C.c_size_t, C.c_double, C.c_size_t, C.c_int, f64p,
+                                                f64p, C.c_int, C.POINTER(SolveInfo)]
+    L.fereg_absorber_fit_rows.argtypes = [P, f64p, C.c_size_t, C.c_size_t, f64p]
+    L.fereg_absorber_term_values.argtypes = [P, f64p, C.c_size_t, C.c_size_t, f64p]
+    L.fereg_absorber_info.argtypes = [P, u64p]
+    L.fereg_absorber_apply.argtypes = [P, f64p, C.c_size_t, f64p]
+    L.fereg_absorber_rhs.argtypes = [P, f64p, C.c_size_t, f64p, f64p, f64p, f64p]
+    L.fereg_absorber_precond.argtypes = [P, f64p, C.c_size_t, f64p]
+    L.fereg_absorber_weight_state.argtypes = [P, f64p, f64p, f64p, u8p, f64p]
+    L.fereg_absorber_stream.argtypes = [P]
+    L.fereg_absorber_stream.restype = P
+    L.fereg_absorber_set_profiling.argtypes = [P, C.c_int]
+    L.fereg_absorber_phase_times.argtypes = [P, f64p, u64p]
+    L.fereg_absorber_launches.argtypes = [P]
+    L.fereg_absorber_launches.restype = C.c_uint64
+
+
+def declared_symbols():
+    """Function names declared in include/fereg_b200.h."""
+    import re
+
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(fereg_[a-z0-9_]+)\s*\(", text)))
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def _check(rc):
+    if rc:
+        raise FeregError(rc, lib().fereg_last_error().decode())
+
+
+class Absorber:
+    """Host mirror of the reference `Absorber` (absorber.rs:62-97) over the B200 solver."""
+
+    def __init__(self, codes, g, w=None):
+        self.n = len(codes[0]) if codes else 0
+        self._codes = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
+        self.g = np.asarray(g, dtype=np.uint32)
+        ptrs = (u32p * max(1, len(self._codes)))(*[_p(a, u32p) for a in self._codes])
+        wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        h = P()
+        _check(lib().fereg_absorber_create(ptrs, _p(self.g, u32p), len(self._codes), _p(wa, f64p), self.n, None,
+                                           C.byref(h)))
+        self.h = h
+        info = np.zeros(8, dtype=np.uint64)
+        _check(lib().fereg_absorber_info(self.h, _p(info, u64p)))
+        self.m, self.g1, self.ncells, self.nb, self.m_small = (int(v) for v in info[1:6])
+        self.fe1 = int(np.int64(info[6]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fereg_absorber_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def row_order(self):
+        out = np.empty(self.n, dtype=np.uint32)
+        _check(lib().fereg_absorber_row_order(self.h, _p(out, u32p)))
+        return out
+
+    def weights(self):
+        out = np.empty(self.n)
+        has = C.c_int()
+        _check(lib().fereg_absorber_weights(self.h, _p(out, f64p), C.byref(has)))
+        return out if has.value else None
+
+    def set_weights(self, w_rows):
+        wa = None if w_rows is None else np.ascontiguousarray(w_rows, dtype=np.float64)
+        _check(lib().fereg_absorber_set_weights(self.h, _p(wa, f64p)))
+
+    def residualize(self, z, tol=1e-8, maxiter=16000, want_coefs=False, warm=None, precision=PREC_F64):
+        """Residualizes the n x r row-major host block `z` (row order) in place."""
+        assert z.dtype == np.float64 and z.flags.c_contiguous
+        r = z.shape[1] if z.ndim == 2 else 1
+        coefs = np.empty((self.m + self.g1, r)) if want_coefs else None
+        wa = None if warm is None else np.ascontiguousarray(warm, dtype=np.float64)
+        info = SolveInfo()
+        _check(lib().fereg_absorber_residualize_ex(self.h, z.ctypes.data_as(P), 0, r, tol, maxiter, int(want_coefs),
+                                                   _p(wa, f64p), _p(coefs, f64p), precision, C.byref(info)))
+        return dict(iterations=int(info.iterations), exact=bool(info.exact), escalated=bool(info.escalated),
+                    coefs=coefs)
+
+    def residualize_device(self, z_ptr, r, tol=1e-8, maxiter=16000, want_coefs=False, warm=None,
+                           precision=PREC_F64):
+        """Residualizes an n x r row-major block already in device memory (pointer `z_ptr`)."""
+        coefs = np.empty((self.m + self.g1, r)) if want_coefs else None
+        wa = None if warm is None else np.ascontiguousarray(warm, dtype=np.float64)
+        info = SolveInfo()
+        _check(lib().fereg_absorber_residualize_ex(self.h, P(z_ptr), 1, r, tol, maxiter, int(want_coefs),
+                                                   _p(wa, f64p), _p(coefs, f64p), precision, C.byref(info)))
+        return dict(iterations=int(info.iterations), exact=bool(info.exact), escalated=bool(info.escalated),
+                    coefs=coefs)
+
+    def fit_rows(self, coefs, col):
+        coefs = np.ascontiguousarray(coefs, dtype=np.float64)
+        out = np.empty(self.n)
+        _check(lib().fereg_absorber_fit_rows(self.h, _p(coefs, f64p), coefs.shape[1], col, _p(out, f64p)))
+        return out
+
+    def term_values(self, coefs, col):
+        coefs = np.ascontiguousarray(coefs, dtype=np.float64)
+        out = np.zeros(int(self.g.sum()))
+        _check(lib().fereg_absorber_term_values(self.h, _p(coefs, f64p), coefs.shape[1], col, _p(out, f64p)))
+        res, o = [], 0
+        for gq in self.g:
+            res.append(out[o:o + gq].copy())
+            o += int(gq)
+        return res
+
+    PHASES = ["rhs_seg", "rhs_pull", "apply", "precond", "vector", "residualize", "h2d", "d2h"]
+
+    def stream(self):
+        """The handle's cudaStream_t as an integer."""
+        return int(lib().fereg_absorber_stream(self.h) or 0)
+
+    def set_profiling(self, on=True):
+        _check(lib().fereg_absorber_set_profiling(self.h, int(on)))
+
+    def phase_times(self):
+        ms = np.zeros(8)
+        cnt = np.zeros(8, dtype=np.uint64)
+        _check(lib().fereg_absorber_phase_times(self.h, _p(ms, f64p), _p(cnt, u64p)))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PHASES)}
+
+    def launches(self):
+        return int(lib().fereg_absorber_launches(self.h))
+
+    # kernel-level parity hooks
+    def apply(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        y = np.empty_like(p)
+        _check(lib().fereg_absorber_apply(self.h, _p(p, f64p), p.shape[1], _p(y, f64p)))
+        return y
+
+    def rhs(self, rows):
+        rows = np.ascontiguousarray(rows, dtype=np.float64)
+        r = rows.shape[1]
+        y = np.empty((self.m, r))
+        b1 = np.empty((self.g1, r))
+        wsq = np.empty(r)
+        wsum = np.empty(r)
+        _check(lib().fereg_absorber_rhs(self.h, _p(rows, f64p), r, _p(y, f64p), _p(b1, f64p), _p(wsq, f64p),
+                                        _p(wsum, f64p)))
+        return y, b1, wsq, wsum
+
+    def precond(self, r_):
+        r_ = np.ascontiguousarray(r_, dtype=np.float64)
+        z = np.empty_like(r_)
+        _check(lib().fereg_absorber_precond(self.h, _p(r_, f64p), r_.shape[1], _p(z, f64p)))
+        return z
+
+    def weight_state(self):
+        n1 = np.empty(self.g1)
+        nr = np.empty(self.m)
+        diag = np.empty(self.m)
+        red = np.empty(self.m, dtype=np.uint8)
+        sw = C.c_double()
+        _check(lib().fereg_absorber_weight_state(self.h, _p(n1, f64p), _p(nr, f64p), _p(diag, f64p), _p(red, u8p),
+                                                 C.byref(sw)))
+        return dict(n1=n1, nr=nr, diag=diag, redundant=red.astype(bool), sw=sw.value)

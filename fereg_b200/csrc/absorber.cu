@@ -1,0 +1,943 @@
+// GpuAbsorber: structure on the host, the solve on the B200.
+//
+// residualize (solve.rs:1141-1311) runs the rhs pass over the rows (k_seg_rhs + k_pull_rhs),
+// lockstep PCG on the reduced system (k_seg_apply + k_pull_apply per matvec; Jacobi / grounded
+// dense small-block preconditioner; per-column scalars on the device), and the in-place
+// residualization pass (k_residualize). With Precision::F32_REFINED the PCG iterations run in
+// FP32 on the correction of an FP64 iterate whose true residual is recomputed in FP64 between
+// rounds (iterative refinement); the stopping rule is evaluated on the FP64 quantities.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+#include "absorber.h"
+#include "kernels.cuh"
+
+namespace fereg {
+
+namespace {
+constexpr int THREADS = TB;
+constexpr int GRID_T = 148 * 6;  // tile kernels: up to 6 resident CTAs per SM
+constexpr int GRID_V = 148 * 2;  // vector kernels with per-CTA partials
+constexpr int GRID_S = 148 * 4;  // warp-tile kernels (CTAs of WPB warps)
+constexpr double REDUNDANT = 1e-12;  // operator.rs:21
+// Largest small super-block factored densely on the device. Beyond it the small coordinates keep
+// Jacobi, as the reference does when the dense factor costs more than a few PCG iterations
+// (solve.rs:541-548 defer_small); the converged answer is the same within the tolerance.
+constexpr size_t DENSE_SMALL_MAX = 1024;
+// Refinement: an FP32 inner solve stops once its preconditioned residual fell by this factor
+// (squared), well above FP32 rounding; the FP64 true residual then restarts it.
+constexpr double REFINE_DROP = 1e-9;
+constexpr int REFINE_ROUNDS = 12;
+
+inline int grid_for(size_t total) {
+    size_t b = (total + THREADS - 1) / THREADS;
+    return int(std::max<size_t>(1, std::min<size_t>(b, size_t(GRID_T) * 4)));
+}
+
+struct DevTiles {
+    DBuf<u32> k0, k1, e0, e1, fix_k, fix_p0, fix_np;
+    DBuf<int> part, fixidx;
+    u32 n = 0, nfix = 0, nparts = 0;
+    void upload(const TileList& t, cudaStream_t s) {
+        k0.upload(t.k0, s);
+        k1.upload(t.k1, s);
+        e0.upload(t.e0, s);
+        e1.upload(t.e1, s);
+        part.upload(t.part, s);
+        fixidx.upload(t.fixidx, s);
+        fix_k.upload(t.fix_k, s);
+        fix_p0.upload(t.fix_p0, s);
+        fix_np.upload(t.fix_np, s);
+        n = u32(t.k0.size());
+        nfix = u32(t.fix_k.size());
+        nparts = t.nparts;
+    }
+    TileSet set() const { return TileSet{n, k0.p, k1.p, e0.p, e1.p, part.p, fixidx.p, nfix, fix_k.p, fix_p0.p, fix_np.p, nparts}; }
+};
+
+struct DevWarpTiles {
+    DBuf<u32> k0, k1, e0, e1;
+    u32 n = 0;
+    void upload(const WarpTileList& t, cudaStream_t s) {
+        k0.upload(t.k0, s);
+        k1.upload(t.k1, s);
+        e0.upload(t.e0, s);
+        e1.upload(t.e1, s);
+        n = u32(t.k0.size());
+    }
+    WarpTiles set() const { return WarpTiles{n, k0.p, k1.p, e0.p, e1.p}; }
+};
+
+// Dynamic shared memory of the warp-tile kernels for a chunk of Rc columns.
+inline size_t wseg_smem(int Rc, size_t tsz, u32 ms_acc) { return WPB * (wseg_bytes(Rc, tsz) + size_t(ms_acc) * Rc * tsz); }
+inline size_t wrows_smem(int Rc, u32 ms_acc) {
+    return WPB * (wrows_bytes(Rc) + size_t(ms_acc) * Rc * 8 + 2 * size_t(Rc) * 8);
+}
+}  // namespace
+
+struct Scratch {
+    // structure
+    DBuf<u32> seg_off, coord, cell_row, pl_off, pl_cell, pl_seg, pl_other;
+    DevTiles seg_tiles, pull_tiles;      // CTA tiles of the long lists
+    DevWarpTiles wseg, wpull;            // warp tiles of the short lists
+    u32 ms_acc = 0, ns_acc = 0;  // small coordinates / blocks summed in the segment passes
+    // weights
+    DBuf<double> w_rows, cell_w, n1inv, nr, inv_diag, minv;
+    // solve (FP64)
+    DBuf<double> rows, rhs, b1, coefs, r, z, p, q, t, part, cta, cta2, colsum, along, small;
+    // inner FP32 buffers of the refined solve
+    DBuf<float> fx, fb, fr, fz, fp, fq, ft, fpart, frhs, fx0, fsmall;
+    DBuf<double> cg_rho, cg_rho_new, cg_pq, cg_gamma, cg_beta, cg_xb, cg_ss1, cg_floor, cg_ring, cg_xconst, cg_pfloor;
+    DBuf<int> cg_active, cg_nactive;
+    int* h_nactive = nullptr;  // pinned
+    // phase timing
+    bool prof = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ev_slot;
+    double ms[GpuAbsorber::P_NSLOTS] = {};
+    u64 cnt[GpuAbsorber::P_NSLOTS] = {};
+    std::vector<cudaEvent_t> pool_;
+    u64 launches = 0;
+
+    DevStruct ds(const HostStructure& hs) const {
+        DevStruct s{};
+        s.M = u32(hs.ncells);
+        s.g1 = hs.g1;
+        s.nb = u32(hs.nb());
+        s.m = u32(hs.m);
+        s.ms = u32(hs.m_small);
+        s.ms_acc = ms_acc;
+        s.ns_acc = ns_acc;
+        s.seg_off = seg_off.p;
+        s.coord = coord.p;
+        s.cell_row = cell_row.p;
+        s.pl_off = pl_off.p;
+        s.pl_cell = pl_cell.p;
+        s.pl_seg = pl_seg.p;
+        s.pl_other = pl_other.p;
+        s.seg = seg_tiles.set();
+        s.pull = pull_tiles.set();
+        return s;
+    }
+    DevWeights dw() const { return DevWeights{w_rows.p, cell_w.p, n1inv.p, nr.p}; }
+    CgState cg() {
+        return CgState{cg_rho.p, cg_rho_new.p, cg_pq.p,   cg_gamma.p,  cg_beta.p,   cg_xb.p,     cg_ss1.p,
+                       cg_floor.p, cg_ring.p, cg_xconst.p, cg_pfloor.p, cg_active.p, cg_nactive.p};
+    }
+    cudaEvent_t get_event() {
+        if (!pool_.empty()) {
+            cudaEvent_t e = pool_.back();
+            pool_.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        return e;
+    }
+    int begin(int slot, cudaStream_t st) {
+        if (!prof) return -1;
+        cudaEvent_t a = get_event();
+        CK(cudaEventRecord(a, st));
+        ev.push_back(a);
+        ev.push_back(nullptr);
+        ev_slot.push_back(slot);
+        return int(ev.size()) - 2;
+    }
+    void end(int h, cudaStream_t st) {
+        if (h < 0) return;
+        cudaEvent_t b = get_event();
+        CK(cudaEventRecord(b, st));
+        ev[size_t(h) + 1] = b;
+    }
+    void collect() {
+        for (size_t i = 0; i + 1 < ev.size(); i += 2) {
+            float t = 0;
+            if (ev[i + 1]) {
+                CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+                ms[ev_slot[i / 2]] += t;
+                cnt[ev_slot[i / 2]]++;
+                pool_.push_back(ev[i + 1]);
+            }
+            pool_.push_back(ev[i]);
+        }
+        ev.clear();
+        ev_slot.clear();
+    }
+    ~Scratch() {
+        if (h_nactive) cudaFreeHost(h_nactive);
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+        for (auto e : pool_) cudaEventDestroy(e);
+    }
+};
+
+GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector<u32>& g, const double* w, size_t n,
+                         const Ctx& ctx)
+    : g_(g), ctx_(ctx) {
+    for (size_t q = 0; q < codes.size(); q++)
+        for (size_t i = 0; i < n; i++)
+            if (codes[q][i] >= g[q]) throw Error(RC_INVALID_INPUT, "term code out of range of its level count");
+    if (w)
+        for (size_t i = 0; i < n; i++)
+            if (!(std::isfinite(w[i]) && w[i] > 0.0)) throw Error(RC_INVALID_INPUT, "weights must be positive and finite");
+    hs_ = build_structure(codes, g, n, SMALL_LIMIT);
+    norm_fe1_ = fe1_index(g);
+    ctx_.check();
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    d_ = std::make_unique<Scratch>();
+    CK(cudaHostAlloc(&d_->h_nactive, sizeof(int), cudaHostAllocDefault));
+    d_->seg_off.upload(hs_.seg_off, stream_);
+    d_->coord.upload(hs_.coord, stream_);
+    if (!hs_.trivial()) d_->cell_row.upload(hs_.cell_row, stream_);
+    {
+        // segments weigh max(cells, rows): short ones go to warp tiles, the others to CTA tiles
+        std::vector<u32> wgt(hs_.g1);
+        for (u32 s = 0; s < hs_.g1; s++) {
+            const u32 c0 = hs_.seg_off[s], c1 = hs_.seg_off[s + 1];
+            const u32 rows = hs_.trivial() ? c1 - c0 : hs_.cell_row[c1] - hs_.cell_row[c0];
+            wgt[s] = std::max(c1 - c0, rows);
+        }
+        WarpTileList wt;
+        TileList ct;
+        split_tiles(hs_.seg_off, &wgt, 0, hs_.g1, WT, WT, TILE, wt, ct);
+        d_->wseg.upload(wt, stream_);
+        d_->seg_tiles.upload(ct, stream_);
+        CK(cudaStreamSynchronize(stream_));
+    }
+    {
+        u32 ns = 0;
+        for (auto& b : hs_.blocks) ns += b.small;
+        if (hs_.m_small > 0 && hs_.m_small <= size_t(SACC_MAX) && ns <= u32(SACC_BLOCKS)) {
+            d_->ms_acc = u32(hs_.m_small);
+            d_->ns_acc = ns;
+        }
+    }
+    if (hs_.m > 0) {
+        PullTable pt = build_pull_table(hs_);
+        d_->pl_off.upload(pt.off, stream_);
+        d_->pl_cell.upload(pt.cell, stream_);
+        d_->pl_seg.upload(pt.seg, stream_);
+        d_->pl_other.upload(pt.other, stream_);
+        WarpTileList wt;
+        TileList ct;
+        split_tiles(pt.off, nullptr, d_->ms_acc, u32(hs_.m), PULL_WARP_MAX, 32, TILE, wt, ct);
+        d_->wpull.upload(wt, stream_);
+        d_->pull_tiles.upload(ct, stream_);
+        CK(cudaStreamSynchronize(stream_));  // host tables die here
+    }
+    CK(cudaStreamSynchronize(stream_));
+    refresh_weights(w);
+}
+
+GpuAbsorber::~GpuAbsorber() {
+    d_.reset();
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+bool GpuAbsorber::weights(double* out) const {
+    if (!weighted_) return false;
+    if (out) std::copy(w_rows_.begin(), w_rows_.end(), out);
+    return true;
+}
+
+// operator.rs:211-338 refresh_weights + :344-570 level_weights (host form).
+void GpuAbsorber::refresh_weights(const double* w_kept) {
+    const HostStructure& st = hs_;
+    weighted_ = w_kept != nullptr;
+    w_rows_.clear();
+    cell_w_.clear();
+    if (w_kept) {
+        w_rows_.resize(st.n);
+        for (size_t r = 0; r < st.n; r++) w_rows_[r] = w_kept[st.pi[r]];
+    }
+    if (!st.trivial()) {
+        cell_w_.resize(st.ncells);
+        for (size_t c = 0; c < st.ncells; c++) {
+            double s = 0;
+            for (u32 r = st.cell_row[c]; r < st.cell_row[c + 1]; r++) s += w_kept ? w_rows_[r] : 1.0;
+            cell_w_[c] = s;
+        }
+    } else if (w_kept) {
+        cell_w_ = w_rows_;
+    }
+    auto cw = [&](size_t c) { return cell_w_.empty() ? 1.0 : cell_w_[c]; };
+    const size_t M = st.ncells, nb = st.nb(), m = st.m;
+    n1_.assign(st.g1, 0.0);
+    for (u32 s = 0; s < st.g1; s++) {
+        double a = 0;
+        for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++) a += cw(c);
+        n1_[s] = a;
+    }
+    sw_ = 0;
+    for (double v : n1_) sw_ += v;
+    nr_.assign(m, 0.0);
+    std::vector<double> dq(m, 0.0), cs(m, 0.0);
+    for (u32 s = 0; s < st.g1; s++) {
+        const u32 c0 = st.seg_off[s], c1 = st.seg_off[s + 1];
+        for (u32 c = c0; c < c1; c++)
+            for (size_t b = 0; b < nb; b++) cs[st.coord[b * M + c]] += cw(c);
+        for (u32 c = c0; c < c1; c++)
+            for (size_t b = 0; b < nb; b++) {
+                const u32 k = st.coord[b * M + c];
+                nr_[k] += cw(c);
+                dq[k] += cw(c) * cs[k] / n1_[s];
+            }
+        for (u32 c = c0; c < c1; c++)
+            for (size_t b = 0; b < nb; b++) cs[st.coord[b * M + c]] = 0.0;
+    }
+    diag_.resize(m);
+    red_.resize(m);
+    for (size_t k = 0; k < m; k++) {
+        diag_[k] = nr_[k] - dq[k];
+        red_[k] = diag_[k] <= REDUNDANT * nr_[k];
+    }
+    pre_fresh_ = false;
+    upload_weights();
+}
+
+void GpuAbsorber::upload_weights() {
+    if (weighted_) d_->w_rows.upload(w_rows_, stream_);
+    else d_->w_rows.release();
+    if (!cell_w_.empty()) d_->cell_w.upload(cell_w_, stream_);
+    else d_->cell_w.release();
+    std::vector<double> inv(n1_.size());
+    for (size_t s = 0; s < n1_.size(); s++) inv[s] = 1.0 / n1_[s];
+    d_->n1inv.upload(inv, stream_);
+    d_->nr.upload(nr_, stream_);
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void GpuAbsorber::set_weights(const double* w_rows) {
+    ctx_.check();
+    std::vector<double> kept;
+    if (w_rows) {
+        kept.resize(hs_.n);
+        for (size_t r = 0; r < hs_.n; r++) {
+            if (!(std::isfinite(w_rows[r]) && w_rows[r] > 0.0))
+                throw Error(RC_INVALID_INPUT, "weights must be positive and finite");
+            kept[hs_.pi[r]] = w_rows[r];
+        }
+    }
+    refresh_weights(w_rows ? kept.data() : nullptr);
+}
+
+void GpuAbsorber::weight_state(double* n1, double* nr, double* diag, uint8_t* red, double* sw) const {
+    if (n1) std::copy(n1_.begin(), n1_.end(), n1);
+    if (nr) std::copy(nr_.begin(), nr_.end(), nr);
+    if (diag) std::copy(diag_.begin(), diag_.end(), diag);
+    if (red) std::copy(red_.begin(), red_.end(), red);
+    if (sw) *sw = sw_;
+}
+
+// Jacobi entries (precond/jacobi.rs:7) and the exact dense factor of the small super-block
+// (precond/dense.rs:79-160): S_SS assembled on the host (operator.rs:1457-1523), scaled to unit
+// diagonal over the kept coordinates, factored with grounding and inverted on the device.
+void GpuAbsorber::ensure_precond() {
+    if (pre_fresh_) return;
+    const HostStructure& st = hs_;
+    const size_t m = st.m, ms = st.m_small, M = st.ncells;
+    std::vector<double> inv(m);
+    for (size_t i = 0; i < m; i++) inv[i] = (red_[i] || !(diag_[i] > 0.0)) ? 0.0 : 1.0 / diag_[i];
+    d_->inv_diag.upload(inv, stream_);
+    small_ok_ = false;
+    if (ms > 0 && ms <= DENSE_SMALL_MAX) {
+        auto cw = [&](size_t c) { return cell_w_.empty() ? 1.0 : cell_w_[c]; };
+        size_t ns = 0;
+        for (auto& b : st.blocks) ns += b.small;
+        std::vector<double> a(ms * ms, 0.0), cs(ms, 0.0);
+        std::vector<u32> touched;
+        for (u32 s = 0; s < st.g1; s++) {
+            touched.clear();
+            for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++) {
+                const double w = cw(c);
+                for (size_t b = 0; b < ns; b++) {
+                    const u32 k = st.coord[b * M + c];
+                    if (cs[k] == 0.0) touched.push_back(k);
+                    cs[k] += w;
+                    a[k * ms + k] += w;
+                    for (size_t b2 = 0; b2 < ns; b2++)
+                        if (b2 != b) a[k * ms + st.coord[b2 * M + c]] += w;
+                }
+            }
+            std::sort(touched.begin(), touched.end());
+            touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+            const double inv1 = 1.0 / n1_[s];
+            for (u32 k : touched)
+                for (u32 l : touched) a[size_t(k) * ms + l] -= cs[k] * cs[l] * inv1;
+            for (u32 k : touched) cs[k] = 0.0;
+        }
+        std::vector<u32> keep;
+        for (size_t i = 0; i < ms; i++)
+            if (!red_[i] && a[i * ms + i] > 0.0) keep.push_back(u32(i));
+        const size_t k = keep.size();
+        std::vector<double> scale(k), ak(k * k);
+        for (size_t i = 0; i < k; i++) scale[i] = 1.0 / std::sqrt(a[size_t(keep[i]) * (ms + 1)]);
+        for (size_t i = 0; i < k; i++)
+            for (size_t j = 0; j < k; j++) ak[i * k + j] = a[size_t(keep[i]) * ms + keep[j]] * scale[i] * scale[j];
+        DBuf<double> da, dd, dx, dscale;
+        DBuf<u32> dkeep;
+        d_->minv.alloc(ms * ms);
+        CK(cudaMemsetAsync(d_->minv.p, 0, ms * ms * sizeof(double), stream_));
+        if (k > 0) {
+            da.upload(ak, stream_);
+            dd.alloc(k);
+            dx.alloc(k * k);
+            dscale.upload(scale, stream_);
+            dkeep.upload(keep, stream_);
+            k_ldlt_ground<<<1, 1024, 0, stream_>>>(da.p, dd.p, int(k));
+            CK(cudaGetLastError());
+            k_ldlt_inverse<<<int((k + 127) / 128), 128, 0, stream_>>>(da.p, dd.p, int(k), dx.p);
+            CK(cudaGetLastError());
+            k_expand_minv<<<grid_for(k * k), THREADS, 0, stream_>>>(dx.p, dkeep.p, dscale.p, int(k), u32(ms), d_->minv.p);
+            CK(cudaGetLastError());
+            d_->launches += 3;
+        }
+        CK(cudaStreamSynchronize(stream_));
+        small_ok_ = true;
+    }
+    pre_fresh_ = true;
+}
+
+namespace {
+
+// Lets `kernel` take `bytes` of dynamic shared memory (beyond the 48 KB default).
+template <class K>
+void allow_smem(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+}
+
+// Per-CTA partial rows of the small coordinates: GRID_S rows of the short-segment kernels, then
+// GRID_T rows of the long-segment tiles, then GRID_T rows of the long-segment slices.
+inline size_t small_rows() { return size_t(GRID_S) + 2 * size_t(GRID_T); }
+
+template <class T>
+void launch_small_reduce(Scratch& d, const DevStruct& S, T* small, int R, T* Y, cudaStream_t st) {
+    const u32 len = S.ms_acc * u32(R);
+    T* sb = small + size_t(GRID_S) * len;
+    T* sc = sb + size_t(GRID_T) * len;
+    k_small_reduce<T><<<std::max<u32>(1, std::min<u32>((len + 7) / 8, GRID_V)), THREADS, 0, st>>>(
+        small, GRID_S, S.seg.n ? sb : nullptr, GRID_T, S.seg.nfix ? sc : nullptr, GRID_T, len, Y);
+    d.launches++;
+}
+
+// Y = S P. Short segments: one thread per (segment, column) (t, small coordinates); long
+// segments: tiles (t; slices' partials completed by k_fix, then their small coordinates).
+// Short coordinate lists: one thread per (coordinate, column); long ones: tiles and k_fix.
+// The small coordinates' partial rows are summed last.
+template <class T>
+void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* P, int R, T* Y, T* t, T* part,
+                  T* small, cudaStream_t st) {
+    const int h = d.begin(GpuAbsorber::P_APPLY, st);
+    const bool acc = S.ms_acc > 0;
+    const u32 len = S.ms_acc * u32(R);
+    if (d.wseg.n)
+        for (int j0 = 0; j0 < R; j0 += WCOLS) {
+            const int Rc = std::min(WCOLS, R - j0);
+            const size_t shm = wseg_smem(Rc, sizeof(T), S.ms_acc);
+            allow_smem(k_wseg_apply<T>, shm);
+            k_wseg_apply<T><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), P, R, j0, Rc, t, acc ? small : nullptr);
+            d.launches++;
+        }
+    else if (acc)
+        CK(cudaMemsetAsync(small, 0, size_t(GRID_S) * len * sizeof(T), st));
+    if (S.seg.n) {
+        T* sb = small + size_t(GRID_S) * len;
+        k_seg_apply<T><<<GRID_T, THREADS, 0, st>>>(S, W, P, R, t, part, false, acc ? sb : nullptr);
+        d.launches++;
+        if (S.seg.nfix) {
+            k_fix<T><<<std::min<u32>(S.seg.nfix, GRID_T), THREADS, 0, st>>>(S.seg, W, P, part, R, 1, t);
+            d.launches++;
+            if (acc) {
+                k_seg_small_slices<T><<<GRID_T, THREADS, 0, st>>>(S, W, P, t, R, sb + size_t(GRID_T) * len);
+                d.launches++;
+            }
+        }
+    }
+    if (d.wpull.n)
+        for (int j0 = 0; j0 < R; j0 += WCOLS) {
+            const int Rc = std::min(WCOLS, R - j0);
+            k_wpull_apply<T><<<GRID_S, WPB * 32, 0, st>>>(S, W, d.wpull.set(), P, t, R, j0, Rc, Y);
+            d.launches++;
+        }
+    if (S.pull.n) {
+        k_pull_apply<T><<<GRID_T, THREADS, 0, st>>>(S, W, P, t, R, Y, part);
+        d.launches++;
+        if (S.pull.nfix) {
+            k_fix<T><<<std::min<u32>(S.pull.nfix, GRID_T), THREADS, 0, st>>>(S.pull, W, P, part, R, 0, Y);
+            d.launches++;
+        }
+    }
+    if (acc) launch_small_reduce<T>(d, S, small, R, Y, st);
+    CK(cudaGetLastError());
+    d.end(h, st);
+}
+
+template <class T>
+void launch_precond(Scratch& d, const DevStruct& S, bool small_ok, const T* r, T* z, int R, cudaStream_t st) {
+    const int h = d.begin(GpuAbsorber::P_PRECOND, st);
+    const u32 ms = small_ok ? S.ms : 0;
+    if (S.m > ms) {
+        k_jacobi<T><<<grid_for(size_t(S.m - ms) * R), THREADS, 0, st>>>(r, z, d.inv_diag.p, ms, S.m, R);
+        d.launches++;
+    }
+    if (ms > 0) {
+        k_small_apply<T><<<grid_for(size_t(ms) * R), THREADS, 0, st>>>(d.minv.p, ms, r, z, R);
+        d.launches++;
+    }
+    CK(cudaGetLastError());
+    d.end(h, st);
+}
+
+void reduce_cols(Scratch& d, const double* part, int nparts, int ncols, double* out, cudaStream_t st,
+                 const double* part2 = nullptr, int nparts2 = 0) {
+    k_reduce_cols<<<std::max(1, std::min(GRID_V, (ncols + 7) / 8)), THREADS, 0, st>>>(part, nparts, part2, nparts2,
+                                                                                       ncols, out);
+    d.launches++;
+    CK(cudaGetLastError());
+}
+
+// rhs pass: b1 per segment, [sum w v^2, sum w v, sum b1^2/n1] per column into colsum (3R), and
+// the reduced right-hand side (small coordinates in the segment passes, the others pulled).
+void launch_rhs(Scratch& d, const DevStruct& S, const DevWeights& W, const double* rows, int R, double* b1,
+                double* rhs, double* colsum, cudaStream_t st) {
+    const bool acc = S.ms_acc > 0;
+    const u32 len = S.ms_acc * u32(R);
+    double* small = d.small.p;
+    int h = d.begin(GpuAbsorber::P_RHS_SEG, st);
+    if (d.wseg.n) {
+        for (int j0 = 0; j0 < R; j0 += WCOLS) {
+            const int Rc = std::min(WCOLS, R - j0);
+            const size_t shm = wrows_smem(Rc, S.ms_acc);
+            allow_smem(k_wseg_rhs, shm);
+            k_wseg_rhs<<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, b1, d.cta2.p,
+                                                       acc ? small : nullptr);
+            d.launches++;
+        }
+    } else {
+        CK(cudaMemsetAsync(d.cta2.p, 0, size_t(GRID_S) * 2 * R * sizeof(double), st));
+        if (acc) CK(cudaMemsetAsync(small, 0, size_t(GRID_S) * len * sizeof(double), st));
+    }
+    if (S.seg.n) {
+        double* sb = small + size_t(GRID_S) * len;
+        k_seg_rhs<<<GRID_T, THREADS, 0, st>>>(S, W, rows, R, b1, d.part.p, d.cta.p, acc ? sb : nullptr);
+        d.launches++;
+        if (S.seg.nfix) {
+            k_fix<double><<<std::min<u32>(S.seg.nfix, GRID_T), THREADS, 0, st>>>(S.seg, W, nullptr, d.part.p, R, 2, b1);
+            d.launches++;
+            if (acc) {
+                k_rhs_small_slices<<<GRID_T, THREADS, 0, st>>>(S, W, rows, b1, R, sb + size_t(GRID_T) * len);
+                d.launches++;
+            }
+        }
+    }
+    d.end(h, st);
+    h = d.begin(GpuAbsorber::P_VECTOR, st);
+    reduce_cols(d, d.cta2.p, GRID_S, 2 * R, colsum, st, S.seg.n ? d.cta.p : nullptr, GRID_T);
+    k_b1sq<<<GRID_V, THREADS, 0, st>>>(S.g1, b1, W.n1inv, R, d.cta.p);
+    d.launches++;
+    reduce_cols(d, d.cta.p, GRID_V, R, colsum + 2 * R, st);
+    d.end(h, st);
+    if (S.m > 0) {
+        h = d.begin(GpuAbsorber::P_RHS_PULL, st);
+        if (d.wpull.n)
+            for (int j0 = 0; j0 < R; j0 += WCOLS) {
+                const int Rc = std::min(WCOLS, R - j0);
+                k_wpull_rhs<<<GRID_S, WPB * 32, 0, st>>>(S, W, d.wpull.set(), rows, b1, R, j0, Rc, rhs);
+                d.launches++;
+            }
+        if (S.pull.n) {
+            k_pull_rhs<<<GRID_T, THREADS, 0, st>>>(S, W, rows, b1, R, rhs, d.part.p);
+            d.launches++;
+            if (S.pull.nfix) {
+                k_fix<double><<<std::min<u32>(S.pull.nfix, GRID_T), THREADS, 0, st>>>(S.pull, W, nullptr, d.part.p, R, 2, rhs);
+                d.launches++;
+            }
+        }
+        if (acc) launch_small_reduce<double>(d, S, small, R, rhs, st);
+        d.end(h, st);
+    }
+    CK(cudaGetLastError());
+}
+
+}  // namespace
+
+void GpuAbsorber::apply_host(const double* p, size_t r, double* y) {
+    const size_t m = hs_.m;
+    const DevStruct S = d_->ds(hs_);
+    d_->p.alloc(m * r);
+    d_->q.alloc(m * r);
+    d_->t.alloc(size_t(hs_.g1) * r);
+    d_->part.alloc(std::max<size_t>(1, size_t(std::max(S.seg.nparts, S.pull.nparts)) * r));
+    d_->small.alloc(std::max<size_t>(1, small_rows() * d_->ms_acc * r));
+    CK(cudaMemcpyAsync(d_->p.p, p, m * r * 8, cudaMemcpyHostToDevice, stream_));
+    launch_apply<double>(*d_, S, d_->dw(), d_->p.p, int(r), d_->q.p, d_->t.p, d_->part.p, d_->small.p, stream_);
+    CK(cudaMemcpyAsync(y, d_->q.p, m * r * 8, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    d_->collect();
+}
+
+void GpuAbsorber::precond_host(const double* rr, size_t r, double* z) {
+    ensure_precond();
+    const size_t m = hs_.m;
+    d_->r.alloc(m * r);
+    d_->z.alloc(m * r);
+    CK(cudaMemcpyAsync(d_->r.p, rr, m * r * 8, cudaMemcpyHostToDevice, stream_));
+    launch_precond<double>(*d_, d_->ds(hs_), small_ok_, d_->r.p, d_->z.p, int(r), stream_);
+    CK(cudaMemcpyAsync(z, d_->z.p, m * r * 8, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    d_->collect();
+}
+
+void GpuAbsorber::rhs_host(const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum) {
+    const size_t n = hs_.n, m = hs_.m, g1 = hs_.g1;
+    const DevStruct S = d_->ds(hs_);
+    d_->rows.alloc(n * r);
+    d_->rhs.alloc(std::max<size_t>(1, m * r));
+    d_->b1.alloc(g1 * r);
+    d_->part.alloc(std::max<size_t>(1, size_t(std::max(S.seg.nparts, S.pull.nparts)) * r));
+    d_->cta.alloc(size_t(std::max(GRID_T, GRID_V)) * 3 * r);
+    d_->cta2.alloc(size_t(GRID_S) * 2 * r);
+    d_->colsum.alloc(3 * r);
+    d_->small.alloc(std::max<size_t>(1, small_rows() * d_->ms_acc * r));
+    CK(cudaMemcpyAsync(d_->rows.p, rows, n * r * 8, cudaMemcpyHostToDevice, stream_));
+    launch_rhs(*d_, S, d_->dw(), d_->rows.p, int(r), d_->b1.p, d_->rhs.p, d_->colsum.p, stream_);
+    if (m > 0) CK(cudaMemcpyAsync(y, d_->rhs.p, m * r * 8, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(b1, d_->b1.p, g1 * r * 8, cudaMemcpyDeviceToHost, stream_));
+    std::vector<double> cs(3 * r);
+    CK(cudaMemcpyAsync(cs.data(), d_->colsum.p, 3 * r * 8, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    d_->collect();
+    for (size_t j = 0; j < r; j++) {
+        wsq[j] = cs[j];
+        wsum[j] = cs[r + j];
+    }
+}
+
+SolveInfo GpuAbsorber::residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
+                                   double* coefs, Precision prec) {
+    const size_t n = hs_.n;
+    d_->rows.alloc(std::max<size_t>(1, n * r));
+    int h = d_->begin(P_H2D, stream_);
+    CK(cudaMemcpyAsync(d_->rows.p, z, n * r * 8, cudaMemcpyHostToDevice, stream_));
+    d_->end(h, stream_);
+    SolveInfo info = solve(d_->rows.p, r, tol, maxiter, want_coefs, warm, coefs, prec);
+    h = d_->begin(P_D2H, stream_);
+    CK(cudaMemcpyAsync(z, d_->rows.p, n * r * 8, cudaMemcpyDeviceToHost, stream_));
+    d_->end(h, stream_);
+    CK(cudaStreamSynchronize(stream_));
+    d_->collect();
+    return info;
+}
+
+SolveInfo GpuAbsorber::residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
+                                          const double* warm, double* coefs, Precision prec) {
+    return solve(z_dev, r, tol, maxiter, want_coefs, warm, coefs, prec);
+}
+
+// One PCG run (cg.rs:132-292) on the m x R system S d = b in precision T, from d = 0 unless
+// `x_is_start` (then d holds the start and b - S d is formed first). The stopping rule tests the
+// FP64 quantities of the full iterate x0 + d: ss_k = ss1 - (x0'rhs + d'rhs + x0'r + d'r), with
+// x0'rhs in cg_xconst and x0 (as T) in `x0` (null when d is the whole iterate). With `drop` > 0
+// a column also stops (state 2: another refinement round) once its preconditioned residual fell
+// by that factor. Returns the iterations run.
+template <class T>
+static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x, const T* b,
+                   const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small, int R, double tol,
+                   double drop, u64 iters_done, size_t maxiter, bool x_is_start, const Ctx& ctx, cudaStream_t st) {
+    const size_t m = S.m, tot = m * size_t(R);
+    CgState cg = d.cg();
+    if (x_is_start) {
+        launch_apply<T>(d, S, W, x, R, q, t, part, small, st);
+        k_sub<T><<<grid_for(tot), THREADS, 0, st>>>(r, b, q, tot);
+        d.launches++;
+    } else {
+        CK(cudaMemcpyAsync(r, b, tot * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    }
+    launch_precond<T>(d, S, small_ok, r, z, R, st);
+    int h = d.begin(GpuAbsorber::P_VECTOR, st);
+    k_dot<T><<<GRID_V, THREADS, 0, st>>>(r, z, u32(m), R, d.cta.p);
+    reduce_cols(d, d.cta.p, GRID_V, R, d.cg_rho.p, st);
+    k_cg_start<<<1, THREADS, 0, st>>>(cg, R, drop);
+    k_mask_copy<T><<<grid_for(tot), THREADS, 0, st>>>(p, z, d.cg_active.p, tot, R);
+    d.launches += 3;
+    CK(cudaMemcpyAsync(d.h_nactive, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    d.end(h, st);
+    CK(cudaStreamSynchronize(st));
+    bool any_active = *d.h_nactive > 0;
+    u64 it = 0;
+    int k = 0;
+    while (any_active) {
+        if (iters_done + it >= maxiter) {
+            std::ostringstream os;
+            os << "convergence not achieved in " << maxiter << " iterations";
+            throw Error(RC_CONVERGENCE, os.str());
+        }
+        ctx.check();
+        launch_apply<T>(d, S, W, p, R, q, t, part, small, st);
+        h = d.begin(GpuAbsorber::P_VECTOR, st);
+        k_dot<T><<<GRID_V, THREADS, 0, st>>>(p, q, u32(m), R, d.cta.p);
+        reduce_cols(d, d.cta.p, GRID_V, R, d.cg_pq.p, st);
+        k_cg_gamma<<<1, THREADS, 0, st>>>(cg, R);
+        k_update_xr<T><<<GRID_V, THREADS, 0, st>>>(x, r, p, q, rhs_true, x0, d.cg_gamma.p, u32(m), R, d.cta.p);
+        reduce_cols(d, d.cta.p, GRID_V, 3 * R, d.cg_xb.p, st);
+        d.launches += 3;
+        d.end(h, st);
+        launch_precond<T>(d, S, small_ok, r, z, R, st);
+        h = d.begin(GpuAbsorber::P_VECTOR, st);
+        k_dot<T><<<GRID_V, THREADS, 0, st>>>(r, z, u32(m), R, d.cta.p);
+        reduce_cols(d, d.cta.p, GRID_V, R, d.cg_rho_new.p, st);
+        it++;
+        k++;
+        k_cg_stop<<<1, THREADS, 0, st>>>(cg, R, k, tol);
+        k_update_p<T><<<grid_for(tot), THREADS, 0, st>>>(p, z, d.cg_beta.p, d.cg_active.p, u32(m), R);
+        d.launches += 3;
+        CK(cudaMemcpyAsync(d.h_nactive, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        d.end(h, st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        any_active = *d.h_nactive > 0;
+    }
+    return it;
+}
+
+// solve.rs:1141-1311 residualize.
+SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
+                             double* coefs, Precision prec) {
+    SolveInfo info;
+    const size_t m = hs_.m, g1 = hs_.g1;
+    if (r == 0) {
+        info.iterations = 1;
+        info.exact = true;
+        return info;
+    }
+    ctx_.check();
+    ensure_precond();
+    const int R = int(r);
+    const DevStruct S = d_->ds(hs_);
+    const DevWeights W = d_->dw();
+    cudaStream_t st = stream_;
+    Scratch& d = *d_;
+    const size_t nparts = std::max<size_t>(1, size_t(std::max(S.seg.nparts, S.pull.nparts)));
+    d.rhs.alloc(std::max<size_t>(1, m * r));
+    d.b1.alloc(g1 * r);
+    d.coefs.alloc((m + g1) * r);
+    d.part.alloc(nparts * r);
+    d.cta.alloc(size_t(std::max(GRID_T, GRID_V)) * 3 * r);
+    d.colsum.alloc(3 * r);
+    d.t.alloc(g1 * r);
+    d.cta2.alloc(size_t(GRID_S) * 2 * r);
+    d.small.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * r));
+    launch_rhs(d, S, W, rows, R, d.b1.p, d.rhs.p, d.colsum.p, st);
+    std::vector<double> cs(3 * r);
+    CK(cudaMemcpyAsync(cs.data(), d.colsum.p, 3 * r * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    ctx_.check();
+    std::vector<double> ss0(r), ss1(r);
+    for (size_t j = 0; j < r; j++) {  // solve.rs:1210-1217
+        const double wsq = cs[j], wsum = cs[r + j], b1sq = cs[2 * r + j];
+        const double s = wsq - wsum * wsum / sw_;
+        ss0[j] = s > 1e-15 * wsq ? s : 0.0;
+        ss1[j] = wsq - b1sq;
+    }
+    double* x = d.coefs.p;
+    if (warm) {
+        std::vector<double> w0(warm, warm + m * r);
+        for (size_t j = 0; j < r; j++)
+            if (ss0[j] == 0.0)
+                for (size_t i = 0; i < m; i++) w0[i * r + j] = 0.0;
+        if (m > 0) CK(cudaMemcpyAsync(x, w0.data(), m * r * 8, cudaMemcpyHostToDevice, st));
+    } else if (m > 0) {
+        CK(cudaMemsetAsync(x, 0, m * r * 8, st));
+    }
+    u64 iterations = 1;
+    bool exact = true;
+    if (m > 0) {
+        const size_t tot = m * r;
+        d.r.alloc(tot);
+        d.z.alloc(tot);
+        d.p.alloc(tot);
+        d.q.alloc(tot);
+        for (auto* b : {&d.cg_rho, &d.cg_rho_new, &d.cg_pq, &d.cg_gamma, &d.cg_beta, &d.cg_ss1, &d.cg_floor, &d.cg_xconst,
+                        &d.cg_pfloor})
+            b->alloc(r);
+        d.cg_xb.alloc(3 * r);
+        d.cg_ring.alloc(r * WINDOW);
+        d.cg_active.alloc(r);
+        d.cg_nactive.alloc(1);
+        std::vector<int> act(r);
+        std::vector<double> fl(r), zero(r, 0.0);
+        for (size_t j = 0; j < r; j++) {
+            act[j] = ss0[j] > 0.0;
+            fl[j] = 1e-26 * ss0[j];
+        }
+        CK(cudaMemcpyAsync(d.cg_active.p, act.data(), r * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.cg_ss1.p, ss1.data(), r * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.cg_floor.p, fl.data(), r * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.cg_xconst.p, zero.data(), r * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(d.cg_ring.p, 0, r * WINDOW * 8, st));
+        const bool exact_pre = small_ok_ && hs_.m_small == hs_.m;
+        if (exact_pre) {
+            // x* = x + M^-1 (rhs - S x) (cg.rs:171-198)
+            if (warm) {
+                launch_apply<double>(d, S, W, x, R, d.q.p, d.t.p, d.part.p, d.small.p, st);
+                k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhs.p, d.q.p, tot);
+                d.launches++;
+            } else {
+                CK(cudaMemcpyAsync(d.r.p, d.rhs.p, tot * 8, cudaMemcpyDeviceToDevice, st));
+            }
+            launch_precond<double>(d, S, small_ok_, d.r.p, d.z.p, R, st);
+            k_add_active<double><<<grid_for(tot), THREADS, 0, st>>>(x, d.z.p, d.cg_active.p, tot, R);
+            d.launches++;
+            CK(cudaGetLastError());
+        } else if (prec == Precision::F64) {
+            iterations = run_pcg<double>(d, S, W, small_ok_, x, d.rhs.p, d.rhs.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p,
+                                         d.t.p, d.part.p, d.small.p, R, tol, 0.0, 0, maxiter,
+                                         warm != nullptr, ctx_, st);
+            exact = false;
+        } else {
+            // FP32 inner PCG on the correction, FP64 true residual between rounds.
+            for (auto* b : {&d.fx, &d.fb, &d.fr, &d.fz, &d.fp, &d.fq, &d.frhs, &d.fx0}) b->alloc(tot);
+            d.ft.alloc(g1 * r);
+            d.fpart.alloc(nparts * r);
+            d.fsmall.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * r));
+            k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.rhs.p, d.frhs.p, tot);
+            d.launches++;
+            iterations = 0;
+            bool start_nonzero = warm != nullptr;
+            for (int round = 0; round < REFINE_ROUNDS; round++) {
+                // true residual b = rhs - S x in FP64, x'rhs, and the FP32 copies
+                if (start_nonzero) {
+                    launch_apply<double>(d, S, W, x, R, d.q.p, d.t.p, d.part.p, d.small.p, st);
+                    k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhs.p, d.q.p, tot);
+                    d.launches++;
+                } else {
+                    CK(cudaMemcpyAsync(d.r.p, d.rhs.p, tot * 8, cudaMemcpyDeviceToDevice, st));
+                }
+                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.rhs.p, u32(m), R, d.cta.p);
+                reduce_cols(d, d.cta.p, GRID_V, R, d.cg_xconst.p, st);
+                k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.fb.p, tot);
+                k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(x, d.fx0.p, tot);
+                CK(cudaMemsetAsync(d.fx.p, 0, tot * 4, st));
+                CK(cudaMemsetAsync(d.cg_ring.p, 0, r * WINDOW * 8, st));
+                d.launches += 3;
+                iterations += run_pcg<float>(d, S, W, small_ok_, d.fx.p, d.fb.p, d.frhs.p, d.fx0.p, d.fr.p, d.fz.p,
+                                             d.fp.p, d.fq.p, d.ft.p, d.fpart.p, d.fsmall.p, R, tol,
+                                             REFINE_DROP, iterations, maxiter, false, ctx_, st);
+                k_add_correction<<<grid_for(tot), THREADS, 0, st>>>(x, d.fx.p, tot);
+                d.launches++;
+                start_nonzero = true;
+                // columns stopped by the FP32 precision floor go another round
+                CK(cudaMemcpyAsync(act.data(), d.cg_active.p, r * sizeof(int), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                bool again = false;
+                for (size_t j = 0; j < r; j++) again |= act[j] == 2;
+                if (!again) break;
+                for (size_t j = 0; j < r; j++) act[j] = act[j] == 2 ? 1 : 0;
+                CK(cudaMemcpyAsync(d.cg_active.p, act.data(), r * sizeof(int), cudaMemcpyHostToDevice, st));
+            }
+            iterations = std::max<u64>(iterations, 1);
+            exact = false;
+        }
+        if (!exact) {
+            bool all0 = true;
+            for (double s : ss0) all0 &= s == 0.0;
+            exact = all0;
+        }
+    }
+    ctx_.check();
+    int h = d.begin(P_RESID, st);
+    double* alpha = want_coefs ? x + m * r : nullptr;
+    if (d.wseg.n)
+        for (int j0 = 0; j0 < R; j0 += WCOLS) {
+            const int Rc = std::min(WCOLS, R - j0);
+            const size_t shm = wrows_smem(Rc, 0);
+            allow_smem(k_wresid, shm);
+            k_wresid<<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, x, d.b1.p, alpha);
+            d.launches++;
+        }
+    if (S.seg.nfix) {
+        d.along.alloc(size_t(S.seg.nfix) * r);
+        k_seg_apply<double><<<GRID_T, THREADS, 0, st>>>(S, W, x, R, d.t.p, d.part.p, true, nullptr);
+        k_fix_alpha<<<std::min<u32>(S.seg.nfix, GRID_T), THREADS, 0, st>>>(S.seg, W, d.part.p, d.b1.p, R, d.along.p, alpha);
+        d.launches += 2;
+    }
+    if (S.seg.n) {
+        k_residualize<<<GRID_T, THREADS, 0, st>>>(S, W, rows, R, x, d.b1.p, d.along.p, alpha);
+        d.launches++;
+    }
+    d.end(h, st);
+    CK(cudaGetLastError());
+    if (want_coefs && coefs) CK(cudaMemcpyAsync(coefs, x, (m + g1) * r * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    d.collect();
+    info.iterations = iterations;
+    info.exact = exact;
+    return info;
+}
+
+void GpuAbsorber::set_profiling(bool on) {
+    d_->prof = on;
+    if (on) {
+        std::fill(d_->ms, d_->ms + P_NSLOTS, 0.0);
+        std::fill(d_->cnt, d_->cnt + P_NSLOTS, u64(0));
+    }
+}
+
+void GpuAbsorber::phase_times(double* ms, u64* counts) const {
+    for (int i = 0; i < P_NSLOTS; i++) {
+        if (ms) ms[i] = d_->ms[i];
+        if (counts) counts[i] = d_->cnt[i];
+    }
+}
+
+u64 GpuAbsorber::launches() const { return d_->launches; }
+
+void GpuAbsorber::fit_rows(const double* coefs, size_t r, size_t col, double* out) const {
+    const HostStructure& st = hs_;
+    const size_t m = st.m, M = st.ncells, nb = st.nb();
+    for (u32 s = 0; s < st.g1; s++)
+        for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++) {
+            double f = coefs[(m + s) * r + col];
+            for (size_t b = 0; b < nb; b++) f += coefs[size_t(st.coord[b * M + c]) * r + col];
+            const u32 r0 = st.trivial() ? c : st.cell_row[c], r1 = st.trivial() ? c + 1 : st.cell_row[c + 1];
+            for (u32 row = r0; row < r1; row++) out[row] = f;
+        }
+}
+
+void GpuAbsorber::term_values(const double* coefs, size_t r, size_t col, double* out) const {
+    const HostStructure& st = hs_;
+    const size_t nterms = g_.size();
+    if (st.fe1 < 0 || norm_fe1_ < 0) return;
+    std::vector<std::vector<double>> vals(nterms), lw(nterms);
+    vals[size_t(st.fe1)].resize(st.g1);
+    for (size_t s = 0; s < st.g1; s++) vals[size_t(st.fe1)][s] = coefs[(st.m + s) * r + col];
+    lw[size_t(st.fe1)] = n1_;
+    for (auto& b : st.blocks) {
+        vals[b.term].resize(b.g);
+        lw[b.term].resize(b.g);
+        for (size_t l = 0; l < b.g; l++) {
+            vals[b.term][l] = coefs[(b.off + l) * r + col];
+            lw[b.term][l] = nr_[b.off + l];
+        }
+    }
+    double shift = 0;
+    for (size_t t = 0; t < nterms; t++) {
+        if (int(t) == norm_fe1_) continue;
+        double mean = 0;
+        for (size_t l = 0; l < vals[t].size(); l++) mean += vals[t][l] * lw[t][l];
+        mean /= sw_;
+        for (auto& v : vals[t]) v -= mean;
+        shift += mean;
+    }
+    for (auto& v : vals[size_t(norm_fe1_)]) v += shift;
+    size_t o = 0;
+    for (size_t t = 0; t < nterms; t++) {
+        std::copy(vals[t].begin(), vals[t].end(), out + o);
+        o += g_[t];
+    }
+}
+
+}  // namespace fereg

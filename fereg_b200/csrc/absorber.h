@@ -1,0 +1,110 @@
+// GpuAbsorber: the B200 implementation of the reference's `Absorber` trait
+// (crates/fereg-core/src/absorber.rs:62-97) over the cell structure of `FeSolver`
+// (crates/fereg-core/src/solve.rs:351-1344).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+
+#include "common.h"
+#include "device.cuh"
+
+namespace fereg {
+
+struct Ctx {
+    int (*interrupt)(void*) = nullptr;
+    void* interrupt_data = nullptr;
+    void (*log)(void*, const char*) = nullptr;
+    void* log_data = nullptr;
+    int verbose = 0;
+    void check() const {
+        if (interrupt && interrupt(interrupt_data)) throw Error(RC_INTERRUPTED, "--Break--");
+    }
+    void logf(const std::string& s) const {
+        if (log && verbose >= 2) log(log_data, s.c_str());
+    }
+};
+
+// absorber.rs:27-37 SolveInfo (coefficients returned through a caller buffer).
+struct SolveInfo {
+    u64 iterations = 0;
+    bool escalated = false;
+    bool exact = false;
+};
+
+// Precision of the inner PCG: FP64 throughout, or FP32 iterations inside FP64 refinement.
+enum class Precision : int { F64 = 0, F32_REFINED = 1 };
+
+struct Scratch;
+
+class GpuAbsorber {
+   public:
+    // `codes[q]` are the kept-order codes of term q (< g[q]); `w` kept-order weights or null.
+    GpuAbsorber(const std::vector<const u32*>& codes, const std::vector<u32>& g, const double* w, size_t n, const Ctx& ctx);
+    ~GpuAbsorber();
+
+    size_t n() const { return hs_.n; }
+    size_t m() const { return hs_.m; }
+    size_t g1() const { return hs_.g1; }
+    size_t coefs_len() const { return hs_.m + hs_.g1; }
+    const std::vector<u32>& row_order() const { return hs_.pi; }
+    const HostStructure& structure() const { return hs_; }
+    // Row-order weights (false: all ones).
+    bool weights(double* out) const;
+    // Row-order weights (null = ones), strictly positive and finite (solve.rs:1010-1139).
+    void set_weights(const double* w_rows);
+
+    // Residualizes the N x R row-major block `z` in place (rows in row order). `z` is host
+    // memory for `residualize`, device memory for `residualize_device`. `warm` and `coefs` are
+    // (m + g1) x R row-major host buffers ([x; alpha1], solve.rs:7-9) or null.
+    SolveInfo residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
+                          double* coefs, Precision prec = Precision::F64);
+    SolveInfo residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
+                                 const double* warm, double* coefs, Precision prec = Precision::F64);
+
+    // FE fit of coefficient column `col` per row (row order) (absorber.rs:88).
+    void fit_rows(const double* coefs, size_t r, size_t col, double* out) const;
+    // Values per session term, normalized as solve.rs:1319-1343; `out` holds sum_q g_q values.
+    void term_values(const double* coefs, size_t r, size_t col, double* out) const;
+
+    cudaStream_t stream() const { return stream_; }
+
+    // Phase timing with CUDA events on the solver's stream (the reference's PhaseTimer,
+    // timing.rs): per-slot milliseconds and launch counts, accumulated while enabled.
+    enum Slot { P_RHS_SEG = 0, P_RHS_PULL, P_APPLY, P_PRECOND, P_VECTOR, P_RESID, P_H2D, P_D2H, P_NSLOTS };
+    void set_profiling(bool on);
+    void phase_times(double* ms, u64* counts) const;
+    u64 launches() const;
+    void set_ctx(const Ctx& c) { ctx_ = c; }
+
+    // Kernel-level entry points for the parity tests (device work, host buffers).
+    void apply_host(const double* p, size_t r, double* y);
+    void rhs_host(const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum);
+    void precond_host(const double* rr, size_t r, double* z);
+    // Weight state (n1, nr, diag, redundant) as held for the kernels.
+    void weight_state(double* n1, double* nr, double* diag, uint8_t* red, double* sw) const;
+
+   private:
+    HostStructure hs_;
+    std::vector<u32> g_;
+    int norm_fe1_ = -1;
+    Ctx ctx_;
+    cudaStream_t stream_ = nullptr;
+    // host weight state (operator.rs:44-63)
+    std::vector<double> w_rows_, cell_w_, n1_, nr_, diag_;
+    std::vector<uint8_t> red_;
+    double sw_ = 0;
+    bool weighted_ = false;
+    bool pre_fresh_ = false;
+    bool small_ok_ = false;  // the dense small factor exists
+    std::unique_ptr<Scratch> d_;
+
+    void refresh_weights(const double* w_kept);
+    void upload_weights();
+    void ensure_precond();
+    SolveInfo solve(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
+                    double* coefs, Precision prec);
+};
+
+}  // namespace fereg

@@ -1,0 +1,194 @@
+// extern "C" boundary: exceptions become the reference's return codes plus a thread-local
+// message; nothing throws across.
+
+#include <new>
+
+#include "../../include/fereg_b200.h"
+#include "absorber.h"
+
+using namespace fereg;
+
+struct fereg_absorber {
+    GpuAbsorber a;
+    template <class... A>
+    explicit fereg_absorber(A&&... args) : a(std::forward<A>(args)...) {}
+};
+
+namespace {
+
+template <class F>
+int guard(F f) {
+    try {
+        f();
+        return RC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.rc;
+    } catch (const std::bad_alloc&) {
+        set_last_error("fereg: insufficient memory");
+        return RC_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        set_last_error(std::string("fereg internal error: ") + e.what());
+        return RC_INTERNAL;
+    } catch (...) {
+        set_last_error("fereg internal error");
+        return RC_INTERNAL;
+    }
+}
+
+Ctx to_ctx(const fereg_ctx* c) {
+    Ctx x;
+    if (c) {
+        x.interrupt = c->interrupt;
+        x.interrupt_data = c->interrupt_data;
+        x.log = c->log;
+        x.log_data = c->log_data;
+        x.verbose = c->verbose;
+    }
+    return x;
+}
+
+void fill(fereg_solve_info* info, const SolveInfo& s) {
+    if (!info) return;
+    info->iterations = s.iterations;
+    info->escalated = s.escalated;
+    info->exact = s.exact;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fereg_last_error(void) { return last_error(); }
+
+int fereg_absorber_create(const uint32_t* const* codes, const uint32_t* g, int nterms, const double* w, size_t n,
+                          const fereg_ctx* ctx, fereg_absorber** out) {
+    return guard([&] {
+        if (!out) throw Error(RC_INVALID_INPUT, "fereg_absorber_create: out is NULL");
+        *out = nullptr;
+        if (nterms < 0 || (nterms > 0 && (!codes || !g))) throw Error(RC_INVALID_INPUT, "fereg_absorber_create: bad terms");
+        if (n < 2) throw Error(RC_TOO_FEW_OBS, "insufficient observations");
+        if (n >= (size_t(1) << 32)) throw Error(RC_INVALID_INPUT, "more than 2^32 - 1 rows");
+        std::vector<const u32*> cs(codes, codes + nterms);
+        std::vector<u32> gs(g, g + nterms);
+        for (int q = 0; q < nterms; q++)
+            if (!cs[size_t(q)] || gs[size_t(q)] == 0) throw Error(RC_INVALID_INPUT, "fereg_absorber_create: empty term");
+        *out = new fereg_absorber(cs, gs, w, n, to_ctx(ctx));
+    });
+}
+
+void fereg_absorber_destroy(fereg_absorber* h) { delete h; }
+
+size_t fereg_absorber_n(const fereg_absorber* h) { return h ? h->a.n() : 0; }
+
+size_t fereg_absorber_coefs_len(const fereg_absorber* h) { return h ? h->a.coefs_len() : 0; }
+
+int fereg_absorber_row_order(const fereg_absorber* h, uint32_t* out) {
+    return guard([&] {
+        if (!h || !out) throw Error(RC_INVALID_INPUT, "fereg_absorber_row_order: NULL argument");
+        const auto& pi = h->a.row_order();
+        std::copy(pi.begin(), pi.end(), out);
+    });
+}
+
+int fereg_absorber_weights(const fereg_absorber* h, double* out, int* has) {
+    return guard([&] {
+        if (!h || !has) throw Error(RC_INVALID_INPUT, "fereg_absorber_weights: NULL argument");
+        *has = h->a.weights(out) ? 1 : 0;
+    });
+}
+
+int fereg_absorber_set_weights(fereg_absorber* h, const double* w) {
+    return guard([&] {
+        if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_set_weights: NULL handle");
+        h->a.set_weights(w);
+    });
+}
+
+int fereg_absorber_residualize(fereg_absorber* h, double* z, size_t r, double tol, size_t maxiter, int want_coefs,
+                               const double* warm, double* coefs_out, fereg_solve_info* info) {
+    return fereg_absorber_residualize_ex(h, z, 0, r, tol, maxiter, want_coefs, warm, coefs_out, FEREG_PREC_F64, info);
+}
+
+int fereg_absorber_residualize_ex(fereg_absorber* h, double* z, int z_on_device, size_t r, double tol, size_t maxiter,
+                                  int want_coefs, const double* warm, double* coefs_out, int precision,
+                                  fereg_solve_info* info) {
+    return guard([&] {
+        if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_residualize: NULL handle");
+        if (r > 0 && !z) throw Error(RC_INVALID_INPUT, "residualize: block size differs from n*R");
+        if (!(tol > 0.0)) throw Error(RC_INVALID_INPUT, "residualize: tol must be positive");
+        if (precision != FEREG_PREC_F64 && precision != FEREG_PREC_F32_REFINED)
+            throw Error(RC_INVALID_INPUT, "residualize: unknown precision");
+        const Precision p = Precision(precision);
+        SolveInfo s = z_on_device ? h->a.residualize_device(z, r, tol, maxiter, want_coefs != 0, warm, coefs_out, p)
+                                  : h->a.residualize(z, r, tol, maxiter, want_coefs != 0, warm, coefs_out, p);
+        fill(info, s);
+    });
+}
+
+int fereg_absorber_fit_rows(const fereg_absorber* h, const double* coefs, size_t r, size_t col, double* out) {
+    return guard([&] {
+        if (!h || !coefs || !out) throw Error(RC_INVALID_INPUT, "fereg_absorber_fit_rows: NULL argument");
+        if (col >= r) throw Error(RC_INVALID_INPUT, "fit_rows: column out of range");
+        h->a.fit_rows(coefs, r, col, out);
+    });
+}
+
+int fereg_absorber_term_values(const fereg_absorber* h, const double* coefs, size_t r, size_t col, double* out) {
+    return guard([&] {
+        if (!h || !coefs || !out) throw Error(RC_INVALID_INPUT, "fereg_absorber_term_values: NULL argument");
+        if (col >= r) throw Error(RC_INVALID_INPUT, "term_values: column out of range");
+        h->a.term_values(coefs, r, col, out);
+    });
+}
+
+void* fereg_absorber_stream(const fereg_absorber* h) { return h ? static_cast<void*>(h->a.stream()) : nullptr; }
+
+int fereg_absorber_set_profiling(fereg_absorber* h, int on) {
+    return guard([&] {
+        if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_set_profiling: NULL handle");
+        h->a.set_profiling(on != 0);
+    });
+}
+
+int fereg_absorber_phase_times(const fereg_absorber* h, double* ms8, uint64_t* counts8) {
+    return guard([&] {
+        if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_phase_times: NULL handle");
+        h->a.phase_times(ms8, counts8);
+    });
+}
+
+uint64_t fereg_absorber_launches(const fereg_absorber* h) { return h ? h->a.launches() : 0; }
+
+int fereg_absorber_info(const fereg_absorber* h, uint64_t* o) {
+    return guard([&] {
+        if (!h || !o) throw Error(RC_INVALID_INPUT, "fereg_absorber_info: NULL argument");
+        const auto& st = h->a.structure();
+        o[0] = st.n;
+        o[1] = st.m;
+        o[2] = st.g1;
+        o[3] = st.ncells;
+        o[4] = st.nb();
+        o[5] = st.m_small;
+        o[6] = uint64_t(int64_t(st.fe1));
+        o[7] = st.small_work;
+    });
+}
+
+int fereg_absorber_apply(fereg_absorber* h, const double* p, size_t r, double* y) {
+    return guard([&] { h->a.apply_host(p, r, y); });
+}
+
+int fereg_absorber_rhs(fereg_absorber* h, const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum) {
+    return guard([&] { h->a.rhs_host(rows, r, y, b1, wsq, wsum); });
+}
+
+int fereg_absorber_precond(fereg_absorber* h, const double* rr, size_t r, double* z) {
+    return guard([&] { h->a.precond_host(rr, r, z); });
+}
+
+int fereg_absorber_weight_state(const fereg_absorber* h, double* n1, double* nr, double* diag, uint8_t* redundant, double* sw) {
+    return guard([&] { h->a.weight_state(n1, nr, diag, redundant, sw); });
+}
+
+}  // extern "C"

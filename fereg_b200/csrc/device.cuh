@@ -1,0 +1,79 @@
+// Device helpers: error checks, buffers, warp lane layouts.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+
+#include "common.h"
+
+namespace fereg {
+
+inline void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    if (e == cudaErrorMemoryAllocation) throw Error(RC_OUT_OF_MEMORY, std::string("fereg: insufficient memory (") + what + ")");
+    throw Error(RC_INTERNAL, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+#define CK(x) ::fereg::cuda_check((x), #x)
+
+// Owned device allocation.
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; return *this; }
+    ~DBuf() { release(); }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) return;
+        CK(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) CK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void upload(const std::vector<T>& h, cudaStream_t s) { upload(h.data(), h.size(), s); }
+};
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// Lane layout of a warp over (entry slot, column) pairs for a block of R columns: with R <= 32
+// the warp holds G = 32/R slots of R consecutive columns (lane = slot*R + col), so consecutive
+// lanes touch consecutive doubles of a row-major row block; with R > 32 the columns are walked
+// in chunks of 32 with one slot.
+struct LaneMap {
+    int G, slot, col;
+    bool on;
+};
+
+__device__ __forceinline__ int col_chunks(int R) { return R <= 32 ? 1 : (R + 31) / 32; }
+
+__device__ __forceinline__ LaneMap lane_map(int R, int lane, int chunk) {
+    if (R <= 32) {
+        int G = 32 / R;
+        return {G, lane / R, lane % R, lane < G * R};
+    }
+    int col = chunk * 32 + lane;
+    return {1, 0, col, col < R};
+}
+
+// Sum of `v` over the slots holding the same column, in slot order (every lane gets the sum;
+// inactive lanes must hold 0).
+template <class T>
+__device__ __forceinline__ T slot_sum(T v, const LaneMap& L, int R) {
+    if (L.G == 1) return v;
+    T s = T(0);
+    const int col = R <= 32 ? (threadIdx.x & 31) % R : 0;
+    for (int g = 0; g < L.G; g++) s += __shfl_sync(FULL, v, g * R + col);
+    return s;
+}
+
+}  // namespace fereg

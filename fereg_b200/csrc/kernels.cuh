@@ -1,0 +1,308 @@
+// sm_100a kernels of the fixed-effects solve.
+//
+// Layout in HBM (one absorber):
+//   seg_off[g1+1]       cells of each FE1 level (segment), cells sorted by (FE1, codes, obs)
+//   coord[nb*M]         block-major global reduced coordinate of every cell
+//   cell_row[M+1]       first row of each cell (absent when every cell holds one row)
+//   pl_off[m+1], pl_cell/pl_seg[E], pl_other[E*(nb-1)]
+//                       coordinate-sorted cell lists (transpose of coord) with each cell's
+//                       segment and other-block coordinates beside it
+//   rows[n*R]           the caller's row-major column block (FP64), rows in row order
+//   reduced vectors     m x R row-major
+//
+// Every kernel is deterministic: per-cell values are never scattered; sums by coordinate are
+// pulls over the coordinate-sorted lists in list order (tiles.cuh), and column sums combine
+// fixed per-CTA partials in CTA order. No floating-point atomics.
+#pragma once
+
+#include "short.cuh"
+
+namespace fereg {
+
+__device__ __forceinline__ int gwarp() { return int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
+__device__ __forceinline__ int nwarps() { return int((gridDim.x * blockDim.x) >> 5); }
+__device__ __forceinline__ int lane_id() { return int(threadIdx.x & 31); }
+
+// ---------------------------------------------------------------------------------------------
+// PCG vector work on m x R blocks (cg.rs), column sums as per-CTA partials (gridDim x R).
+template <class T>
+__global__ void __launch_bounds__(TB) k_dot(const T* __restrict__ a, const T* __restrict__ b, u32 m, int R,
+                                            double* __restrict__ cta_part) {
+    __shared__ double red[TB];
+    for (int j0 = 0; j0 < R; j0 += RC_MAX) {
+        const ColMap cm = colmap(R, j0);
+        double acc = 0.0;
+        if (cm.on)
+            for (u32 i = blockIdx.x * u32(cm.nslot) + u32(cm.slot); i < m; i += gridDim.x * u32(cm.nslot)) {
+                const size_t o = size_t(i) * R + j0 + cm.col;
+                acc += double(a[o]) * double(b[o]);
+            }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        if (int(threadIdx.x) < cm.Rc) {
+            double s = 0.0;
+            for (int sl = 0; sl < cm.nslot; sl++) s += red[sl * cm.Rc + threadIdx.x];
+            cta_part[size_t(blockIdx.x) * R + j0 + threadIdx.x] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// Column sums of [nparts x ncols] partials (plus a second array when given) in a fixed order:
+// one warp per column, lane l sums parts l, l+32, ..., then a fixed butterfly.
+__global__ void k_reduce_cols(const double* __restrict__ part, int nparts, const double* __restrict__ part2,
+                              int nparts2, int ncols, double* __restrict__ out) {
+    const int lane = lane_id();
+    for (int col = gwarp(); col < ncols; col += nwarps()) {
+        double acc = 0.0;
+        for (int p = lane; p < nparts; p += 32) acc += part[size_t(p) * ncols + col];
+        if (part2)
+            for (int p = lane; p < nparts2; p += 32) acc += part2[size_t(p) * ncols + col];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+        if (lane == 0) out[col] = acc;
+    }
+}
+
+// Per-column PCG state (cg.rs:132-292), kept on the device. active: 1 iterating, 0 stopped by
+// the reference's rules, 2 stopped at the FP32 precision floor of a refinement round.
+struct CgState {
+    double* rho;
+    double* rho_new;
+    double* pq;
+    double* gamma;
+    double* beta;
+    double* xb;      // d'rhs, d'r, x0'r (3R)
+    double* ss1;
+    double* floor_;  // 1e-26 * ss0
+    double* ring;    // R x WINDOW
+    double* xconst;  // x0'rhs
+    double* pfloor;  // precision floor of the preconditioned residual (0: none)
+    int* active;
+    int* n_active;
+};
+
+constexpr int WINDOW = 5;
+
+// After rho = r'z of a (re)start: columns with rho <= 0 stop (cg.rs:201-205); the precision
+// floor is drop * rho; counts the active columns. Single block.
+__global__ void k_cg_start(CgState st, int R, double drop) {
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    int local = 0;
+    for (int j = threadIdx.x; j < R; j += blockDim.x) {
+        if (st.active[j] == 1 && !(st.rho[j] > 0.0)) st.active[j] = 0;
+        st.pfloor[j] = drop * st.rho[j];
+        local += st.active[j] == 1;
+    }
+    atomicAdd(&cnt, local);  // integer count: order independent
+    __syncthreads();
+    if (threadIdx.x == 0) *st.n_active = cnt;
+}
+
+// gamma = rho / p'q for the active columns (a non-positive or non-finite p'q deactivates).
+__global__ void k_cg_gamma(CgState st, int R) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < R; j += gridDim.x * blockDim.x) {
+        double g = 0.0;
+        if (st.active[j] == 1) {
+            const double pq = st.pq[j];
+            if (pq > 0.0 && isfinite(pq)) g = st.rho[j] / pq;
+            else st.active[j] = 0;
+        }
+        st.gamma[j] = g;
+    }
+}
+
+// x += gamma p, r -= gamma q, with per-CTA partials of x'rhs, x'r and x0'r (gridDim x 3R;
+// x0 null: 0).
+template <class T>
+__global__ void __launch_bounds__(TB) k_update_xr(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                                                  const T* __restrict__ q, const T* __restrict__ rhs,
+                                                  const T* __restrict__ x0, const double* __restrict__ gamma, u32 m,
+                                                  int R, double* __restrict__ cta_part) {
+    __shared__ double red[3 * TB];
+    for (int j0 = 0; j0 < R; j0 += RC_MAX) {
+        const ColMap cm = colmap(R, j0);
+        double xb = 0.0, xr = 0.0, x0r = 0.0;
+        if (cm.on) {
+            const T g = T(gamma[j0 + cm.col]);
+            for (u32 i = blockIdx.x * u32(cm.nslot) + u32(cm.slot); i < m; i += gridDim.x * u32(cm.nslot)) {
+                const size_t o = size_t(i) * R + j0 + cm.col;
+                const T xv = x[o] + g * p[o];
+                const T rv = r[o] - g * q[o];
+                x[o] = xv;
+                r[o] = rv;
+                xb += double(xv) * double(rhs[o]);
+                xr += double(xv) * double(rv);
+                if (x0) x0r += double(x0[o]) * double(rv);
+            }
+        }
+        red[threadIdx.x] = xb;
+        red[TB + threadIdx.x] = xr;
+        red[2 * TB + threadIdx.x] = x0r;
+        __syncthreads();
+        if (int(threadIdx.x) < cm.Rc) {
+            double a = 0.0, b = 0.0, c = 0.0;
+            for (int sl = 0; sl < cm.nslot; sl++) {
+                a += red[sl * cm.Rc + threadIdx.x];
+                b += red[TB + sl * cm.Rc + threadIdx.x];
+                c += red[2 * TB + sl * cm.Rc + threadIdx.x];
+            }
+            double* o = cta_part + size_t(blockIdx.x) * 3 * R + j0 + threadIdx.x;
+            o[0] = a;
+            o[R] = b;
+            o[2 * R] = c;
+        }
+        __syncthreads();
+    }
+}
+
+// Stopping rule (cg.rs:239-253) and beta; counts the active columns. Single block.
+__global__ void k_cg_stop(CgState st, int R, int k, double tol) {
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    int local = 0;
+    for (int j = threadIdx.x; j < R; j += blockDim.x) {
+        double beta = 0.0;
+        if (st.active[j] == 1) {
+            double* ring = st.ring + size_t(j) * WINDOW;
+            ring[(k - 1) % WINDOW] = st.gamma[j] * st.rho[j];
+            const double ssk = st.ss1[j] - (st.xconst[j] + st.xb[j] + st.xb[R + j] + st.xb[2 * R + j]);
+            const double thr = fmax(tol * tol * ssk, st.floor_[j]);
+            double sum = 0.0;
+            for (int w = 0; w < WINDOW; w++) sum += ring[w];
+            const double rn = st.rho_new[j];
+            const bool done = k >= WINDOW && sum <= thr;
+            const bool at_roundoff = rn <= st.floor_[j];
+            if (done || at_roundoff || !(rn > 0.0)) st.active[j] = 0;
+            else if (rn <= st.pfloor[j]) st.active[j] = 2;
+            else beta = rn / st.rho[j];
+        }
+        st.beta[j] = beta;
+        st.rho[j] = st.rho_new[j];
+        local += st.active[j] == 1;
+    }
+    atomicAdd(&cnt, local);  // integer count: order independent
+    __syncthreads();
+    if (threadIdx.x == 0) *st.n_active = cnt;
+}
+
+// p = z + beta p on the active columns, 0 on the others.
+template <class T>
+__global__ void k_update_p(T* __restrict__ p, const T* __restrict__ z, const double* __restrict__ beta,
+                           const int* __restrict__ active, u32 m, int R) {
+    const size_t total = size_t(m) * R;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const int j = int(i % R);
+        p[i] = active[j] == 1 ? z[i] + T(beta[j]) * p[i] : T(0);
+    }
+}
+
+template <class Src, class Dst>
+__global__ void k_convert(const Src* __restrict__ a, Dst* __restrict__ b, size_t total) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x)
+        b[i] = Dst(a[i]);
+}
+
+// x += d (the FP32 correction of a refinement round).
+__global__ void k_add_correction(double* __restrict__ x, const float* __restrict__ d, size_t total) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x)
+        x[i] += double(d[i]);
+}
+
+// r = a - b
+template <class T>
+__global__ void k_sub(T* __restrict__ r, const T* __restrict__ a, const T* __restrict__ b, size_t total) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x)
+        r[i] = a[i] - b[i];
+}
+
+// p = z masked by the active columns.
+template <class T>
+__global__ void k_mask_copy(T* __restrict__ p, const T* __restrict__ z, const int* __restrict__ active, size_t total, int R) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x)
+        p[i] = active[i % R] == 1 ? z[i] : T(0);
+}
+
+// x += z on the active columns (exact preconditioner, cg.rs:171-198).
+template <class T>
+__global__ void k_add_active(T* __restrict__ x, const T* __restrict__ z, const int* __restrict__ active, size_t total, int R) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x)
+        if (active[i % R] == 1) x[i] += z[i];
+}
+
+// Jacobi on coordinates [k0, m): z = inv_diag .* r (precond/jacobi.rs:12-42).
+template <class T>
+__global__ void k_jacobi(const T* __restrict__ r, T* __restrict__ z, const double* __restrict__ inv_diag, u32 k0, u32 m, int R) {
+    const size_t total = size_t(m - k0) * R;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const size_t o = size_t(k0) * R + i;
+        z[o] = T(inv_diag[k0 + i / R]) * r[o];
+    }
+}
+
+// Small super-block: z[0..ms) = Minv r[0..ms) with the expanded, scaled generalized inverse.
+template <class T>
+__global__ void k_small_apply(const double* __restrict__ minv, u32 ms, const T* __restrict__ r, T* __restrict__ z, int R) {
+    const size_t total = size_t(ms) * R;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const u32 row = u32(i / R);
+        const int col = int(i % R);
+        double acc = 0.0;
+        const double* mr = minv + size_t(row) * ms;
+        for (u32 l = 0; l < ms; l++) acc += mr[l] * double(r[size_t(l) * R + col]);
+        z[i] = T(acc);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Grounded LDL^T of the unit-diagonal-scaled small block (precond/dense.rs:26-38, 79-100): a
+// pivot at or below PIVOT_TOL is replaced by GROUND. Right-looking, one block; `a` is k x k
+// row-major, its strict lower part becomes the unit-lower factor, `d` the pivots.
+constexpr double PIVOT_TOL = 1e-10;
+constexpr double GROUND = 1e30;
+
+__global__ void k_ldlt_ground(double* __restrict__ a, double* __restrict__ d, int k) {
+    for (int j = 0; j < k; j++) {
+        __syncthreads();
+        double dj = a[size_t(j) * k + j];
+        if (dj <= PIVOT_TOL) dj = GROUND;
+        if (threadIdx.x == 0) d[j] = dj;
+        for (int i = j + 1; i < k; i++) {
+            const double f = a[size_t(i) * k + j] / dj;
+            for (int l = j + 1 + int(threadIdx.x); l <= i; l += int(blockDim.x)) a[size_t(i) * k + l] -= f * a[size_t(l) * k + j];
+        }
+        __syncthreads();
+        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) a[size_t(i) * k + j] /= dj;
+    }
+}
+
+// X = L^-T D^-1 L^-1 column by column (one thread per identity column), into x (k x k row-major).
+__global__ void k_ldlt_inverse(const double* __restrict__ a, const double* __restrict__ d, int k, double* __restrict__ x) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= k) return;
+    for (int i = 0; i < k; i++) {
+        double v = i == col ? 1.0 : 0.0;
+        for (int p = col; p < i; p++) v -= a[size_t(i) * k + p] * x[size_t(p) * k + col];
+        x[size_t(i) * k + col] = v;
+    }
+    for (int i = 0; i < k; i++) x[size_t(i) * k + col] /= d[i];
+    for (int i = k - 1; i >= 0; i--) {
+        double v = x[size_t(i) * k + col];
+        for (int p = i + 1; p < k; p++) v -= a[size_t(p) * k + i] * x[size_t(p) * k + col];
+        x[size_t(i) * k + col] = v;
+    }
+}
+
+// minv (ms x ms, zero outside the kept coordinates) = S^-1 X S^-1 scattered to the kept rows/cols.
+__global__ void k_expand_minv(const double* __restrict__ x, const u32* __restrict__ keep, const double* __restrict__ scale,
+                              int k, u32 ms, double* __restrict__ minv) {
+    const size_t total = size_t(k) * k;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const int a = int(i / k), b = int(i % k);
+        minv[size_t(keep[a]) * ms + keep[b]] = scale[a] * x[i] * scale[b];
+    }
+}
+
+}  // namespace fereg

@@ -1,0 +1,341 @@
+// Cell structure of the intercept-only FE design, built on the host once per sample.
+//
+// Follows the reference's structure::build (crates/fereg-core/src/structure.rs:247-527): the
+// eliminated term (FE1) minimises the assembly work E with three or more terms, the other terms
+// are blocks (small ones first while their levels total at most SMALL_LIMIT), rows are sorted by
+// (FE1 code, block codes in block order, observation) and cut into cells and segments. The sort
+// is a stable LSD counting sort, so equal keys keep observation order; the result is unique and
+// therefore identical to the reference's (which sorts per segment in parallel).
+
+#include <algorithm>
+#include <numeric>
+
+#include "common.h"
+
+namespace fereg {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+// absorber.rs:100-108: the intercept-only term with the most levels, first on ties.
+int fe1_index(const std::vector<u32>& g) {
+    int best = -1;
+    for (size_t q = 0; q < g.size(); q++)
+        if (best < 0 || g[q] > g[size_t(best)]) best = int(q);
+    return best;
+}
+
+// Stable counting sort of `ids` by key(id) < g.
+template <class Key>
+static void counting_pass(std::vector<u32>& ids, std::vector<u32>& tmp, u32 g, Key key) {
+    std::vector<u32> cnt(size_t(g) + 1, 0);
+    for (u32 i : ids) cnt[key(i) + 1]++;
+    for (u32 k = 0; k < g; k++) cnt[k + 1] += cnt[k];
+    tmp.resize(ids.size());
+    for (u32 i : ids) tmp[cnt[key(i)]++] = i;
+    ids.swap(tmp);
+}
+
+// structure.rs:256-352 choose_elimination (E = sum over the other terms o and the levels s of
+// the candidate of d_{s,o}^2, d the distinct levels of o within s).
+static int choose_elimination(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n) {
+    const int f0 = fe1_index(g);
+    if (f0 < 0 || codes.size() < 3) return f0;
+    std::vector<size_t> cands;
+    for (size_t q = 0; q < g.size(); q++)
+        if (size_t(g[q]) * 4 >= g[size_t(f0)]) cands.push_back(q);
+    if (cands.size() < 2) return f0;
+    std::vector<u64> size(g[size_t(f0)], 0);
+    for (size_t i = 0; i < n; i++) size[codes[size_t(f0)][i]]++;
+    u64 bound = 0;
+    for (u64 s : size) bound += s * s;
+    bound *= u64(codes.size() - 1);
+    if (bound <= 64 * u64(n)) return f0;
+    bool have = false;
+    u64 best_e = 0;
+    u32 best_g = 0;
+    size_t best_f = 0;
+    for (size_t f : cands) {
+        std::vector<u32> off(size_t(g[f]) + 1, 0), ids(n);
+        for (size_t i = 0; i < n; i++) off[codes[f][i] + 1]++;
+        for (u32 k = 0; k < g[f]; k++) off[k + 1] += off[k];
+        {
+            std::vector<u32> cur(off.begin(), off.end() - 1);
+            for (size_t i = 0; i < n; i++) ids[cur[codes[f][i]]++] = u32(i);
+        }
+        u64 e = 0;
+        for (size_t o = 0; o < codes.size(); o++) {
+            if (o == f) continue;
+            std::vector<u32> stamp(g[o], 0);
+            for (u32 s = 0; s < g[f]; s++) {
+                u64 d = 0;
+                for (u32 p = off[s]; p < off[s + 1]; p++) {
+                    u32 c = codes[o][ids[p]];
+                    if (stamp[c] != s + 1) { stamp[c] = s + 1; d++; }
+                }
+                e += d * d;
+            }
+        }
+        bool better = !have || e < best_e || (e == best_e && (g[f] > best_g || (g[f] == best_g && f < best_f)));
+        if (better) { have = true; best_e = e; best_g = g[f]; best_f = f; }
+    }
+    return int(best_f);
+}
+
+HostStructure build_structure(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n,
+                              size_t small_limit) {
+    HostStructure st;
+    st.n = n;
+    st.fe1 = choose_elimination(codes, g, n);
+    st.g1 = st.fe1 >= 0 ? g[size_t(st.fe1)] : 1;
+
+    // Small/large classification: ascending G (term index on ties) while the total stays within
+    // small_limit (structure.rs:366-378); small blocks first, then large, each in term order.
+    std::vector<size_t> others;
+    for (size_t q = 0; q < g.size(); q++)
+        if (int(q) != st.fe1) others.push_back(q);
+    std::vector<size_t> by_g = others;
+    std::stable_sort(by_g.begin(), by_g.end(), [&](size_t a, size_t b) { return g[a] < g[b]; });
+    std::vector<bool> small(g.size(), false);
+    size_t total = 0;
+    for (size_t q : by_g) {
+        if (total + g[q] > small_limit) break;
+        total += g[q];
+        small[q] = true;
+    }
+    u32 off = 0;
+    for (int pass = 0; pass < 2; pass++)
+        for (size_t q : others)
+            if (small[q] == (pass == 0)) {
+                st.blocks.push_back({u32(q), g[q], off, bool(small[q])});
+                off += g[q];
+            }
+    st.m = off;
+    for (auto& b : st.blocks)
+        if (b.small) st.m_small += b.g;
+    const size_t nb = st.blocks.size();
+
+    // Rows by (FE1, block codes, obs): check the order first (panels usually arrive sorted).
+    auto key_less_eq = [&](u32 a, u32 b) {  // key(a) <= key(b), ignoring obs
+        if (st.fe1 >= 0) {
+            u32 ca = codes[size_t(st.fe1)][a], cb = codes[size_t(st.fe1)][b];
+            if (ca != cb) return ca < cb;
+        }
+        for (size_t k = 0; k < nb; k++) {
+            u32 ca = codes[st.blocks[k].term][a], cb = codes[st.blocks[k].term][b];
+            if (ca != cb) return ca < cb;
+        }
+        return true;
+    };
+    bool sorted = true;
+    for (size_t i = 1; i < n && sorted; i++) sorted = key_less_eq(u32(i - 1), u32(i));
+    st.pi.resize(n);
+    std::iota(st.pi.begin(), st.pi.end(), 0u);
+    if (!sorted) {
+        std::vector<u32> tmp;
+        for (size_t k = nb; k-- > 0;) {
+            const u32* c = codes[st.blocks[k].term];
+            counting_pass(st.pi, tmp, st.blocks[k].g, [c](u32 i) { return c[i]; });
+        }
+        if (st.fe1 >= 0) {
+            const u32* c = codes[size_t(st.fe1)];
+            counting_pass(st.pi, tmp, st.g1, [c](u32 i) { return c[i]; });
+        }
+    }
+
+    // Cells and segments in one pass.
+    st.seg_off.assign(size_t(st.g1) + 1, 0);
+    std::vector<u32> starts;
+    starts.reserve(n);
+    std::vector<std::vector<u32>> cc(nb);
+    for (auto& v : cc) v.reserve(n);
+    const u32* c1 = st.fe1 >= 0 ? codes[size_t(st.fe1)] : nullptr;
+    for (size_t r = 0; r < n; r++) {
+        const u32 o = st.pi[r];
+        bool open = r == 0;
+        if (!open) {
+            const u32 p = st.pi[r - 1];
+            if (c1 && c1[o] != c1[p]) open = true;
+            for (size_t k = 0; k < nb && !open; k++) open = codes[st.blocks[k].term][o] != codes[st.blocks[k].term][p];
+        }
+        if (open) {
+            starts.push_back(u32(r));
+            st.seg_off[(c1 ? c1[o] : 0) + 1]++;
+            for (size_t k = 0; k < nb; k++) cc[k].push_back(st.blocks[k].off + codes[st.blocks[k].term][o]);
+        }
+    }
+    for (u32 s = 0; s < st.g1; s++) st.seg_off[s + 1] += st.seg_off[s];
+    st.ncells = starts.size();
+    if (st.ncells != n) {
+        st.cell_row = std::move(starts);
+        st.cell_row.push_back(u32(n));
+    }
+    st.coord.resize(nb * st.ncells);
+    for (size_t k = 0; k < nb; k++) std::copy(cc[k].begin(), cc[k].end(), st.coord.begin() + k * st.ncells);
+
+    // Dense small-block work sum_s (distinct small coordinates)^2 (structure.rs:521-525).
+    if (st.m_small > 0) {
+        std::vector<u32> mark(st.m_small, 0);
+        u64 work = 0;
+        for (u32 s = 0; s < st.g1; s++) {
+            u64 d = 0;
+            for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++)
+                for (size_t k = 0; k < nb; k++) {
+                    if (!st.blocks[k].small) continue;
+                    u32 x = st.coord[k * st.ncells + c];
+                    if (mark[x] != s + 1) { mark[x] = s + 1; d++; }
+                }
+            work += d * d;
+        }
+        st.small_work = work;
+        if (work > 64 * u64(st.ncells)) {
+            for (auto& b : st.blocks) b.small = false;
+            st.m_small = 0;
+        }
+    }
+    return st;
+}
+
+PullTable build_pull_table(const HostStructure& st) {
+    PullTable t;
+    const size_t nb = st.nb(), M = st.ncells;
+    const size_t E = M * nb;
+    t.off.assign(st.m + 1, 0);
+    for (size_t k = 0; k < nb; k++)
+        for (size_t c = 0; c < M; c++) t.off[st.coord[k * M + c] + 1]++;
+    for (size_t k = 0; k < st.m; k++) t.off[k + 1] += t.off[k];
+    t.cell.resize(E);
+    t.seg.resize(E);
+    t.other.resize(E * (nb > 0 ? nb - 1 : 0));
+    std::vector<u32> cur(t.off.begin(), t.off.end() - 1);
+    for (u32 s = 0; s < st.g1; s++)
+        for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++)
+            for (size_t k = 0; k < nb; k++) {
+                const u32 x = st.coord[k * M + c];
+                const u32 e = cur[x]++;
+                t.cell[e] = c;
+                t.seg[e] = s;
+                size_t o = 0;
+                for (size_t k2 = 0; k2 < nb; k2++)
+                    if (k2 != k) t.other[size_t(e) * (nb - 1) + o++] = st.coord[k2 * M + c];
+            }
+    return t;
+}
+
+TileList build_tiles(const std::vector<u32>& off, u32 k_begin, u32 k_end, u32 cap, u32 min_len) {
+    TileList it;
+    u32 k = k_begin;
+    while (k < k_end) {
+        const u32 cnt = off[k + 1] - off[k];
+        if (cnt <= min_len) {  // left to the one-thread-per-list kernels
+            k++;
+            continue;
+        }
+        if (cnt > cap) {
+            const u32 np = (cnt + cap - 1) / cap;
+            const int32_t f = int32_t(it.fix_k.size());
+            it.fix_k.push_back(k);
+            it.fix_p0.push_back(it.nparts);
+            it.fix_np.push_back(np);
+            for (u32 p = 0; p < np; p++) {
+                it.k0.push_back(k);
+                it.k1.push_back(k + 1);
+                it.e0.push_back(off[k] + p * cap);
+                it.e1.push_back(std::min(off[k] + (p + 1) * cap, off[k + 1]));
+                it.part.push_back(int32_t(it.nparts + p));
+                it.fixidx.push_back(f);
+            }
+            it.nparts += np;
+            k++;
+            continue;
+        }
+        u32 k1 = k, tot = 0;
+        while (k1 < k_end) {
+            const u32 c = off[k1 + 1] - off[k1];
+            if (c <= min_len || c > cap || (tot + c > cap && k1 > k)) break;
+            tot += c;
+            k1++;
+        }
+        it.k0.push_back(k);
+        it.k1.push_back(k1);
+        it.e0.push_back(off[k]);
+        it.e1.push_back(off[k1]);
+        it.part.push_back(-1);
+        it.fixidx.push_back(-1);
+        k = k1;
+    }
+    return it;
+}
+
+}  // namespace fereg
+
+namespace fereg {
+
+void split_tiles(const std::vector<u32>& off, const std::vector<u32>* weight, u32 k_begin, u32 k_end, u32 warp_max,
+                 u32 pack, u32 cta_cap, WarpTileList& wt, TileList& ct) {
+    auto wgt = [&](u32 k) { return weight ? (*weight)[k] : off[k + 1] - off[k]; };
+    // warp tiles: consecutive lists of weight <= warp_max, packed while the total stays <= pack
+    u32 k = k_begin;
+    while (k < k_end) {
+        if (wgt(k) > warp_max) {
+            k++;
+            continue;
+        }
+        u32 k1 = k, tot = 0;
+        while (k1 < k_end) {
+            const u32 w = wgt(k1);
+            if (w > warp_max || (tot + w > pack && k1 > k)) break;
+            tot += w;
+            k1++;
+        }
+        wt.k0.push_back(k);
+        wt.k1.push_back(k1);
+        wt.e0.push_back(off[k]);
+        wt.e1.push_back(off[k1]);
+        k = k1;
+    }
+    // CTA tiles over the others (lists longer than warp_max by weight)
+    k = k_begin;
+    while (k < k_end) {
+        if (wgt(k) <= warp_max) {
+            k++;
+            continue;
+        }
+        const u32 cnt = off[k + 1] - off[k];
+        if (cnt > cta_cap) {
+            const u32 np = (cnt + cta_cap - 1) / cta_cap;
+            const int32_t f = int32_t(ct.fix_k.size());
+            ct.fix_k.push_back(k);
+            ct.fix_p0.push_back(ct.nparts);
+            ct.fix_np.push_back(np);
+            for (u32 p = 0; p < np; p++) {
+                ct.k0.push_back(k);
+                ct.k1.push_back(k + 1);
+                ct.e0.push_back(off[k] + p * cta_cap);
+                ct.e1.push_back(std::min(off[k] + (p + 1) * cta_cap, off[k + 1]));
+                ct.part.push_back(int32_t(ct.nparts + p));
+                ct.fixidx.push_back(f);
+            }
+            ct.nparts += np;
+            k++;
+            continue;
+        }
+        u32 k1 = k, tot = 0;
+        while (k1 < k_end) {
+            const u32 c = off[k1 + 1] - off[k1];
+            if (wgt(k1) <= warp_max || c > cta_cap || (tot + c > cta_cap && k1 > k)) break;
+            tot += c;
+            k1++;
+        }
+        ct.k0.push_back(k);
+        ct.k1.push_back(k1);
+        ct.e0.push_back(off[k]);
+        ct.e1.push_back(off[k1]);
+        ct.part.push_back(-1);
+        ct.fixidx.push_back(-1);
+        k = k1;
+    }
+}
+
+}  // namespace fereg

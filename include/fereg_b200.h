@@ -1,0 +1,127 @@
+/* fereg_b200 — C ABI of the B200 fixed-effects solver.
+ *
+ * The entry points replace the reference's `Absorber` trait
+ * (leoliu0/fereg, crates/fereg-core/src/absorber.rs:62-97) as implemented by `FeSolver`
+ * (crates/fereg-core/src/solve.rs:351-1344), constructed where the reference calls
+ * `solve::build` (solve.rs:338, selected by `build_absorber`, session.rs:606). A Rust shim
+ * `impl Absorber for GpuAbsorber` binds them.
+ *
+ * Conventions
+ *   - Plain pointers and sizes. Row blocks are N x R row-major doubles in the absorber's row
+ *     order (fereg_absorber_row_order); FE coefficients are (m + g1) x R row-major,
+ *     [x (m x R); alpha1 (g1 x R)] (solve.rs:7-9).
+ *   - Return codes are the reference's `RfError::rc` (error.rs:24-34): 0 ok, 1 interrupted,
+ *     198 invalid input, 430 convergence, 909 out of memory, 2001 too few observations,
+ *     9999 internal. The message of the last failure on the calling thread is
+ *     fereg_last_error(). No exception or panic crosses this boundary.
+ *   - One handle is used by one host thread at a time (the reference's `Ctx` is !Sync,
+ *     api.rs:198-210). Work runs on the handle's own CUDA stream.
+ */
+#ifndef FEREG_B200_H
+#define FEREG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fereg_absorber fereg_absorber;
+
+/* Mirror of the reference's `Ctx` hooks (api.rs:198-229): `interrupt` is polled between kernels
+ * and iterations (nonzero = stop with rc 1); `log` receives phase messages when verbose >= 2. */
+typedef struct fereg_ctx {
+    int (*interrupt)(void* data);
+    void* interrupt_data;
+    void (*log)(void* data, const char* msg);
+    void* log_data;
+    int verbose;
+} fereg_ctx;
+
+/* absorber.rs:27-37 SolveInfo. */
+typedef struct fereg_solve_info {
+    uint64_t iterations; /* PCG iterations (1 for closed forms, as reghdfe e(ic)) */
+    int32_t escalated;   /* the preconditioner was strengthened during this solve */
+    int32_t exact;       /* solved by a direct factor or in closed form */
+} fereg_solve_info;
+
+/* Inner precision of fereg_absorber_residualize_ex. */
+enum { FEREG_PREC_F64 = 0, FEREG_PREC_F32_REFINED = 1 };
+
+/* Message of the last failed call on this thread. */
+const char* fereg_last_error(void);
+
+/* solve::build / FeSolver::new (solve.rs:338, 396): builds the cell structure of the
+ * intercept-only terms and the weight state. codes[q] holds the n kept-order codes of term q,
+ * each < g[q]; w (kept order, strictly positive) or NULL. ctx may be NULL. */
+int fereg_absorber_create(const uint32_t* const* codes, const uint32_t* g, int nterms, const double* w, size_t n,
+                          const fereg_ctx* ctx, fereg_absorber** out);
+
+void fereg_absorber_destroy(fereg_absorber* h);
+
+/* Absorber::n (absorber.rs:64). */
+size_t fereg_absorber_n(const fereg_absorber* h);
+
+/* p = m + g1, the rows of an FeCoefs block (absorber.rs:41-46). */
+size_t fereg_absorber_coefs_len(const fereg_absorber* h);
+
+/* Absorber::row_order (absorber.rs:67): kept-observation index of each row (n values). */
+int fereg_absorber_row_order(const fereg_absorber* h, uint32_t* out);
+
+/* Absorber::weights (absorber.rs:70): row-order weights into out (n values) and *has = 1, or
+ * *has = 0 when every weight is 1. */
+int fereg_absorber_weights(const fereg_absorber* h, double* out, int* has);
+
+/* Absorber::set_weights (absorber.rs:75, solve.rs:1010-1139): row-order weights, strictly
+ * positive and finite (else 198), or NULL for ones. */
+int fereg_absorber_set_weights(fereg_absorber* h, const double* w);
+
+/* Absorber::residualize (absorber.rs:78-86, solve.rs:1141-1311): residualizes the n x r
+ * row-major host block z in place. tol: relative W-norm accuracy of each column; maxiter: PCG
+ * cap (430 when reached); warm: (m+g1) x r start or NULL; coefs_out: (m+g1) x r or NULL
+ * (filled when want_coefs). */
+int fereg_absorber_residualize(fereg_absorber* h, double* z, size_t r, double tol, size_t maxiter, int want_coefs,
+                               const double* warm, double* coefs_out, fereg_solve_info* info);
+
+/* As fereg_absorber_residualize with a choice of inner precision (FEREG_PREC_*) and z either
+ * host memory (z_on_device = 0) or device memory on the current device (z_on_device = 1). */
+int fereg_absorber_residualize_ex(fereg_absorber* h, double* z, int z_on_device, size_t r, double tol, size_t maxiter,
+                                  int want_coefs, const double* warm, double* coefs_out, int precision,
+                                  fereg_solve_info* info);
+
+/* Absorber::fit_rows (absorber.rs:88): FE fit of coefficient column col per row (row order). */
+int fereg_absorber_fit_rows(const fereg_absorber* h, const double* coefs, size_t r, size_t col, double* out);
+
+/* Absorber::term_values (absorber.rs:90-96, solve.rs:1319-1343): level values of column col per
+ * session term, concatenated in term order (sum_q g[q] values); every term but the one with
+ * the most levels has weighted mean 0. */
+int fereg_absorber_term_values(const fereg_absorber* h, const double* coefs, size_t r, size_t col, double* out);
+
+/* The handle's CUDA stream (cudaStream_t), for callers that order their own device work or
+ * record CUDA events against the solver's kernels. */
+void* fereg_absorber_stream(const fereg_absorber* h);
+
+/* Phase timing with CUDA events on the handle's stream (the reference's PhaseTimer, timing.rs;
+ * reported under verbose >= 2 as in solve.rs:387-392). Enabling resets the totals. Slots:
+ * 0 rhs segment pass, 1 rhs pull, 2 operator S*P, 3 preconditioner, 4 PCG vector work,
+ * 5 residualize pass, 6 host-to-device rows, 7 device-to-host rows. */
+int fereg_absorber_set_profiling(fereg_absorber* h, int on);
+int fereg_absorber_phase_times(const fereg_absorber* h, double* ms8, uint64_t* counts8);
+
+/* Kernel launches issued by this handle so far. */
+uint64_t fereg_absorber_launches(const fereg_absorber* h);
+
+/* Kernel-level entry points used by the parity tests (device work, host buffers). */
+int fereg_absorber_info(const fereg_absorber* h, uint64_t* out8); /* n, m, g1, ncells, nb, m_small, fe1, small_work */
+int fereg_absorber_apply(fereg_absorber* h, const double* p, size_t r, double* y);
+int fereg_absorber_rhs(fereg_absorber* h, const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum);
+int fereg_absorber_precond(fereg_absorber* h, const double* rr, size_t r, double* z);
+int fereg_absorber_weight_state(const fereg_absorber* h, double* n1, double* nr, double* diag, uint8_t* redundant,
+                                double* sw);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
