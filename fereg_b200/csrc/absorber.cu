@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <sstream>
+#include <type_traits>
 
 #include "absorber.h"
 #include "kernels.cuh"
@@ -58,23 +59,49 @@ struct DevTiles {
     TileSet set() const { return TileSet{n, k0.p, k1.p, e0.p, e1.p, part.p, fixidx.p, nfix, fix_k.p, fix_p0.p, fix_np.p, nparts}; }
 };
 
+// Warp tiles packed as (k0, k1, e0, e1) in one 16-byte load.
 struct DevWarpTiles {
-    DBuf<u32> k0, k1, e0, e1;
+    DBuf<uint4> t;
     u32 n = 0;
-    void upload(const WarpTileList& t, cudaStream_t s) {
-        k0.upload(t.k0, s);
-        k1.upload(t.k1, s);
-        e0.upload(t.e0, s);
-        e1.upload(t.e1, s);
-        n = u32(t.k0.size());
+    void upload(const WarpTileList& l, cudaStream_t s) {
+        std::vector<uint4> h(l.k0.size());
+        for (size_t i = 0; i < h.size(); i++) h[i] = make_uint4(l.k0[i], l.k1[i], l.e0[i], l.e1[i]);
+        t.upload(h, s);
+        n = u32(h.size());
     }
-    WarpTiles set() const { return WarpTiles{n, k0.p, k1.p, e0.p, e1.p}; }
+    WarpTiles set() const { return WarpTiles{n, t.p}; }
 };
 
-// Dynamic shared memory of the warp-tile kernels for a chunk of Rc columns.
-inline size_t wseg_smem(int Rc, size_t tsz, u32 ms_acc) { return WPB * (wseg_bytes(Rc, tsz) + size_t(ms_acc) * Rc * tsz); }
-inline size_t wrows_smem(int Rc, u32 ms_acc) {
-    return WPB * (wrows_bytes(Rc) + size_t(ms_acc) * Rc * 8 + 2 * size_t(Rc) * 8);
+// Dynamic shared memory of the warp-tile kernels for a chunk of Rc columns (per-warp parts, then
+// the lane-private small-coordinate slots and column partials).
+inline size_t wseg_smem(int Rc, size_t tsz, u32 ms_acc) { return WPB * (wseg_bytes(Rc, tsz) + size_t(ms_acc) * 32 * tsz); }
+inline size_t wrhs_smem(int Rc, u32 ms_acc) { return WPB * (wrhs_bytes(Rc) + size_t(ms_acc) * 32 * 8 + 2 * 32 * 8); }
+inline size_t wresid_smem(int Rc) { return WPB * wresid_bytes(Rc); }
+inline size_t wpull_smem() { return WPB * pull_bytes(); }
+
+// Calls f(RCP, NBK) as integral constants: RCP the padded width of an Rc-column chunk, NBK the
+// block-count key of nb blocks (from MIN_NBK: apply and list kernels never run without blocks).
+template <int RCP, int MIN_NBK, class F>
+void with_nbk(u32 nb, F&& f) {
+    using std::integral_constant;
+    switch (std::max(nbk_of(nb), MIN_NBK)) {
+        case 0: f(integral_constant<int, RCP>{}, integral_constant<int, 0 < MIN_NBK ? MIN_NBK : 0>{}); break;
+        case 1: f(integral_constant<int, RCP>{}, integral_constant<int, 1>{}); break;
+        case 2: f(integral_constant<int, RCP>{}, integral_constant<int, 2>{}); break;
+        case 3: f(integral_constant<int, RCP>{}, integral_constant<int, 3>{}); break;
+        default: f(integral_constant<int, RCP>{}, integral_constant<int, WNB>{}); break;
+    }
+}
+template <int MIN_NBK = 0, class F>
+void with_rcp(int Rc, u32 nb, F&& f) {
+    switch (rcp_of(Rc)) {
+        case 1: with_nbk<1, MIN_NBK>(nb, f); break;
+        case 2: with_nbk<2, MIN_NBK>(nb, f); break;
+        case 4: with_nbk<4, MIN_NBK>(nb, f); break;
+        case 8: with_nbk<8, MIN_NBK>(nb, f); break;
+        case 16: with_nbk<16, MIN_NBK>(nb, f); break;
+        default: with_nbk<32, MIN_NBK>(nb, f); break;
+    }
 }
 }  // namespace
 
@@ -202,7 +229,7 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
         }
         WarpTileList wt;
         TileList ct;
-        split_tiles(hs_.seg_off, &wgt, 0, hs_.g1, WT, WT, TILE, wt, ct);
+        split_tiles(hs_.seg_off, &wgt, 0, hs_.g1, WT, WT, WSEG, TILE, wt, ct);
         d_->wseg.upload(wt, stream_);
         d_->seg_tiles.upload(ct, stream_);
         CK(cudaStreamSynchronize(stream_));
@@ -223,7 +250,7 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
         d_->pl_other.upload(pt.other, stream_);
         WarpTileList wt;
         TileList ct;
-        split_tiles(pt.off, nullptr, d_->ms_acc, u32(hs_.m), PULL_WARP_MAX, 32, TILE, wt, ct);
+        split_tiles(pt.off, nullptr, d_->ms_acc, u32(hs_.m), PULL_WARP_MAX, PULL_WARP_MAX, WLIST, TILE, wt, ct);
         d_->wpull.upload(wt, stream_);
         d_->pull_tiles.upload(ct, stream_);
         CK(cudaStreamSynchronize(stream_));  // host tables die here
@@ -437,8 +464,12 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
             const size_t shm = wseg_smem(Rc, sizeof(T), S.ms_acc);
-            allow_smem(k_wseg_apply<T>, shm);
-            k_wseg_apply<T><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), P, R, j0, Rc, t, acc ? small : nullptr);
+            with_rcp<1>(Rc, S.nb, [&](auto c, auto nbk) {
+                constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
+                allow_smem(k_wseg_apply<T, RCP, NBK>, shm);
+                k_wseg_apply<T, RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), P, R, j0, Rc, t,
+                                                                          acc ? small : nullptr);
+            });
             d.launches++;
         }
     else if (acc)
@@ -459,7 +490,11 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
     if (d.wpull.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            k_wpull_apply<T><<<GRID_S, WPB * 32, 0, st>>>(S, W, d.wpull.set(), P, t, R, j0, Rc, Y);
+            with_rcp<1>(Rc, S.nb, [&](auto c, auto nbk) {
+                constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
+                k_wpull_apply<T, RCP, NBK><<<GRID_S, WPB * 32, wpull_smem(), st>>>(S, W, d.wpull.set(), P, t, R, j0,
+                                                                                    Rc, Y);
+            });
             d.launches++;
         }
     if (S.pull.n) {
@@ -510,10 +545,13 @@ void launch_rhs(Scratch& d, const DevStruct& S, const DevWeights& W, const doubl
     if (d.wseg.n) {
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = wrows_smem(Rc, S.ms_acc);
-            allow_smem(k_wseg_rhs, shm);
-            k_wseg_rhs<<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, b1, d.cta2.p,
-                                                       acc ? small : nullptr);
+            const size_t shm = wrhs_smem(Rc, S.ms_acc);
+            with_rcp<WNB>(Rc, WNB, [&](auto c, auto) {
+                constexpr int RCP = decltype(c)::value;
+                allow_smem(k_wseg_rhs<RCP>, shm);
+                k_wseg_rhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, b1, d.cta2.p,
+                                                                acc ? small : nullptr);
+            });
             d.launches++;
         }
     } else {
@@ -545,7 +583,11 @@ void launch_rhs(Scratch& d, const DevStruct& S, const DevWeights& W, const doubl
         if (d.wpull.n)
             for (int j0 = 0; j0 < R; j0 += WCOLS) {
                 const int Rc = std::min(WCOLS, R - j0);
-                k_wpull_rhs<<<GRID_S, WPB * 32, 0, st>>>(S, W, d.wpull.set(), rows, b1, R, j0, Rc, rhs);
+                with_rcp<WNB>(Rc, WNB, [&](auto c, auto) {
+                    constexpr int RCP = decltype(c)::value;
+                    k_wpull_rhs<RCP><<<GRID_S, WPB * 32, wpull_smem(), st>>>(S, W, d.wpull.set(), rows, b1, R, j0, Rc,
+                                                                              rhs);
+                });
                 d.launches++;
             }
         if (S.pull.n) {
@@ -853,9 +895,13 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     if (d.wseg.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = wrows_smem(Rc, 0);
-            allow_smem(k_wresid, shm);
-            k_wresid<<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, x, d.b1.p, alpha);
+            const size_t shm = wresid_smem(Rc);
+            with_rcp<0>(Rc, S.nb, [&](auto c, auto nbk) {
+                constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
+                allow_smem(k_wresid<RCP, NBK>, shm);
+                k_wresid<RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, x, d.b1.p,
+                                                                   alpha);
+            });
             d.launches++;
         }
     if (S.seg.nfix) {

@@ -99,9 +99,9 @@ struct WarpTileList {
 
 // Splits the lists [k_begin, k_end) of a CSR-like array by weight (`weight[k]`, or the entry
 // count when null): lists of weight <= warp_max go to warp tiles, packed consecutively while the
-// summed weight stays <= pack; the others go to CTA tiles of at most cta_cap entries (slices of
-// longer lists write partials).
+// summed weight stays <= pack and the tile holds at most max_lists lists; the others go to CTA
+// tiles of at most cta_cap entries (slices of longer lists write partials).
 void split_tiles(const std::vector<u32>& off, const std::vector<u32>* weight, u32 k_begin, u32 k_end, u32 warp_max,
-                 u32 pack, u32 cta_cap, WarpTileList& wt, TileList& ct);
+                 u32 pack, u32 max_lists, u32 cta_cap, WarpTileList& wt, TileList& ct);
 
 }  // namespace fereg

@@ -2,439 +2,652 @@
 // coordinate lists of at most PULL_WARP_MAX entries. Longer lists go to the CTA tiles
 // (tiles.cuh).
 //
-// A warp takes one warp tile at a time (whole consecutive segments with at most WT cells and WT
-// rows in all, or whole consecutive coordinate lists): lanes first load the tile's indices (one
-// lane per cell or entry, coalesced) and, in the row passes, the tile's rows (flat, coalesced)
-// into the warp's shared memory; then lanes (group, column) gather the reduced vectors with all
-// gathers of a round in flight, and sums run per column in list order. Warps never wait on each
-// other inside the loop. Column blocks wider than WCOLS are launched per column chunk.
+// A warp takes one warp tile at a time: whole consecutive segments (at most WSEG segments, WT
+// cells and WT rows in all) or whole consecutive coordinate lists (at most PULL_WARP_MAX entries).
+// The tile's indices are staged first, one lane per cell, segment or entry, into the warp's
+// shared memory. Then every loop runs on all lanes as (group g, column j) pairs: a column chunk
+// of Rc columns is padded to RCP (a power of two, a template parameter), the warp holds
+// G = 32 / RCP groups, and cells and rows are dealt to the groups in turn (cell i to group
+// i mod G). Lanes of a group read consecutive columns of one row (coalesced); the per-cell loops
+// are unrolled with their loads batched in registers, so a tile's gathers are in flight together.
 //
-// The small coordinates (when summed in the segment passes) accumulate in the warp's shared
-// memory with each column owned by one lane; at the end the CTA adds its warps in warp order into
-// its own partial row. All sums have a fixed order: results do not depend on timing.
+// Segment sums: while a lane walks its cells (in order) it keeps a running sum of the current
+// segment and parks it in a lane-private slot when the segment ends; the segment's value is then
+// the sum of its G slots in group order. The small coordinates (when summed in the segment
+// passes) accumulate in lane-private slots as well; the CTA adds warps and groups in a fixed
+// order into its own partial row. All sums have a fixed order: results do not depend on timing.
+//
+// The number of blocks is a template parameter NBK (the exact count up to WNB - 1; WNB means
+// WNB or more, the ones past WNB read from global memory).
 #pragma once
 
 #include "tiles.cuh"
 
 namespace fereg {
 
-constexpr int WT = 32;                 // cells (rows) per warp tile
-constexpr int WCOLS = 32;              // columns per launch of the warp kernels
-constexpr int WPB = 8;                 // warps per CTA
-constexpr u32 PULL_WARP_MAX = 8192;    // entries of one coordinate list walked by one warp
-constexpr int LMAX = WT;               // segments up to this many cells use the warp tiles
-constexpr u32 PULL_THR_MAX = PULL_WARP_MAX;
+constexpr int WT = 32;                // cells (rows) per segment tile
+constexpr int WSEG = 8;               // segments per segment tile
+constexpr int WCOLS = 32;             // columns per launch of the warp kernels
+constexpr int WPB = 8;                // warps per CTA
+constexpr u32 PULL_WARP_MAX = 256;    // entries of the coordinate lists of one list tile
+constexpr int WLIST = 32;             // lists per list tile
+constexpr int WNB = 4;                // blocks whose coordinates a segment tile stages
+constexpr int WNO = WNB - 1;          // other blocks whose coordinates a list tile stages
 
-// Warp tiles over short lists.
+// Warp tiles over short lists: (k0, k1, e0, e1) = lists [k0, k1) covering entries [e0, e1).
 struct WarpTiles {
     u32 n;
-    const u32* k0;
-    const u32* k1;
-    const u32* e0;
-    const u32* e1;
+    const uint4* t;
 };
 
 __device__ __forceinline__ u32 wlane() { return threadIdx.x & 31u; }
 __device__ __forceinline__ u32 wid_in_cta() { return threadIdx.x >> 5; }
 
-// Lane layout over (group, column) for a chunk of Rc <= 32 columns: G = 32 / Rc groups.
-struct GMap {
-    int Rc, G, g, j;
+// Padded chunk width for Rc columns, and the block-count key.
+__host__ __device__ constexpr int rcp_of(int Rc) {
+    return Rc <= 1 ? 1 : Rc <= 2 ? 2 : Rc <= 4 ? 4 : Rc <= 8 ? 8 : Rc <= 16 ? 16 : 32;
+}
+__host__ __device__ constexpr int nbk_of(u32 nb) { return nb < u32(WNB) ? int(nb) : WNB; }
+
+// Lane = (group g, column j) for a chunk padded to RCP columns.
+template <int RCP>
+struct Lanes {
+    static constexpr int G = 32 / RCP;
+    static constexpr int KN = WT / G;           // tile cells (rows) per group
+    static constexpr int CH = KN < 8 ? KN : 8;  // loads held in registers at once
+    u32 lane, g, j;
     bool on;
+    __device__ __forceinline__ explicit Lanes(int Rc)
+        : lane(wlane()), g(wlane() / RCP), j(wlane() % RCP), on(int(wlane() % RCP) < Rc) {}
 };
-__device__ __forceinline__ GMap gmap(int Rc) {
-    const int G = 32 / Rc;
-    const int l = int(wlane());
-    return {Rc, G, l / Rc, l % Rc, l < G * Rc};
+
+// Sum of v over the groups (same column), groups in order; every lane gets its column's sum.
+template <int RCP, class T>
+__device__ __forceinline__ T group_total(T v, const Lanes<RCP>& L) {
+    if constexpr (RCP == 32) {
+        return v;
+    } else {
+        T s = T(0);
+#pragma unroll
+        for (int g = 0; g < 32 / RCP; g++) s += __shfl_sync(FULL, v, g * RCP + int(L.j));
+        return s;
+    }
 }
 
-// Sum of v over the groups holding the same column, groups in order (all lanes get the sum;
-// inactive lanes must hold 0).
-template <class T>
-__device__ __forceinline__ T group_sum(T v, const GMap& m) {
-    if (m.G == 1) return v;
-    T s = T(0);
-    for (int g = 0; g < m.G; g++) s += __shfl_sync(FULL, v, g * m.Rc + m.j);
+__host__ __device__ constexpr size_t al16(size_t b) { return (b + 15) / 16 * 16; }
+
+// Per-warp staging of a segment tile.
+struct SegStage {
+    u32* send;    // local end (cell) of each segment of the tile (WSEG)
+    double* n1i;  // 1/n1 of each segment (WSEG)
+    double* cw;   // cell weights
+    u32* code;    // block coordinates of the cells (WNB x WT)
+    u32* row0;    // first row of each cell (WT + 1), rows passes
+    u32* rcell;   // local cell of each local row, rows passes
+    u32* segl;    // local segment of each cell
+};
+__host__ __device__ constexpr size_t segstage_bytes() {
+    return al16(WSEG * 4) + al16(WSEG * 8) + al16(WT * 8) + al16(WNB * WT * 4) + al16((WT + 1) * 4) + 2 * al16(WT * 4);
+}
+__device__ __forceinline__ SegStage seg_stage_at(unsigned char* p) {
+    SegStage s;
+    s.send = reinterpret_cast<u32*>(p);
+    p += al16(WSEG * 4);
+    s.n1i = reinterpret_cast<double*>(p);
+    p += al16(WSEG * 8);
+    s.cw = reinterpret_cast<double*>(p);
+    p += al16(WT * 8);
+    s.code = reinterpret_cast<u32*>(p);
+    p += al16(WNB * WT * 4);
+    s.row0 = reinterpret_cast<u32*>(p);
+    p += al16((WT + 1) * 4);
+    s.rcell = reinterpret_cast<u32*>(p);
+    p += al16(WT * 4);
+    s.segl = reinterpret_cast<u32*>(p);
     return s;
 }
 
-// Per-warp shared memory, laid out for a column chunk of Rc columns (sizes in bytes, 16-byte
-// aligned parts): the per-cell vectors first, then the per-cell indices.
-__host__ __device__ constexpr size_t al16(size_t b) { return (b + 15) / 16 * 16; }
-__host__ __device__ constexpr size_t idx_bytes() { return al16(WT * 8) + al16(4 * WT * 4) + al16(WT * 4) + al16((WT + 1) * 4); }
-// segment kernels: u (per-cell, T)
-__host__ __device__ constexpr size_t wseg_bytes(int Rc, size_t tsz) { return al16(WT * Rc * tsz) + idx_bytes(); }
-// row kernels: v (the tile's rows), u (per cell), both double, + row weights
-__host__ __device__ constexpr size_t wrows_bytes(int Rc) { return 2 * al16(WT * Rc * 8) + al16(WT * 8) + idx_bytes(); }
+// Bytes per warp (Rc columns): per-cell values u (WT x Rc), lane-private segment slots ps
+// (WSEG x 32), the staging; the residualization adds the tile's b1 (WSEG x Rc).
+__host__ __device__ constexpr size_t wseg_bytes(int Rc, size_t tsz) {
+    return al16(WT * Rc * tsz) + al16(WSEG * 32 * tsz) + segstage_bytes();
+}
+__host__ __device__ constexpr size_t wrhs_bytes(int Rc) { return wseg_bytes(Rc, 8); }
+__host__ __device__ constexpr size_t wresid_bytes(int Rc) { return wseg_bytes(Rc, 8) + al16(WSEG * Rc * 8); }
 
-template <class T>
-struct WSeg {
-    T* u;
-    double* cw;
-    u32* code;
-    u32* segl;
-    u32* row0;
-};
-
-template <class T>
-__device__ __forceinline__ WSeg<T> wseg_at(unsigned char* base, int Rc) {
-    unsigned char* p = base + size_t(wid_in_cta()) * wseg_bytes(Rc, sizeof(T));
-    WSeg<T> w;
-    w.u = reinterpret_cast<T*>(p);
-    p += al16(WT * Rc * sizeof(T));
-    w.cw = reinterpret_cast<double*>(p);
-    p += al16(WT * 8);
-    w.code = reinterpret_cast<u32*>(p);
-    p += al16(4 * WT * 4);
-    w.segl = reinterpret_cast<u32*>(p);
-    p += al16(WT * 4);
-    w.row0 = reinterpret_cast<u32*>(p);
-    return w;
+// Stages the tile's per-segment scalars and the cells' weights, first `ncode` block coordinates
+// and (with `rows`, non-trivial cells) first rows. The caller syncs the warp afterwards.
+__device__ __forceinline__ void stage_cells(const DevStruct& S, const DevWeights& W, u32 s0, u32 s1, u32 c0, u32 c1,
+                                            const SegStage& st, u32 ncode, bool rows) {
+    const u32 lane = wlane();
+    if (lane < s1 - s0) {
+        st.send[lane] = S.seg_off[s0 + lane + 1] - c0;
+        st.n1i[lane] = W.n1inv[s0 + lane];
+    }
+    const u32 c = c0 + lane;
+    if (c < c1) {
+        st.cw[lane] = cellw(W, c);
+#pragma unroll
+        for (u32 b = 0; b < u32(WNB); b++)
+            if (b < ncode) st.code[b * WT + lane] = __ldcs(S.coord + size_t(b) * S.M + c);
+        if (rows && S.cell_row) {
+            st.row0[lane] = S.cell_row[c];
+            if (c == c1 - 1) st.row0[lane + 1] = S.cell_row[c + 1];
+        }
+    }
 }
 
-// CTA end: adds the warps' small-coordinate accumulators (wacc, ms_acc x Rc per warp) in warp
-// order into the CTA's partial row.
+// After the staging (and a __syncwarp): local segment of each cell and, for non-trivial cells
+// in the rows passes, local cell of each tile row.
+__device__ __forceinline__ void stage_maps(u32 nc, const SegStage& st, bool rcell) {
+    const u32 lane = wlane();
+    if (lane < nc) {
+        u32 s = 0;
+        while (st.send[s] <= lane) s++;
+        st.segl[lane] = s;
+        if (rcell) {
+            const u32 base = st.row0[0];
+            for (u32 r = st.row0[lane] - base; r < st.row0[lane + 1] - base; r++) st.rcell[r] = lane;
+        }
+    }
+}
+
+// Sum over the blocks of src[coord_b(cell)]: code points at the cell's staged coordinates
+// (stride WT per block), src at this lane's column, ci = the cell's global index.
+template <int NBK, class T>
+__device__ __forceinline__ T gather_cell(const DevStruct& S, const u32* code, const T* __restrict__ src, u32 Ru,
+                                         u32 ci) {
+    T v = T(0);
+#pragma unroll
+    for (int b = 0; b < NBK; b++) v += src[size_t(code[b * WT]) * Ru];
+    if constexpr (NBK == WNB)
+        for (u32 b = WNB; b < S.nb; b++) v += src[size_t(S.coord[size_t(b) * S.M + ci]) * Ru];
+    return v;
+}
+
+// Running sum of a lane over the tile's segments (its cells come in segment order): the sum of
+// each segment is parked in the lane-private slot ps[segment * 32 + lane] (0 when the lane has
+// no cell of the segment).
 template <class T>
+struct SegRun {
+    u32 cur = 0;
+    T run = T(0);
+    __device__ __forceinline__ void add(u32 s, T w, T* ps, u32 lane) {
+        while (cur < s) {
+            ps[cur * 32 + lane] = run;
+            run = T(0);
+            cur++;
+        }
+        run += w;
+    }
+    __device__ __forceinline__ void finish(u32 ns, T* ps, u32 lane) {
+        while (cur < ns) {
+            ps[cur * 32 + lane] = run;
+            run = T(0);
+            cur++;
+        }
+    }
+};
+
+// Segment value of column j: the groups' slots added in group order.
+template <int RCP, class T>
+__device__ __forceinline__ T seg_total(const T* ps, u32 sl, u32 j) {
+    T s = T(0);
+#pragma unroll
+    for (int g = 0; g < 32 / RCP; g++) s += ps[sl * 32 + g * RCP + j];
+    return s;
+}
+
+// Lane-private small-coordinate slots: wacc[k * 32 + lane] for small code k.
+template <class T>
+__device__ __forceinline__ void small_add(const DevStruct& S, const SegStage& st, u32 i, T z, T* wacc, u32 lane) {
+    for (u32 b = 0; b < S.ns_acc; b++) wacc[st.code[b * WT + i] * 32 + lane] += z;
+}
+
+// CTA end: adds the lane-private small-coordinate slots (ms_acc x 32 per warp) of the warps and
+// groups, in that order, into the CTA's partial row (cta_small[blockIdx][k * R + j0 + j]).
+template <int RCP, class T>
 __device__ __forceinline__ void flush_wacc(const T* wacc_all, u32 ms_acc, int Rc, int j0, int R, T* cta_small) {
     __syncthreads();
     T* mine = cta_small + size_t(blockIdx.x) * ms_acc * R;
     for (u32 i = threadIdx.x; i < ms_acc * u32(Rc); i += blockDim.x) {
+        const u32 k = i / u32(Rc), j = i % u32(Rc);
         T s = T(0);
-        for (int w = 0; w < WPB; w++) s += wacc_all[size_t(w) * ms_acc * Rc + i];
-        mine[size_t(i / Rc) * R + j0 + i % Rc] = s;
+        for (int w = 0; w < WPB; w++)
+#pragma unroll
+            for (int g = 0; g < 32 / RCP; g++) s += wacc_all[(size_t(w) * ms_acc + k) * 32 + g * RCP + j];
+        mine[size_t(k) * R + j0 + j] = s;
     }
 }
 
-// Loads the tile's per-cell indices into the warp's shared memory (lane = cell).
-template <class T>
-__device__ __forceinline__ void load_cells(const DevStruct& S, const DevWeights& W, u32 c0, u32 c1, u32 s0,
-                                           const WSeg<T>& sm) {
-    const u32 lane = wlane();
-    const u32 c = c0 + lane;
-    if (c < c1) {
-        sm.cw[lane] = cellw(W, c);
-        for (u32 b = 0; b < S.nb && b < 4; b++) sm.code[b * WT + lane] = __ldcs(S.coord + size_t(b) * S.M + c);
-        u32 s = s0;
-        while (S.seg_off[s + 1] <= c) s++;
-        sm.segl[lane] = s - s0;
+// Small-coordinate phase of a segment tile: every cell adds z_c = u_c - W_c sv_{s(c)} (sv: the
+// per-segment values parked in the group-0 slots of ps) to its small codes' slots.
+template <int RCP, class T>
+__device__ __forceinline__ void small_phase(const DevStruct& S, const SegStage& st, const Lanes<RCP>& L, u32 nc, int Rc,
+                                            const T* u, const T* ps, T* wacc) {
+    constexpr int G = Lanes<RCP>::G;
+    if (!L.on) return;
+#pragma unroll 4
+    for (int k = 0; k < Lanes<RCP>::KN; k++) {
+        const u32 i = L.g + u32(k * G);
+        if (i < nc) small_add(S, st, i, u[i * Rc + L.j] - T(st.cw[i]) * ps[st.segl[i] * 32 + L.j], wacc, L.lane);
     }
-    __syncwarp();
 }
 
 // ---------------------------------------------------------------------------------------------
 // Operator pass 1 (operator.rs:894-948) on short segments: t_s = sum_c W_c u_c / n1_s with
 // u_c = sum_b P[coord_b(c)]; small coordinates: sum of W_c (u_c - t_s) per small code.
-template <class T>
-__global__ void __launch_bounds__(WPB * 32) k_wseg_apply(DevStruct S, DevWeights W, WarpTiles wt, const T* __restrict__ P,
-                                                         int R, int j0, int Rc, T* __restrict__ t,
-                                                         T* __restrict__ cta_small) {
+template <class T, int RCP, int NBK>
+__global__ void __launch_bounds__(WPB * 32, 4) k_wseg_apply(DevStruct S, DevWeights W, WarpTiles wt,
+                                                            const T* __restrict__ P, int R, int j0, int Rc,
+                                                            T* __restrict__ t, T* __restrict__ cta_small) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const WSeg<T> sm = wseg_at<T>(smem_raw, Rc);
+    using L_t = Lanes<RCP>;
+    constexpr int G = L_t::G;
+    unsigned char* mine = smem_raw + size_t(wid_in_cta()) * wseg_bytes(Rc, sizeof(T));
+    T* u = reinterpret_cast<T*>(mine);
+    T* ps = reinterpret_cast<T*>(mine + al16(WT * Rc * sizeof(T)));
+    const SegStage st = seg_stage_at(mine + al16(WT * Rc * sizeof(T)) + al16(WSEG * 32 * sizeof(T)));
     T* wacc_all = reinterpret_cast<T*>(smem_raw + WPB * wseg_bytes(Rc, sizeof(T)));
-    T* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * Rc;
+    T* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 32;
     const bool acc = cta_small != nullptr;
-    const u32 lane = wlane();
+    const L_t L(Rc);
+    const u32 Ru = u32(R);
     if (acc)
-        for (u32 i = lane; i < S.ms_acc * u32(Rc); i += 32) wacc[i] = T(0);
-    const GMap gm = gmap(Rc);
+        for (u32 i = L.lane; i < S.ms_acc * 32; i += 32) wacc[i] = T(0);
+    const T* Pj = P + j0 + L.j;
+    const u32 ncode = NBK < WNB ? u32(NBK) : u32(WNB);
     const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
+    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
     for (u32 tile = wid; tile < wt.n; tile += nw) {
-        const u32 s0 = wt.k0[tile], s1 = wt.k1[tile], c0 = wt.e0[tile], c1 = wt.e1[tile];
-        const u32 nc = c1 - c0;
-        load_cells(S, W, c0, c1, s0, sm);
-        // gathers: lane (g, j) over cells i = g, g+G, ...
-        if (gm.on) {
-#pragma unroll 4
-            for (u32 i = gm.g; i < nc; i += gm.G) {
-                T v = T(0);
-                for (u32 b = 0; b < S.nb; b++) v += P[size_t(sm.code[b * WT + i]) * R + j0 + gm.j];
-                sm.u[i * Rc + gm.j] = T(sm.cw[i]) * v;
+        const u32 s0 = tb.x, ns = tb.y - tb.x, c0 = tb.z, nc = tb.w - tb.z;
+        stage_cells(S, W, s0, tb.y, c0, tb.w, st, ncode, false);
+        if (tile + nw < wt.n) tb = wt.t[tile + nw];
+        __syncwarp();
+        stage_maps(nc, st, false);
+        __syncwarp();
+        if (L.on) {
+            SegRun<T> sr;
+            const u32* cg = st.code + L.g;
+#pragma unroll
+            for (int k0 = 0; k0 < L_t::KN; k0 += L_t::CH) {
+                T v[L_t::CH];
+#pragma unroll
+                for (int k = 0; k < L_t::CH; k++) {
+                    const u32 i = L.g + u32((k0 + k) * G);
+                    v[k] = i < nc ? gather_cell<NBK>(S, cg + (k0 + k) * G, Pj, Ru, c0 + i) : T(0);
+                }
+#pragma unroll
+                for (int k = 0; k < L_t::CH; k++) {
+                    const u32 i = L.g + u32((k0 + k) * G);
+                    if (i < nc) {
+                        const T w = T(st.cw[i]) * v[k];
+                        if (acc) u[i * Rc + L.j] = w;
+                        sr.add(st.segl[i], w, ps, L.lane);
+                    }
+                }
             }
+            sr.finish(ns, ps, L.lane);
         }
         __syncwarp();
-        // per segment, column sums in cell order (lane = column)
-        for (u32 jj = lane; jj < u32(Rc); jj += 32) {
-            u32 i = 0;
-            for (u32 s = s0; s < s1; s++) {
-                const u32 e = S.seg_off[s + 1] - c0;
-                T sum = T(0);
-                const u32 ib = i;
-                for (; i < e; i++) sum += sm.u[i * Rc + jj];
-                const T tsv = sum * T(W.n1inv[s]);
-                t[size_t(s) * R + j0 + jj] = tsv;
-                if (acc)
-                    for (u32 q = ib; q < e; q++) {
-                        const T z = sm.u[q * Rc + jj] - T(sm.cw[q]) * tsv;
-                        for (u32 b = 0; b < S.ns_acc; b++) wacc[sm.code[b * WT + q] * Rc + jj] += z;
-                    }
+        if (L.on)
+            for (u32 sl = L.g; sl < ns; sl += G) {
+                const T tv = seg_total<RCP>(ps, sl, L.j) * T(st.n1i[sl]);
+                t[size_t(s0 + sl) * Ru + j0 + L.j] = tv;
+                ps[sl * 32 + L.j] = tv;
             }
+        if (acc) {
+            __syncwarp();
+            small_phase(S, st, L, nc, Rc, u, ps, wacc);
         }
         __syncwarp();
     }
-    if (acc) flush_wacc(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
+    if (acc) flush_wacc<RCP>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
+}
+
+// Staging of a coordinate-list tile: list ends and the entries' indices.
+struct PullStage {
+    u32* kend;  // local end (entry) of each list (WLIST lists at most)
+    u32* seg;   // PULL_WARP_MAX entries
+    u32* cell;
+    u32* oth;   // WNO x PULL_WARP_MAX
+};
+__host__ __device__ constexpr size_t pull_bytes() {
+    return al16(WLIST * 4) + al16(PULL_WARP_MAX * 4) * 2 + al16(WNO * PULL_WARP_MAX * 4);
+}
+__device__ __forceinline__ PullStage pull_stage_at(unsigned char* p) {
+    PullStage s;
+    s.kend = reinterpret_cast<u32*>(p);
+    p += al16(WLIST * 4);
+    s.seg = reinterpret_cast<u32*>(p);
+    p += al16(PULL_WARP_MAX * 4);
+    s.cell = reinterpret_cast<u32*>(p);
+    p += al16(PULL_WARP_MAX * 4);
+    s.oth = reinterpret_cast<u32*>(p);
+    return s;
+}
+
+__device__ __forceinline__ void stage_pull(const DevStruct& S, u32 k0, u32 k1, u32 e0, u32 e1, const PullStage& st,
+                                           bool cells, u32 nstage) {
+    const u32 lane = wlane();
+    if (lane < k1 - k0) st.kend[lane] = S.pl_off[k0 + lane + 1] - e0;
+    const u32 no = S.nb - 1;
+    for (u32 i = lane; i < e1 - e0; i += 32) {
+        const u32 e = e0 + i;
+        st.seg[i] = __ldcs(S.pl_seg + e);
+        if (cells) st.cell[i] = __ldcs(S.pl_cell + e);
+#pragma unroll
+        for (u32 o = 0; o < u32(WNO); o++)
+            if (o < nstage) st.oth[o * PULL_WARP_MAX + i] = __ldcs(S.pl_other + size_t(e) * no + o);
+    }
 }
 
 // Operator pass 2 on short coordinate lists (k >= ms_acc): Y[k] = nr_k P[k] + sum over the cells
-// c of k of W_c (sum_{other b} P[coord_b(c)] - t_{s(c)}). Lanes (g, j) walk the entries of a
-// round (indices prefetched by lane = entry), groups combined in order per coordinate.
-template <class T>
-__global__ void __launch_bounds__(WPB * 32) k_wpull_apply(DevStruct S, DevWeights W, WarpTiles wt,
-                                                          const T* __restrict__ P, const T* __restrict__ t, int R,
-                                                          int j0, int Rc, T* __restrict__ Y) {
-    __shared__ u32 seg_s[WPB][32];
-    __shared__ u32 oth_s[WPB][3 * 32];
-    __shared__ double w_s[WPB][32];
-    const u32 wi = wid_in_cta(), lane = wlane();
-    const GMap gm = gmap(Rc);
+// c of k of W_c (sum_{other b} P[coord_b(c)] - t_{s(c)}).
+template <class T, int RCP, int NBK>
+__global__ void __launch_bounds__(WPB * 32, 4) k_wpull_apply(DevStruct S, DevWeights W, WarpTiles wt,
+                                                             const T* __restrict__ P, const T* __restrict__ t, int R,
+                                                             int j0, int Rc, T* __restrict__ Y) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using L_t = Lanes<RCP>;
+    constexpr int G = L_t::G;
+    constexpr int NO = NBK - 1;  // staged other blocks (all of them below WNB blocks)
+    const PullStage st = pull_stage_at(smem_raw + size_t(wid_in_cta()) * pull_bytes());
+    const L_t L(Rc);
+    const u32 Ru = u32(R);
     const u32 no = S.nb - 1;
-    const u32 wid = blockIdx.x * WPB + wi, nw = gridDim.x * WPB;
+    const bool weighted = W.cell_w != nullptr;
+    const T* Pj = P + j0 + L.j;
+    const T* tj = t + j0 + L.j;
+    const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
+    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
     for (u32 tile = wid; tile < wt.n; tile += nw) {
-        const u32 k0 = wt.k0[tile], k1 = wt.k1[tile];
-        for (u32 k = k0; k < k1; k++) {
-            const u32 a = S.pl_off[k], b = S.pl_off[k + 1];
+        const u32 k0 = tb.x, k1 = tb.y, e0 = tb.z;
+        stage_pull(S, k0, k1, e0, tb.w, st, weighted, u32(NO));
+        if (tile + nw < wt.n) tb = wt.t[tile + nw];
+        __syncwarp();
+        u32 i0 = 0;
+        for (u32 kl = 0; kl < k1 - k0; kl++) {
+            const u32 ie = st.kend[kl];
             T acc = T(0);
-            for (u32 base = a; base < b; base += 32) {
-                const u32 e = base + lane;
-                if (e < b) {
-                    seg_s[wi][lane] = __ldcs(S.pl_seg + e);
-                    for (u32 o = 0; o < no && o < 3; o++) oth_s[wi][o * 32 + lane] = __ldcs(S.pl_other + size_t(e) * no + o);
-                    w_s[wi][lane] = W.cell_w ? W.cell_w[__ldcs(S.pl_cell + e)] : 1.0;
-                }
-                __syncwarp();
-                const u32 cnt = min(32u, b - base);
-                if (gm.on) {
+            if (L.on) {
 #pragma unroll 8
-                    for (u32 i = gm.g; i < cnt; i += gm.G) {
-                        T u = -__ldcg(t + size_t(seg_s[wi][i]) * R + j0 + gm.j);
-                        for (u32 o = 0; o < no; o++) u += P[size_t(oth_s[wi][o * 32 + i]) * R + j0 + gm.j];
-                        acc += T(w_s[wi][i]) * u;
-                    }
+                for (u32 i = i0 + L.g; i < ie; i += G) {
+                    T v = -__ldcg(tj + size_t(st.seg[i]) * Ru);
+#pragma unroll
+                    for (int o = 0; o < NO; o++) v += Pj[size_t(st.oth[o * PULL_WARP_MAX + i]) * Ru];
+                    if constexpr (NBK == WNB)
+                        for (u32 o = WNO; o < no; o++) v += Pj[size_t(S.pl_other[size_t(e0 + i) * no + o]) * Ru];
+                    acc += weighted ? T(W.cell_w[st.cell[i]]) * v : v;
                 }
-                __syncwarp();
             }
-            acc = group_sum(acc, gm);
-            if (gm.on && gm.g == 0) {
-                const size_t o = size_t(k) * R + j0 + gm.j;
-                Y[o] = T(W.nr[k]) * P[o] + acc;
+            acc = group_total(acc, L);
+            if (L.on && L.g == 0) {
+                const size_t o = size_t(k0 + kl) * Ru + j0 + L.j;
+                Y[o] = T(W.nr[k0 + kl]) * P[o] + acc;
             }
+            i0 = ie;
         }
+        __syncwarp();
     }
 }
 
 // ---------------------------------------------------------------------------------------------
-// Per-warp shared memory of the row passes (wrows_bytes(Rc) per warp).
-struct WRows {
-    double* v;
-    double* u;
-    double* wr;
-    double* cw;
-    u32* code;
-    u32* segl;
-    u32* row0;
-};
-
-__device__ __forceinline__ WRows wrows_at(unsigned char* base, int Rc) {
-    unsigned char* p = base + size_t(wid_in_cta()) * wrows_bytes(Rc);
-    WRows w;
-    w.v = reinterpret_cast<double*>(p);
-    p += al16(WT * Rc * 8);
-    w.u = reinterpret_cast<double*>(p);
-    p += al16(WT * Rc * 8);
-    w.wr = reinterpret_cast<double*>(p);
-    p += al16(WT * 8);
-    w.cw = reinterpret_cast<double*>(p);
-    p += al16(WT * 8);
-    w.code = reinterpret_cast<u32*>(p);
-    p += al16(4 * WT * 4);
-    w.segl = reinterpret_cast<u32*>(p);
-    p += al16(WT * 4);
-    w.row0 = reinterpret_cast<u32*>(p);
-    return w;
-}
-
-// Flat coalesced load of rows [r0, r1) x columns [j0, j0 + Rc) into v.
-__device__ __forceinline__ void load_rows(const double* __restrict__ rows, int R, int j0, int Rc, u32 r0, u32 r1,
-                                          const double* w_rows, const WRows& sm) {
-    const u32 lane = wlane();
-    const u32 ne = (r1 - r0) * u32(Rc);
-#pragma unroll 4
-    for (u32 f = lane; f < ne; f += 32) sm.v[f] = __ldcs(rows + size_t(r0 + f / Rc) * R + j0 + f % Rc);
-    if (w_rows && lane < r1 - r0) sm.wr[lane] = w_rows[r0 + lane];
-}
-
-__device__ __forceinline__ void load_cells_rows(const DevStruct& S, const DevWeights& W, u32 c0, u32 c1, u32 s0,
-                                                const WRows& sm) {
-    const u32 lane = wlane();
-    const u32 c = c0 + lane;
-    if (c < c1) {
-        sm.cw[lane] = cellw(W, c);
-        for (u32 b = 0; b < S.nb && b < 4; b++) sm.code[b * WT + lane] = __ldcs(S.coord + size_t(b) * S.M + c);
-        u32 s = s0;
-        while (S.seg_off[s + 1] <= c) s++;
-        sm.segl[lane] = s - s0;
-        sm.row0[lane] = row0_of(S, c);
-        if (c == c1 - 1) sm.row0[lane + 1] = row1_of(S, c);
-    }
-}
-
-// Right-hand side pass 1 (operator.rs:969-1066) on short segments: b1_s = sum over the rows of s
-// of w v; per-CTA partials of [sum w v^2, sum w v] (cta_part[blockIdx][2R], this chunk's
-// columns); small coordinates' sums of s_c - W_c b1_s / n1_s into cta_small.
-__global__ void __launch_bounds__(WPB * 32) k_wseg_rhs(DevStruct S, DevWeights W, WarpTiles wt,
-                                                       const double* __restrict__ rows, int R, int j0, int Rc,
-                                                       double* __restrict__ b1, double* __restrict__ cta_part,
-                                                       double* __restrict__ cta_small) {
+// Right-hand side pass 1 (operator.rs:969-1066) on short segments: s_c = sum over the rows of c of
+// w v, b1_s = sum_c s_c; per-CTA partials of [sum w v^2, sum w v] (cta_part[blockIdx][2R], this
+// chunk's columns); small coordinates' sums of s_c - W_c b1_s / n1_s into cta_small.
+template <int RCP>
+__global__ void __launch_bounds__(WPB * 32, 4) k_wseg_rhs(DevStruct S, DevWeights W, WarpTiles wt,
+                                                          const double* __restrict__ rows, int R, int j0, int Rc,
+                                                          double* __restrict__ b1, double* __restrict__ cta_part,
+                                                          double* __restrict__ cta_small) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const WRows sm = wrows_at(smem_raw, Rc);
-    double* wacc_all = reinterpret_cast<double*>(smem_raw + WPB * wrows_bytes(Rc));
-    double* colsum = wacc_all + size_t(WPB) * S.ms_acc * Rc;  // WPB x 2 x Rc
-    double* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * Rc;
+    using L_t = Lanes<RCP>;
+    constexpr int G = L_t::G;
+    unsigned char* mine = smem_raw + size_t(wid_in_cta()) * wrhs_bytes(Rc);
+    double* u = reinterpret_cast<double*>(mine);
+    double* ps = reinterpret_cast<double*>(mine + al16(WT * Rc * 8));
+    const SegStage st = seg_stage_at(mine + al16(WT * Rc * 8) + al16(WSEG * 32 * 8));
+    double* wacc_all = reinterpret_cast<double*>(smem_raw + WPB * wrhs_bytes(Rc));
+    double* colsum = wacc_all + size_t(WPB) * S.ms_acc * 32;  // WPB x 2 x 32
+    double* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 32;
     const bool acc = cta_small != nullptr;
-    const u32 lane = wlane();
+    const bool trivial = S.cell_row == nullptr;
+    const L_t L(Rc);
+    const u32 Ru = u32(R);
     if (acc)
-        for (u32 i = lane; i < S.ms_acc * u32(Rc); i += 32) wacc[i] = 0.0;
-    double q = 0.0, ws = 0.0;  // column lane's totals (lane < Rc)
+        for (u32 i = L.lane; i < S.ms_acc * 32; i += 32) wacc[i] = 0.0;
+    double q = 0.0, ws = 0.0;  // this lane's [sum w v^2, sum w v]
+    const double* vj = rows + j0 + L.j;
+    const u32 ncode = acc ? S.ns_acc : 0u;
     const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
+    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
     for (u32 tile = wid; tile < wt.n; tile += nw) {
-        const u32 s0 = wt.k0[tile], s1 = wt.k1[tile], c0 = wt.e0[tile], c1 = wt.e1[tile];
-        const u32 r0 = row0_of(S, c0), r1 = row0_of(S, c1);
-        load_rows(rows, R, j0, Rc, r0, r1, W.w_rows, sm);
-        load_cells_rows(S, W, c0, c1, s0, sm);
+        const u32 s0 = tb.x, ns = tb.y - tb.x, c0 = tb.z, nc = tb.w - tb.z;
+        stage_cells(S, W, s0, tb.y, c0, tb.w, st, ncode, true);
+        if (tile + nw < wt.n) tb = wt.t[tile + nw];
         __syncwarp();
-        for (u32 jj = lane; jj < u32(Rc); jj += 32) {
-            u32 i = 0;
-            for (u32 s = s0; s < s1; s++) {
-                const u32 e = S.seg_off[s + 1] - c0;
-                double sum = 0.0;
-                for (u32 ci = i; ci < e; ci++) {
+        stage_maps(nc, st, false);
+        __syncwarp();
+        if (L.on) {
+            SegRun<double> sr;
+            if (trivial) {  // one row per cell: row = cell
+#pragma unroll
+                for (int k0 = 0; k0 < L_t::KN; k0 += L_t::CH) {
+                    double x[L_t::CH], w[L_t::CH];
+#pragma unroll
+                    for (int k = 0; k < L_t::CH; k++) {
+                        const u32 i = L.g + u32((k0 + k) * G);
+                        x[k] = i < nc ? __ldcs(vj + size_t(c0 + i) * Ru) : 0.0;
+                        w[k] = i < nc && W.w_rows ? W.w_rows[c0 + i] : 1.0;
+                    }
+#pragma unroll
+                    for (int k = 0; k < L_t::CH; k++) {
+                        const u32 i = L.g + u32((k0 + k) * G);
+                        if (i < nc) {
+                            const double wx = w[k] * x[k];
+                            q += wx * x[k];
+                            if (acc) u[i * Rc + L.j] = wx;
+                            sr.add(st.segl[i], wx, ps, L.lane);
+                        }
+                    }
+                }
+            } else {
+                for (u32 i = L.g; i < nc; i += G) {
                     double sc = 0.0;
-                    for (u32 rr = sm.row0[ci] - r0; rr < sm.row0[ci + 1] - r0; rr++) {
-                        const double x = sm.v[rr * Rc + jj];
-                        const double wx = W.w_rows ? sm.wr[rr] * x : x;
+                    for (u32 r = st.row0[i]; r < st.row0[i + 1]; r++) {
+                        const double x = __ldcs(vj + size_t(r) * Ru);
+                        const double wx = W.w_rows ? W.w_rows[r] * x : x;
                         sc += wx;
                         q += wx * x;
                     }
-                    sm.u[ci * Rc + jj] = sc;
-                    sum += sc;
+                    if (acc) u[i * Rc + L.j] = sc;
+                    sr.add(st.segl[i], sc, ps, L.lane);
                 }
-                ws += sum;
-                b1[size_t(s) * R + j0 + jj] = sum;
-                if (acc) {
-                    const double bt = sum * W.n1inv[s];
-                    for (u32 ci = i; ci < e; ci++) {
-                        const double z = sm.u[ci * Rc + jj] - sm.cw[ci] * bt;
-                        for (u32 b = 0; b < S.ns_acc; b++) wacc[sm.code[b * WT + ci] * Rc + jj] += z;
-                    }
-                }
-                i = e;
             }
+            sr.finish(ns, ps, L.lane);
+        }
+        __syncwarp();
+        if (L.on)
+            for (u32 sl = L.g; sl < ns; sl += G) {
+                const double b = seg_total<RCP>(ps, sl, L.j);
+                ws += b;
+                b1[size_t(s0 + sl) * Ru + j0 + L.j] = b;
+                ps[sl * 32 + L.j] = b * st.n1i[sl];
+            }
+        if (acc) {
+            __syncwarp();
+            small_phase(S, st, L, nc, Rc, u, ps, wacc);
         }
         __syncwarp();
     }
-    for (u32 jj = lane; jj < u32(Rc); jj += 32) {
-        colsum[(size_t(wid_in_cta()) * 2) * Rc + jj] = q;
-        colsum[(size_t(wid_in_cta()) * 2 + 1) * Rc + jj] = ws;
-    }
+    colsum[(size_t(wid_in_cta()) * 2) * 32 + L.lane] = L.on ? q : 0.0;
+    colsum[(size_t(wid_in_cta()) * 2 + 1) * 32 + L.lane] = L.on ? ws : 0.0;
     __syncthreads();
     for (u32 i = threadIdx.x; i < 2 * u32(Rc); i += blockDim.x) {
+        const u32 half = i / u32(Rc), j = i % u32(Rc);
         double s = 0.0;
-        for (int w = 0; w < WPB; w++) s += colsum[size_t(w) * 2 * Rc + i];
-        const u32 half = i / Rc, jj = i % Rc;
-        cta_part[size_t(blockIdx.x) * 2 * R + half * R + j0 + jj] = s;
+        for (int w = 0; w < WPB; w++)
+#pragma unroll
+            for (int g = 0; g < G; g++) s += colsum[(size_t(w) * 2 + half) * 32 + g * RCP + j];
+        cta_part[size_t(blockIdx.x) * 2 * R + half * R + j0 + j] = s;
     }
-    if (acc) flush_wacc(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
+    if (acc) flush_wacc<RCP>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
 }
 
 // Right-hand side pass 2 on short coordinate lists (k >= ms_acc): rhs[k] = sum over the cells c
 // of k of (s_c - W_c b1_{s(c)} / n1_{s(c)}).
-__global__ void __launch_bounds__(WPB * 32) k_wpull_rhs(DevStruct S, DevWeights W, WarpTiles wt,
-                                                        const double* __restrict__ rows, const double* __restrict__ b1,
-                                                        int R, int j0, int Rc, double* __restrict__ Y) {
-    __shared__ u32 cell_s[WPB][32];
-    __shared__ u32 seg_s[WPB][32];
-    const u32 wi = wid_in_cta(), lane = wlane();
-    const GMap gm = gmap(Rc);
-    const u32 wid = blockIdx.x * WPB + wi, nw = gridDim.x * WPB;
+template <int RCP>
+__global__ void __launch_bounds__(WPB * 32, 4) k_wpull_rhs(DevStruct S, DevWeights W, WarpTiles wt,
+                                                           const double* __restrict__ rows,
+                                                           const double* __restrict__ b1, int R, int j0, int Rc,
+                                                           double* __restrict__ Y) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using L_t = Lanes<RCP>;
+    constexpr int G = L_t::G;
+    const PullStage st = pull_stage_at(smem_raw + size_t(wid_in_cta()) * pull_bytes());
+    const L_t L(Rc);
+    const u32 Ru = u32(R);
+    const bool trivial = S.cell_row == nullptr;
+    const double* vj = rows + j0 + L.j;
+    const double* bj = b1 + j0 + L.j;
+    const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
+    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
     for (u32 tile = wid; tile < wt.n; tile += nw) {
-        const u32 k0 = wt.k0[tile], k1 = wt.k1[tile];
-        for (u32 k = k0; k < k1; k++) {
-            const u32 a = S.pl_off[k], b = S.pl_off[k + 1];
+        const u32 k0 = tb.x, k1 = tb.y;
+        stage_pull(S, k0, k1, tb.z, tb.w, st, true, 0u);
+        if (tile + nw < wt.n) tb = wt.t[tile + nw];
+        __syncwarp();
+        u32 i0 = 0;
+        for (u32 kl = 0; kl < k1 - k0; kl++) {
+            const u32 ie = st.kend[kl];
             double acc = 0.0;
-            for (u32 base = a; base < b; base += 32) {
-                const u32 e = base + lane;
-                if (e < b) {
-                    cell_s[wi][lane] = __ldcs(S.pl_cell + e);
-                    seg_s[wi][lane] = __ldcs(S.pl_seg + e);
-                }
-                __syncwarp();
-                const u32 cnt = min(32u, b - base);
-                if (gm.on) {
+            if (L.on) {
+                if (trivial) {
 #pragma unroll 8
-                    for (u32 i = gm.g; i < cnt; i += gm.G) {
-                        const u32 c = cell_s[wi][i], s = seg_s[wi][i];
+                    for (u32 i = i0 + L.g; i < ie; i += G) {
+                        const u32 c = st.cell[i], s = st.seg[i];
+                        const double x = __ldcs(vj + size_t(c) * Ru);
+                        const double sc = W.w_rows ? W.w_rows[c] * x : x;
+                        acc += sc - cellw(W, c) * __ldcg(bj + size_t(s) * Ru) * W.n1inv[s];
+                    }
+                } else {
+#pragma unroll 4
+                    for (u32 i = i0 + L.g; i < ie; i += G) {
+                        const u32 c = st.cell[i], s = st.seg[i];
                         double sc = 0.0;
-                        const u32 re = row1_of(S, c);
-                        for (u32 row = row0_of(S, c); row < re; row++) {
-                            const double x = rows[size_t(row) * R + j0 + gm.j];
-                            sc += W.w_rows ? W.w_rows[row] * x : x;
+                        const u32 re = S.cell_row[c + 1];
+                        for (u32 r = S.cell_row[c]; r < re; r++) {
+                            const double x = __ldcs(vj + size_t(r) * Ru);
+                            sc += W.w_rows ? W.w_rows[r] * x : x;
                         }
-                        acc += sc - cellw(W, c) * __ldcg(b1 + size_t(s) * R + j0 + gm.j) * W.n1inv[s];
+                        acc += sc - cellw(W, c) * __ldcg(bj + size_t(s) * Ru) * W.n1inv[s];
                     }
                 }
-                __syncwarp();
             }
-            acc = group_sum(acc, gm);
-            if (gm.on && gm.g == 0) Y[size_t(k) * R + j0 + gm.j] = acc;
+            acc = group_total(acc, L);
+            if (L.on && L.g == 0) Y[size_t(k0 + kl) * Ru + j0 + L.j] = acc;
+            i0 = ie;
         }
+        __syncwarp();
     }
 }
 
 // Residualization of short segments (operator.rs:1107-1179): alpha_s = (b1_s - sum W_c u_c) / n1_s,
 // u_c = sum_b x[coord_b(c)]; every row of cell c loses alpha_s + u_c.
-__global__ void __launch_bounds__(WPB * 32) k_wresid(DevStruct S, DevWeights W, WarpTiles wt, double* __restrict__ rows,
-                                                     int R, int j0, int Rc, const double* __restrict__ x,
-                                                     const double* __restrict__ b1, double* __restrict__ alpha) {
+template <int RCP, int NBK>
+__global__ void __launch_bounds__(WPB * 32, 4) k_wresid(DevStruct S, DevWeights W, WarpTiles wt,
+                                                        double* __restrict__ rows, int R, int j0, int Rc,
+                                                        const double* __restrict__ x, const double* __restrict__ b1,
+                                                        double* __restrict__ alpha) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const WRows sm = wrows_at(smem_raw, Rc);
-    const u32 lane = wlane();
-    const GMap gm = gmap(Rc);
+    using L_t = Lanes<RCP>;
+    constexpr int G = L_t::G;
+    constexpr int KS = (WSEG + G - 1) / G;  // tile segments per group
+    unsigned char* mine = smem_raw + size_t(wid_in_cta()) * wresid_bytes(Rc);
+    double* u = reinterpret_cast<double*>(mine);
+    double* ps = reinterpret_cast<double*>(mine + al16(WT * Rc * 8));
+    const SegStage st = seg_stage_at(mine + al16(WT * Rc * 8) + al16(WSEG * 32 * 8));
+    double* bs = reinterpret_cast<double*>(mine + wseg_bytes(Rc, 8));  // the tile's b1 (WSEG x Rc)
+    const bool trivial = S.cell_row == nullptr;
+    const L_t L(Rc);
+    const u32 Ru = u32(R);
+    const double* xj = x + j0 + L.j;
+    double* vj = rows + j0 + L.j;
+    const u32 ncode = NBK < WNB ? u32(NBK) : u32(WNB);
     const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
+    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
     for (u32 tile = wid; tile < wt.n; tile += nw) {
-        const u32 s0 = wt.k0[tile], s1 = wt.k1[tile], c0 = wt.e0[tile], c1 = wt.e1[tile];
-        const u32 nc = c1 - c0;
-        const u32 r0 = row0_of(S, c0), r1 = row0_of(S, c1);
-        load_rows(rows, R, j0, Rc, r0, r1, nullptr, sm);
-        load_cells_rows(S, W, c0, c1, s0, sm);
-        __syncwarp();
-        if (gm.on) {
-#pragma unroll 4
-            for (u32 i = gm.g; i < nc; i += gm.G) {
-                double v = 0.0;
-                for (u32 b = 0; b < S.nb; b++) v += x[size_t(sm.code[b * WT + i]) * R + j0 + gm.j];
-                sm.u[i * Rc + gm.j] = v;
+        const u32 s0 = tb.x, ns = tb.y - tb.x, c0 = tb.z, nc = tb.w - tb.z;
+        stage_cells(S, W, s0, tb.y, c0, tb.w, st, ncode, !trivial);
+        if (L.on) {
+            double v[KS];
+#pragma unroll
+            for (int k = 0; k < KS; k++) {
+                const u32 sl = L.g + u32(k * G);
+                v[k] = sl < ns ? b1[size_t(s0 + sl) * Ru + j0 + L.j] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < KS; k++) {
+                const u32 sl = L.g + u32(k * G);
+                if (sl < ns) bs[sl * Rc + L.j] = v[k];
             }
         }
+        if (tile + nw < wt.n) tb = wt.t[tile + nw];
         __syncwarp();
-        // per segment (lane = column): alpha, then the segment's rows lose alpha + u_c in place
-        for (u32 jj = lane; jj < u32(Rc); jj += 32) {
-            u32 i = 0;
-            for (u32 s = s0; s < s1; s++) {
-                const u32 e = S.seg_off[s + 1] - c0;
-                double sum = 0.0;
-                for (u32 ci = i; ci < e; ci++) sum += sm.cw[ci] * sm.u[ci * Rc + jj];
-                const double al = (b1[size_t(s) * R + j0 + jj] - sum) * W.n1inv[s];
-                if (alpha) alpha[size_t(s) * R + j0 + jj] = al;
-                for (; i < e; i++) {
-                    const double f = al + sm.u[i * Rc + jj];
-                    for (u32 rr = sm.row0[i] - r0; rr < sm.row0[i + 1] - r0; rr++) sm.v[rr * Rc + jj] -= f;
+        stage_maps(nc, st, !trivial);
+        __syncwarp();
+        if (L.on) {
+            SegRun<double> sr;
+            const u32* cg = st.code + L.g;
+#pragma unroll
+            for (int k0 = 0; k0 < L_t::KN; k0 += L_t::CH) {
+                double v[L_t::CH];
+#pragma unroll
+                for (int k = 0; k < L_t::CH; k++) {
+                    const u32 i = L.g + u32((k0 + k) * G);
+                    v[k] = i < nc ? gather_cell<NBK>(S, cg + (k0 + k) * G, xj, Ru, c0 + i) : 0.0;
+                }
+#pragma unroll
+                for (int k = 0; k < L_t::CH; k++) {
+                    const u32 i = L.g + u32((k0 + k) * G);
+                    if (i < nc) {
+                        u[i * Rc + L.j] = v[k];
+                        sr.add(st.segl[i], st.cw[i] * v[k], ps, L.lane);
+                    }
+                }
+            }
+            sr.finish(ns, ps, L.lane);
+        }
+        __syncwarp();
+        if (L.on)
+            for (u32 sl = L.g; sl < ns; sl += G) {
+                const double al = (bs[sl * Rc + L.j] - seg_total<RCP>(ps, sl, L.j)) * st.n1i[sl];
+                if (alpha) alpha[size_t(s0 + sl) * Ru + j0 + L.j] = al;
+                ps[sl * 32 + L.j] = al;
+            }
+        __syncwarp();
+        if (L.on) {
+            const u32 r0 = trivial ? c0 : st.row0[0];
+            const u32 nr = trivial ? nc : st.row0[nc] - r0;
+#pragma unroll
+            for (int k0 = 0; k0 < L_t::KN; k0 += L_t::CH) {
+                double v[L_t::CH];
+#pragma unroll
+                for (int k = 0; k < L_t::CH; k++) {
+                    const u32 r = L.g + u32((k0 + k) * G);
+                    v[k] = r < nr ? __ldcs(vj + size_t(r0 + r) * Ru) : 0.0;
+                }
+#pragma unroll
+                for (int k = 0; k < L_t::CH; k++) {
+                    const u32 r = L.g + u32((k0 + k) * G);
+                    if (r < nr) {
+                        const u32 i = trivial ? r : st.rcell[r];
+                        __stcs(vj + size_t(r0 + r) * Ru, v[k] - (ps[st.segl[i] * 32 + L.j] + u[i * Rc + L.j]));
+                    }
                 }
             }
         }
-        __syncwarp();
-        // coalesced store of the tile's rows
-        const u32 ne = (r1 - r0) * u32(Rc);
-#pragma unroll 4
-        for (u32 f = lane; f < ne; f += 32) __stcs(rows + size_t(r0 + f / Rc) * R + j0 + f % Rc, sm.v[f]);
         __syncwarp();
     }
 }

@@ -273,7 +273,7 @@ TileList build_tiles(const std::vector<u32>& off, u32 k_begin, u32 k_end, u32 ca
 namespace fereg {
 
 void split_tiles(const std::vector<u32>& off, const std::vector<u32>* weight, u32 k_begin, u32 k_end, u32 warp_max,
-                 u32 pack, u32 cta_cap, WarpTileList& wt, TileList& ct) {
+                 u32 pack, u32 max_lists, u32 cta_cap, WarpTileList& wt, TileList& ct) {
     auto wgt = [&](u32 k) { return weight ? (*weight)[k] : off[k + 1] - off[k]; };
     // warp tiles: consecutive lists of weight <= warp_max, packed while the total stays <= pack
     u32 k = k_begin;
@@ -285,7 +285,7 @@ void split_tiles(const std::vector<u32>& off, const std::vector<u32>* weight, u3
         u32 k1 = k, tot = 0;
         while (k1 < k_end) {
             const u32 w = wgt(k1);
-            if (w > warp_max || (tot + w > pack && k1 > k)) break;
+            if (w > warp_max || (k1 > k && (tot + w > pack || k1 - k >= max_lists))) break;
             tot += w;
             k1++;
         }

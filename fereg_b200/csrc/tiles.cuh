@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(TB) k_b1sq(u32 g1, const double* __restrict__ 
 // latency overlaps the gathers of x.
 constexpr int PF = TILE / (TB / RC_MAX);  // row elements per thread and chunk (one row per cell)
 
-__global__ void __launch_bounds__(TB) k_residualize(DevStruct S, DevWeights W, double* __restrict__ rows, int R,
+__global__ void __launch_bounds__(TB, 4) k_residualize(DevStruct S, DevWeights W, double* __restrict__ rows, int R,
                                                     const double* __restrict__ x, const double* __restrict__ b1,
                                                     const double* __restrict__ along, double* __restrict__ alpha) {
     __shared__ double vals[TILE * RC_MAX];

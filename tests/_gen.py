@@ -9,7 +9,7 @@ import numpy as np
 
 
 def panel(n_ind=600, years=10, n_firm=None, firm="random", seed=0, weighted=False, repeat=1, r=3,
-          disconnected=False, drop=0.0):
+          disconnected=False, drop=0.0, extra=()):
     rng = np.random.default_rng(seed)
     n = n_ind * years * repeat
     ind = np.repeat(np.arange(n_ind), years * repeat)
@@ -29,6 +29,9 @@ def panel(n_ind=600, years=10, n_firm=None, firm="random", seed=0, weighted=Fals
             f = np.where(half, n_firm // 2 + f % (n_firm - n_firm // 2), f % (n_firm // 2))
         codes.append(f.astype(np.uint32))
         g.append(n_firm)
+    for levels in extra:  # further random terms (designs with more than three FE)
+        codes.append(rng.integers(0, levels, n).astype(np.uint32))
+        g.append(levels)
     keep = np.ones(n, dtype=bool)
     if drop > 0:
         keep = rng.random(n) >= drop

@@ -28,6 +28,8 @@ CASES = {
     "one_fe": dict(n_ind=400, years=5, seed=9),
     # 160 rows per individual with random firms: FE1 levels of ~160 cells, split across tiles
     "long_segments": dict(n_ind=5000, years=10, n_firm=4500, seed=11, repeat=16, weighted=True),
+    # six terms: five blocks behind FE1, more than the warp tiles stage in shared memory
+    "six_fe": dict(n_ind=8000, years=6, n_firm=2000, seed=12, extra=(40, 300, 5000), weighted=True),
 }
 
 
@@ -157,3 +159,21 @@ def test_refined_fp32_matches_oracle(pair):
     for j in range(z.shape[1]):
         fit = gpu.fit_rows(i1["coefs"], j)
         assert rel(z[:, j] - fit, z1[:, j]) <= 1e-9
+
+
+@pytest.mark.parametrize("case", ["three_fe_weighted", "repeated_cells", "small_firms"])
+@pytest.mark.parametrize("r", [1, 2, 7, 16, 37])
+def test_column_counts_match_oracle(case, r):
+    """Column blocks of every padded width (1..32) and blocks wider than one chunk."""
+    spec = dict(CASES[case], r=r)
+    codes, g, w, z = panel(**spec)
+    gpu, orc = fb.Absorber(codes, g, w), oracle.Absorber(codes, g, w)
+    z1, z2 = z.copy(), z.copy()
+    gpu.residualize(z1, tol=1e-12, maxiter=100000)
+    orc.residualize(z2, tol=1e-12, maxiter=100000)
+    for j in range(r):
+        assert rel(z1[:, j], z2[:, j]) <= 1e-9, (case, r, j)
+    y1, b11, q1, s1 = gpu.rhs(z)
+    y2, b12, q2, s2 = orc.rhs(z)
+    assert rel(y1, y2) <= 1e-12 and rel(b11, b12) <= 1e-12
+    assert rel(q1, q2) <= 1e-12 and rel(s1, s2) <= 1e-12
