@@ -71,6 +71,7 @@ def _setup(L):
     L.fereg_absorber_rhs.argtypes = [P, f64p, C.c_size_t, f64p, f64p, f64p, f64p]
     L.fereg_absorber_precond.argtypes = [P, f64p, C.c_size_t, f64p]
     L.fereg_absorber_weight_state.argtypes = [P, f64p, f64p, f64p, u8p, f64p]
+    L.fereg_absorber_rhs_noalloc.argtypes = [P, P, C.c_size_t, P, P, P]
     L.fereg_absorber_stream.argtypes = [P]
     L.fereg_absorber_stream.restype = P
     L.fereg_absorber_set_profiling.argtypes = [P, C.c_int]
@@ -210,6 +211,10 @@ class Absorber:
         _check(lib().fereg_absorber_rhs(self.h, _p(rows, f64p), r, _p(y, f64p), _p(b1, f64p), _p(wsq, f64p),
                                         _p(wsum, f64p)))
         return y, b1, wsq, wsum
+
+    def rhs_noalloc(self, rows_ptr, r, y_ptr, b1_ptr, colsum_ptr):
+        """fereg_absorber_rhs_noalloc on device pointers (queued on the handle's stream)."""
+        _check(lib().fereg_absorber_rhs_noalloc(self.h, P(rows_ptr), r, P(y_ptr), P(b1_ptr), P(colsum_ptr)))
 
     def precond(self, r_):
         r_ = np.ascontiguousarray(r_, dtype=np.float64)

@@ -604,6 +604,94 @@ void launch_rhs(Scratch& d, const DevStruct& S, const DevWeights& W, const doubl
     CK(cudaGetLastError());
 }
 
+// Scratch of the right-hand side pass held outside the handle (the allocation-free entry point):
+// per-CTA column partials of the short (cta2) and long (cta) segment kernels, slice partials of
+// the long lists (part) and the small coordinates' partial rows (small). Sizes in doubles.
+struct RhsScratch {
+    double *cta2, *cta, *part, *small;
+};
+inline size_t rhs_scratch_part(size_t doubles) { return (doubles + 31) / 32 * 32; }  // 256-byte steps
+inline size_t rhs_scratch_need(const DevStruct& S, size_t r, u32 ms_acc) {
+    return rhs_scratch_part(size_t(GRID_S) * 2 * r) + rhs_scratch_part(size_t(std::max(GRID_T, GRID_V)) * 3 * r) +
+           rhs_scratch_part(std::max<size_t>(1, size_t(std::max(S.seg.nparts, S.pull.nparts)) * r)) +
+           rhs_scratch_part(std::max<size_t>(1, small_rows() * ms_acc * r));
+}
+inline RhsScratch rhs_scratch_carve(double* p, const DevStruct& S, size_t r, u32 ms_acc) {
+    RhsScratch s;
+    s.cta2 = p;
+    p += rhs_scratch_part(size_t(GRID_S) * 2 * r);
+    s.cta = p;
+    p += rhs_scratch_part(size_t(std::max(GRID_T, GRID_V)) * 3 * r);
+    s.part = p;
+    p += rhs_scratch_part(std::max<size_t>(1, size_t(std::max(S.seg.nparts, S.pull.nparts)) * r));
+    s.small = p;
+    return s;
+}
+
+// The kernels of launch_rhs, in the same order, on the scratch `x` (no phase timing).
+void launch_rhs_scratch(Scratch& d, const DevStruct& S, const DevWeights& W, const double* rows, int R, double* b1,
+                        double* rhs, double* colsum, const RhsScratch& x, cudaStream_t st) {
+    const bool acc = S.ms_acc > 0;
+    const u32 len = S.ms_acc * u32(R);
+    if (d.wseg.n) {
+        for (int j0 = 0; j0 < R; j0 += WCOLS) {
+            const int Rc = std::min(WCOLS, R - j0);
+            const size_t shm = wrhs_smem(Rc, S.ms_acc);
+            with_rcp<WNB>(Rc, WNB, [&](auto c, auto) {
+                constexpr int RCP = decltype(c)::value;
+                allow_smem(k_wseg_rhs<RCP>, shm);
+                k_wseg_rhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, b1, x.cta2,
+                                                                acc ? x.small : nullptr);
+            });
+            d.launches++;
+        }
+    } else {
+        // the short-segment partials start at zero when no short-segment kernel writes them
+        CK(cudaMemsetAsync(x.cta2, 0, size_t(GRID_S) * 2 * R * sizeof(double), st));
+        if (acc) CK(cudaMemsetAsync(x.small, 0, size_t(GRID_S) * len * sizeof(double), st));
+    }
+    if (S.seg.n) {
+        double* sb = x.small + size_t(GRID_S) * len;
+        k_seg_rhs<<<GRID_T, THREADS, 0, st>>>(S, W, rows, R, b1, x.part, x.cta, acc ? sb : nullptr);
+        d.launches++;
+        if (S.seg.nfix) {
+            k_fix<double><<<std::min<u32>(S.seg.nfix, GRID_T), THREADS, 0, st>>>(S.seg, W, nullptr, x.part, R, 2, b1);
+            d.launches++;
+            if (acc) {
+                k_rhs_small_slices<<<GRID_T, THREADS, 0, st>>>(S, W, rows, b1, R, sb + size_t(GRID_T) * len);
+                d.launches++;
+            }
+        }
+    }
+    reduce_cols(d, x.cta2, GRID_S, 2 * R, colsum, st, S.seg.n ? x.cta : nullptr, GRID_T);
+    k_b1sq<<<GRID_V, THREADS, 0, st>>>(S.g1, b1, W.n1inv, R, x.cta);
+    d.launches++;
+    reduce_cols(d, x.cta, GRID_V, R, colsum + 2 * R, st);
+    if (S.m > 0) {
+        if (d.wpull.n)
+            for (int j0 = 0; j0 < R; j0 += WCOLS) {
+                const int Rc = std::min(WCOLS, R - j0);
+                with_rcp<WNB>(Rc, WNB, [&](auto c, auto) {
+                    constexpr int RCP = decltype(c)::value;
+                    k_wpull_rhs<RCP><<<GRID_S, WPB * 32, wpull_smem(), st>>>(S, W, d.wpull.set(), rows, b1, R, j0, Rc,
+                                                                              rhs);
+                });
+                d.launches++;
+            }
+        if (S.pull.n) {
+            k_pull_rhs<<<GRID_T, THREADS, 0, st>>>(S, W, rows, b1, R, rhs, x.part);
+            d.launches++;
+            if (S.pull.nfix) {
+                k_fix<double><<<std::min<u32>(S.pull.nfix, GRID_T), THREADS, 0, st>>>(S.pull, W, nullptr, x.part, R, 2,
+                                                                                      rhs);
+                d.launches++;
+            }
+        }
+        if (acc) launch_small_reduce<double>(d, S, x.small, R, rhs, st);
+    }
+    CK(cudaGetLastError());
+}
+
 }  // namespace
 
 void GpuAbsorber::apply_host(const double* p, size_t r, double* y) {
@@ -656,6 +744,21 @@ void GpuAbsorber::rhs_host(const double* rows, size_t r, double* y, double* b1, 
         wsq[j] = cs[j];
         wsum[j] = cs[r + j];
     }
+}
+
+void GpuAbsorber::rhs_device_scratch(const double* rows, size_t r, double* rhs, double* b1, double* colsum,
+                                     double* scratch, size_t cap) {
+    if (r == 0) return;
+    const DevStruct S = d_->ds(hs_);
+    const size_t need = rhs_scratch_need(S, r, d_->ms_acc);
+    if (need > cap) {
+        std::ostringstream o;
+        o << "fereg: the allocation-free rhs pass needs " << need * sizeof(double) << " bytes of scratch for " << r
+          << " columns; its static scratch holds " << cap * sizeof(double) << " bytes";
+        throw Error(RC_INVALID_INPUT, o.str());
+    }
+    launch_rhs_scratch(*d_, S, d_->dw(), rows, int(r), b1, rhs, colsum, rhs_scratch_carve(scratch, S, r, d_->ms_acc),
+                       stream_);
 }
 
 SolveInfo GpuAbsorber::residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,

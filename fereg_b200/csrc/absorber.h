@@ -82,6 +82,12 @@ class GpuAbsorber {
     void apply_host(const double* p, size_t r, double* y);
     void rhs_host(const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum);
     void precond_host(const double* rr, size_t r, double* z);
+    // The right-hand side pass on caller device buffers with caller-provided scratch: queues the
+    // pass on the solver's stream and allocates nothing. rows: n x r; rhs: m x r; b1: g1 x r;
+    // colsum: 3 x r ([sum w v^2; sum w v; sum b1^2 / n1]). scratch holds `cap` doubles (256-byte
+    // aligned); a call that needs more is rejected (198).
+    void rhs_device_scratch(const double* rows, size_t r, double* rhs, double* b1, double* colsum, double* scratch,
+                            size_t cap);
     // Weight state (n1, nr, diag, redundant) as held for the kernels.
     void weight_state(double* n1, double* nr, double* diag, uint8_t* red, double* sw) const;
 

@@ -1,6 +1,7 @@
 // extern "C" boundary: exceptions become the reference's return codes plus a thread-local
 // message; nothing throws across.
 
+#include <mutex>
 #include <new>
 
 #include "../../include/fereg_b200.h"
@@ -46,6 +47,30 @@ Ctx to_ctx(const fereg_ctx* c) {
         x.verbose = c->verbose;
     }
     return x;
+}
+
+// Scratch of fereg_absorber_rhs_noalloc: a file-scope device array, so the call needs no
+// allocation. Its address is resolved once per device (cudaGetSymbolAddress, that device current)
+// by the first call on the device. Every call on a device uses the same array.
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(FEREG_RHS_NOALLOC_SCRATCH_BYTES);
+static __device__ __align__(256) double g_rhs_scratch[NOALLOC_SCRATCH_BYTES / sizeof(double)];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double* g_rhs_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_rhs_scratch_mu;
+
+double* rhs_scratch_on_current_device() {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) throw Error(RC_INTERNAL, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) throw Error(RC_INTERNAL, "fereg: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_rhs_scratch_mu);
+    if (!g_rhs_scratch_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_rhs_scratch);
+        if (e != cudaSuccess) throw Error(RC_INTERNAL, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_rhs_scratch_addr[dev] = static_cast<double*>(p);
+    }
+    return g_rhs_scratch_addr[dev];
 }
 
 void fill(fereg_solve_info* info, const SolveInfo& s) {
@@ -181,6 +206,15 @@ int fereg_absorber_apply(fereg_absorber* h, const double* p, size_t r, double* y
 
 int fereg_absorber_rhs(fereg_absorber* h, const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum) {
     return guard([&] { h->a.rhs_host(rows, r, y, b1, wsq, wsum); });
+}
+
+int fereg_absorber_rhs_noalloc(fereg_absorber* h, const double* rows, size_t r, double* y, double* b1,
+                               double* colsum) {
+    return guard([&] {
+        if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_rhs_noalloc: NULL handle");
+        double* scratch = rhs_scratch_on_current_device();
+        h->a.rhs_device_scratch(rows, r, y, b1, colsum, scratch, NOALLOC_SCRATCH_BYTES / sizeof(double));
+    });
 }
 
 int fereg_absorber_precond(fereg_absorber* h, const double* rr, size_t r, double* z) {

@@ -120,6 +120,25 @@ int fereg_absorber_precond(fereg_absorber* h, const double* rr, size_t r, double
 int fereg_absorber_weight_state(const fereg_absorber* h, double* n1, double* nr, double* diag, uint8_t* redundant,
                                 double* sw);
 
+/* Bytes of the static device scratch of fereg_absorber_rhs_noalloc. */
+#define FEREG_RHS_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* The right-hand side pass of fereg_absorber_rhs on device buffers, allocating nothing. No
+ * counterpart in the reference. It serves callers that must not allocate device memory once they
+ * run: a serving loop that shares the GPU with other streams (cudaFree waits for the whole device,
+ * cudaMalloc can stall) and hosts that hand all device memory to their own pool at start-up (an
+ * allocation inside the call could fail mid-run).
+ * rows: n x r row-major (row order); y: m x r; b1: g1 x r; colsum: 3 x r ([sum w v^2; sum w v;
+ * sum b1^2 / n1] per column); all device memory of the current device, which is the handle's.
+ * Scratch comes from one static device array of FEREG_RHS_NOALLOC_SCRATCH_BYTES (16 MiB); a call
+ * that needs more (many columns, many slices of long lists) returns 198 with the size in the
+ * message. The first call on a device resolves the array's address (cudaGetSymbolAddress): make
+ * that first call before any stream capture. The work is queued on the handle's stream
+ * (fereg_absorber_stream) and the call returns without waiting for it. Every call on a device
+ * uses the same scratch: calls that can overlap in time (other handles, or streams not ordered
+ * against the handle's) race. */
+int fereg_absorber_rhs_noalloc(fereg_absorber* h, const double* rows, size_t r, double* y, double* b1, double* colsum);
+
 #ifdef __cplusplus
 }
 #endif
