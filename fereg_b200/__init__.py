@@ -39,6 +39,27 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_uint64), ("escalated", C.c_int32), ("exact", C.c_int32)]
 
 
+OLS_SCALARS = ["N", "rank", "df_r", "df_m", "df_a", "df_a_initial", "df_a_redundant", "df_a_nested", "N_clust",
+               "N_clustervars", "N_clust1", "N_clust2", "num_singletons", "N_full", "report_constant", "rss", "tss",
+               "tss_within", "mss", "rmse", "r2", "r2_a", "r2_within", "r2_a_within", "ll", "ll_0", "F",
+               "sumweights", "ic"]
+VCE = {"unadjusted": 0, "robust": 1, "cluster": 2}
+WEIGHT_KIND = {None: 0, "aweight": 1, "fweight": 2, "pweight": 3}
+
+
+class OlsSpec(C.Structure):
+    _fields_ = [("vce", C.c_int), ("noconstant", C.c_int), ("firstpair", C.c_int), ("want_groupvar", C.c_int),
+                ("tol", C.c_double), ("maxiter", C.c_size_t), ("precision", C.c_int)]
+
+
+class OlsOut(C.Structure):
+    _fields_ = ([("b", C.POINTER(C.c_double)), ("V", C.POINTER(C.c_double)), ("status", C.POINTER(C.c_uint8)),
+                 ("resid", C.POINTER(C.c_double)), ("d", C.POINTER(C.c_double)),
+                 ("groupvar", C.POINTER(C.c_double)), ("dof_table", C.POINTER(C.c_double)),
+                 ("nslots", C.c_int32), ("k_all", C.c_int32), ("y_absorbed", C.c_int32)]
+                + [(k, C.c_double) for k in OLS_SCALARS])
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -72,6 +93,15 @@ def _setup(L):
     L.fereg_absorber_precond.argtypes = [P, f64p, C.c_size_t, f64p]
     L.fereg_absorber_weight_state.argtypes = [P, f64p, f64p, f64p, u8p, f64p]
     L.fereg_absorber_rhs_noalloc.argtypes = [P, P, C.c_size_t, P, P, P]
+    L.fereg_session_create.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.POINTER(u32p), u32p, C.c_int, f64p, C.c_int,
+                                       C.c_size_t, C.c_uint64, P, C.POINTER(P)]
+    L.fereg_session_destroy.argtypes = [P]
+    L.fereg_session_row_order.argtypes = [P, u32p]
+    L.fereg_session_ols.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(OlsSpec), C.POINTER(OlsOut)]
+    L.fereg_session_launches.argtypes = [P]
+    L.fereg_session_launches.restype = C.c_uint64
+    L.fereg_session_stream.argtypes = [P]
+    L.fereg_session_stream.restype = P
     L.fereg_absorber_stream.argtypes = [P]
     L.fereg_absorber_stream.restype = P
     L.fereg_absorber_set_profiling.argtypes = [P, C.c_int]
@@ -176,7 +206,7 @@ class Absorber:
             o += int(gq)
         return res
 
-    PHASES = ["rhs_seg", "rhs_pull", "apply", "precond", "vector", "residualize", "h2d", "d2h"]
+    PHASES = ["rhs_seg", "rhs_pull", "apply_seg", "precond", "vector", "residualize", "h2d", "d2h", "apply_pull"]
 
     def stream(self):
         """The handle's cudaStream_t as an integer."""
@@ -186,8 +216,8 @@ class Absorber:
         _check(lib().fereg_absorber_set_profiling(self.h, int(on)))
 
     def phase_times(self):
-        ms = np.zeros(8)
-        cnt = np.zeros(8, dtype=np.uint64)
+        ms = np.zeros(len(self.PHASES))
+        cnt = np.zeros(len(self.PHASES), dtype=np.uint64)
         _check(lib().fereg_absorber_phase_times(self.h, _p(ms, f64p), _p(cnt, u64p)))
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PHASES)}
 
@@ -231,3 +261,77 @@ class Absorber:
         _check(lib().fereg_absorber_weight_state(self.h, _p(n1, f64p), _p(nr, f64p), _p(diag, f64p), _p(red, u8p),
                                                  C.byref(sw)))
         return dict(n1=n1, nr=nr, diag=diag, redundant=red.astype(bool), sw=sw.value)
+
+
+class Session:
+    """Host mirror of the reference `Session` as `Session::ols` uses it (ols.rs:199-470), on the
+    B200 absorber. codes / clusters: prepared kept-order codes; w: kept-order weights of
+    weight_kind ("aweight", "fweight", "pweight") or None."""
+
+    def __init__(self, codes, g, clusters=(), cl_g=(), w=None, weight_kind=None, num_singletons=0):
+        n = len(codes[0]) if len(codes) else len(clusters[0]) if len(clusters) else len(w)
+        self._codes = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
+        self._cl = [np.ascontiguousarray(c, dtype=np.uint32) for c in clusters]
+        garr = np.asarray(g, dtype=np.uint32)
+        cgarr = np.asarray(cl_g, dtype=np.uint32)
+        cp = (u32p * max(1, len(self._codes)))(*[_p(c, u32p) for c in self._codes])
+        clp = (u32p * max(1, len(self._cl)))(*[_p(c, u32p) for c in self._cl])
+        wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        h = P()
+        _check(lib().fereg_session_create(cp, _p(garr, u32p), len(self._codes), clp, _p(cgarr, u32p), len(self._cl),
+                                          _p(wa, f64p), WEIGHT_KIND[weight_kind if w is not None else None], n,
+                                          int(num_singletons), None, C.byref(h)))
+        self.h = h
+        self.n = n
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fereg_session_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def row_order(self):
+        out = np.empty(self.n, dtype=np.uint32)
+        _check(lib().fereg_session_row_order(self.h, _p(out, u32p)))
+        return out
+
+    def launches(self):
+        return int(lib().fereg_session_launches(self.h))
+
+    def stream(self):
+        return int(lib().fereg_session_stream(self.h) or 0)
+
+    def _call(self, ptr, on_device, nx, vce, noconstant, firstpair, want_groupvar, want_resid, want_d, tol, maxiter,
+              precision):
+        k_all = nx + 1
+        b = np.zeros(k_all)
+        V = np.zeros((k_all, k_all))
+        status = np.zeros(max(1, nx), dtype=np.uint8)
+        resid = np.empty(self.n) if want_resid else None
+        d = np.empty(self.n) if want_d else None
+        gv = np.empty(self.n) if want_groupvar else None
+        table = np.zeros((64, 5))
+        spec = OlsSpec(VCE[vce], int(noconstant), int(firstpair), int(want_groupvar), tol, maxiter, precision)
+        out = OlsOut(_p(b, f64p), _p(V, f64p), _p(status, u8p), _p(resid, f64p), _p(d, f64p), _p(gv, f64p),
+                     _p(table, f64p))
+        _check(lib().fereg_session_ols(self.h, P(ptr), int(on_device), nx, C.byref(spec), C.byref(out)))
+        k = out.k_all
+        return dict(b=b[:k], V=V.ravel()[: k * k].reshape(k, k).copy(), status=status[:nx],
+                    resid=resid, d=d, groupvar=gv, dof_table=table[: out.nslots], y_absorbed=bool(out.y_absorbed),
+                    scalars={s: getattr(out, s) for s in OLS_SCALARS})
+
+    def ols(self, rows, nx=None, vce="unadjusted", noconstant=False, firstpair=False, want_groupvar=False,
+            want_resid=False, want_d=False, tol=1e-8, maxiter=16000, precision=PREC_F64):
+        """OLS of column 0 on the other columns of the n x (1 + nx) host block (row order);
+        the block is residualized in place."""
+        assert rows.dtype == np.float64 and rows.flags.c_contiguous
+        nx = rows.shape[1] - 1 if nx is None else nx
+        return self._call(rows.ctypes.data, 0, nx, vce, noconstant, firstpair, want_groupvar, want_resid, want_d,
+                          tol, maxiter, precision)
+
+    def ols_device(self, ptr, nx, vce="unadjusted", noconstant=False, firstpair=False, want_groupvar=False,
+                   want_resid=False, want_d=False, tol=1e-8, maxiter=16000, precision=PREC_F64):
+        """As ols() on an n x (1 + nx) block in device memory (pointer)."""
+        return self._call(ptr, 1, nx, vce, noconstant, firstpair, want_groupvar, want_resid, want_d, tol, maxiter,
+                          precision)

@@ -457,7 +457,7 @@ void launch_small_reduce(Scratch& d, const DevStruct& S, T* small, int R, T* Y, 
 template <class T>
 void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* P, int R, T* Y, T* t, T* part,
                   T* small, cudaStream_t st) {
-    const int h = d.begin(GpuAbsorber::P_APPLY, st);
+    int h = d.begin(GpuAbsorber::P_APPLY, st);
     const bool acc = S.ms_acc > 0;
     const u32 len = S.ms_acc * u32(R);
     if (d.wseg.n)
@@ -487,6 +487,8 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
             }
         }
     }
+    d.end(h, st);
+    h = d.begin(GpuAbsorber::P_APPLY_PULL, st);
     if (d.wpull.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);

@@ -6,6 +6,7 @@
 
 #include "../../include/fereg_b200.h"
 #include "absorber.h"
+#include "session.h"
 
 using namespace fereg;
 
@@ -13,6 +14,12 @@ struct fereg_absorber {
     GpuAbsorber a;
     template <class... A>
     explicit fereg_absorber(A&&... args) : a(std::forward<A>(args)...) {}
+};
+
+struct fereg_session {
+    GpuSession s;
+    template <class... A>
+    explicit fereg_session(A&&... args) : s(std::forward<A>(args)...) {}
 };
 
 namespace {
@@ -176,10 +183,10 @@ int fereg_absorber_set_profiling(fereg_absorber* h, int on) {
     });
 }
 
-int fereg_absorber_phase_times(const fereg_absorber* h, double* ms8, uint64_t* counts8) {
+int fereg_absorber_phase_times(const fereg_absorber* h, double* ms, uint64_t* counts) {
     return guard([&] {
         if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_phase_times: NULL handle");
-        h->a.phase_times(ms8, counts8);
+        h->a.phase_times(ms, counts);
     });
 }
 
@@ -223,6 +230,102 @@ int fereg_absorber_precond(fereg_absorber* h, const double* rr, size_t r, double
 
 int fereg_absorber_weight_state(const fereg_absorber* h, double* n1, double* nr, double* diag, uint8_t* redundant, double* sw) {
     return guard([&] { h->a.weight_state(n1, nr, diag, redundant, sw); });
+}
+
+
+int fereg_session_create(const uint32_t* const* codes, const uint32_t* g, int nterms, const uint32_t* const* cl_codes,
+                         const uint32_t* cl_g, int ncl, const double* w, int weight_kind, size_t n,
+                         uint64_t num_singletons, const fereg_ctx* ctx, fereg_session** out) {
+    return guard([&] {
+        if (!out) throw Error(RC_INVALID_INPUT, "fereg_session_create: out is NULL");
+        *out = nullptr;
+        if (nterms < 0 || ncl < 0 || (nterms > 0 && (!codes || !g)) || (ncl > 0 && (!cl_codes || !cl_g)))
+            throw Error(RC_INVALID_INPUT, "fereg_session_create: bad terms or clusters");
+        if (n < 2) throw Error(RC_TOO_FEW_OBS, "insufficient observations");
+        if (n >= (size_t(1) << 31)) throw Error(RC_INVALID_INPUT, "more than 2^31 - 1 rows");
+        std::vector<const u32*> cs(codes, codes + nterms), cc(cl_codes, cl_codes + ncl);
+        std::vector<u32> gs(g, g + nterms), cgs(cl_g, cl_g + ncl);
+        for (int q = 0; q < nterms; q++)
+            if (!cs[size_t(q)] || gs[size_t(q)] == 0) throw Error(RC_INVALID_INPUT, "fereg_session_create: empty term");
+        for (int c = 0; c < ncl; c++)
+            if (!cc[size_t(c)] || cgs[size_t(c)] == 0) throw Error(RC_INVALID_INPUT, "fereg_session_create: empty cluster");
+        *out = new fereg_session(cs, gs, cc, cgs, w, weight_kind, n, num_singletons, to_ctx(ctx));
+    });
+}
+
+void fereg_session_destroy(fereg_session* s) { delete s; }
+
+int fereg_session_row_order(const fereg_session* s, uint32_t* out) {
+    return guard([&] {
+        if (!s || !out) throw Error(RC_INVALID_INPUT, "fereg_session_row_order: NULL argument");
+        const auto& pi = const_cast<fereg_session*>(s)->s.absorber().row_order();
+        std::copy(pi.begin(), pi.end(), out);
+    });
+}
+
+int fereg_session_ols(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_ols_spec* spec,
+                      fereg_ols_out* out) {
+    return guard([&] {
+        if (!s || !rows || !spec || !out) throw Error(RC_INVALID_INPUT, "fereg_session_ols: NULL argument");
+        if (spec->precision != FEREG_PREC_F64 && spec->precision != FEREG_PREC_F32_REFINED)
+            throw Error(RC_INVALID_INPUT, "fereg_session_ols: unknown precision");
+        OlsSpec sp;
+        sp.vce = spec->vce;
+        sp.noconstant = spec->noconstant;
+        sp.firstpair = spec->firstpair;
+        sp.want_groupvar = spec->want_groupvar;
+        sp.tol = spec->tol;
+        sp.maxiter = spec->maxiter;
+        sp.prec = spec->precision == FEREG_PREC_F32_REFINED ? Precision::F32_REFINED : Precision::F64;
+        if (sp.vce < 0 || sp.vce > 2) throw Error(RC_INVALID_INPUT, "fereg_session_ols: unknown vce");
+        OlsOut o;
+        o.b = out->b;
+        o.V = out->V;
+        o.status = out->status;
+        o.resid = out->resid;
+        o.d = out->d;
+        o.groupvar = out->groupvar;
+        o.dof_table = out->dof_table;
+        s->s.ols(rows, rows_on_device != 0, nx, sp, o);
+        out->nslots = o.nslots;
+        out->k_all = o.k_all;
+        out->y_absorbed = o.y_absorbed;
+        out->N = o.N;
+        out->rank = o.rank;
+        out->df_r = o.df_r;
+        out->df_m = o.df_m;
+        out->df_a = o.df_a;
+        out->df_a_initial = o.df_a_initial;
+        out->df_a_redundant = o.df_a_redundant;
+        out->df_a_nested = o.df_a_nested;
+        out->N_clust = o.N_clust;
+        out->N_clustervars = o.N_clustervars;
+        out->N_clust1 = o.N_clust1;
+        out->N_clust2 = o.N_clust2;
+        out->num_singletons = o.num_singletons;
+        out->N_full = o.N_full;
+        out->report_constant = o.report_constant;
+        out->rss = o.rss;
+        out->tss = o.tss;
+        out->tss_within = o.tss_within;
+        out->mss = o.mss;
+        out->rmse = o.rmse;
+        out->r2 = o.r2;
+        out->r2_a = o.r2_a;
+        out->r2_within = o.r2_within;
+        out->r2_a_within = o.r2_a_within;
+        out->ll = o.ll;
+        out->ll_0 = o.ll_0;
+        out->F = o.F;
+        out->sumweights = o.sumweights;
+        out->ic = o.ic;
+    });
+}
+
+uint64_t fereg_session_launches(const fereg_session* s) { return s ? s->s.launches() : 0; }
+
+void* fereg_session_stream(const fereg_session* s) {
+    return s ? static_cast<void*>(const_cast<fereg_session*>(s)->s.absorber().stream()) : nullptr;
 }
 
 }  // extern "C"

@@ -1,0 +1,640 @@
+// GpuSession: Session::ols (ols.rs:199-470) on the B200 absorber.
+//
+// Per call: column statistics of the raw rows (two device passes, stats.rs:40), the FE solve in
+// place (the absorber), the weighted Gram of the residualized block (one device pass,
+// stats.rs:195), collinearity and the coefficients by sweeps on the standardized Gram (host,
+// K x K), the residuals and their sum of squares (device), and the variance: iid from the
+// residual sum of squares, HC1 from a device meat pass, CRV1 from per-cluster score sums (device,
+// rows grouped by a stable cluster permutation) and S^T S, with the inclusion-exclusion of
+// multiway clusters and the eigenvalue clip (vcov.rs:480-720). Degrees of freedom
+// (dof.rs:64-180) use device union-find for the mobility groups of FE pairs.
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <numeric>
+#include <sstream>
+
+#include "linalg.h"
+#include "session.h"
+#include "stats.cuh"
+
+namespace fereg {
+
+namespace {
+
+constexpr double SWEEP_TOL = 1e-13;     // vcov.rs invsym tolerance
+constexpr double F_SWEEP_TOL = 1e-9;    // ols.rs Wald F: greedy sweep of the slope variance
+constexpr int MAX_TABLE = 64;           // dof table slots reported
+
+double nanv() { return std::numeric_limits<double>::quiet_NaN(); }
+double finite_or_nan(double x) { return std::isfinite(x) ? x : nanv(); }
+
+int blocks_for(size_t n, int tb) { return int(std::max<size_t>(1, std::min<size_t>((n + tb - 1) / tb, 148 * 16))); }
+
+// Interaction codes of several dimensions (factor.rs:255 combine): the tuple key in mixed radix
+// (first dimension most significant), distinct keys numbered in ascending order.
+void combine_codes(const std::vector<const std::vector<u32>*>& dims, const std::vector<u32>& gs, size_t n,
+                   std::vector<u32>& out, u32& g) {
+    if (dims.size() == 1) {
+        out = *dims[0];
+        g = gs[0];
+        return;
+    }
+    std::vector<u64> key(n, 0);
+    for (size_t d = 0; d < dims.size(); d++)
+        for (size_t i = 0; i < n; i++) key[i] = key[i] * u64(gs[d]) + (*dims[d])[i];
+    std::vector<u64> uniq(key);
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    out.resize(n);
+    for (size_t i = 0; i < n; i++) out[i] = u32(std::lower_bound(uniq.begin(), uniq.end(), key[i]) - uniq.begin());
+    g = u32(uniq.size());
+}
+
+}  // namespace
+
+// Device state of a session.
+struct SessionDev {
+    std::vector<DBuf<u32>> tcodes, ccodes;  // kept order
+    struct Subset {
+        DBuf<int> perm;  // rows (row order) grouped by cluster, stable
+        DBuf<u32> coff;  // G + 1
+        u32 G = 0;
+        double sign = 1.0;
+    };
+    std::vector<Subset> subsets;
+    DBuf<double> w_raw, wv;  // row order
+    DBuf<double> rows, part, sums, e, om, S, shift, beta;
+    DBuf<int> col, err;
+    DBuf<u32> uf, flags, scan, bsum, total, gv, map;
+    DBuf<double> pstat;
+    cudaStream_t st = nullptr;
+    u64 launches = 0;
+};
+
+GpuSession::GpuSession(const std::vector<const u32*>& codes, const std::vector<u32>& g,
+                       const std::vector<const u32*>& cl_codes, const std::vector<u32>& cl_g, const double* w,
+                       int weight_kind, size_t n, u64 num_singletons, const Ctx& ctx)
+    : n_(n), kind_(w ? weight_kind : 0), nsing_(num_singletons) {
+    if (weight_kind < 0 || weight_kind > 3) throw Error(RC_INVALID_INPUT, "fereg_session_create: bad weight kind");
+    if (w && weight_kind == 0) throw Error(RC_INVALID_INPUT, "fereg_session_create: weights need a weight kind");
+    std::vector<const u32*> tptr = codes;
+    std::vector<u32> tg = g;
+    std::vector<u32> constant;
+    if (tptr.empty()) {  // noabsorb: the constant is the only absorbed term (ols.rs:263, dof.rs:64)
+        constant.assign(n, 0u);
+        tptr.push_back(constant.data());
+        tg.push_back(1u);
+    }
+    tg_ = tg;
+    cg_ = cl_g;
+    for (size_t q = 0; q < tptr.size(); q++) tcodes_.emplace_back(tptr[q], tptr[q] + n);
+    for (size_t c = 0; c < cl_codes.size(); c++) ccodes_.emplace_back(cl_codes[c], cl_codes[c] + n);
+    if (w) {
+        wk_.assign(w, w + n);
+        sumw_ = 0.0;
+        for (double x : wk_) sumw_ += x;
+    } else {
+        sumw_ = double(n);
+    }
+    ab_ = std::make_unique<GpuAbsorber>(tptr, tg, w, n, ctx);
+    d_ = std::make_unique<SessionDev>();
+    SessionDev& d = *d_;
+    d.st = ab_->stream();
+    for (auto& c : tcodes_) {
+        d.tcodes.emplace_back();
+        d.tcodes.back().upload(c, d.st);
+    }
+    for (auto& c : ccodes_) {
+        d.ccodes.emplace_back();
+        d.ccodes.back().upload(c, d.st);
+    }
+    const std::vector<u32>& pi = ab_->row_order();
+    if (w) {
+        std::vector<double> raw(n), wv(n);
+        for (size_t i = 0; i < n; i++) raw[i] = wk_[pi[i]];
+        // ols.rs:77-108 Weights: aweights and pweights normalized to sum n, fweights as given
+        const double f = (kind_ == 1 || kind_ == 3) ? double(n) / sumw_ : 1.0;
+        for (size_t i = 0; i < n; i++) wv[i] = raw[i] * f;
+        d.w_raw.upload(raw, d.st);
+        d.wv.upload(wv, d.st);
+    }
+    // cluster subsets (inclusion-exclusion of vcov.rs:480-560): every non-empty subset of the
+    // dimensions, its rows grouped by the combined code
+    const size_t q = ccodes_.size();
+    for (u32 mask = 1; mask < (1u << q); mask++) {
+        std::vector<const std::vector<u32>*> dims;
+        std::vector<u32> gs;
+        for (size_t c = 0; c < q; c++)
+            if (mask & (1u << c)) {
+                dims.push_back(&ccodes_[c]);
+                gs.push_back(cg_[c]);
+            }
+        std::vector<u32> kc;
+        u32 G = 0;
+        combine_codes(dims, gs, n, kc, G);
+        std::vector<u32> coff(size_t(G) + 1, 0);
+        for (size_t i = 0; i < n; i++) coff[kc[pi[i]] + 1]++;
+        for (u32 k = 0; k < G; k++) coff[k + 1] += coff[k];
+        std::vector<int> perm(n);
+        std::vector<u32> pos(coff.begin(), coff.end() - 1);
+        for (size_t i = 0; i < n; i++) perm[pos[kc[pi[i]]]++] = int(i);
+        d.subsets.emplace_back();
+        auto& s = d.subsets.back();
+        s.perm.upload(perm, d.st);
+        s.coff.upload(coff, d.st);
+        s.G = G;
+        s.sign = dims.size() % 2 == 1 ? 1.0 : -1.0;
+    }
+    CK(cudaStreamSynchronize(d.st));
+}
+
+GpuSession::~GpuSession() {
+    d_.reset();
+    ab_.reset();
+}
+
+u64 GpuSession::launches() const { return d_->launches + ab_->launches(); }
+
+// dof.rs:222-256 mobility_groups of terms qa, qb on the device; save: keep the row labels.
+u64 GpuSession::mobility_groups(size_t qa, size_t qb, bool save) {
+    SessionDev& d = *d_;
+    const u32 ga = tg_[qa], gb = tg_[qb], nv = ga + gb;
+    d.uf.alloc(nv);
+    d.flags.alloc(ga);
+    d.scan.alloc(ga);
+    d.bsum.alloc((ga + SCAN_TILE - 1) / SCAN_TILE + 1);
+    d.total.alloc(1);
+    d.err.alloc(1);
+    CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), d.st));
+    k_uf_init<<<blocks_for(nv, 256), 256, 0, d.st>>>(d.uf.p, nv);
+    k_uf_union<<<blocks_for(n_, 256), 256, 0, d.st>>>(d.tcodes[qa].p, d.tcodes[qb].p, ga, n_, d.uf.p, d.err.p);
+    k_uf_flatten<<<blocks_for(nv, 256), 256, 0, d.st>>>(d.uf.p, nv);
+    k_uf_roots<<<blocks_for(ga, 256), 256, 0, d.st>>>(d.uf.p, ga, d.flags.p);
+    const u32 nblk = (ga + SCAN_TILE - 1) / SCAN_TILE;
+    k_scan_sums<<<nblk, SCAN_TB, 0, d.st>>>(d.flags.p, ga, d.bsum.p);
+    k_scan_top<<<1, SCAN_TB, 0, d.st>>>(d.bsum.p, nblk, d.total.p);
+    k_scan_apply<<<nblk, SCAN_TB, 0, d.st>>>(d.flags.p, ga, d.bsum.p, d.scan.p);
+    d.launches += 7;
+    if (save) {
+        d.gv.alloc(n_);
+        k_uf_label<<<blocks_for(n_, 256), 256, 0, d.st>>>(d.tcodes[qa].p, n_, d.uf.p, d.scan.p, d.gv.p);
+        d.launches++;
+    }
+    u32 total = 0;
+    int err = 0;
+    CK(cudaMemcpyAsync(&total, d.total.p, sizeof(u32), cudaMemcpyDeviceToHost, d.st));
+    CK(cudaMemcpyAsync(&err, d.err.p, sizeof(int), cudaMemcpyDeviceToHost, d.st));
+    CK(cudaStreamSynchronize(d.st));
+    if (err) throw Error(RC_INTERNAL, "fereg: union-find did not settle");
+    return total;
+}
+
+// dof.rs:184 nested_within: every level of term q lies in one level of cluster dimension c.
+bool GpuSession::nested_within(size_t q, size_t c) {
+    SessionDev& d = *d_;
+    d.map.alloc(tg_[q]);
+    d.err.alloc(1);
+    CK(cudaMemsetAsync(d.map.p, 0xff, size_t(tg_[q]) * sizeof(u32), d.st));
+    CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), d.st));
+    k_nested<<<blocks_for(n_, 256), 256, 0, d.st>>>(d.tcodes[q].p, d.ccodes[c].p, n_, d.map.p, d.err.p);
+    d.launches++;
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, d.err.p, sizeof(int), cudaMemcpyDeviceToHost, d.st));
+    CK(cudaStreamSynchronize(d.st));
+    return flag == 0;
+}
+
+// dof.rs:64-180 estimate_dof (intercept-only terms, the default options: clusters and pairwise;
+// firstpair instead of both). Slot i: k levels, m redundant, exact, nested in a cluster.
+GpuSession::Dof GpuSession::estimate_dof(bool clusters, bool firstpair, bool want_groupvar) {
+    Dof dof;
+    const size_t nt = tg_.size();
+    std::vector<bool> live(nt, true);
+    for (size_t q = 0; q < nt; q++) dof.slots.push_back(DofSlot{tg_[q], 0, false, false});
+    if (clusters && !firstpair)
+        for (size_t c = 0; c < ccodes_.size(); c++) {
+            if (std::none_of(live.begin(), live.end(), [](bool x) { return x; })) break;
+            for (size_t q = 0; q < nt; q++) {
+                if (!live[q] || dof.slots[q].exact) continue;
+                if (nested_within(q, c)) {
+                    dof.slots[q].m = dof.slots[q].k;
+                    dof.slots[q].exact = dof.slots[q].nested = true;
+                    dof.df_a_nested += dof.slots[q].k;
+                    live[q] = false;
+                }
+            }
+        }
+    const size_t remaining = size_t(std::count(live.begin(), live.end(), true));
+    if (remaining > 1 || (remaining > 0 && dof.df_a_nested > 0)) {
+        // each live term but the first keeps one redundant level (the constant), unless a term
+        // nested in a cluster already carries it
+        bool skip = dof.df_a_nested == 0;
+        for (size_t q = 0; q < nt; q++) {
+            if (!live[q]) continue;
+            if (skip) {
+                skip = false;
+                continue;
+            }
+            dof.slots[q].m = 1;
+        }
+    }
+    for (size_t q = 0; q < nt; q++)
+        if (live[q]) {
+            dof.slots[q].exact = true;
+            break;
+        }
+    std::vector<size_t> idx;
+    for (size_t q = 0; q < nt; q++)
+        if (live[q]) idx.push_back(q);
+    int pairs = 0;
+    for (size_t a = 0; a < idx.size(); a++) {
+        bool stop = false;
+        for (size_t b = a + 1; b < idx.size(); b++) {
+            pairs++;
+            const bool save = pairs == 1 && want_groupvar;
+            const u64 m = mobility_groups(idx[a], idx[b], save);
+            if (save) dof.has_groupvar = true;
+            dof.slots[idx[b]].m = std::max(dof.slots[idx[b]].m, m);
+            if (pairs == 1) dof.slots[idx[b]].exact = true;
+            if (firstpair) {
+                stop = true;
+                break;
+            }
+        }
+        if (stop) break;
+    }
+    for (auto& s : dof.slots) {
+        dof.df_a_initial += s.k;
+        dof.df_a_redundant += s.m;
+    }
+    dof.df_a = dof.df_a_initial - dof.df_a_redundant;
+    return dof;
+}
+
+void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out) {
+    SessionDev& d = *d_;
+    cudaStream_t st = d.st;
+    const size_t n = n_, r = 1 + nx;
+    const int R = int(r);
+    if (r + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg ols: at most 62 regressors on the device path");
+    double* rows = rows_in;
+    if (!on_device) {
+        d.rows.alloc(n * r);
+        CK(cudaMemcpyAsync(d.rows.p, rows_in, n * r * 8, cudaMemcpyHostToDevice, st));
+        rows = d.rows.p;
+    }
+    const std::vector<u32>& pi = ab_->row_order();
+    const int kind = kind_;
+    const bool weighted = !wk_.empty();
+    const double sumw = sumw_;
+    const double bigN = kind == 2 ? sumw : double(n);
+    int vce = spec.vce;
+    if (vce == 0 && kind == 3) vce = 1;  // ols.rs:150 pweights imply robust
+    if (vce == 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg ols: cluster variance without clusters");
+    const bool has_intercept = true;  // intercept-only terms (or noabsorb) contain the constant
+    const bool report_constant = has_intercept && !spec.noconstant;
+
+    const Dof dof = estimate_dof(vce == 2, spec.firstpair != 0, spec.want_groupvar != 0 && out.groupvar);
+
+    // Pass A: column statistics of the raw rows (stats.rs:40), raw weights
+    const double* wr = weighted ? d.w_raw.p : nullptr;
+    d.part.alloc(size_t(ST_GRID) * r * 4);
+    d.sums.alloc(r * 4);
+    for (int j0 = 0; j0 < R; j0 += 32) {
+        const int Rc = std::min(32, R - j0);
+        k_colstats<4><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, 1, nullptr, nullptr, d.part.p);
+        d.launches++;
+    }
+    k_sum_parts<<<(R * 4 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 4, d.sums.p);
+    std::vector<double> s1(r * 4);
+    CK(cudaMemcpyAsync(s1.data(), d.sums.p, r * 4 * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<double> mean(r), wmean(r), sumsq(r), wss_unc(r);
+    for (size_t j = 0; j < r; j++) {
+        mean[j] = s1[j * 4] / double(n);
+        wmean[j] = s1[j * 4 + 1] / sumw;
+        sumsq[j] = s1[j * 4 + 2];
+        wss_unc[j] = s1[j * 4 + 3];
+    }
+    d.pstat.alloc(2 * r);
+    CK(cudaMemcpyAsync(d.pstat.p, mean.data(), r * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d.pstat.p + r, wmean.data(), r * 8, cudaMemcpyHostToDevice, st));
+    for (int j0 = 0; j0 < R; j0 += 32) {
+        const int Rc = std::min(32, R - j0);
+        k_colstats<2><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, 2, d.pstat.p, d.pstat.p + r, d.part.p);
+        d.launches++;
+    }
+    k_sum_parts<<<(R * 2 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 2, d.sums.p);
+    d.launches += 2;
+    std::vector<double> s2(r * 2);
+    CK(cudaMemcpyAsync(s2.data(), d.sums.p, r * 2 * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<double> sd(r), wss(r);
+    for (size_t j = 0; j < r; j++) {
+        sd[j] = std::max(std::sqrt(s2[j * 2] / (double(n) - 1.0)), 1e-3);
+        wss[j] = s2[j * 2 + 1];
+    }
+    const double tscale = (kind == 1 || kind == 3) ? double(n) / sumw : 1.0;
+    const double tss_y = (has_intercept ? wss[0] : wss_unc[0]) * tscale;
+
+    // The FE solve, in place
+    const bool want_coefs = out.d != nullptr;
+    const size_t p_len = ab_->coefs_len();
+    std::vector<double> coefs(want_coefs ? p_len * r : 0);
+    const SolveInfo info =
+        ab_->residualize_device(rows, r, spec.tol, spec.maxiter, want_coefs, nullptr, want_coefs ? coefs.data() : nullptr,
+                                spec.prec);
+
+    // Outer products over the block: sum om a a^T of columns `cols` shifted by `shift` (+ the
+    // constant), optionally the plain sums of squares; returns the full msz x msz matrix.
+    auto outer = [&](const double* src, size_t nrows, int srcR, const std::vector<int>& cols,
+                     const std::vector<double>* shift, bool cst, const double* om, const int* perm, bool ssq,
+                     std::vector<double>* ss_out) {
+        const int k = int(cols.size()), msz = k + (cst ? 1 : 0);
+        const int P = msz * (msz + 1) / 2;
+        std::vector<double> m(size_t(msz) * msz, 0.0);
+        if (msz == 0) return m;
+        d.col.alloc(size_t(k) + 1);
+        CK(cudaMemcpyAsync(d.col.p, cols.data(), size_t(k) * sizeof(int), cudaMemcpyHostToDevice, st));
+        if (shift) {
+            d.shift.alloc(size_t(k) + 1);
+            CK(cudaMemcpyAsync(d.shift.p, shift->data(), size_t(k) * 8, cudaMemcpyHostToDevice, st));
+        }
+        std::vector<double> pairs(P), sq(k);
+        for (int p0 = 0; p0 < P; p0 += OP_MAXP) {
+            const int np = std::min(OP_MAXP, P - p0);
+            const bool with_sq = ssq && p0 == 0;
+            const int len = np + (with_sq ? k : 0);
+            d.part.alloc(size_t(ST_GRID) * len);
+            d.sums.alloc(size_t(len));
+            OpSpec s{src, nrows, srcR, d.col.p, shift ? d.shift.p : nullptr, k, cst ? 1 : 0, msz, om, perm, p0, np,
+                     with_sq ? 1 : 0};
+            k_outer<<<ST_GRID, ST_TB, 0, st>>>(s, d.part.p);
+            k_sum_parts<<<(len + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
+            d.launches += 2;
+            std::vector<double> h(len);
+            CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            std::copy(h.begin(), h.begin() + np, pairs.begin() + p0);
+            if (with_sq) std::copy(h.begin() + np, h.end(), sq.begin());
+        }
+        int p = 0;
+        for (int a = 0; a < msz; a++)
+            for (int b = a; b < msz; b++, p++) m[size_t(a) * msz + b] = m[size_t(b) * msz + a] = pairs[p];
+        if (ss_out) *ss_out = sq;
+        return m;
+    };
+
+    // Pass B: weighted Gram of the residualized block (stats.rs:195)
+    const double* wv = weighted ? d.wv.p : nullptr;
+    std::vector<int> all_cols(r);
+    std::iota(all_cols.begin(), all_cols.end(), 0);
+    std::vector<double> ss_res;
+    std::vector<double> g = outer(rows, n, R, all_cols, nullptr, false, wv, nullptr, true, &ss_res);
+
+    // Collinearity, stage 1 (ols.rs:38 stage1_absorbed): a column absorbed by the FE
+    const double ctol = std::min(1e-6, spec.tol / 10.0);
+    std::vector<uint8_t> status(nx, 0);
+    std::vector<bool> absorbed(r);
+    for (size_t j = 0; j < r; j++) absorbed[j] = ss_res[j] / sumsq[j] <= ctol;
+    const bool y_abs = nx >= 1 && absorbed[0];
+    if (y_abs) {  // reghdfe zeroes the partialled-out depvar
+        k_zero_col<<<blocks_for(n, 256), 256, 0, st>>>(rows, n, R, 0);
+        d.launches++;
+        for (size_t j = 0; j < r; j++) g[j] = g[j * r] = 0.0;
+    }
+    for (size_t j = 1; j < r; j++)
+        if (absorbed[j]) status[j - 1] = 2;
+    // stage 2: sweeps on the standardized Gram of the candidates (ols.rs:46, vcov.rs:22)
+    std::vector<size_t> cand;
+    for (size_t j = 1; j < r; j++)
+        if (status[j - 1] == 0) cand.push_back(j);
+    const size_t kc = cand.size();
+    la::Mat gs(kc * kc);
+    for (size_t a = 0; a < kc; a++)
+        for (size_t b = 0; b < kc; b++) gs[a * kc + b] = g[cand[a] * r + cand[b]] / (sd[cand[a]] * sd[cand[b]]);
+    std::vector<bool> dropped;
+    const la::Mat inv_c = la::sweep_inverse(gs, kc, SWEEP_TOL, false, dropped);
+    std::vector<size_t> keep_pos, kept;
+    for (size_t c = 0; c < kc; c++) {
+        if (dropped[c]) status[cand[c] - 1] = 3;
+        else {
+            keep_pos.push_back(c);
+            kept.push_back(cand[c]);
+        }
+    }
+    const size_t k = kept.size();
+    la::Mat inv_s(k * k);
+    for (size_t a = 0; a < k; a++)
+        for (size_t b = 0; b < k; b++) inv_s[a * k + b] = inv_c[keep_pos[a] * kc + keep_pos[b]];
+    const double sd_y = sd[0];
+    std::vector<double> b_s(k, 0.0), beta(k);
+    for (size_t a = 0; a < k; a++)
+        for (size_t b = 0; b < k; b++) b_s[a] += inv_s[a * k + b] * (g[kept[b] * r] / (sd[kept[b]] * sd_y));
+    for (size_t a = 0; a < k; a++) beta[a] = b_s[a] * sd_y / sd[kept[a]];
+
+    // residuals and their weighted sum of squares
+    std::vector<int> kcols(kept.begin(), kept.end());
+    d.col.alloc(k + 1);
+    d.beta.alloc(k + 1);
+    if (k) {
+        CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
+    }
+    d.e.alloc(n);
+    d.part.alloc(ST_GRID);
+    d.sums.alloc(1);
+    k_resid_e<<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, d.col.p, d.beta.p, int(k), y_abs ? 1 : 0, wv, d.e.p, d.part.p);
+    k_sum_parts<<<1, 32, 0, st>>>(d.part.p, ST_GRID, 1, d.sums.p);
+    d.launches += 2;
+    double rss = 0.0;
+    CK(cudaMemcpyAsync(&rss, d.sums.p, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const double rss_s = rss / (sd_y * sd_y);
+
+    // bread: the standardized inverse, bordered by the constant (vcov.rs:220)
+    std::vector<double> means_s(k), xbar(k);
+    for (size_t a = 0; a < k; a++) {
+        means_s[a] = wmean[kept[a]] / sd[kept[a]];
+        xbar[a] = wmean[kept[a]];
+    }
+    double b0_s = wmean[0] / sd_y;
+    for (size_t a = 0; a < k; a++) b0_s -= means_s[a] * b_s[a];
+    const size_t msz = k + (report_constant ? 1 : 0);
+    const double n_const = (kind == 1 || kind == 3) ? double(n) : sumw;
+    const la::Mat bread = report_constant ? la::bordered(inv_s, k, means_s, n_const) : inv_s;
+    std::vector<double> b_full_s = b_s;
+    if (report_constant) b_full_s.push_back(b0_s);
+
+    const double df_a = double(dof.df_a), df_m = double(k);
+    double df_r = bigN - df_a - df_m;
+    double g_min = 0.0;
+    if (!cg_.empty()) g_min = double(*std::min_element(cg_.begin(), cg_.end()));
+    std::vector<double> sc(msz);
+    for (size_t a = 0; a < k; a++) sc[a] = sd[kept[a]];
+    if (report_constant) sc[k] = 1.0;
+    auto standardize = [&](la::Mat& mt) {
+        for (size_t a = 0; a < msz; a++)
+            for (size_t b = 0; b < msz; b++) mt[a * msz + b] /= sc[a] * sc[b] * sd_y * sd_y;
+    };
+    la::Mat v_s(msz * msz, 0.0);
+    if (msz > 0) {
+        if (vce == 0) {
+            const double f = (rss_s / bigN) * (bigN / df_r);
+            for (size_t i = 0; i < msz * msz; i++) v_s[i] = f * bread[i];
+        } else if (vce == 1) {
+            d.om.alloc(n);
+            k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 0, d.om.p);
+            d.launches++;
+            const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+            la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
+            standardize(meat);
+            v_s = la::sandwich(bread, meat, msz, bigN / (bigN - df_a - df_m));
+        } else {
+            d.om.alloc(n);
+            k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 1, d.om.p);
+            d.launches++;
+            const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+            if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+            la::Mat meat(msz * msz, 0.0);
+            for (auto& sub : d.subsets) {
+                d.S.alloc(size_t(sub.G) * msz);
+                d.shift.alloc(k + 1);
+                if (k) CK(cudaMemcpyAsync(d.shift.p, shift.data(), k * 8, cudaMemcpyHostToDevice, st));
+                k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(rows, R, d.col.p, d.shift.p, int(k), report_constant ? 1 : 0,
+                                                           d.om.p, sub.perm.p, sub.coff.p, sub.G, d.S.p);
+                d.launches++;
+                std::vector<int> scols(msz);
+                std::iota(scols.begin(), scols.end(), 0);
+                const la::Mat part = outer(d.S.p, sub.G, int(msz), scols, nullptr, false, nullptr, nullptr, false, nullptr);
+                for (size_t i = 0; i < msz * msz; i++) meat[i] += sub.sign * part[i];
+                // the next subset's scores need the kept columns again
+                if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+            }
+            standardize(meat);
+            const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
+            const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
+            v_s = la::sandwich(bread, meat, msz, q_cluster);
+            if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
+        }
+    }
+    if (vce == 2) df_r = std::min(df_r, g_min - 1.0);
+    for (size_t i = 0; i < msz; i++)
+        for (size_t j = 0; j < i; j++) v_s[j * msz + i] = v_s[i * msz + j];
+
+    // Wald F of the slopes (greedy sweep of their variance)
+    double f_stat = nanv();
+    if (k > 0) {
+        la::Mat vkk(k * k);
+        for (size_t a = 0; a < k; a++)
+            for (size_t b = 0; b < k; b++) vkk[a * k + b] = v_s[a * msz + b];
+        std::vector<bool> dv;
+        const la::Mat iv = la::sweep_inverse(vkk, k, F_SWEEP_TOL, true, dv);
+        if (std::none_of(dv.begin(), dv.end(), [](bool x) { return x; })) {
+            double qf = 0.0;
+            for (size_t a = 0; a < k; a++)
+                for (size_t b = 0; b < k; b++) qf += b_s[a] * iv[a * k + b] * b_s[b];
+            f_stat = finite_or_nan(qf / df_m);
+        }
+    }
+    if (std::any_of(v_s.begin(), v_s.end(), [](double x) { return std::isnan(x); })) std::fill(v_s.begin(), v_s.end(), 0.0);
+
+    // back to the raw scale, in the caller's column positions
+    std::vector<double> sx(msz), b_raw(msz), v_raw(msz * msz);
+    for (size_t a = 0; a < msz; a++) sx[a] = sc[a] / sd_y;
+    for (size_t a = 0; a < msz; a++) b_raw[a] = b_full_s[a] / sx[a];
+    for (size_t a = 0; a < msz; a++)
+        for (size_t b = 0; b < msz; b++) v_raw[a * msz + b] = v_s[a * msz + b] / (sx[a] * sx[b]);
+    const double b0 = report_constant ? b_raw[k] : 0.0;
+    const size_t k_all = nx + (report_constant ? 1 : 0);
+    std::vector<size_t> pos;
+    for (size_t c : kept) pos.push_back(c - 1);
+    if (report_constant) pos.push_back(nx);
+    if (out.b) std::fill(out.b, out.b + k_all, 0.0);
+    if (out.V) std::fill(out.V, out.V + k_all * k_all, 0.0);
+    for (size_t a = 0; a < pos.size(); a++) {
+        if (out.b) out.b[pos[a]] = b_raw[a];
+        if (out.V)
+            for (size_t b = 0; b < pos.size(); b++) out.V[pos[a] * k_all + pos[b]] = v_raw[a * msz + b];
+    }
+    if (out.status) std::copy(status.begin(), status.end(), out.status);
+    out.k_all = int(k_all);
+    out.y_absorbed = y_abs ? 1 : 0;
+
+    const double tss = tss_y, tss_within = g[0];
+    const double used_df_r = bigN - df_a - df_m - double(dof.df_a_nested);
+    const double hi = has_intercept ? 1.0 : 0.0;
+    const double ln2pi = std::log(2.0 * M_PI);
+    out.N = bigN;
+    out.rank = df_m;
+    out.df_r = df_r;
+    out.df_m = df_m;
+    out.df_a = df_a;
+    out.df_a_initial = double(dof.df_a_initial);
+    out.df_a_redundant = double(dof.df_a_redundant);
+    out.df_a_nested = double(dof.df_a_nested);
+    out.N_clust = vce == 2 ? g_min : nanv();
+    out.N_clustervars = vce == 2 ? double(ccodes_.size()) : nanv();
+    out.N_clust1 = vce == 2 && !cg_.empty() ? double(cg_[0]) : nanv();
+    out.N_clust2 = vce == 2 && cg_.size() > 1 ? double(cg_[1]) : nanv();
+    out.num_singletons = double(nsing_);
+    out.N_full = bigN + double(nsing_);
+    out.report_constant = report_constant ? 1.0 : 0.0;
+    out.rss = finite_or_nan(rss);
+    out.tss = finite_or_nan(tss);
+    out.tss_within = finite_or_nan(tss_within);
+    out.mss = finite_or_nan(tss - rss);
+    out.rmse = finite_or_nan(used_df_r != 0.0 ? std::sqrt(rss / used_df_r) : std::sqrt(rss));
+    out.r2 = finite_or_nan(1.0 - rss / tss);
+    out.r2_a = finite_or_nan(1.0 - (rss / used_df_r) / (tss / (bigN - hi)));
+    out.r2_within = finite_or_nan(1.0 - rss / tss_within);
+    out.r2_a_within = finite_or_nan(1.0 - (rss / used_df_r) / (tss_within / (used_df_r + df_m)));
+    out.ll = finite_or_nan(-0.5 * bigN * (1.0 + ln2pi + std::log(rss / bigN)));
+    out.ll_0 = finite_or_nan(-0.5 * bigN * (1.0 + ln2pi + std::log(tss_within / bigN)));
+    out.F = f_stat;
+    out.sumweights = sumw;
+    out.ic = double(info.iterations);
+    out.nslots = int(dof.slots.size());
+    if (out.dof_table)
+        for (size_t i = 0; i < dof.slots.size() && i < size_t(MAX_TABLE); i++) {
+            const auto& s = dof.slots[i];
+            double* t = out.dof_table + 5 * i;
+            t[0] = double(s.k);
+            t[1] = double(s.m);
+            t[2] = double(s.k - s.m);
+            t[3] = s.exact ? 0.0 : 1.0;
+            t[4] = s.nested ? 1.0 : 0.0;
+        }
+    if (out.resid) {
+        std::vector<double> e(n);
+        CK(cudaMemcpyAsync(e.data(), d.e.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < n; i++) out.resid[pi[i]] = e[i];
+    }
+    if (out.d) {
+        // sum of the fixed effects: the FE fit of y minus the slopes' FE fits, less the constant
+        std::vector<double> comb(p_len, 0.0), fit(n);
+        for (size_t i = 0; i < p_len; i++) {
+            double v = coefs[i * r];
+            for (size_t a = 0; a < k; a++) v -= beta[a] * coefs[i * r + kept[a]];
+            comb[i] = v;
+        }
+        ab_->fit_rows(comb.data(), 1, 0, fit.data());
+        for (size_t i = 0; i < n; i++) out.d[pi[i]] = fit[i] - b0;
+    }
+    if (out.groupvar) {
+        if (dof.has_groupvar) {
+            std::vector<u32> gv(n);
+            CK(cudaMemcpyAsync(gv.data(), d.gv.p, n * sizeof(u32), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (size_t i = 0; i < n; i++) out.groupvar[i] = double(gv[i]);
+        } else {
+            std::fill(out.groupvar, out.groupvar + n, nanv());
+        }
+    }
+    CK(cudaGetLastError());
+}
+
+}  // namespace fereg

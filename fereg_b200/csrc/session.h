@@ -1,0 +1,89 @@
+// GpuSession: the estimation session around the B200 absorber, the part of the reference's
+// `Session` (crates/fereg-core/src/session.rs) that `Session::ols` (ols.rs:199-470) uses: the
+// kept-order FE term codes, cluster codes, weights and their kind, and the absorber built on the
+// terms. The OLS call runs its row passes on the device (column statistics, the solve, the Gram,
+// residuals and meats) and its K x K algebra on the host.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "absorber.h"
+
+namespace fereg {
+
+struct OlsSpec {
+    int vce = 0;  // 0 unadjusted, 1 robust (HC1), 2 cluster (CRV1, one- or multiway)
+    int noconstant = 0;
+    int firstpair = 0;
+    int want_groupvar = 0;
+    double tol = 1e-8;
+    size_t maxiter = 16000;
+    Precision prec = Precision::F64;
+};
+
+// Results of ols.rs:263-470 (EstResult): caller buffers may be null.
+struct OlsOut {
+    double* b = nullptr;         // nx + 1 ([x..., _cons])
+    double* V = nullptr;         // (nx + 1)^2
+    uint8_t* status = nullptr;   // nx: 0 ok, 2 absorbed by the FE, 3 collinear
+    double* resid = nullptr;     // n, kept order
+    double* d = nullptr;         // n, kept order: sum of the fixed effects
+    double* groupvar = nullptr;  // n, kept order: mobility group of the first FE pair
+    double* dof_table = nullptr; // 5 per FE term (max 64): levels, redundant, k - m, inexact, nested
+    int nslots = 0, k_all = 0, y_absorbed = 0;
+    double N = 0, rank = 0, df_r = 0, df_m = 0, df_a = 0, df_a_initial = 0, df_a_redundant = 0, df_a_nested = 0;
+    double N_clust = 0, N_clustervars = 0, N_clust1 = 0, N_clust2 = 0, num_singletons = 0, N_full = 0;
+    double report_constant = 0;
+    double rss = 0, tss = 0, tss_within = 0, mss = 0, rmse = 0, r2 = 0, r2_a = 0, r2_within = 0, r2_a_within = 0;
+    double ll = 0, ll_0 = 0, F = 0, sumweights = 0, ic = 0;
+};
+
+struct SessionDev;
+
+class GpuSession {
+   public:
+    // codes[q]: kept-order codes of FE term q (< g[q]); no terms = the constant alone (noabsorb).
+    // cl_codes[c]: kept-order codes of cluster dimension c. w: raw kept-order weights or null;
+    // weight_kind 0 none, 1 aweight, 2 fweight, 3 pweight. num_singletons: rows the session's
+    // preparation dropped as singletons (reported in N_full).
+    GpuSession(const std::vector<const u32*>& codes, const std::vector<u32>& g,
+               const std::vector<const u32*>& cl_codes, const std::vector<u32>& cl_g, const double* w, int weight_kind,
+               size_t n, u64 num_singletons, const Ctx& ctx);
+    ~GpuSession();
+
+    GpuAbsorber& absorber() { return *ab_; }
+    size_t n() const { return n_; }
+    // Kernel launches of the session passes and its absorber so far.
+    u64 launches() const;
+
+    // OLS of column 0 on columns 1..nx of the n x (1 + nx) row-major block `rows` (row order;
+    // host memory, or device memory when on_device). The block is residualized in place.
+    void ols(double* rows, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out);
+
+   private:
+    size_t n_ = 0;
+    int kind_ = 0;
+    u64 nsing_ = 0;
+    std::vector<u32> tg_, cg_;
+    std::vector<std::vector<u32>> tcodes_, ccodes_;  // kept order (host)
+    std::vector<double> wk_;                         // raw kept-order weights
+    double sumw_ = 0;
+    std::unique_ptr<GpuAbsorber> ab_;
+    std::unique_ptr<SessionDev> d_;
+
+    struct DofSlot {
+        u64 k = 0, m = 0;
+        bool exact = false, nested = false;
+    };
+    struct Dof {
+        std::vector<DofSlot> slots;
+        u64 df_a = 0, df_a_initial = 0, df_a_redundant = 0, df_a_nested = 0;
+        bool has_groupvar = false;
+    };
+    Dof estimate_dof(bool clusters, bool firstpair, bool want_groupvar);
+    u64 mobility_groups(size_t qa, size_t qb, bool save);
+    bool nested_within(size_t q, size_t c);
+};
+
+}  // namespace fereg

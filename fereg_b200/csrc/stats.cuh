@@ -1,0 +1,381 @@
+// Device passes of the OLS call around the solve (stats.rs, ols.rs, vcov.rs, dof.rs):
+//   - column statistics of the raw rows (stats.rs:40 col_stats, two passes: sums, then sums of
+//     squares about the means);
+//   - weighted outer-product sums sum_i w_i a_i a_i^T over selected, shifted columns of a row
+//     block (the Gram of stats.rs:195, the robust meat of vcov.rs:292, and S^T S of the cluster
+//     scores of vcov.rs:320);
+//   - residuals e = y - X b with their weighted sum of squares;
+//   - cluster score sums over rows grouped by cluster (a stable cluster permutation);
+//   - connected components of two FE terms (dof.rs:222 mobility_groups) by lock-free
+//     union-find, and the nested-within check (dof.rs:184).
+// Every floating-point sum is a per-CTA partial combined in a fixed order: results do not depend
+// on timing.
+#pragma once
+
+#include <cstdint>
+
+#include "device.cuh"
+
+namespace fereg {
+
+constexpr int ST_TB = 256;          // threads per CTA of the stats passes
+constexpr int ST_GRID = 148 * 2;    // CTAs of the row passes
+constexpr int OP_ROWS = 32;         // rows staged per tile of the outer-product pass
+constexpr int OP_PPT = 8;           // pairs per thread of one outer-product launch
+constexpr int OP_MAXP = ST_TB * OP_PPT;  // pairs of one launch
+constexpr int OP_MAXM = 64;         // largest staged vector length (msz) of one launch
+
+// ---------------------------------------------------------------------------------------------
+// Column statistics. Lane = (group, column) over a column chunk [j0, j0 + Rc), Rc <= 32; rows are
+// dealt to the groups of all warps in turn. Pass 1: [sum x, sum w x, sum x^2, sum w x^2] per
+// column; pass 2: [sum (x - mean)^2, sum w (x - wmean)^2]. part[cta][col][NV].
+template <int NV>
+__device__ __forceinline__ void colstat_add(double x, double w, int pass, const double* mean, const double* wmean,
+                                            int col, double* a) {
+    if (pass == 1) {
+        a[0] += x;
+        a[1] += w * x;
+        a[2] += x * x;
+        a[3] += w * x * x;
+    } else {
+        const double d = x - mean[col], dw = x - wmean[col];
+        a[0] += d * d;
+        a[1] += w * dw * dw;
+    }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(ST_TB) k_colstats(const double* __restrict__ rows, size_t n, int R, int j0, int Rc,
+                                                    const double* __restrict__ w, int pass,
+                                                    const double* __restrict__ mean,
+                                                    const double* __restrict__ wmean, double* __restrict__ part) {
+    __shared__ double red[ST_TB / 32][32][NV];
+    int rcp = 1;
+    while (rcp < Rc) rcp <<= 1;
+    const int G = 32 / rcp;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / rcp, j = lane % rcp;
+    const bool on = j < Rc;
+    double a[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) a[v] = 0.0;
+    const size_t gw = size_t(blockIdx.x) * (ST_TB / 32) + warp, nw = size_t(gridDim.x) * (ST_TB / 32);
+    if (on)
+        for (size_t r = gw * G + g; r < n; r += nw * G) {
+            const double x = rows[r * R + j0 + j];
+            colstat_add<NV>(x, w ? w[r] : 1.0, pass, mean, wmean, j0 + j, a);
+        }
+#pragma unroll
+    for (int v = 0; v < NV; v++) red[warp][lane][v] = on ? a[v] : 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < Rc * NV; i += ST_TB) {
+        const int col = i / NV, v = i % NV;
+        double s = 0.0;
+        for (int wp = 0; wp < ST_TB / 32; wp++)
+            for (int gg = 0; gg < G; gg++) s += red[wp][gg * rcp + col][v];
+        part[(size_t(blockIdx.x) * R + j0 + col) * NV + v] = s;
+    }
+}
+
+// Sum of `parts` rows of length len (fixed order), one thread per element.
+__global__ void k_sum_parts(const double* __restrict__ part, int parts, int len, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= len) return;
+    double s = 0.0;
+    for (int p = 0; p < parts; p++) s += part[size_t(p) * len + i];
+    out[i] = s;
+}
+
+// Sum of the weights (sum w, and the count) over rows.
+__global__ void __launch_bounds__(ST_TB) k_sum_w(const double* __restrict__ w, size_t n, double* __restrict__ part) {
+    __shared__ double red[ST_TB];
+    double s = 0.0;
+    for (size_t i = size_t(blockIdx.x) * ST_TB + threadIdx.x; i < n; i += size_t(gridDim.x) * ST_TB) s += w[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = ST_TB / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Weighted outer products: sum_i om_i a_i a_i^T, a_i[p] = x_i[col[p]] + shift[p] for p < k and
+// a_i[k] = 1 when cst. Pairs (a, b), a <= b, in row-major upper-triangle order, pairs
+// [p0, p0 + np) of this launch (np <= OP_MAXP); ssq: also sum_i x_i[col[p]]^2 (unweighted) for
+// p < k. part[cta][np (+ k)].
+struct OpSpec {
+    const double* rows;   // n x R row-major
+    size_t n;
+    int R;
+    const int* col;       // k column indices (device)
+    const double* shift;  // k shifts (device) or null
+    int k, cst, msz;      // msz = k + cst
+    const double* om;     // per-row weight or null (= 1)
+    const int* perm;      // row i of the pass is rows[perm[i]] (null = identity)
+    int p0, np;
+    int ssq;
+};
+
+__global__ void __launch_bounds__(ST_TB) k_outer(OpSpec s, double* __restrict__ part) {
+    __shared__ double tile[OP_ROWS][OP_MAXM + 1];
+    __shared__ double tom[OP_ROWS];
+    __shared__ short pa[OP_MAXP], pb[OP_MAXP];
+    for (int q = threadIdx.x; q < s.np; q += ST_TB) {
+        // pair p0 + q -> (a, b): row a holds msz - a pairs
+        int p = s.p0 + q, a = 0;
+        while (p >= s.msz - a) {
+            p -= s.msz - a;
+            a++;
+        }
+        pa[q] = short(a);
+        pb[q] = short(a + p);
+    }
+    double acc[OP_PPT];
+#pragma unroll
+    for (int t = 0; t < OP_PPT; t++) acc[t] = 0.0;
+    double sq = 0.0;  // thread tid < k: sum x^2 of column tid
+    const size_t ntile = (s.n + OP_ROWS - 1) / OP_ROWS;
+    for (size_t tl = blockIdx.x; tl < ntile; tl += gridDim.x) {
+        __syncthreads();
+        const size_t r0 = tl * OP_ROWS;
+        const int nr = int((s.n - r0 < size_t(OP_ROWS) ? s.n - r0 : size_t(OP_ROWS)));
+        for (int e = threadIdx.x; e < nr * s.msz; e += ST_TB) {
+            const int i = e / s.msz, p = e % s.msz;
+            const size_t row = s.perm ? size_t(s.perm[r0 + i]) : r0 + i;
+            tile[i][p] = p < s.k ? s.rows[row * s.R + s.col[p]] + (s.shift ? s.shift[p] : 0.0) : 1.0;
+        }
+        for (int i = threadIdx.x; i < nr; i += ST_TB) {
+            const size_t row = s.perm ? size_t(s.perm[r0 + i]) : r0 + i;
+            tom[i] = s.om ? s.om[row] : 1.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < OP_PPT; t++) {
+            const int q = threadIdx.x + t * ST_TB;
+            if (q < s.np) {
+                const int a = pa[q], b = pb[q];
+                double v = acc[t];
+                for (int i = 0; i < nr; i++) v += tom[i] * tile[i][a] * tile[i][b];
+                acc[t] = v;
+            }
+        }
+        if (s.ssq && threadIdx.x < s.k) {
+            const double sh = s.shift ? s.shift[threadIdx.x] : 0.0;
+            for (int i = 0; i < nr; i++) {
+                const double x = tile[i][threadIdx.x] - sh;
+                sq += x * x;
+            }
+        }
+    }
+    const int len = s.np + (s.ssq ? s.k : 0);
+#pragma unroll
+    for (int t = 0; t < OP_PPT; t++) {
+        const int q = threadIdx.x + t * ST_TB;
+        if (q < s.np) part[size_t(blockIdx.x) * len + q] = acc[t];
+    }
+    if (s.ssq && threadIdx.x < s.k) part[size_t(blockIdx.x) * len + s.np + threadIdx.x] = sq;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Residuals: e_i = y_i - sum_p beta[p] x_i[col[p]] (y = column 0, or 0 when y_zero); per-CTA
+// partials of sum om_i e_i^2.
+__global__ void __launch_bounds__(ST_TB) k_resid_e(const double* __restrict__ rows, size_t n, int R,
+                                                   const int* __restrict__ col, const double* __restrict__ beta, int k,
+                                                   int y_zero, const double* __restrict__ om, double* __restrict__ e,
+                                                   double* __restrict__ part) {
+    __shared__ double red[ST_TB];
+    double s = 0.0;
+    for (size_t i = size_t(blockIdx.x) * ST_TB + threadIdx.x; i < n; i += size_t(gridDim.x) * ST_TB) {
+        const double* row = rows + i * R;
+        double v = y_zero ? 0.0 : row[0];
+        for (int p = 0; p < k; p++) v -= beta[p] * row[col[p]];
+        e[i] = v;
+        s += (om ? om[i] : 1.0) * v * v;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = ST_TB / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// Robust meat weights (vcov.rs:292): e^2 (no weights), e^2 w (fweights), (e w)^2 (aweights,
+// pweights); cluster score weights: e w.
+__global__ void k_meat_weights(const double* __restrict__ e, const double* __restrict__ w, size_t n, int kind,
+                               int cluster, double* __restrict__ om) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const double wi = w ? w[i] : 1.0, ei = e[i];
+        if (cluster) om[i] = ei * wi;
+        else if (!w) om[i] = ei * ei;
+        else if (kind == 2) om[i] = ei * ei * wi;
+        else om[i] = (ei * wi) * (ei * wi);
+    }
+}
+
+// Cluster scores: S[g][p] = sum over the rows of cluster g (perm[coff[g]..coff[g+1]], in order)
+// of om_i a_i[p]; a warp per cluster, lanes over p.
+__global__ void __launch_bounds__(ST_TB) k_cluster_scores(const double* __restrict__ rows, int R,
+                                                          const int* __restrict__ col,
+                                                          const double* __restrict__ shift, int k, int cst,
+                                                          const double* __restrict__ om, const int* __restrict__ perm,
+                                                          const u32* __restrict__ coff, u32 G, double* __restrict__ S) {
+    const int lane = threadIdx.x & 31;
+    const int msz = k + cst;
+    const size_t gw = size_t(blockIdx.x) * (ST_TB / 32) + (threadIdx.x >> 5), nw = size_t(gridDim.x) * (ST_TB / 32);
+    for (size_t g = gw; g < G; g += nw) {
+        for (int p0 = 0; p0 < msz; p0 += 32) {
+            const int p = p0 + lane;
+            double s = 0.0;
+            if (p < msz)
+                for (u32 q = coff[g]; q < coff[g + 1]; q++) {
+                    const size_t row = size_t(perm[q]);
+                    const double a = p < k ? rows[row * R + col[p]] + (shift ? shift[p] : 0.0) : 1.0;
+                    s += om[row] * a;
+                }
+            if (p < msz) S[g * msz + p] = s;
+        }
+    }
+}
+
+__global__ void k_zero_col(double* __restrict__ rows, size_t n, int R, int c) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        rows[i * R + c] = 0.0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Connected components of the bipartite graph of two terms (vertices: a-levels 0..ga-1, then
+// b-levels ga..ga+gb-1). Linking always hangs the larger root below the smaller one, so a
+// component's root is its smallest vertex: its smallest a-level (every b-level meets some
+// a-level). The partition is unique, so labels do not depend on timing.
+__global__ void k_uf_init(u32* __restrict__ parent, u32 nv) {
+    for (u32 v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) parent[v] = v;
+}
+
+__device__ __forceinline__ u32 uf_find(u32* parent, u32 v) {
+    // Path halving. Parents only decrease (a link sets parent[hi] = lo < hi; halving sets an
+    // ancestor), so the walk strictly descends and ends at a root. Reads bypass L1: parents
+    // change under concurrent links.
+    u32 p = __ldcg(parent + v);
+    while (p != v) {
+        const u32 gp = __ldcg(parent + p);
+        if (gp != p) parent[v] = gp;  // benign race: any ancestor is a valid parent
+        v = p;
+        p = __ldcg(parent + v);
+    }
+    return v;
+}
+
+// err: set to 1 if a union step ran out of its retry budget (never expected).
+__global__ void k_uf_union(const u32* __restrict__ a, const u32* __restrict__ b, u32 ga, size_t n, u32* parent,
+                           int* err) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        u32 u = a[i], v = ga + b[i];
+        for (int it = 0; it < (1 << 20); it++) {
+            u = uf_find(parent, u);
+            v = uf_find(parent, v);
+            if (u == v) break;
+            const u32 lo = min(u, v), hi = max(u, v);
+            const u32 old = atomicCAS(parent + hi, hi, lo);
+            if (old == hi) break;  // linked
+            u = lo;
+            v = old;  // hi already had a new parent: retry from there
+            if (it == (1 << 20) - 1) atomicExch(err, 1);
+        }
+    }
+}
+
+__global__ void k_uf_flatten(u32* parent, u32 nv) {
+    for (u32 v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        parent[v] = uf_find(parent, v);
+}
+
+// flags[l] = 1 when a-level l is its component's root.
+__global__ void k_uf_roots(const u32* __restrict__ parent, u32 ga, u32* __restrict__ flags) {
+    for (u32 l = blockIdx.x * blockDim.x + threadIdx.x; l < ga; l += gridDim.x * blockDim.x)
+        flags[l] = parent[l] == l ? 1u : 0u;
+}
+
+// groupvar[i] = 1-based component number of row i (components numbered by their smallest
+// a-level): id = exclusive scan of the root flags + 1.
+__global__ void k_uf_label(const u32* __restrict__ a, size_t n, const u32* __restrict__ parent,
+                           const u32* __restrict__ scan, u32* __restrict__ gv) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        gv[i] = scan[parent[a[i]]] + 1u;
+}
+
+// Nested within (dof.rs:184): map[level] takes the first cluster value seen; any other value
+// marks the term as not nested (flag = 1). Rows in any order give the same verdict.
+__global__ void k_nested(const u32* __restrict__ codes, const u32* __restrict__ cl, size_t n, u32* map, int* flag) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const u32 old = atomicCAS(map + codes[i], 0xffffffffu, cl[i]);
+        if (old != 0xffffffffu && old != cl[i]) atomicExch(flag, 1);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Exclusive scan of u32 (three passes: block sums, a scan of the block sums in one CTA, block
+// scans plus their offsets). total (device) receives the sum.
+constexpr int SCAN_TB = 256, SCAN_ITEMS = 8, SCAN_TILE = SCAN_TB * SCAN_ITEMS;
+
+__device__ __forceinline__ u32 block_excl_scan(u32 v, u32* sh, u32* total) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < SCAN_TB; off <<= 1) {
+        const u32 t = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
+        __syncthreads();
+        sh[threadIdx.x] += t;
+        __syncthreads();
+    }
+    const u32 incl = sh[threadIdx.x];
+    if (total) *total = sh[SCAN_TB - 1];
+    __syncthreads();
+    return incl - v;
+}
+
+__global__ void __launch_bounds__(SCAN_TB) k_scan_sums(const u32* __restrict__ in, size_t n, u32* __restrict__ bsum) {
+    __shared__ u32 sh[SCAN_TB];
+    const size_t base = size_t(blockIdx.x) * SCAN_TILE + size_t(threadIdx.x) * SCAN_ITEMS;
+    u32 s = 0;
+    for (int t = 0; t < SCAN_ITEMS; t++)
+        if (base + t < n) s += in[base + t];
+    u32 tot;
+    block_excl_scan(s, sh, &tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SCAN_TB) k_scan_top(u32* bsum, u32 nb, u32* total) {
+    __shared__ u32 sh[SCAN_TB];
+    u32 carry = 0;
+    for (u32 b0 = 0; b0 < nb; b0 += SCAN_TB) {
+        const u32 b = b0 + threadIdx.x;
+        const u32 v = b < nb ? bsum[b] : 0u;
+        u32 tot;
+        const u32 ex = block_excl_scan(v, sh, &tot);
+        if (b < nb) bsum[b] = carry + ex;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_TB) k_scan_apply(const u32* __restrict__ in, size_t n,
+                                                        const u32* __restrict__ bsum, u32* __restrict__ out) {
+    __shared__ u32 sh[SCAN_TB];
+    const size_t base = size_t(blockIdx.x) * SCAN_TILE + size_t(threadIdx.x) * SCAN_ITEMS;
+    u32 v[SCAN_ITEMS], s = 0;
+    for (int t = 0; t < SCAN_ITEMS; t++) {
+        v[t] = base + t < n ? in[base + t] : 0u;
+        s += v[t];
+    }
+    u32 run = block_excl_scan(s, sh, nullptr) + bsum[blockIdx.x];
+    for (int t = 0; t < SCAN_ITEMS; t++) {
+        if (base + t < n) out[base + t] = run;
+        run += v[t];
+    }
+}
+
+}  // namespace fereg

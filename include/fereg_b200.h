@@ -103,11 +103,13 @@ int fereg_absorber_term_values(const fereg_absorber* h, const double* coefs, siz
 void* fereg_absorber_stream(const fereg_absorber* h);
 
 /* Phase timing with CUDA events on the handle's stream (the reference's PhaseTimer, timing.rs;
- * reported under verbose >= 2 as in solve.rs:387-392). Enabling resets the totals. Slots:
- * 0 rhs segment pass, 1 rhs pull, 2 operator S*P, 3 preconditioner, 4 PCG vector work,
- * 5 residualize pass, 6 host-to-device rows, 7 device-to-host rows. */
+ * reported under verbose >= 2 as in solve.rs:387-392). Enabling resets the totals. Slots
+ * (FEREG_PHASE_SLOTS): 0 rhs segment pass, 1 rhs coordinate-list pass, 2 operator S*P segment
+ * pass, 3 preconditioner, 4 PCG vector work, 5 residualize pass, 6 host-to-device rows,
+ * 7 device-to-host rows, 8 operator S*P coordinate-list pass. */
+#define FEREG_PHASE_SLOTS 9
 int fereg_absorber_set_profiling(fereg_absorber* h, int on);
-int fereg_absorber_phase_times(const fereg_absorber* h, double* ms8, uint64_t* counts8);
+int fereg_absorber_phase_times(const fereg_absorber* h, double* ms, uint64_t* counts);
 
 /* Kernel launches issued by this handle so far. */
 uint64_t fereg_absorber_launches(const fereg_absorber* h);
@@ -119,6 +121,64 @@ int fereg_absorber_rhs(fereg_absorber* h, const double* rows, size_t r, double* 
 int fereg_absorber_precond(fereg_absorber* h, const double* rr, size_t r, double* z);
 int fereg_absorber_weight_state(const fereg_absorber* h, double* n1, double* nr, double* diag, uint8_t* redundant,
                                 double* sw);
+
+/* ---------------------------------------------------------------------------------------------
+ * Estimation session: the part of the reference's `Session` (session.rs) that `Session::ols`
+ * (ols.rs:199-470) uses, over the B200 absorber. Codes are the prepared kept-order codes
+ * (after factorize / drop_singletons / restrict, session.rs:243-280). */
+typedef struct fereg_session fereg_session;
+
+/* ols.rs Spec: vce 0 unadjusted, 1 robust (HC1), 2 cluster (CRV1 over all the session's cluster
+ * dimensions, multiway by inclusion-exclusion); firstpair: dof from the first FE pair only
+ * (dof.rs DofOptions); want_groupvar: mobility groups of the first pair into out->groupvar. */
+typedef struct fereg_ols_spec {
+    int vce;
+    int noconstant;
+    int firstpair;
+    int want_groupvar;
+    double tol;
+    size_t maxiter;
+    int precision; /* FEREG_PREC_* of the FE solve */
+} fereg_ols_spec;
+
+/* EstResult of ols.rs:263-470. Buffers (NULL to skip): b (nx + 1, the constant last),
+ * V ((nx + 1)^2), status (nx: 0 ok, 2 absorbed by the FE, 3 collinear), resid / d / groupvar
+ * (n, kept order; d = sum of the fixed effects), dof_table (5 per FE term: levels, redundant,
+ * levels - redundant, inexact, nested; 64 terms at most). */
+typedef struct fereg_ols_out {
+    double* b;
+    double* V;
+    uint8_t* status;
+    double* resid;
+    double* d;
+    double* groupvar;
+    double* dof_table;
+    int32_t nslots, k_all, y_absorbed;
+    double N, rank, df_r, df_m, df_a, df_a_initial, df_a_redundant, df_a_nested;
+    double N_clust, N_clustervars, N_clust1, N_clust2, num_singletons, N_full, report_constant;
+    double rss, tss, tss_within, mss, rmse, r2, r2_a, r2_within, r2_a_within, ll, ll_0, F, sumweights, ic;
+} fereg_ols_out;
+
+/* Session over nterms kept-order FE terms (codes[q] < g[q]; nterms = 0: noabsorb), ncl cluster
+ * dimensions (kept-order codes), weights w (kept order, NULL for none) of weight_kind 1 aweight,
+ * 2 fweight, 3 pweight, n kept rows; num_singletons as dropped by the preparation. */
+int fereg_session_create(const uint32_t* const* codes, const uint32_t* g, int nterms, const uint32_t* const* cl_codes,
+                         const uint32_t* cl_g, int ncl, const double* w, int weight_kind, size_t n,
+                         uint64_t num_singletons, const fereg_ctx* ctx, fereg_session** out);
+void fereg_session_destroy(fereg_session* s);
+
+/* Session::row_order: the rows of an ols block (n values, kept-observation indices). */
+int fereg_session_row_order(const fereg_session* s, uint32_t* out);
+
+/* Session::ols (ols.rs:199): OLS of column 0 on columns 1..nx of the n x (1 + nx) row-major
+ * block `rows` in row order, host memory or (rows_on_device = 1) device memory of the current
+ * device. The block is residualized in place. */
+int fereg_session_ols(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_ols_spec* spec,
+                      fereg_ols_out* out);
+
+/* Kernel launches of the session so far (its passes and its absorber), and its CUDA stream. */
+uint64_t fereg_session_launches(const fereg_session* s);
+void* fereg_session_stream(const fereg_session* s);
 
 /* Bytes of the static device scratch of fereg_absorber_rhs_noalloc. */
 #define FEREG_RHS_NOALLOC_SCRATCH_BYTES (16u << 20)
