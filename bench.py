@@ -1,19 +1,25 @@
-"""Benchmark of the B200 fixed-effects solve on the 1e7-observation 3-FE OLS panel.
+"""Benchmark of the B200 OLS call on the 1e7-observation 3-FE panel (and the 1e5 2-FE panel).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config c2|c1]
+                    [--precision f64|f32r]
 
-One step is one call of the solve on the workload: the n x R block [y, x1..x10] (R = 11)
-residualized against indiv + firm + year (Absorber::residualize, the FE solve of the OLS call). `value` times the step with the block already resident in
-HBM; `e2e` times the same call through the C ABI with the block in pinned host memory (the
-host-to-device copy of the inputs and the device-to-host copy of the residualized block inside
-the timed region). Inputs (880 MB) exceed the 126 MB L2, so no flush runs between steps.
+One step is one OLS call (Session::ols, ols.rs:199-470) on a prepared session: degrees of
+freedom (mobility groups of the FE pairs), column statistics of the raw block, the FE solve of
+[y, x1..x10] against indiv + firm + year, the weighted Gram, collinearity, coefficients, the
+residuals and the iid variance. The session (the cell structure, built once from the FE codes)
+is prepared outside the timed region; its time is reported as `config.prepare_s`.
+
+`value` times the call with the n x R block already resident in HBM (a fresh copy before each
+call, outside the events); `e2e` times the same call through the C ABI with the block in pinned
+host memory: the host-to-device copy of the block and the copies of the results to the host are
+inside the timed region. Inputs (880 MB) exceed the 126 MB L2, so no flush runs between steps.
 
 Multi-GPU (torchrun): independent replicas, one per GPU (a single solve does not shard at this
 size); the step time is the max over ranks and `value` is seconds per call of the whole job.
 
 `--impl reference` times the reference's algorithm on the host cores: the CPU oracle (a C++
-restatement of the reference solver; the reference's Rust crate cannot be built here), with all
-host threads, on the same workload, metric and unit.
+restatement of the reference's session OLS; the reference's Rust crate cannot be built here),
+with all host threads, on the same prepared session, workload, metric and unit.
 """
 
 import argparse
@@ -36,6 +42,7 @@ CONFIGS = {
     "c1": dict(n_ind=10_000, years=10, n_firm=0, k=1, seed=10**5 * 100 + 42),
 }
 TOL = 1e-8
+METRIC = "sec/call (1e7-obs 3-FE OLS)"
 
 
 def make_data(cfg):
@@ -72,16 +79,10 @@ def make_data(cfg):
     return codes, g, rows
 
 
-def ols_from_residualized(zr):
-    """OLS coefficients and iid variance from the residualized block (FP64 on the device)."""
-    import torch
-
-    X = zr[:, 1:]
-    y = zr[:, 0]
-    G = X.T @ X
-    b = torch.linalg.solve(G, X.T @ y)
-    e = y - X @ b
-    return b, e @ e, G
+def workload_name(cfg_name):
+    if cfg_name == "c2":
+        return "OLS y~x1..x10 | indiv(1e6)+firm(1e5, row mod 1e5)+year(10), n=1e7, iid SEs"
+    return "OLS y~x1 | indiv(1e4)+year(10), n=1e5, iid SEs"
 
 
 class ClockSampler:
@@ -149,8 +150,9 @@ def peaks():
 
 
 def traffic_from_profiles(kernel, workload):
-    """Per-launch DRAM bytes of `kernel` on `workload` from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    """Per-launch DRAM bytes (read + write) of `kernel` on `workload` from the committed ncu
+    summary profiles/dram_traffic.txt (lines: kernel workload bytes)."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     try:
         with open(path) as f:
             for ln in f:
@@ -162,7 +164,34 @@ def traffic_from_profiles(kernel, workload):
     return None
 
 
-def dist_setup(n_gpus):
+def phase_bytes(info, n, R, weighted, s_v=8):
+    """Algorithmic (compulsory) DRAM bytes of one call of each timed phase.
+
+    M cells, nb blocks (ns of them small), g1 FE1 levels, m reduced coordinates, E = M (nb - ns)
+    coordinate-list entries. Gathers that stay in L2 (P, t rows) count once."""
+    M, nb, g1, m = info["ncells"], info["nb"], info["g1"], info["m"]
+    ns = info["small_blocks"]
+    E = M * (nb - ns)
+    wrow = n * 8 if weighted else 0
+    wcell = M * 8 if weighted else 0
+    return {
+        "rhs_seg": n * R * 8 + wrow + g1 * R * 8 + g1 * 4 + g1 * 8 + M * ns * 4,
+        "rhs_pull": E * 8 + E * R * 8 + g1 * R * 8 + g1 * 8 + m * R * 8,
+        "apply_seg": M * nb * 4 + wcell + g1 * 8 + g1 * 4 + g1 * R * s_v + m * R * s_v,
+        "apply_pull": E * nb * 4 + g1 * R * s_v + 2 * m * R * s_v + m * 12,
+        "residualize": 2 * n * R * 8 + M * nb * 4 + g1 * R * 8 + g1 * 8 + g1 * 4 + m * R * 8,
+        "colstats": 2 * (n * R * 8 + wrow),
+        "gram": n * R * 8 + wrow,
+        "variance": n * R * 8 + n * 8 + wrow,
+    }
+
+
+PHASE_KERNEL = {"rhs_seg": "k_wseg_rhs", "rhs_pull": "k_wpull_rhs", "apply_seg": "k_wseg_apply",
+                "apply_pull": "k_wpull_apply", "residualize": "k_wresid", "colstats": "k_colstats",
+                "gram": "k_outer", "variance": "k_resid_e"}
+
+
+def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -192,43 +221,44 @@ def barrier(pg):
         pg.barrier()
 
 
+def oracle_session(codes, g, rows):
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    sess = oracle.Session(codes, g)
+    prep = time.perf_counter() - t0
+    return sess, np.ascontiguousarray(rows[sess.row_order()]), prep
+
+
 def run_reference(args, cfg_name, cfg, rank, world):
-    """The reference's algorithm on the host cores (the CPU oracle), same metric and unit."""
+    """The reference's session OLS on the host cores (the CPU oracle), same metric and unit."""
     if rank != 0:
         return
     from oracle import oracle
 
     codes, g, rows = make_data(cfg)
-    threads = oracle.max_threads()
-    ab = oracle.Absorber(codes, g)
+    sess, rows_ro, prep = oracle_session(codes, g, rows)
     times = []
     for it in range(args.warmup + args.steps):
-        z = rows.copy()
+        z = rows_ro.copy()
         t0 = time.perf_counter()
-        ab.residualize(z, tol=TOL)
+        sess.ols(z, tol=TOL)
         t1 = time.perf_counter()
         if it >= args.warmup:
             times.append(t1 - t0)
     v = float(np.mean(times))
+    threads = oracle.max_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(cfg_name, cfg), "n": len(rows), "R": rows.shape[1]},
+        "config": {"workload": workload_name(cfg_name), "n": len(rows), "R": rows.shape[1], "prepare_s": prep},
         "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
-                         "sample": "full workload per step (C++ FP64 restatement of the reference solver, OpenMP)"},
+                         "sample": "one OLS call on the full workload per step (C++ FP64 restatement of the "
+                                   "reference's session OLS, OpenMP, all host threads)"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-METRIC = "sec/call (1e7-obs 3-FE OLS)"
-
-
-def workload_name(cfg_name, cfg):
-    if cfg_name == "c2":
-        return "OLS y~x1..x10 | indiv(1e6)+firm(1e5, row mod 1e5)+year(10), n=1e7, iid SEs"
-    return "OLS y~x1 | indiv(1e4)+year(10), n=1e5, iid SEs"
 
 
 def main():
@@ -244,7 +274,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     cfg = CONFIGS[args.config]
-    rank, world, local, pg = dist_setup(args.gpus)
+    rank, world, local, pg = dist_setup()
     if args.impl == "reference":
         run_reference(args, args.config, cfg, rank, world)
         if pg is not None:
@@ -260,12 +290,13 @@ def main():
     prec = fb.PREC_F64 if args.precision == "f64" else fb.PREC_F32_REFINED
     codes, g, rows = make_data(cfg)
     n, R = rows.shape
+    nx = R - 1
     t0 = time.perf_counter()
-    ab = fb.Absorber(codes, g)
+    sess = fb.Session(codes, g)
     prepare_s = time.perf_counter() - t0
-    pi = ab.row_order()
-    rows = np.ascontiguousarray(rows[pi])  # the caller hands rows in the absorber's row order
-    stream = torch.cuda.ExternalStream(ab.stream(), device=device)
+    info = sess.info()
+    rows = np.ascontiguousarray(rows[sess.row_order()])  # the caller hands rows in the session's row order
+    stream = torch.cuda.ExternalStream(sess.stream(), device=device)
     src = torch.from_numpy(rows).to(device)
     work = torch.empty_like(src)
 
@@ -275,40 +306,40 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        info = ab.residualize_device(work.data_ptr(), R, tol=TOL, precision=prec)
+        res = sess.ols_device(work.data_ptr(), nx, tol=TOL, precision=prec)
         e1.record(stream)
         e1.synchronize()
-        return e0.elapsed_time(e1) / 1e3, info, None
+        return e0.elapsed_time(e1) / 1e3, res
 
     for _ in range(args.warmup):
         step_device()
     barrier(pg)
     torch.cuda.synchronize(device)
-    ab.set_profiling(True)
-    l0 = ab.launches()
+    sess.set_profiling(True)
+    l0 = sess.launches()
     times = []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            dt, info, b = step_device()
+            dt, res = step_device()
             times.append(dt)
     torch.cuda.synchronize(device)
     barrier(pg)
-    launches = ab.launches() - l0
-    phases = ab.phase_times()
-    ab.set_profiling(False)
+    launches = sess.launches() - l0
+    phases = sess.phase_times()
+    sess.set_profiling(False)
     step_s = max_over_ranks(float(np.mean(times)), pg, device)
     value = step_s / world
 
     # e2e: the same call through the C ABI with the block in pinned host memory
     pinned = torch.empty((n, R), dtype=torch.float64, pin_memory=True)
     host = pinned.numpy()
+    np.copyto(host, rows)
 
     def step_e2e():
-        np.copyto(host, rows)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        ab.residualize(host, tol=TOL, precision=prec)
+        sess.ols(host, tol=TOL, precision=prec)
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1) / 1e3
@@ -320,54 +351,55 @@ def main():
         barrier(pg)
         e2e_times = [step_e2e() for _ in range(max(3, args.steps // 2))]
         e2e_s = max_over_ranks(float(np.mean(e2e_times)), pg, device) / world
+    k_all = nx + 1
+    d2h = (k_all + k_all * k_all + nx) * 8
 
-    # roofline of the dominant kernel (largest share of the timed phases)
+    # roofline of the dominant kernel phase (largest share of the timed phases)
     hbm, peak_kind = peaks()
-    M, nb, g1 = ab.ncells, ab.nb, ab.g1
-    algo = {
-        "residualize": 2 * n * R * 8 + M * nb * 4 + g1 * R * 8 + g1 * 8,
-        "rhs_seg": n * R * 8 + g1 * R * 8 + (g1 + 1) * 4,
-    }
-    dom = max(algo, key=lambda k: phases[k][0])
-    ms, cnt = phases[dom]
-    achieved = algo[dom] / (ms / cnt / 1e3) / 1e9 if cnt else None
-    kern = {"residualize": "k_residualize", "rhs_seg": "k_rhs_seg"}[dom]
+    algo = phase_bytes(info, n, R, False, 8 if prec == fb.PREC_F64 else 4)
+    timed = {k: v for k, v in phases.items() if k in algo and v[1]}
+    dom = max(timed, key=lambda k: timed[k][0])
+    ms, cnt = timed[dom]
+    achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
+    kern = PHASE_KERNEL[dom]
     traffic = traffic_from_profiles(kern, args.config)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle
 
-        oab = oracle.Absorber(codes, g)
+        osess, orows, oprep = oracle_session(codes, g, make_data(cfg)[2])
         ts = []
-        for _ in range(3):
-            z = rows.copy()
+        for _ in range(2):
+            z = orows.copy()
             t1 = time.perf_counter()
-            oab.residualize(z, tol=TOL)
+            osess.ols(z, tol=TOL)
             ts.append(time.perf_counter() - t1)
         cpu = {"value": float(np.mean(ts)), "unit": "s", "cores": oracle.max_threads(), "kind": "port",
-               "sample": "full workload, 3 calls (C++ FP64 restatement of the reference solver, OpenMP)"}
+               "sample": "2 OLS calls on the full workload (C++ FP64 restatement of the reference's session OLS, "
+                         f"OpenMP); its session prepare took {oprep:.3f} s"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == fb.PREC_F64 else "f32+f64", "data": "synthetic",
-            "config": {"workload": workload_name(args.config, cfg), "n": n, "R": R, "cells": M, "m": ab.m,
-                       "g1": g1, "iterations": info["iterations"], "tol": TOL,
+            "config": {"workload": workload_name(args.config), "n": n, "R": R, "cells": info["ncells"],
+                       "m": info["m"], "g1": info["g1"], "pcg_iterations": int(res["scalars"]["ic"]), "tol": TOL,
                        "precision": args.precision, "l2": "inputs (880 MB) larger than L2, no flush",
-                       "parallelism": f"replicas x{world}", "prepare_s": prepare_s},
-            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm if achieved else None, "traffic": traffic,
-                         "peak_kind": peak_kind, "algorithmic_bytes": algo[dom]},
+                       "parallelism": f"replicas x{world}", "prepare_s": prepare_s,
+                       "b_x1": float(res["b"][0])},
+            "roofline": {"bound": "hbm", "kernel": kern, "phase": dom, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                         "algorithmic_bytes": algo[dom]},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
-            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": n * R * 8, "d2h_bytes_per_step": n * R * 8},
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": n * R * 8, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
-    ab.close()
+    sess.close()
     if pg is not None:
         barrier(pg)
         pg.destroy_process_group()

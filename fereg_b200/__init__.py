@@ -102,6 +102,9 @@ def _setup(L):
     L.fereg_session_launches.restype = C.c_uint64
     L.fereg_session_stream.argtypes = [P]
     L.fereg_session_stream.restype = P
+    L.fereg_session_set_profiling.argtypes = [P, C.c_int]
+    L.fereg_session_info.argtypes = [P, u64p]
+    L.fereg_session_phase_times.argtypes = [P, f64p, u64p]
     L.fereg_absorber_stream.argtypes = [P]
     L.fereg_absorber_stream.restype = P
     L.fereg_absorber_set_profiling.argtypes = [P, C.c_int]
@@ -140,7 +143,7 @@ class Absorber:
         _check(lib().fereg_absorber_create(ptrs, _p(self.g, u32p), len(self._codes), _p(wa, f64p), self.n, None,
                                            C.byref(h)))
         self.h = h
-        info = np.zeros(8, dtype=np.uint64)
+        info = np.zeros(9, dtype=np.uint64)
         _check(lib().fereg_absorber_info(self.h, _p(info, u64p)))
         self.m, self.g1, self.ncells, self.nb, self.m_small = (int(v) for v in info[1:6])
         self.fe1 = int(np.int64(info[6]))
@@ -296,8 +299,29 @@ class Session:
         _check(lib().fereg_session_row_order(self.h, _p(out, u32p)))
         return out
 
+    def info(self):
+        """Structure of the session's absorber: n, m, g1, ncells, nb, m_small, fe1, small_work,
+        small_blocks."""
+        v = np.zeros(9, dtype=np.uint64)
+        _check(lib().fereg_session_info(self.h, _p(v, u64p)))
+        keys = ["n", "m", "g1", "ncells", "nb", "m_small", "fe1", "small_work", "small_blocks"]
+        out = {k: int(x) for k, x in zip(keys, v)}
+        out["fe1"] = int(np.int64(v[6]))
+        return out
+
     def launches(self):
         return int(lib().fereg_session_launches(self.h))
+
+    PHASES = Absorber.PHASES + ["dof", "colstats", "gram", "variance"]
+
+    def set_profiling(self, on=True):
+        _check(lib().fereg_session_set_profiling(self.h, int(on)))
+
+    def phase_times(self):
+        ms = np.zeros(len(self.PHASES))
+        cnt = np.zeros(len(self.PHASES), dtype=np.uint64)
+        _check(lib().fereg_session_phase_times(self.h, _p(ms, f64p), _p(cnt, u64p)))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PHASES)}
 
     def stream(self):
         return int(lib().fereg_session_stream(self.h) or 0)
@@ -324,7 +348,7 @@ class Session:
     def ols(self, rows, nx=None, vce="unadjusted", noconstant=False, firstpair=False, want_groupvar=False,
             want_resid=False, want_d=False, tol=1e-8, maxiter=16000, precision=PREC_F64):
         """OLS of column 0 on the other columns of the n x (1 + nx) host block (row order);
-        the block is residualized in place."""
+        the block is copied to the device (left unchanged)."""
         assert rows.dtype == np.float64 and rows.flags.c_contiguous
         nx = rows.shape[1] - 1 if nx is None else nx
         return self._call(rows.ctypes.data, 0, nx, vce, noconstant, firstpair, want_groupvar, want_resid, want_d,

@@ -80,6 +80,22 @@ double* rhs_scratch_on_current_device() {
     return g_rhs_scratch_addr[dev];
 }
 
+// fereg_absorber_info: n, m, g1, ncells, nb, m_small, fe1, small_work, small blocks.
+void fill_info(const GpuAbsorber& a, uint64_t* o) {
+    const auto& st = a.structure();
+    o[0] = st.n;
+    o[1] = st.m;
+    o[2] = st.g1;
+    o[3] = st.ncells;
+    o[4] = st.nb();
+    o[5] = st.m_small;
+    o[6] = uint64_t(int64_t(st.fe1));
+    o[7] = st.small_work;
+    u64 ns = 0;
+    for (const auto& b : st.blocks) ns += b.small ? 1 : 0;
+    o[8] = ns;
+}
+
 void fill(fereg_solve_info* info, const SolveInfo& s) {
     if (!info) return;
     info->iterations = s.iterations;
@@ -195,15 +211,14 @@ uint64_t fereg_absorber_launches(const fereg_absorber* h) { return h ? h->a.laun
 int fereg_absorber_info(const fereg_absorber* h, uint64_t* o) {
     return guard([&] {
         if (!h || !o) throw Error(RC_INVALID_INPUT, "fereg_absorber_info: NULL argument");
-        const auto& st = h->a.structure();
-        o[0] = st.n;
-        o[1] = st.m;
-        o[2] = st.g1;
-        o[3] = st.ncells;
-        o[4] = st.nb();
-        o[5] = st.m_small;
-        o[6] = uint64_t(int64_t(st.fe1));
-        o[7] = st.small_work;
+        fill_info(h->a, o);
+    });
+}
+
+int fereg_session_info(const fereg_session* s, uint64_t* o) {
+    return guard([&] {
+        if (!s || !o) throw Error(RC_INVALID_INPUT, "fereg_session_info: NULL argument");
+        fill_info(s->s.absorber(), o);
     });
 }
 
@@ -319,6 +334,20 @@ int fereg_session_ols(fereg_session* s, double* rows, int rows_on_device, size_t
         out->F = o.F;
         out->sumweights = o.sumweights;
         out->ic = o.ic;
+    });
+}
+
+int fereg_session_set_profiling(fereg_session* s, int on) {
+    return guard([&] {
+        if (!s) throw Error(RC_INVALID_INPUT, "fereg_session_set_profiling: NULL handle");
+        s->s.set_profiling(on != 0);
+    });
+}
+
+int fereg_session_phase_times(const fereg_session* s, double* ms, uint64_t* counts) {
+    return guard([&] {
+        if (!s) throw Error(RC_INVALID_INPUT, "fereg_session_phase_times: NULL handle");
+        s->s.phase_times(ms, counts);
     });
 }
 

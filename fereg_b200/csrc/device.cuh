@@ -45,6 +45,12 @@ struct DBuf {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Padded width (a power of two up to 32) of a chunk of Rc columns: lanes of a warp form
+// 32 / width groups of `width` consecutive columns.
+__host__ __device__ constexpr int rcp_of(int Rc) {
+    return Rc <= 1 ? 1 : Rc <= 2 ? 2 : Rc <= 4 ? 4 : Rc <= 8 ? 8 : Rc <= 16 ? 16 : 32;
+}
+
 // Lane layout of a warp over (entry slot, column) pairs for a block of R columns: with R <= 32
 // the warp holds G = 32/R slots of R consecutive columns (lane = slot*R + col), so consecutive
 // lanes touch consecutive doubles of a row-major row block; with R > 32 the columns are walked

@@ -71,6 +71,58 @@ struct SessionDev {
     DBuf<double> pstat;
     cudaStream_t st = nullptr;
     u64 launches = 0;
+    // phase timing (CUDA events on the session's stream)
+    bool prof = false;
+    double ms[GpuSession::S_NSLOTS] = {};
+    u64 cnt[GpuSession::S_NSLOTS] = {};
+    std::vector<cudaEvent_t> pool;
+    struct Open {
+        int slot;
+        cudaEvent_t a, b;
+    };
+    std::vector<Open> open;
+    cudaEvent_t event() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        return e;
+    }
+    int begin(int slot) {
+        if (!prof) return -1;
+        open.push_back(Open{slot, event(), nullptr});
+        CK(cudaEventRecord(open.back().a, st));
+        return int(open.size()) - 1;
+    }
+    void end(int h) {
+        if (h < 0) return;
+        open[size_t(h)].b = event();
+        CK(cudaEventRecord(open[size_t(h)].b, st));
+    }
+    void collect() {
+        for (auto& o : open) {
+            if (o.b) {
+                CK(cudaEventSynchronize(o.b));
+                float t = 0;
+                CK(cudaEventElapsedTime(&t, o.a, o.b));
+                ms[o.slot] += t;
+                cnt[o.slot]++;
+                pool.push_back(o.b);
+            }
+            pool.push_back(o.a);
+        }
+        open.clear();
+    }
+    ~SessionDev() {
+        for (auto& o : open) {
+            cudaEventDestroy(o.a);
+            if (o.b) cudaEventDestroy(o.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
 };
 
 GpuSession::GpuSession(const std::vector<const u32*>& codes, const std::vector<u32>& g,
@@ -156,6 +208,23 @@ GpuSession::~GpuSession() {
 }
 
 u64 GpuSession::launches() const { return d_->launches + ab_->launches(); }
+
+void GpuSession::set_profiling(bool on) {
+    d_->prof = on;
+    if (on) {
+        std::fill(d_->ms, d_->ms + S_NSLOTS, 0.0);
+        std::fill(d_->cnt, d_->cnt + S_NSLOTS, u64(0));
+    }
+    ab_->set_profiling(on);
+}
+
+void GpuSession::phase_times(double* ms, u64* counts) const {
+    ab_->phase_times(ms, counts);
+    for (int i = 0; i < S_NSLOTS; i++) {
+        if (ms) ms[GpuAbsorber::P_NSLOTS + i] = d_->ms[i];
+        if (counts) counts[GpuAbsorber::P_NSLOTS + i] = d_->cnt[i];
+    }
+}
 
 // dof.rs:222-256 mobility_groups of terms qa, qb on the device; save: keep the row labels.
 u64 GpuSession::mobility_groups(size_t qa, size_t qb, bool save) {
@@ -296,48 +365,47 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     const bool has_intercept = true;  // intercept-only terms (or noabsorb) contain the constant
     const bool report_constant = has_intercept && !spec.noconstant;
 
+    int ph = d.begin(S_DOF);
     const Dof dof = estimate_dof(vce == 2, spec.firstpair != 0, spec.want_groupvar != 0 && out.groupvar);
+    d.end(ph);
+    ph = d.begin(S_COLSTATS);
 
-    // Pass A: column statistics of the raw rows (stats.rs:40), raw weights
+    // Pass A: column statistics of the raw rows (stats.rs:40), raw weights, in one device pass
+    // about each column's first value
     const double* wr = weighted ? d.w_raw.p : nullptr;
-    d.part.alloc(size_t(ST_GRID) * r * 4);
-    d.sums.alloc(r * 4);
+    d.part.alloc(size_t(ST_GRID) * r * 6);
+    d.sums.alloc(r * 6);
     for (int j0 = 0; j0 < R; j0 += 32) {
         const int Rc = std::min(32, R - j0);
-        k_colstats<4><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, 1, nullptr, nullptr, d.part.p);
+        switch (rcp_of(Rc)) {
+            case 1: k_colstats1<1><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 2: k_colstats1<2><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 4: k_colstats1<4><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 8: k_colstats1<8><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 16: k_colstats1<16><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            default: k_colstats1<32><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+        }
         d.launches++;
     }
-    k_sum_parts<<<(R * 4 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 4, d.sums.p);
-    std::vector<double> s1(r * 4);
-    CK(cudaMemcpyAsync(s1.data(), d.sums.p, r * 4 * 8, cudaMemcpyDeviceToHost, st));
+    k_sum_parts<<<(R * 6 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 6, d.sums.p);
+    d.launches++;
+    std::vector<double> s1(r * 6), c0(r);
+    CK(cudaMemcpyAsync(s1.data(), d.sums.p, r * 6 * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c0.data(), rows, r * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    std::vector<double> mean(r), wmean(r), sumsq(r), wss_unc(r);
+    std::vector<double> wmean(r), sumsq(r), wss_unc(r), sd(r), wss(r);
     for (size_t j = 0; j < r; j++) {
-        mean[j] = s1[j * 4] / double(n);
-        wmean[j] = s1[j * 4 + 1] / sumw;
-        sumsq[j] = s1[j * 4 + 2];
-        wss_unc[j] = s1[j * 4 + 3];
-    }
-    d.pstat.alloc(2 * r);
-    CK(cudaMemcpyAsync(d.pstat.p, mean.data(), r * 8, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(d.pstat.p + r, wmean.data(), r * 8, cudaMemcpyHostToDevice, st));
-    for (int j0 = 0; j0 < R; j0 += 32) {
-        const int Rc = std::min(32, R - j0);
-        k_colstats<2><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, 2, d.pstat.p, d.pstat.p + r, d.part.p);
-        d.launches++;
-    }
-    k_sum_parts<<<(R * 2 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 2, d.sums.p);
-    d.launches += 2;
-    std::vector<double> s2(r * 2);
-    CK(cudaMemcpyAsync(s2.data(), d.sums.p, r * 2 * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    std::vector<double> sd(r), wss(r);
-    for (size_t j = 0; j < r; j++) {
-        sd[j] = std::max(std::sqrt(s2[j * 2] / (double(n) - 1.0)), 1e-3);
-        wss[j] = s2[j * 2 + 1];
+        const double* a = s1.data() + j * 6;
+        const double m2 = std::max(0.0, a[1] - a[0] * a[0] / double(n));
+        sd[j] = std::max(std::sqrt(m2 / (double(n) - 1.0)), 1e-3);
+        wmean[j] = c0[j] + a[2] / sumw;
+        wss[j] = std::max(0.0, a[3] - a[2] * a[2] / sumw);
+        sumsq[j] = a[4];
+        wss_unc[j] = a[5];
     }
     const double tscale = (kind == 1 || kind == 3) ? double(n) / sumw : 1.0;
     const double tss_y = (has_intercept ? wss[0] : wss_unc[0]) * tscale;
+    d.end(ph);
 
     // The FE solve, in place
     const bool want_coefs = out.d != nullptr;
@@ -363,6 +431,28 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
             CK(cudaMemcpyAsync(d.shift.p, shift->data(), size_t(k) * 8, cudaMemcpyHostToDevice, st));
         }
         std::vector<double> pairs(P), sq(k);
+        if (msz <= 32) {
+            const int len = msz * msz + (ssq ? k : 0);
+            d.part.alloc(size_t(ST_GRID) * len);
+            d.sums.alloc(size_t(len));
+            OpSpec sp{src, nrows, srcR, d.col.p, shift ? d.shift.p : nullptr, k, cst ? 1 : 0, msz, om, perm, 0, 0,
+                      ssq ? 1 : 0};
+            switch ((msz + 7) / 8) {
+                case 1: k_outer_mma<1><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+                case 2: k_outer_mma<2><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+                case 3: k_outer_mma<3><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+                default: k_outer_mma<4><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+            }
+            k_sum_parts<<<(len + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
+            d.launches += 2;
+            std::vector<double> h(len);
+            CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (int a = 0; a < msz; a++)
+                for (int b = a; b < msz; b++) m[size_t(a) * msz + b] = m[size_t(b) * msz + a] = h[size_t(a) * msz + b];
+            if (ss_out) *ss_out = std::vector<double>(h.begin() + msz * msz, h.end());
+            return m;
+        }
         for (int p0 = 0; p0 < P; p0 += OP_MAXP) {
             const int np = std::min(OP_MAXP, P - p0);
             const bool with_sq = ssq && p0 == 0;
@@ -388,11 +478,13 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     };
 
     // Pass B: weighted Gram of the residualized block (stats.rs:195)
+    ph = d.begin(S_GRAM);
     const double* wv = weighted ? d.wv.p : nullptr;
     std::vector<int> all_cols(r);
     std::iota(all_cols.begin(), all_cols.end(), 0);
     std::vector<double> ss_res;
     std::vector<double> g = outer(rows, n, R, all_cols, nullptr, false, wv, nullptr, true, &ss_res);
+    d.end(ph);
 
     // Collinearity, stage 1 (ols.rs:38 stage1_absorbed): a column absorbed by the FE
     const double ctol = std::min(1e-6, spec.tol / 10.0);
@@ -436,6 +528,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     for (size_t a = 0; a < k; a++) beta[a] = b_s[a] * sd_y / sd[kept[a]];
 
     // residuals and their weighted sum of squares
+    ph = d.begin(S_VARIANCE);
     std::vector<int> kcols(kept.begin(), kept.end());
     d.col.alloc(k + 1);
     d.beta.alloc(k + 1);
@@ -520,6 +613,8 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
             if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
         }
     }
+    d.end(ph);
+    d.collect();
     if (vce == 2) df_r = std::min(df_r, g_min - 1.0);
     for (size_t i = 0; i < msz; i++)
         for (size_t j = 0; j < i; j++) v_s[j * msz + i] = v_s[i * msz + j];

@@ -53,12 +53,19 @@ class GpuSession {
     ~GpuSession();
 
     GpuAbsorber& absorber() { return *ab_; }
+    const GpuAbsorber& absorber() const { return *ab_; }
     size_t n() const { return n_; }
     // Kernel launches of the session passes and its absorber so far.
     u64 launches() const;
 
+    // Phase timing: the absorber's slots (GpuAbsorber::Slot), then the session's own.
+    enum Slot { S_DOF = 0, S_COLSTATS, S_GRAM, S_VARIANCE, S_NSLOTS };
+    void set_profiling(bool on);
+    void phase_times(double* ms, u64* counts) const;  // GpuAbsorber::P_NSLOTS + S_NSLOTS slots
+
     // OLS of column 0 on columns 1..nx of the n x (1 + nx) row-major block `rows` (row order;
-    // host memory, or device memory when on_device). The block is residualized in place.
+    // host memory, or device memory when on_device). A device block is residualized in place; a
+    // host block is copied to the device and left unchanged.
     void ols(double* rows, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out);
 
    private:

@@ -43,10 +43,7 @@ struct WarpTiles {
 __device__ __forceinline__ u32 wlane() { return threadIdx.x & 31u; }
 __device__ __forceinline__ u32 wid_in_cta() { return threadIdx.x >> 5; }
 
-// Padded chunk width for Rc columns, and the block-count key.
-__host__ __device__ constexpr int rcp_of(int Rc) {
-    return Rc <= 1 ? 1 : Rc <= 2 ? 2 : Rc <= 4 ? 4 : Rc <= 8 ? 8 : Rc <= 16 ? 16 : 32;
-}
+// The block-count key.
 __host__ __device__ constexpr int nbk_of(u32 nb) { return nb < u32(WNB) ? int(nb) : WNB; }
 
 // Lane = (group g, column j) for a chunk padded to RCP columns.

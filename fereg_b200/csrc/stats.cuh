@@ -178,6 +178,228 @@ __global__ void __launch_bounds__(ST_TB) k_outer(OpSpec s, double* __restrict__ 
     if (s.ssq && threadIdx.x < s.k) part[size_t(blockIdx.x) * len + s.np + threadIdx.x] = sq;
 }
 
+// Outer products for msz <= 32 (the common case): lane = (group g, column j) of a chunk padded
+// to RCP; each group holds one row's vector a_i, and lane j accumulates row j of the matrix,
+// om_i a_i[j] a_i[b] for every b, taking a_i[b] from lane (g, b) by shuffle. Rows come U groups
+// at a time with their loads batched. Sums: per lane in row order, then groups and warps in a
+// fixed order into the CTA's partial part[cta][msz * msz (+ k)].
+template <int RCP>
+__global__ void __launch_bounds__(ST_TB) k_outer_small(OpSpec s, double* __restrict__ part) {
+    constexpr int G = 32 / RCP;
+    constexpr int U = RCP >= 32 ? 2 : 4;
+    __shared__ double red[RCP * RCP + RCP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / RCP, j = lane % RCP;
+    const bool on = j < s.msz;
+    const int colj = j < s.k ? s.col[j] : -1;
+    const double shj = (j < s.k && s.shift) ? s.shift[j] : 0.0;
+    for (int i = threadIdx.x; i < RCP * RCP + RCP; i += ST_TB) red[i] = 0.0;
+    double acc[RCP];
+#pragma unroll
+    for (int b = 0; b < RCP; b++) acc[b] = 0.0;
+    double sq = 0.0;
+    const size_t gw = size_t(blockIdx.x) * (ST_TB / 32) + warp, nw = size_t(gridDim.x) * (ST_TB / 32);
+    for (size_t base = gw * U * G; base < s.n; base += nw * U * G) {
+        double x[U], om[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const size_t r = base + size_t(u) * G + g;
+            x[u] = 0.0;
+            om[u] = 0.0;
+            if (r < s.n) {
+                const size_t row = s.perm ? size_t(s.perm[r]) : r;
+                if (on) x[u] = colj >= 0 ? s.rows[row * s.R + colj] + shj : 1.0;
+                om[u] = s.om ? s.om[row] : 1.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const double wx = om[u] * x[u];
+            if (s.ssq && colj >= 0) {
+                const double d = x[u] - shj;
+                sq += d * d;
+            }
+#pragma unroll
+            for (int b = 0; b < RCP; b++) acc[b] += wx * __shfl_sync(FULL, x[u], g * RCP + b);
+        }
+    }
+    // groups in order (lane (0, j) ends with the warp's row j), then warps in order
+#pragma unroll
+    for (int b = 0; b < RCP; b++) {
+        double t = 0.0;
+#pragma unroll
+        for (int gg = 0; gg < G; gg++) t += __shfl_sync(FULL, acc[b], gg * RCP + j);
+        acc[b] = t;
+    }
+    double tq = 0.0;
+#pragma unroll
+    for (int gg = 0; gg < G; gg++) tq += __shfl_sync(FULL, sq, gg * RCP + j);
+    __syncthreads();
+    for (int w = 0; w < ST_TB / 32; w++) {
+        if (warp == w && g == 0 && on) {
+#pragma unroll
+            for (int b = 0; b < RCP; b++) red[j * RCP + b] += acc[b];
+            red[RCP * RCP + j] += tq;
+        }
+        __syncthreads();
+    }
+    const int mm = s.msz * s.msz;
+    const int len = mm + (s.ssq ? s.k : 0);
+    for (int i = threadIdx.x; i < len; i += ST_TB)
+        part[size_t(blockIdx.x) * len + i] = i < mm ? red[(i / s.msz) * RCP + i % s.msz] : red[RCP * RCP + (i - mm)];
+}
+
+// Outer products on the FP64 tensor cores (mma.sync m8n8k4, f64 in and out), msz <= 8 NB: the
+// matrix is tiled by 8 x 8 blocks (bi <= bj). A warp takes 4 rows per MMA step: lane l holds
+// a_i[8 b + (l >> 2)] of row 4 t + (l & 3) for each column block b, which is both its A fragment
+// (scaled by om_i: A[m][k] = om a[8 bi + m] of row k) and its B fragment (B[k][n] =
+// a[8 bj + n] of row k). Each warp accumulates its rows in MMA order, then warps are added in a
+// fixed order into the CTA's partial part[cta][msz * msz (+ k)] (upper blocks filled).
+__device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int NB>
+__global__ void __launch_bounds__(ST_TB) k_outer_mma(OpSpec s, double* __restrict__ part) {
+    constexpr int NT = NB * (NB + 1) / 2, U = 4, W = 8 * NB;
+    __shared__ double red[W * W + W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int kr = lane & 3, cj = lane >> 2;
+    // column source of each block: >= 0 a row column, -1 the constant, -2 padding
+    int csrc[NB];
+    double csh[NB];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        const int c = 8 * b + cj;
+        csrc[b] = c < s.k ? s.col[c] : (c < s.msz ? -1 : -2);
+        csh[b] = (c < s.k && s.shift) ? s.shift[c] : 0.0;
+    }
+    for (int i = threadIdx.x; i < W * W + W; i += ST_TB) red[i] = 0.0;
+    double acc[NT][2];
+#pragma unroll
+    for (int t = 0; t < NT; t++) acc[t][0] = acc[t][1] = 0.0;
+    double sq[NB];
+#pragma unroll
+    for (int b = 0; b < NB; b++) sq[b] = 0.0;
+    const size_t gw = size_t(blockIdx.x) * (ST_TB / 32) + warp, nw = size_t(gridDim.x) * (ST_TB / 32);
+    for (size_t base = gw * U * 4; base < s.n; base += nw * U * 4) {
+        double v[U][NB], om[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const size_t r = base + size_t(u) * 4 + kr;
+            om[u] = 0.0;
+#pragma unroll
+            for (int b = 0; b < NB; b++) v[u][b] = 0.0;
+            if (r < s.n) {
+                const size_t row = s.perm ? size_t(s.perm[r]) : r;
+                om[u] = s.om ? s.om[row] : 1.0;
+#pragma unroll
+                for (int b = 0; b < NB; b++)
+                    v[u][b] = csrc[b] >= 0 ? s.rows[row * s.R + csrc[b]] + csh[b] : (csrc[b] == -1 ? 1.0 : 0.0);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (s.ssq) {
+#pragma unroll
+                for (int b = 0; b < NB; b++) {
+                    const double x = csrc[b] >= 0 ? v[u][b] - csh[b] : 0.0;
+                    sq[b] += x * x;
+                }
+            }
+            int t = 0;
+#pragma unroll
+            for (int bi = 0; bi < NB; bi++) {
+                const double a = om[u] * v[u][bi];
+#pragma unroll
+                for (int bj = bi; bj < NB; bj++, t++) dmma884(acc[t][0], acc[t][1], a, v[u][bj]);
+            }
+        }
+    }
+    // sums of squares: the 4 lanes of a column (l & 3 = 0..3) in order
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        double q = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) q += __shfl_sync(FULL, sq[b], (cj << 2) + k);
+        sq[b] = q;
+    }
+    __syncthreads();
+    for (int w = 0; w < ST_TB / 32; w++) {
+        if (warp == w) {
+            int t = 0;
+#pragma unroll
+            for (int bi = 0; bi < NB; bi++)
+#pragma unroll
+                for (int bj = bi; bj < NB; bj++, t++) {
+                    const int rr = 8 * bi + cj, cc = 8 * bj + 2 * kr;
+                    red[rr * W + cc] += acc[t][0];
+                    red[rr * W + cc + 1] += acc[t][1];
+                }
+            if (kr == 0)
+#pragma unroll
+                for (int b = 0; b < NB; b++) red[W * W + 8 * b + cj] += sq[b];
+        }
+        __syncthreads();
+    }
+    const int mm = s.msz * s.msz;
+    const int len = mm + (s.ssq ? s.k : 0);
+    for (int i = threadIdx.x; i < len; i += ST_TB)
+        part[size_t(blockIdx.x) * len + i] = i < mm ? red[(i / s.msz) * W + i % s.msz] : red[W * W + (i - mm)];
+}
+
+// Column statistics in one pass, about a shift c per column (the column's first value):
+// [sum (x-c), sum (x-c)^2, sum w (x-c), sum w (x-c)^2, sum x^2, sum w x^2] per column; the means
+// and the sums of squares about them follow exactly up to rounding (m2 = S2 - S1^2 / n).
+// Lane = (group, column) over a column chunk [j0, j0 + Rc) padded to RCP; rows U groups at a time.
+template <int RCP>
+__global__ void __launch_bounds__(ST_TB) k_colstats1(const double* __restrict__ rows, size_t n, int R, int j0, int Rc,
+                                                     const double* __restrict__ w, double* __restrict__ part) {
+    constexpr int G = 32 / RCP, U = 4, NV = 6;
+    __shared__ double red[ST_TB / 32][32][NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / RCP, j = lane % RCP;
+    const bool on = j < Rc;
+    const double c = on ? rows[j0 + j] : 0.0;
+    double a[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) a[v] = 0.0;
+    const size_t gw = size_t(blockIdx.x) * (ST_TB / 32) + warp, nw = size_t(gridDim.x) * (ST_TB / 32);
+    if (on)
+        for (size_t base = gw * U * G; base < n; base += nw * U * G) {
+            double x[U], wv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const size_t r = base + size_t(u) * G + g;
+                x[u] = r < n ? rows[r * R + j0 + j] : c;
+                wv[u] = r < n ? (w ? w[r] : 1.0) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (base + size_t(u) * G + g >= n) continue;
+                const double d = x[u] - c;
+                a[0] += d;
+                a[1] += d * d;
+                a[2] += wv[u] * d;
+                a[3] += wv[u] * d * d;
+                a[4] += x[u] * x[u];
+                a[5] += wv[u] * x[u] * x[u];
+            }
+        }
+#pragma unroll
+    for (int v = 0; v < NV; v++) red[warp][lane][v] = on ? a[v] : 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < Rc * NV; i += ST_TB) {
+        const int col = i / NV, v = i % NV;
+        double t = 0.0;
+        for (int wp = 0; wp < ST_TB / 32; wp++)
+            for (int gg = 0; gg < G; gg++) t += red[wp][gg * RCP + col][v];
+        part[(size_t(blockIdx.x) * R + j0 + col) * NV + v] = t;
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Residuals: e_i = y_i - sum_p beta[p] x_i[col[p]] (y = column 0, or 0 when y_zero); per-CTA
 // partials of sum om_i e_i^2.

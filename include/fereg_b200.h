@@ -115,7 +115,8 @@ int fereg_absorber_phase_times(const fereg_absorber* h, double* ms, uint64_t* co
 uint64_t fereg_absorber_launches(const fereg_absorber* h);
 
 /* Kernel-level entry points used by the parity tests (device work, host buffers). */
-int fereg_absorber_info(const fereg_absorber* h, uint64_t* out8); /* n, m, g1, ncells, nb, m_small, fe1, small_work */
+/* n, m, g1, ncells, nb, m_small, fe1, small_work, blocks in the small super-block (9 values) */
+int fereg_absorber_info(const fereg_absorber* h, uint64_t* out9);
 int fereg_absorber_apply(fereg_absorber* h, const double* p, size_t r, double* y);
 int fereg_absorber_rhs(fereg_absorber* h, const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum);
 int fereg_absorber_precond(fereg_absorber* h, const double* rr, size_t r, double* z);
@@ -172,9 +173,19 @@ int fereg_session_row_order(const fereg_session* s, uint32_t* out);
 
 /* Session::ols (ols.rs:199): OLS of column 0 on columns 1..nx of the n x (1 + nx) row-major
  * block `rows` in row order, host memory or (rows_on_device = 1) device memory of the current
- * device. The block is residualized in place. */
+ * device. A device block is residualized in place; a host block is copied to the device and left
+ * unchanged. */
 int fereg_session_ols(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_ols_spec* spec,
                       fereg_ols_out* out);
+
+/* Phase timing of the session's calls: the FEREG_PHASE_SLOTS slots of its absorber, then
+ * 9 degrees of freedom, 10 column statistics, 11 Gram, 12 residuals and variance. */
+#define FEREG_SESSION_PHASE_SLOTS (FEREG_PHASE_SLOTS + 4)
+int fereg_session_set_profiling(fereg_session* s, int on);
+int fereg_session_phase_times(const fereg_session* s, double* ms, uint64_t* counts);
+
+/* fereg_absorber_info of the session's absorber (9 values). */
+int fereg_session_info(const fereg_session* s, uint64_t* out9);
 
 /* Kernel launches of the session so far (its passes and its absorber), and its CUDA stream. */
 uint64_t fereg_session_launches(const fereg_session* s);

@@ -1387,82 +1387,61 @@ struct OrcOlsOut {
 
 static double nanv() { return std::nan(""); }
 
-int orc_ols(const OrcOlsSpec* sp, OrcOlsOut* out) {
-    if (sp->threads > 0) omp_set_num_threads(sp->threads);
-    size_t n0 = sp->n_input;
-    // factorize
-    std::vector<std::vector<u32>> fcodes(sp->nfactors);
-    std::vector<u32> fg(sp->nfactors);
-    for (int f = 0; f < sp->nfactors; f++) {
-        int rc = factorize_f64(sp->factors[f], n0, fcodes[f], fg[f]);
-        if (rc) return rc;
-    }
-    auto interact = [&](const int* fs, int nf, std::vector<u32>& out_, u32& g_) {
-        std::vector<const std::vector<u32>*> ptrs;
-        std::vector<u32> gs;
-        for (int i = 0; i < nf; i++) { ptrs.push_back(&fcodes[fs[i]]); gs.push_back(fg[fs[i]]); }
-        combine(ptrs, gs, out_, g_);
-    };
-    std::vector<std::vector<u32>> tcodes(sp->nterms);
-    std::vector<u32> tg(sp->nterms);
-    {
-        int o = 0;
-        for (int t = 0; t < sp->nterms; t++) { interact(sp->term_f + o, sp->term_nf[t], tcodes[t], tg[t]); o += sp->term_nf[t]; }
-    }
-    std::vector<std::vector<u32>> ccodes(sp->ncl);
-    std::vector<u32> cg(sp->ncl);
-    {
-        int o = 0;
-        for (int c = 0; c < sp->ncl; c++) { interact(sp->cl_f + o, sp->cl_nf[c], ccodes[c], cg[c]); o += sp->cl_nf[c]; }
-    }
-    // singletons
-    std::vector<uint8_t> alive(n0, 1);
-    const double* fw = sp->weight_kind == 2 ? sp->w : nullptr;
-    u64 nsing = sp->drop_singletons ? drop_singletons(tcodes, tg, fw, alive) : 0;
-    std::vector<u32> kept;
-    for (size_t i = 0; i < n0; i++) if (alive[i]) kept.push_back(u32(i));
-    size_t n = kept.size();
-    if (n < 2) { g_err = "insufficient observations"; return 2001; }
-    for (int t = 0; t < sp->nterms; t++) { std::vector<u32> c; u32 g; restrict_codes(tcodes[t], tg[t], kept, c, g); tcodes[t] = c; tg[t] = g; }
-    for (int c = 0; c < sp->ncl; c++) { std::vector<u32> cc; u32 g; restrict_codes(ccodes[c], cg[c], kept, cc, g); ccodes[c] = cc; cg[c] = g; }
-    std::vector<double> wk;
-    if (sp->w) { wk.resize(n); for (size_t i = 0; i < n; i++) wk[i] = sp->w[kept[i]]; }
-
-    // absorber
+// A prepared session: kept-order term and cluster codes, raw kept-order weights and their kind,
+// and the absorber built on the terms (session.rs).
+struct OrcSession {
     Absorber ab;
-    ab.st = build_structure(tcodes, tg, n, SMALL_LIMIT);
-    ab.norm_fe1 = fe1_index(tg);
-    refresh_weights(ab.st, ab.ws, sp->w ? wk.data() : nullptr);
-    const auto& pi = ab.st.pi;
+    std::vector<std::vector<u32>> tcodes, ccodes;
+    std::vector<u32> tg, cg;
+    std::vector<double> wk;
+    int kind = 0;
+    size_t n = 0;
+    u64 nsing = 0;
+};
 
-    // rows [y, x...] in row order
-    size_t nx = sp->nx, r = 1 + nx;
-    std::vector<double> rows(n * r);
-    for (size_t i = 0; i < n; i++) {
-        size_t o = kept[pi[i]];
-        rows[i * r] = sp->y[o];
-        for (size_t j = 0; j < nx; j++) rows[i * r + 1 + j] = sp->x[j][o];
-    }
+static void session_build(OrcSession& s) {
+    s.ab.st = build_structure(s.tcodes, s.tg, s.n, SMALL_LIMIT);
+    s.ab.norm_fe1 = fe1_index(s.tg);
+    refresh_weights(s.ab.st, s.ab.ws, s.wk.empty() ? nullptr : s.wk.data());
+}
+
+// The OLS call on a prepared session (ols.rs:263-470): rows (n x (1 + nx), row order) are
+// residualized in place; outputs in kept order.
+struct OlsArgs {
+    int vce, noconstant, firstpair;
+    double tol;
+    size_t maxiter;
+};
+
+static int session_ols(OrcSession& s, std::vector<double>& rows, size_t nx, const OlsArgs& a, OrcOlsOut* out) {
+    Absorber& ab = s.ab;
+    const size_t n = s.n, r = 1 + nx;
+    const auto& pi = ab.st.pi;
+    const auto& tcodes = s.tcodes;
+    const auto& tg = s.tg;
+    const auto& ccodes = s.ccodes;
+    const auto& cg = s.cg;
+    const u64 nsing = s.nsing;
     // weights (ols.rs:77-108)
-    int kind = sp->weight_kind;
+    int kind = s.kind;
     std::vector<double> raw, wv;
     double sumw = double(n);
-    if (sp->w) {
+    if (!s.wk.empty()) {
         raw.resize(n);
         sumw = 0;
-        for (size_t i = 0; i < n; i++) { raw[i] = wk[pi[i]]; sumw += raw[i]; }
+        for (size_t i = 0; i < n; i++) { raw[i] = s.wk[pi[i]]; sumw += raw[i]; }
         if (kind == 1 || kind == 3) { wv.resize(n); for (size_t i = 0; i < n; i++) wv[i] = raw[i] * double(n) / sumw; }
         else if (kind == 2) wv = raw;
     }
     double bigN = kind == 2 ? sumw : double(n);
     auto wvf = [&](size_t i) { return wv.empty() ? 1.0 : wv[i]; };
-    int vce = sp->vce;
+    int vce = a.vce;
     if (vce == 0 && kind == 3) vce = 1;  // ols.rs:150 pweight + unadjusted -> robust
     bool has_intercept = true;  // intercept-only absorb terms (or noabsorb) contain the constant
-    bool report_constant = has_intercept && !sp->noconstant;
+    bool report_constant = has_intercept && !a.noconstant;
 
     // dof (needs cluster codes in kept order)
-    Dof dof = estimate_dof(tcodes, tg, vce == 2 ? ccodes : std::vector<std::vector<u32>>{}, n, sp->firstpair != 0, out->groupvar != nullptr);
+    Dof dof = estimate_dof(tcodes, tg, vce == 2 ? ccodes : std::vector<std::vector<u32>>{}, n, a.firstpair != 0, out->groupvar != nullptr);
 
     ColStats cs = col_stats(rows.data(), n, r, raw.empty() ? nullptr : raw.data());
     Vec tss_all(r);
@@ -1475,12 +1454,12 @@ int orc_ols(const OrcOlsSpec* sp, OrcOlsOut* out) {
     std::vector<double> coefs((m + g1) * r);
     size_t iters = 0;
     int exact = 0;
-    int rc = ab.residualize(rows.data(), r, sp->tol, sp->maxiter, want_coefs, nullptr, coefs.data(), &iters, &exact);
+    int rc = ab.residualize(rows.data(), r, a.tol, a.maxiter, want_coefs, nullptr, coefs.data(), &iters, &exact);
     if (rc) return rc;
 
     Vec g, ss_res;
     gram(rows.data(), n, r, wv.empty() ? nullptr : wv.data(), g, ss_res);
-    double ctol = std::min(1e-6, sp->tol / 10.0);
+    double ctol = std::min(1e-6, a.tol / 10.0);
     std::vector<bool> absorbed(r);
     for (size_t j = 0; j < r; j++) absorbed[j] = ss_res[j] / cs.sumsq[j] <= ctol;
     std::vector<uint8_t> status(nx, 0);
@@ -1640,7 +1619,6 @@ int orc_ols(const OrcOlsSpec* sp, OrcOlsOut* out) {
     }
     out->k_all = int(k_all);
     std::copy(status.begin(), status.end(), out->status);
-    for (size_t i = 0; i < n0; i++) out->sample[i] = alive[i];
 
     double tss = tss_all[0], tss_within = g[0];
     double used_df_r = bigN - df_a - df_m - double(dof.df_a_nested);
@@ -1690,6 +1668,111 @@ int orc_ols(const OrcOlsSpec* sp, OrcOlsOut* out) {
         for (size_t i = 0; i < n; i++) out->groupvar[i] = dof.has_groupvar ? double(dof.groupvar[i]) : nanv();
     }
     return 0;
+}
+
+int orc_ols(const OrcOlsSpec* sp, OrcOlsOut* out) {
+    if (sp->threads > 0) omp_set_num_threads(sp->threads);
+    size_t n0 = sp->n_input;
+    // factorize
+    std::vector<std::vector<u32>> fcodes(sp->nfactors);
+    std::vector<u32> fg(sp->nfactors);
+    for (int f = 0; f < sp->nfactors; f++) {
+        int rc = factorize_f64(sp->factors[f], n0, fcodes[f], fg[f]);
+        if (rc) return rc;
+    }
+    auto interact = [&](const int* fs, int nf, std::vector<u32>& out_, u32& g_) {
+        std::vector<const std::vector<u32>*> ptrs;
+        std::vector<u32> gs;
+        for (int i = 0; i < nf; i++) { ptrs.push_back(&fcodes[fs[i]]); gs.push_back(fg[fs[i]]); }
+        combine(ptrs, gs, out_, g_);
+    };
+    std::vector<std::vector<u32>> tcodes(sp->nterms);
+    std::vector<u32> tg(sp->nterms);
+    {
+        int o = 0;
+        for (int t = 0; t < sp->nterms; t++) { interact(sp->term_f + o, sp->term_nf[t], tcodes[t], tg[t]); o += sp->term_nf[t]; }
+    }
+    std::vector<std::vector<u32>> ccodes(sp->ncl);
+    std::vector<u32> cg(sp->ncl);
+    {
+        int o = 0;
+        for (int c = 0; c < sp->ncl; c++) { interact(sp->cl_f + o, sp->cl_nf[c], ccodes[c], cg[c]); o += sp->cl_nf[c]; }
+    }
+    // singletons
+    std::vector<uint8_t> alive(n0, 1);
+    const double* fw = sp->weight_kind == 2 ? sp->w : nullptr;
+    u64 nsing = sp->drop_singletons ? drop_singletons(tcodes, tg, fw, alive) : 0;
+    std::vector<u32> kept;
+    for (size_t i = 0; i < n0; i++) if (alive[i]) kept.push_back(u32(i));
+    size_t n = kept.size();
+    if (n < 2) { g_err = "insufficient observations"; return 2001; }
+    for (int t = 0; t < sp->nterms; t++) { std::vector<u32> c; u32 g; restrict_codes(tcodes[t], tg[t], kept, c, g); tcodes[t] = c; tg[t] = g; }
+    for (int c = 0; c < sp->ncl; c++) { std::vector<u32> cc; u32 g; restrict_codes(ccodes[c], cg[c], kept, cc, g); ccodes[c] = cc; cg[c] = g; }
+    std::vector<double> wk;
+    if (sp->w) { wk.resize(n); for (size_t i = 0; i < n; i++) wk[i] = sp->w[kept[i]]; }
+
+    OrcSession sess;
+    sess.tcodes = tcodes;
+    sess.tg = tg;
+    sess.ccodes = ccodes;
+    sess.cg = cg;
+    sess.n = n;
+    sess.nsing = nsing;
+    sess.kind = sp->w ? sp->weight_kind : 0;
+    sess.wk = wk;
+    session_build(sess);
+    const auto& pi = sess.ab.st.pi;
+
+    // rows [y, x...] in row order
+    size_t nx = sp->nx, r = 1 + nx;
+    std::vector<double> rows(n * r);
+    for (size_t i = 0; i < n; i++) {
+        size_t o = kept[pi[i]];
+        rows[i * r] = sp->y[o];
+        for (size_t j = 0; j < nx; j++) rows[i * r + 1 + j] = sp->x[j][o];
+    }
+    int rc = session_ols(sess, rows, nx, OlsArgs{sp->vce, sp->noconstant, sp->firstpair, sp->tol, sp->maxiter}, out);
+    if (rc) return rc;
+    for (size_t i = 0; i < n0; i++) out->sample[i] = alive[i];
+    return 0;
+}
+
+// Session entry points (the bench's CPU arm): a prepared session reused across OLS calls.
+int orc_session_create(const uint32_t* const* codes, const uint32_t* g, int nterms, const uint32_t* const* cl,
+                       const uint32_t* cl_g, int ncl, const double* w, int kind, size_t n, uint64_t nsing,
+                       void** out) {
+    auto* s = new OrcSession();
+    for (int q = 0; q < nterms; q++) {
+        s->tcodes.emplace_back(codes[q], codes[q] + n);
+        s->tg.push_back(g[q]);
+    }
+    for (int c = 0; c < ncl; c++) {
+        s->ccodes.emplace_back(cl[c], cl[c] + n);
+        s->cg.push_back(cl_g[c]);
+    }
+    if (w) s->wk.assign(w, w + n);
+    s->kind = w ? kind : 0;
+    s->n = n;
+    s->nsing = nsing;
+    session_build(*s);
+    *out = s;
+    return 0;
+}
+
+void orc_session_destroy(void* s) { delete static_cast<OrcSession*>(s); }
+
+void orc_session_row_order(const void* s, uint32_t* out) {
+    const auto& pi = static_cast<const OrcSession*>(s)->ab.st.pi;
+    std::copy(pi.begin(), pi.end(), out);
+}
+
+int orc_session_ols(void* s, double* rows, size_t nx, int vce, int noconstant, int firstpair, double tol,
+                    size_t maxiter, OrcOlsOut* out) {
+    auto* ss = static_cast<OrcSession*>(s);
+    std::vector<double> v(rows, rows + ss->n * (1 + nx));
+    int rc = session_ols(*ss, v, nx, OlsArgs{vce, noconstant, firstpair, tol, maxiter}, out);
+    std::copy(v.begin(), v.end(), rows);
+    return rc;
 }
 
 }  // extern "C"

@@ -106,6 +106,12 @@ def _setup(L):
     L.orc_absorber_fit_rows.argtypes = [P, f64p, C.c_size_t, C.c_size_t, f64p]
     L.orc_absorber_term_values.argtypes = [P, f64p, C.c_size_t, C.c_size_t, u32p, C.c_int, f64p]
     L.orc_ols.argtypes = [C.POINTER(OlsSpec), C.POINTER(OlsOut)]
+    L.orc_session_create.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.POINTER(u32p), u32p, C.c_int, f64p, C.c_int,
+                                     C.c_size_t, C.c_uint64, C.POINTER(P)]
+    L.orc_session_destroy.argtypes = [P]
+    L.orc_session_row_order.argtypes = [P, u32p]
+    L.orc_session_ols.argtypes = [P, f64p, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_double, C.c_size_t,
+                                  C.POINTER(OlsOut)]
     L.orc_factorize_f64.argtypes = [f64p, C.c_size_t, u32p, u32p]
     L.orc_drop_singletons.restype = C.c_uint64
     L.orc_drop_singletons.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, f64p, u8p]
@@ -318,3 +324,54 @@ def ols(factors, absorb, y, x, clusters=(), weights=None, weight_kind=None, vce=
     if want_groupvar:
         res["groupvar"] = gv[:nk]
     return res
+
+
+class Session:
+    """A prepared oracle session (kept-order codes) reused across OLS calls: the CPU arm of the
+    benchmark's OLS call."""
+
+    def __init__(self, codes, g, clusters=(), cl_g=(), w=None, weight_kind=None, num_singletons=0):
+        n = len(codes[0]) if len(codes) else len(clusters[0])
+        self._c = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
+        self._k = [np.ascontiguousarray(c, dtype=np.uint32) for c in clusters]
+        garr = np.asarray(g, dtype=np.uint32)
+        cgarr = np.asarray(cl_g, dtype=np.uint32)
+        cp = (u32p * max(1, len(self._c)))(*[_p(c, u32p) for c in self._c])
+        kp = (u32p * max(1, len(self._k)))(*[_p(c, u32p) for c in self._k])
+        wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        h = P()
+        lib().orc_session_create(cp, _p(garr, u32p), len(self._c), kp, _p(cgarr, u32p), len(self._k), _p(wa, f64p),
+                                 WEIGHT_KINDS[weight_kind if w is not None else None], n, int(num_singletons),
+                                 C.byref(h))
+        self.h = h
+        self.n = n
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().orc_session_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def row_order(self):
+        out = np.empty(self.n, dtype=np.uint32)
+        lib().orc_session_row_order(self.h, _p(out, u32p))
+        return out
+
+    def ols(self, rows, vce="unadjusted", noconstant=False, firstpair=False, tol=1e-8, maxiter=16000):
+        """OLS of column 0 on the other columns of the n x r row-order block (residualized in place)."""
+        assert rows.dtype == np.float64 and rows.flags.c_contiguous
+        nx = rows.shape[1] - 1
+        k_all = nx + 1
+        b = np.zeros(k_all)
+        V = np.zeros(k_all * k_all)
+        status = np.zeros(max(1, nx), dtype=np.uint8)
+        dof_table = np.zeros(5 * 64)
+        out = OlsOut(_p(b, f64p), _p(V, f64p), _p(status, u8p), None, None, None, None, _p(dof_table, f64p))
+        rc = lib().orc_session_ols(self.h, _p(rows, f64p), nx, {"unadjusted": 0, "robust": 1, "cluster": 2}[vce],
+                                   int(noconstant), int(firstpair), tol, maxiter, C.byref(out))
+        if rc:
+            raise RuntimeError(f"rc={rc}: {lib().orc_last_error().decode()}")
+        ka = out.k_all
+        return dict(b=b[:ka], V=V[: ka * ka].reshape(ka, ka), status=status[:nx].copy(),
+                    scalars={s: getattr(out, s) for s in SCALARS})
