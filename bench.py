@@ -180,15 +180,15 @@ def phase_bytes(info, n, R, weighted, s_v=8):
         "apply_seg": M * nb * 4 + wcell + g1 * 8 + g1 * 4 + g1 * R * s_v + m * R * s_v,
         "apply_pull": E * nb * 4 + g1 * R * s_v + 2 * m * R * s_v + m * 12,
         "residualize": 2 * n * R * 8 + M * nb * 4 + g1 * R * 8 + g1 * 8 + g1 * 4 + m * R * 8,
-        "colstats": 2 * (n * R * 8 + wrow),
+        "colstats": n * R * 8 + wrow,
         "gram": n * R * 8 + wrow,
         "variance": n * R * 8 + n * 8 + wrow,
     }
 
 
 PHASE_KERNEL = {"rhs_seg": "k_wseg_rhs", "rhs_pull": "k_wpull_rhs", "apply_seg": "k_wseg_apply",
-                "apply_pull": "k_wpull_apply", "residualize": "k_wresid", "colstats": "k_colstats",
-                "gram": "k_outer", "variance": "k_resid_e"}
+                "apply_pull": "k_wpull_apply", "residualize": "k_wresid", "colstats": "k_colstats1",
+                "gram": "k_outer_mma", "variance": "k_resid_e"}
 
 
 def dist_setup():
