@@ -40,6 +40,9 @@ CONFIGS = {
     "c2": dict(n_ind=1_000_000, years=10, n_firm=100_000, k=10, seed=10**7 * 100 + 43),
     # OLS y ~ x1 | indiv + year, n = 1e4 indiv x 10 years.
     "c1": dict(n_ind=10_000, years=10, n_firm=0, k=1, seed=10**5 * 100 + 42),
+    # WCR11 wild cluster bootstrap of b_x1 (H0 true): y ~ x1 | indiv + year + firm, cluster firm,
+    # n = 1e5 indiv x 10 years, firm random in 2e4, 9,999 Rademacher draws (seed 1).
+    "c3": dict(n_ind=100_000, years=10, n_firm=20_000, k=1, seed=10**6 * 100 + 44, reps=9_999),
 }
 TOL = 1e-8
 METRIC = "sec/call (1e7-obs 3-FE OLS)"
@@ -77,6 +80,122 @@ def make_data(cfg):
     g.append(years)
     rows[:, 0] = y
     return codes, g, rows
+
+
+def make_boot_data(cfg):
+    """Synthetic C3 panel: firms drawn at random (seeded), y = 0 x1 + effects + noise."""
+    n_ind, years, n_firm = cfg["n_ind"], cfg["years"], cfg["n_firm"]
+    n = n_ind * years
+    rng = np.random.default_rng(cfg["seed"])
+    i = np.arange(n)
+    ind = (i // years).astype(np.uint32)
+    year = (i % years).astype(np.uint32)
+    firm = rng.integers(0, n_firm, n).astype(np.uint32)
+    _, firm = np.unique(firm, return_inverse=True)
+    firm = firm.astype(np.uint32)
+    x1 = rng.standard_normal(n)
+    y = rng.standard_normal(n_ind)[ind] + rng.normal(0.0, np.sqrt(0.5), years)[year] + \
+        rng.standard_normal(n_firm)[firm] + rng.standard_normal(n)
+    rows = np.column_stack([y, x1])
+    return [ind, year, firm], [n_ind, years, int(firm.max()) + 1], firm, rows
+
+
+BOOT_METRIC = "wild-boot reps/s (WCR11, 9,999 Rademacher draws, n=1e6, 3 FE, cluster firm 2e4)"
+
+
+def run_boot(args, cfg, rank, world, local, pg):
+    """C3: one WCR11 bootstrap call per step; value = draws per second of the whole job."""
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import oracle
+
+        codes, g, firm, rows = make_boot_data(cfg)
+        ab = oracle.Absorber(codes, g)
+        rng = np.random.default_rng(1)
+        nd = 16
+        z = np.ascontiguousarray(rows[ab.row_order(), :1] * rng.choice([-1.0, 1.0], size=(rows.shape[0], nd)))
+        times = []
+        for it in range(max(1, args.warmup // 3) + max(1, args.steps // 3)):
+            zz = z.copy()
+            t0 = time.perf_counter()
+            ab.residualize(zz, tol=TOL)
+            times.append(time.perf_counter() - t0)
+        v = nd / float(np.mean(times[1:] if len(times) > 1 else times))
+        line = {"impl": "reference", "metric": BOOT_METRIC, "value": v, "unit": "reps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "c3", "n": rows.shape[0], "reps": cfg["reps"]},
+                "cpu_baseline": {"value": v, "unit": "reps/s", "cores": oracle.max_threads(), "kind": "port",
+                                 "sample": f"the FE solve of {nd} draw columns per step (the per-draw refit's "
+                                           "dominant cost), C++ FP64 restatement, all host threads"},
+                "e2e": {"value": v, "unit": "reps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+
+    import fereg_b200 as fb
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    codes, g, firm, rows = make_boot_data(cfg)
+    n = rows.shape[0]
+    t0 = time.perf_counter()
+    sess = fb.Session(codes, g, [firm], [g[2]])
+    prepare_s = time.perf_counter() - t0
+    rows = np.ascontiguousarray(rows[sess.row_order()])
+    prec = fb.PREC_F64 if args.precision == "f64" else fb.PREC_F32_REFINED
+    stream = torch.cuda.ExternalStream(sess.stream(), device=device)
+    src = torch.from_numpy(rows).to(device)
+    work = torch.empty_like(src)
+    reps = cfg["reps"]
+
+    def step(on_device):
+        if on_device:
+            work.copy_(src)
+            torch.cuda.synchronize(device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = sess.wildboot(work.data_ptr() if on_device else rows, coef=0, reps=reps, seed=1, tile=args.boot_tile,
+                            tol=TOL, boot_precision=prec, on_device=on_device, nx=1)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, res
+
+    for _ in range(args.warmup):
+        step(True)
+    barrier(pg)
+    sess.set_profiling(True)
+    l0 = sess.launches()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            dt, res = step(True)
+            times.append(dt)
+    launches = sess.launches() - l0
+    phases = sess.phase_times()
+    sess.set_profiling(False)
+    step_s = max_over_ranks(float(np.mean(times)), pg, device)
+    e2e = None
+    if not args.no_e2e:
+        et = [step(False)[0] for _ in range(2)]
+        e2e = world * reps / max_over_ranks(float(np.mean(et)), pg, device)
+    if rank == 0:
+        line = {"metric": BOOT_METRIC, "value": world * reps / step_s, "unit": "reps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == fb.PREC_F64 else "f32+f64",
+                "data": "synthetic",
+                "config": {"workload": "c3", "n": n, "reps": int(res["reps"]), "tile": args.boot_tile,
+                           "precision": args.precision, "prepare_s": prepare_s, "stat": res["stat"],
+                           "pvalue": res["pvalue"], "parallelism": f"replicas x{world}"},
+                "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
+                "clocks": clk.summary(),
+                "e2e": {"value": e2e, "unit": "reps/s", "h2d_bytes_per_step": n * 2 * 8,
+                        "d2h_bytes_per_step": int(res["reps"]) * 8 + 64},
+                "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    sess.close()
 
 
 def workload_name(cfg_name):
@@ -271,10 +390,17 @@ def main():
     ap.add_argument("--precision", default="f64", choices=["f64", "f32r"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing (profiling runs)")
+    ap.add_argument("--boot-tile", type=int, default=512, help="draws per block-PCG tile (c3)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     cfg = CONFIGS[args.config]
     rank, world, local, pg = dist_setup()
+    if args.config == "c3":
+        run_boot(args, cfg, rank, world, local, pg)
+        if pg is not None:
+            barrier(pg)
+            pg.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, args.config, cfg, rank, world)
         if pg is not None:

@@ -52,6 +52,16 @@ class OlsSpec(C.Structure):
                 ("tol", C.c_double), ("maxiter", C.c_size_t), ("precision", C.c_int)]
 
 
+class BootSpec(C.Structure):
+    _fields_ = [("coef", C.c_size_t), ("r0", C.c_double), ("reps", C.c_size_t), ("seed", C.c_uint64),
+                ("tile", C.c_size_t), ("tol", C.c_double), ("maxiter", C.c_size_t), ("precision", C.c_int)]
+
+
+class BootOut(C.Structure):
+    _fields_ = [("stat", C.c_double), ("se", C.c_double), ("point", C.c_double), ("pvalue", C.c_double),
+                ("reps", C.c_uint64), ("full_enum", C.c_int32), ("t_boot", C.POINTER(C.c_double))]
+
+
 class OlsOut(C.Structure):
     _fields_ = ([("b", C.POINTER(C.c_double)), ("V", C.POINTER(C.c_double)), ("status", C.POINTER(C.c_uint8)),
                  ("resid", C.POINTER(C.c_double)), ("d", C.POINTER(C.c_double)),
@@ -104,6 +114,8 @@ def _setup(L):
     L.fereg_session_stream.restype = P
     L.fereg_session_set_profiling.argtypes = [P, C.c_int]
     L.fereg_session_info.argtypes = [P, u64p]
+    L.fereg_session_wildboot.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(OlsSpec), C.POINTER(BootSpec),
+                                         C.POINTER(BootOut)]
     L.fereg_session_phase_times.argtypes = [P, f64p, u64p]
     L.fereg_absorber_stream.argtypes = [P]
     L.fereg_absorber_stream.restype = P
@@ -359,3 +371,26 @@ class Session:
         """As ols() on an n x (1 + nx) block in device memory (pointer)."""
         return self._call(ptr, 1, nx, vce, noconstant, firstpair, want_groupvar, want_resid, want_d, tol, maxiter,
                           precision)
+
+    def wildboot(self, rows, coef=0, r0=0.0, reps=999, seed=1, tile=256, tol=1e-8, maxiter=16000,
+                 precision=PREC_F64, boot_tol=None, boot_precision=None, noconstant=False, firstpair=False,
+                 on_device=False, nx=None):
+        """WCR11 wild cluster bootstrap of regressor `coef` (H0: b[coef] = r0) on the n x (1 + nx)
+        block (row order; host array, or a device pointer with on_device=True). Returns stat, se,
+        point, pvalue, reps, full_enum and the draws' t statistics."""
+        if on_device:
+            ptr = rows
+            assert nx is not None
+        else:
+            assert rows.dtype == np.float64 and rows.flags.c_contiguous
+            ptr = rows.ctypes.data
+            nx = rows.shape[1] - 1
+        spec = OlsSpec(2, int(noconstant), int(firstpair), 0, tol, maxiter, precision)
+        bs = BootSpec(coef, r0, reps, seed, tile, tol if boot_tol is None else boot_tol, maxiter,
+                      precision if boot_precision is None else boot_precision)
+        t = np.full(reps, np.nan)
+        out = BootOut(0, 0, 0, 0, 0, 0, _p(t, f64p))
+        _check(lib().fereg_session_wildboot(self.h, P(ptr), int(on_device), nx, C.byref(spec), C.byref(bs),
+                                            C.byref(out)))
+        return dict(stat=out.stat, se=out.se, point=out.point, pvalue=out.pvalue, reps=int(out.reps),
+                    full_enum=bool(out.full_enum), t_boot=t[: int(out.reps)].copy())

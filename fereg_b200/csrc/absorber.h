@@ -78,6 +78,7 @@ class GpuAbsorber {
     void phase_times(double* ms, u64* counts) const;
     u64 launches() const;
     void set_ctx(const Ctx& c) { ctx_ = c; }
+    const Ctx& ctx() const { return ctx_; }
 
     // Kernel-level entry points for the parity tests (device work, host buffers).
     void apply_host(const double* p, size_t r, double* y);

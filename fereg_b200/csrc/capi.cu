@@ -337,6 +337,42 @@ int fereg_session_ols(fereg_session* s, double* rows, int rows_on_device, size_t
     });
 }
 
+int fereg_session_wildboot(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_ols_spec* spec,
+                           const fereg_boot_spec* boot, fereg_boot_out* out) {
+    return guard([&] {
+        if (!s || !rows || !spec || !boot || !out) throw Error(RC_INVALID_INPUT, "fereg_session_wildboot: NULL argument");
+        if (spec->precision != FEREG_PREC_F64 && spec->precision != FEREG_PREC_F32_REFINED)
+            throw Error(RC_INVALID_INPUT, "fereg_session_wildboot: unknown precision");
+        if (boot->precision != FEREG_PREC_F64 && boot->precision != FEREG_PREC_F32_REFINED)
+            throw Error(RC_INVALID_INPUT, "fereg_session_wildboot: unknown bootstrap precision");
+        OlsSpec sp;
+        sp.vce = 2;
+        sp.noconstant = spec->noconstant;
+        sp.firstpair = spec->firstpair;
+        sp.tol = spec->tol;
+        sp.maxiter = spec->maxiter;
+        sp.prec = spec->precision == FEREG_PREC_F32_REFINED ? Precision::F32_REFINED : Precision::F64;
+        GpuSession::BootSpec bs;
+        bs.coef = boot->coef;
+        bs.r0 = boot->r0;
+        bs.reps = boot->reps;
+        bs.seed = boot->seed;
+        bs.tile = boot->tile;
+        bs.tol = boot->tol;
+        bs.maxiter = boot->maxiter;
+        bs.prec = boot->precision == FEREG_PREC_F32_REFINED ? Precision::F32_REFINED : Precision::F64;
+        GpuSession::BootOut bo;
+        bo.t_boot = out->t_boot;
+        s->s.wildboot(rows, rows_on_device != 0, nx, sp, bs, bo);
+        out->stat = bo.stat;
+        out->se = bo.se;
+        out->point = bo.point;
+        out->pvalue = bo.pvalue;
+        out->reps = bo.reps;
+        out->full_enum = bo.full_enum ? 1 : 0;
+    });
+}
+
 int fereg_session_set_profiling(fereg_session* s, int on) {
     return guard([&] {
         if (!s) throw Error(RC_INVALID_INPUT, "fereg_session_set_profiling: NULL handle");

@@ -17,6 +17,8 @@
 
 #include "linalg.h"
 #include "session.h"
+#include "boot.cuh"
+#include "session_dev.h"
 #include "stats.cuh"
 
 namespace fereg {
@@ -53,77 +55,6 @@ void combine_codes(const std::vector<const std::vector<u32>*>& dims, const std::
 }
 
 }  // namespace
-
-// Device state of a session.
-struct SessionDev {
-    std::vector<DBuf<u32>> tcodes, ccodes;  // kept order
-    struct Subset {
-        DBuf<int> perm;  // rows (row order) grouped by cluster, stable
-        DBuf<u32> coff;  // G + 1
-        u32 G = 0;
-        double sign = 1.0;
-    };
-    std::vector<Subset> subsets;
-    DBuf<double> w_raw, wv;  // row order
-    DBuf<double> rows, part, sums, e, om, S, shift, beta;
-    DBuf<int> col, err;
-    DBuf<u32> uf, flags, scan, bsum, total, gv, map;
-    DBuf<double> pstat;
-    cudaStream_t st = nullptr;
-    u64 launches = 0;
-    // phase timing (CUDA events on the session's stream)
-    bool prof = false;
-    double ms[GpuSession::S_NSLOTS] = {};
-    u64 cnt[GpuSession::S_NSLOTS] = {};
-    std::vector<cudaEvent_t> pool;
-    struct Open {
-        int slot;
-        cudaEvent_t a, b;
-    };
-    std::vector<Open> open;
-    cudaEvent_t event() {
-        if (!pool.empty()) {
-            cudaEvent_t e = pool.back();
-            pool.pop_back();
-            return e;
-        }
-        cudaEvent_t e;
-        CK(cudaEventCreate(&e));
-        return e;
-    }
-    int begin(int slot) {
-        if (!prof) return -1;
-        open.push_back(Open{slot, event(), nullptr});
-        CK(cudaEventRecord(open.back().a, st));
-        return int(open.size()) - 1;
-    }
-    void end(int h) {
-        if (h < 0) return;
-        open[size_t(h)].b = event();
-        CK(cudaEventRecord(open[size_t(h)].b, st));
-    }
-    void collect() {
-        for (auto& o : open) {
-            if (o.b) {
-                CK(cudaEventSynchronize(o.b));
-                float t = 0;
-                CK(cudaEventElapsedTime(&t, o.a, o.b));
-                ms[o.slot] += t;
-                cnt[o.slot]++;
-                pool.push_back(o.b);
-            }
-            pool.push_back(o.a);
-        }
-        open.clear();
-    }
-    ~SessionDev() {
-        for (auto& o : open) {
-            cudaEventDestroy(o.a);
-            if (o.b) cudaEventDestroy(o.b);
-        }
-        for (auto e : pool) cudaEventDestroy(e);
-    }
-};
 
 GpuSession::GpuSession(const std::vector<const u32*>& codes, const std::vector<u32>& g,
                        const std::vector<const u32*>& cl_codes, const std::vector<u32>& cl_g, const double* w,
@@ -526,6 +457,16 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     for (size_t a = 0; a < k; a++)
         for (size_t b = 0; b < k; b++) b_s[a] += inv_s[a * k + b] * (g[kept[b] * r] / (sd[kept[b]] * sd_y));
     for (size_t a = 0; a < k; a++) beta[a] = b_s[a] * sd_y / sd[kept[a]];
+    // the fitted state the wild bootstrap starts from: kept columns, raw (X~'W X~)^-1, beta
+    fit_ = FitState{};
+    fit_.kept = kept;
+    fit_.beta = beta;
+    fit_.A.assign(k * k, 0.0);
+    for (size_t a = 0; a < k; a++)
+        for (size_t b = 0; b < k; b++) fit_.A[a * k + b] = inv_s[a * k + b] / (sd[kept[a]] * sd[kept[b]]);
+    fit_.rows = rows;
+    fit_.R = r;
+    fit_.y_absorbed = y_abs;
 
     // residuals and their weighted sum of squares
     ph = d.begin(S_VARIANCE);
@@ -609,6 +550,8 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
             standardize(meat);
             const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
             const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
+            fit_.crv1_scale = q_cluster;
+            fit_.ok = true;
             v_s = la::sandwich(bread, meat, msz, q_cluster);
             if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
         }
@@ -732,4 +675,168 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     CK(cudaGetLastError());
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Wild cluster bootstrap WCR11 of coefficient bs.coef (H0: beta = r0): Rademacher weights on
+// the clusters of the session's first cluster dimension, restricted residuals (impose_null),
+// CRV1 over all the session's cluster dimensions, two-tailed p-value
+// (wildboot/ols.rs:243-650, weights.rs:39-160, mod.rs:529 compute_pvalue). Each tile of draws is
+// one n x tile block residualized by the absorber as block-PCG columns; see boot.cuh.
+void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec& ospec, const BootSpec& bs,
+                          BootOut& out) {
+    if (ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg wildboot: the session has no cluster dimension");
+    if (bs.coef >= nx) throw Error(RC_INVALID_INPUT, "fereg wildboot: coefficient index out of range");
+    if (bs.reps == 0 || bs.tile == 0) throw Error(RC_INVALID_INPUT, "fereg wildboot: reps and tile must be positive");
+    if (d_->subsets.size() > size_t(BOOT_MAX_SUB)) throw Error(RC_INVALID_INPUT, "fereg wildboot: at most 3 cluster dimensions");
+    OlsSpec os = ospec;
+    os.vce = 2;
+    const size_t k_all = nx + 1;
+    std::vector<double> b(k_all), V(k_all * k_all);
+    OlsOut oo;
+    oo.b = b.data();
+    oo.V = V.data();
+    ols(rows, on_device, nx, os, oo);
+    if (!fit_.ok) throw Error(RC_INTERNAL, "fereg wildboot: no cluster variance");
+    SessionDev& d = *d_;
+    cudaStream_t st = d.st;
+    const size_t n = n_, k = fit_.kept.size();
+    const int R = int(fit_.R);
+    size_t pj = k;
+    for (size_t a = 0; a < k; a++)
+        if (fit_.kept[a] == bs.coef + 1) pj = a;
+    if (pj == k) throw Error(RC_INVALID_INPUT, "fereg wildboot: the tested coefficient was dropped (collinear or absorbed)");
+    const std::vector<double>& A = fit_.A;
+    const std::vector<double>& beta = fit_.beta;
+    // restricted coefficients (q = 1): beta_r = beta - A e_j (beta_j - r0) / A_jj
+    std::vector<double> beta_r(k), ca(k);
+    const double lam = (beta[pj] - bs.r0) / A[pj * k + pj];
+    for (size_t a = 0; a < k; a++) {
+        beta_r[a] = beta[a] - A[a * k + pj] * lam;
+        ca[a] = -A[pj * k + a];  // k_resid_e on a zero y gives c = a' x~
+    }
+    const double* wv = wk_.empty() ? nullptr : d.wv.p;
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+    std::vector<int> kcols(fit_.kept.begin(), fit_.kept.end());
+    DBuf<int> col;
+    DBuf<double> bvec, er, cvec, cw, om, Phi, part;
+    col.upload(kcols, st);
+    bvec.upload(beta_r, st);
+    er.alloc(n);
+    cvec.alloc(n);
+    cw.alloc(n);
+    om.alloc(n);
+    part.alloc(ST_GRID);
+    k_resid_e<<<ST_GRID, ST_TB, 0, st>>>(fit_.rows, n, R, col.p, bvec.p, int(k), fit_.y_absorbed ? 1 : 0, nullptr, er.p,
+                                         part.p);
+    bvec.upload(ca, st);
+    k_resid_e<<<ST_GRID, ST_TB, 0, st>>>(fit_.rows, n, R, col.p, bvec.p, int(k), 1, nullptr, cvec.p, part.p);
+    k_mul<<<blocks, 256, 0, st>>>(cvec.p, wv, n, cw.p);      // w c
+    k_mul<<<blocks, 256, 0, st>>>(er.p, wv, n, om.p);        // w e_r
+    d.launches += 4;
+    // phi_g over the bootstrap clusters (first dimension), psi_{s,g} and the original statistic's
+    // cluster sums over every subset
+    const auto& s0 = d.subsets[0];
+    Phi.alloc(size_t(s0.G) * k + 1);
+    k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(fit_.rows, R, col.p, nullptr, int(k), 0, om.p, s0.perm.p, s0.coff.p,
+                                               s0.G, Phi.p);
+    DBuf<double> ucw;
+    ucw.alloc(n);
+    k_mul<<<blocks, 256, 0, st>>>(cw.p, d.e.p, n, ucw.p);   // w c e_u
+    std::vector<DBuf<double>> Psi(d.subsets.size()), T1(d.subsets.size()), Tu(d.subsets.size());
+    double v_orig = 0.0;
+    for (size_t si = 0; si < d.subsets.size(); si++) {
+        const auto& sub = d.subsets[si];
+        Psi[si].alloc(size_t(sub.G) * k + 1);
+        k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(fit_.rows, R, col.p, nullptr, int(k), 0, cw.p, sub.perm.p,
+                                                   sub.coff.p, sub.G, Psi[si].p);
+        Tu[si].alloc(sub.G);
+        k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(fit_.rows, R, col.p, nullptr, 0, 1, ucw.p, sub.perm.p, sub.coff.p,
+                                                   sub.G, Tu[si].p);
+        d.launches += 2;
+        std::vector<double> h(sub.G);
+        CK(cudaMemcpyAsync(h.data(), Tu[si].p, size_t(sub.G) * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double acc = 0.0;
+        for (double x : h) acc += x * x;
+        v_orig += sub.sign * acc;
+    }
+    d.launches += 3;
+    v_orig *= fit_.crv1_scale;
+    out.point = beta[pj];
+    out.se = v_orig > 0.0 ? std::sqrt(v_orig) : nanv();
+    out.stat = v_orig > 0.0 ? (beta[pj] - bs.r0) / out.se : nanv();
+
+    // draws (weights.rs:39-63 resolve_reps): full enumeration of the 2^G sign patterns when
+    // G <= 20 and 2^G <= reps
+    const u32 G0 = s0.G;
+    const bool full = G0 <= 20 && (size_t(1) << G0) <= bs.reps;
+    const size_t reps = full ? (size_t(1) << G0) : bs.reps;
+    out.reps = reps;
+    out.full_enum = full;
+    const u32 nwords = (G0 + 63) / 64;
+    const std::vector<u32>& pi = ab_->row_order();
+    std::vector<u32> bcode(n);
+    for (size_t i = 0; i < n; i++) bcode[i] = ccodes_[0][pi[i]];
+    DBuf<u32> bcode_d;
+    bcode_d.upload(bcode, st);
+    DBuf<double> Adev, U, D, Z, tb;
+    Adev.upload(A, st);
+    const size_t tile = std::min(bs.tile, reps);
+    DBuf<u64> Wd;
+    Wd.alloc(tile * nwords);
+    U.alloc(tile * k + 1);
+    D.alloc(tile * k + 1);
+    Z.alloc(n * tile);
+    tb.alloc(tile);
+    for (size_t si = 0; si < d.subsets.size(); si++) T1[si].alloc(size_t(d.subsets[si].G) * tile);
+    std::vector<double> t_host(reps);
+    for (size_t b0 = 0; b0 < reps; b0 += tile) {
+        ab_->ctx().check();
+        const u32 bt = u32(std::min(tile, reps - b0));
+        k_boot_words<<<std::max(1, int((size_t(bt) * nwords + 255) / 256)), 256, 0, st>>>(bs.seed, b0, bt, nwords,
+                                                                                         full ? 1 : 0, Wd.p);
+        k_boot_gen<<<int(std::min<size_t>((n * bt + 255) / 256, 148 * 32)), 256, 0, st>>>(n, bt, er.p, bcode_d.p, Wd.p,
+                                                                                          nwords, Z.p);
+        d.launches += 2;
+        ab_->residualize_device(Z.p, bt, bs.tol, bs.maxiter, false, nullptr, nullptr, bs.prec);
+        if (k) {
+            k_boot_u<<<std::max(1, int((size_t(bt) * k + 127) / 128)), 128, 0, st>>>(bt, G0, int(k), Wd.p, nwords, Phi.p,
+                                                                                    U.p);
+            k_boot_delta<<<std::max(1, int((size_t(bt) * k + 127) / 128)), 128, 0, st>>>(bt, int(k), Adev.p, U.p, D.p);
+            d.launches += 2;
+        }
+        BootSubsets subs{};
+        subs.n = int(d.subsets.size());
+        for (size_t si = 0; si < d.subsets.size(); si++) {
+            const auto& sub = d.subsets[si];
+            const size_t warps = size_t(sub.G) * ((bt + 31) / 32);
+            k_boot_t1<<<int(std::min<size_t>((warps * 32 + 255) / 256, 148 * 32)), 256, 0, st>>>(Z.p, bt, cw.p, sub.perm.p,
+                                                                                               sub.coff.p, sub.G, T1[si].p);
+            d.launches++;
+            subs.T1[si] = T1[si].p;
+            subs.Psi[si] = Psi[si].p;
+            subs.G[si] = sub.G;
+            subs.sign[si] = sub.sign;
+        }
+        k_boot_var<<<int(std::min<u32>(bt, 148 * 8)), BOOT_TB, 0, st>>>(bt, subs, D.p, int(k), int(pj), fit_.crv1_scale,
+                                                                      tb.p);
+        d.launches++;
+        CK(cudaMemcpyAsync(t_host.data() + b0, tb.p, size_t(bt) * 8, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    if (out.t_boot) std::copy(t_host.begin(), t_host.end(), out.t_boot);
+    // mod.rs:529 compute_pvalue, two-tailed: share of finite draws with |t*| > |t| + 1e-12 (1 + |t|)
+    out.pvalue = nanv();
+    if (std::isfinite(out.stat)) {
+        const double eps = 1e-12 * (1.0 + std::fabs(out.stat));
+        size_t feas = 0, hi = 0;
+        for (double x : t_host) {
+            if (!std::isfinite(x)) continue;
+            feas++;
+            if (std::fabs(x) > std::fabs(out.stat) + eps) hi++;
+        }
+        if (feas) out.pvalue = double(hi) / double(feas);
+    }
+}
 }  // namespace fereg

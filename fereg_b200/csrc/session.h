@@ -68,6 +68,25 @@ class GpuSession {
     // host block is copied to the device and left unchanged.
     void ols(double* rows, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out);
 
+    // Wild cluster bootstrap of one coefficient (see boot.cu).
+    struct BootSpec {
+        size_t coef = 0;    // index among the nx regressors
+        double r0 = 0.0;    // H0: beta[coef] = r0
+        size_t reps = 999;  // draws (full enumeration when 2^G <= reps and G <= 20)
+        u64 seed = 1;
+        size_t tile = 256;  // draws residualized together as block-PCG columns
+        double tol = 1e-8;
+        size_t maxiter = 16000;
+        Precision prec = Precision::F64;
+    };
+    struct BootOut {
+        double stat = 0, se = 0, point = 0, pvalue = 0;
+        u64 reps = 0;
+        bool full_enum = false;
+        double* t_boot = nullptr;  // reps values
+    };
+    void wildboot(double* rows, bool on_device, size_t nx, const OlsSpec& ospec, const BootSpec& bs, BootOut& out);
+
    private:
     size_t n_ = 0;
     int kind_ = 0;
@@ -89,6 +108,17 @@ class GpuSession {
         bool has_groupvar = false;
     };
     Dof estimate_dof(bool clusters, bool firstpair, bool want_groupvar);
+    // What the last ols() call fitted (the bootstrap's starting point).
+    struct FitState {
+        bool ok = false;                // a cluster variance was computed
+        std::vector<size_t> kept;       // columns (1..nx) of the kept regressors
+        std::vector<double> A, beta;    // raw (X~'W X~)^-1 of the kept columns, coefficients
+        double crv1_scale = 0.0;        // CRV1 small-sample factor
+        double* rows = nullptr;         // the residualized block (device)
+        size_t R = 0;
+        bool y_absorbed = false;
+    };
+    FitState fit_;
     u64 mobility_groups(size_t qa, size_t qb, bool save);
     bool nested_within(size_t q, size_t c);
 };

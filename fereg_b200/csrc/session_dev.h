@@ -1,0 +1,82 @@
+// Device state of a GpuSession (shared by the OLS call and the wild bootstrap).
+#pragma once
+
+#include <vector>
+
+#include "device.cuh"
+#include "session.h"
+
+namespace fereg {
+
+// Device state of a session.
+struct SessionDev {
+    std::vector<DBuf<u32>> tcodes, ccodes;  // kept order
+    struct Subset {
+        DBuf<int> perm;  // rows (row order) grouped by cluster, stable
+        DBuf<u32> coff;  // G + 1
+        u32 G = 0;
+        double sign = 1.0;
+    };
+    std::vector<Subset> subsets;
+    DBuf<double> w_raw, wv;  // row order
+    DBuf<double> rows, part, sums, e, om, S, shift, beta;
+    DBuf<int> col, err;
+    DBuf<u32> uf, flags, scan, bsum, total, gv, map;
+    DBuf<double> pstat;
+    cudaStream_t st = nullptr;
+    u64 launches = 0;
+    // phase timing (CUDA events on the session's stream)
+    bool prof = false;
+    double ms[GpuSession::S_NSLOTS] = {};
+    u64 cnt[GpuSession::S_NSLOTS] = {};
+    std::vector<cudaEvent_t> pool;
+    struct Open {
+        int slot;
+        cudaEvent_t a, b;
+    };
+    std::vector<Open> open;
+    cudaEvent_t event() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        return e;
+    }
+    int begin(int slot) {
+        if (!prof) return -1;
+        open.push_back(Open{slot, event(), nullptr});
+        CK(cudaEventRecord(open.back().a, st));
+        return int(open.size()) - 1;
+    }
+    void end(int h) {
+        if (h < 0) return;
+        open[size_t(h)].b = event();
+        CK(cudaEventRecord(open[size_t(h)].b, st));
+    }
+    void collect() {
+        for (auto& o : open) {
+            if (o.b) {
+                CK(cudaEventSynchronize(o.b));
+                float t = 0;
+                CK(cudaEventElapsedTime(&t, o.a, o.b));
+                ms[o.slot] += t;
+                cnt[o.slot]++;
+                pool.push_back(o.b);
+            }
+            pool.push_back(o.a);
+        }
+        open.clear();
+    }
+    ~SessionDev() {
+        for (auto& o : open) {
+            cudaEventDestroy(o.a);
+            if (o.b) cudaEventDestroy(o.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+}  // namespace fereg

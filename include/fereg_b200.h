@@ -178,6 +178,33 @@ int fereg_session_row_order(const fereg_session* s, uint32_t* out);
 int fereg_session_ols(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_ols_spec* spec,
                       fereg_ols_out* out);
 
+/* Wild cluster bootstrap (ols.rs:204 ols_with_wildboot, wildboot/ols.rs:243-650 run_cluster_11):
+ * WCR11 test of H0: b[coef] = r0 with Rademacher weights on the clusters of the session's first
+ * cluster dimension (full enumeration when G <= 20 and 2^G <= reps), restricted residuals, CRV1
+ * over every cluster dimension, two-tailed p-value. Draw b uses SplitMix64 stream (seed, b)
+ * (rng.rs, weights.rs:65-79). Each `tile` draws are residualized together as columns of one block
+ * PCG. t_boot (reps values, or 2^G under full enumeration) may be NULL. */
+typedef struct fereg_boot_spec {
+    size_t coef;
+    double r0;
+    size_t reps;
+    uint64_t seed;
+    size_t tile;
+    double tol;
+    size_t maxiter;
+    int precision; /* FEREG_PREC_* of the bootstrap solves */
+} fereg_boot_spec;
+
+typedef struct fereg_boot_out {
+    double stat, se, point, pvalue;
+    uint64_t reps;
+    int32_t full_enum;
+    double* t_boot;
+} fereg_boot_out;
+
+int fereg_session_wildboot(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_ols_spec* spec,
+                           const fereg_boot_spec* boot, fereg_boot_out* out);
+
 /* Phase timing of the session's calls: the FEREG_PHASE_SLOTS slots of its absorber, then
  * 9 degrees of freedom, 10 column statistics, 11 Gram, 12 residuals and variance. */
 #define FEREG_SESSION_PHASE_SLOTS (FEREG_PHASE_SLOTS + 4)
