@@ -62,6 +62,18 @@ class BootOut(C.Structure):
                 ("reps", C.c_uint64), ("full_enum", C.c_int32), ("t_boot", C.POINTER(C.c_double))]
 
 
+class GlmSpec(C.Structure):
+    _fields_ = [("vce", C.c_int), ("tol", C.c_double), ("maxiter", C.c_size_t), ("inner_maxiter", C.c_size_t),
+                ("precision", C.c_int)]
+
+
+class GlmOut(C.Structure):
+    _fields_ = [("b", C.POINTER(C.c_double)), ("V", C.POINTER(C.c_double)), ("status", C.POINTER(C.c_uint8)),
+                ("N", C.c_double), ("deviance", C.c_double), ("ll", C.c_double), ("chi2", C.c_double),
+                ("df_m", C.c_double), ("N_clust", C.c_double), ("iterations", C.c_uint64),
+                ("pcg_iterations", C.c_uint64), ("converged", C.c_int32)]
+
+
 class OlsOut(C.Structure):
     _fields_ = ([("b", C.POINTER(C.c_double)), ("V", C.POINTER(C.c_double)), ("status", C.POINTER(C.c_uint8)),
                  ("resid", C.POINTER(C.c_double)), ("d", C.POINTER(C.c_double)),
@@ -91,6 +103,7 @@ def _setup(L):
     L.fereg_absorber_row_order.argtypes = [P, u32p]
     L.fereg_absorber_weights.argtypes = [P, f64p, C.POINTER(C.c_int)]
     L.fereg_absorber_set_weights.argtypes = [P, f64p]
+    L.fereg_absorber_set_weights_device.argtypes = [P, P]
     L.fereg_absorber_residualize.argtypes = [P, f64p, C.c_size_t, C.c_double, C.c_size_t, C.c_int, f64p, f64p,
                                              C.POINTER(SolveInfo)]
     L.fereg_absorber_residualize_ex.argtypes = [P, P, C.c_int, C.c_size_t, C.c_double, C.c_size_t, C.c_int, f64p,
@@ -114,6 +127,7 @@ def _setup(L):
     L.fereg_session_stream.restype = P
     L.fereg_session_set_profiling.argtypes = [P, C.c_int]
     L.fereg_session_info.argtypes = [P, u64p]
+    L.fereg_session_poisson.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(GlmSpec), C.POINTER(GlmOut)]
     L.fereg_session_wildboot.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(OlsSpec), C.POINTER(BootSpec),
                                          C.POINTER(BootOut)]
     L.fereg_session_phase_times.argtypes = [P, f64p, u64p]
@@ -177,6 +191,10 @@ class Absorber:
         has = C.c_int()
         _check(lib().fereg_absorber_weights(self.h, _p(out, f64p), C.byref(has)))
         return out if has.value else None
+
+    def set_weights_device(self, ptr):
+        """Row-order weights in device memory (pointer); the weight state is computed on the device."""
+        _check(lib().fereg_absorber_set_weights_device(self.h, P(ptr)))
 
     def set_weights(self, w_rows):
         wa = None if w_rows is None else np.ascontiguousarray(w_rows, dtype=np.float64)
@@ -394,3 +412,24 @@ class Session:
                                             C.byref(out)))
         return dict(stat=out.stat, se=out.se, point=out.point, pvalue=out.pvalue, reps=int(out.reps),
                     full_enum=bool(out.full_enum), t_boot=t[: int(out.reps)].copy())
+
+    def poisson(self, rows, vce="robust", tol=1e-8, maxiter=10000, inner_maxiter=16000, precision=PREC_F64,
+                on_device=False, nx=None):
+        """Poisson PML of column 0 (y >= 0) on the other columns of the n x (1 + nx) block (row
+        order; host array, or a device pointer with on_device=True)."""
+        if on_device:
+            ptr = rows
+            assert nx is not None
+        else:
+            assert rows.dtype == np.float64 and rows.flags.c_contiguous
+            ptr = rows.ctypes.data
+            nx = rows.shape[1] - 1
+        b = np.zeros(max(1, nx))
+        V = np.zeros((max(1, nx), max(1, nx)))
+        status = np.zeros(max(1, nx), dtype=np.uint8)
+        spec = GlmSpec({"robust": 1, "cluster": 2}[vce], tol, maxiter, inner_maxiter, precision)
+        out = GlmOut(_p(b, f64p), _p(V, f64p), _p(status, u8p))
+        _check(lib().fereg_session_poisson(self.h, P(ptr), int(on_device), nx, C.byref(spec), C.byref(out)))
+        return dict(b=b[:nx], V=V[:nx, :nx], status=status[:nx], N=out.N, deviance=out.deviance, ll=out.ll,
+                    chi2=out.chi2, df_m=out.df_m, N_clust=out.N_clust, iterations=int(out.iterations),
+                    pcg_iterations=int(out.pcg_iterations), converged=bool(out.converged))

@@ -15,6 +15,7 @@
 
 #include "absorber.h"
 #include "kernels.cuh"
+#include "weights.cuh"
 
 namespace fereg {
 
@@ -113,6 +114,9 @@ struct Scratch {
     u32 ms_acc = 0, ns_acc = 0;  // small coordinates / blocks summed in the segment passes
     // weights
     DBuf<double> w_rows, cell_w, n1inv, nr, inv_diag, minv;
+    DBuf<double> n1, diag, wpart;  // device weight refresh
+    DBuf<uint8_t> red;
+    DBuf<int> wflag;
     // solve (FP64)
     DBuf<double> rows, rhs, b1, coefs, r, z, p, q, t, part, cta, cta2, colsum, along, small;
     // inner FP32 buffers of the refined solve
@@ -266,13 +270,89 @@ GpuAbsorber::~GpuAbsorber() {
 
 bool GpuAbsorber::weights(double* out) const {
     if (!weighted_) return false;
+    sync_host_weights();
     if (out) std::copy(w_rows_.begin(), w_rows_.end(), out);
     return true;
+}
+
+// Device form of refresh_weights for row-order weights already in device memory: every array
+// of the weight state is computed on the device (weights.cuh); the host mirrors are copied back
+// only when a host-side reader needs them.
+void GpuAbsorber::set_weights_device(const double* w_dev) {
+    ctx_.check();
+    const HostStructure& st = hs_;
+    const size_t n = st.n, M = st.ncells, g1 = st.g1, m = st.m;
+    Scratch& d = *d_;
+    d.wflag.alloc(1);
+    CK(cudaMemsetAsync(d.wflag.p, 0, sizeof(int), stream_));
+    k_check_weights<<<grid_for(n), THREADS, 0, stream_>>>(w_dev, n, d.wflag.p);
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, d.wflag.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    if (bad) throw Error(RC_INVALID_INPUT, "weights must be positive and finite");
+    d.w_rows.alloc(n);
+    CK(cudaMemcpyAsync(d.w_rows.p, w_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    d.cell_w.alloc(M);
+    if (st.trivial()) CK(cudaMemcpyAsync(d.cell_w.p, w_dev, M * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    else k_cell_weights<<<grid_for(M), THREADS, 0, stream_>>>(w_dev, d.cell_row.p, u32(M), d.cell_w.p);
+    d.n1.alloc(g1);
+    d.n1inv.alloc(g1);
+    k_seg_weights<<<grid_for(g1), THREADS, 0, stream_>>>(d.cell_w.p, d.seg_off.p, u32(g1), d.n1.p, d.n1inv.p);
+    d.launches += 3;
+    if (m > 0) {
+        d.nr.alloc(m);
+        d.diag.alloc(m);
+        d.red.alloc(m);
+        d.inv_diag.alloc(m);
+        k_coord_weights<<<int(std::min<size_t>((m * 32 + THREADS - 1) / THREADS, size_t(GRID_T) * 4)), THREADS, 0,
+                          stream_>>>(d.pl_off.p, d.pl_cell.p, d.pl_seg.p, u32(m), d.cell_w.p, d.n1inv.p, d.nr.p,
+                                     d.diag.p, d.red.p, d.inv_diag.p);
+        d.launches++;
+    }
+    d.wpart.alloc(GRID_V);
+    k_vec_sum<<<GRID_V, 256, 0, stream_>>>(d.n1.p, g1, d.wpart.p);
+    d.launches++;
+    std::vector<double> part(GRID_V);
+    CK(cudaMemcpyAsync(part.data(), d.wpart.p, GRID_V * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaGetLastError());
+    sw_ = 0.0;
+    for (double v : part) sw_ += v;
+    weighted_ = true;
+    host_stale_ = true;
+    dev_jacobi_ = m > 0;
+    pre_fresh_ = false;
+}
+
+// Copies the device weight state back into the host mirrors after set_weights_device.
+void GpuAbsorber::sync_host_weights() const {
+    if (!host_stale_) return;
+    const HostStructure& st = hs_;
+    const size_t n = st.n, M = st.ncells, g1 = st.g1, m = st.m;
+    Scratch& d = *d_;
+    w_rows_.resize(n);
+    cell_w_.resize(M);
+    n1_.resize(g1);
+    nr_.resize(m);
+    diag_.resize(m);
+    red_.resize(m);
+    CK(cudaMemcpyAsync(w_rows_.data(), d.w_rows.p, n * 8, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(cell_w_.data(), d.cell_w.p, M * 8, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(n1_.data(), d.n1.p, g1 * 8, cudaMemcpyDeviceToHost, stream_));
+    if (m > 0) {
+        CK(cudaMemcpyAsync(nr_.data(), d.nr.p, m * 8, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(diag_.data(), d.diag.p, m * 8, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(red_.data(), d.red.p, m, cudaMemcpyDeviceToHost, stream_));
+    }
+    CK(cudaStreamSynchronize(stream_));
+    host_stale_ = false;
 }
 
 // operator.rs:211-338 refresh_weights + :344-570 level_weights (host form).
 void GpuAbsorber::refresh_weights(const double* w_kept) {
     const HostStructure& st = hs_;
+    host_stale_ = false;
+    dev_jacobi_ = false;
     weighted_ = w_kept != nullptr;
     w_rows_.clear();
     cell_w_.clear();
@@ -352,6 +432,7 @@ void GpuAbsorber::set_weights(const double* w_rows) {
 }
 
 void GpuAbsorber::weight_state(double* n1, double* nr, double* diag, uint8_t* red, double* sw) const {
+    sync_host_weights();
     if (n1) std::copy(n1_.begin(), n1_.end(), n1);
     if (nr) std::copy(nr_.begin(), nr_.end(), nr);
     if (diag) std::copy(diag_.begin(), diag_.end(), diag);
@@ -366,11 +447,15 @@ void GpuAbsorber::ensure_precond() {
     if (pre_fresh_) return;
     const HostStructure& st = hs_;
     const size_t m = st.m, ms = st.m_small, M = st.ncells;
-    std::vector<double> inv(m);
-    for (size_t i = 0; i < m; i++) inv[i] = (red_[i] || !(diag_[i] > 0.0)) ? 0.0 : 1.0 / diag_[i];
-    d_->inv_diag.upload(inv, stream_);
+    const bool small = ms > 0 && ms <= DENSE_SMALL_MAX;
+    if (small) sync_host_weights();  // the dense small block is assembled on the host
+    if (!dev_jacobi_) {  // after set_weights_device the Jacobi factors are already on the device
+        std::vector<double> inv(m);
+        for (size_t i = 0; i < m; i++) inv[i] = (red_[i] || !(diag_[i] > 0.0)) ? 0.0 : 1.0 / diag_[i];
+        d_->inv_diag.upload(inv, stream_);
+    }
     small_ok_ = false;
-    if (ms > 0 && ms <= DENSE_SMALL_MAX) {
+    if (small) {
         auto cw = [&](size_t c) { return cell_w_.empty() ? 1.0 : cell_w_[c]; };
         size_t ns = 0;
         for (auto& b : st.blocks) ns += b.small;
@@ -1059,6 +1144,7 @@ void GpuAbsorber::fit_rows(const double* coefs, size_t r, size_t col, double* ou
 }
 
 void GpuAbsorber::term_values(const double* coefs, size_t r, size_t col, double* out) const {
+    sync_host_weights();
     const HostStructure& st = hs_;
     const size_t nterms = g_.size();
     if (st.fe1 < 0 || norm_fe1_ < 0) return;

@@ -54,6 +54,9 @@ class GpuAbsorber {
     bool weights(double* out) const;
     // Row-order weights (null = ones), strictly positive and finite (solve.rs:1010-1139).
     void set_weights(const double* w_rows);
+    // The same for row-order weights in device memory; the weight state is computed on the
+    // device (the host mirrors follow when a host-side reader needs them).
+    void set_weights_device(const double* w_rows_dev);
 
     // Residualizes the N x R row-major block `z` in place (rows in row order). `z` is host
     // memory for `residualize`, device memory for `residualize_device`. `warm` and `coefs` are
@@ -99,9 +102,12 @@ class GpuAbsorber {
     int norm_fe1_ = -1;
     Ctx ctx_;
     cudaStream_t stream_ = nullptr;
-    // host weight state (operator.rs:44-63)
-    std::vector<double> w_rows_, cell_w_, n1_, nr_, diag_;
-    std::vector<uint8_t> red_;
+    // host weight state (operator.rs:44-63); after set_weights_device these mirrors are copied
+    // back from the device on first use (host_stale_)
+    mutable std::vector<double> w_rows_, cell_w_, n1_, nr_, diag_;
+    mutable std::vector<uint8_t> red_;
+    mutable bool host_stale_ = false;
+    bool dev_jacobi_ = false;  // inv_diag was computed on the device
     double sw_ = 0;
     bool weighted_ = false;
     bool pre_fresh_ = false;
@@ -109,6 +115,7 @@ class GpuAbsorber {
     std::unique_ptr<Scratch> d_;
 
     void refresh_weights(const double* w_kept);
+    void sync_host_weights() const;
     void upload_weights();
     void ensure_precond();
     SolveInfo solve(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,

@@ -153,6 +153,13 @@ int fereg_absorber_set_weights(fereg_absorber* h, const double* w) {
     });
 }
 
+int fereg_absorber_set_weights_device(fereg_absorber* h, const double* w_dev) {
+    return guard([&] {
+        if (!h || !w_dev) throw Error(RC_INVALID_INPUT, "fereg_absorber_set_weights_device: NULL argument");
+        h->a.set_weights_device(w_dev);
+    });
+}
+
 int fereg_absorber_residualize(fereg_absorber* h, double* z, size_t r, double tol, size_t maxiter, int want_coefs,
                                const double* warm, double* coefs_out, fereg_solve_info* info) {
     return fereg_absorber_residualize_ex(h, z, 0, r, tol, maxiter, want_coefs, warm, coefs_out, FEREG_PREC_F64, info);
@@ -370,6 +377,36 @@ int fereg_session_wildboot(fereg_session* s, double* rows, int rows_on_device, s
         out->pvalue = bo.pvalue;
         out->reps = bo.reps;
         out->full_enum = bo.full_enum ? 1 : 0;
+    });
+}
+
+int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
+                          fereg_glm_out* out) {
+    return guard([&] {
+        if (!s || !rows || !spec || !out) throw Error(RC_INVALID_INPUT, "fereg_session_poisson: NULL argument");
+        if (spec->vce != 1 && spec->vce != 2) throw Error(RC_INVALID_INPUT, "fereg_session_poisson: vce is 1 or 2");
+        if (spec->precision != FEREG_PREC_F64 && spec->precision != FEREG_PREC_F32_REFINED)
+            throw Error(RC_INVALID_INPUT, "fereg_session_poisson: unknown precision");
+        GpuSession::GlmSpec gs;
+        gs.vce = spec->vce;
+        gs.tol = spec->tol;
+        gs.maxiter = spec->maxiter;
+        gs.inner_maxiter = spec->inner_maxiter;
+        gs.prec = spec->precision == FEREG_PREC_F32_REFINED ? Precision::F32_REFINED : Precision::F64;
+        GpuSession::GlmOut go;
+        go.b = out->b;
+        go.V = out->V;
+        go.status = out->status;
+        s->s.poisson(rows, rows_on_device != 0, nx, gs, go);
+        out->N = go.N;
+        out->deviance = go.deviance;
+        out->ll = go.ll;
+        out->chi2 = go.chi2;
+        out->df_m = go.df_m;
+        out->N_clust = go.N_clust;
+        out->iterations = go.iterations;
+        out->pcg_iterations = go.pcg_iterations;
+        out->converged = go.converged ? 1 : 0;
     });
 }
 

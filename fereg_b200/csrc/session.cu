@@ -18,6 +18,7 @@
 #include "linalg.h"
 #include "session.h"
 #include "boot.cuh"
+#include "glm.cuh"
 #include "session_dev.h"
 #include "stats.cuh"
 
@@ -273,6 +274,71 @@ GpuSession::Dof GpuSession::estimate_dof(bool clusters, bool firstpair, bool wan
     return dof;
 }
 
+// Outer products sum om_i a_i a_i^T over `nrows` rows of the srcR-column block src:
+// a_i = [x_i[cols] + shift, 1 (cst)]; optionally the plain sums of squares of the columns.
+// Returns the full msz x msz matrix (device passes, host copy of the result).
+std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, int srcR, const std::vector<int>& cols,
+                                               const std::vector<double>* shift, bool cst, const double* om,
+                                               const int* perm, bool ssq, std::vector<double>* ss_out) {
+    SessionDev& d = *d_;
+    cudaStream_t st = d.st;
+    const int k = int(cols.size()), msz = k + (cst ? 1 : 0);
+    const int P = msz * (msz + 1) / 2;
+    std::vector<double> m(size_t(msz) * msz, 0.0);
+    if (msz == 0) return m;
+    d.col.alloc(size_t(k) + 1);
+    CK(cudaMemcpyAsync(d.col.p, cols.data(), size_t(k) * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (shift) {
+        d.shift.alloc(size_t(k) + 1);
+        CK(cudaMemcpyAsync(d.shift.p, shift->data(), size_t(k) * 8, cudaMemcpyHostToDevice, st));
+    }
+    std::vector<double> pairs(P), sq(k);
+    if (msz <= 32) {
+        const int len = msz * msz + (ssq ? k : 0);
+        d.part.alloc(size_t(ST_GRID) * len);
+        d.sums.alloc(size_t(len));
+        OpSpec sp{src, nrows, srcR, d.col.p, shift ? d.shift.p : nullptr, k, cst ? 1 : 0, msz, om, perm, 0, 0,
+                  ssq ? 1 : 0};
+        switch ((msz + 7) / 8) {
+            case 1: k_outer_mma<1><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+            case 2: k_outer_mma<2><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+            case 3: k_outer_mma<3><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+            default: k_outer_mma<4><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+        }
+        k_sum_parts<<<(len + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
+        d.launches += 2;
+        std::vector<double> h(len);
+        CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int a = 0; a < msz; a++)
+            for (int b = a; b < msz; b++) m[size_t(a) * msz + b] = m[size_t(b) * msz + a] = h[size_t(a) * msz + b];
+        if (ss_out) *ss_out = std::vector<double>(h.begin() + msz * msz, h.end());
+        return m;
+    }
+    for (int p0 = 0; p0 < P; p0 += OP_MAXP) {
+        const int np = std::min(OP_MAXP, P - p0);
+        const bool with_sq = ssq && p0 == 0;
+        const int len = np + (with_sq ? k : 0);
+        d.part.alloc(size_t(ST_GRID) * len);
+        d.sums.alloc(size_t(len));
+        OpSpec s{src, nrows, srcR, d.col.p, shift ? d.shift.p : nullptr, k, cst ? 1 : 0, msz, om, perm, p0, np,
+                 with_sq ? 1 : 0};
+        k_outer<<<ST_GRID, ST_TB, 0, st>>>(s, d.part.p);
+        k_sum_parts<<<(len + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
+        d.launches += 2;
+        std::vector<double> h(len);
+        CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::copy(h.begin(), h.begin() + np, pairs.begin() + p0);
+        if (with_sq) std::copy(h.begin() + np, h.end(), sq.begin());
+    }
+    int p = 0;
+    for (int a = 0; a < msz; a++)
+        for (int b = a; b < msz; b++, p++) m[size_t(a) * msz + b] = m[size_t(b) * msz + a] = pairs[p];
+    if (ss_out) *ss_out = sq;
+    return m;
+    }
+
 void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out) {
     SessionDev& d = *d_;
     cudaStream_t st = d.st;
@@ -281,9 +347,9 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     if (r + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg ols: at most 62 regressors on the device path");
     double* rows = rows_in;
     if (!on_device) {
-        d.rows.alloc(n * r);
-        CK(cudaMemcpyAsync(d.rows.p, rows_in, n * r * 8, cudaMemcpyHostToDevice, st));
-        rows = d.rows.p;
+    d.rows.alloc(n * r);
+    CK(cudaMemcpyAsync(d.rows.p, rows_in, n * r * 8, cudaMemcpyHostToDevice, st));
+    rows = d.rows.p;
     }
     const std::vector<u32>& pi = ab_->row_order();
     const int kind = kind_;
@@ -307,16 +373,16 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     d.part.alloc(size_t(ST_GRID) * r * 6);
     d.sums.alloc(r * 6);
     for (int j0 = 0; j0 < R; j0 += 32) {
-        const int Rc = std::min(32, R - j0);
-        switch (rcp_of(Rc)) {
-            case 1: k_colstats1<1><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            case 2: k_colstats1<2><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            case 4: k_colstats1<4><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            case 8: k_colstats1<8><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            case 16: k_colstats1<16><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            default: k_colstats1<32><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-        }
-        d.launches++;
+    const int Rc = std::min(32, R - j0);
+    switch (rcp_of(Rc)) {
+        case 1: k_colstats1<1><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+        case 2: k_colstats1<2><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+        case 4: k_colstats1<4><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+        case 8: k_colstats1<8><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+        case 16: k_colstats1<16><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+        default: k_colstats1<32><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+    }
+    d.launches++;
     }
     k_sum_parts<<<(R * 6 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 6, d.sums.p);
     d.launches++;
@@ -326,13 +392,13 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     CK(cudaStreamSynchronize(st));
     std::vector<double> wmean(r), sumsq(r), wss_unc(r), sd(r), wss(r);
     for (size_t j = 0; j < r; j++) {
-        const double* a = s1.data() + j * 6;
-        const double m2 = std::max(0.0, a[1] - a[0] * a[0] / double(n));
-        sd[j] = std::max(std::sqrt(m2 / (double(n) - 1.0)), 1e-3);
-        wmean[j] = c0[j] + a[2] / sumw;
-        wss[j] = std::max(0.0, a[3] - a[2] * a[2] / sumw);
-        sumsq[j] = a[4];
-        wss_unc[j] = a[5];
+    const double* a = s1.data() + j * 6;
+    const double m2 = std::max(0.0, a[1] - a[0] * a[0] / double(n));
+    sd[j] = std::max(std::sqrt(m2 / (double(n) - 1.0)), 1e-3);
+    wmean[j] = c0[j] + a[2] / sumw;
+    wss[j] = std::max(0.0, a[3] - a[2] * a[2] / sumw);
+    sumsq[j] = a[4];
+    wss_unc[j] = a[5];
     }
     const double tscale = (kind == 1 || kind == 3) ? double(n) / sumw : 1.0;
     const double tss_y = (has_intercept ? wss[0] : wss_unc[0]) * tscale;
@@ -343,69 +409,15 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     const size_t p_len = ab_->coefs_len();
     std::vector<double> coefs(want_coefs ? p_len * r : 0);
     const SolveInfo info =
-        ab_->residualize_device(rows, r, spec.tol, spec.maxiter, want_coefs, nullptr, want_coefs ? coefs.data() : nullptr,
-                                spec.prec);
+    ab_->residualize_device(rows, r, spec.tol, spec.maxiter, want_coefs, nullptr, want_coefs ? coefs.data() : nullptr,
+                            spec.prec);
 
     // Outer products over the block: sum om a a^T of columns `cols` shifted by `shift` (+ the
     // constant), optionally the plain sums of squares; returns the full msz x msz matrix.
     auto outer = [&](const double* src, size_t nrows, int srcR, const std::vector<int>& cols,
-                     const std::vector<double>* shift, bool cst, const double* om, const int* perm, bool ssq,
-                     std::vector<double>* ss_out) {
-        const int k = int(cols.size()), msz = k + (cst ? 1 : 0);
-        const int P = msz * (msz + 1) / 2;
-        std::vector<double> m(size_t(msz) * msz, 0.0);
-        if (msz == 0) return m;
-        d.col.alloc(size_t(k) + 1);
-        CK(cudaMemcpyAsync(d.col.p, cols.data(), size_t(k) * sizeof(int), cudaMemcpyHostToDevice, st));
-        if (shift) {
-            d.shift.alloc(size_t(k) + 1);
-            CK(cudaMemcpyAsync(d.shift.p, shift->data(), size_t(k) * 8, cudaMemcpyHostToDevice, st));
-        }
-        std::vector<double> pairs(P), sq(k);
-        if (msz <= 32) {
-            const int len = msz * msz + (ssq ? k : 0);
-            d.part.alloc(size_t(ST_GRID) * len);
-            d.sums.alloc(size_t(len));
-            OpSpec sp{src, nrows, srcR, d.col.p, shift ? d.shift.p : nullptr, k, cst ? 1 : 0, msz, om, perm, 0, 0,
-                      ssq ? 1 : 0};
-            switch ((msz + 7) / 8) {
-                case 1: k_outer_mma<1><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
-                case 2: k_outer_mma<2><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
-                case 3: k_outer_mma<3><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
-                default: k_outer_mma<4><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
-            }
-            k_sum_parts<<<(len + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
-            d.launches += 2;
-            std::vector<double> h(len);
-            CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            for (int a = 0; a < msz; a++)
-                for (int b = a; b < msz; b++) m[size_t(a) * msz + b] = m[size_t(b) * msz + a] = h[size_t(a) * msz + b];
-            if (ss_out) *ss_out = std::vector<double>(h.begin() + msz * msz, h.end());
-            return m;
-        }
-        for (int p0 = 0; p0 < P; p0 += OP_MAXP) {
-            const int np = std::min(OP_MAXP, P - p0);
-            const bool with_sq = ssq && p0 == 0;
-            const int len = np + (with_sq ? k : 0);
-            d.part.alloc(size_t(ST_GRID) * len);
-            d.sums.alloc(size_t(len));
-            OpSpec s{src, nrows, srcR, d.col.p, shift ? d.shift.p : nullptr, k, cst ? 1 : 0, msz, om, perm, p0, np,
-                     with_sq ? 1 : 0};
-            k_outer<<<ST_GRID, ST_TB, 0, st>>>(s, d.part.p);
-            k_sum_parts<<<(len + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
-            d.launches += 2;
-            std::vector<double> h(len);
-            CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            std::copy(h.begin(), h.begin() + np, pairs.begin() + p0);
-            if (with_sq) std::copy(h.begin() + np, h.end(), sq.begin());
-        }
-        int p = 0;
-        for (int a = 0; a < msz; a++)
-            for (int b = a; b < msz; b++, p++) m[size_t(a) * msz + b] = m[size_t(b) * msz + a] = pairs[p];
-        if (ss_out) *ss_out = sq;
-        return m;
+                 const std::vector<double>* shift, bool cst, const double* om, const int* perm, bool ssq,
+                 std::vector<double>* ss_out) {
+    return outer_products(src, nrows, srcR, cols, shift, cst, om, perm, ssq, ss_out);
     };
 
     // Pass B: weighted Gram of the residualized block (stats.rs:195)
@@ -424,38 +436,38 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     for (size_t j = 0; j < r; j++) absorbed[j] = ss_res[j] / sumsq[j] <= ctol;
     const bool y_abs = nx >= 1 && absorbed[0];
     if (y_abs) {  // reghdfe zeroes the partialled-out depvar
-        k_zero_col<<<blocks_for(n, 256), 256, 0, st>>>(rows, n, R, 0);
-        d.launches++;
-        for (size_t j = 0; j < r; j++) g[j] = g[j * r] = 0.0;
+    k_zero_col<<<blocks_for(n, 256), 256, 0, st>>>(rows, n, R, 0);
+    d.launches++;
+    for (size_t j = 0; j < r; j++) g[j] = g[j * r] = 0.0;
     }
     for (size_t j = 1; j < r; j++)
-        if (absorbed[j]) status[j - 1] = 2;
+    if (absorbed[j]) status[j - 1] = 2;
     // stage 2: sweeps on the standardized Gram of the candidates (ols.rs:46, vcov.rs:22)
     std::vector<size_t> cand;
     for (size_t j = 1; j < r; j++)
-        if (status[j - 1] == 0) cand.push_back(j);
+    if (status[j - 1] == 0) cand.push_back(j);
     const size_t kc = cand.size();
     la::Mat gs(kc * kc);
     for (size_t a = 0; a < kc; a++)
-        for (size_t b = 0; b < kc; b++) gs[a * kc + b] = g[cand[a] * r + cand[b]] / (sd[cand[a]] * sd[cand[b]]);
+    for (size_t b = 0; b < kc; b++) gs[a * kc + b] = g[cand[a] * r + cand[b]] / (sd[cand[a]] * sd[cand[b]]);
     std::vector<bool> dropped;
     const la::Mat inv_c = la::sweep_inverse(gs, kc, SWEEP_TOL, false, dropped);
     std::vector<size_t> keep_pos, kept;
     for (size_t c = 0; c < kc; c++) {
-        if (dropped[c]) status[cand[c] - 1] = 3;
-        else {
-            keep_pos.push_back(c);
-            kept.push_back(cand[c]);
-        }
+    if (dropped[c]) status[cand[c] - 1] = 3;
+    else {
+        keep_pos.push_back(c);
+        kept.push_back(cand[c]);
+    }
     }
     const size_t k = kept.size();
     la::Mat inv_s(k * k);
     for (size_t a = 0; a < k; a++)
-        for (size_t b = 0; b < k; b++) inv_s[a * k + b] = inv_c[keep_pos[a] * kc + keep_pos[b]];
+    for (size_t b = 0; b < k; b++) inv_s[a * k + b] = inv_c[keep_pos[a] * kc + keep_pos[b]];
     const double sd_y = sd[0];
     std::vector<double> b_s(k, 0.0), beta(k);
     for (size_t a = 0; a < k; a++)
-        for (size_t b = 0; b < k; b++) b_s[a] += inv_s[a * k + b] * (g[kept[b] * r] / (sd[kept[b]] * sd_y));
+    for (size_t b = 0; b < k; b++) b_s[a] += inv_s[a * k + b] * (g[kept[b] * r] / (sd[kept[b]] * sd_y));
     for (size_t a = 0; a < k; a++) beta[a] = b_s[a] * sd_y / sd[kept[a]];
     // the fitted state the wild bootstrap starts from: kept columns, raw (X~'W X~)^-1, beta
     fit_ = FitState{};
@@ -463,7 +475,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     fit_.beta = beta;
     fit_.A.assign(k * k, 0.0);
     for (size_t a = 0; a < k; a++)
-        for (size_t b = 0; b < k; b++) fit_.A[a * k + b] = inv_s[a * k + b] / (sd[kept[a]] * sd[kept[b]]);
+    for (size_t b = 0; b < k; b++) fit_.A[a * k + b] = inv_s[a * k + b] / (sd[kept[a]] * sd[kept[b]]);
     fit_.rows = rows;
     fit_.R = r;
     fit_.y_absorbed = y_abs;
@@ -474,8 +486,8 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     d.col.alloc(k + 1);
     d.beta.alloc(k + 1);
     if (k) {
-        CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
     }
     d.e.alloc(n);
     d.part.alloc(ST_GRID);
@@ -491,8 +503,8 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     // bread: the standardized inverse, bordered by the constant (vcov.rs:220)
     std::vector<double> means_s(k), xbar(k);
     for (size_t a = 0; a < k; a++) {
-        means_s[a] = wmean[kept[a]] / sd[kept[a]];
-        xbar[a] = wmean[kept[a]];
+    means_s[a] = wmean[kept[a]] / sd[kept[a]];
+    xbar[a] = wmean[kept[a]];
     }
     double b0_s = wmean[0] / sd_y;
     for (size_t a = 0; a < k; a++) b0_s -= means_s[a] * b_s[a];
@@ -510,72 +522,72 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     for (size_t a = 0; a < k; a++) sc[a] = sd[kept[a]];
     if (report_constant) sc[k] = 1.0;
     auto standardize = [&](la::Mat& mt) {
-        for (size_t a = 0; a < msz; a++)
-            for (size_t b = 0; b < msz; b++) mt[a * msz + b] /= sc[a] * sc[b] * sd_y * sd_y;
+    for (size_t a = 0; a < msz; a++)
+        for (size_t b = 0; b < msz; b++) mt[a * msz + b] /= sc[a] * sc[b] * sd_y * sd_y;
     };
     la::Mat v_s(msz * msz, 0.0);
     if (msz > 0) {
-        if (vce == 0) {
-            const double f = (rss_s / bigN) * (bigN / df_r);
-            for (size_t i = 0; i < msz * msz; i++) v_s[i] = f * bread[i];
-        } else if (vce == 1) {
-            d.om.alloc(n);
-            k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 0, d.om.p);
+    if (vce == 0) {
+        const double f = (rss_s / bigN) * (bigN / df_r);
+        for (size_t i = 0; i < msz * msz; i++) v_s[i] = f * bread[i];
+    } else if (vce == 1) {
+        d.om.alloc(n);
+        k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 0, d.om.p);
+        d.launches++;
+        const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+        la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
+        standardize(meat);
+        v_s = la::sandwich(bread, meat, msz, bigN / (bigN - df_a - df_m));
+    } else {
+        d.om.alloc(n);
+        k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 1, d.om.p);
+        d.launches++;
+        const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+        if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+        la::Mat meat(msz * msz, 0.0);
+        for (auto& sub : d.subsets) {
+            d.S.alloc(size_t(sub.G) * msz);
+            d.shift.alloc(k + 1);
+            if (k) CK(cudaMemcpyAsync(d.shift.p, shift.data(), k * 8, cudaMemcpyHostToDevice, st));
+            k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(rows, R, d.col.p, d.shift.p, int(k), report_constant ? 1 : 0,
+                                                       d.om.p, sub.perm.p, sub.coff.p, sub.G, d.S.p);
             d.launches++;
-            const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
-            la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
-            standardize(meat);
-            v_s = la::sandwich(bread, meat, msz, bigN / (bigN - df_a - df_m));
-        } else {
-            d.om.alloc(n);
-            k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 1, d.om.p);
-            d.launches++;
-            const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+            std::vector<int> scols(msz);
+            std::iota(scols.begin(), scols.end(), 0);
+            const la::Mat part = outer(d.S.p, sub.G, int(msz), scols, nullptr, false, nullptr, nullptr, false, nullptr);
+            for (size_t i = 0; i < msz * msz; i++) meat[i] += sub.sign * part[i];
+            // the next subset's scores need the kept columns again
             if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
-            la::Mat meat(msz * msz, 0.0);
-            for (auto& sub : d.subsets) {
-                d.S.alloc(size_t(sub.G) * msz);
-                d.shift.alloc(k + 1);
-                if (k) CK(cudaMemcpyAsync(d.shift.p, shift.data(), k * 8, cudaMemcpyHostToDevice, st));
-                k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(rows, R, d.col.p, d.shift.p, int(k), report_constant ? 1 : 0,
-                                                           d.om.p, sub.perm.p, sub.coff.p, sub.G, d.S.p);
-                d.launches++;
-                std::vector<int> scols(msz);
-                std::iota(scols.begin(), scols.end(), 0);
-                const la::Mat part = outer(d.S.p, sub.G, int(msz), scols, nullptr, false, nullptr, nullptr, false, nullptr);
-                for (size_t i = 0; i < msz * msz; i++) meat[i] += sub.sign * part[i];
-                // the next subset's scores need the kept columns again
-                if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
-            }
-            standardize(meat);
-            const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
-            const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
-            fit_.crv1_scale = q_cluster;
-            fit_.ok = true;
-            v_s = la::sandwich(bread, meat, msz, q_cluster);
-            if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
         }
+        standardize(meat);
+        const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
+        const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
+        fit_.crv1_scale = q_cluster;
+        fit_.ok = true;
+        v_s = la::sandwich(bread, meat, msz, q_cluster);
+        if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
+    }
     }
     d.end(ph);
     d.collect();
     if (vce == 2) df_r = std::min(df_r, g_min - 1.0);
     for (size_t i = 0; i < msz; i++)
-        for (size_t j = 0; j < i; j++) v_s[j * msz + i] = v_s[i * msz + j];
+    for (size_t j = 0; j < i; j++) v_s[j * msz + i] = v_s[i * msz + j];
 
     // Wald F of the slopes (greedy sweep of their variance)
     double f_stat = nanv();
     if (k > 0) {
-        la::Mat vkk(k * k);
+    la::Mat vkk(k * k);
+    for (size_t a = 0; a < k; a++)
+        for (size_t b = 0; b < k; b++) vkk[a * k + b] = v_s[a * msz + b];
+    std::vector<bool> dv;
+    const la::Mat iv = la::sweep_inverse(vkk, k, F_SWEEP_TOL, true, dv);
+    if (std::none_of(dv.begin(), dv.end(), [](bool x) { return x; })) {
+        double qf = 0.0;
         for (size_t a = 0; a < k; a++)
-            for (size_t b = 0; b < k; b++) vkk[a * k + b] = v_s[a * msz + b];
-        std::vector<bool> dv;
-        const la::Mat iv = la::sweep_inverse(vkk, k, F_SWEEP_TOL, true, dv);
-        if (std::none_of(dv.begin(), dv.end(), [](bool x) { return x; })) {
-            double qf = 0.0;
-            for (size_t a = 0; a < k; a++)
-                for (size_t b = 0; b < k; b++) qf += b_s[a] * iv[a * k + b] * b_s[b];
-            f_stat = finite_or_nan(qf / df_m);
-        }
+            for (size_t b = 0; b < k; b++) qf += b_s[a] * iv[a * k + b] * b_s[b];
+        f_stat = finite_or_nan(qf / df_m);
+    }
     }
     if (std::any_of(v_s.begin(), v_s.end(), [](double x) { return std::isnan(x); })) std::fill(v_s.begin(), v_s.end(), 0.0);
 
@@ -584,7 +596,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     for (size_t a = 0; a < msz; a++) sx[a] = sc[a] / sd_y;
     for (size_t a = 0; a < msz; a++) b_raw[a] = b_full_s[a] / sx[a];
     for (size_t a = 0; a < msz; a++)
-        for (size_t b = 0; b < msz; b++) v_raw[a * msz + b] = v_s[a * msz + b] / (sx[a] * sx[b]);
+    for (size_t b = 0; b < msz; b++) v_raw[a * msz + b] = v_s[a * msz + b] / (sx[a] * sx[b]);
     const double b0 = report_constant ? b_raw[k] : 0.0;
     const size_t k_all = nx + (report_constant ? 1 : 0);
     std::vector<size_t> pos;
@@ -593,9 +605,9 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     if (out.b) std::fill(out.b, out.b + k_all, 0.0);
     if (out.V) std::fill(out.V, out.V + k_all * k_all, 0.0);
     for (size_t a = 0; a < pos.size(); a++) {
-        if (out.b) out.b[pos[a]] = b_raw[a];
-        if (out.V)
-            for (size_t b = 0; b < pos.size(); b++) out.V[pos[a] * k_all + pos[b]] = v_raw[a * msz + b];
+    if (out.b) out.b[pos[a]] = b_raw[a];
+    if (out.V)
+        for (size_t b = 0; b < pos.size(); b++) out.V[pos[a] * k_all + pos[b]] = v_raw[a * msz + b];
     }
     if (out.status) std::copy(status.begin(), status.end(), out.status);
     out.k_all = int(k_all);
@@ -636,41 +648,41 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     out.ic = double(info.iterations);
     out.nslots = int(dof.slots.size());
     if (out.dof_table)
-        for (size_t i = 0; i < dof.slots.size() && i < size_t(MAX_TABLE); i++) {
-            const auto& s = dof.slots[i];
-            double* t = out.dof_table + 5 * i;
-            t[0] = double(s.k);
-            t[1] = double(s.m);
-            t[2] = double(s.k - s.m);
-            t[3] = s.exact ? 0.0 : 1.0;
-            t[4] = s.nested ? 1.0 : 0.0;
-        }
+    for (size_t i = 0; i < dof.slots.size() && i < size_t(MAX_TABLE); i++) {
+        const auto& s = dof.slots[i];
+        double* t = out.dof_table + 5 * i;
+        t[0] = double(s.k);
+        t[1] = double(s.m);
+        t[2] = double(s.k - s.m);
+        t[3] = s.exact ? 0.0 : 1.0;
+        t[4] = s.nested ? 1.0 : 0.0;
+    }
     if (out.resid) {
-        std::vector<double> e(n);
-        CK(cudaMemcpyAsync(e.data(), d.e.p, n * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        for (size_t i = 0; i < n; i++) out.resid[pi[i]] = e[i];
+    std::vector<double> e(n);
+    CK(cudaMemcpyAsync(e.data(), d.e.p, n * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < n; i++) out.resid[pi[i]] = e[i];
     }
     if (out.d) {
-        // sum of the fixed effects: the FE fit of y minus the slopes' FE fits, less the constant
-        std::vector<double> comb(p_len, 0.0), fit(n);
-        for (size_t i = 0; i < p_len; i++) {
-            double v = coefs[i * r];
-            for (size_t a = 0; a < k; a++) v -= beta[a] * coefs[i * r + kept[a]];
-            comb[i] = v;
-        }
-        ab_->fit_rows(comb.data(), 1, 0, fit.data());
-        for (size_t i = 0; i < n; i++) out.d[pi[i]] = fit[i] - b0;
+    // sum of the fixed effects: the FE fit of y minus the slopes' FE fits, less the constant
+    std::vector<double> comb(p_len, 0.0), fit(n);
+    for (size_t i = 0; i < p_len; i++) {
+        double v = coefs[i * r];
+        for (size_t a = 0; a < k; a++) v -= beta[a] * coefs[i * r + kept[a]];
+        comb[i] = v;
+    }
+    ab_->fit_rows(comb.data(), 1, 0, fit.data());
+    for (size_t i = 0; i < n; i++) out.d[pi[i]] = fit[i] - b0;
     }
     if (out.groupvar) {
-        if (dof.has_groupvar) {
-            std::vector<u32> gv(n);
-            CK(cudaMemcpyAsync(gv.data(), d.gv.p, n * sizeof(u32), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            for (size_t i = 0; i < n; i++) out.groupvar[i] = double(gv[i]);
-        } else {
-            std::fill(out.groupvar, out.groupvar + n, nanv());
-        }
+    if (dof.has_groupvar) {
+        std::vector<u32> gv(n);
+        CK(cudaMemcpyAsync(gv.data(), d.gv.p, n * sizeof(u32), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < n; i++) out.groupvar[i] = double(gv[i]);
+    } else {
+        std::fill(out.groupvar, out.groupvar + n, nanv());
+    }
     }
     CK(cudaGetLastError());
 }
@@ -838,5 +850,205 @@ void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec
         }
         if (feas) out.pvalue = double(hi) / double(feas);
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Poisson PML by IRLS (glm/irls.rs:367-560 with ppmlhdfe conventions, glm/mod.rs:1053-1140 for
+// the variance). Each iteration: w = mu and z = eta - 1 + y / mu (device), the weight state
+// refreshed on the device, [z, X] residualized warm-started from the previous FE coefficients at
+// an inner tolerance tightened toward max(1e-12, 0.1 tol), the weighted regression on the
+// residualized block (device Gram, host sweep), eta = z - e and mu = exp(eta) with the deviance
+// (device). Stops when the relative deviance change |D - D'| / max(min(D, D'), 0.1) < tol with the
+// inner tolerance at its floor. Collinearity is settled in the first iteration (ppmlhdfe
+// remove_collinears): columns absorbed by the FE, then columns collinear with the others. The
+// variance uses the last iteration's weights: robust, (X~'WX~)^-1 [sum (e w)^2 x~ x~'] (X~'WX~)^-1
+// N / (N - 1), or clustered with G / (G - 1) and the multiway eigenvalue clip.
+void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out) {
+    if (!wk_.empty()) throw Error(RC_INVALID_INPUT, "fereg poisson: weighted sessions are not supported");
+    if (gs.vce == 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg poisson: cluster variance without clusters");
+    if (1 + nx + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg poisson: at most 62 regressors");
+    SessionDev& d = *d_;
+    cudaStream_t st = d.st;
+    const size_t n = n_, r = 1 + nx;
+    const int R = int(r);
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+    DBuf<double> raw, B, mu, eta, z, w, e, part, om;
+    DBuf<int> flag;
+    raw.alloc(n * r);
+    CK(cudaMemcpyAsync(raw.p, rows_in, n * r * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    B.alloc(n * r);
+    mu.alloc(n);
+    eta.alloc(n);
+    z.alloc(n);
+    w.alloc(n);
+    e.alloc(n);
+    om.alloc(n);
+    part.alloc(GLM_TB * 8);
+    flag.alloc(1);
+    CK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    k_glm_ysum<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, part.p, flag.p);
+    auto host_sum = [&](int parts) {
+        std::vector<double> h(static_cast<size_t>(parts));
+        CK(cudaMemcpyAsync(h.data(), part.p, size_t(parts) * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double t = 0.0;
+        for (double x : h) t += x;
+        return t;
+    };
+    const double ysum = host_sum(GLM_TB);
+    int neg = 0;
+    CK(cudaMemcpyAsync(&neg, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (neg) throw Error(RC_INVALID_INPUT, "fereg poisson: the dependent variable must be nonnegative");
+    if (!(ysum > 0.0)) throw Error(RC_TOO_FEW_OBS, "insufficient observations (the dependent variable is all zero)");
+    k_glm_start<<<blocks, 256, 0, st>>>(raw.p, n, R, ysum / double(n), mu.p, eta.p);
+    d.launches += 2;
+
+    // unweighted sums of squares of the raw regressors (stage-1 collinearity, ols.rs:38)
+    std::vector<int> all(r);
+    std::iota(all.begin(), all.end(), 0);
+    std::vector<double> sumsq;
+    outer_products(raw.p, n, R, all, nullptr, false, nullptr, nullptr, true, &sumsq);
+    const double highest = std::max(1e-12, 0.1 * gs.tol);
+    double tol_in = std::max(1e-4, gs.tol);
+    double dev_old = nanv(), dev = nanv();
+    std::vector<double> warm, coefs((ab_->coefs_len()) * r);
+    bool have_warm = false, converged = false;
+    std::vector<uint8_t> status(nx, 0);
+    std::vector<size_t> kept;
+    la::Mat inv;
+    std::vector<double> beta;
+    u64 iters = 0, pcg = 0;
+    for (size_t it = 1; it <= gs.maxiter; it++) {
+        ab_->ctx().check();
+        iters = it;
+        k_glm_work<<<blocks, 256, 0, st>>>(raw.p, n, R, mu.p, eta.p, B.p, z.p, w.p);
+        d.launches++;
+        ab_->set_weights_device(w.p);
+        const SolveInfo si = ab_->residualize_device(B.p, r, tol_in, gs.inner_maxiter, true,
+                                                     have_warm ? warm.data() : nullptr, coefs.data(), gs.prec);
+        pcg += si.iterations;
+        std::vector<double> ss_res;
+        const std::vector<double> G = outer_products(B.p, n, R, all, nullptr, false, w.p, nullptr, true, &ss_res);
+        if (it == 1) {  // columns absorbed by the FE, then collinear ones
+            const double ctol = std::min(1e-6, gs.tol / 10.0);
+            std::vector<size_t> cand;
+            for (size_t j = 1; j < r; j++) {
+                if (ss_res[j] / sumsq[j] <= ctol) status[j - 1] = 2;
+                else cand.push_back(j);
+            }
+            const size_t kc = cand.size();
+            la::Mat gc(kc * kc);
+            for (size_t a = 0; a < kc; a++)
+                for (size_t b = 0; b < kc; b++) gc[a * kc + b] = G[cand[a] * r + cand[b]];
+            std::vector<bool> dropped;
+            la::sweep_inverse(gc, kc, SWEEP_TOL, false, dropped);
+            for (size_t c = 0; c < kc; c++) {
+                if (dropped[c]) status[cand[c] - 1] = 3;
+                else kept.push_back(cand[c]);
+            }
+        }
+        const size_t k = kept.size();
+        la::Mat gk(k * k);
+        for (size_t a = 0; a < k; a++)
+            for (size_t b = 0; b < k; b++) gk[a * k + b] = G[kept[a] * r + kept[b]];
+        std::vector<bool> dk;
+        inv = la::sweep_inverse(gk, k, SWEEP_TOL, false, dk);
+        beta.assign(k, 0.0);
+        for (size_t a = 0; a < k; a++)
+            for (size_t b = 0; b < k; b++) beta[a] += inv[a * k + b] * G[kept[b] * r];
+        std::vector<int> kc(kept.begin(), kept.end());
+        d.col.alloc(k + 1);
+        d.beta.alloc(k + 1);
+        if (k) {
+            CK(cudaMemcpyAsync(d.col.p, kc.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
+        }
+        k_resid_e<<<ST_GRID, ST_TB, 0, st>>>(B.p, n, R, d.col.p, d.beta.p, int(k), 0, nullptr, e.p, part.p);
+        k_glm_update<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, z.p, e.p, eta.p, mu.p, part.p);
+        d.launches += 2;
+        dev = host_sum(GLM_TB);
+        if (!std::isfinite(dev)) throw Error(RC_CONVERGENCE, "fereg poisson: the deviance is not finite");
+        std::swap(warm, coefs);
+        if (coefs.size() != warm.size()) coefs.resize(warm.size());
+        have_warm = true;
+        if (it > 1) {
+            const double eps = std::fabs(dev - dev_old) / std::max(std::min(dev, dev_old), 0.1);
+            if (eps < gs.tol && tol_in <= highest) {
+                converged = true;
+                dev_old = dev;
+                break;
+            }
+            if (eps < tol_in) tol_in = std::max(highest, tol_in * 0.1);
+        }
+        dev_old = dev;
+    }
+    if (!converged) throw Error(RC_CONVERGENCE, "fereg poisson: IRLS did not converge");
+
+    // variance on the last iteration's weights (w, e and the residualized block B)
+    const size_t k = kept.size();
+    std::vector<int> kc(kept.begin(), kept.end());
+    la::Mat V(k * k, 0.0);
+    const double bigN = double(n);
+    if (k) {
+        if (gs.vce == 2) {
+            k_glm_score<<<blocks, 256, 0, st>>>(e.p, w.p, n, 0, om.p);
+            d.launches++;
+            la::Mat meat(k * k, 0.0);
+            for (auto& sub : d.subsets) {
+                d.S.alloc(size_t(sub.G) * k);
+                d.col.alloc(k + 1);
+                CK(cudaMemcpyAsync(d.col.p, kc.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+                k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(B.p, R, d.col.p, nullptr, int(k), 0, om.p, sub.perm.p,
+                                                           sub.coff.p, sub.G, d.S.p);
+                d.launches++;
+                std::vector<int> sc(k);
+                std::iota(sc.begin(), sc.end(), 0);
+                const la::Mat pm = outer_products(d.S.p, sub.G, int(k), sc, nullptr, false, nullptr, nullptr, false, nullptr);
+                for (size_t i = 0; i < k * k; i++) meat[i] += sub.sign * pm[i];
+            }
+            const double gmin = double(*std::min_element(cg_.begin(), cg_.end()));
+            V = la::sandwich(inv, meat, k, gmin > 1.0 ? gmin / (gmin - 1.0) : 0.0);
+            if (ccodes_.size() > 1) la::fix_psd(V, k, false);
+            out.N_clust = gmin;
+        } else {
+            k_glm_score<<<blocks, 256, 0, st>>>(e.p, w.p, n, 1, om.p);
+            d.launches++;
+            const la::Mat meat = outer_products(B.p, n, R, kc, nullptr, false, om.p, nullptr, false, nullptr);
+            V = la::sandwich(inv, meat, k, bigN / (bigN - 1.0));
+        }
+    }
+    // Wald chi2 of the slopes (greedy sweep of V)
+    double chi2 = nanv();
+    if (k) {
+        std::vector<bool> dv;
+        const la::Mat iv = la::sweep_inverse(V, k, F_SWEEP_TOL, true, dv);
+        if (std::none_of(dv.begin(), dv.end(), [](bool x) { return x; })) {
+            double q = 0.0;
+            for (size_t a = 0; a < k; a++)
+                for (size_t b = 0; b < k; b++) q += beta[a] * iv[a * k + b] * beta[b];
+            chi2 = finite_or_nan(q);
+        }
+    }
+    k_glm_ll<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, eta.p, mu.p, part.p);
+    d.launches++;
+    const double ll = host_sum(GLM_TB);
+    if (out.b) std::fill(out.b, out.b + nx, 0.0);
+    if (out.V) std::fill(out.V, out.V + nx * nx, 0.0);
+    for (size_t a = 0; a < k; a++) {
+        if (out.b) out.b[kept[a] - 1] = beta[a];
+        if (out.V)
+            for (size_t b = 0; b < k; b++) out.V[(kept[a] - 1) * nx + (kept[b] - 1)] = V[a * k + b];
+    }
+    if (out.status) std::copy(status.begin(), status.end(), out.status);
+    out.N = bigN;
+    out.deviance = dev;
+    out.ll = ll;
+    out.chi2 = chi2;
+    out.df_m = double(k);
+    out.iterations = iters;
+    out.pcg_iterations = pcg;
+    out.converged = converged;
+    CK(cudaGetLastError());
 }
 }  // namespace fereg

@@ -87,6 +87,24 @@ class GpuSession {
     };
     void wildboot(double* rows, bool on_device, size_t nx, const OlsSpec& ospec, const BootSpec& bs, BootOut& out);
 
+    // Poisson PML by IRLS on the session's FE (see session.cu).
+    struct GlmSpec {
+        int vce = 1;  // 1 robust, 2 cluster (ppmlhdfe reports no unadjusted Poisson variance)
+        double tol = 1e-8;
+        size_t maxiter = 10000;
+        size_t inner_maxiter = 16000;
+        Precision prec = Precision::F64;
+    };
+    struct GlmOut {
+        double* b = nullptr;        // nx (absorbed / collinear columns 0)
+        double* V = nullptr;        // nx x nx
+        uint8_t* status = nullptr;  // nx: 0 ok, 2 absorbed, 3 collinear
+        double N = 0, deviance = 0, ll = 0, chi2 = 0, df_m = 0, N_clust = 0;
+        u64 iterations = 0, pcg_iterations = 0;
+        bool converged = false;
+    };
+    void poisson(double* rows, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out);
+
    private:
     size_t n_ = 0;
     int kind_ = 0;
@@ -108,6 +126,9 @@ class GpuSession {
         bool has_groupvar = false;
     };
     Dof estimate_dof(bool clusters, bool firstpair, bool want_groupvar);
+    std::vector<double> outer_products(const double* src, size_t nrows, int srcR, const std::vector<int>& cols,
+                                       const std::vector<double>* shift, bool cst, const double* om, const int* perm,
+                                       bool ssq, std::vector<double>* ss_out);
     // What the last ols() call fitted (the bootstrap's starting point).
     struct FitState {
         bool ok = false;                // a cluster variance was computed

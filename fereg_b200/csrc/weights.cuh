@@ -1,0 +1,117 @@
+// Device refresh of the weight state (operator.rs:211-338 refresh_weights, :344-570
+// level_weights): cell weights W_c = sum of the cell's row weights, n1_s = sum of the segment's
+// W_c, and for every reduced coordinate k: n_k = sum of W_c over the cells of k, and
+// diag_k = n_k - sum_s c_{s,k}^2 / n1_s with c_{s,k} the weight of k's cells in segment s; k is
+// redundant when diag_k <= 1e-12 n_k (operator.rs:21), and the Jacobi factor is 1 / diag_k
+// otherwise. The coordinate-sorted lists hold each coordinate's cells in cell order, hence in
+// segment order, so c_{s,k} are the sums over runs of equal segment: a warp walks a list 32
+// entries at a time with a segmented scan and carries the open run into the next chunk. All
+// sums have a fixed order.
+#pragma once
+
+#include "device.cuh"
+
+namespace fereg {
+
+// flag = 1 when a weight is not positive and finite.
+__global__ void k_check_weights(const double* __restrict__ w, size_t n, int* flag) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const double x = w[i];
+        if (!(x > 0.0 && x <= 1.7976931348623157e308)) atomicExch(flag, 1);
+    }
+}
+
+// W_c = sum of the row weights of cell c (rows cell_row[c] .. cell_row[c+1]).
+__global__ void k_cell_weights(const double* __restrict__ w, const u32* __restrict__ cell_row, u32 M,
+                               double* __restrict__ cw) {
+    for (u32 c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (u32 r = cell_row[c]; r < cell_row[c + 1]; r++) s += w[r];
+        cw[c] = s;
+    }
+}
+
+// n1_s = sum of W_c over the segment's cells (cw null: 1 per cell); n1inv = 1 / n1.
+__global__ void k_seg_weights(const double* __restrict__ cw, const u32* __restrict__ seg_off, u32 g1,
+                              double* __restrict__ n1, double* __restrict__ n1inv) {
+    for (u32 s = blockIdx.x * blockDim.x + threadIdx.x; s < g1; s += gridDim.x * blockDim.x) {
+        double a = 0.0;
+        for (u32 c = seg_off[s]; c < seg_off[s + 1]; c++) a += cw ? cw[c] : 1.0;
+        n1[s] = a;
+        n1inv[s] = 1.0 / a;
+    }
+}
+
+// n_k, diag_k, redundant_k and the Jacobi factor of every coordinate; a warp per list.
+__global__ void k_coord_weights(const u32* __restrict__ pl_off, const u32* __restrict__ pl_cell,
+                                const u32* __restrict__ pl_seg, u32 m, const double* __restrict__ cw,
+                                const double* __restrict__ n1inv, double* __restrict__ nr, double* __restrict__ diag,
+                                uint8_t* __restrict__ red, double* __restrict__ inv_diag) {
+    const int lane = threadIdx.x & 31;
+    const size_t gw = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5, nw = (size_t(gridDim.x) * blockDim.x) >> 5;
+    constexpr u32 NONE = 0xffffffffu;
+    for (size_t k = gw; k < m; k += nw) {
+        const u32 e0 = pl_off[k], e1 = pl_off[k + 1];
+        double nr_acc = 0.0, dq_acc = 0.0;
+        u32 carry_s = NONE;
+        double carry = 0.0;
+        for (u32 base = e0; base < e1; base += 32) {
+            const u32 e = base + u32(lane);
+            const bool valid = e < e1;
+            const double wv = valid ? (cw ? cw[pl_cell[e]] : 1.0) : 0.0;
+            const u32 s = valid ? pl_seg[e] : NONE;
+            nr_acc += wv;
+            // the run carried from the previous chunk ends here unless this chunk continues it
+            const u32 s0 = __shfl_sync(FULL, s, 0);
+            if (lane == 0 && carry_s != NONE && s0 != carry_s) dq_acc += carry * carry * n1inv[carry_s];
+            // inclusive scan of wv over the lane's run (runs are contiguous: equal segment at
+            // distance d means the whole span is one run)
+            double x = wv;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const double y = __shfl_up_sync(FULL, x, d);
+                const u32 sy = __shfl_up_sync(FULL, s, d);
+                if (lane >= d && sy == s) x += y;
+            }
+            if (valid && s == carry_s) x += carry;  // the run left open by the previous chunk
+            const u32 s_next = __shfl_down_sync(FULL, s, 1);
+            const bool tail = valid && (lane == 31 || s_next != s);
+            const int last = int(min(31u, e1 - 1 - base));
+            const u32 s_last = __shfl_sync(FULL, s, last);
+            const double x_last = __shfl_sync(FULL, x, last);
+            const bool final_chunk = base + 32 >= e1;
+            if (tail && (final_chunk || s != s_last)) dq_acc += x * x * n1inv[s];
+            carry_s = s_last;
+            carry = x_last;
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            nr_acc += __shfl_down_sync(FULL, nr_acc, d);
+            dq_acc += __shfl_down_sync(FULL, dq_acc, d);
+        }
+        if (lane == 0) {
+            const double dg = nr_acc - dq_acc;
+            const bool r = dg <= 1e-12 * nr_acc;
+            nr[k] = nr_acc;
+            diag[k] = dg;
+            red[k] = r ? 1 : 0;
+            inv_diag[k] = (r || !(dg > 0.0)) ? 0.0 : 1.0 / dg;
+        }
+    }
+}
+
+// Sum of a vector into per-CTA partials (fixed tree); the host adds the partials in CTA order.
+__global__ void __launch_bounds__(256) k_vec_sum(const double* __restrict__ v, size_t n, double* __restrict__ part) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (size_t i = size_t(blockIdx.x) * 256 + threadIdx.x; i < n; i += size_t(gridDim.x) * 256) s += v[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+}  // namespace fereg

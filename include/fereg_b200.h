@@ -77,6 +77,12 @@ int fereg_absorber_weights(const fereg_absorber* h, double* out, int* has);
  * positive and finite (else 198), or NULL for ones. */
 int fereg_absorber_set_weights(fereg_absorber* h, const double* w);
 
+/* Absorber::set_weights with the n row-order weights in device memory of the current device:
+ * the weight state (cell weights, n1, n_r, diag(S), redundant coordinates, Jacobi factors) is
+ * computed on the device, as IRLS needs every iteration (glm/irls.rs:367-560). 198 when a weight
+ * is not positive and finite. */
+int fereg_absorber_set_weights_device(fereg_absorber* h, const double* w_dev);
+
 /* Absorber::residualize (absorber.rs:78-86, solve.rs:1141-1311): residualizes the n x r
  * row-major host block z in place. tol: relative W-norm accuracy of each column; maxiter: PCG
  * cap (430 when reached); warm: (m+g1) x r start or NULL; coefs_out: (m+g1) x r or NULL
@@ -204,6 +210,33 @@ typedef struct fereg_boot_out {
 
 int fereg_session_wildboot(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_ols_spec* spec,
                            const fereg_boot_spec* boot, fereg_boot_out* out);
+
+/* Poisson PML by IRLS on the session's fixed effects (glm/irls.rs:367-560, glm/mod.rs with
+ * ppmlhdfe conventions): y >= 0 in column 0 of the n x (1 + nx) row-order block, regressors
+ * after it; every iteration refreshes the weight state on the device and residualizes
+ * [z, X] warm-started from the previous FE coefficients. vce 1 robust (N / (N - 1)), 2 cluster
+ * over the session's cluster dimensions (G / (G - 1), multiway eigenvalue clip). The sample is
+ * taken as prepared (singletons and separated observations already dropped); unweighted
+ * sessions only. 430 when IRLS does not converge within maxiter. */
+typedef struct fereg_glm_spec {
+    int vce;
+    double tol;
+    size_t maxiter;
+    size_t inner_maxiter;
+    int precision; /* FEREG_PREC_* of the FE solves */
+} fereg_glm_spec;
+
+typedef struct fereg_glm_out {
+    double* b;        /* nx; absorbed or collinear regressors 0 */
+    double* V;        /* nx x nx */
+    uint8_t* status;  /* nx: 0 ok, 2 absorbed by the FE, 3 collinear */
+    double N, deviance, ll, chi2, df_m, N_clust;
+    uint64_t iterations, pcg_iterations;
+    int32_t converged;
+} fereg_glm_out;
+
+int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
+                          fereg_glm_out* out);
 
 /* Phase timing of the session's calls: the FEREG_PHASE_SLOTS slots of its absorber, then
  * 9 degrees of freedom, 10 column statistics, 11 Gram, 12 residuals and variance. */

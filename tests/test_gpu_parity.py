@@ -177,3 +177,30 @@ def test_column_counts_match_oracle(case, r):
     y2, b12, q2, s2 = orc.rhs(z)
     assert rel(y1, y2) <= 1e-12 and rel(b11, b12) <= 1e-12
     assert rel(q1, q2) <= 1e-12 and rel(s1, s2) <= 1e-12
+
+
+def test_device_weights_match_oracle(pair):
+    """set_weights_device (the weight state computed on the device) against the oracle's."""
+    import torch
+
+    name, gpu, orc, z = pair
+    rng = np.random.default_rng(17)
+    w = rng.uniform(0.3, 3.0, gpu.n)
+    wd = torch.from_numpy(w).to("cuda")
+    gpu.set_weights_device(wd.data_ptr())
+    orc.set_weights(w)
+    try:
+        a, b = gpu.weight_state(), orc.weight_state()
+        assert np.array_equal(a["redundant"], b["redundant"]), name
+        for key in ("n1", "nr", "diag"):
+            assert rel(a[key], b[key]) <= 1e-12, (name, key)
+        assert abs(a["sw"] - b["sw"]) <= 1e-12 * b["sw"]
+        assert np.array_equal(gpu.weights(), w)
+        z1, z2 = z.copy(), z.copy()
+        gpu.residualize(z1, tol=1e-12, maxiter=100000)
+        orc.residualize(z2, tol=1e-12, maxiter=100000)
+        for j in range(z.shape[1]):
+            assert rel(z1[:, j], z2[:, j]) <= 1e-9, (name, j)
+    finally:
+        gpu.set_weights(None)
+        orc.set_weights(None)
