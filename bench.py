@@ -43,6 +43,10 @@ CONFIGS = {
     # WCR11 wild cluster bootstrap of b_x1 (H0 true): y ~ x1 | indiv + year + firm, cluster firm,
     # n = 1e5 indiv x 10 years, firm random in 2e4, 9,999 Rademacher draws (seed 1).
     "c3": dict(n_ind=100_000, years=10, n_firm=20_000, k=1, seed=10**6 * 100 + 44, reps=9_999),
+    # Poisson PML (gravity): trade ~ x1 + log dist | exporter#year + importer#year + pair, 200
+    # countries x 50 years, 39,800 directed pairs x 5 rows (sectors) per pair-year, ~40% zeros,
+    # robust SEs.
+    "c4": dict(countries=200, years=50, sectors=5, seed=10**7 * 100 + 45, zero_share=0.40),
 }
 TOL = 1e-8
 METRIC = "sec/call (1e7-obs 3-FE OLS)"
@@ -98,6 +102,137 @@ def make_boot_data(cfg):
         rng.standard_normal(n_firm)[firm] + rng.standard_normal(n)
     rows = np.column_stack([y, x1])
     return [ind, year, firm], [n_ind, years, int(firm.max()) + 1], firm, rows
+
+
+def make_gravity_data(cfg):
+    """Synthetic C4 gravity panel (seeded numpy): rows ordered pair-major; FE codes
+    exporter#year, importer#year, pair; y ~ Poisson(exp(0.5 x1 - 0.2 log dist + effects + c)) with
+    c set so that about 40% of y are 0; effects ~ N(0, 0.5^2)."""
+    C, T, S = cfg["countries"], cfg["years"], cfg["sectors"]
+    rng = np.random.default_rng(cfg["seed"])
+    ex, im = np.meshgrid(np.arange(C), np.arange(C), indexing="ij")
+    off = ex != im
+    ex, im = ex[off], im[off]
+    P = len(ex)
+    pair = np.repeat(np.arange(P), T * S)
+    year = np.tile(np.repeat(np.arange(T), S), P)
+    e_i, i_i = ex[pair], im[pair]
+    ey = (e_i * T + year).astype(np.uint32)
+    iy = (i_i * T + year).astype(np.uint32)
+    n = len(pair)
+    ldist = rng.uniform(np.log(100.0), np.log(2e4), P)[pair]
+    x1 = rng.standard_normal(n)
+    lin = 0.5 * x1 - 0.2 * ldist + rng.normal(0, 0.5, C * T)[ey] + rng.normal(0, 0.5, C * T)[iy] + \
+        rng.normal(0, 0.5, P)[pair]
+    # intercept for ~40% zeros: P(y = 0) = mean exp(-exp(lin + c))
+    lo, hi = -20.0, 20.0
+    for _ in range(60):
+        c = 0.5 * (lo + hi)
+        if np.mean(np.exp(-np.exp(lin + c))) > cfg["zero_share"]:
+            lo = c
+        else:
+            hi = c
+    y = rng.poisson(np.exp(lin + c)).astype(float)
+    for codes in (ey, iy, pair):  # no FE group may be all zero (the `fe` separation rule)
+        assert np.all(np.bincount(codes, weights=y) > 0)
+    rows = np.column_stack([y, x1, ldist])
+    return [ey, iy, pair.astype(np.uint32)], [C * T, C * T, P], rows
+
+
+GLM_METRIC = "sec/call (Poisson PML, n=9.95e6, exporter#year + importer#year + pair, robust SEs)"
+
+
+def run_glm(args, cfg, rank, world, local, pg):
+    """C4: one PPML IRLS call per step (seconds per call)."""
+    codes, g, rows = make_gravity_data(cfg)
+    n = rows.shape[0]
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import oracle
+
+        ab = oracle.Absorber(codes, g)
+        rng = np.random.default_rng(1)
+        w = rng.uniform(0.5, 2.0, n)
+        ab.set_weights(w)
+        z = np.ascontiguousarray(rows[ab.row_order()])
+        ts = []
+        for _ in range(2):
+            zz = z.copy()
+            t0 = time.perf_counter()
+            ab.residualize(zz, tol=1e-8)
+            ts.append(time.perf_counter() - t0)
+        per_it = float(np.mean(ts))
+        iters = 12
+        v = per_it * iters
+        line = {"impl": "reference", "metric": GLM_METRIC, "value": v, "unit": "s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": "c4", "n": n},
+                "cpu_baseline": {"value": v, "unit": "s", "cores": oracle.max_threads(), "kind": "port",
+                                 "sample": f"one weighted FE solve of [z, x1, ldist] ({per_it:.3f} s, C++ FP64 "
+                                           f"restatement, all host threads) times {iters} IRLS iterations"},
+                "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+
+    import fereg_b200 as fb
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    sess = fb.Session(codes, g)
+    prepare_s = time.perf_counter() - t0
+    rows = np.ascontiguousarray(rows[sess.row_order()])
+    prec = fb.PREC_F64 if args.precision == "f64" else fb.PREC_F32_REFINED
+    stream = torch.cuda.ExternalStream(sess.stream(), device=device)
+    src = torch.from_numpy(rows).to(device)
+    pinned = torch.empty(rows.shape, dtype=torch.float64, pin_memory=True)
+    host = pinned.numpy()
+    np.copyto(host, rows)
+
+    def step(on_device):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = sess.poisson(src.data_ptr() if on_device else host, vce="robust", tol=1e-8, precision=prec,
+                           on_device=on_device, nx=2)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, res
+
+    for _ in range(args.warmup):
+        step(True)
+    barrier(pg)
+    sess.set_profiling(True)
+    l0 = sess.launches()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            dt, res = step(True)
+            times.append(dt)
+    launches = sess.launches() - l0
+    phases = sess.phase_times()
+    sess.set_profiling(False)
+    step_s = max_over_ranks(float(np.mean(times)), pg, device)
+    e2e = None
+    if not args.no_e2e:
+        e2e = max_over_ranks(float(np.mean([step(False)[0] for _ in range(2)])), pg, device) / world
+    if rank == 0:
+        line = {"metric": GLM_METRIC, "value": step_s / world, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if prec == fb.PREC_F64 else "f32+f64", "data": "synthetic",
+                "config": {"workload": "c4", "n": n, "irls_iterations": res["iterations"],
+                           "pcg_iterations": res["pcg_iterations"], "b_x1": float(res["b"][0]),
+                           "status": [int(x) for x in res["status"]], "zero_share": float(np.mean(rows[:, 0] == 0)),
+                           "prepare_s": prepare_s, "precision": args.precision,
+                           "parallelism": f"replicas x{world}"},
+                "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
+                "clocks": clk.summary(),
+                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": n * 3 * 8, "d2h_bytes_per_step": 96},
+                "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    sess.close()
 
 
 BOOT_METRIC = "wild-boot reps/s (WCR11, 9,999 Rademacher draws, n=1e6, 3 FE, cluster firm 2e4)"
@@ -395,8 +530,8 @@ def main():
     args.warmup = max(3, args.warmup)
     cfg = CONFIGS[args.config]
     rank, world, local, pg = dist_setup()
-    if args.config == "c3":
-        run_boot(args, cfg, rank, world, local, pg)
+    if args.config in ("c3", "c4"):
+        (run_boot if args.config == "c3" else run_glm)(args, cfg, rank, world, local, pg)
         if pg is not None:
             barrier(pg)
             pg.destroy_process_group()
