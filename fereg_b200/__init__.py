@@ -64,7 +64,22 @@ class BootOut(C.Structure):
 
 class GlmSpec(C.Structure):
     _fields_ = [("vce", C.c_int), ("tol", C.c_double), ("maxiter", C.c_size_t), ("inner_maxiter", C.c_size_t),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("family", C.c_int)]
+
+
+class IvSpec(C.Structure):
+    _fields_ = [("vce", C.c_int), ("tol", C.c_double), ("maxiter", C.c_size_t), ("precision", C.c_int)]
+
+
+class IvOut(C.Structure):
+    _fields_ = ([("b", C.POINTER(C.c_double)), ("V", C.POINTER(C.c_double)), ("status", C.POINTER(C.c_uint8))]
+                + [(k, C.c_double) for k in ("N", "df_r", "df_m", "df_a", "sdofminus", "rss", "rmse", "F",
+                                             "N_clust", "ic")]
+                + [("endog_ct", C.c_int32), ("inexog_ct", C.c_int32), ("exexog_ct", C.c_int32)])
+
+
+FAMILY_POISSON = 1
+FAMILY_LOGIT = 2
 
 
 class GlmOut(C.Structure):
@@ -128,6 +143,9 @@ def _setup(L):
     L.fereg_session_set_profiling.argtypes = [P, C.c_int]
     L.fereg_session_info.argtypes = [P, u64p]
     L.fereg_session_poisson.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(GlmSpec), C.POINTER(GlmOut)]
+    L.fereg_session_iv.argtypes = [P, P, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(IvSpec),
+                                   C.POINTER(IvOut)]
+    L.fereg_session_glm.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(GlmSpec), C.POINTER(GlmOut)]
     L.fereg_session_wildboot.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(OlsSpec), C.POINTER(BootSpec),
                                          C.POINTER(BootOut)]
     L.fereg_session_phase_times.argtypes = [P, f64p, u64p]
@@ -413,10 +431,42 @@ class Session:
         return dict(stat=out.stat, se=out.se, point=out.point, pvalue=out.pvalue, reps=int(out.reps),
                     full_enum=bool(out.full_enum), t_boot=t[: int(out.reps)].copy())
 
+    def iv(self, rows, nx, nendog, ninst, vce="unadjusted", tol=1e-8, maxiter=16000, precision=PREC_F64,
+           on_device=False):
+        """2SLS of column 0 on [exog (nx), endog (nendog)] with instruments [inst (ninst), exog]:
+        the n x (1 + nx + nendog + ninst) block [y, exog, endog, inst] in row order (host array,
+        or a device pointer with on_device=True). b and V are in the order [endog, exog]."""
+        if on_device:
+            ptr = rows
+        else:
+            assert rows.dtype == np.float64 and rows.flags.c_contiguous
+            assert rows.shape[1] == 1 + nx + nendog + ninst
+            ptr = rows.ctypes.data
+        k = nendog + nx
+        b = np.zeros(max(1, k))
+        V = np.zeros((max(1, k), max(1, k)))
+        status = np.zeros(max(1, nx + nendog + ninst), dtype=np.uint8)
+        spec = IvSpec({"unadjusted": 0, "robust": 1, "cluster": 2}[vce], tol, maxiter, precision)
+        out = IvOut(_p(b, f64p), _p(V, f64p), _p(status, u8p))
+        _check(lib().fereg_session_iv(self.h, P(ptr), int(on_device), nx, nendog, ninst, C.byref(spec),
+                                      C.byref(out)))
+        sc = {k_: getattr(out, k_) for k_ in ("N", "df_r", "df_m", "df_a", "sdofminus", "rss", "rmse", "F",
+                                               "N_clust", "ic", "endog_ct", "inexog_ct", "exexog_ct")}
+        return dict(b=b[:k], V=V[:k, :k], status=status[: nx + nendog + ninst], scalars=sc)
+
     def poisson(self, rows, vce="robust", tol=1e-8, maxiter=10000, inner_maxiter=16000, precision=PREC_F64,
                 on_device=False, nx=None):
         """Poisson PML of column 0 (y >= 0) on the other columns of the n x (1 + nx) block (row
         order; host array, or a device pointer with on_device=True)."""
+        return self.glm(rows, "poisson", vce, tol, maxiter, inner_maxiter, precision, on_device, nx)
+
+    def logit(self, rows, vce="oim", tol=1e-8, maxiter=10000, inner_maxiter=16000, precision=PREC_F64,
+              on_device=False, nx=None):
+        """Logit of column 0 (y in {0, 1}) on the other columns, as `poisson`."""
+        return self.glm(rows, "logit", vce, tol, maxiter, inner_maxiter, precision, on_device, nx)
+
+    def glm(self, rows, family, vce="robust", tol=1e-8, maxiter=10000, inner_maxiter=16000, precision=PREC_F64,
+            on_device=False, nx=None):
         if on_device:
             ptr = rows
             assert nx is not None
@@ -427,9 +477,10 @@ class Session:
         b = np.zeros(max(1, nx))
         V = np.zeros((max(1, nx), max(1, nx)))
         status = np.zeros(max(1, nx), dtype=np.uint8)
-        spec = GlmSpec({"robust": 1, "cluster": 2}[vce], tol, maxiter, inner_maxiter, precision)
+        fam = {"poisson": FAMILY_POISSON, "logit": FAMILY_LOGIT}[family]
+        spec = GlmSpec({"oim": 0, "robust": 1, "cluster": 2}[vce], tol, maxiter, inner_maxiter, precision, fam)
         out = GlmOut(_p(b, f64p), _p(V, f64p), _p(status, u8p))
-        _check(lib().fereg_session_poisson(self.h, P(ptr), int(on_device), nx, C.byref(spec), C.byref(out)))
+        _check(lib().fereg_session_glm(self.h, P(ptr), int(on_device), nx, C.byref(spec), C.byref(out)))
         return dict(b=b[:nx], V=V[:nx, :nx], status=status[:nx], N=out.N, deviance=out.deviance, ll=out.ll,
                     chi2=out.chi2, df_m=out.df_m, N_clust=out.N_clust, iterations=int(out.iterations),
                     pcg_iterations=int(out.pcg_iterations), converged=bool(out.converged))

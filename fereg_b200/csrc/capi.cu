@@ -380,14 +380,51 @@ int fereg_session_wildboot(fereg_session* s, double* rows, int rows_on_device, s
     });
 }
 
-int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
-                          fereg_glm_out* out) {
+int fereg_session_iv(fereg_session* s, double* rows, int rows_on_device, size_t nx, size_t nendog, size_t ninst,
+                     const fereg_iv_spec* spec, fereg_iv_out* out) {
     return guard([&] {
-        if (!s || !rows || !spec || !out) throw Error(RC_INVALID_INPUT, "fereg_session_poisson: NULL argument");
-        if (spec->vce != 1 && spec->vce != 2) throw Error(RC_INVALID_INPUT, "fereg_session_poisson: vce is 1 or 2");
+        if (!s || !rows || !spec || !out) throw Error(RC_INVALID_INPUT, "fereg_session_iv: NULL argument");
+        if (spec->vce < 0 || spec->vce > 2) throw Error(RC_INVALID_INPUT, "fereg_session_iv: vce is 0, 1 or 2");
         if (spec->precision != FEREG_PREC_F64 && spec->precision != FEREG_PREC_F32_REFINED)
-            throw Error(RC_INVALID_INPUT, "fereg_session_poisson: unknown precision");
+            throw Error(RC_INVALID_INPUT, "fereg_session_iv: unknown precision");
+        GpuSession::IvSpec is;
+        is.vce = spec->vce;
+        is.tol = spec->tol;
+        is.maxiter = spec->maxiter;
+        is.prec = spec->precision == FEREG_PREC_F32_REFINED ? Precision::F32_REFINED : Precision::F64;
+        GpuSession::IvOut io;
+        io.b = out->b;
+        io.V = out->V;
+        io.status = out->status;
+        s->s.iv(rows, rows_on_device != 0, nx, nendog, ninst, is, io);
+        out->N = io.N;
+        out->df_r = io.df_r;
+        out->df_m = io.df_m;
+        out->df_a = io.df_a;
+        out->sdofminus = io.sdofminus;
+        out->rss = io.rss;
+        out->rmse = io.rmse;
+        out->F = io.F;
+        out->N_clust = io.N_clust;
+        out->ic = io.ic;
+        out->endog_ct = io.endog_ct;
+        out->inexog_ct = io.inexog_ct;
+        out->exexog_ct = io.exexog_ct;
+    });
+}
+
+static int session_glm(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
+                       fereg_glm_out* out, int family) {
+    return guard([&] {
+        if (!s || !rows || !spec || !out) throw Error(RC_INVALID_INPUT, "fereg_session_glm: NULL argument");
+        if (family != FEREG_FAMILY_POISSON && family != FEREG_FAMILY_LOGIT)
+            throw Error(RC_INVALID_INPUT, "fereg_session_glm: family is Poisson or logit");
+        if (spec->vce != 1 && spec->vce != 2 && !(spec->vce == 0 && family == FEREG_FAMILY_LOGIT))
+            throw Error(RC_INVALID_INPUT, "fereg_session_glm: vce is 1 or 2 (0 for logit)");
+        if (spec->precision != FEREG_PREC_F64 && spec->precision != FEREG_PREC_F32_REFINED)
+            throw Error(RC_INVALID_INPUT, "fereg_session_glm: unknown precision");
         GpuSession::GlmSpec gs;
+        gs.family = family == FEREG_FAMILY_LOGIT ? 1 : 0;
         gs.vce = spec->vce;
         gs.tol = spec->tol;
         gs.maxiter = spec->maxiter;
@@ -397,7 +434,7 @@ int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, si
         go.b = out->b;
         go.V = out->V;
         go.status = out->status;
-        s->s.poisson(rows, rows_on_device != 0, nx, gs, go);
+        s->s.glm(rows, rows_on_device != 0, nx, gs, go);
         out->N = go.N;
         out->deviance = go.deviance;
         out->ll = go.ll;
@@ -408,6 +445,16 @@ int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, si
         out->pcg_iterations = go.pcg_iterations;
         out->converged = go.converged ? 1 : 0;
     });
+}
+
+int fereg_session_glm(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
+                      fereg_glm_out* out) {
+    return session_glm(s, rows, rows_on_device, nx, spec, out, spec ? spec->family : 0);
+}
+
+int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
+                          fereg_glm_out* out) {
+    return session_glm(s, rows, rows_on_device, nx, spec, out, FEREG_FAMILY_POISSON);
 }
 
 int fereg_session_set_profiling(fereg_session* s, int on) {

@@ -19,6 +19,7 @@ enum Rc : int {
     RC_INTERRUPTED = 1,
     RC_INVALID_INPUT = 198,
     RC_CONVERGENCE = 430,
+    RC_NOT_IDENTIFIED = 481,
     RC_OUT_OF_MEMORY = 909,
     RC_TOO_FEW_OBS = 2001,
     RC_INTERNAL = 9999,

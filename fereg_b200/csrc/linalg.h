@@ -94,6 +94,53 @@ inline Mat mul(const Mat& a, const Mat& b, size_t k) {
     return out;
 }
 
+// Inverse of a symmetric positive definite matrix by its Cholesky factor L L^T (the 2SLS cross
+// products, iv.rs dense::spd_inv); false when a pivot is not positive.
+inline bool spd_inv(const Mat& a, size_t k, Mat& out) {
+    Mat l(k * k, 0.0);
+    for (size_t j = 0; j < k; j++) {
+        double d = a[j * k + j];
+        for (size_t p = 0; p < j; p++) d -= l[j * k + p] * l[j * k + p];
+        if (!(d > 0.0)) return false;
+        const double ljj = std::sqrt(d);
+        l[j * k + j] = ljj;
+        for (size_t i = j + 1; i < k; i++) {
+            double s = a[i * k + j];
+            for (size_t p = 0; p < j; p++) s -= l[i * k + p] * l[j * k + p];
+            l[i * k + j] = s / ljj;
+        }
+    }
+    // L^-1 by forward substitution, then (L^-1)^T L^-1
+    Mat li(k * k, 0.0);
+    for (size_t c = 0; c < k; c++) {
+        li[c * k + c] = 1.0 / l[c * k + c];
+        for (size_t i = c + 1; i < k; i++) {
+            double s = 0.0;
+            for (size_t p = c; p < i; p++) s -= l[i * k + p] * li[p * k + c];
+            li[i * k + c] = s / l[i * k + i];
+        }
+    }
+    out.assign(k * k, 0.0);
+    for (size_t i = 0; i < k; i++)
+        for (size_t j = 0; j <= i; j++) {
+            double s = 0.0;
+            for (size_t p = i; p < k; p++) s += li[p * k + i] * li[p * k + j];
+            out[i * k + j] = out[j * k + i] = s;
+        }
+    return true;
+}
+
+// Row-major product of an m x p and a p x q matrix.
+inline Mat mul_rect(const Mat& a, const Mat& b, size_t m, size_t p, size_t q) {
+    Mat out(m * q, 0.0);
+    for (size_t i = 0; i < m; i++)
+        for (size_t l = 0; l < p; l++) {
+            const double x = a[i * p + l];
+            for (size_t j = 0; j < q; j++) out[i * q + j] += x * b[l * q + j];
+        }
+    return out;
+}
+
 // scale * bread * meat * bread, symmetrized.
 inline Mat sandwich(const Mat& bread, const Mat& meat, size_t k, double scale) {
     Mat v = mul(mul(bread, meat, k), bread, k);

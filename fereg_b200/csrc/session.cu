@@ -339,6 +339,53 @@ std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, 
     return m;
     }
 
+// Column statistics of the raw rows (stats.rs:40) in one device pass about each column's first
+// value: sd (unweighted, floored at 1e-3), weighted mean, sum of squares, weighted centered and
+// uncentered sums of squares.
+GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
+    SessionDev& d = *d_;
+    cudaStream_t st = d.st;
+    const size_t n = n_, r = size_t(R);
+    const double* wr = wk_.empty() ? nullptr : d.w_raw.p;
+    const double sumw = sumw_;
+    d.part.alloc(size_t(ST_GRID) * r * 6);
+    d.sums.alloc(r * 6);
+    for (int j0 = 0; j0 < R; j0 += 32) {
+        const int Rc = std::min(32, R - j0);
+        switch (rcp_of(Rc)) {
+            case 1: k_colstats1<1><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 2: k_colstats1<2><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 4: k_colstats1<4><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 8: k_colstats1<8><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 16: k_colstats1<16><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            default: k_colstats1<32><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+        }
+        d.launches++;
+    }
+    k_sum_parts<<<(R * 6 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 6, d.sums.p);
+    d.launches++;
+    std::vector<double> s1(r * 6), c0(r);
+    CK(cudaMemcpyAsync(s1.data(), d.sums.p, r * 6 * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c0.data(), rows, r * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    ColStats cs;
+    cs.wmean.resize(r);
+    cs.sumsq.resize(r);
+    cs.wss_unc.resize(r);
+    cs.sd.resize(r);
+    cs.wss.resize(r);
+    for (size_t j = 0; j < r; j++) {
+        const double* a = s1.data() + j * 6;
+        const double m2 = std::max(0.0, a[1] - a[0] * a[0] / double(n));
+        cs.sd[j] = std::max(std::sqrt(m2 / (double(n) - 1.0)), 1e-3);
+        cs.wmean[j] = c0[j] + a[2] / sumw;
+        cs.wss[j] = std::max(0.0, a[3] - a[2] * a[2] / sumw);
+        cs.sumsq[j] = a[4];
+        cs.wss_unc[j] = a[5];
+    }
+    return cs;
+}
+
 void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out) {
     SessionDev& d = *d_;
     cudaStream_t st = d.st;
@@ -368,38 +415,8 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     ph = d.begin(S_COLSTATS);
 
     // Pass A: column statistics of the raw rows (stats.rs:40), raw weights, in one device pass
-    // about each column's first value
-    const double* wr = weighted ? d.w_raw.p : nullptr;
-    d.part.alloc(size_t(ST_GRID) * r * 6);
-    d.sums.alloc(r * 6);
-    for (int j0 = 0; j0 < R; j0 += 32) {
-    const int Rc = std::min(32, R - j0);
-    switch (rcp_of(Rc)) {
-        case 1: k_colstats1<1><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-        case 2: k_colstats1<2><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-        case 4: k_colstats1<4><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-        case 8: k_colstats1<8><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-        case 16: k_colstats1<16><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-        default: k_colstats1<32><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-    }
-    d.launches++;
-    }
-    k_sum_parts<<<(R * 6 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 6, d.sums.p);
-    d.launches++;
-    std::vector<double> s1(r * 6), c0(r);
-    CK(cudaMemcpyAsync(s1.data(), d.sums.p, r * 6 * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(c0.data(), rows, r * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    std::vector<double> wmean(r), sumsq(r), wss_unc(r), sd(r), wss(r);
-    for (size_t j = 0; j < r; j++) {
-    const double* a = s1.data() + j * 6;
-    const double m2 = std::max(0.0, a[1] - a[0] * a[0] / double(n));
-    sd[j] = std::max(std::sqrt(m2 / (double(n) - 1.0)), 1e-3);
-    wmean[j] = c0[j] + a[2] / sumw;
-    wss[j] = std::max(0.0, a[3] - a[2] * a[2] / sumw);
-    sumsq[j] = a[4];
-    wss_unc[j] = a[5];
-    }
+    const ColStats cs = column_stats(rows, R);
+    const std::vector<double>&wmean = cs.wmean, &sumsq = cs.sumsq, &wss_unc = cs.wss_unc, &sd = cs.sd, &wss = cs.wss;
     const double tscale = (kind == 1 || kind == 3) ? double(n) / sumw : 1.0;
     const double tss_y = (has_intercept ? wss[0] : wss_unc[0]) * tscale;
     d.end(ph);
@@ -689,6 +706,217 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
 
 
 // ---------------------------------------------------------------------------------------------
+// IV / 2SLS with ivreghdfe conventions (iv.rs:299-700: ivreg2 on the residualized block with
+// `small` and `noconstant`, sdofminus = max(df_a, 1)). The block is [y, exog (nx), endog (ne),
+// inst (ni)] in row order, residualized in ONE absorber call (iv.rs:409); the weighted Gram of
+// the residualized block is the only other pass over all columns. Collinearity: stage 1 (absorbed
+// by the FE) on every column, stage 2 on Z = [exog, inst] and then on X = [exog, endog]. With
+// X = [endog, exog], Z = [inst, exog] (the coefficient order of e(b)):
+//   b = (X'P_Z X)^-1 X'Z (Z'Z)^-1 Z'y,  B = (X'P_Z X)^-1 X'Z (Z'Z)^-1,
+//   unadjusted V = rss / (N - K - sdof) (X'P_Z X)^-1,
+//   robust V = B [sum m_i z_i z_i'] B' N / (N - K - sdof) (m_i the reghdfe robust multiplier),
+//   cluster V = B [sum_g s_g s_g'] B' (N - 1) / (N - K - sdof) G / (G - 1), s_g = sum e w_v z,
+// multiway by inclusion-exclusion without an eigenvalue clip (iv.rs:612-640).
+void GpuSession::iv(double* rows_in, bool on_device, size_t nx, size_t ne, size_t ni, const IvSpec& spec,
+                    IvOut& out) {
+    SessionDev& d = *d_;
+    cudaStream_t st = d.st;
+    const size_t n = n_, r = 1 + nx + ne + ni;
+    const int R = int(r);
+    if (tg_.empty()) throw Error(RC_INVALID_INPUT, "fereg iv: the session absorbs no fixed effects");
+    if (ne == 0) throw Error(RC_INVALID_INPUT, "fereg iv: no endogenous regressor");
+    if (r + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg iv: at most 62 columns on the device path");
+    double* rows = rows_in;
+    if (!on_device) {
+        d.rows.alloc(n * r);
+        CK(cudaMemcpyAsync(d.rows.p, rows_in, n * r * 8, cudaMemcpyHostToDevice, st));
+        rows = d.rows.p;
+    }
+    const int kind = kind_;
+    const bool weighted = !wk_.empty();
+    const double bigN = kind == 2 ? sumw_ : double(n);
+    int vce = spec.vce;
+    if (vce == 0 && kind == 3) vce = 1;  // pweights imply robust
+    if (vce == 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg iv: cluster variance without clusters");
+
+    int ph = d.begin(S_DOF);
+    const Dof dof = estimate_dof(vce == 2, false, false);
+    d.end(ph);
+    ph = d.begin(S_COLSTATS);
+    const ColStats cs = column_stats(rows, R);
+    d.end(ph);
+    const SolveInfo info = ab_->residualize_device(rows, r, spec.tol, spec.maxiter, false, nullptr, nullptr, spec.prec);
+    ph = d.begin(S_GRAM);
+    const double* wv = weighted ? d.wv.p : nullptr;
+    std::vector<int> all(r);
+    std::iota(all.begin(), all.end(), 0);
+    std::vector<double> ss_res;
+    const std::vector<double> g = outer_products(rows, n, R, all, nullptr, false, wv, nullptr, true, &ss_res);
+    d.end(ph);
+
+    // collinearity (iv.rs:443-490)
+    const double ctol = std::min(1e-6, spec.tol / 10.0);
+    std::vector<uint8_t> status(r - 1, 0);
+    for (size_t j = 1; j < r; j++)
+        if (ss_res[j] / cs.sumsq[j] <= ctol) status[j - 1] = 2;
+    auto alive = [&](size_t c) { return status[c - 1] == 0; };
+    auto stage2 = [&](const std::vector<size_t>& cand) {
+        const size_t kc = cand.size();
+        la::Mat gs(kc * kc);
+        for (size_t a = 0; a < kc; a++)
+            for (size_t b = 0; b < kc; b++)
+                gs[a * kc + b] = g[cand[a] * r + cand[b]] / (cs.sd[cand[a]] * cs.sd[cand[b]]);
+        std::vector<bool> dropped;
+        la::sweep_inverse(gs, kc, SWEEP_TOL, false, dropped);
+        for (size_t c = 0; c < kc; c++)
+            if (dropped[c]) status[cand[c] - 1] = 3;
+    };
+    auto exog = [&](size_t j) { return 1 + j; };
+    auto endog = [&](size_t j) { return 1 + nx + j; };
+    auto inst = [&](size_t j) { return 1 + nx + ne + j; };
+    std::vector<size_t> zc, xc;
+    for (size_t j = 0; j < nx; j++)
+        if (alive(exog(j))) zc.push_back(exog(j));
+    for (size_t j = 0; j < ni; j++)
+        if (alive(inst(j))) zc.push_back(inst(j));
+    stage2(zc);
+    for (size_t j = 0; j < nx; j++)
+        if (alive(exog(j))) xc.push_back(exog(j));
+    for (size_t j = 0; j < ne; j++)
+        if (alive(endog(j))) xc.push_back(endog(j));
+    stage2(xc);
+    std::vector<size_t> en, ex, iz;
+    for (size_t j = 0; j < ne; j++)
+        if (alive(endog(j))) en.push_back(endog(j));
+    for (size_t j = 0; j < nx; j++)
+        if (alive(exog(j))) ex.push_back(exog(j));
+    for (size_t j = 0; j < ni; j++)
+        if (alive(inst(j))) iz.push_back(inst(j));
+    if (iz.size() < en.size())
+        throw Error(RC_NOT_IDENTIFIED,
+                    "equation not identified; must have at least as many instruments not in the regression as there "
+                    "are instrumented variables");
+    std::vector<size_t> xcols(en), zcols(iz);
+    xcols.insert(xcols.end(), ex.begin(), ex.end());
+    zcols.insert(zcols.end(), ex.begin(), ex.end());
+    const size_t k = xcols.size(), l = zcols.size();
+    if (k == 0) throw Error(RC_INVALID_INPUT, "fereg iv: every regressor was dropped");
+
+    // cross products and 2SLS (s_crossprods, s_gmm1s)
+    la::Mat xz(k * l), zz(l * l), zy(l);
+    for (size_t a = 0; a < k; a++)
+        for (size_t b = 0; b < l; b++) xz[a * l + b] = g[xcols[a] * r + zcols[b]];
+    for (size_t a = 0; a < l; a++) {
+        zy[a] = g[zcols[a] * r];
+        for (size_t b = 0; b < l; b++) zz[a * l + b] = g[zcols[a] * r + zcols[b]];
+    }
+    la::Mat zzinv, xpzx_inv;
+    if (!la::spd_inv(zz, l, zzinv)) throw Error(RC_INVALID_INPUT, "fereg iv: Z'Z is not positive definite");
+    const la::Mat xz_zzinv = la::mul_rect(xz, zzinv, k, l, l);
+    la::Mat xzt(l * k);
+    for (size_t a = 0; a < k; a++)
+        for (size_t b = 0; b < l; b++) xzt[b * k + a] = xz[a * l + b];
+    la::Mat xpzx = la::mul_rect(xz_zzinv, xzt, k, l, k);
+    la::symmetrize(xpzx, k);
+    if (!la::spd_inv(xpzx, k, xpzx_inv)) throw Error(RC_INVALID_INPUT, "fereg iv: X'P_Z X is not positive definite");
+    const la::Mat bmat = la::mul_rect(xpzx_inv, xz_zzinv, k, k, l);
+    const la::Mat beta = la::mul_rect(bmat, zy, k, l, 1);
+
+    // residuals and their weighted sum of squares
+    ph = d.begin(S_VARIANCE);
+    std::vector<int> kx(xcols.begin(), xcols.end()), kz(zcols.begin(), zcols.end());
+    d.col.alloc(std::max(k, l) + 1);
+    d.beta.alloc(k + 1);
+    CK(cudaMemcpyAsync(d.col.p, kx.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
+    d.e.alloc(n);
+    d.part.alloc(ST_GRID);
+    d.sums.alloc(1);
+    k_resid_e<<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, d.col.p, d.beta.p, int(k), 0, wv, d.e.p, d.part.p);
+    k_sum_parts<<<1, 32, 0, st>>>(d.part.p, ST_GRID, 1, d.sums.p);
+    d.launches += 2;
+    double rss = 0.0;
+    CK(cudaMemcpyAsync(&rss, d.sums.p, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+
+    const double sdof = std::max<double>(double(dof.df_a), 1.0);
+    const double nk = bigN - double(k) - sdof;
+    const double g_min = cg_.empty() ? 0.0 : double(*std::min_element(cg_.begin(), cg_.end()));
+    la::Mat V(k * k, 0.0);
+    if (vce == 0) {
+        for (size_t i = 0; i < k * k; i++) V[i] = xpzx_inv[i] * (rss / nk);
+    } else {
+        d.om.alloc(n);
+        k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, vce == 2 ? 1 : 0, d.om.p);
+        d.launches++;
+        la::Mat S(l * l, 0.0);
+        if (vce == 1) {
+            S = outer_products(rows, n, R, kz, nullptr, false, d.om.p, nullptr, false, nullptr);
+        } else {
+            for (auto& sub : d.subsets) {
+                CK(cudaMemcpyAsync(d.col.p, kz.data(), l * sizeof(int), cudaMemcpyHostToDevice, st));
+                d.S.alloc(size_t(sub.G) * l);
+                k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(rows, R, d.col.p, nullptr, int(l), 0, d.om.p, sub.perm.p,
+                                                           sub.coff.p, sub.G, d.S.p);
+                d.launches++;
+                std::vector<int> sc(l);
+                std::iota(sc.begin(), sc.end(), 0);
+                const la::Mat part = outer_products(d.S.p, sub.G, int(l), sc, nullptr, false, nullptr, nullptr, false,
+                                                    nullptr);
+                for (size_t i = 0; i < l * l; i++) S[i] += sub.sign * part[i];
+            }
+        }
+        la::Mat bt(l * k);
+        for (size_t a = 0; a < k; a++)
+            for (size_t b = 0; b < l; b++) bt[b * k + a] = bmat[a * l + b];
+        V = la::mul_rect(la::mul_rect(bmat, S, k, l, l), bt, k, l, k);
+        la::symmetrize(V, k);
+        const double adj = vce == 2 ? (bigN - 1.0) / (bigN - double(k) - sdof) * g_min / (g_min - 1.0) : bigN / nk;
+        for (double& x : V) x *= adj;
+    }
+    d.end(ph);
+    d.collect();
+
+    // Wald F of all coefficients (greedy sweep of V)
+    double f_stat = nanv();
+    {
+        std::vector<bool> dv;
+        const la::Mat vi = la::sweep_inverse(V, k, F_SWEEP_TOL, true, dv);
+        if (std::none_of(dv.begin(), dv.end(), [](bool x) { return x; })) {
+            double q = 0.0;
+            for (size_t a = 0; a < k; a++)
+                for (size_t b = 0; b < k; b++) q += beta[a] * vi[a * k + b] * beta[b];
+            f_stat = finite_or_nan(q / double(k));
+        }
+    }
+    // results in e(b) order [endog..., exog...]
+    const size_t k_all = ne + nx;
+    auto pos = [&](size_t c) { return c > nx ? c - 1 - nx : ne + (c - 1); };
+    if (out.b) std::fill(out.b, out.b + k_all, 0.0);
+    if (out.V) std::fill(out.V, out.V + k_all * k_all, 0.0);
+    for (size_t a = 0; a < k; a++) {
+        if (out.b) out.b[pos(xcols[a])] = beta[a];
+        if (out.V)
+            for (size_t b = 0; b < k; b++) out.V[pos(xcols[a]) * k_all + pos(xcols[b])] = V[a * k + b];
+    }
+    if (out.status) std::copy(status.begin(), status.end(), out.status);
+    out.N = bigN;
+    out.df_m = double(k);
+    out.df_r = vce == 2 ? g_min - 1.0 : nk;
+    out.df_a = double(dof.df_a);
+    out.sdofminus = sdof;
+    out.rss = rss;
+    out.rmse = std::sqrt(rss / nk);
+    out.F = f_stat;
+    out.N_clust = vce == 2 ? g_min : nanv();
+    out.ic = double(info.iterations);
+    out.endog_ct = int(en.size());
+    out.inexog_ct = int(ex.size());
+    out.exexog_ct = int(iz.size());
+    CK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------------------
 // Wild cluster bootstrap WCR11 of coefficient bs.coef (H0: beta = r0): Rademacher weights on
 // the clusters of the session's first cluster dimension, restricted residuals (impose_null),
 // CRV1 over all the session's cluster dimensions, two-tailed p-value
@@ -853,8 +1081,8 @@ void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec
 }
 
 // ---------------------------------------------------------------------------------------------
-// Poisson PML by IRLS (glm/irls.rs:367-560 with ppmlhdfe conventions, glm/mod.rs:1053-1140 for
-// the variance). Each iteration: w = mu and z = eta - 1 + y / mu (device), the weight state
+// GLM by IRLS, Poisson PML or logit (glm/irls.rs:367-560 with ppmlhdfe conventions,
+// glm/mod.rs:1053-1140 for the variance). Each iteration: the family's w and z (device), the weight state
 // refreshed on the device, [z, X] residualized warm-started from the previous FE coefficients at
 // an inner tolerance tightened toward max(1e-12, 0.1 tol), the weighted regression on the
 // residualized block (device Gram, host sweep), eta = z - e and mu = exp(eta) with the deviance
@@ -862,23 +1090,27 @@ void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec
 // inner tolerance at its floor. Collinearity is settled in the first iteration (ppmlhdfe
 // remove_collinears): columns absorbed by the FE, then columns collinear with the others. The
 // variance uses the last iteration's weights: robust, (X~'WX~)^-1 [sum (e w)^2 x~ x~'] (X~'WX~)^-1
-// N / (N - 1), or clustered with G / (G - 1) and the multiway eigenvalue clip.
-void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out) {
-    if (!wk_.empty()) throw Error(RC_INVALID_INPUT, "fereg poisson: weighted sessions are not supported");
-    if (gs.vce == 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg poisson: cluster variance without clusters");
-    if (1 + nx + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg poisson: at most 62 regressors");
+// N / (N - 1), clustered with G / (G - 1) and the multiway eigenvalue clip, or (logit `oim`)
+// the inverse Hessian (X~'WX~)^-1.
+void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out) {
+    if (!wk_.empty()) throw Error(RC_INVALID_INPUT, "fereg glm: weighted sessions are not supported");
+    if (gs.family != 0 && gs.family != 1) throw Error(RC_INVALID_INPUT, "fereg glm: family is 0 (Poisson) or 1 (logit)");
+    const int fam = gs.family;
+    if (gs.vce == 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg glm: cluster variance without clusters");
+    if (1 + nx + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg glm: at most 62 regressors");
     SessionDev& d = *d_;
     cudaStream_t st = d.st;
     const size_t n = n_, r = 1 + nx;
     const int R = int(r);
     const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
-    DBuf<double> raw, B, mu, eta, z, w, e, part, om;
+    DBuf<double> raw, B, mu, eta, eta_old, z, w, e, part, om;
     DBuf<int> flag;
     raw.alloc(n * r);
     CK(cudaMemcpyAsync(raw.p, rows_in, n * r * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
     B.alloc(n * r);
     mu.alloc(n);
     eta.alloc(n);
+    if (fam == 1) eta_old.alloc(n);
     z.alloc(n);
     w.alloc(n);
     e.alloc(n);
@@ -886,7 +1118,7 @@ void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSp
     part.alloc(GLM_TB * 8);
     flag.alloc(1);
     CK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
-    k_glm_ysum<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, part.p, flag.p);
+    k_glm_ysum<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, fam, part.p, flag.p);
     auto host_sum = [&](int parts) {
         std::vector<double> h(static_cast<size_t>(parts));
         CK(cudaMemcpyAsync(h.data(), part.p, size_t(parts) * 8, cudaMemcpyDeviceToHost, st));
@@ -899,9 +1131,12 @@ void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSp
     int neg = 0;
     CK(cudaMemcpyAsync(&neg, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (neg) throw Error(RC_INVALID_INPUT, "fereg poisson: the dependent variable must be nonnegative");
+    if (neg)
+        throw Error(RC_INVALID_INPUT, fam == 0 ? "fereg glm: the dependent variable must be nonnegative"
+                                               : "fereg glm: the logit outcome must be 0 or 1");
     if (!(ysum > 0.0)) throw Error(RC_TOO_FEW_OBS, "insufficient observations (the dependent variable is all zero)");
-    k_glm_start<<<blocks, 256, 0, st>>>(raw.p, n, R, ysum / double(n), mu.p, eta.p);
+    if (fam == 1 && !(ysum < double(n))) throw Error(RC_TOO_FEW_OBS, "insufficient observations (the outcome never varies)");
+    k_glm_start<<<blocks, 256, 0, st>>>(raw.p, n, R, fam == 0 ? ysum / double(n) : 0.5, fam, mu.p, eta.p);
     d.launches += 2;
 
     // unweighted sums of squares of the raw regressors (stage-1 collinearity, ols.rs:38)
@@ -922,7 +1157,7 @@ void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSp
     for (size_t it = 1; it <= gs.maxiter; it++) {
         ab_->ctx().check();
         iters = it;
-        k_glm_work<<<blocks, 256, 0, st>>>(raw.p, n, R, mu.p, eta.p, B.p, z.p, w.p);
+        k_glm_work<<<blocks, 256, 0, st>>>(raw.p, n, R, fam, mu.p, eta.p, B.p, z.p, w.p);
         d.launches++;
         ab_->set_weights_device(w.p);
         const SolveInfo si = ab_->residualize_device(B.p, r, tol_in, gs.inner_maxiter, true,
@@ -965,10 +1200,20 @@ void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSp
             CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
         }
         k_resid_e<<<ST_GRID, ST_TB, 0, st>>>(B.p, n, R, d.col.p, d.beta.p, int(k), 0, nullptr, e.p, part.p);
-        k_glm_update<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, z.p, e.p, eta.p, mu.p, part.p);
+        k_glm_update<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, fam, z.p, e.p, eta.p, fam == 1 ? eta_old.p : nullptr,
+                                                mu.p, part.p);
         d.launches += 2;
-        dev = host_sum(GLM_TB);
-        if (!std::isfinite(dev)) throw Error(RC_CONVERGENCE, "fereg poisson: the deviance is not finite");
+        dev = 2.0 * host_sum(GLM_TB);
+        // logit step halving while the deviance rose (irls.rs:739-748, at most 25 halvings)
+        if (fam == 1 && it > 1) {
+            for (int h = 0; h < 25 && (std::isnan(dev) || dev > dev_old + 1e-9 * std::max(std::fabs(dev_old), 1.0));
+                 h++) {
+                k_glm_halve<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, fam, eta_old.p, eta.p, mu.p, part.p);
+                d.launches++;
+                dev = 2.0 * host_sum(GLM_TB);
+            }
+        }
+        if (!std::isfinite(dev)) throw Error(RC_CONVERGENCE, "fereg glm: the deviance is not finite");
         std::swap(warm, coefs);
         if (coefs.size() != warm.size()) coefs.resize(warm.size());
         have_warm = true;
@@ -983,7 +1228,7 @@ void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSp
         }
         dev_old = dev;
     }
-    if (!converged) throw Error(RC_CONVERGENCE, "fereg poisson: IRLS did not converge");
+    if (!converged) throw Error(RC_CONVERGENCE, "fereg glm: IRLS did not converge");
 
     // variance on the last iteration's weights (w, e and the residualized block B)
     const size_t k = kept.size();
@@ -1011,11 +1256,13 @@ void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSp
             V = la::sandwich(inv, meat, k, gmin > 1.0 ? gmin / (gmin - 1.0) : 0.0);
             if (ccodes_.size() > 1) la::fix_psd(V, k, false);
             out.N_clust = gmin;
-        } else {
+        } else if (gs.vce == 1) {
             k_glm_score<<<blocks, 256, 0, st>>>(e.p, w.p, n, 1, om.p);
             d.launches++;
             const la::Mat meat = outer_products(B.p, n, R, kc, nullptr, false, om.p, nullptr, false, nullptr);
             V = la::sandwich(inv, meat, k, bigN / (bigN - 1.0));
+        } else {
+            V = inv;  // oim: the inverse Hessian (X~'WX~)^-1
         }
     }
     // Wald chi2 of the slopes (greedy sweep of V)
@@ -1030,7 +1277,7 @@ void GpuSession::poisson(double* rows_in, bool on_device, size_t nx, const GlmSp
             chi2 = finite_or_nan(q);
         }
     }
-    k_glm_ll<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, eta.p, mu.p, part.p);
+    k_glm_ll<<<GLM_TB, GLM_TB, 0, st>>>(raw.p, n, R, fam, eta.p, mu.p, part.p);
     d.launches++;
     const double ll = host_sum(GLM_TB);
     if (out.b) std::fill(out.b, out.b + nx, 0.0);

@@ -87,9 +87,26 @@ class GpuSession {
     };
     void wildboot(double* rows, bool on_device, size_t nx, const OlsSpec& ospec, const BootSpec& bs, BootOut& out);
 
-    // Poisson PML by IRLS on the session's FE (see session.cu).
+    // IV / 2SLS on the session's FE (see session.cu).
+    struct IvSpec {
+        int vce = 0;  // 0 unadjusted, 1 robust, 2 cluster (one- or multiway)
+        double tol = 1e-8;
+        size_t maxiter = 16000;
+        Precision prec = Precision::F64;
+    };
+    struct IvOut {
+        double* b = nullptr;        // ne + nx: [endog..., exog...]; dropped columns 0
+        double* V = nullptr;        // (ne + nx)^2
+        uint8_t* status = nullptr;  // nx + ne + ni in block order: 0 ok, 2 absorbed, 3 collinear
+        double N = 0, df_r = 0, df_m = 0, df_a = 0, sdofminus = 0, rss = 0, rmse = 0, F = 0, N_clust = 0, ic = 0;
+        int endog_ct = 0, inexog_ct = 0, exexog_ct = 0;
+    };
+    void iv(double* rows, bool on_device, size_t nx, size_t ne, size_t ni, const IvSpec& spec, IvOut& out);
+
+    // GLM by IRLS on the session's FE (see session.cu): Poisson PML or logit.
     struct GlmSpec {
-        int vce = 1;  // 1 robust, 2 cluster (ppmlhdfe reports no unadjusted Poisson variance)
+        int family = 0;  // 0 Poisson, 1 logit
+        int vce = 1;     // 0 oim (inverse Hessian), 1 robust, 2 cluster
         double tol = 1e-8;
         size_t maxiter = 10000;
         size_t inner_maxiter = 16000;
@@ -103,7 +120,7 @@ class GpuSession {
         u64 iterations = 0, pcg_iterations = 0;
         bool converged = false;
     };
-    void poisson(double* rows, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out);
+    void glm(double* rows, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out);
 
    private:
     size_t n_ = 0;
@@ -126,6 +143,10 @@ class GpuSession {
         bool has_groupvar = false;
     };
     Dof estimate_dof(bool clusters, bool firstpair, bool want_groupvar);
+    struct ColStats {
+        std::vector<double> wmean, sumsq, wss_unc, sd, wss;
+    };
+    ColStats column_stats(const double* rows, int R);
     std::vector<double> outer_products(const double* src, size_t nrows, int srcR, const std::vector<int>& cols,
                                        const std::vector<double>* shift, bool cst, const double* om, const int* perm,
                                        bool ssq, std::vector<double>* ss_out);

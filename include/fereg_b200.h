@@ -211,19 +211,49 @@ typedef struct fereg_boot_out {
 int fereg_session_wildboot(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_ols_spec* spec,
                            const fereg_boot_spec* boot, fereg_boot_out* out);
 
-/* Poisson PML by IRLS on the session's fixed effects (glm/irls.rs:367-560, glm/mod.rs with
- * ppmlhdfe conventions): y >= 0 in column 0 of the n x (1 + nx) row-order block, regressors
- * after it; every iteration refreshes the weight state on the device and residualizes
- * [z, X] warm-started from the previous FE coefficients. vce 1 robust (N / (N - 1)), 2 cluster
+/* IV / 2SLS on the session's fixed effects with ivreghdfe conventions (replaces Session::iv,
+ * iv.rs:299, for b and V): rows is the n x (1 + nx + nendog + ninst) row-order block
+ * [y, exog, endog, inst] (Layout {nx, nendog, ninst}, api.rs), residualized in one absorber
+ * call; ivreg2 with `small` and sdofminus = max(df_a, 1). vce 0 unadjusted (pweights imply
+ * robust), 1 robust, 2 cluster over the session's cluster dimensions. b and V are in e(b) order
+ * [endog..., exog...] (nendog + nx); status has nx + nendog + ninst entries in block order.
+ * 481 when fewer excluded instruments than endogenous regressors survive collinearity. */
+typedef struct fereg_iv_spec {
+    int vce;
+    double tol;
+    size_t maxiter;
+    int precision;
+} fereg_iv_spec;
+
+typedef struct fereg_iv_out {
+    double* b;
+    double* V;
+    uint8_t* status;
+    double N, df_r, df_m, df_a, sdofminus, rss, rmse, F, N_clust, ic;
+    int32_t endog_ct, inexog_ct, exexog_ct;
+} fereg_iv_out;
+
+int fereg_session_iv(fereg_session* s, double* rows, int rows_on_device, size_t nx, size_t nendog, size_t ninst,
+                     const fereg_iv_spec* spec, fereg_iv_out* out);
+
+/* GLM by IRLS on the session's fixed effects (glm/irls.rs:367-560, glm/mod.rs; replaces the
+ * engine's glm_fit, engine.rs:1038, for unweighted samples): Poisson PML (ppmlhdfe conventions,
+ * y >= 0) or logit (y in {0, 1}, step halving when the deviance rises) with y in column 0 of the
+ * n x (1 + nx) row-order block and the regressors after it; every iteration refreshes the
+ * weight state on the device and residualizes [z, X] warm-started from the previous FE
+ * coefficients. vce 0 oim (the inverse Hessian; logit only), 1 robust (N / (N - 1)), 2 cluster
  * over the session's cluster dimensions (G / (G - 1), multiway eigenvalue clip). The sample is
  * taken as prepared (singletons and separated observations already dropped); unweighted
  * sessions only. 430 when IRLS does not converge within maxiter. */
+#define FEREG_FAMILY_POISSON 1 /* api.rs Family::Poisson */
+#define FEREG_FAMILY_LOGIT 2   /* api.rs Family::Logit */
 typedef struct fereg_glm_spec {
     int vce;
     double tol;
     size_t maxiter;
     size_t inner_maxiter;
     int precision; /* FEREG_PREC_* of the FE solves */
+    int family;    /* FEREG_FAMILY_*; fereg_session_poisson ignores it */
 } fereg_glm_spec;
 
 typedef struct fereg_glm_out {
@@ -235,6 +265,9 @@ typedef struct fereg_glm_out {
     int32_t converged;
 } fereg_glm_out;
 
+int fereg_session_glm(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
+                      fereg_glm_out* out);
+/* fereg_session_glm with the Poisson family. */
 int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
                           fereg_glm_out* out);
 

@@ -37,3 +37,41 @@ def model_args(spec, data):
         weights=data[spec["weight"]] if spec["weight"] else None, weight_kind=spec["weight_kind"], vce=vce,
         singletons=spec["singletons"], noconstant=spec["noconstant"], firstpair=spec["firstpair"],
     )
+
+
+def load_csv(name):
+    with open(os.path.join(GOLDEN, name)) as f:
+        rows = list(csv.DictReader(f))
+    return {k: np.array([float(r[k]) for r in rows]) for k in rows[0]}
+
+
+def load_json(name):
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+def restrict(codes, alive):
+    """Codes of the kept rows, renumbered densely in ascending order, and their count."""
+    u, inv = np.unique(codes[alive], return_inverse=True)
+    return inv.astype(np.uint32), len(u)
+
+
+def prepare_iv(spec, data):
+    """Sample preparation of an IV fixture as the reference's Session::prepare does it
+    (factorize, drop_singletons with fweights, restrict): kept mask, singletons dropped, FE
+    terms, cluster dimensions, kept weights."""
+    from oracle import oracle
+
+    fac = {f: oracle.factorize(data[f]) for f in ("idcode", "year")}
+    terms = [fac[f] for f in spec["absorb"]]
+    w = data[spec["weight"]] if spec["weight"] else None
+    fw = w if spec["weight_kind"] == "fweight" else None
+    alive, nsing = oracle.drop_singletons([c for c, _ in terms], [g for _, g in terms], fw)
+    terms = [restrict(c, alive) for c, _ in terms]
+    clusters = [restrict(fac[c][0], alive) for c in spec["cluster"]]
+    return alive, nsing, terms, clusters, (None if w is None else w[alive])
+
+
+def iv_block(spec, data, alive):
+    cols = [spec["y"]] + spec["exog"] + spec["endog"] + spec["inst"]
+    return np.ascontiguousarray(np.stack([data[c][alive] for c in cols], axis=1))

@@ -1,4 +1,4 @@
-"""Extracts the reference's frozen reghdfe fixtures into tests/golden/.
+"""Extracts the reference's frozen Stata fixtures into tests/golden/.
 
 The reference (leoliu0/fereg) pins its OLS path against reghdfe 6.13.1 run at tol(1e-14)
 (crates/fereg-core/tests/data/ols_data.csv + ols_s*.json, generated there by
@@ -6,6 +6,11 @@ gen_ols_fixtures.do). This script copies the data columns and the parts of each 
 tests here compare (b, V, dof_table, sample, resid, d, groupvar, scalars), and records each
 fixture's model specification as restated from the reference's harness
 (crates/fereg-core/tests/ols.rs:803-827).
+
+It also extracts the IV fixtures (ivreghdfe 1.1.4 on an nlswork subset, iv_nls.csv +
+iv_nls_{a,b}_{unadj,robust,cl1,cl2}_{none,aw,fw,pw}.json; harness tests/iv.rs:216-248) and the
+logit fixtures (Stata `logit y x1 x2 i.fe1 i.fe2`, glm_logit.csv + glm_l_*.json; harness
+tests/glm.rs:319-325, 659-672): b, V, sample and the scalars compared here.
 
 Run once in a container that has the reference mounted:
     python tests/golden/make_golden.py /path/to/reference
@@ -80,5 +85,65 @@ def main(ref):
     print(f"wrote {len(out)} fixtures, {len(rows)} rows")
 
 
+IV_COLUMNS = ["idcode", "year", "ln_wage", "age", "tenure", "union", "south", "msp", "w", "fw"]
+IV_SCALARS = ["N", "df_r", "df_m", "df_a", "sdofminus", "rss", "rmse", "F", "N_clust", "endog_ct", "inexog_ct",
+              "exexog_ct"]
+LOGIT_COLUMNS = ["y", "y2", "x1", "x2", "fe1", "fe2", "c"]
+# tests/glm.rs:659-672: unweighted logit fixtures with absorbed FE (fw / pw / noabsorb are outside
+# the device path's scope)
+LOGIT_SPECS = [
+    dict(name="l_oim", absorb=["fe1", "fe2"], vce="oim", cluster=None),
+    dict(name="l_robust", absorb=["fe1", "fe2"], vce="robust", cluster=None),
+    dict(name="l_cluster", absorb=["fe1", "fe2"], vce="cluster", cluster="c"),
+    dict(name="l_onefe", absorb=["fe1"], vce="oim", cluster=None),
+]
+
+
+def copy_csv(src, dst, columns):
+    with open(src) as f:
+        rows = list(csv.DictReader(f))
+    with open(dst, "w", newline="") as f:
+        w = csv.writer(f)
+        w.writerow(columns)
+        for r in rows:
+            w.writerow([r[c] for c in columns])
+    return len(rows)
+
+
+def main_iv_logit(ref):
+    data_dir = os.path.join(ref, "crates", "fereg-core", "tests", "data")
+    copy_csv(os.path.join(data_dir, "iv_nls.csv"), os.path.join(HERE, "iv_nls.csv"), IV_COLUMNS)
+    out = []
+    for tag, inst in (("a", ["union", "south"]), ("b", ["union", "south", "msp"])):
+        for v in ("unadj", "robust", "cl1", "cl2"):
+            for wt in ("none", "aw", "fw", "pw"):
+                name = f"nls_{tag}_{v}_{wt}"
+                with open(os.path.join(data_dir, f"iv_{name}.json")) as f:
+                    j = json.load(f)
+                spec = dict(name=name, absorb=["idcode", "year"], y="ln_wage", exog=["age"], endog=["tenure"],
+                            inst=inst, weight={"aw": "w", "pw": "w", "fw": "fw"}.get(wt),
+                            weight_kind={"aw": "aweight", "pw": "pweight", "fw": "fweight"}.get(wt),
+                            cluster={"cl1": ["idcode"], "cl2": ["idcode", "year"]}.get(v, []),
+                            vce={"unadj": "unadjusted", "robust": "robust"}.get(v, "cluster"))
+                sc = {k: j["scalars"].get(k) for k in IV_SCALARS}
+                out.append(dict(spec=spec, cmdline=j["cmdline"], b=j["b"], V=j["V"], sample=j["sample"], scalars=sc))
+    with open(os.path.join(HERE, "iv_fixtures.json"), "w") as f:
+        json.dump(out, f)
+    copy_csv(os.path.join(data_dir, "glm_logit.csv"), os.path.join(HERE, "glm_logit.csv"), LOGIT_COLUMNS)
+    out = []
+    for spec in LOGIT_SPECS:
+        with open(os.path.join(data_dir, f"glm_{spec['name']}.json")) as f:
+            j = json.load(f)
+        p = len(j["b"])
+        V = [j["V"][a * p + b] for a in range(2) for b in range(2)]
+        sc = {k: j["scalars"][k] for k in ("N", "ll", "ll_0", "converged")}
+        out.append(dict(spec=spec, cmdline=j["cmdline"], b=j["b"][:2], V=V, sample=j["sample"], scalars=sc))
+    with open(os.path.join(HERE, "logit_fixtures.json"), "w") as f:
+        json.dump(out, f)
+    print("wrote the IV and logit fixtures")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    main(ref)
+    main_iv_logit(ref)

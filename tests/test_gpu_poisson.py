@@ -1,8 +1,8 @@
 """The device Poisson PML (fereg_session_poisson) against a dense explicit-dummy fit.
 
 The Poisson maximum-likelihood estimate is unique, so the reference here is the same model fitted
-densely: explicit FE dummies, IRLS on the full design until the deviance stops changing
-(relative 1e-15). The variance follows ppmlhdfe's conventions as the reference restates them
+densely by the oracle (oracle/glm.py): explicit FE dummies, IRLS on the full design until the
+deviance stops changing (relative 1e-15). The variance follows ppmlhdfe's conventions as the reference restates them
 (crates/fereg-core/src/glm/mod.rs:1-22, 1053-1140): robust
 (X~'WX~)^-1 [sum (y - mu)^2 x~ x~'] (X~'WX~)^-1 N / (N - 1), clustered with G / (G - 1), where X~
 is X residualized on the dummies with weights mu.
@@ -12,47 +12,15 @@ Tolerances: b 1e-7, V 1e-6 relative, deviance and log-likelihood 1e-9 relative.
 
 import numpy as np
 import pytest
-from scipy.special import gammaln
 
 import fereg_b200 as fb
+from oracle import glm as oglm
 
 pytestmark = pytest.mark.gpu
 
 
 def dense_ppml(terms, y, X, cl=None):
-    n = len(y)
-    D = np.concatenate([np.eye(g)[c] for c, g in terms], axis=1)
-    Z = np.concatenate([X, D], axis=1)
-    mu = (y + y.mean()) / 2
-    eta = np.log(mu)
-    dev_old = np.inf
-    for _ in range(200):
-        z = eta - 1 + y / mu
-        sw = np.sqrt(mu)[:, None]
-        coef, *_ = np.linalg.lstsq(Z * sw, z * sw[:, 0], rcond=None)
-        eta = Z @ coef
-        mu = np.exp(eta)
-        dev = 2 * np.sum(np.where(y > 0, y * np.log(np.where(y > 0, y, 1) / mu), 0) - (y - mu))
-        if abs(dev - dev_old) <= 1e-15 * dev:
-            break
-        dev_old = dev
-    k = X.shape[1]
-    b = coef[:k]
-    w = mu
-    sw = np.sqrt(w)[:, None]
-    cd, *_ = np.linalg.lstsq(D * sw, X * sw, rcond=None)
-    Xt = X - D @ cd
-    A = np.linalg.inv(Xt.T @ (w[:, None] * Xt))
-    s = (y - mu)[:, None] * Xt
-    if cl is None:
-        V = A @ (s.T @ s) @ A * n / (n - 1)
-    else:
-        codes, G = cl
-        S = np.zeros((G, k))
-        np.add.at(S, codes, s)
-        V = A @ (S.T @ S) @ A * G / (G - 1)
-    ll = np.sum(y * eta - mu - gammaln(y + 1))
-    return b, V, dev, ll
+    return oglm.dense_glm("poisson", terms, y, X, "robust" if cl is None else "cluster", cl)
 
 
 def panel(seed, n_ind, years, n_firm, k):
