@@ -78,6 +78,28 @@ class IvOut(C.Structure):
                 + [("endog_ct", C.c_int32), ("inexog_ct", C.c_int32), ("exexog_ct", C.c_int32)])
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("workers", C.c_int), ("hbm_budget", C.c_size_t), ("dry_run", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("model", C.c_int), ("codes", C.POINTER(u32p)), ("g", u32p), ("nterms", C.c_int),
+                ("cl_codes", C.POINTER(u32p)), ("cl_g", u32p), ("ncl", C.c_int), ("w", f64p),
+                ("weight_kind", C.c_int), ("n", C.c_size_t), ("cols", C.POINTER(f64p)), ("nx", C.c_size_t),
+                ("nendog", C.c_size_t), ("ninst", C.c_size_t), ("vce", C.c_int), ("tol", C.c_double),
+                ("maxiter", C.c_size_t), ("precision", C.c_int), ("b", f64p), ("V", f64p),
+                ("dry_run_us", C.c_uint64)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("rc", C.c_int), ("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
+                ("bytes", C.c_uint64), ("N", C.c_double), ("iterations", C.c_uint64), ("converged", C.c_int32)]
+
+
+MODELS = {"ols": 0, "iv": 1, "logit": 2, "poisson": 3}
+VCES = {"ols": {"unadjusted": 0, "robust": 1, "cluster": 2}, "iv": {"unadjusted": 0, "robust": 1, "cluster": 2},
+        "logit": {"oim": 0, "robust": 1, "cluster": 2}, "poisson": {"robust": 1, "cluster": 2}}
+
 FAMILY_POISSON = 1
 FAMILY_LOGIT = 2
 
@@ -145,6 +167,12 @@ def _setup(L):
     L.fereg_session_poisson.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(GlmSpec), C.POINTER(GlmOut)]
     L.fereg_session_iv.argtypes = [P, P, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(IvSpec),
                                    C.POINTER(IvOut)]
+    L.fereg_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(P)]
+    L.fereg_server_submit.argtypes = [P, C.POINTER(Request), C.POINTER(C.c_uint64)]
+    L.fereg_server_wait.argtypes = [P, C.c_uint64, C.POINTER(RequestResult), C.c_char_p, C.c_size_t]
+    L.fereg_server_stats.argtypes = [P, u64p]
+    L.fereg_server_destroy.argtypes = [P]
+    L.fereg_server_destroy.restype = None
     L.fereg_session_glm.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(GlmSpec), C.POINTER(GlmOut)]
     L.fereg_session_wildboot.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(OlsSpec), C.POINTER(BootSpec),
                                          C.POINTER(BootOut)]
@@ -484,3 +512,67 @@ class Session:
         return dict(b=b[:nx], V=V[:nx, :nx], status=status[:nx], N=out.N, deviance=out.deviance, ll=out.ll,
                     chi2=out.chi2, df_m=out.df_m, N_clust=out.N_clust, iterations=int(out.iterations),
                     pcg_iterations=int(out.pcg_iterations), converged=bool(out.converged))
+
+
+class Server:
+    """The library's serving engine (fereg_server_*): requests are admitted in arrival order
+    while their estimated device memory fits `hbm_budget` bytes (None: 80% of the free memory),
+    and `workers` of them run at once, each on its own session and CUDA stream. submit() returns
+    a ticket; wait(ticket) blocks and returns the result. The arrays a request points to are kept
+    alive here until it is waited for."""
+
+    def __init__(self, workers=4, hbm_budget=None, dry_run=False):
+        cfg = ServerConfig(workers, int(hbm_budget or 0), int(dry_run))
+        h = P()
+        _check(lib().fereg_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._live = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fereg_server_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def submit(self, model, codes, g, cols, nx, nendog=0, ninst=0, clusters=(), cl_g=(), w=None, weight_kind=None,
+               vce=None, tol=1e-8, maxiter=16000, precision=PREC_F64, dry_run_us=0, n=None):
+        """cols: kept-order columns [y, exog (nx), endog (nendog), inst (ninst)]."""
+        codes = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
+        cl = [np.ascontiguousarray(c, dtype=np.uint32) for c in clusters]
+        cols = [np.ascontiguousarray(c, dtype=np.float64) for c in cols]
+        garr = np.asarray(g, dtype=np.uint32)
+        cgarr = np.asarray(cl_g, dtype=np.uint32)
+        wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        n = len(cols[0]) if n is None else n
+        k_all = {"ols": nx + 1, "iv": nendog + nx, "logit": nx, "poisson": nx}[model]
+        b = np.zeros(max(1, k_all))
+        V = np.zeros((max(1, k_all), max(1, k_all)))
+        cp = (u32p * max(1, len(codes)))(*[_p(c, u32p) for c in codes])
+        clp = (u32p * max(1, len(cl)))(*[_p(c, u32p) for c in cl])
+        colp = (f64p * len(cols))(*[_p(c, f64p) for c in cols])
+        if vce is None:
+            vce = {"ols": "unadjusted", "iv": "unadjusted", "logit": "oim", "poisson": "robust"}[model]
+        req = Request(MODELS[model], cp, _p(garr, u32p), len(codes), clp, _p(cgarr, u32p), len(cl), _p(wa, f64p),
+                      WEIGHT_KIND[weight_kind if w is not None else None], n, colp, nx, nendog, ninst,
+                      VCES[model][vce], tol, maxiter, precision, _p(b, f64p), _p(V, f64p), int(dry_run_us))
+        t = C.c_uint64()
+        _check(lib().fereg_server_submit(self.h, C.byref(req), C.byref(t)))
+        self._live[t.value] = (codes, cl, cols, garr, cgarr, wa, b, V, cp, clp, colp, k_all)
+        return t.value
+
+    def wait(self, ticket):
+        res = RequestResult()
+        msg = C.create_string_buffer(512)
+        _check(lib().fereg_server_wait(self.h, ticket, C.byref(res), msg, 512))
+        keep = self._live.pop(ticket)
+        b, V, k_all = keep[6], keep[7], keep[11]
+        return dict(rc=res.rc, msg=msg.value.decode(), b=b[:k_all], V=V[:k_all, :k_all], submit_s=res.submit_s,
+                    admit_s=res.admit_s, done_s=res.done_s, bytes=int(res.bytes), N=res.N,
+                    iterations=int(res.iterations), converged=bool(res.converged))
+
+    def stats(self):
+        v = np.zeros(7, dtype=np.uint64)
+        _check(lib().fereg_server_stats(self.h, _p(v, u64p)))
+        keys = ["submitted", "completed", "rejected", "peak_bytes", "peak_running", "budget", "running"]
+        return {k: int(x) for k, x in zip(keys, v)}

@@ -218,6 +218,7 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
     norm_fe1_ = fe1_index(g);
     ctx_.check();
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    AllocScope alloc_scope(stream_);
     d_ = std::make_unique<Scratch>();
     CK(cudaHostAlloc(&d_->h_nactive, sizeof(int), cudaHostAllocDefault));
     d_->seg_off.upload(hs_.seg_off, stream_);
@@ -279,6 +280,7 @@ bool GpuAbsorber::weights(double* out) const {
 // of the weight state is computed on the device (weights.cuh); the host mirrors are copied back
 // only when a host-side reader needs them.
 void GpuAbsorber::set_weights_device(const double* w_dev) {
+    AllocScope alloc_scope(stream_);
     ctx_.check();
     const HostStructure& st = hs_;
     const size_t n = st.n, M = st.ncells, g1 = st.g1, m = st.m;
@@ -326,6 +328,7 @@ void GpuAbsorber::set_weights_device(const double* w_dev) {
 
 // Copies the device weight state back into the host mirrors after set_weights_device.
 void GpuAbsorber::sync_host_weights() const {
+    AllocScope alloc_scope(stream_);
     if (!host_stale_) return;
     const HostStructure& st = hs_;
     const size_t n = st.n, M = st.ncells, g1 = st.g1, m = st.m;
@@ -418,6 +421,7 @@ void GpuAbsorber::upload_weights() {
 }
 
 void GpuAbsorber::set_weights(const double* w_rows) {
+    AllocScope alloc_scope(stream_);
     ctx_.check();
     std::vector<double> kept;
     if (w_rows) {
@@ -782,6 +786,7 @@ void launch_rhs_scratch(Scratch& d, const DevStruct& S, const DevWeights& W, con
 }  // namespace
 
 void GpuAbsorber::apply_host(const double* p, size_t r, double* y) {
+    AllocScope alloc_scope(stream_);
     const size_t m = hs_.m;
     const DevStruct S = d_->ds(hs_);
     d_->p.alloc(m * r);
@@ -797,6 +802,7 @@ void GpuAbsorber::apply_host(const double* p, size_t r, double* y) {
 }
 
 void GpuAbsorber::precond_host(const double* rr, size_t r, double* z) {
+    AllocScope alloc_scope(stream_);
     ensure_precond();
     const size_t m = hs_.m;
     d_->r.alloc(m * r);
@@ -809,6 +815,7 @@ void GpuAbsorber::precond_host(const double* rr, size_t r, double* z) {
 }
 
 void GpuAbsorber::rhs_host(const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum) {
+    AllocScope alloc_scope(stream_);
     const size_t n = hs_.n, m = hs_.m, g1 = hs_.g1;
     const DevStruct S = d_->ds(hs_);
     d_->rows.alloc(n * r);
@@ -850,6 +857,7 @@ void GpuAbsorber::rhs_device_scratch(const double* rows, size_t r, double* rhs, 
 
 SolveInfo GpuAbsorber::residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
                                    double* coefs, Precision prec) {
+    AllocScope alloc_scope(stream_);
     const size_t n = hs_.n;
     d_->rows.alloc(std::max<size_t>(1, n * r));
     int h = d_->begin(P_H2D, stream_);
@@ -866,6 +874,7 @@ SolveInfo GpuAbsorber::residualize(double* z, size_t r, double tol, size_t maxit
 
 SolveInfo GpuAbsorber::residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
                                           const double* warm, double* coefs, Precision prec) {
+    AllocScope alloc_scope(stream_);
     return solve(z_dev, r, tol, maxiter, want_coefs, warm, coefs, prec);
 }
 
@@ -1115,6 +1124,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
 }
 
 void GpuAbsorber::set_profiling(bool on) {
+    AllocScope alloc_scope(stream_);
     d_->prof = on;
     if (on) {
         std::fill(d_->ms, d_->ms + P_NSLOTS, 0.0);
@@ -1132,6 +1142,7 @@ void GpuAbsorber::phase_times(double* ms, u64* counts) const {
 u64 GpuAbsorber::launches() const { return d_->launches; }
 
 void GpuAbsorber::fit_rows(const double* coefs, size_t r, size_t col, double* out) const {
+    AllocScope alloc_scope(stream_);
     const HostStructure& st = hs_;
     const size_t m = st.m, M = st.ncells, nb = st.nb();
     for (u32 s = 0; s < st.g1; s++)
@@ -1144,6 +1155,7 @@ void GpuAbsorber::fit_rows(const double* coefs, size_t r, size_t col, double* ou
 }
 
 void GpuAbsorber::term_values(const double* coefs, size_t r, size_t col, double* out) const {
+    AllocScope alloc_scope(stream_);
     sync_host_weights();
     const HostStructure& st = hs_;
     const size_t nterms = g_.size();

@@ -6,6 +6,7 @@
 
 #include "../../include/fereg_b200.h"
 #include "absorber.h"
+#include "server.h"
 #include "session.h"
 
 using namespace fereg;
@@ -478,3 +479,75 @@ void* fereg_session_stream(const fereg_session* s) {
 }
 
 }  // extern "C"
+
+struct fereg_server {
+    fereg::Server s;
+    fereg_server(int w, uint64_t b, bool dry) : s(w, b, dry) {}
+};
+
+int fereg_server_create(const fereg_server_config* cfg, fereg_server** out) {
+    return guard([&] {
+        if (!cfg || !out) throw Error(RC_INVALID_INPUT, "fereg_server_create: NULL argument");
+        *out = new fereg_server(cfg->workers, cfg->hbm_budget, cfg->dry_run != 0);
+    });
+}
+
+int fereg_server_submit(fereg_server* srv, const fereg_request* q, uint64_t* ticket) {
+    return guard([&] {
+        if (!srv || !q || !ticket) throw Error(RC_INVALID_INPUT, "fereg_server_submit: NULL argument");
+        if (q->nterms < 0 || q->ncl < 0) throw Error(RC_INVALID_INPUT, "fereg_server_submit: negative count");
+        if (q->nterms && (!q->codes || !q->g)) throw Error(RC_INVALID_INPUT, "fereg_server_submit: NULL codes");
+        if (q->ncl && (!q->cl_codes || !q->cl_g)) throw Error(RC_INVALID_INPUT, "fereg_server_submit: NULL clusters");
+        if (!q->cols) throw Error(RC_INVALID_INPUT, "fereg_server_submit: NULL columns");
+        ServeRequest r;
+        r.model = q->model;
+        r.codes.assign(q->codes, q->codes + q->nterms);
+        r.g.assign(q->g, q->g + q->nterms);
+        r.cl_codes.assign(q->cl_codes, q->cl_codes + q->ncl);
+        r.cl_g.assign(q->cl_g, q->cl_g + q->ncl);
+        r.w = q->w;
+        r.weight_kind = q->weight_kind;
+        r.n = q->n;
+        r.nx = q->nx;
+        r.ne = q->nendog;
+        r.ni = q->ninst;
+        r.cols.assign(q->cols, q->cols + 1 + q->nx + q->nendog + q->ninst);
+        r.vce = q->vce;
+        r.tol = q->tol;
+        r.maxiter = q->maxiter;
+        r.precision = q->precision;
+        r.b = q->b;
+        r.V = q->V;
+        r.dry_run_us = q->dry_run_us;
+        *ticket = srv->s.submit(r);
+    });
+}
+
+int fereg_server_wait(fereg_server* srv, uint64_t ticket, fereg_request_result* out, char* msg, size_t msg_cap) {
+    return guard([&] {
+        if (!srv || !out) throw Error(RC_INVALID_INPUT, "fereg_server_wait: NULL argument");
+        const ServeResult r = srv->s.wait(ticket);
+        out->rc = r.rc;
+        out->submit_s = r.submit_s;
+        out->admit_s = r.admit_s;
+        out->done_s = r.done_s;
+        out->bytes = r.bytes;
+        out->N = r.N;
+        out->iterations = r.iterations;
+        out->converged = r.converged ? 1 : 0;
+        if (msg && msg_cap) {
+            const size_t k = std::min(msg_cap - 1, r.msg.size());
+            std::copy(r.msg.begin(), r.msg.begin() + k, msg);
+            msg[k] = 0;
+        }
+    });
+}
+
+int fereg_server_stats(const fereg_server* srv, uint64_t* out7) {
+    return guard([&] {
+        if (!srv || !out7) throw Error(RC_INVALID_INPUT, "fereg_server_stats: NULL argument");
+        srv->s.stats(out7);
+    });
+}
+
+void fereg_server_destroy(fereg_server* srv) { delete srv; }

@@ -17,30 +17,77 @@ inline void cuda_check(cudaError_t e, const char* what) {
 }
 #define CK(x) ::fereg::cuda_check((x), #x)
 
+// Stream-ordered allocation. While an AllocScope is active on a thread, DBuf allocations made on
+// that thread come from the device's memory pool in the order of the scope's stream
+// (cudaMallocAsync / cudaFreeAsync on the stream the owner runs all its work on), so that
+// releasing a buffer does not wait for the whole device, as cudaFree does; concurrent sessions
+// on their own streams then never stall one another. Without a scope DBuf uses cudaMalloc /
+// cudaFree.
+inline cudaStream_t& alloc_stream() {
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+struct AllocScope {
+    cudaStream_t prev;
+    explicit AllocScope(cudaStream_t s) : prev(alloc_stream()) { alloc_stream() = s; }
+    ~AllocScope() { alloc_stream() = prev; }
+    AllocScope(const AllocScope&) = delete;
+    AllocScope& operator=(const AllocScope&) = delete;
+};
+
 // Owned device allocation.
 template <class T>
 struct DBuf {
     T* p = nullptr;
     size_t n = 0;
+    cudaStream_t s = nullptr;  // the stream of a pooled allocation
+    bool pooled = false;
     DBuf() = default;
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
-    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
-    DBuf& operator=(DBuf&& o) noexcept { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; return *this; }
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s), pooled(o.pooled) {
+        o.p = nullptr;
+        o.n = 0;
+    }
+    DBuf& operator=(DBuf&& o) noexcept {
+        release();
+        p = o.p;
+        n = o.n;
+        s = o.s;
+        pooled = o.pooled;
+        o.p = nullptr;
+        o.n = 0;
+        return *this;
+    }
     ~DBuf() { release(); }
-    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    void release() {
+        if (p) {
+            if (pooled) cudaFreeAsync(p, s);
+            else cudaFree(p);
+        }
+        p = nullptr;
+        n = 0;
+    }
     void alloc(size_t count) {
         if (count <= n && p) return;
         release();
         if (count == 0) return;
-        CK(cudaMalloc(&p, count * sizeof(T)));
+        const cudaStream_t st = alloc_stream();
+        if (st) {
+            CK(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), st));
+            s = st;
+            pooled = true;
+        } else {
+            CK(cudaMalloc(&p, count * sizeof(T)));
+            pooled = false;
+        }
         n = count;
     }
-    void upload(const T* h, size_t count, cudaStream_t s) {
+    void upload(const T* h, size_t count, cudaStream_t st) {
         alloc(count);
-        if (count) CK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+        if (count) CK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
     }
-    void upload(const std::vector<T>& h, cudaStream_t s) { upload(h.data(), h.size(), s); }
+    void upload(const std::vector<T>& h, cudaStream_t st) { upload(h.data(), h.size(), st); }
 };
 
 constexpr unsigned FULL = 0xffffffffu;

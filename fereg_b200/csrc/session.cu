@@ -86,6 +86,7 @@ GpuSession::GpuSession(const std::vector<const u32*>& codes, const std::vector<u
     d_ = std::make_unique<SessionDev>();
     SessionDev& d = *d_;
     d.st = ab_->stream();
+    AllocScope alloc_scope(d.st);
     for (auto& c : tcodes_) {
         d.tcodes.emplace_back();
         d.tcodes.back().upload(c, d.st);
@@ -142,6 +143,7 @@ GpuSession::~GpuSession() {
 u64 GpuSession::launches() const { return d_->launches + ab_->launches(); }
 
 void GpuSession::set_profiling(bool on) {
+    AllocScope alloc_scope(ab_->stream());
     d_->prof = on;
     if (on) {
         std::fill(d_->ms, d_->ms + S_NSLOTS, 0.0);
@@ -339,6 +341,25 @@ std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, 
     return m;
     }
 
+double* GpuSession::gather_columns(const double* const* cols, size_t R) {
+    AllocScope alloc_scope(ab_->stream());
+    SessionDev& d = *d_;
+    cudaStream_t st = d.st;
+    const size_t n = n_;
+    if (R == 0 || R + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg gather: 1 to 62 columns");
+    for (size_t j = 0; j < R; j++)
+        if (!cols[j]) throw Error(RC_INVALID_INPUT, "fereg gather: NULL column");
+    if (!d.pi.p) d.pi.upload(ab_->row_order(), st);
+    d.colbuf.alloc(n * R);
+    for (size_t j = 0; j < R; j++)
+        CK(cudaMemcpyAsync(d.colbuf.p + j * n, cols[j], n * 8, cudaMemcpyHostToDevice, st));
+    d.rows.alloc(n * R);
+    k_gather_cols<<<blocks_for(n, 256), 256, 0, st>>>(d.colbuf.p, d.pi.p, n, int(R), d.rows.p);
+    d.launches++;
+    CK(cudaGetLastError());
+    return d.rows.p;
+}
+
 // Column statistics of the raw rows (stats.rs:40) in one device pass about each column's first
 // value: sd (unweighted, floored at 1e-3), weighted mean, sum of squares, weighted centered and
 // uncentered sums of squares.
@@ -387,6 +408,7 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
 }
 
 void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out) {
+    AllocScope alloc_scope(ab_->stream());
     SessionDev& d = *d_;
     cudaStream_t st = d.st;
     const size_t n = n_, r = 1 + nx;
@@ -719,6 +741,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
 // multiway by inclusion-exclusion without an eigenvalue clip (iv.rs:612-640).
 void GpuSession::iv(double* rows_in, bool on_device, size_t nx, size_t ne, size_t ni, const IvSpec& spec,
                     IvOut& out) {
+    AllocScope alloc_scope(ab_->stream());
     SessionDev& d = *d_;
     cudaStream_t st = d.st;
     const size_t n = n_, r = 1 + nx + ne + ni;
@@ -924,6 +947,7 @@ void GpuSession::iv(double* rows_in, bool on_device, size_t nx, size_t ne, size_
 // one n x tile block residualized by the absorber as block-PCG columns; see boot.cuh.
 void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec& ospec, const BootSpec& bs,
                           BootOut& out) {
+    AllocScope alloc_scope(ab_->stream());
     if (ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg wildboot: the session has no cluster dimension");
     if (bs.coef >= nx) throw Error(RC_INVALID_INPUT, "fereg wildboot: coefficient index out of range");
     if (bs.reps == 0 || bs.tile == 0) throw Error(RC_INVALID_INPUT, "fereg wildboot: reps and tile must be positive");
@@ -1093,6 +1117,7 @@ void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec
 // N / (N - 1), clustered with G / (G - 1) and the multiway eigenvalue clip, or (logit `oim`)
 // the inverse Hessian (X~'WX~)^-1.
 void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out) {
+    AllocScope alloc_scope(ab_->stream());
     if (!wk_.empty()) throw Error(RC_INVALID_INPUT, "fereg glm: weighted sessions are not supported");
     if (gs.family != 0 && gs.family != 1) throw Error(RC_INVALID_INPUT, "fereg glm: family is 0 (Poisson) or 1 (logit)");
     const int fam = gs.family;

@@ -63,6 +63,11 @@ class GpuSession {
     void set_profiling(bool on);
     void phase_times(double* ms, u64* counts) const;  // GpuAbsorber::P_NSLOTS + S_NSLOTS slots
 
+    // Gathers R kept-order host columns (n values each) into the session's device row-order
+    // block (n x R row-major, the layout every estimator reads) and returns it; it stays valid
+    // until the next gather or estimator call with host rows.
+    double* gather_columns(const double* const* cols, size_t R);
+
     // OLS of column 0 on columns 1..nx of the n x (1 + nx) row-major block `rows` (row order;
     // host memory, or device memory when on_device). A device block is residualized in place; a
     // host block is copied to the device and left unchanged.

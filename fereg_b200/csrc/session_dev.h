@@ -23,6 +23,8 @@ struct SessionDev {
     DBuf<int> col, err;
     DBuf<u32> uf, flags, scan, bsum, total, gv, map;
     DBuf<double> pstat;
+    DBuf<double> colbuf;  // kept-order columns of a gather
+    DBuf<u32> pi;         // row order -> kept position
     cudaStream_t st = nullptr;
     u64 launches = 0;
     // phase timing (CUDA events on the session's stream)

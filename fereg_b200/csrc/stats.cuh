@@ -463,6 +463,17 @@ __global__ void __launch_bounds__(ST_TB) k_cluster_scores(const double* __restri
     }
 }
 
+// Row gather of kept-order columns into the row-order block: rows[i R + j] = cols[j n + pi[i]]
+// (the reference's Session::gather, session.rs, on the device). A warp per row chunk: lanes over
+// consecutive rows i read the index pi[i] once and write R values each.
+__global__ void k_gather_cols(const double* __restrict__ cols, const u32* __restrict__ pi, size_t n, int R,
+                              double* __restrict__ rows) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const size_t src = pi[i];
+        for (int j = 0; j < R; j++) rows[i * R + j] = cols[size_t(j) * n + src];
+    }
+}
+
 __global__ void k_zero_col(double* __restrict__ rows, size_t n, int R, int c) {
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
         rows[i * R + c] = 0.0;

@@ -271,6 +271,70 @@ int fereg_session_glm(fereg_session* s, double* rows, int rows_on_device, size_t
 int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
                           fereg_glm_out* out);
 
+/* Serving: a request loop over independent regressions on one GPU. Requests are admitted in
+ * arrival order while their estimated device memory fits the budget (hbm_budget bytes; 0 = 80%
+ * of the free memory at creation); `workers` requests run at once, each on its own session and
+ * CUDA stream. A request larger than the whole budget is rejected by fereg_server_submit (909).
+ * Results do not depend on the other requests in flight. dry_run: the scheduler alone, no GPU
+ * (each request sleeps dry_run_us; needs an explicit budget). */
+typedef struct fereg_server fereg_server;
+typedef struct fereg_server_config {
+    int workers;
+    size_t hbm_budget;
+    int dry_run;
+} fereg_server_config;
+
+#define FEREG_MODEL_OLS 0
+#define FEREG_MODEL_IV 1
+#define FEREG_MODEL_LOGIT 2
+#define FEREG_MODEL_POISSON 3
+
+/* One regression: the prepared sample as for fereg_session_create (kept order), the data as
+ * kept-order columns [y, exog (nx), endog (nendog), inst (ninst)], the estimator's options
+ * (vce as the estimator's own entry point; maxiter is the inner solve's) and caller buffers for
+ * b and V (k_all and k_all^2 values: OLS nx + 1, IV nendog + nx, GLM nx). Everything the
+ * request points to must stay valid until fereg_server_wait returns for it. */
+typedef struct fereg_request {
+    int model;
+    const uint32_t* const* codes;
+    const uint32_t* g;
+    int nterms;
+    const uint32_t* const* cl_codes;
+    const uint32_t* cl_g;
+    int ncl;
+    const double* w;
+    int weight_kind;
+    size_t n;
+    const double* const* cols;
+    size_t nx, nendog, ninst;
+    int vce;
+    double tol;
+    size_t maxiter;
+    int precision;
+    double* b;
+    double* V;
+    uint64_t dry_run_us;
+} fereg_request;
+
+typedef struct fereg_request_result {
+    int rc;                            /* the estimator's return code */
+    double submit_s, admit_s, done_s;  /* seconds since the server started */
+    uint64_t bytes;                    /* the admission estimate */
+    double N;
+    uint64_t iterations;               /* PCG iterations (GLM: over all IRLS steps) */
+    int32_t converged;
+} fereg_request_result;
+
+int fereg_server_create(const fereg_server_config* cfg, fereg_server** out);
+int fereg_server_submit(fereg_server* srv, const fereg_request* req, uint64_t* ticket);
+/* Blocks until the request is done; msg (msg_cap bytes, may be NULL) receives its error text.
+ * One waiter per ticket. */
+int fereg_server_wait(fereg_server* srv, uint64_t ticket, fereg_request_result* out, char* msg, size_t msg_cap);
+/* 7 values: submitted, completed, rejected, peak admitted bytes, peak running, budget, running. */
+int fereg_server_stats(const fereg_server* srv, uint64_t* out7);
+/* Waits for the running requests; pending ones are dropped. */
+void fereg_server_destroy(fereg_server* srv);
+
 /* Phase timing of the session's calls: the FEREG_PHASE_SLOTS slots of its absorber, then
  * 9 degrees of freedom, 10 column statistics, 11 Gram, 12 residuals and variance. */
 #define FEREG_SESSION_PHASE_SLOTS (FEREG_PHASE_SLOTS + 4)
