@@ -47,6 +47,9 @@ CONFIGS = {
     # countries x 50 years, 39,800 directed pairs x 5 rows (sectors) per pair-year, ~40% zeros,
     # robust SEs.
     "c4": dict(countries=200, years=50, sectors=5, seed=10**7 * 100 + 45, zero_share=0.40),
+    # Serving stream: 2,000 requests, exponential inter-arrivals at 70% of the measured capacity,
+    # n log-uniform in 1e4..5e6, 1-4 FEs, 60% OLS / 20% IV / 20% logit, 1-12 regressors.
+    "c5": dict(requests=2000, seed=10**6 * 100 + 46, load=0.7, tol=1e-10, cpu_sample=12),
 }
 TOL = 1e-8
 METRIC = "sec/call (1e7-obs 3-FE OLS)"
@@ -233,6 +236,315 @@ def run_glm(args, cfg, rank, world, local, pg):
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     sess.close()
+
+
+SERVE_METRIC = "served p99 latency (s), mixed stream of 2,000 regressions (60% OLS / 20% IV / 20% logit)"
+SERVE_NMAX = 5_000_000
+
+
+class ServePool:
+    """Seeded master columns (5e6 rows, pinned host memory) that the requests of the C5 stream
+    slice at offsets that are multiples of 10 (one individual = 10 consecutive rows):
+    x1..x12, z1, z2 ~ N(0, 1); endog = 0.7 z1 - 0.4 z2 + 0.5 u + N(0, 1) (u the structural error);
+    y = sum_j x_j / j + 0.5 endog + u + N(0, 1); ybin ~ Bernoulli(logistic(0.3 x1 - 0.2 x2)) with
+    rows 0 and 1 of every individual set to 1 and 0 (no individual without variation, so the
+    `fe` separation rule drops nothing)."""
+
+    def __init__(self, seed, pinned=True):
+        import torch
+
+        rng = np.random.default_rng(seed)
+        n = SERVE_NMAX
+        names = ["y", "ybin", "endog", "z1", "z2"] + [f"x{j}" for j in range(1, 13)]
+        self.buf = torch.empty((len(names), n), dtype=torch.float64, pin_memory=pinned)
+        a = self.buf.numpy()
+        self.col = {k: a[i] for i, k in enumerate(names)}
+        X = [rng.standard_normal(n) for _ in range(12)]
+        for j in range(12):
+            self.col[f"x{j + 1}"][:] = X[j]
+        self.col["z1"][:] = rng.standard_normal(n)
+        self.col["z2"][:] = rng.standard_normal(n)
+        u = rng.standard_normal(n)
+        self.col["endog"][:] = 0.7 * self.col["z1"] - 0.4 * self.col["z2"] + 0.5 * u + rng.standard_normal(n)
+        y = 0.5 * self.col["endog"] + u + rng.standard_normal(n)
+        for j in range(12):
+            y += X[j] / (j + 1)
+        self.col["y"][:] = y
+        p = 1 / (1 + np.exp(-(0.3 * X[0] - 0.2 * X[1])))
+        yb = (rng.random(n) < p).astype(np.float64)
+        yb[0::10] = 1.0
+        yb[1::10] = 0.0
+        self.col["ybin"][:] = yb
+
+
+def serve_request(i, seed, pool):
+    """Request i of the C5 stream (its own seed): n = exp(U(ln 1e4, ln 5e6)) rounded down to whole
+    individuals, 1-4 FEs among indiv (n/10), year (10), firm (n/50 levels; random, or cyclic
+    firm = (indiv + year) mod levels), occupation (100 levels, random); model 60% OLS / 20% IV
+    (1 endogenous regressor, 2 instruments) / 20% logit; 1-12 regressors; variance iid / robust /
+    cluster (on firm, or indiv when the request has no firm). Returns the submit arguments."""
+    rng = np.random.default_rng(seed + i)
+    n = int(np.exp(rng.uniform(np.log(1e4), np.log(SERVE_NMAX)))) // 10 * 10
+    off = int(rng.integers(0, (SERVE_NMAX - n) // 10 + 1)) * 10
+    u = rng.random()
+    model = "ols" if u < 0.6 else "iv" if u < 0.8 else "logit"
+    nfe = int(rng.integers(1, 5))
+    k = int(rng.integers(1, 13))
+    idx = np.arange(n, dtype=np.uint32)
+    ind = idx // 10
+    year = idx % 10
+    codes, g = [ind], [n // 10]
+    firm = None
+    if nfe >= 2:
+        codes.append(year)
+        g.append(10)
+    if nfe >= 3:
+        F = max(2, n // 50)
+        if rng.random() < 0.5:
+            firm = (ind + year) % F
+        else:
+            firm = rng.integers(0, F, n).astype(np.uint32)
+            present = np.bincount(firm, minlength=F) > 0
+            remap = (np.cumsum(present) - 1).astype(np.uint32)
+            firm = remap[firm]
+            F = int(present.sum())
+        codes.append(firm.astype(np.uint32))
+        g.append(F)
+    if nfe >= 4:
+        occ = rng.integers(0, 100, n).astype(np.uint32)
+        codes.append(occ)
+        g.append(100)
+    sl = slice(off, off + n)
+    c = pool.col
+    vce = ["unadjusted", "robust", "cluster"][int(rng.integers(0, 3))]
+    if model == "logit":
+        vce = {"unadjusted": "oim"}.get(vce, vce)
+    clusters, cl_g = [], []
+    if vce == "cluster":
+        if firm is not None:
+            clusters, cl_g = [codes[2]], [g[2]]
+        else:
+            clusters, cl_g = [ind], [n // 10]
+    if model == "iv":
+        nx = k - 1
+        cols = [c["y"][sl]] + [c[f"x{j}"][sl] for j in range(1, nx + 1)] + [c["endog"][sl], c["z1"][sl], c["z2"][sl]]
+        kw = dict(nendog=1, ninst=2)
+    elif model == "logit":
+        nx = k
+        cols = [c["ybin"][sl]] + [c[f"x{j}"][sl] for j in range(1, nx + 1)]
+        kw = {}
+    else:
+        nx = k
+        cols = [c["y"][sl]] + [c[f"x{j}"][sl] for j in range(1, nx + 1)]
+        kw = {}
+    return dict(model=model, codes=codes, g=g, cols=cols, nx=nx, clusters=clusters, cl_g=cl_g, vce=vce, n=n, kw=kw)
+
+
+def submit_request(srv, r, tol):
+    import fereg_b200 as fb
+
+    return srv.submit(r["model"], r["codes"], r["g"], r["cols"], r["nx"], clusters=r["clusters"], cl_g=r["cl_g"],
+                      vce=r["vce"], tol=tol, precision=fb.PREC_F64, **r["kw"])
+
+
+def run_serve(args, cfg, rank, world, local, pg):
+    """C5: a stream of 2,000 regressions with exponential inter-arrival times at ~70% of the
+    measured capacity through the serving engine (fereg_server_*); value = p99 latency (submit to
+    result) of the whole stream. The capacity is measured first on a burst of 64 requests
+    submitted at once (the warm-up)."""
+    nreq = cfg["requests"]
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        run_serve_reference(args, cfg, world)
+        return
+    import torch
+
+    import fereg_b200 as fb
+
+    torch.cuda.set_device(local)
+    pool = ServePool(cfg["seed"] + 7919 * rank)
+    srv = fb.Server(workers=args.serve_workers)
+    tol = cfg["tol"]
+
+    def collect(tickets, out):
+        for t in tickets:
+            out.append(srv.wait(t))
+
+    # capacity: a burst of 64 requests (seeds after the stream's) submitted at once
+    burst = [serve_request(nreq + 1000 + i, cfg["seed"], pool) for i in range(64)]
+    t0 = time.perf_counter()
+    tk = [submit_request(srv, r, tol) for r in burst]
+    res_b = [srv.wait(t) for t in tk]
+    burst_s = time.perf_counter() - t0
+    assert all(r["rc"] == 0 for r in res_b), [r["msg"] for r in res_b if r["rc"]]
+    rows_b = sum(r["n"] for r in burst)
+    cap_rows = rows_b / burst_s  # rows per second at full load
+    mean_rows = (SERVE_NMAX - 1e4) / np.log(SERVE_NMAX / 1e4)  # mean of the log-uniform n
+    rate = cfg["load"] * cap_rows / mean_rows  # requests per second
+    arrivals = np.cumsum(np.random.default_rng(cfg["seed"] - 1).exponential(1.0 / rate, nreq))
+    barrier(pg)
+    results, tickets = [], []
+    lock = threading.Lock()
+    done_list = []
+    waiter_q = []
+    cv = threading.Condition(lock)
+
+    def waiter():
+        i = 0
+        while i < nreq:
+            with cv:
+                while len(waiter_q) <= i:
+                    cv.wait()
+                t = waiter_q[i]
+            done_list.append(srv.wait(t))
+            i += 1
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    rows_total = 0
+    mix = {"ols": 0, "iv": 0, "logit": 0}
+    late = []
+    h2d = d2h = 0
+    sample = []  # (index, request) of the CPU-baseline sample: the first requests with n <= 2e5
+    with ClockSampler(local) as clk:
+        t_start = time.perf_counter()
+        for i in range(nreq):
+            r = serve_request(i, cfg["seed"], pool)
+            rows_total += r["n"]
+            mix[r["model"]] += 1
+            h2d += r["n"] * (8 * len(r["cols"]) + 4 * (len(r["codes"]) + len(r["clusters"])))
+            k_all = r["nx"] + (1 if r["model"] == "ols" else 1 if r["model"] == "iv" else 0)
+            d2h += 8 * (k_all + k_all * k_all)
+            if r["n"] <= 200_000 and len(sample) < cfg["cpu_sample"]:
+                sample.append((i, r))
+            now = time.perf_counter() - t_start
+            if now < arrivals[i]:
+                time.sleep(arrivals[i] - now)
+            else:
+                late.append(now - arrivals[i])
+            t = submit_request(srv, r, tol)
+            with cv:
+                waiter_q.append(t)
+                cv.notify()
+        th.join()
+        wall = time.perf_counter() - t_start
+    res = done_list
+    bad = [r for r in res if r["rc"] != 0]
+    lat = np.array([r["done_s"] - r["submit_s"] for r in res])
+    queue = np.array([r["admit_s"] - r["submit_s"] for r in res])
+    first = min(r["submit_s"] for r in res)
+    last = max(r["done_s"] for r in res)
+    span = last - first
+    st = srv.stats()
+    p50, p99 = float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+    p99 = max_over_ranks(p99, pg, torch.device("cuda", local))
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = serve_cpu_sample(sample, [res[i] for i, _ in sample], tol)
+    if rank == 0:
+        line = {"metric": SERVE_METRIC, "value": p99, "unit": "s", "n_gpus": world, "steps": 1,
+                "warmup": 1, "ms_per_step": span * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "c5", "requests": nreq, "mix": mix, "rows_total": rows_total,
+                           "offered_rate_req_s": rate, "load": cfg["load"], "workers": args.serve_workers,
+                           "tol": tol, "burst_rows_per_s": cap_rows, "late_submits": len(late),
+                           "max_submit_lag_s": float(max(late)) if late else 0.0,
+                           "parallelism": f"replicas x{world}", "errors": len(bad),
+                           "l2": "inputs of most requests exceed L2; no flush"},
+                "p50_s": p50, "p99_s": p99, "mean_queue_s": float(queue.mean()),
+                "throughput_req_s": nreq * world / span, "throughput_rows_s": rows_total * world / span,
+                "server": st, "clocks": clk.summary(), "gpu_launches": st["launches"],
+                "e2e": {"value": p99, "unit": "s", "h2d_bytes_per_step": int(h2d / nreq),
+                        "d2h_bytes_per_step": int(d2h / nreq),
+                        "note": "a step is one request; host columns in, b and V out, submit to result"}}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu["cpu_baseline"]
+            line["parity_vs_oracle"] = cpu["parity"]
+        print(json.dumps(line), flush=True)
+    srv.close()
+
+
+def oracle_request(r, tol):
+    """The CPU oracle on one request: the session OLS, the 2SLS restatement on the oracle's
+    residualized block, or the absorbed logit IRLS. Returns b, V in the server's order."""
+    from oracle import glm as oglm
+    from oracle import iv as oiv
+    from oracle import oracle
+
+    cols = np.column_stack(r["cols"])
+    if r["model"] == "ols":
+        sess = oracle.Session(r["codes"], r["g"], r["clusters"], r["cl_g"])
+        z = np.ascontiguousarray(cols[sess.row_order()])
+        out = sess.ols(z, vce=r["vce"], tol=tol)
+        return out["b"], out["V"]
+    if r["model"] == "iv":
+        Yt = oiv.residualize(r["codes"], r["g"], cols, tol=tol)
+        sess = oracle.Session(r["codes"], r["g"], r["clusters"], r["cl_g"])
+        df_a = sess.ols(np.ascontiguousarray(cols[sess.row_order()][:, :2]), vce=r["vce"], tol=tol)["scalars"]["df_a"]
+        b, V, _, _ = oiv.tsls(Yt, r["nx"], 1, 2, vce=r["vce"], clusters=r["clusters"], df_a=int(df_a))
+        return b, V
+    cl = (r["clusters"][0], r["cl_g"][0]) if r["clusters"] else None
+    b, V, _, _, _ = oglm.irls_absorbed(r["codes"], r["g"], cols[:, 0], cols[:, 1:], "logit", r["vce"], cl, tol=tol)
+    return b, V
+
+
+def serve_cpu_sample(sample, served, tol):
+    """cpu_baseline of C5: the CPU oracle (all host threads) on a bounded sample of the stream's
+    requests, one after another; value = the p99 (the maximum, for the sample's size) of their
+    service times. The served results of the same requests are compared with the oracle's."""
+    from oracle import oracle
+
+    times, errs = [], []
+    rows = 0
+    for (i, r), s in zip(sample, served):
+        t0 = time.perf_counter()
+        b, V = oracle_request(r, tol)
+        times.append(time.perf_counter() - t0)
+        rows += r["n"]
+        kb = len(b)
+        se = np.sqrt(np.maximum(np.diag(V), 0.0))
+        eb = np.max(np.abs(s["b"][:kb] - b) / np.maximum(np.abs(b), se))
+        ev = np.max(np.abs(s["V"][:kb, :kb] - V) / np.max(np.abs(V)))
+        errs.append((float(eb), float(ev)))
+    return {"cpu_baseline": {"value": float(np.percentile(times, 99)), "unit": "s", "cores": oracle.max_threads(),
+                             "kind": "port",
+                             "sample": f"{len(sample)} requests of the stream with n <= 2e5 ({rows} rows), each run "
+                                       f"alone on the C++ FP64 oracle (session OLS, 2SLS on its residualized block, "
+                                       f"absorbed logit IRLS); service time only, no queueing; mean "
+                                       f"{float(np.mean(times)):.3f} s, {rows / sum(times):.3g} rows/s"},
+            "parity": {"requests": len(errs), "b_err": "|b - b_oracle| / max(|b_oracle|, se_oracle)",
+                       "max_rel_err_b": max(e[0] for e in errs),
+                       "max_rel_err_V": max(e[1] for e in errs)}}
+
+
+def run_serve_reference(args, cfg, world):
+    """The reference arm of C5: the CPU oracle serves the stream's first requests with n <= 2e5
+    one at a time (bounded sample); value = p99 of their service times."""
+    pool = ServePool(cfg["seed"], pinned=False)
+    sample = []
+    i = 0
+    while len(sample) < cfg["cpu_sample"]:
+        r = serve_request(i, cfg["seed"], pool)
+        if r["n"] <= 200_000:
+            sample.append(r)
+        i += 1
+    from oracle import oracle
+
+    times = []
+    for r in sample:
+        t0 = time.perf_counter()
+        oracle_request(r, cfg["tol"])
+        times.append(time.perf_counter() - t0)
+    v = float(np.percentile(times, 99))
+    line = {"impl": "reference", "metric": SERVE_METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": 1,
+            "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "c5", "requests": len(sample)},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": oracle.max_threads(), "kind": "port",
+                             "sample": f"the stream's first {len(sample)} requests with n <= 2e5, each alone on the "
+                                       f"C++ FP64 oracle; service time, no queueing"},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 BOOT_METRIC = "wild-boot reps/s (WCR11, 9,999 Rademacher draws, n=1e6, 3 FE, cluster firm 2e4)"
@@ -526,12 +838,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing (profiling runs)")
     ap.add_argument("--boot-tile", type=int, default=512, help="draws per block-PCG tile (c3)")
+    ap.add_argument("--serve-workers", type=int, default=8, help="requests in flight (c5)")
+    ap.add_argument("--requests", type=int, default=0, help="stream length override (c5)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.requests:
+        cfg["requests"] = args.requests
     rank, world, local, pg = dist_setup()
-    if args.config in ("c3", "c4"):
-        (run_boot if args.config == "c3" else run_glm)(args, cfg, rank, world, local, pg)
+    if args.config in ("c3", "c4", "c5"):
+        {"c3": run_boot, "c4": run_glm, "c5": run_serve}[args.config](args, cfg, rank, world, local, pg)
         if pg is not None:
             barrier(pg)
             pg.destroy_process_group()

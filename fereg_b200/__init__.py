@@ -93,7 +93,8 @@ class Request(C.Structure):
 
 class RequestResult(C.Structure):
     _fields_ = [("rc", C.c_int), ("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
-                ("bytes", C.c_uint64), ("N", C.c_double), ("iterations", C.c_uint64), ("converged", C.c_int32)]
+                ("bytes", C.c_uint64), ("N", C.c_double), ("iterations", C.c_uint64), ("converged", C.c_int32),
+                ("launches", C.c_uint64)]
 
 
 MODELS = {"ols": 0, "iv": 1, "logit": 2, "poisson": 3}
@@ -569,10 +570,10 @@ class Server:
         b, V, k_all = keep[6], keep[7], keep[11]
         return dict(rc=res.rc, msg=msg.value.decode(), b=b[:k_all], V=V[:k_all, :k_all], submit_s=res.submit_s,
                     admit_s=res.admit_s, done_s=res.done_s, bytes=int(res.bytes), N=res.N,
-                    iterations=int(res.iterations), converged=bool(res.converged))
+                    iterations=int(res.iterations), converged=bool(res.converged), launches=int(res.launches))
 
     def stats(self):
-        v = np.zeros(7, dtype=np.uint64)
+        v = np.zeros(8, dtype=np.uint64)
         _check(lib().fereg_server_stats(self.h, _p(v, u64p)))
-        keys = ["submitted", "completed", "rejected", "peak_bytes", "peak_running", "budget", "running"]
+        keys = ["submitted", "completed", "rejected", "peak_bytes", "peak_running", "budget", "running", "launches"]
         return {k: int(x) for k, x in zip(keys, v)}

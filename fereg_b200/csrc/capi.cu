@@ -535,6 +535,7 @@ int fereg_server_wait(fereg_server* srv, uint64_t ticket, fereg_request_result* 
         out->N = r.N;
         out->iterations = r.iterations;
         out->converged = r.converged ? 1 : 0;
+        out->launches = r.launches;
         if (msg && msg_cap) {
             const size_t k = std::min(msg_cap - 1, r.msg.size());
             std::copy(r.msg.begin(), r.msg.begin() + k, msg);
@@ -543,10 +544,10 @@ int fereg_server_wait(fereg_server* srv, uint64_t ticket, fereg_request_result* 
     });
 }
 
-int fereg_server_stats(const fereg_server* srv, uint64_t* out7) {
+int fereg_server_stats(const fereg_server* srv, uint64_t* out8) {
     return guard([&] {
-        if (!srv || !out7) throw Error(RC_INVALID_INPUT, "fereg_server_stats: NULL argument");
-        srv->s.stats(out7);
+        if (!srv || !out8) throw Error(RC_INVALID_INPUT, "fereg_server_stats: NULL argument");
+        srv->s.stats(out8);
     });
 }
 

@@ -100,6 +100,7 @@ void Server::stats(u64* out) const {
     out[4] = u64(peak_running_);
     out[5] = budget_;
     out[6] = u64(running_);
+    out[7] = launches_;
 }
 
 void Server::worker() {
@@ -129,6 +130,7 @@ void Server::worker() {
             in_use_ -= e->res.bytes;
             running_--;
             completed_++;
+            launches_ += e->res.launches;
             e->res.done_s = now();
             e->done = true;
         }
@@ -189,6 +191,7 @@ void Server::run(Entry& e) {
             res.iterations = o.pcg_iterations;
             res.converged = o.converged;
         }
+        res.launches = s.launches();
     } catch (const Error& ex) {
         res.rc = ex.rc;
         res.msg = ex.what();

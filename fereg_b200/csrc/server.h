@@ -53,6 +53,7 @@ struct ServeResult {
     u64 bytes = 0;
     double N = 0;
     u64 iterations = 0;
+    u64 launches = 0;  // kernels the request's session launched
     bool converged = true;
 };
 
@@ -65,7 +66,8 @@ class Server {
     ~Server();
     u64 submit(const ServeRequest& r);  // ticket; throws Error(909) when larger than the budget
     ServeResult wait(u64 ticket);       // blocks until the request is done
-    // submitted, completed, rejected, peak admitted bytes, peak running, budget, running
+    // submitted, completed, rejected, peak admitted bytes, peak running, budget, running, kernel
+    // launches of the completed requests
     void stats(u64* out) const;
 
    private:
@@ -81,7 +83,7 @@ class Server {
     int device_ = 0;
     bool dry_ = false;
     u64 budget_ = 0, in_use_ = 0, peak_ = 0;
-    u64 next_ = 1, submitted_ = 0, completed_ = 0, rejected_ = 0;
+    u64 next_ = 1, submitted_ = 0, completed_ = 0, rejected_ = 0, launches_ = 0;
     int running_ = 0, peak_running_ = 0;
     bool stop_ = false;
     std::chrono::steady_clock::time_point t0_;

@@ -323,6 +323,7 @@ typedef struct fereg_request_result {
     double N;
     uint64_t iterations;               /* PCG iterations (GLM: over all IRLS steps) */
     int32_t converged;
+    uint64_t launches;                 /* kernels the request launched */
 } fereg_request_result;
 
 int fereg_server_create(const fereg_server_config* cfg, fereg_server** out);
@@ -330,8 +331,9 @@ int fereg_server_submit(fereg_server* srv, const fereg_request* req, uint64_t* t
 /* Blocks until the request is done; msg (msg_cap bytes, may be NULL) receives its error text.
  * One waiter per ticket. */
 int fereg_server_wait(fereg_server* srv, uint64_t ticket, fereg_request_result* out, char* msg, size_t msg_cap);
-/* 7 values: submitted, completed, rejected, peak admitted bytes, peak running, budget, running. */
-int fereg_server_stats(const fereg_server* srv, uint64_t* out7);
+/* 8 values: submitted, completed, rejected, peak admitted bytes, peak running, budget, running,
+ * kernel launches of the completed requests. */
+int fereg_server_stats(const fereg_server* srv, uint64_t* out8);
 /* Waits for the running requests; pending ones are dropped. */
 void fereg_server_destroy(fereg_server* srv);
 
