@@ -519,10 +519,25 @@ void GpuAbsorber::ensure_precond() {
 
 namespace {
 
-// Lets `kernel` take `bytes` of dynamic shared memory (beyond the 48 KB default).
+// Lets `kernel` take `bytes` of dynamic shared memory (beyond the 48 KB default). The limit is a
+// per-kernel attribute shared by every thread and stream of the process, so it is always set to
+// the same value, the most the kernel can take (the per-block opt-in maximum less its static
+// shared memory): concurrent sessions that need different amounts then never lower the limit
+// under one another's launches.
 template <class K>
 void allow_smem(K kernel, size_t bytes) {
-    if (bytes > 48 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    if (bytes <= 48 * 1024) return;
+    static const int optin = [] {
+        int dev = 0, v = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        return v;
+    }();
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, kernel));
+    const int lim = optin - int(fa.sharedSizeBytes);
+    if (bytes > size_t(lim)) throw Error(RC_INTERNAL, "fereg: a kernel needs more shared memory than a block can take");
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
 }
 
 // Per-CTA partial rows of the small coordinates: GRID_S rows of the short-segment kernels, then
