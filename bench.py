@@ -280,7 +280,7 @@ class ServePool:
 def serve_request(i, seed, pool):
     """Request i of the C5 stream (its own seed): n = exp(U(ln 1e4, ln 5e6)) rounded down to whole
     individuals, 1-4 FEs among indiv (n/10), year (10), firm (n/50 levels; random, or cyclic
-    firm = (indiv + year) mod levels), occupation (100 levels, random); model 60% OLS / 20% IV
+    firm = row mod levels as in the 1e7 panel), occupation (100 levels, random); model 60% OLS / 20% IV
     (1 endogenous regressor, 2 instruments) / 20% logit; 1-12 regressors; variance iid / robust /
     cluster (on firm, or indiv when the request has no firm). Returns the submit arguments."""
     rng = np.random.default_rng(seed + i)
@@ -301,7 +301,7 @@ def serve_request(i, seed, pool):
     if nfe >= 3:
         F = max(2, n // 50)
         if rng.random() < 0.5:
-            firm = (ind + year) % F
+            firm = idx % F  # cyclic, as in the 1e7 panel: firm = row mod levels
         else:
             firm = rng.integers(0, F, n).astype(np.uint32)
             present = np.bincount(firm, minlength=F) > 0
@@ -406,11 +406,14 @@ def run_serve(args, cfg, rank, world, local, pg):
     mix = {"ols": 0, "iv": 0, "logit": 0}
     late = []
     h2d = d2h = 0
+    reqs_meta = []
     sample = []  # (index, request) of the CPU-baseline sample: the first requests with n <= 2e5
     with ClockSampler(local) as clk:
         t_start = time.perf_counter()
         for i in range(nreq):
             r = serve_request(i, cfg["seed"], pool)
+            reqs_meta.append({"model": r["model"], "n": r["n"], "nfe": len(r["codes"]), "nx": r["nx"], "vce": r["vce"],
+                              "R": len(r["cols"])})
             rows_total += r["n"]
             mix[r["model"]] += 1
             h2d += r["n"] * (8 * len(r["cols"]) + 4 * (len(r["codes"]) + len(r["clusters"])))
@@ -458,6 +461,10 @@ def run_serve(args, cfg, rank, world, local, pg):
                 "e2e": {"value": p99, "unit": "s", "h2d_bytes_per_step": int(h2d / nreq),
                         "d2h_bytes_per_step": int(d2h / nreq),
                         "note": "a step is one request; host columns in, b and V out, submit to result"}}
+        if args.dump:
+            with open(args.dump, "w") as f:
+                json.dump([{k: x[k] for k in ("submit_s", "admit_s", "done_s", "prep_s", "iterations", "launches")}
+                           | r for x, r in zip(res, reqs_meta)], f)
         if cpu is not None:
             line["cpu_baseline"] = cpu["cpu_baseline"]
             line["parity_vs_oracle"] = cpu["parity"]
@@ -840,6 +847,7 @@ def main():
     ap.add_argument("--boot-tile", type=int, default=512, help="draws per block-PCG tile (c3)")
     ap.add_argument("--serve-workers", type=int, default=8, help="requests in flight (c5)")
     ap.add_argument("--requests", type=int, default=0, help="stream length override (c5)")
+    ap.add_argument("--dump", default="", help="write per-request timings to this file (c5)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     cfg = dict(CONFIGS[args.config])

@@ -94,7 +94,7 @@ class Request(C.Structure):
 class RequestResult(C.Structure):
     _fields_ = [("rc", C.c_int), ("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
                 ("bytes", C.c_uint64), ("N", C.c_double), ("iterations", C.c_uint64), ("converged", C.c_int32),
-                ("launches", C.c_uint64)]
+                ("launches", C.c_uint64), ("prep_s", C.c_double)]
 
 
 MODELS = {"ols": 0, "iv": 1, "logit": 2, "poisson": 3}
@@ -570,7 +570,8 @@ class Server:
         b, V, k_all = keep[6], keep[7], keep[11]
         return dict(rc=res.rc, msg=msg.value.decode(), b=b[:k_all], V=V[:k_all, :k_all], submit_s=res.submit_s,
                     admit_s=res.admit_s, done_s=res.done_s, bytes=int(res.bytes), N=res.N,
-                    iterations=int(res.iterations), converged=bool(res.converged), launches=int(res.launches))
+                    iterations=int(res.iterations), converged=bool(res.converged), launches=int(res.launches),
+                    prep_s=res.prep_s)
 
     def stats(self):
         v = np.zeros(8, dtype=np.uint64)

@@ -536,6 +536,7 @@ int fereg_server_wait(fereg_server* srv, uint64_t ticket, fereg_request_result* 
         out->iterations = r.iterations;
         out->converged = r.converged ? 1 : 0;
         out->launches = r.launches;
+        out->prep_s = r.prep_s;
         if (msg && msg_cap) {
             const size_t k = std::min(msg_cap - 1, r.msg.size());
             std::copy(r.msg.begin(), r.msg.begin() + k, msg);

@@ -149,8 +149,10 @@ void Server::run(Entry& e) {
     }
     try {
         Ctx ctx;
+        const double t0 = now();
         GpuSession s(q.codes, q.g, q.cl_codes, q.cl_g, q.w, q.w ? q.weight_kind : 0, q.n, 0, ctx);
         double* rows = s.gather_columns(q.cols.data(), q.cols.size());
+        res.prep_s = now() - t0;
         const Precision prec = q.precision == 1 ? Precision::F32_REFINED : Precision::F64;
         if (q.model == 0) {
             OlsSpec sp;

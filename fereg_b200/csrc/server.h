@@ -50,6 +50,7 @@ struct ServeResult {
     int rc = 0;
     std::string msg;
     double submit_s = 0, admit_s = 0, done_s = 0;  // seconds since the server started
+    double prep_s = 0;  // session preparation (cell structure, uploads) and the row gather
     u64 bytes = 0;
     double N = 0;
     u64 iterations = 0;

@@ -324,6 +324,7 @@ typedef struct fereg_request_result {
     uint64_t iterations;               /* PCG iterations (GLM: over all IRLS steps) */
     int32_t converged;
     uint64_t launches;                 /* kernels the request launched */
+    double prep_s;                     /* session preparation and row gather (inside admit..done) */
 } fereg_request_result;
 
 int fereg_server_create(const fereg_server_config* cfg, fereg_server** out);
