@@ -184,6 +184,7 @@ def _setup(L):
     L.fereg_absorber_phase_times.argtypes = [P, f64p, u64p]
     L.fereg_absorber_launches.argtypes = [P]
     L.fereg_absorber_launches.restype = C.c_uint64
+    L.fereg_absorber_escalations.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
 
 
 def declared_symbols():
@@ -303,6 +304,12 @@ class Absorber:
 
     def launches(self):
         return int(lib().fereg_absorber_launches(self.h))
+
+    def escalations(self):
+        """Escalations so far (large blocks moved from Jacobi to the multigrid V-cycle)."""
+        e = C.c_uint64()
+        _check(lib().fereg_absorber_escalations(self.h, C.byref(e), None))
+        return int(e.value)
 
     # kernel-level parity hooks
     def apply(self, p):

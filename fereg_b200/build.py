@@ -18,7 +18,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
                   "-ccbin", "/usr/bin/g++"]
-SOURCES = ["structure.cpp", "absorber.cu", "session.cu", "server.cu", "capi.cu"]
+SOURCES = ["structure.cpp", "amg.cpp", "absorber.cu", "session.cu", "server.cu", "capi.cu"]
 
 
 def _headers():
@@ -35,7 +35,7 @@ def _compile(src, force):
         return obj, False
     cmd = [NVCC] + CUFLAGS + ["-x", "cu" if src.endswith(".cu") else "c++", "-c", srcp, "-o", obj]
     if not src.endswith(".cu"):
-        cmd = ["/usr/bin/g++", "-O3", "-std=c++17", "-fPIC", "-march=x86-64-v3", "-Wall", "-Wextra",
+        cmd = ["/usr/bin/g++", "-O3", "-std=c++17", "-fPIC", "-march=x86-64-v3", "-fopenmp", "-Wall", "-Wextra",
                "-I/usr/local/cuda/include", "-c", srcp, "-o", obj]
     subprocess.run(cmd, check=True)
     return obj, True
@@ -49,7 +49,7 @@ def build(force=False, verbose=True):
     relink = force or not os.path.exists(LIB) or any(c for _, c in results) or any(
         os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs)
     if relink:
-        subprocess.run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"], check=True)
+        subprocess.run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lgomp"], check=True)
     if verbose:
         print(f"built {LIB}" if relink else f"up to date: {LIB}")
     return LIB

@@ -10,10 +10,13 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <sstream>
 #include <type_traits>
 
 #include "absorber.h"
+#include "amg.cuh"
+#include "amg.h"
 #include "kernels.cuh"
 #include "weights.cuh"
 
@@ -106,7 +109,33 @@ void with_rcp(int Rc, u32 nb, F&& f) {
 }
 }  // namespace
 
+// Device form of an escalated block's hierarchy (amg.h) and its V-cycle work vectors.
+struct DevAmgBlock {
+    u32 off = 0, g = 0;  // the block's coordinates [off, off + g)
+    std::vector<DevAmgLevel> lv;
+    std::vector<DBuf<u32>> iu;     // CSR index arrays of every level
+    std::vector<DBuf<double>> dv;  // CSR values and dinv of every level
+    DBuf<double> minv;             // generalized inverse of the coarsest level
+    // per level l: right-hand side (l >= 1), output (l >= 1), and the residual / prolongated value
+    std::vector<DBuf<double>> wd;
+    std::vector<DBuf<float>> wf;
+};
+
+template <class T>
+std::vector<DBuf<T>>& amg_work(DevAmgBlock& a);
+template <>
+std::vector<DBuf<double>>& amg_work<double>(DevAmgBlock& a) {
+    return a.wd;
+}
+template <>
+std::vector<DBuf<float>>& amg_work<float>(DevAmgBlock& a) {
+    return a.wf;
+}
+
 struct Scratch {
+    // escalated large blocks
+    std::vector<DevAmgBlock> amg;
+    u64 escalations = 0;
     // structure
     DBuf<u32> seg_off, coord, cell_row, pl_off, pl_cell, pl_seg, pl_other;
     DevTiles seg_tiles, pull_tiles;      // CTA tiles of the long lists
@@ -264,6 +293,114 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
     refresh_weights(w);
 }
 
+// Escalation: the reference escalates once, when the probe finds slow contraction (cg.rs:24-37,
+// solve.rs:838-876). Every large block above 2 AMG_COARSE levels gets a multigrid hierarchy;
+// after new weights the hierarchies are rebuilt at the next solve without waiting for a probe.
+bool GpuAbsorber::escalate() {
+    if (amg_wanted_) return false;
+    bool any = false;
+    for (auto& b : hs_.blocks) any |= !b.small && b.g > 2 * AMG_COARSE;
+    if (!any) return false;
+    amg_wanted_ = true;
+    build_amg();
+    d_->escalations++;
+    return !d_->amg.empty();
+}
+
+constexpr u32 AMG_DENSE_MAX = 2048;  // the largest coarsest level inverted densely
+
+void GpuAbsorber::build_amg() {
+    AllocScope alloc_scope(stream_);
+    sync_host_weights();
+    d_->amg.clear();
+    for (size_t b = 0; b < hs_.blocks.size(); b++) {
+        const Block& B = hs_.blocks[b];
+        if (B.small || B.g <= 2 * AMG_COARSE) continue;
+        AmgHierarchy H =
+            amg_build(hs_, b, cell_w_.empty() ? nullptr : cell_w_.data(), n1_.data(), diag_.data(), red_.data());
+        const u32 nL = H.levels.back().n;
+        if (nL > AMG_DENSE_MAX) continue;  // aggregation stalled: the block keeps Jacobi
+        DevAmgBlock A;
+        A.off = B.off;
+        A.g = B.g;
+        const size_t L = H.levels.size();
+        auto up_u = [&](const std::vector<u32>& v) {
+            A.iu.emplace_back();
+            A.iu.back().upload(v, stream_);
+            return A.iu.size() - 1;
+        };
+        auto up_d = [&](const std::vector<double>& v) {
+            A.dv.emplace_back();
+            A.dv.back().upload(v, stream_);
+            return A.dv.size() - 1;
+        };
+        struct Idx {
+            size_t a[3], p[3], t[3], dinv;
+        };
+        std::vector<Idx> ix(L);
+        for (size_t l = 0; l < L; l++) {
+            const AmgLevel& Lv = H.levels[l];
+            ix[l].a[0] = up_u(Lv.A.ptr);
+            ix[l].a[1] = up_u(Lv.A.col);
+            ix[l].a[2] = up_d(Lv.A.val);
+            ix[l].dinv = up_d(Lv.dinv);
+            if (l + 1 < L) {
+                ix[l].p[0] = up_u(Lv.P.ptr);
+                ix[l].p[1] = up_u(Lv.P.col);
+                ix[l].p[2] = up_d(Lv.P.val);
+                ix[l].t[0] = up_u(Lv.Pt.ptr);
+                ix[l].t[1] = up_u(Lv.Pt.col);
+                ix[l].t[2] = up_d(Lv.Pt.val);
+            }
+        }
+        // the pointers, once every upload is in place (the buffer vectors no longer grow)
+        for (size_t l = 0; l < L; l++) {
+            const Idx& q = ix[l];
+            DevAmgLevel dl{};
+            dl.n = H.levels[l].n;
+            dl.A = DevCsr{A.iu[q.a[0]].p, A.iu[q.a[1]].p, A.dv[q.a[2]].p};
+            dl.dinv = A.dv[q.dinv].p;
+            if (l + 1 < L) {
+                dl.P = DevCsr{A.iu[q.p[0]].p, A.iu[q.p[1]].p, A.dv[q.p[2]].p};
+                dl.Pt = DevCsr{A.iu[q.t[0]].p, A.iu[q.t[1]].p, A.dv[q.t[2]].p};
+            }
+            A.lv.push_back(dl);
+        }
+        // generalized inverse of the coarsest level: unit-diagonal scaling over the nodes with a
+        // positive diagonal, grounded LDL^T, explicit inverse (the small block's kernels)
+        std::vector<u32> keep;
+        for (u32 i = 0; i < nL; i++)
+            if (H.coarse[size_t(i) * nL + i] > 0.0) keep.push_back(i);
+        const size_t k = keep.size();
+        std::vector<double> scale(k), ak(k * k);
+        for (size_t i = 0; i < k; i++) scale[i] = 1.0 / std::sqrt(H.coarse[size_t(keep[i]) * (nL + 1)]);
+        for (size_t i = 0; i < k; i++)
+            for (size_t j = 0; j < k; j++) ak[i * k + j] = H.coarse[size_t(keep[i]) * nL + keep[j]] * scale[i] * scale[j];
+        A.minv.alloc(size_t(nL) * nL);
+        CK(cudaMemsetAsync(A.minv.p, 0, size_t(nL) * nL * sizeof(double), stream_));
+        if (k > 0) {
+            DBuf<double> da, dd, dx, dscale;
+            DBuf<u32> dkeep;
+            da.upload(ak, stream_);
+            dd.alloc(k);
+            dx.alloc(k * k);
+            dscale.upload(scale, stream_);
+            dkeep.upload(keep, stream_);
+            k_ldlt_ground<<<1, 1024, 0, stream_>>>(da.p, dd.p, int(k));
+            k_ldlt_inverse<<<int((k + 127) / 128), 128, 0, stream_>>>(da.p, dd.p, int(k), dx.p);
+            k_expand_minv<<<grid_for(k * k), THREADS, 0, stream_>>>(dx.p, dkeep.p, dscale.p, int(k), nL, A.minv.p);
+            CK(cudaGetLastError());
+            d_->launches += 3;
+            CK(cudaStreamSynchronize(stream_));
+        }
+        d_->amg.push_back(std::move(A));
+    }
+    CK(cudaStreamSynchronize(stream_));
+}
+
+size_t GpuAbsorber::escalated_blocks() const { return d_->amg.size(); }
+u64 GpuAbsorber::escalations() const { return d_->escalations; }
+
 GpuAbsorber::~GpuAbsorber() {
     d_.reset();
     if (stream_) cudaStreamDestroy(stream_);
@@ -324,6 +461,7 @@ void GpuAbsorber::set_weights_device(const double* w_dev) {
     host_stale_ = true;
     dev_jacobi_ = m > 0;
     pre_fresh_ = false;
+    d.amg.clear();
 }
 
 // Copies the device weight state back into the host mirrors after set_weights_device.
@@ -405,6 +543,7 @@ void GpuAbsorber::refresh_weights(const double* w_kept) {
         red_[k] = diag_[k] <= REDUNDANT * nr_[k];
     }
     pre_fresh_ = false;
+    if (d_) d_->amg.clear();
     upload_weights();
 }
 
@@ -514,6 +653,7 @@ void GpuAbsorber::ensure_precond() {
         CK(cudaStreamSynchronize(stream_));
         small_ok_ = true;
     }
+    if (amg_wanted_ && d_->amg.empty()) build_amg();
     pre_fresh_ = true;
 }
 
@@ -616,6 +756,46 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
     d.end(h, st);
 }
 
+// One V(1,1) cycle (amg.cuh) on the block's slice of r into the same slice of z.
+template <class T>
+void launch_amg(Scratch& d, DevAmgBlock& A, const T* r, T* z, int R, cudaStream_t st) {
+    const size_t L = A.lv.size();
+    std::vector<DBuf<T>>& w = amg_work<T>(A);
+    if (w.size() != 3 * L) w.resize(3 * L);
+    std::vector<const T*> rin(L);
+    std::vector<T*> zout(L), z1(L);
+    rin[0] = r + size_t(A.off) * R;
+    zout[0] = z + size_t(A.off) * R;
+    for (size_t l = 0; l < L; l++) {
+        const size_t len = size_t(A.lv[l].n) * R;
+        if (l > 0) {
+            w[3 * l].alloc(len);
+            w[3 * l + 1].alloc(len);
+            rin[l] = w[3 * l].p;
+            zout[l] = w[3 * l + 1].p;
+        }
+        if (l + 1 < L) {
+            w[3 * l + 2].alloc(len);
+            z1[l] = w[3 * l + 2].p;
+        }
+    }
+    for (size_t l = 0; l + 1 < L; l++) {
+        const u32 nc = A.lv[l + 1].n;
+        k_amg_resid<T><<<grid_for(size_t(A.lv[l].n) * R), THREADS, 0, st>>>(A.lv[l], rin[l], R, z1[l]);
+        k_amg_restrict<T><<<grid_for(size_t(nc) * R), THREADS, 0, st>>>(A.lv[l].Pt, nc, z1[l], R, w[3 * (l + 1)].p);
+        d.launches += 2;
+    }
+    k_amg_dense<T><<<grid_for(size_t(A.lv[L - 1].n) * R), THREADS, 0, st>>>(A.minv.p, A.lv[L - 1].n, rin[L - 1], R,
+                                                                          zout[L - 1]);
+    d.launches++;
+    for (size_t l = L - 1; l-- > 0;) {
+        const size_t len = size_t(A.lv[l].n) * R;
+        k_amg_up1<T><<<grid_for(len), THREADS, 0, st>>>(A.lv[l], rin[l], zout[l + 1], R, z1[l]);
+        k_amg_up2<T><<<grid_for(len), THREADS, 0, st>>>(A.lv[l], rin[l], z1[l], R, zout[l]);
+        d.launches += 2;
+    }
+}
+
 template <class T>
 void launch_precond(Scratch& d, const DevStruct& S, bool small_ok, const T* r, T* z, int R, cudaStream_t st) {
     const int h = d.begin(GpuAbsorber::P_PRECOND, st);
@@ -628,6 +808,7 @@ void launch_precond(Scratch& d, const DevStruct& S, bool small_ok, const T* r, T
         k_small_apply<T><<<grid_for(size_t(ms) * R), THREADS, 0, st>>>(d.minv.p, ms, r, z, R);
         d.launches++;
     }
+    for (auto& a : d.amg) launch_amg<T>(d, a, r, z, R, st);  // escalated blocks replace their Jacobi values
     CK(cudaGetLastError());
     d.end(h, st);
 }
@@ -899,12 +1080,24 @@ SolveInfo GpuAbsorber::residualize_device(double* z_dev, size_t r, double tol, s
 // x0'rhs in cg_xconst and x0 (as T) in `x0` (null when d is the whole iterate). With `drop` > 0
 // a column also stops (state 2: another refinement round) once its preconditioned residual fell
 // by that factor. Returns the iterations run.
+// At PROBE_AT iterations after the start (and after a restart) the contraction
+// rhohat = (rho_12 / rho_7)^(1/5) of the slowest active column is measured (cg.rs:24-37,
+// 254-279); above PROBE_RATIO the system escalates (when `escalate` can) and PCG restarts from
+// the current x.
+constexpr int PROBE_FROM = 7, PROBE_AT = 12;
+constexpr double PROBE_RATIO = 0.6;
+
 template <class T>
 static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x, const T* b,
                    const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small, int R, double tol,
-                   double drop, u64 iters_done, size_t maxiter, bool x_is_start, const Ctx& ctx, cudaStream_t st) {
+                   double drop, u64 iters_done, size_t maxiter, bool x_is_start, const Ctx& ctx, cudaStream_t st,
+                   const std::function<bool()>& escalate) {
     const size_t m = S.m, tot = m * size_t(R);
     CgState cg = d.cg();
+    u64 it = 0;
+    std::vector<double> rho_from(R), rho_at(R);
+    std::vector<int> act(R);
+restart:
     if (x_is_start) {
         launch_apply<T>(d, S, W, x, R, q, t, part, small, st);
         k_sub<T><<<grid_for(tot), THREADS, 0, st>>>(r, b, q, tot);
@@ -923,7 +1116,6 @@ static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool sma
     d.end(h, st);
     CK(cudaStreamSynchronize(st));
     bool any_active = *d.h_nactive > 0;
-    u64 it = 0;
     int k = 0;
     while (any_active) {
         if (iters_done + it >= maxiter) {
@@ -951,10 +1143,26 @@ static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool sma
         k_update_p<T><<<grid_for(tot), THREADS, 0, st>>>(p, z, d.cg_beta.p, d.cg_active.p, u32(m), R);
         d.launches += 3;
         CK(cudaMemcpyAsync(d.h_nactive, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (escalate && (k == PROBE_FROM || k == PROBE_AT)) {
+            CK(cudaMemcpyAsync(k == PROBE_FROM ? rho_from.data() : rho_at.data(), d.cg_rho.p, R * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(act.data(), d.cg_active.p, R * sizeof(int), cudaMemcpyDeviceToHost, st));
+        }
         d.end(h, st);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(st));
         any_active = *d.h_nactive > 0;
+        if (escalate && any_active && k == PROBE_AT) {
+            double rho_hat = 0.0;
+            for (int j = 0; j < R; j++)
+                if (act[j] == 1 && rho_from[j] > 0.0)
+                    rho_hat = std::max(rho_hat, std::pow(rho_at[j] / rho_from[j], 1.0 / double(PROBE_AT - PROBE_FROM)));
+            if (rho_hat > PROBE_RATIO && escalate()) {
+                CK(cudaMemsetAsync(d.cg_ring.p, 0, size_t(R) * WINDOW * sizeof(double), st));
+                x_is_start = true;
+                goto restart;
+            }
+        }
     }
     return it;
 }
@@ -1035,6 +1243,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         CK(cudaMemcpyAsync(d.cg_xconst.p, zero.data(), r * 8, cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(d.cg_ring.p, 0, r * WINDOW * 8, st));
         const bool exact_pre = small_ok_ && hs_.m_small == hs_.m;
+        const std::function<bool()> esc = [this] { return escalate(); };
         if (exact_pre) {
             // x* = x + M^-1 (rhs - S x) (cg.rs:171-198)
             if (warm) {
@@ -1051,7 +1260,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         } else if (prec == Precision::F64) {
             iterations = run_pcg<double>(d, S, W, small_ok_, x, d.rhs.p, d.rhs.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p,
                                          d.t.p, d.part.p, d.small.p, R, tol, 0.0, 0, maxiter,
-                                         warm != nullptr, ctx_, st);
+                                         warm != nullptr, ctx_, st, esc);
             exact = false;
         } else {
             // FP32 inner PCG on the correction, FP64 true residual between rounds.
@@ -1081,7 +1290,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
                 d.launches += 3;
                 iterations += run_pcg<float>(d, S, W, small_ok_, d.fx.p, d.fb.p, d.frhs.p, d.fx0.p, d.fr.p, d.fz.p,
                                              d.fp.p, d.fq.p, d.ft.p, d.fpart.p, d.fsmall.p, R, tol,
-                                             REFINE_DROP, iterations, maxiter, false, ctx_, st);
+                                             REFINE_DROP, iterations, maxiter, false, ctx_, st, esc);
                 k_add_correction<<<grid_for(tot), THREADS, 0, st>>>(x, d.fx.p, tot);
                 d.launches++;
                 start_nonzero = true;
@@ -1135,6 +1344,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     d.collect();
     info.iterations = iterations;
     info.exact = exact;
+    info.escalated = !d.amg.empty();
     return info;
 }
 

@@ -80,6 +80,9 @@ class GpuAbsorber {
     void set_profiling(bool on);
     void phase_times(double* ms, u64* counts) const;
     u64 launches() const;
+    // Large blocks currently preconditioned by a multigrid V-cycle, and the escalations so far.
+    size_t escalated_blocks() const;
+    u64 escalations() const;
     void set_ctx(const Ctx& c) { ctx_ = c; }
     const Ctx& ctx() const { return ctx_; }
 
@@ -112,7 +115,13 @@ class GpuAbsorber {
     bool weighted_ = false;
     bool pre_fresh_ = false;
     bool small_ok_ = false;  // the dense small factor exists
+    bool amg_wanted_ = false;  // large blocks were escalated: rebuild their hierarchies on new weights
     std::unique_ptr<Scratch> d_;
+
+    // Escalation (cg.rs:24-37 probe, solve.rs:838 escalate_block): multigrid hierarchies of the
+    // large blocks; true when a stronger preconditioner now exists.
+    bool escalate();
+    void build_amg();
 
     void refresh_weights(const double* w_kept);
     void sync_host_weights() const;

@@ -216,6 +216,14 @@ int fereg_absorber_phase_times(const fereg_absorber* h, double* ms, uint64_t* co
 
 uint64_t fereg_absorber_launches(const fereg_absorber* h) { return h ? h->a.launches() : 0; }
 
+int fereg_absorber_escalations(const fereg_absorber* h, uint64_t* escalations, uint64_t* blocks) {
+    return guard([&] {
+        if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_escalations: NULL handle");
+        if (escalations) *escalations = h->a.escalations();
+        if (blocks) *blocks = h->a.escalated_blocks();
+    });
+}
+
 int fereg_absorber_info(const fereg_absorber* h, uint64_t* o) {
     return guard([&] {
         if (!h || !o) throw Error(RC_INVALID_INPUT, "fereg_absorber_info: NULL argument");

@@ -119,6 +119,10 @@ int fereg_absorber_phase_times(const fereg_absorber* h, double* ms, uint64_t* co
 
 /* Kernel launches issued by this handle so far. */
 uint64_t fereg_absorber_launches(const fereg_absorber* h);
+/* Escalations so far (cg.rs:24-37 probe: a large block whose Jacobi PCG contracts slower than
+ * 0.6 per iteration at iteration 12 gets a multigrid V-cycle, and PCG restarts), and the large
+ * blocks currently preconditioned that way. */
+int fereg_absorber_escalations(const fereg_absorber* h, uint64_t* escalations, uint64_t* blocks);
 
 /* Kernel-level entry points used by the parity tests (device work, host buffers). */
 /* n, m, g1, ncells, nb, m_small, fe1, small_work, blocks in the small super-block (9 values) */

@@ -1,0 +1,100 @@
+"""Escalation of a slowly contracting large block to the multigrid preconditioner.
+
+A ring firm graph (indiv x 10 years, firm = row mod F with F not a multiple of 10: each
+individual's 10 firms overlap the next individual's) has a Laplacian whose Jacobi-preconditioned
+PCG needs thousands of iterations. At iteration 12 the contraction estimate exceeds 0.6
+(cg.rs:24-37), the firm block escalates to the smoothed-aggregation V-cycle and PCG restarts from
+the current iterate. The converged answer must not change: residualized columns match the
+oracle (Jacobi only, run to the same tolerance) to 1e-8 relative in the W-norm, in FP64, in the
+FP32-refined solve and with weights; the iteration count falls by two orders of magnitude; a
+repeated solve gives the same bits.
+"""
+
+import numpy as np
+import pytest
+
+import fereg_b200 as fb
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def ring(n_ind, F, seed, years=10):
+    rng = np.random.default_rng(seed)
+    n = n_ind * years
+    i = np.arange(n)
+    ind = (i // years).astype(np.uint32)
+    year = (i % years).astype(np.uint32)
+    firm = (i % F).astype(np.uint32)
+    z = np.column_stack([rng.standard_normal(n) + np.sin(firm / 50.0), rng.standard_normal(n)])
+    return [ind, firm, year], [n_ind, F, years], z
+
+
+def residualize_both(codes, g, z, w=None, prec=fb.PREC_F64, tol=1e-10):
+    ab = fb.Absorber(codes, g, w)
+    pi = ab.row_order()
+    zr = np.ascontiguousarray(z[pi])
+    a = zr.copy()
+    info = ab.residualize(a, tol=tol, maxiter=100000, precision=prec)
+    ob = oracle.Absorber(codes, g, w)
+    assert np.array_equal(ob.row_order(), pi)
+    o = zr.copy()
+    oinfo = ob.residualize(o, tol=tol, maxiter=200000)
+    return ab, a, o, info, oinfo, (None if w is None else w[pi])
+
+
+def wnorm_err(a, o, w):
+    w = np.ones(len(a)) if w is None else w
+    return np.sqrt(np.sum(w[:, None] * (a - o) ** 2, axis=0) / np.sum(w[:, None] * o ** 2, axis=0)).max()
+
+
+@pytest.mark.parametrize("prec", [fb.PREC_F64, fb.PREC_F32_REFINED])
+def test_ring_graph_escalates_and_matches_oracle(prec):
+    codes, g, z = ring(20000, 3997, 1)
+    ab, a, o, info, oinfo, w = residualize_both(codes, g, z, prec=prec)
+    assert info["escalated"] and ab.escalations() == 1
+    assert oinfo["iterations"] > 400, oinfo  # Jacobi alone is slow on this graph
+    assert info["iterations"] < oinfo["iterations"] / 5, (info, oinfo)
+    assert wnorm_err(a, o, w) <= 1e-8
+
+
+def test_weighted_ring_graph_escalates():
+    codes, g, z = ring(15000, 2999, 2)
+    w = np.random.default_rng(3).uniform(0.5, 2.0, len(z))
+    ab, a, o, info, oinfo, wr = residualize_both(codes, g, z, w=w)
+    assert info["escalated"]
+    assert wnorm_err(a, o, wr) <= 1e-8
+
+
+def test_escalated_solve_is_deterministic_and_rebuilt_on_new_weights():
+    codes, g, z = ring(12000, 2399, 4)
+    ab = fb.Absorber(codes, g)
+    zr = np.ascontiguousarray(z[ab.row_order()])
+    a1 = zr.copy()
+    i1 = ab.residualize(a1, tol=1e-10, maxiter=100000)
+    a2 = zr.copy()
+    i2 = ab.residualize(a2, tol=1e-10, maxiter=100000)
+    assert i1["escalated"] and i2["escalated"] and np.array_equal(a1, a2)
+    assert ab.escalations() == 1  # the second solve reuses the hierarchy
+    w = np.random.default_rng(5).uniform(0.5, 2.0, len(z))
+    ab.set_weights(w[ab.row_order()])
+    a3 = zr.copy()
+    i3 = ab.residualize(a3, tol=1e-10, maxiter=100000)
+    assert i3["escalated"] and i3["iterations"] < 200  # rebuilt for the new weights at the start
+    ob = oracle.Absorber(codes, g, w)
+    o3 = zr.copy()
+    ob.residualize(o3, tol=1e-10, maxiter=200000)
+    assert wnorm_err(a3, o3, w[ab.row_order()]) <= 1e-8
+
+
+def test_easy_graph_does_not_escalate():
+    rng = np.random.default_rng(6)
+    n_ind, years, F = 5000, 10, 800
+    n = n_ind * years
+    ind = np.repeat(np.arange(n_ind), years).astype(np.uint32)
+    year = np.tile(np.arange(years), n_ind).astype(np.uint32)
+    firm = rng.integers(0, F, n).astype(np.uint32)
+    ab = fb.Absorber([ind, firm, year], [n_ind, F, years])
+    zr = np.ascontiguousarray(rng.standard_normal((n, 2))[ab.row_order()])
+    info = ab.residualize(zr, tol=1e-10, maxiter=100000)
+    assert not info["escalated"] and ab.escalations() == 0
