@@ -294,12 +294,13 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
 }
 
 // Escalation: the reference escalates once, when the probe finds slow contraction (cg.rs:24-37,
-// solve.rs:838-876). Every large block above 2 AMG_COARSE levels gets a multigrid hierarchy;
+// solve.rs:838-876). Every Jacobi-preconditioned block above 2 AMG_COARSE levels (the large
+// blocks, and the blocks of a small super-block without its dense factor) gets a hierarchy;
 // after new weights the hierarchies are rebuilt at the next solve without waiting for a probe.
 bool GpuAbsorber::escalate() {
     if (amg_wanted_) return false;
     bool any = false;
-    for (auto& b : hs_.blocks) any |= !b.small && b.g > 2 * AMG_COARSE;
+    for (auto& b : hs_.blocks) any |= (!b.small || !small_ok_) && b.g > 2 * AMG_COARSE;
     if (!any) return false;
     amg_wanted_ = true;
     build_amg();
@@ -315,7 +316,8 @@ void GpuAbsorber::build_amg() {
     d_->amg.clear();
     for (size_t b = 0; b < hs_.blocks.size(); b++) {
         const Block& B = hs_.blocks[b];
-        if (B.small || B.g <= 2 * AMG_COARSE) continue;
+        // large blocks, and the blocks of a small super-block too big for its dense factor
+        if ((B.small && small_ok_) || B.g <= 2 * AMG_COARSE) continue;
         AmgHierarchy H =
             amg_build(hs_, b, cell_w_.empty() ? nullptr : cell_w_.data(), n1_.data(), diag_.data(), red_.data());
         const u32 nL = H.levels.back().n;

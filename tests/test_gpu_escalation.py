@@ -48,9 +48,11 @@ def wnorm_err(a, o, w):
     return np.sqrt(np.sum(w[:, None] * (a - o) ** 2, axis=0) / np.sum(w[:, None] * o ** 2, axis=0)).max()
 
 
-@pytest.mark.parametrize("prec", [fb.PREC_F64, fb.PREC_F32_REFINED])
-def test_ring_graph_escalates_and_matches_oracle(prec):
-    codes, g, z = ring(20000, 3997, 1)
+@pytest.mark.parametrize("prec,n_ind,F", [(fb.PREC_F64, 20000, 3997), (fb.PREC_F32_REFINED, 20000, 3997),
+                                          (fb.PREC_F64, 30000, 6007)])
+def test_ring_graph_escalates_and_matches_oracle(prec, n_ind, F):
+    """F = 3997: a small block too big for the dense factor; F = 6007: a large block."""
+    codes, g, z = ring(n_ind, F, 1)
     ab, a, o, info, oinfo, w = residualize_both(codes, g, z, prec=prec)
     assert info["escalated"] and ab.escalations() == 1
     assert oinfo["iterations"] > 400, oinfo  # Jacobi alone is slow on this graph
