@@ -107,7 +107,7 @@ __global__ void k_cg_gamma(CgState st, int R) {
         if (st.active[j] == 1) {
             const double pq = st.pq[j];
             if (pq > 0.0 && isfinite(pq)) g = st.rho[j] / pq;
-            else st.active[j] = 0;
+            else st.active[j] = st.pfloor[j] > 0.0 ? 2 : 0;  // inner rounds: FP64 restart, not a stop
         }
         st.gamma[j] = g;
     }
@@ -175,7 +175,10 @@ __global__ void k_cg_stop(CgState st, int R, int k, double tol) {
             const double rn = st.rho_new[j];
             const bool done = k >= WINDOW && sum <= thr;
             const bool at_roundoff = rn <= st.floor_[j];
-            if (done || at_roundoff || !(rn > 0.0)) st.active[j] = 0;
+            // In an FP32 round (pfloor > 0) a breakdown or the FP32 round-off floor ends the round
+            // with another FP64 restart (state 2); only the window rule stops the column.
+            if (done) st.active[j] = 0;
+            else if (at_roundoff || !(rn > 0.0)) st.active[j] = st.pfloor[j] > 0.0 ? 2 : 0;
             else if (rn <= st.pfloor[j]) st.active[j] = 2;
             else beta = rn / st.rho[j];
         }

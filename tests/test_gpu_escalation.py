@@ -55,8 +55,10 @@ def test_ring_graph_escalates_and_matches_oracle(prec, n_ind, F):
     codes, g, z = ring(n_ind, F, 1)
     ab, a, o, info, oinfo, w = residualize_both(codes, g, z, prec=prec)
     assert info["escalated"] and ab.escalations() == 1
-    assert oinfo["iterations"] > 400, oinfo  # Jacobi alone is slow on this graph
-    assert info["iterations"] < oinfo["iterations"] / 5, (info, oinfo)
+    # Jacobi alone needs ~(F / 10) * 2 iterations on this ring (the oracle's exact dense small
+    # block solves F = 3997 directly; its Jacobi PCG needs > 1000 for F = 6007)
+    assert info["iterations"] < 150, info
+    assert F < 4096 or oinfo["iterations"] > 1000, oinfo
     assert wnorm_err(a, o, w) <= 1e-8
 
 
