@@ -295,15 +295,19 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
 
 // Escalation: the reference escalates once, when the probe finds slow contraction (cg.rs:24-37,
 // solve.rs:838-876). Every Jacobi-preconditioned block above 2 AMG_COARSE levels (the large
-// blocks, and the blocks of a small super-block without its dense factor) gets a hierarchy;
-// after new weights the hierarchies are rebuilt at the next solve without waiting for a probe.
+// blocks, and the blocks of a small super-block without its dense factor) gets a hierarchy.
+// New weights leave the hierarchies in place as a stale but still symmetric positive
+// preconditioner (the reference keeps stale factors across IRLS weights, solve.rs:554
+// stale_refresh_pays); they are rebuilt only when a later probe finds slow contraction again.
 bool GpuAbsorber::escalate() {
-    if (amg_wanted_) return false;
+    if (!d_->amg.empty() && !amg_stale_) return false;  // the hierarchies are current: nothing stronger
+    if (d_->amg.empty() && amg_wanted_) return false;    // aggregation stalled before: keep Jacobi
     bool any = false;
     for (auto& b : hs_.blocks) any |= (!b.small || !small_ok_) && b.g > 2 * AMG_COARSE;
     if (!any) return false;
     amg_wanted_ = true;
     build_amg();
+    amg_stale_ = false;
     d_->escalations++;
     return !d_->amg.empty();
 }
@@ -463,7 +467,7 @@ void GpuAbsorber::set_weights_device(const double* w_dev) {
     host_stale_ = true;
     dev_jacobi_ = m > 0;
     pre_fresh_ = false;
-    d.amg.clear();
+    amg_stale_ = true;
 }
 
 // Copies the device weight state back into the host mirrors after set_weights_device.
@@ -545,7 +549,7 @@ void GpuAbsorber::refresh_weights(const double* w_kept) {
         red_[k] = diag_[k] <= REDUNDANT * nr_[k];
     }
     pre_fresh_ = false;
-    if (d_) d_->amg.clear();
+    amg_stale_ = true;
     upload_weights();
 }
 
@@ -655,7 +659,6 @@ void GpuAbsorber::ensure_precond() {
         CK(cudaStreamSynchronize(stream_));
         small_ok_ = true;
     }
-    if (amg_wanted_ && d_->amg.empty()) build_amg();
     pre_fresh_ = true;
 }
 

@@ -115,7 +115,8 @@ class GpuAbsorber {
     bool weighted_ = false;
     bool pre_fresh_ = false;
     bool small_ok_ = false;  // the dense small factor exists
-    bool amg_wanted_ = false;  // large blocks were escalated: rebuild their hierarchies on new weights
+    bool amg_wanted_ = false;  // blocks were escalated (their hierarchies are kept across weights)
+    bool amg_stale_ = false;   // the hierarchies were built for earlier weights
     std::unique_ptr<Scratch> d_;
 
     // Escalation (cg.rs:24-37 probe, solve.rs:838 escalate_block): multigrid hierarchies of the

@@ -89,7 +89,9 @@ def test_escalated_solve_is_deterministic_and_rebuilt_on_new_weights():
     ab.set_weights(w[ab.row_order()])
     a3 = zr.copy()
     i3 = ab.residualize(a3, tol=1e-10, maxiter=100000)
-    assert i3["escalated"] and i3["iterations"] < 200  # rebuilt for the new weights at the start
+    # the hierarchy of the unit weights stays as a stale preconditioner; a probe that finds it
+    # slow rebuilds it for the new weights
+    assert i3["escalated"] and i3["iterations"] < 200
     ob = oracle.Absorber(codes, g, w)
     o3 = zr.copy()
     ob.residualize(o3, tol=1e-10, maxiter=200000)
