@@ -300,6 +300,14 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
 // preconditioner (the reference keeps stale factors across IRLS weights, solve.rs:554
 // stale_refresh_pays); they are rebuilt only when a later probe finds slow contraction again.
 bool GpuAbsorber::escalate() {
+    if (small_stale_) {  // a stale dense small factor is refreshed first, with stale hierarchies
+        refresh_small();
+        if (!d_->amg.empty() && amg_stale_) {
+            build_amg();
+            amg_stale_ = false;
+        }
+        return true;
+    }
     if (!d_->amg.empty() && !amg_stale_) return false;  // the hierarchies are current: nothing stronger
     if (d_->amg.empty() && amg_wanted_) return false;    // aggregation stalled before: keep Jacobi
     bool any = false;
@@ -310,6 +318,12 @@ bool GpuAbsorber::escalate() {
     amg_stale_ = false;
     d_->escalations++;
     return !d_->amg.empty();
+}
+
+void GpuAbsorber::refresh_small() {
+    pre_fresh_ = false;
+    ensure_precond();
+    small_stale_ = false;
 }
 
 constexpr u32 AMG_DENSE_MAX = 2048;  // the largest coarsest level inverted densely
@@ -466,7 +480,10 @@ void GpuAbsorber::set_weights_device(const double* w_dev) {
     weighted_ = true;
     host_stale_ = true;
     dev_jacobi_ = m > 0;
-    pre_fresh_ = false;
+    // the dense small factor of earlier weights stays as a stale preconditioner (the Jacobi
+    // factors are current); a slow probe refreshes it (escalate)
+    small_stale_ = small_ok_;
+    pre_fresh_ = small_ok_;
     amg_stale_ = true;
 }
 
@@ -1073,6 +1090,14 @@ SolveInfo GpuAbsorber::residualize(double* z, size_t r, double tol, size_t maxit
     return info;
 }
 
+SolveInfo GpuAbsorber::residualize_device_warm_last(double* z_dev, size_t r, double tol, size_t maxiter,
+                                                    Precision prec) {
+    AllocScope alloc_scope(stream_);
+    ctx_.check();
+    if (r == 0) return SolveInfo{1, false, true};
+    return solve(z_dev, r, tol, maxiter, false, nullptr, nullptr, prec, true);
+}
+
 SolveInfo GpuAbsorber::residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
                                           const double* warm, double* coefs, Precision prec) {
     AllocScope alloc_scope(stream_);
@@ -1174,7 +1199,7 @@ restart:
 
 // solve.rs:1141-1311 residualize.
 SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
-                             double* coefs, Precision prec) {
+                             double* coefs, Precision prec, bool warm_last) {
     SolveInfo info;
     const size_t m = hs_.m, g1 = hs_.g1;
     if (r == 0) {
@@ -1184,6 +1209,8 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     }
     ctx_.check();
     ensure_precond();
+    // the closed form x + M^-1 (rhs - S x) needs the current factor, not a stale one
+    if (small_stale_ && small_ok_ && hs_.m_small == hs_.m) refresh_small();
     const int R = int(r);
     const DevStruct S = d_->ds(hs_);
     const DevWeights W = d_->dw();
@@ -1212,7 +1239,18 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         ss1[j] = wsq - b1sq;
     }
     double* x = d.coefs.p;
-    if (warm) {
+    const bool have_last = warm_last && last_r_ == r && m > 0;
+    if (have_last) {  // the previous solution, already in place; zero the columns with ss0 = 0
+        std::vector<int> zc(r);
+        bool any = false;
+        for (size_t j = 0; j < r; j++) any |= (zc[j] = ss0[j] == 0.0) != 0;
+        if (any) {
+            d.cg_active.alloc(r);
+            CK(cudaMemcpyAsync(d.cg_active.p, zc.data(), r * sizeof(int), cudaMemcpyHostToDevice, st));
+            k_zero_masked<<<grid_for(m * r), THREADS, 0, st>>>(x, d.cg_active.p, m * r, R);
+            d.launches++;
+        }
+    } else if (warm) {
         std::vector<double> w0(warm, warm + m * r);
         for (size_t j = 0; j < r; j++)
             if (ss0[j] == 0.0)
@@ -1251,7 +1289,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         const std::function<bool()> esc = [this] { return escalate(); };
         if (exact_pre) {
             // x* = x + M^-1 (rhs - S x) (cg.rs:171-198)
-            if (warm) {
+            if (warm || have_last) {
                 launch_apply<double>(d, S, W, x, R, d.q.p, d.t.p, d.part.p, d.small.p, st);
                 k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhs.p, d.q.p, tot);
                 d.launches++;
@@ -1265,7 +1303,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         } else if (prec == Precision::F64) {
             iterations = run_pcg<double>(d, S, W, small_ok_, x, d.rhs.p, d.rhs.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p,
                                          d.t.p, d.part.p, d.small.p, R, tol, 0.0, 0, maxiter,
-                                         warm != nullptr, ctx_, st, esc);
+                                         warm != nullptr || have_last, ctx_, st, esc);
             exact = false;
         } else {
             // FP32 inner PCG on the correction, FP64 true residual between rounds.
@@ -1276,7 +1314,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.rhs.p, d.frhs.p, tot);
             d.launches++;
             iterations = 0;
-            bool start_nonzero = warm != nullptr;
+            bool start_nonzero = warm != nullptr || have_last;
             for (int round = 0; round < REFINE_ROUNDS; round++) {
                 // true residual b = rhs - S x in FP64, x'rhs, and the FP32 copies
                 if (start_nonzero) {
@@ -1346,6 +1384,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     CK(cudaGetLastError());
     if (want_coefs && coefs) CK(cudaMemcpyAsync(coefs, x, (m + g1) * r * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    last_r_ = r;
     d.collect();
     info.iterations = iterations;
     info.exact = exact;

@@ -65,6 +65,11 @@ class GpuAbsorber {
                           double* coefs, Precision prec = Precision::F64);
     SolveInfo residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
                                  const double* warm, double* coefs, Precision prec = Precision::F64);
+    // The same, warm-started from the reduced solution the previous solve left on the device
+    // (the IRLS warm start without the host round trip); the previous solve must have had the
+    // same column count.
+    SolveInfo residualize_device_warm_last(double* z_dev, size_t r, double tol, size_t maxiter,
+                                           Precision prec = Precision::F64);
 
     // FE fit of coefficient column `col` per row (row order) (absorber.rs:88).
     void fit_rows(const double* coefs, size_t r, size_t col, double* out) const;
@@ -123,13 +128,16 @@ class GpuAbsorber {
     // large blocks; true when a stronger preconditioner now exists.
     bool escalate();
     void build_amg();
+    void refresh_small();
 
     void refresh_weights(const double* w_kept);
     void sync_host_weights() const;
     void upload_weights();
     void ensure_precond();
     SolveInfo solve(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
-                    double* coefs, Precision prec);
+                    double* coefs, Precision prec, bool warm_last = false);
+    size_t last_r_ = 0;        // column count of the solution left in the solve scratch
+    bool small_stale_ = false;  // the dense small factor was built for earlier weights
 };
 
 }  // namespace fereg

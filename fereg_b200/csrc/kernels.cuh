@@ -228,6 +228,12 @@ __global__ void k_mask_copy(T* __restrict__ p, const T* __restrict__ z, const in
         p[i] = active[i % R] == 1 ? z[i] : T(0);
 }
 
+// x = 0 on the columns whose mask is 1 (warm starts of zero columns, solve.rs:1209-1217).
+__global__ void k_zero_masked(double* __restrict__ x, const int* __restrict__ mask, size_t total, int R) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x)
+        if (mask[i % R]) x[i] = 0.0;
+}
+
 // x += z on the active columns (exact preconditioner, cg.rs:171-198).
 template <class T>
 __global__ void k_add_active(T* __restrict__ x, const T* __restrict__ z, const int* __restrict__ active, size_t total, int R) {

@@ -1172,7 +1172,6 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
     const double highest = std::max(1e-12, 0.1 * gs.tol);
     double tol_in = std::max(1e-4, gs.tol);
     double dev_old = nanv(), dev = nanv();
-    std::vector<double> warm, coefs((ab_->coefs_len()) * r);
     bool have_warm = false, converged = false;
     std::vector<uint8_t> status(nx, 0);
     std::vector<size_t> kept;
@@ -1185,8 +1184,10 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
         k_glm_work<<<blocks, 256, 0, st>>>(raw.p, n, R, fam, mu.p, eta.p, B.p, z.p, w.p);
         d.launches++;
         ab_->set_weights_device(w.p);
-        const SolveInfo si = ab_->residualize_device(B.p, r, tol_in, gs.inner_maxiter, true,
-                                                     have_warm ? warm.data() : nullptr, coefs.data(), gs.prec);
+        // warm start: the previous iteration's reduced solution, left on the device
+        const SolveInfo si = have_warm ? ab_->residualize_device_warm_last(B.p, r, tol_in, gs.inner_maxiter, gs.prec)
+                                       : ab_->residualize_device(B.p, r, tol_in, gs.inner_maxiter, false, nullptr,
+                                                                 nullptr, gs.prec);
         pcg += si.iterations;
         std::vector<double> ss_res;
         const std::vector<double> G = outer_products(B.p, n, R, all, nullptr, false, w.p, nullptr, true, &ss_res);
@@ -1239,8 +1240,6 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
             }
         }
         if (!std::isfinite(dev)) throw Error(RC_CONVERGENCE, "fereg glm: the deviance is not finite");
-        std::swap(warm, coefs);
-        if (coefs.size() != warm.size()) coefs.resize(warm.size());
         have_warm = true;
         if (it > 1) {
             const double eps = std::fabs(dev - dev_old) / std::max(std::min(dev, dev_old), 0.1);
