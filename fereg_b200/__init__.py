@@ -396,7 +396,7 @@ class Session:
     def launches(self):
         return int(lib().fereg_session_launches(self.h))
 
-    PHASES = Absorber.PHASES + ["dof", "colstats", "gram", "variance"]
+    PHASES = Absorber.PHASES + ["dof", "colstats", "gram", "variance", "weights"]
 
     def set_profiling(self, on=True):
         _check(lib().fereg_session_set_profiling(self.h, int(on)))

@@ -1181,16 +1181,21 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
     for (size_t it = 1; it <= gs.maxiter; it++) {
         ab_->ctx().check();
         iters = it;
+        int ph = d.begin(S_WEIGHTS);
         k_glm_work<<<blocks, 256, 0, st>>>(raw.p, n, R, fam, mu.p, eta.p, B.p, z.p, w.p);
         d.launches++;
         ab_->set_weights_device(w.p);
+        d.end(ph);
         // warm start: the previous iteration's reduced solution, left on the device
         const SolveInfo si = have_warm ? ab_->residualize_device_warm_last(B.p, r, tol_in, gs.inner_maxiter, gs.prec)
                                        : ab_->residualize_device(B.p, r, tol_in, gs.inner_maxiter, false, nullptr,
                                                                  nullptr, gs.prec);
         pcg += si.iterations;
         std::vector<double> ss_res;
+        ph = d.begin(S_GRAM);
         const std::vector<double> G = outer_products(B.p, n, R, all, nullptr, false, w.p, nullptr, true, &ss_res);
+        d.end(ph);
+        ph = d.begin(S_VARIANCE);
         if (it == 1) {  // columns absorbed by the FE, then collinear ones
             const double ctol = std::min(1e-6, gs.tol / 10.0);
             std::vector<size_t> cand;
@@ -1239,6 +1244,7 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
                 dev = 2.0 * host_sum(GLM_TB);
             }
         }
+        d.end(ph);
         if (!std::isfinite(dev)) throw Error(RC_CONVERGENCE, "fereg glm: the deviance is not finite");
         have_warm = true;
         if (it > 1) {
@@ -1320,6 +1326,7 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
     out.iterations = iters;
     out.pcg_iterations = pcg;
     out.converged = converged;
+    d.collect();
     CK(cudaGetLastError());
 }
 }  // namespace fereg

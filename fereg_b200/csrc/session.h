@@ -59,7 +59,7 @@ class GpuSession {
     u64 launches() const;
 
     // Phase timing: the absorber's slots (GpuAbsorber::Slot), then the session's own.
-    enum Slot { S_DOF = 0, S_COLSTATS, S_GRAM, S_VARIANCE, S_NSLOTS };
+    enum Slot { S_DOF = 0, S_COLSTATS, S_GRAM, S_VARIANCE, S_WEIGHTS, S_NSLOTS };
     void set_profiling(bool on);
     void phase_times(double* ms, u64* counts) const;  // GpuAbsorber::P_NSLOTS + S_NSLOTS slots
 

@@ -343,8 +343,9 @@ int fereg_server_stats(const fereg_server* srv, uint64_t* out8);
 void fereg_server_destroy(fereg_server* srv);
 
 /* Phase timing of the session's calls: the FEREG_PHASE_SLOTS slots of its absorber, then
- * 9 degrees of freedom, 10 column statistics, 11 Gram, 12 residuals and variance. */
-#define FEREG_SESSION_PHASE_SLOTS (FEREG_PHASE_SLOTS + 4)
+ * 9 degrees of freedom, 10 column statistics, 11 Gram, 12 residuals and variance (GLM: the
+ * regression update and the deviance), 13 GLM working variables and the device weight refresh. */
+#define FEREG_SESSION_PHASE_SLOTS (FEREG_PHASE_SLOTS + 5)
 int fereg_session_set_profiling(fereg_session* s, int on);
 int fereg_session_phase_times(const fereg_session* s, double* ms, uint64_t* counts);
 
