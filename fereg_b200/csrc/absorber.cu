@@ -300,8 +300,10 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
 // preconditioner (the reference keeps stale factors across IRLS weights, solve.rs:554
 // stale_refresh_pays); they are rebuilt only when a later probe finds slow contraction again.
 bool GpuAbsorber::escalate() {
-    if (small_stale_) {  // a stale dense small factor is refreshed first, with stale hierarchies
-        refresh_small();
+    if (coord_stale_ || small_stale_) {  // stale preconditioner pieces are refreshed first
+        AllocScope alloc_scope(stream_);
+        refresh_coord();
+        if (small_stale_) refresh_small();
         if (!d_->amg.empty() && amg_stale_) {
             build_amg();
             amg_stale_ = false;
@@ -457,20 +459,9 @@ void GpuAbsorber::set_weights_device(const double* w_dev) {
     d.n1.alloc(g1);
     d.n1inv.alloc(g1);
     k_seg_weights<<<grid_for(g1), THREADS, 0, stream_>>>(d.cell_w.p, d.seg_off.p, u32(g1), d.n1.p, d.n1inv.p);
-    d.launches += 3;
-    if (m > 0) {
-        d.nr.alloc(m);
-        d.diag.alloc(m);
-        d.red.alloc(m);
-        d.inv_diag.alloc(m);
-        k_coord_weights<<<int(std::min<size_t>((m * 32 + THREADS - 1) / THREADS, size_t(GRID_T) * 4)), THREADS, 0,
-                          stream_>>>(d.pl_off.p, d.pl_cell.p, d.pl_seg.p, u32(m), d.cell_w.p, d.n1inv.p, d.nr.p,
-                                     d.diag.p, d.red.p, d.inv_diag.p);
-        d.launches++;
-    }
     d.wpart.alloc(GRID_V);
     k_vec_sum<<<GRID_V, 256, 0, stream_>>>(d.n1.p, g1, d.wpart.p);
-    d.launches++;
+    d.launches += 4;
     std::vector<double> part(GRID_V);
     CK(cudaMemcpyAsync(part.data(), d.wpart.p, GRID_V * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -479,18 +470,40 @@ void GpuAbsorber::set_weights_device(const double* w_dev) {
     for (double v : part) sw_ += v;
     weighted_ = true;
     host_stale_ = true;
-    dev_jacobi_ = m > 0;
-    // the dense small factor of earlier weights stays as a stale preconditioner (the Jacobi
-    // factors are current); a slow probe refreshes it (escalate)
+    // The coordinate weight state (nr, diag, the Jacobi factors) and the dense small factor of
+    // earlier weights stay as stale preconditioners, and hierarchies stay too: none of them
+    // changes the operator, only the iteration count. They are recomputed when a host reader
+    // needs the weight state or a slow probe asks for a stronger preconditioner (escalate);
+    // redundancy is structural (it does not depend on positive weights).
+    coord_stale_ = m > 0;
     small_stale_ = small_ok_;
     pre_fresh_ = small_ok_;
     amg_stale_ = true;
+}
+
+// nr, diag, redundant and the Jacobi factors on the device for the current cell weights.
+void GpuAbsorber::refresh_coord() const {
+    if (!coord_stale_) return;
+    const size_t m = hs_.m;
+    Scratch& d = *d_;
+    d.nr.alloc(m);
+    d.diag.alloc(m);
+    d.red.alloc(m);
+    d.inv_diag.alloc(m);
+    k_coord_weights<<<int(std::min<size_t>((m * 32 + THREADS - 1) / THREADS, size_t(GRID_T) * 4)), THREADS, 0,
+                      stream_>>>(d.pl_off.p, d.pl_cell.p, d.pl_seg.p, u32(m), d.cell_w.p, d.n1inv.p, d.nr.p, d.diag.p,
+                                 d.red.p, d.inv_diag.p);
+    d.launches++;
+    CK(cudaGetLastError());
+    coord_stale_ = false;
+    dev_jacobi_ = true;
 }
 
 // Copies the device weight state back into the host mirrors after set_weights_device.
 void GpuAbsorber::sync_host_weights() const {
     AllocScope alloc_scope(stream_);
     if (!host_stale_) return;
+    refresh_coord();
     const HostStructure& st = hs_;
     const size_t n = st.n, M = st.ncells, g1 = st.g1, m = st.m;
     Scratch& d = *d_;
@@ -517,6 +530,7 @@ void GpuAbsorber::refresh_weights(const double* w_kept) {
     const HostStructure& st = hs_;
     host_stale_ = false;
     dev_jacobi_ = false;
+    coord_stale_ = false;
     weighted_ = w_kept != nullptr;
     w_rows_.clear();
     cell_w_.clear();

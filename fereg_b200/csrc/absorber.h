@@ -115,7 +115,8 @@ class GpuAbsorber {
     mutable std::vector<double> w_rows_, cell_w_, n1_, nr_, diag_;
     mutable std::vector<uint8_t> red_;
     mutable bool host_stale_ = false;
-    bool dev_jacobi_ = false;  // inv_diag was computed on the device
+    mutable bool dev_jacobi_ = false;   // inv_diag was computed on the device
+    mutable bool coord_stale_ = false;  // nr / diag / Jacobi on the device are of earlier weights
     double sw_ = 0;
     bool weighted_ = false;
     bool pre_fresh_ = false;
@@ -129,6 +130,7 @@ class GpuAbsorber {
     bool escalate();
     void build_amg();
     void refresh_small();
+    void refresh_coord() const;
 
     void refresh_weights(const double* w_kept);
     void sync_host_weights() const;
