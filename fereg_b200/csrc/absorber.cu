@@ -144,6 +144,9 @@ struct Scratch {
     // weights
     DBuf<double> w_rows, cell_w, n1inv, nr, inv_diag, minv;
     DBuf<double> n1, diag, wpart;  // device weight refresh
+    DBuf<u32> cw_e0, cw_e1, cw_list_off;  // chunks of the coordinate lists (weights.cuh)
+    DBuf<double> cw_chunks;
+    u32 cw_nchunks = 0;
     DBuf<uint8_t> red;
     DBuf<int> wflag;
     // solve (FP64)
@@ -278,6 +281,20 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
     }
     if (hs_.m > 0) {
         PullTable pt = build_pull_table(hs_);
+        {  // chunks of the lists for the device weight refresh (weights.cuh)
+            std::vector<u32> e0, e1, loff(hs_.m + 1, 0);
+            for (size_t k = 0; k < hs_.m; k++) {
+                for (u32 a = pt.off[k]; a < pt.off[k + 1]; a += CW_CHUNK) {
+                    e0.push_back(a);
+                    e1.push_back(std::min<u32>(pt.off[k + 1], a + CW_CHUNK));
+                }
+                loff[k + 1] = u32(e0.size());
+            }
+            d_->cw_nchunks = u32(e0.size());
+            d_->cw_e0.upload(e0, stream_);
+            d_->cw_e1.upload(e1, stream_);
+            d_->cw_list_off.upload(loff, stream_);
+        }
         d_->pl_off.upload(pt.off, stream_);
         d_->pl_cell.upload(pt.cell, stream_);
         d_->pl_seg.upload(pt.seg, stream_);
@@ -470,12 +487,12 @@ void GpuAbsorber::set_weights_device(const double* w_dev) {
     for (double v : part) sw_ += v;
     weighted_ = true;
     host_stale_ = true;
-    // The coordinate weight state (nr, diag, the Jacobi factors) and the dense small factor of
-    // earlier weights stay as stale preconditioners, and hierarchies stay too: none of them
-    // changes the operator, only the iteration count. They are recomputed when a host reader
-    // needs the weight state or a slow probe asks for a stronger preconditioner (escalate);
-    // redundancy is structural (it does not depend on positive weights).
+    // nr is part of the operator (the diagonal of S P), so the coordinate weight state is
+    // recomputed now; the dense small factor and the hierarchies of earlier weights stay as
+    // stale preconditioners (they change the iteration count, not the operator) until a slow
+    // probe asks for a stronger preconditioner (escalate).
     coord_stale_ = m > 0;
+    refresh_coord();
     small_stale_ = small_ok_;
     pre_fresh_ = small_ok_;
     amg_stale_ = true;
@@ -490,10 +507,14 @@ void GpuAbsorber::refresh_coord() const {
     d.diag.alloc(m);
     d.red.alloc(m);
     d.inv_diag.alloc(m);
-    k_coord_weights<<<int(std::min<size_t>((m * 32 + THREADS - 1) / THREADS, size_t(GRID_T) * 4)), THREADS, 0,
-                      stream_>>>(d.pl_off.p, d.pl_cell.p, d.pl_seg.p, u32(m), d.cell_w.p, d.n1inv.p, d.nr.p, d.diag.p,
-                                 d.red.p, d.inv_diag.p);
-    d.launches++;
+    const u32 nch = d.cw_nchunks;
+    d.cw_chunks.alloc(size_t(nch) * sizeof(CwChunk) / sizeof(double));
+    CwChunk* ch = reinterpret_cast<CwChunk*>(d.cw_chunks.p);
+    k_coord_chunks<<<int(std::min<size_t>((size_t(nch) * 32 + THREADS - 1) / THREADS, size_t(GRID_T) * 8)), THREADS, 0,
+                     stream_>>>(d.cw_e0.p, d.cw_e1.p, nch, d.pl_cell.p, d.pl_seg.p, d.cell_w.p, d.n1inv.p, ch);
+    k_coord_combine<<<grid_for(m), THREADS, 0, stream_>>>(d.cw_list_off.p, u32(m), ch, d.n1inv.p, d.nr.p, d.diag.p,
+                                                          d.red.p, d.inv_diag.p);
+    d.launches += 2;
     CK(cudaGetLastError());
     coord_stale_ = false;
     dev_jacobi_ = true;

@@ -4,9 +4,9 @@
 // diag_k = n_k - sum_s c_{s,k}^2 / n1_s with c_{s,k} the weight of k's cells in segment s; k is
 // redundant when diag_k <= 1e-12 n_k (operator.rs:21), and the Jacobi factor is 1 / diag_k
 // otherwise. The coordinate-sorted lists hold each coordinate's cells in cell order, hence in
-// segment order, so c_{s,k} are the sums over runs of equal segment: a warp walks a list 32
-// entries at a time with a segmented scan and carries the open run into the next chunk. All
-// sums have a fixed order.
+// segment order, so c_{s,k} are the sums over runs of equal segment: warps walk chunks of the
+// lists 32 entries at a time with a segmented scan, and a per-coordinate pass stitches the runs
+// that cross chunk boundaries. All sums have a fixed order.
 #pragma once
 
 #include "device.cuh"
@@ -42,17 +42,32 @@ __global__ void k_seg_weights(const double* __restrict__ cw, const u32* __restri
     }
 }
 
-// n_k, diag_k, redundant_k and the Jacobi factor of every coordinate; a warp per list.
-__global__ void k_coord_weights(const u32* __restrict__ pl_off, const u32* __restrict__ pl_cell,
-                                const u32* __restrict__ pl_seg, u32 m, const double* __restrict__ cw,
-                                const double* __restrict__ n1inv, double* __restrict__ nr, double* __restrict__ diag,
-                                uint8_t* __restrict__ red, double* __restrict__ inv_diag) {
+// n_k, diag_k, redundant_k and the Jacobi factor of every coordinate, in two passes so that a
+// long list (a 10-level year block holds n/10 entries per list) does not serialize on one warp.
+//
+// Pass 1, a warp per chunk of at most CW_CHUNK entries of one list: the chunk's sum of weights,
+// its sum of squared runs as if the chunk were the whole list (dq_iso = sum_runs x^2 / n1_s), and
+// its first and last runs (segment, partial sum). A segment's entries are contiguous in a list
+// (lists are in cell order, cells in segment order), so the first run is every entry of the
+// first entry's segment, and likewise for the last.
+constexpr u32 CW_CHUNK = 512;
+
+struct CwChunk {
+    double nr, dq, xf, xl;
+    u32 sf, sl;
+};
+
+__global__ void k_coord_chunks(const u32* __restrict__ chunk_e0, const u32* __restrict__ chunk_e1, u32 nchunks,
+                               const u32* __restrict__ pl_cell, const u32* __restrict__ pl_seg,
+                               const double* __restrict__ cw, const double* __restrict__ n1inv,
+                               CwChunk* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const size_t gw = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5, nw = (size_t(gridDim.x) * blockDim.x) >> 5;
     constexpr u32 NONE = 0xffffffffu;
-    for (size_t k = gw; k < m; k += nw) {
-        const u32 e0 = pl_off[k], e1 = pl_off[k + 1];
-        double nr_acc = 0.0, dq_acc = 0.0;
+    for (size_t c = gw; c < nchunks; c += nw) {
+        const u32 e0 = chunk_e0[c], e1 = chunk_e1[c];
+        const u32 sf = pl_seg[e0], sl = pl_seg[e1 - 1];
+        double nr_acc = 0.0, dq_acc = 0.0, xf = 0.0, xl = 0.0;
         u32 carry_s = NONE;
         double carry = 0.0;
         for (u32 base = e0; base < e1; base += 32) {
@@ -61,11 +76,12 @@ __global__ void k_coord_weights(const u32* __restrict__ pl_off, const u32* __res
             const double wv = valid ? (cw ? cw[pl_cell[e]] : 1.0) : 0.0;
             const u32 s = valid ? pl_seg[e] : NONE;
             nr_acc += wv;
-            // the run carried from the previous chunk ends here unless this chunk continues it
+            if (s == sf) xf += wv;
+            if (s == sl) xl += wv;
+            // the run carried from the previous sub-chunk ends here unless this one continues it
             const u32 s0 = __shfl_sync(FULL, s, 0);
             if (lane == 0 && carry_s != NONE && s0 != carry_s) dq_acc += carry * carry * n1inv[carry_s];
-            // inclusive scan of wv over the lane's run (runs are contiguous: equal segment at
-            // distance d means the whole span is one run)
+            // inclusive scan of wv over the lane's run (runs are contiguous)
             double x = wv;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
@@ -73,14 +89,14 @@ __global__ void k_coord_weights(const u32* __restrict__ pl_off, const u32* __res
                 const u32 sy = __shfl_up_sync(FULL, s, d);
                 if (lane >= d && sy == s) x += y;
             }
-            if (valid && s == carry_s) x += carry;  // the run left open by the previous chunk
+            if (valid && s == carry_s) x += carry;  // the run left open by the previous sub-chunk
             const u32 s_next = __shfl_down_sync(FULL, s, 1);
             const bool tail = valid && (lane == 31 || s_next != s);
             const int last = int(min(31u, e1 - 1 - base));
             const u32 s_last = __shfl_sync(FULL, s, last);
             const double x_last = __shfl_sync(FULL, x, last);
-            const bool final_chunk = base + 32 >= e1;
-            if (tail && (final_chunk || s != s_last)) dq_acc += x * x * n1inv[s];
+            const bool final_sub = base + 32 >= e1;
+            if (tail && (final_sub || s != s_last)) dq_acc += x * x * n1inv[s];
             carry_s = s_last;
             carry = x_last;
         }
@@ -88,15 +104,50 @@ __global__ void k_coord_weights(const u32* __restrict__ pl_off, const u32* __res
         for (int d = 16; d > 0; d >>= 1) {
             nr_acc += __shfl_down_sync(FULL, nr_acc, d);
             dq_acc += __shfl_down_sync(FULL, dq_acc, d);
+            xf += __shfl_down_sync(FULL, xf, d);
+            xl += __shfl_down_sync(FULL, xl, d);
         }
-        if (lane == 0) {
-            const double dg = nr_acc - dq_acc;
-            const bool r = dg <= 1e-12 * nr_acc;
-            nr[k] = nr_acc;
-            diag[k] = dg;
-            red[k] = r ? 1 : 0;
-            inv_diag[k] = (r || !(dg > 0.0)) ? 0.0 : 1.0 / dg;
+        if (lane == 0) out[c] = CwChunk{nr_acc, dq_acc, xf, xl, sf, sl};
+    }
+}
+
+// Pass 2, a thread per coordinate: the chunks of its list in order. Sums of nr and dq_iso; a run
+// that spans chunks (its parts x_i) contributes (sum x_i)^2 - sum x_i^2 more. Then diag_k =
+// n_k - dq_k, redundant when diag_k <= 1e-12 n_k (operator.rs:21), Jacobi factor 1 / diag_k.
+__global__ void k_coord_combine(const u32* __restrict__ list_chunk_off, u32 m, const CwChunk* __restrict__ ch,
+                                const double* __restrict__ n1inv, double* __restrict__ nr, double* __restrict__ diag,
+                                uint8_t* __restrict__ red, double* __restrict__ inv_diag) {
+    constexpr u32 NONE = 0xffffffffu;
+    for (u32 k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        double n_acc = 0.0, dq = 0.0, X = 0.0, Q = 0.0;
+        u32 cs = NONE;
+        for (u32 c = list_chunk_off[k]; c < list_chunk_off[k + 1]; c++) {
+            const CwChunk h = ch[c];
+            n_acc += h.nr;
+            dq += h.dq;
+            if (h.sf == cs) {
+                X += h.xf;
+                Q += h.xf * h.xf;
+            } else {
+                if (cs != NONE) dq += (X * X - Q) * n1inv[cs];
+                cs = h.sf;
+                X = h.xf;
+                Q = h.xf * h.xf;
+            }
+            if (h.sl != h.sf) {  // the chunk holds more runs: the carried run ends at its first
+                dq += (X * X - Q) * n1inv[cs];
+                cs = h.sl;
+                X = h.xl;
+                Q = h.xl * h.xl;
+            }
         }
+        if (cs != NONE) dq += (X * X - Q) * n1inv[cs];
+        const double dg = n_acc - dq;
+        const bool r = dg <= 1e-12 * n_acc;
+        nr[k] = n_acc;
+        diag[k] = dg;
+        red[k] = r ? 1 : 0;
+        inv_diag[k] = (r || !(dg > 0.0)) ? 0.0 : 1.0 / dg;
     }
 }
 
