@@ -317,17 +317,21 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
 // preconditioner (the reference keeps stale factors across IRLS weights, solve.rs:554
 // stale_refresh_pays); they are rebuilt only when a later probe finds slow contraction again.
 bool GpuAbsorber::escalate() {
-    if (coord_stale_ || small_stale_) {  // stale preconditioner pieces are refreshed first
-        AllocScope alloc_scope(stream_);
+    AllocScope alloc_scope(stream_);
+    // one step per probe, cheapest first: a stale dense small factor, then stale hierarchies,
+    // then new hierarchies
+    if (small_stale_) {
         refresh_coord();
-        if (small_stale_) refresh_small();
-        if (!d_->amg.empty() && amg_stale_) {
-            build_amg();
-            amg_stale_ = false;
-        }
+        refresh_small();
         return true;
     }
-    if (!d_->amg.empty() && !amg_stale_) return false;  // the hierarchies are current: nothing stronger
+    if (!d_->amg.empty() && amg_stale_) {
+        build_amg();
+        amg_stale_ = false;
+        d_->escalations++;
+        return true;
+    }
+    if (!d_->amg.empty()) return false;  // the hierarchies are current: nothing stronger
     if (d_->amg.empty() && amg_wanted_) return false;    // aggregation stalled before: keep Jacobi
     bool any = false;
     for (auto& b : hs_.blocks) any |= (!b.small || !small_ok_) && b.g > 2 * AMG_COARSE;
