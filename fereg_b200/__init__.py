@@ -287,7 +287,8 @@ class Absorber:
             o += int(gq)
         return res
 
-    PHASES = ["rhs_seg", "rhs_pull", "apply_seg", "precond", "vector", "residualize", "h2d", "d2h", "apply_pull"]
+    PHASES = ["rhs_seg", "rhs_pull", "apply_seg", "precond", "vector", "residualize", "h2d", "d2h", "apply_pull",
+              "escalate"]
 
     def stream(self):
         """The handle's cudaStream_t as an integer."""

@@ -8,6 +8,7 @@
 // rounds (iterative refinement); the stopping rule is evaluated on the FP64 quantities.
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -318,6 +319,17 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
 // stale_refresh_pays); they are rebuilt only when a later probe finds slow contraction again.
 bool GpuAbsorber::escalate() {
     AllocScope alloc_scope(stream_);
+    const auto t0 = std::chrono::steady_clock::now();
+    struct Clock {  // host wall time of the escalation step into its phase slot
+        Scratch& d;
+        std::chrono::steady_clock::time_point t0;
+        ~Clock() {
+            if (!d.prof) return;
+            d.ms[GpuAbsorber::P_ESCALATE] +=
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            d.cnt[GpuAbsorber::P_ESCALATE]++;
+        }
+    } clock{*d_, t0};
     // one step per probe, cheapest first: a stale dense small factor, then stale hierarchies,
     // then new hierarchies
     if (small_stale_) {

@@ -81,7 +81,19 @@ class GpuAbsorber {
     // Phase timing with CUDA events on the solver's stream (the reference's PhaseTimer,
     // timing.rs): per-slot milliseconds and launch counts, accumulated while enabled.
     // P_APPLY is the segment pass of S*P, P_APPLY_PULL its coordinate-list pass.
-    enum Slot { P_RHS_SEG = 0, P_RHS_PULL, P_APPLY, P_PRECOND, P_VECTOR, P_RESID, P_H2D, P_D2H, P_APPLY_PULL, P_NSLOTS };
+    enum Slot {
+        P_RHS_SEG = 0,
+        P_RHS_PULL,
+        P_APPLY,
+        P_PRECOND,
+        P_VECTOR,
+        P_RESID,
+        P_H2D,
+        P_D2H,
+        P_APPLY_PULL,
+        P_ESCALATE,
+        P_NSLOTS
+    };
     void set_profiling(bool on);
     void phase_times(double* ms, u64* counts) const;
     u64 launches() const;

@@ -112,8 +112,9 @@ void* fereg_absorber_stream(const fereg_absorber* h);
  * reported under verbose >= 2 as in solve.rs:387-392). Enabling resets the totals. Slots
  * (FEREG_PHASE_SLOTS): 0 rhs segment pass, 1 rhs coordinate-list pass, 2 operator S*P segment
  * pass, 3 preconditioner, 4 PCG vector work, 5 residualize pass, 6 host-to-device rows,
- * 7 device-to-host rows, 8 operator S*P coordinate-list pass. */
-#define FEREG_PHASE_SLOTS 9
+ * 7 device-to-host rows, 8 operator S*P coordinate-list pass, 9 escalations and preconditioner
+ * refreshes (host wall time of the factor / hierarchy builds). */
+#define FEREG_PHASE_SLOTS 10
 int fereg_absorber_set_profiling(fereg_absorber* h, int on);
 int fereg_absorber_phase_times(const fereg_absorber* h, double* ms, uint64_t* counts);
 
