@@ -317,7 +317,11 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
 // New weights leave the hierarchies in place as a stale but still symmetric positive
 // preconditioner (the reference keeps stale factors across IRLS weights, solve.rs:554
 // stale_refresh_pays); they are rebuilt only when a later probe finds slow contraction again.
-bool GpuAbsorber::escalate() {
+// A stale hierarchy is rebuilt only on clearly slow contraction (a rebuild costs a host
+// assembly; a stale V-cycle still contracts far faster than Jacobi).
+constexpr double STALE_AMG_RATIO = 0.85;
+
+bool GpuAbsorber::escalate(double rho_hat) {
     AllocScope alloc_scope(stream_);
     const auto t0 = std::chrono::steady_clock::now();
     struct Clock {  // host wall time of the escalation step into its phase slot
@@ -338,6 +342,7 @@ bool GpuAbsorber::escalate() {
         return true;
     }
     if (!d_->amg.empty() && amg_stale_) {
+        if (rho_hat <= STALE_AMG_RATIO) return false;
         build_amg();
         amg_stale_ = false;
         d_->escalations++;
@@ -663,16 +668,31 @@ void GpuAbsorber::weight_state(double* n1, double* nr, double* diag, uint8_t* re
 void GpuAbsorber::ensure_precond() {
     if (pre_fresh_) return;
     const HostStructure& st = hs_;
-    const size_t m = st.m, ms = st.m_small, M = st.ncells;
+    const size_t m = st.m, ms = st.m_small;
     const bool small = ms > 0 && ms <= DENSE_SMALL_MAX;
-    if (small) sync_host_weights();  // the dense small block is assembled on the host
+    // weights held on the device (set_weights_device): the small block is assembled there too,
+    // without copying the weight state back
+    const bool dev = host_stale_;
+    if (dev) refresh_coord();
     if (!dev_jacobi_) {  // after set_weights_device the Jacobi factors are already on the device
         std::vector<double> inv(m);
         for (size_t i = 0; i < m; i++) inv[i] = (red_[i] || !(diag_[i] > 0.0)) ? 0.0 : 1.0 / diag_[i];
         d_->inv_diag.upload(inv, stream_);
     }
     small_ok_ = false;
-    if (small) {
+    if (small && dev) {
+        build_small_device();
+    } else if (small) {
+        build_small_host();
+    }
+    pre_fresh_ = true;
+}
+
+// The dense small factor from a host assembly of S_SS (host weight state).
+void GpuAbsorber::build_small_host() {
+    const HostStructure& st = hs_;
+    const size_t ms = st.m_small, M = st.ncells;
+    {
         auto cw = [&](size_t c) { return cell_w_.empty() ? 1.0 : cell_w_[c]; };
         size_t ns = 0;
         for (auto& b : st.blocks) ns += b.small;
@@ -727,7 +747,62 @@ void GpuAbsorber::ensure_precond() {
         CK(cudaStreamSynchronize(stream_));
         small_ok_ = true;
     }
-    pre_fresh_ = true;
+}
+
+// The dense small factor from the device assembly of S_SS (weights.cuh) for the device weight
+// state: per-thread partial matrices over segment ranges, summed in thread order.
+void GpuAbsorber::build_small_device() {
+    const HostStructure& st = hs_;
+    const size_t ms = st.m_small, M = st.ncells;
+    Scratch& d = *d_;
+    int ns = 0;
+    for (auto& b : st.blocks) ns += b.small;
+    const size_t len = ms * ms;
+    const int nparts = int(std::max<size_t>(1, std::min<size_t>({size_t(GRID_V) * 4, size_t(st.g1),
+                                                                   (size_t(64) << 20) / (len * 8)})));
+    DBuf<double> part, acc, a, ak, dd, dx, dscale;
+    DBuf<u32> touched, dkeep;
+    part.alloc(size_t(nparts) * len);
+    acc.alloc(size_t(nparts) * ms);
+    touched.alloc(size_t(nparts) * ms);
+    a.alloc(len);
+    CK(cudaMemsetAsync(part.p, 0, size_t(nparts) * len * sizeof(double), stream_));
+    CK(cudaMemsetAsync(acc.p, 0, size_t(nparts) * ms * sizeof(double), stream_));
+    k_small_assemble<<<(nparts + 63) / 64, 64, 0, stream_>>>(d.seg_off.p, d.coord.p, st.g1, u32(M), ns, u32(ms),
+                                                               nparts, d.cell_w.p, d.n1inv.p, part.p, acc.p,
+                                                               touched.p);
+    k_small_sum_parts<<<grid_for(len), THREADS, 0, stream_>>>(part.p, nparts, len, a.p);
+    d.launches += 2;
+    // kept coordinates (not redundant, positive diagonal) and their unit-diagonal scaling
+    std::vector<double> diag(ms);
+    std::vector<uint8_t> red(ms);
+    CK(cudaMemcpy2DAsync(diag.data(), sizeof(double), a.p, (ms + 1) * sizeof(double), sizeof(double), ms,
+                         cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(red.data(), d.red.p, ms, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    std::vector<u32> keep;
+    for (size_t i = 0; i < ms; i++)
+        if (!red[i] && diag[i] > 0.0) keep.push_back(u32(i));
+    const size_t k = keep.size();
+    std::vector<double> scale(k);
+    for (size_t i = 0; i < k; i++) scale[i] = 1.0 / std::sqrt(diag[keep[i]]);
+    d.minv.alloc(len);
+    CK(cudaMemsetAsync(d.minv.p, 0, len * sizeof(double), stream_));
+    if (k > 0) {
+        dkeep.upload(keep, stream_);
+        dscale.upload(scale, stream_);
+        ak.alloc(k * k);
+        dd.alloc(k);
+        dx.alloc(k * k);
+        k_small_gather<<<grid_for(k * k), THREADS, 0, stream_>>>(a.p, u32(ms), dkeep.p, dscale.p, int(k), ak.p);
+        k_ldlt_ground<<<1, 1024, 0, stream_>>>(ak.p, dd.p, int(k));
+        k_ldlt_inverse<<<int((k + 127) / 128), 128, 0, stream_>>>(ak.p, dd.p, int(k), dx.p);
+        k_expand_minv<<<grid_for(k * k), THREADS, 0, stream_>>>(dx.p, dkeep.p, dscale.p, int(k), u32(ms), d.minv.p);
+        d.launches += 4;
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    small_ok_ = true;
 }
 
 namespace {
@@ -1172,7 +1247,7 @@ template <class T>
 static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x, const T* b,
                    const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small, int R, double tol,
                    double drop, u64 iters_done, size_t maxiter, bool x_is_start, const Ctx& ctx, cudaStream_t st,
-                   const std::function<bool()>& escalate) {
+                   const std::function<bool(double)>& escalate) {
     const size_t m = S.m, tot = m * size_t(R);
     CgState cg = d.cg();
     u64 it = 0;
@@ -1238,7 +1313,7 @@ restart:
             for (int j = 0; j < R; j++)
                 if (act[j] == 1 && rho_from[j] > 0.0)
                     rho_hat = std::max(rho_hat, std::pow(rho_at[j] / rho_from[j], 1.0 / double(PROBE_AT - PROBE_FROM)));
-            if (rho_hat > PROBE_RATIO && escalate()) {
+            if (rho_hat > PROBE_RATIO && escalate(rho_hat)) {
                 CK(cudaMemsetAsync(d.cg_ring.p, 0, size_t(R) * WINDOW * sizeof(double), st));
                 x_is_start = true;
                 goto restart;
@@ -1337,7 +1412,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         CK(cudaMemcpyAsync(d.cg_xconst.p, zero.data(), r * 8, cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(d.cg_ring.p, 0, r * WINDOW * 8, st));
         const bool exact_pre = small_ok_ && hs_.m_small == hs_.m;
-        const std::function<bool()> esc = [this] { return escalate(); };
+        const std::function<bool(double)> esc = [this](double rho_hat) { return escalate(rho_hat); };
         if (exact_pre) {
             // x* = x + M^-1 (rhs - S x) (cg.rs:171-198)
             if (warm || have_last) {

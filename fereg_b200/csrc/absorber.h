@@ -139,10 +139,12 @@ class GpuAbsorber {
 
     // Escalation (cg.rs:24-37 probe, solve.rs:838 escalate_block): multigrid hierarchies of the
     // large blocks; true when a stronger preconditioner now exists.
-    bool escalate();
+    bool escalate(double rho_hat);
     void build_amg();
     void refresh_small();
     void refresh_coord() const;
+    void build_small_host();
+    void build_small_device();
 
     void refresh_weights(const double* w_kept);
     void sync_host_weights() const;
