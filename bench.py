@@ -49,7 +49,7 @@ CONFIGS = {
     "c4": dict(countries=200, years=50, sectors=5, seed=10**7 * 100 + 45, zero_share=0.40),
     # Serving stream: 2,000 requests, exponential inter-arrivals at 70% of the measured capacity,
     # n log-uniform in 1e4..5e6, 1-4 FEs, 60% OLS / 20% IV / 20% logit, 1-12 regressors.
-    "c5": dict(requests=2000, seed=10**6 * 100 + 46, load=0.7, tol=1e-10, cpu_sample=12),
+    "c5": dict(requests=2000, seed=10**6 * 100 + 46, load=0.7, tol=1e-10, glm_tol=1e-8, cpu_sample=12, burst=128),
 }
 TOL = 1e-8
 METRIC = "sec/call (1e7-obs 3-FE OLS)"
@@ -340,11 +340,17 @@ def serve_request(i, seed, pool):
     return dict(model=model, codes=codes, g=g, cols=cols, nx=nx, clusters=clusters, cl_g=cl_g, vce=vce, n=n, kw=kw)
 
 
-def submit_request(srv, r, tol):
+def request_tol(r, cfg):
+    """Solver tolerance of a request: OLS / IV solves at cfg["tol"]; logit at the reference's
+    default deviance tolerance (GlmOptions: tol 1e-8, final inner tolerance 1e-10)."""
+    return cfg["glm_tol"] if r["model"] == "logit" else cfg["tol"]
+
+
+def submit_request(srv, r, cfg):
     import fereg_b200 as fb
 
     return srv.submit(r["model"], r["codes"], r["g"], r["cols"], r["nx"], clusters=r["clusters"], cl_g=r["cl_g"],
-                      vce=r["vce"], tol=tol, precision=fb.PREC_F64, **r["kw"])
+                      vce=r["vce"], tol=request_tol(r, cfg), precision=fb.PREC_F64, **r["kw"])
 
 
 def run_serve(args, cfg, rank, world, local, pg):
@@ -371,17 +377,17 @@ def run_serve(args, cfg, rank, world, local, pg):
         for t in tickets:
             out.append(srv.wait(t))
 
-    # capacity: a burst of 64 requests (seeds after the stream's) submitted at once
-    burst = [serve_request(nreq + 1000 + i, cfg["seed"], pool) for i in range(64)]
+    # capacity: a burst of requests (seeds after the stream's) submitted at once; requests per
+    # second at full load
+    burst = [serve_request(nreq + 1000 + i, cfg["seed"], pool) for i in range(cfg["burst"])]
     t0 = time.perf_counter()
-    tk = [submit_request(srv, r, tol) for r in burst]
+    tk = [submit_request(srv, r, cfg) for r in burst]
     res_b = [srv.wait(t) for t in tk]
     burst_s = time.perf_counter() - t0
     assert all(r["rc"] == 0 for r in res_b), [r["msg"] for r in res_b if r["rc"]]
-    rows_b = sum(r["n"] for r in burst)
-    cap_rows = rows_b / burst_s  # rows per second at full load
-    mean_rows = (SERVE_NMAX - 1e4) / np.log(SERVE_NMAX / 1e4)  # mean of the log-uniform n
-    rate = cfg["load"] * cap_rows / mean_rows  # requests per second
+    cap_rows = sum(r["n"] for r in burst) / burst_s
+    cap_req = len(burst) / burst_s
+    rate = cfg["load"] * cap_req  # requests per second
     arrivals = np.cumsum(np.random.default_rng(cfg["seed"] - 1).exponential(1.0 / rate, nreq))
     barrier(pg)
     results, tickets = [], []
@@ -426,7 +432,7 @@ def run_serve(args, cfg, rank, world, local, pg):
                 time.sleep(arrivals[i] - now)
             else:
                 late.append(now - arrivals[i])
-            t = submit_request(srv, r, tol)
+            t = submit_request(srv, r, cfg)
             with cv:
                 waiter_q.append(t)
                 cv.notify()
@@ -444,14 +450,15 @@ def run_serve(args, cfg, rank, world, local, pg):
     p99 = max_over_ranks(p99, pg, torch.device("cuda", local))
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = serve_cpu_sample(sample, [res[i] for i, _ in sample], tol)
+        cpu = serve_cpu_sample(sample, [res[i] for i, _ in sample], cfg)
     if rank == 0:
         line = {"metric": SERVE_METRIC, "value": p99, "unit": "s", "n_gpus": world, "steps": 1,
                 "warmup": 1, "ms_per_step": span * 1e3, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": "c5", "requests": nreq, "mix": mix, "rows_total": rows_total,
                            "offered_rate_req_s": rate, "load": cfg["load"], "workers": args.serve_workers,
-                           "tol": tol, "burst_rows_per_s": cap_rows, "late_submits": len(late),
+                           "tol": tol, "glm_tol": cfg["glm_tol"], "burst_requests": len(burst),
+                           "burst_req_per_s": cap_req, "burst_rows_per_s": cap_rows, "late_submits": len(late),
                            "max_submit_lag_s": float(max(late)) if late else 0.0,
                            "parallelism": f"replicas x{world}", "errors": len(bad),
                            "l2": "inputs of most requests exceed L2; no flush"},
@@ -472,7 +479,7 @@ def run_serve(args, cfg, rank, world, local, pg):
     srv.close()
 
 
-def oracle_request(r, tol):
+def oracle_request(r, cfg):
     """The CPU oracle on one request: the session OLS, the 2SLS restatement on the oracle's
     residualized block, or the absorbed logit IRLS. Returns b, V in the server's order."""
     from oracle import glm as oglm
@@ -480,6 +487,7 @@ def oracle_request(r, tol):
     from oracle import oracle
 
     cols = np.column_stack(r["cols"])
+    tol = request_tol(r, cfg)
     if r["model"] == "ols":
         sess = oracle.Session(r["codes"], r["g"], r["clusters"], r["cl_g"])
         z = np.ascontiguousarray(cols[sess.row_order()])
@@ -496,7 +504,7 @@ def oracle_request(r, tol):
     return b, V
 
 
-def serve_cpu_sample(sample, served, tol):
+def serve_cpu_sample(sample, served, cfg):
     """cpu_baseline of C5: the CPU oracle (all host threads) on a bounded sample of the stream's
     requests, one after another; value = the p99 (the maximum, for the sample's size) of their
     service times. The served results of the same requests are compared with the oracle's."""
@@ -506,7 +514,7 @@ def serve_cpu_sample(sample, served, tol):
     rows = 0
     for (i, r), s in zip(sample, served):
         t0 = time.perf_counter()
-        b, V = oracle_request(r, tol)
+        b, V = oracle_request(r, cfg)
         times.append(time.perf_counter() - t0)
         rows += r["n"]
         kb = len(b)
@@ -541,7 +549,7 @@ def run_serve_reference(args, cfg, world):
     times = []
     for r in sample:
         t0 = time.perf_counter()
-        oracle_request(r, cfg["tol"])
+        oracle_request(r, cfg)
         times.append(time.perf_counter() - t0)
     v = float(np.percentile(times, 99))
     line = {"impl": "reference", "metric": SERVE_METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": 1,

@@ -64,7 +64,7 @@ class BootOut(C.Structure):
 
 class GlmSpec(C.Structure):
     _fields_ = [("vce", C.c_int), ("tol", C.c_double), ("maxiter", C.c_size_t), ("inner_maxiter", C.c_size_t),
-                ("precision", C.c_int), ("family", C.c_int)]
+                ("precision", C.c_int), ("family", C.c_int), ("itol", C.c_double)]
 
 
 class IvSpec(C.Structure):
@@ -492,18 +492,18 @@ class Session:
         return dict(b=b[:k], V=V[:k, :k], status=status[: nx + nendog + ninst], scalars=sc)
 
     def poisson(self, rows, vce="robust", tol=1e-8, maxiter=10000, inner_maxiter=16000, precision=PREC_F64,
-                on_device=False, nx=None):
+                on_device=False, nx=None, itol=1e-10):
         """Poisson PML of column 0 (y >= 0) on the other columns of the n x (1 + nx) block (row
         order; host array, or a device pointer with on_device=True)."""
-        return self.glm(rows, "poisson", vce, tol, maxiter, inner_maxiter, precision, on_device, nx)
+        return self.glm(rows, "poisson", vce, tol, maxiter, inner_maxiter, precision, on_device, nx, itol)
 
     def logit(self, rows, vce="oim", tol=1e-8, maxiter=10000, inner_maxiter=16000, precision=PREC_F64,
-              on_device=False, nx=None):
+              on_device=False, nx=None, itol=1e-10):
         """Logit of column 0 (y in {0, 1}) on the other columns, as `poisson`."""
-        return self.glm(rows, "logit", vce, tol, maxiter, inner_maxiter, precision, on_device, nx)
+        return self.glm(rows, "logit", vce, tol, maxiter, inner_maxiter, precision, on_device, nx, itol)
 
     def glm(self, rows, family, vce="robust", tol=1e-8, maxiter=10000, inner_maxiter=16000, precision=PREC_F64,
-            on_device=False, nx=None):
+            on_device=False, nx=None, itol=1e-10):
         if on_device:
             ptr = rows
             assert nx is not None
@@ -515,7 +515,7 @@ class Session:
         V = np.zeros((max(1, nx), max(1, nx)))
         status = np.zeros(max(1, nx), dtype=np.uint8)
         fam = {"poisson": FAMILY_POISSON, "logit": FAMILY_LOGIT}[family]
-        spec = GlmSpec({"oim": 0, "robust": 1, "cluster": 2}[vce], tol, maxiter, inner_maxiter, precision, fam)
+        spec = GlmSpec({"oim": 0, "robust": 1, "cluster": 2}[vce], tol, maxiter, inner_maxiter, precision, fam, itol)
         out = GlmOut(_p(b, f64p), _p(V, f64p), _p(status, u8p))
         _check(lib().fereg_session_glm(self.h, P(ptr), int(on_device), nx, C.byref(spec), C.byref(out)))
         return dict(b=b[:nx], V=V[:nx, :nx], status=status[:nx], N=out.N, deviance=out.deviance, ll=out.ll,

@@ -436,6 +436,7 @@ static int session_glm(fereg_session* s, double* rows, int rows_on_device, size_
         gs.family = family == FEREG_FAMILY_LOGIT ? 1 : 0;
         gs.vce = spec->vce;
         gs.tol = spec->tol;
+        gs.itol = spec->itol > 0.0 ? spec->itol : 1e-10;
         gs.maxiter = spec->maxiter;
         gs.inner_maxiter = spec->inner_maxiter;
         gs.prec = spec->precision == FEREG_PREC_F32_REFINED ? Precision::F32_REFINED : Precision::F64;

@@ -1108,7 +1108,7 @@ void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec
 // GLM by IRLS, Poisson PML or logit (glm/irls.rs:367-560 with ppmlhdfe conventions,
 // glm/mod.rs:1053-1140 for the variance). Each iteration: the family's w and z (device), the weight state
 // refreshed on the device, [z, X] residualized warm-started from the previous FE coefficients at
-// an inner tolerance tightened toward max(1e-12, 0.1 tol), the weighted regression on the
+// an inner tolerance tightened toward max(1e-12, min(itol, 0.1 tol)), the weighted regression on the
 // residualized block (device Gram, host sweep), eta = z - e and mu = exp(eta) with the deviance
 // (device). Stops when the relative deviance change |D - D'| / max(min(D, D'), 0.1) < tol with the
 // inner tolerance at its floor. Collinearity is settled in the first iteration (ppmlhdfe
@@ -1169,7 +1169,7 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
     std::iota(all.begin(), all.end(), 0);
     std::vector<double> sumsq;
     outer_products(raw.p, n, R, all, nullptr, false, nullptr, nullptr, true, &sumsq);
-    const double highest = std::max(1e-12, 0.1 * gs.tol);
+    const double highest = std::max(1e-12, std::min(gs.itol, 0.1 * gs.tol));  // glm/mod.rs:826
     double tol_in = std::max(1e-4, gs.tol);
     double dev_old = nanv(), dev = nanv();
     bool have_warm = false, converged = false;

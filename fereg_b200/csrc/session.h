@@ -112,7 +112,8 @@ class GpuSession {
     struct GlmSpec {
         int family = 0;  // 0 Poisson, 1 logit
         int vce = 1;     // 0 oim (inverse Hessian), 1 robust, 2 cluster
-        double tol = 1e-8;
+        double tol = 1e-8;    // deviance tolerance
+        double itol = 1e-10;  // final inner (FE solve) tolerance
         size_t maxiter = 10000;
         size_t inner_maxiter = 16000;
         Precision prec = Precision::F64;

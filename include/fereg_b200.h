@@ -259,6 +259,7 @@ typedef struct fereg_glm_spec {
     size_t inner_maxiter;
     int precision; /* FEREG_PREC_* of the FE solves */
     int family;    /* FEREG_FAMILY_*; fereg_session_poisson ignores it */
+    double itol;   /* final inner tolerance (GlmOptions::itol; 0 = the default 1e-10) */
 } fereg_glm_spec;
 
 typedef struct fereg_glm_out {

@@ -72,12 +72,13 @@ def dense_glm(family, terms, y, X, vce="robust", cl=None, maxiter=200):
     return b, V, dev, ll
 
 
-def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=None, maxiter=1000):
+def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=1e-10, maxiter=1000):
     """IRLS with the fixed effects absorbed by the oracle's FE solver (the reference's loop,
     glm/irls.rs:367-560): each iteration sets the family's weights on the absorber, residualizes
     [z, X] warm-started from the previous FE coefficients, fits the weighted regression on the
     residualized block, and updates eta = z - e; the inner tolerance starts at max(1e-4, tol)
-    and is tightened 10x when the deviance change falls below it, down to max(1e-12, 0.1 tol);
+    and is tightened 10x when the deviance change falls below it, down to
+    max(1e-12, min(itol, 0.1 tol)) (glm/mod.rs:826);
     convergence when the relative deviance change is below tol at the tightest inner tolerance.
     Unweighted samples, no separation checks. Returns b, V, deviance, log-likelihood, iterations."""
     from oracle import oracle
@@ -93,7 +94,7 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
     else:
         mu = (y + 0.5) / 2
         eta = np.log(mu / (1 - mu))
-    highest = max(1e-12, 0.1 * tol) if itol is None else itol
+    highest = max(1e-12, min(itol, 0.1 * tol))
     tol_in = max(1e-4, tol)
     dev_old = np.nan
     warm = None
