@@ -168,6 +168,11 @@ def _setup(L):
     L.fereg_session_poisson.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(GlmSpec), C.POINTER(GlmOut)]
     L.fereg_session_iv.argtypes = [P, P, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(IvSpec),
                                    C.POINTER(IvOut)]
+    L.fereg_factorize.argtypes = [f64p, C.c_size_t, u32p, u32p]
+    L.fereg_combine.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, u32p, u32p]
+    L.fereg_drop_singletons.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, f64p, f64p, C.c_int, C.c_int,
+                                        u8p, u64p, u64p]
+    L.fereg_restrict.argtypes = [u32p, C.c_uint32, u8p, C.c_size_t, u32p, u32p, u64p]
     L.fereg_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(P)]
     L.fereg_server_submit.argtypes = [P, C.POINTER(Request), C.POINTER(C.c_uint64)]
     L.fereg_server_wait.argtypes = [P, C.c_uint64, C.POINTER(RequestResult), C.c_char_p, C.c_size_t]
@@ -586,3 +591,71 @@ class Server:
         _check(lib().fereg_server_stats(self.h, _p(v, u64p)))
         keys = ["submitted", "completed", "rejected", "peak_bytes", "peak_running", "budget", "running", "launches"]
         return {k: int(x) for k, x in zip(keys, v)}
+
+
+# ---------------------------------------------------------------------------------------------
+# Sample preparation on the device (the reference's Session::prepare steps, factor.rs / sample.rs)
+
+FAMILY_CODE = {None: 0, "gaussian": 0, "poisson": 1, "logit": 2}
+
+
+def factorize(x):
+    """factor.rs:38 factorize on the device: (codes in ascending value order, level count)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    codes = np.empty(len(x), dtype=np.uint32)
+    g = C.c_uint32()
+    _check(lib().fereg_factorize(_p(x, f64p), len(x), _p(codes, u32p), C.byref(g)))
+    return codes, int(g.value)
+
+
+def combine(parts, nl):
+    """factor.rs:255 combine on the device: codes of the interaction of code columns."""
+    arrs = [np.ascontiguousarray(c, dtype=np.uint32) for c in parts]
+    ptrs = (u32p * len(arrs))(*[_p(a, u32p) for a in arrs])
+    nla = np.asarray(nl, dtype=np.uint32)
+    out = np.empty(len(arrs[0]), dtype=np.uint32)
+    g = C.c_uint32()
+    _check(lib().fereg_combine(ptrs, _p(nla, u32p), len(arrs), len(out), _p(out, u32p), C.byref(g)))
+    return out, int(g.value)
+
+
+def drop_singletons(codes, g, fw=None, y=None, family=None, singletons=True, alive=None):
+    """sample.rs:44-72 on the device: (alive, singletons dropped, fe-separated dropped)."""
+    n = len(codes[0])
+    arrs = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
+    ptrs = (u32p * len(arrs))(*[_p(a, u32p) for a in arrs])
+    garr = np.asarray(g, dtype=np.uint32)
+    al = np.ones(n, dtype=np.uint8) if alive is None else np.ascontiguousarray(alive, dtype=np.uint8).copy()
+    fwa = None if fw is None else np.ascontiguousarray(fw, dtype=np.float64)
+    ya = None if y is None else np.ascontiguousarray(y, dtype=np.float64)
+    s, f = C.c_uint64(), C.c_uint64()
+    _check(lib().fereg_drop_singletons(ptrs, _p(garr, u32p), len(arrs), n, _p(fwa, f64p), _p(ya, f64p),
+                                       FAMILY_CODE[family], int(singletons), _p(al, u8p), C.byref(s), C.byref(f)))
+    return al.astype(bool), int(s.value), int(f.value)
+
+
+def restrict(codes, g, alive):
+    """factor.rs:281 restrict on the device: the kept rows' codes renumbered densely."""
+    codes = np.ascontiguousarray(codes, dtype=np.uint32)
+    al = np.ascontiguousarray(alive, dtype=np.uint8)
+    out = np.empty(max(1, int(al.sum())), dtype=np.uint32)
+    nl, kept = C.c_uint32(), C.c_uint64()
+    _check(lib().fereg_restrict(_p(codes, u32p), g, _p(al, u8p), len(codes), _p(out, u32p), C.byref(nl),
+                                C.byref(kept)))
+    return out[: int(kept.value)], int(nl.value)
+
+
+def prepare(factors, absorb, fw=None, y=None, family=None, singletons=True):
+    """The sample preparation of Session::prepare for the absorbed terms, on the device:
+    factorize every factor column, combine the factors of each term (interactions), drop
+    singletons (and, with a GLM family and its outcome, fe-separated rows) cyclically, and
+    renumber each term's codes over the kept rows. Returns alive, the drop counts and the kept
+    terms as (codes, levels)."""
+    fac = [factorize(f) for f in factors]
+    terms = [combine([fac[i][0] for i in t], [fac[i][1] for i in t]) for t in absorb]
+    if terms:
+        alive, s, f = drop_singletons([c for c, _ in terms], [g for _, g in terms], fw, y, family, singletons)
+    else:
+        alive, s, f = np.ones(len(factors[0]), dtype=bool), 0, 0
+    kept = [restrict(c, g, alive) for c, g in terms]
+    return dict(alive=alive, num_singletons=s, fe_separated=f, terms=kept)

@@ -6,6 +6,7 @@
 
 #include "../../include/fereg_b200.h"
 #include "absorber.h"
+#include "prep.h"
 #include "server.h"
 #include "session.h"
 
@@ -562,3 +563,48 @@ int fereg_server_stats(const fereg_server* srv, uint64_t* out8) {
 }
 
 void fereg_server_destroy(fereg_server* srv) { delete srv; }
+
+int fereg_factorize(const double* x, size_t n, uint32_t* codes, uint32_t* nlevels) {
+    return guard([&] {
+        if ((n && (!x || !codes)) || !nlevels) throw Error(RC_INVALID_INPUT, "fereg_factorize: NULL argument");
+        if (n > size_t(0xffffffffu)) throw Error(RC_INVALID_INPUT, "fereg_factorize: more than 2^32 - 1 rows");
+        *nlevels = prep_factorize(x, n, codes);
+    });
+}
+
+int fereg_combine(const uint32_t* const* parts, const uint32_t* nl, int np, size_t n, uint32_t* codes,
+                  uint32_t* nlevels) {
+    return guard([&] {
+        if (!parts || !nl || np < 1 || (n && !codes) || !nlevels)
+            throw Error(RC_INVALID_INPUT, "fereg_combine: NULL argument or no part");
+        std::vector<const u32*> p(parts, parts + np);
+        std::vector<u32> g(nl, nl + np);
+        *nlevels = prep_combine(p, g, n, codes);
+    });
+}
+
+int fereg_drop_singletons(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, const double* fw,
+                          const double* y, int family, int singletons, uint8_t* alive, uint64_t* dropped_singletons,
+                          uint64_t* dropped_separated) {
+    return guard([&] {
+        if (nterms < 0 || (nterms && (!codes || !g)) || (n && !alive))
+            throw Error(RC_INVALID_INPUT, "fereg_drop_singletons: NULL argument");
+        if (family < 0 || family > 2 || (family && !y))
+            throw Error(RC_INVALID_INPUT, "fereg_drop_singletons: family 1 / 2 needs the outcome");
+        std::vector<const u32*> c(codes, codes + nterms);
+        std::vector<u32> gg(g, g + nterms);
+        const DropCounts d = prep_drop(c, gg, n, fw, y, family, singletons != 0, alive);
+        if (dropped_singletons) *dropped_singletons = d.singletons;
+        if (dropped_separated) *dropped_separated = d.separated;
+    });
+}
+
+int fereg_restrict(const uint32_t* codes, uint32_t g, const uint8_t* alive, size_t n, uint32_t* out,
+                   uint32_t* nlevels, uint64_t* kept) {
+    return guard([&] {
+        if ((n && (!codes || !alive || !out)) || !nlevels) throw Error(RC_INVALID_INPUT, "fereg_restrict: NULL argument");
+        size_t k = 0;
+        *nlevels = prep_restrict(codes, g, alive, n, out, &k);
+        if (kept) *kept = k;
+    });
+}

@@ -277,6 +277,26 @@ int fereg_session_glm(fereg_session* s, double* rows, int rows_on_device, size_t
 int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
                           fereg_glm_out* out);
 
+/* Sample preparation on the device (Session::prepare's FE-id compression and sample drops;
+ * host arrays in and out). Bit-exact with the reference's definitions.
+ * fereg_factorize: factor.rs:38, dense codes in ascending value order (-0 = +0; NaN: 198).
+ * fereg_combine: factor.rs:255, codes of the interaction of np code columns in lexicographic order.
+ * fereg_drop_singletons: sample.rs:44-72, cyclic passes over the terms in absorb order until
+ *   nterms consecutive passes drop nothing; a level with (fweight) count 1 drops its rows
+ *   (when `singletons`), and with family 1 (Poisson) / 2 (logit) and its outcome y, a level
+ *   whose alive rows have no nonzero outcome (logit: or only nonzero outcomes) is `fe`-separated.
+ *   alive (n bytes, 0/1) is updated in place; counts of both kinds are returned.
+ * fereg_restrict: factor.rs:281, the kept rows' codes renumbered densely in order (out holds
+ *   the kept rows only). */
+int fereg_factorize(const double* x, size_t n, uint32_t* codes, uint32_t* nlevels);
+int fereg_combine(const uint32_t* const* parts, const uint32_t* nl, int np, size_t n, uint32_t* codes,
+                  uint32_t* nlevels);
+int fereg_drop_singletons(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, const double* fw,
+                          const double* y, int family, int singletons, uint8_t* alive, uint64_t* dropped_singletons,
+                          uint64_t* dropped_separated);
+int fereg_restrict(const uint32_t* codes, uint32_t g, const uint8_t* alive, size_t n, uint32_t* out,
+                   uint32_t* nlevels, uint64_t* kept);
+
 /* Serving: a request loop over independent regressions on one GPU. Requests are admitted in
  * arrival order while their estimated device memory fits the budget (hbm_budget bytes; 0 = 80%
  * of the free memory at creation); `workers` requests run at once, each on its own session and

@@ -115,6 +115,7 @@ def _setup(L):
     L.orc_factorize_f64.argtypes = [f64p, C.c_size_t, u32p, u32p]
     L.orc_drop_singletons.restype = C.c_uint64
     L.orc_drop_singletons.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, f64p, u8p]
+    L.orc_combine.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, u32p, u32p]
     L.orc_mobility_groups.restype = C.c_uint64
     L.orc_mobility_groups.argtypes = [u32p, C.c_uint32, u32p, C.c_uint32, C.c_size_t, u32p]
     L.orc_splitmix_fill_u64.argtypes = [C.c_uint64, C.c_uint64, C.c_int, u64p, C.c_size_t]
@@ -142,6 +143,20 @@ def factorize(x):
     if rc:
         raise RuntimeError(lib().orc_last_error().decode())
     return codes, int(g.value)
+
+
+def combine(parts, nl):
+    """factor.rs:255 combine on the oracle: codes of the interaction of code columns."""
+    n = len(parts[0])
+    arrs = [np.ascontiguousarray(c, dtype=np.uint32) for c in parts]
+    ptrs = (u32p * len(arrs))(*[_p(a, u32p) for a in arrs])
+    nla = np.asarray(nl, dtype=np.uint32)
+    out = np.empty(n, dtype=np.uint32)
+    g = C.c_uint32()
+    rc = lib().orc_combine(ptrs, _p(nla, u32p), len(arrs), n, _p(out, u32p), C.byref(g))
+    if rc:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return out, int(g.value)
 
 
 def drop_singletons(codes, g, fw=None):
