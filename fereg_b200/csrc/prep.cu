@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "prep.cuh"
@@ -111,6 +112,12 @@ u32 codes_of_keys(u64* keys, u32* idx, size_t n, u32* codes, cudaStream_t st) {
     return codes_by_sort(keys, idx, n, lo, hi, codes, st);
 }
 
+// Every code of a column must be below its level count (the kernels index by it).
+void check_codes(const u32* c, size_t n, u32 g, const char* what) {
+    for (size_t i = 0; i < n; i++)
+        if (c[i] >= g) throw Error(RC_INVALID_INPUT, std::string(what) + ": a code is not below its level count");
+}
+
 }  // namespace
 
 u32 prep_factorize(const double* x, size_t n, u32* codes_out) {
@@ -173,6 +180,7 @@ u32 prep_combine(const std::vector<const u32*>& parts, const std::vector<u32>& n
     AllocScope alloc_scope(st);
     std::vector<DBuf<u32>> dp(parts.size());
     std::vector<const u32*> ptrs;
+    for (size_t p = 0; p < parts.size(); p++) check_codes(parts[p], n, nl[p], "fereg_combine");
     for (size_t p = 0; p < parts.size(); p++) {
         dp[p].upload(parts[p], n, st);
         ptrs.push_back(dp[p].p);
@@ -202,6 +210,7 @@ DropCounts prep_drop(const std::vector<const u32*>& codes, const std::vector<u32
     cudaStream_t st = S.st;
     AllocScope alloc_scope(st);
     std::vector<DBuf<u32>> dc(nterms);
+    for (size_t t = 0; t < nterms; t++) check_codes(codes[t], n, g[t], "fereg_drop_singletons");
     for (size_t t = 0; t < nterms; t++) dc[t].upload(codes[t], n, st);
     DBuf<uint8_t> dalive;
     DBuf<double> dfw, dy, cnt, pos;
@@ -244,6 +253,7 @@ u32 prep_restrict(const u32* codes, u32 g, const uint8_t* alive, size_t n, u32* 
     AllocScope alloc_scope(st);
     DBuf<u32> dc, present, level_rank, a32, kept_rank, dout;
     DBuf<uint8_t> dalive;
+    check_codes(codes, n, g, "fereg_restrict");
     dc.upload(codes, n, st);
     dalive.upload(alive, n, st);
     present.alloc(std::max<u32>(1, g));
