@@ -20,7 +20,7 @@
 namespace fereg {
 
 constexpr int ST_TB = 256;          // threads per CTA of the stats passes
-constexpr int ST_GRID = 148 * 2;    // CTAs of the row passes
+constexpr int ST_GRID = 148 * 4;    // CTAs of the row passes (4 per SM: 32 warps)
 constexpr int OP_ROWS = 32;         // rows staged per tile of the outer-product pass
 constexpr int OP_PPT = 8;           // pairs per thread of one outer-product launch
 constexpr int OP_MAXP = ST_TB * OP_PPT;  // pairs of one launch
@@ -263,7 +263,7 @@ __device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double
 }
 
 template <int NB>
-__global__ void __launch_bounds__(ST_TB) k_outer_mma(OpSpec s, double* __restrict__ part) {
+__global__ void __launch_bounds__(ST_TB, NB <= 2 ? 4 : 2) k_outer_mma(OpSpec s, double* __restrict__ part) {
     constexpr int NT = NB * (NB + 1) / 2, U = 4, W = 8 * NB;
     __shared__ double red[W * W + W];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(ST_TB) k_outer_mma(OpSpec s, double* __restric
 // and the sums of squares about them follow exactly up to rounding (m2 = S2 - S1^2 / n).
 // Lane = (group, column) over a column chunk [j0, j0 + Rc) padded to RCP; rows U groups at a time.
 template <int RCP>
-__global__ void __launch_bounds__(ST_TB) k_colstats1(const double* __restrict__ rows, size_t n, int R, int j0, int Rc,
+__global__ void __launch_bounds__(ST_TB, 4) k_colstats1(const double* __restrict__ rows, size_t n, int R, int j0, int Rc,
                                                      const double* __restrict__ w, double* __restrict__ part) {
     constexpr int G = 32 / RCP, U = 4, NV = 6;
     __shared__ double red[ST_TB / 32][32][NV];
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(ST_TB) k_colstats1(const double* __restrict__ 
 // ---------------------------------------------------------------------------------------------
 // Residuals: e_i = y_i - sum_p beta[p] x_i[col[p]] (y = column 0, or 0 when y_zero); per-CTA
 // partials of sum om_i e_i^2.
-__global__ void __launch_bounds__(ST_TB) k_resid_e(const double* __restrict__ rows, size_t n, int R,
+__global__ void __launch_bounds__(ST_TB, 4) k_resid_e(const double* __restrict__ rows, size_t n, int R,
                                                    const int* __restrict__ col, const double* __restrict__ beta, int k,
                                                    int y_zero, const double* __restrict__ om, double* __restrict__ e,
                                                    double* __restrict__ part) {
