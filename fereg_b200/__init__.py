@@ -168,6 +168,7 @@ def _setup(L):
     L.fereg_session_poisson.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(GlmSpec), C.POINTER(GlmOut)]
     L.fereg_session_iv.argtypes = [P, P, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(IvSpec),
                                    C.POINTER(IvOut)]
+    L.fereg_amg_probe.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, C.c_int, u32p, u32p, u64p, f64p]
     L.fereg_factorize.argtypes = [f64p, C.c_size_t, u32p, u32p]
     L.fereg_combine.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, u32p, u32p]
     L.fereg_drop_singletons.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, f64p, f64p, C.c_int, C.c_int,
@@ -659,3 +660,19 @@ def prepare(factors, absorb, fw=None, y=None, family=None, singletons=True):
         alive, s, f = np.ones(len(factors[0]), dtype=bool), 0, 0
     kept = [restrict(c, g, alive) for c, g in terms]
     return dict(alive=alive, num_singletons=s, fe_separated=f, terms=kept)
+
+
+def amg_probe(codes, g, max_levels=16):
+    """Host-only test hook: the level sizes, nonzeros and relative row sums of the multigrid
+    hierarchy an escalation would build for the structure's first block above 768 levels."""
+    arrs = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
+    ptrs = (u32p * len(arrs))(*[_p(a, u32p) for a in arrs])
+    garr = np.asarray(g, dtype=np.uint32)
+    sizes = np.zeros(max_levels, dtype=np.uint32)
+    nnz = np.zeros(max_levels, dtype=np.uint64)
+    rs = np.zeros(max_levels)
+    nl = C.c_uint32()
+    _check(lib().fereg_amg_probe(ptrs, _p(garr, u32p), len(arrs), len(arrs[0]), max_levels, C.byref(nl),
+                                 _p(sizes, u32p), _p(nnz, u64p), _p(rs, f64p)))
+    k = min(int(nl.value), max_levels)
+    return dict(levels=int(nl.value), sizes=sizes[:k].astype(int), nnz=nnz[:k].astype(int), row_sum=rs[:k])

@@ -6,6 +6,7 @@
 
 #include "../../include/fereg_b200.h"
 #include "absorber.h"
+#include "amg.h"
 #include "prep.h"
 #include "server.h"
 #include "session.h"
@@ -606,5 +607,59 @@ int fereg_restrict(const uint32_t* codes, uint32_t g, const uint8_t* alive, size
         size_t k = 0;
         *nlevels = prep_restrict(codes, g, alive, n, out, &k);
         if (kept) *kept = k;
+    });
+}
+
+int fereg_amg_probe(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, int max_levels,
+                    uint32_t* levels, uint32_t* sizes, uint64_t* nnz, double* row_sum) {
+    return guard([&] {
+        if (!codes || !g || nterms < 1 || !levels) throw Error(RC_INVALID_INPUT, "fereg_amg_probe: NULL argument");
+        std::vector<const u32*> c(codes, codes + nterms);
+        std::vector<u32> gg(g, g + nterms);
+        const HostStructure hs = build_structure(c, gg, n, SMALL_LIMIT);
+        // unweighted weight state (operator.rs:211-338): n1, nr, diag, redundant
+        const size_t M = hs.ncells, m = hs.m, nb = hs.nb();
+        std::vector<double> cw(M), n1(hs.g1, 0.0), nr(m, 0.0), dq(m, 0.0), cs(m, 0.0), diag(m);
+        std::vector<uint8_t> red(m);
+        for (size_t k = 0; k < M; k++) cw[k] = hs.trivial() ? 1.0 : double(hs.cell_row[k + 1] - hs.cell_row[k]);
+        for (u32 s = 0; s < hs.g1; s++) {
+            for (u32 k = hs.seg_off[s]; k < hs.seg_off[s + 1]; k++) n1[s] += cw[k];
+            for (u32 k = hs.seg_off[s]; k < hs.seg_off[s + 1]; k++)
+                for (size_t b = 0; b < nb; b++) cs[hs.coord[b * M + k]] += cw[k];
+            for (u32 k = hs.seg_off[s]; k < hs.seg_off[s + 1]; k++)
+                for (size_t b = 0; b < nb; b++) {
+                    const u32 q = hs.coord[b * M + k];
+                    nr[q] += cw[k];
+                    dq[q] += cw[k] * cs[q] / n1[s];
+                }
+            for (u32 k = hs.seg_off[s]; k < hs.seg_off[s + 1]; k++)
+                for (size_t b = 0; b < nb; b++) cs[hs.coord[b * M + k]] = 0.0;
+        }
+        for (size_t q = 0; q < m; q++) {
+            diag[q] = nr[q] - dq[q];
+            red[q] = diag[q] <= 1e-12 * nr[q];
+        }
+        *levels = 0;
+        for (size_t b = 0; b < nb; b++) {
+            if (hs.blocks[b].g <= 2 * AMG_COARSE) continue;
+            const AmgHierarchy H = amg_build(hs, b, cw.data(), n1.data(), diag.data(), red.data());
+            *levels = u32(H.levels.size());
+            for (size_t l = 0; l < H.levels.size() && int(l) < max_levels; l++) {
+                const Csr& A = H.levels[l].A;
+                if (sizes) sizes[l] = H.levels[l].n;
+                if (nnz) nnz[l] = A.col.size();
+                double worst = 0.0, dmax = 0.0;
+                for (u32 i = 0; i < A.nr; i++) {
+                    double rs = 0.0;
+                    for (u32 e = A.ptr[i]; e < A.ptr[i + 1]; e++) {
+                        rs += A.val[e];
+                        if (A.col[e] == i) dmax = std::max(dmax, A.val[e]);
+                    }
+                    worst = std::max(worst, std::fabs(rs));
+                }
+                if (row_sum) row_sum[l] = dmax > 0.0 ? worst / dmax : 0.0;
+            }
+            break;
+        }
     });
 }

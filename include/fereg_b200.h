@@ -277,6 +277,14 @@ int fereg_session_glm(fereg_session* s, double* rows, int rows_on_device, size_t
 int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
                           fereg_glm_out* out);
 
+/* Test hook, host only (no device): the multigrid hierarchy that an escalation would build for
+ * the first block above 768 levels of the given unweighted structure. sizes / nnz receive up to
+ * max_levels entries; row_sum receives each level's largest |row sum| relative to its largest
+ * diagonal (0 for a Laplacian, as every level must be). Returns the level count in *levels
+ * (0 when no block qualifies). */
+int fereg_amg_probe(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, int max_levels,
+                    uint32_t* levels, uint32_t* sizes, uint64_t* nnz, double* row_sum);
+
 /* Sample preparation on the device (Session::prepare's FE-id compression and sample drops;
  * host arrays in and out). Bit-exact with the reference's definitions.
  * fereg_factorize: factor.rs:38, dense codes in ascending value order (-0 = +0; NaN: 198).
