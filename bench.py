@@ -152,28 +152,12 @@ def run_glm(args, cfg, rank, world, local, pg):
     if args.impl == "reference":
         if rank != 0:
             return
-        from oracle import oracle
-
-        ab = oracle.Absorber(codes, g)
-        rng = np.random.default_rng(1)
-        w = rng.uniform(0.5, 2.0, n)
-        ab.set_weights(w)
-        z = np.ascontiguousarray(rows[ab.row_order()])
-        ts = []
-        for _ in range(2):
-            zz = z.copy()
-            t0 = time.perf_counter()
-            ab.residualize(zz, tol=1e-8)
-            ts.append(time.perf_counter() - t0)
-        per_it = float(np.mean(ts))
-        iters = 12
-        v = per_it * iters
+        cpu = glm_cpu_sample(codes, g, rows, 12)
+        v = cpu["value"]
         line = {"impl": "reference", "metric": GLM_METRIC, "value": v, "unit": "s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": "c4", "n": n},
-                "cpu_baseline": {"value": v, "unit": "s", "cores": oracle.max_threads(), "kind": "port",
-                                 "sample": f"one weighted FE solve of [z, x1, ldist] ({per_it:.3f} s, C++ FP64 "
-                                           f"restatement, all host threads) times {iters} IRLS iterations"},
+                "cpu_baseline": cpu,
                 "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -231,6 +215,9 @@ def run_glm(args, cfg, rank, world, local, pg):
                            "prepare_s": prepare_s, "precision": args.precision,
                            "parallelism": f"replicas x{world}"},
                 "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
+                "roofline": roofline_of(sess, phases, n, 3, True, 8 if prec == fb.PREC_F64 else 4, "c4"),
+                "cpu_baseline": None if args.no_cpu_baseline or world > 1 else
+                glm_cpu_sample(codes, g, make_gravity_data(cfg)[2], res["iterations"]),
                 "clocks": clk.summary(),
                 "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": n * 3 * 8, "d2h_bytes_per_step": 96},
                 "gpu_launches": launches}
@@ -565,32 +552,77 @@ def run_serve_reference(args, cfg, world):
 BOOT_METRIC = "wild-boot reps/s (WCR11, 9,999 Rademacher draws, n=1e6, 3 FE, cluster firm 2e4)"
 
 
+def boot_cpu_sample(codes, g, rows, rounds=2):
+    """The CPU oracle's cost per bootstrap draw: the FE solve of 16 draw columns (the per-draw
+    refit's dominant cost), all host threads; the first round is a warm-up."""
+    from oracle import oracle
+
+    ab = oracle.Absorber(codes, g)
+    rng = np.random.default_rng(1)
+    nd = 16
+    z = np.ascontiguousarray(rows[ab.row_order(), :1] * rng.choice([-1.0, 1.0], size=(rows.shape[0], nd)))
+    times = []
+    for _ in range(max(2, rounds)):
+        zz = z.copy()
+        t0 = time.perf_counter()
+        ab.residualize(zz, tol=TOL)
+        times.append(time.perf_counter() - t0)
+    v = nd / float(np.mean(times[1:]))
+    return {"value": v, "unit": "reps/s", "cores": oracle.max_threads(), "kind": "port",
+            "sample": f"the FE solve of {nd} draw columns (the per-draw refit's dominant cost), "
+                      f"{len(times) - 1} timed rounds, C++ FP64 restatement, all host threads"}
+
+
+def glm_cpu_sample(codes, g, rows, iters):
+    """The CPU oracle's cost of one PPML call: one weighted FE solve of [z, x1, ldist] (the IRLS
+    iteration's dominant cost) times the iteration count, all host threads."""
+    from oracle import oracle
+
+    ab = oracle.Absorber(codes, g)
+    rng = np.random.default_rng(1)
+    ab.set_weights(rng.uniform(0.5, 2.0, rows.shape[0]))
+    z = np.ascontiguousarray(rows[ab.row_order()])
+    ts = []
+    for _ in range(2):
+        zz = z.copy()
+        t0 = time.perf_counter()
+        ab.residualize(zz, tol=1e-8)
+        ts.append(time.perf_counter() - t0)
+    per_it = float(np.mean(ts))
+    return {"value": per_it * iters, "unit": "s", "cores": oracle.max_threads(), "kind": "port",
+            "sample": f"one weighted FE solve of [z, x1, ldist] ({per_it:.3f} s, C++ FP64 restatement, all host "
+                      f"threads) times {iters} IRLS iterations"}
+
+
+def roofline_of(sess, phases, n, R, weighted, s_v, workload):
+    """Roofline of the dominant timed phase: algorithmic bytes of one call of it (phase_bytes with
+    R columns) over its average duration, against the measured copy bandwidth."""
+    hbm, peak_kind = peaks()
+    info = sess.info()
+    algo = phase_bytes(info, n, R, weighted, s_v)
+    timed = {k: v for k, v in phases.items() if k in algo and v[1]}
+    dom = max(timed, key=lambda k: timed[k][0])
+    ms, cnt = timed[dom]
+    achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
+    kern = PHASE_KERNEL[dom]
+    return {"bound": "hbm", "kernel": kern, "phase": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": traffic_from_profiles(kern, workload), "peak_kind": peak_kind,
+            "algorithmic_bytes": algo[dom], "columns": R}
+
+
 def run_boot(args, cfg, rank, world, local, pg):
     """C3: one WCR11 bootstrap call per step; value = draws per second of the whole job."""
     if args.impl == "reference":
         if rank != 0:
             return
-        from oracle import oracle
-
         codes, g, firm, rows = make_boot_data(cfg)
-        ab = oracle.Absorber(codes, g)
-        rng = np.random.default_rng(1)
-        nd = 16
-        z = np.ascontiguousarray(rows[ab.row_order(), :1] * rng.choice([-1.0, 1.0], size=(rows.shape[0], nd)))
-        times = []
-        for it in range(max(1, args.warmup // 3) + max(1, args.steps // 3)):
-            zz = z.copy()
-            t0 = time.perf_counter()
-            ab.residualize(zz, tol=TOL)
-            times.append(time.perf_counter() - t0)
-        v = nd / float(np.mean(times[1:] if len(times) > 1 else times))
+        cpu = boot_cpu_sample(codes, g, rows, 1 + max(1, args.steps // 3))
+        v = cpu["value"]
         line = {"impl": "reference", "metric": BOOT_METRIC, "value": v, "unit": "reps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": "c3", "n": rows.shape[0], "reps": cfg["reps"]},
-                "cpu_baseline": {"value": v, "unit": "reps/s", "cores": oracle.max_threads(), "kind": "port",
-                                 "sample": f"the FE solve of {nd} draw columns per step (the per-draw refit's "
-                                           "dominant cost), C++ FP64 restatement, all host threads"},
+                "cpu_baseline": cpu,
                 "e2e": {"value": v, "unit": "reps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -652,6 +684,10 @@ def run_boot(args, cfg, rank, world, local, pg):
                            "precision": args.precision, "prepare_s": prepare_s, "stat": res["stat"],
                            "pvalue": res["pvalue"], "parallelism": f"replicas x{world}"},
                 "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
+                # per apply / residualize call of one draw tile (tile columns); the fit's 2-column
+                # solve is counted at the tile's width
+                "roofline": roofline_of(sess, phases, n, args.boot_tile, False, 8 if prec == fb.PREC_F64 else 4, "c3"),
+                "cpu_baseline": None if args.no_cpu_baseline or world > 1 else boot_cpu_sample(codes, g, rows),
                 "clocks": clk.summary(),
                 "e2e": {"value": e2e, "unit": "reps/s", "h2d_bytes_per_step": n * 2 * 8,
                         "d2h_bytes_per_step": int(res["reps"]) * 8 + 64},
