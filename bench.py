@@ -356,7 +356,7 @@ def run_serve(args, cfg, rank, world, local, pg):
     import fereg_b200 as fb
 
     torch.cuda.set_device(local)
-    pool = ServePool(cfg["seed"] + 7919 * rank)
+    pool = ServePool(rank_seed(cfg["seed"], rank))
     srv = fb.Server(workers=args.serve_workers)
     tol = cfg["tol"]
 
@@ -818,19 +818,29 @@ def dist_setup():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        # NCCL on the GPU box; gloo (FEREG_DIST_BACKEND=gloo) for host-only runs of the same logic
+        dist.init_process_group(os.environ.get("FEREG_DIST_BACKEND", "nccl"),
+                                timeout=datetime.timedelta(seconds=300))
         pg = dist
     return rank, world, local, pg
 
 
 def max_over_ranks(x, pg, device):
+    """The max of x over the ranks (the step time of a multi-GPU run); host tensors under gloo."""
     if pg is None:
         return x
     import torch
 
+    if pg.get_backend() == "gloo":
+        device = None
     t = torch.tensor([x], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_seed(seed, rank):
+    """Seed of rank `rank`'s replica: each rank serves its own seeded stream (weak scaling)."""
+    return seed + 7919 * rank
 
 
 def barrier(pg):
