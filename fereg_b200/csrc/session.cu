@@ -1108,7 +1108,8 @@ void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec
 // GLM by IRLS, Poisson PML or logit (glm/irls.rs:367-560 with ppmlhdfe conventions,
 // glm/mod.rs:1053-1140 for the variance). Each iteration: the family's w and z (device), the weight state
 // refreshed on the device, [z, X] residualized warm-started from the previous FE coefficients at
-// an inner tolerance tightened toward max(1e-12, min(itol, 0.1 tol)), the weighted regression on the
+// an inner tolerance tightened toward max(1e-12, min(itol, 0.1 tol)) by ppmlhdfe's heuristic
+// schedule (irls.rs:900-911, with its eps prediction), the weighted regression on the
 // residualized block (device Gram, host sweep), eta = z - e and mu = exp(eta) with the deviance
 // (device). Stops when the relative deviance change |D - D'| / max(min(D, D'), 0.1) < tol with the
 // inner tolerance at its floor. Collinearity is settled in the first iteration (ppmlhdfe
@@ -1116,6 +1117,47 @@ void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec
 // variance uses the last iteration's weights: robust, (X~'WX~)^-1 [sum (e w)^2 x~ x~'] (X~'WX~)^-1
 // N / (N - 1), clustered with G / (G - 1) and the multiway eigenvalue clip, or (logit `oim`)
 // the inverse Hessian (X~'WX~)^-1.
+namespace {
+
+constexpr double EPS1 = 2.220446049250313e-16;  // Mata epsilon(1)
+
+bool inrange(double x, double lb, double ub) { return !std::isnan(lb) && lb <= x && (std::isnan(ub) || x <= ub); }
+
+// ppmlhdfe predict_eps (irls.rs:105-140): ln eps of the last three iterations; once all three
+// are known, the cubic through (i, ln eps_i), i = 1..3 without a constant, evaluated at i = 4.
+struct EpsHistory {
+    double h[3] = {nanv(), nanv(), nanv()};
+    double predict(double eps) {
+        int pos = 0;
+        for (double v : h) pos += !std::isnan(v);
+        const bool abort = pos + 1 < 3;
+        const double le = eps > 0.0 ? std::log(eps) : nanv();
+        if (pos < 3) {
+            h[pos] = le;
+        } else {
+            h[0] = h[1];
+            h[1] = h[2];
+            h[2] = le;
+        }
+        if (abort || std::isnan(h[0]) || std::isnan(h[1]) || std::isnan(h[2])) return nanv();
+        double a[3][4] = {{1, 1, 1, h[0]}, {2, 4, 8, h[1]}, {3, 9, 27, h[2]}};
+        for (int p = 0; p < 3; p++)
+            for (int r = p + 1; r < 3; r++) {
+                const double f = a[r][p] / a[p][p];
+                for (int j = p; j < 4; j++) a[r][j] -= f * a[p][j];
+            }
+        double c[3] = {0, 0, 0};
+        for (int p = 2; p >= 0; p--) {
+            double s = a[p][3];
+            for (int j = p + 1; j < 3; j++) s -= a[p][j] * c[j];
+            c[p] = s / a[p][p];
+        }
+        return std::exp(4.0 * c[0] + 16.0 * c[1] + 64.0 * c[2]);
+    }
+};
+
+}  // namespace
+
 void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out) {
     AllocScope alloc_scope(ab_->stream());
     if (!wk_.empty()) throw Error(RC_INVALID_INPUT, "fereg glm: weighted sessions are not supported");
@@ -1171,7 +1213,8 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
     outer_products(raw.p, n, R, all, nullptr, false, nullptr, nullptr, true, &sumsq);
     const double highest = std::max(1e-12, std::min(gs.itol, 0.1 * gs.tol));  // glm/mod.rs:826
     double tol_in = std::max(1e-4, gs.tol);
-    double dev_old = nanv(), dev = nanv();
+    double dev_old = nanv(), dev = nanv(), eps = nanv(), alt_tol = nanv();
+    EpsHistory hist;
     bool have_warm = false, converged = false;
     std::vector<uint8_t> status(nx, 0);
     std::vector<size_t> kept;
@@ -1181,6 +1224,7 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
     for (size_t it = 1; it <= gs.maxiter; it++) {
         ab_->ctx().check();
         iters = it;
+        const double predicted = hist.predict(eps);
         int ph = d.begin(S_WEIGHTS);
         k_glm_work<<<blocks, 256, 0, st>>>(raw.p, n, R, fam, mu.p, eta.p, B.p, z.p, w.p);
         d.launches++;
@@ -1248,13 +1292,22 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
         if (!std::isfinite(dev)) throw Error(RC_CONVERGENCE, "fereg glm: the deviance is not finite");
         have_warm = true;
         if (it > 1) {
-            const double eps = std::fabs(dev - dev_old) / std::max(std::min(dev, dev_old), 0.1);
-            if (eps < gs.tol && tol_in <= highest) {
+            double delta = dev_old - dev;
+            if (!std::isnan(delta) && dev < 0.1 * delta) delta = dev;
+            eps = std::fabs(delta) / std::max(std::min(dev, dev_old), 0.1);
+            if (eps < gs.tol && tol_in <= 1.1 * highest) {
                 converged = true;
                 dev_old = dev;
                 break;
             }
-            if (eps < tol_in) tol_in = std::max(highest, tol_in * 0.1);
+            // inner tolerance schedule (irls.rs:900-911, ppmlhdfe use_heuristic_tol): a decade,
+            // or down to the decade of 0.1 eps seen at the previous tightening, and one more
+            // decade when the predicted eps is already below tol
+            if (eps < tol_in) {
+                tol_in = std::max(std::min(0.1 * tol_in, alt_tol), highest);
+                alt_tol = std::pow(10.0, -std::ceil(std::log10(1.0 / std::max(0.1 * eps, EPS1))));
+            }
+            if (inrange(gs.tol, predicted, eps) && inrange(tol_in / highest, 1.1, 10.1)) tol_in *= 0.1;
         }
         dev_old = dev;
     }

@@ -72,6 +72,23 @@ def dense_glm(family, terms, y, X, vce="robust", cl=None, maxiter=200):
     return b, V, dev, ll
 
 
+def _predict_eps(hist, eps):
+    """ppmlhdfe predict_eps (glm/irls.rs:105-140): the cubic without a constant through the last
+    three (i, ln eps_i), evaluated at i = 4; NaN until three values are known."""
+    le = np.log(eps) if eps > 0 else np.nan
+    known = [v for v in hist if not np.isnan(v)]
+    abort = len(known) + 1 < 3
+    if len(known) < 3:
+        hist[:] = known + [le]
+    else:
+        hist[:] = known[1:] + [le]
+    if abort or len(hist) < 3 or any(np.isnan(v) for v in hist):
+        return np.nan
+    A = np.array([[1.0, 1.0, 1.0], [2.0, 4.0, 8.0], [3.0, 9.0, 27.0]])
+    c = np.linalg.solve(A, np.array(hist))
+    return float(np.exp(4 * c[0] + 16 * c[1] + 64 * c[2]))
+
+
 def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=1e-10, maxiter=1000):
     """IRLS with the fixed effects absorbed by the oracle's FE solver (the reference's loop,
     glm/irls.rs:367-560): each iteration sets the family's weights on the absorber, residualizes
@@ -98,7 +115,9 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
     tol_in = max(1e-4, tol)
     dev_old = np.nan
     warm = None
+    eps, alt_tol, hist = np.nan, np.inf, []
     for it in range(1, maxiter + 1):
+        predicted = _predict_eps(hist, eps)
         if family == "poisson":
             w = mu
             z = eta - 1 + y / mu
@@ -121,11 +140,19 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
             mu = np.clip(expit(eta), 100 * np.finfo(float).eps, 1 - 100 * np.finfo(float).eps)
             dev = 2 * np.sum(np.logaddexp(0, eta) - y * eta)
         if it > 1:
-            eps = abs(dev - dev_old) / max(min(dev, dev_old), 0.1)
-            if eps < tol and tol_in <= highest:
+            delta = dev_old - dev
+            if dev < 0.1 * delta:
+                delta = dev
+            eps = abs(delta) / max(min(dev, dev_old), 0.1)
+            if eps < tol and tol_in <= 1.1 * highest:
                 break
+            # irls.rs:900-911: a decade, or down to the decade of 0.1 eps of the previous
+            # tightening, and one more when the predicted eps is below tol
             if eps < tol_in:
-                tol_in = max(highest, tol_in * 0.1)
+                tol_in = max(min(0.1 * tol_in, alt_tol), highest)
+                alt_tol = 10.0 ** (-np.ceil(np.log10(1.0 / max(0.1 * eps, np.finfo(float).eps))))
+            if not np.isnan(predicted) and tol <= predicted <= eps and 1.1 <= tol_in / highest <= 10.1:
+                tol_in *= 0.1
         dev_old = dev
     s = (e * w)[:, None] * Xt
     if vce == "oim":
