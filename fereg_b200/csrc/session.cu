@@ -161,57 +161,118 @@ void GpuSession::phase_times(double* ms, u64* counts) const {
 }
 
 // dof.rs:222-256 mobility_groups of terms qa, qb on the device; save: keep the row labels.
-u64 GpuSession::mobility_groups(size_t qa, size_t qb, bool save) {
+// Runs on the dof pass's stream with its buffers.
+u64 GpuSession::mobility_groups(size_t qa, size_t qb, bool save, DofScratch& s) {
     SessionDev& d = *d_;
+    const cudaStream_t st = s.st.s;
     const u32 ga = tg_[qa], gb = tg_[qb], nv = ga + gb;
-    d.uf.alloc(nv);
-    d.flags.alloc(ga);
-    d.scan.alloc(ga);
-    d.bsum.alloc((ga + SCAN_TILE - 1) / SCAN_TILE + 1);
-    d.total.alloc(1);
-    d.err.alloc(1);
-    CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), d.st));
-    k_uf_init<<<blocks_for(nv, 256), 256, 0, d.st>>>(d.uf.p, nv);
-    k_uf_union<<<blocks_for(n_, 256), 256, 0, d.st>>>(d.tcodes[qa].p, d.tcodes[qb].p, ga, n_, d.uf.p, d.err.p);
-    k_uf_flatten<<<blocks_for(nv, 256), 256, 0, d.st>>>(d.uf.p, nv);
-    k_uf_roots<<<blocks_for(ga, 256), 256, 0, d.st>>>(d.uf.p, ga, d.flags.p);
+    s.uf.alloc(nv);
+    s.flags.alloc(ga);
+    s.scan.alloc(ga);
+    s.bsum.alloc((ga + SCAN_TILE - 1) / SCAN_TILE + 1);
+    s.total.alloc(1);
+    s.err.alloc(1);
+    CK(cudaMemsetAsync(s.err.p, 0, sizeof(int), st));
+    k_uf_init<<<blocks_for(nv, 256), 256, 0, st>>>(s.uf.p, nv);
+    k_uf_union<<<blocks_for(n_, 256), 256, 0, st>>>(d.tcodes[qa].p, d.tcodes[qb].p, ga, n_, s.uf.p, s.err.p);
+    k_uf_flatten<<<blocks_for(nv, 256), 256, 0, st>>>(s.uf.p, nv);
+    k_uf_roots<<<blocks_for(ga, 256), 256, 0, st>>>(s.uf.p, ga, s.flags.p);
     const u32 nblk = (ga + SCAN_TILE - 1) / SCAN_TILE;
-    k_scan_sums<<<nblk, SCAN_TB, 0, d.st>>>(d.flags.p, ga, d.bsum.p);
-    k_scan_top<<<1, SCAN_TB, 0, d.st>>>(d.bsum.p, nblk, d.total.p);
-    k_scan_apply<<<nblk, SCAN_TB, 0, d.st>>>(d.flags.p, ga, d.bsum.p, d.scan.p);
-    d.launches += 7;
+    k_scan_sums<<<nblk, SCAN_TB, 0, st>>>(s.flags.p, ga, s.bsum.p);
+    k_scan_top<<<1, SCAN_TB, 0, st>>>(s.bsum.p, nblk, s.total.p);
+    k_scan_apply<<<nblk, SCAN_TB, 0, st>>>(s.flags.p, ga, s.bsum.p, s.scan.p);
+    s.launches += 7;
     if (save) {
-        d.gv.alloc(n_);
-        k_uf_label<<<blocks_for(n_, 256), 256, 0, d.st>>>(d.tcodes[qa].p, n_, d.uf.p, d.scan.p, d.gv.p);
-        d.launches++;
+        s.gv.alloc(n_);
+        k_uf_label<<<blocks_for(n_, 256), 256, 0, st>>>(d.tcodes[qa].p, n_, s.uf.p, s.scan.p, s.gv.p);
+        s.launches++;
     }
     u32 total = 0;
     int err = 0;
-    CK(cudaMemcpyAsync(&total, d.total.p, sizeof(u32), cudaMemcpyDeviceToHost, d.st));
-    CK(cudaMemcpyAsync(&err, d.err.p, sizeof(int), cudaMemcpyDeviceToHost, d.st));
-    CK(cudaStreamSynchronize(d.st));
+    CK(cudaMemcpyAsync(&total, s.total.p, sizeof(u32), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&err, s.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     if (err) throw Error(RC_INTERNAL, "fereg: union-find did not settle");
     return total;
 }
 
 // dof.rs:184 nested_within: every level of term q lies in one level of cluster dimension c.
-bool GpuSession::nested_within(size_t q, size_t c) {
+bool GpuSession::nested_within(size_t q, size_t c, DofScratch& s) {
     SessionDev& d = *d_;
-    d.map.alloc(tg_[q]);
-    d.err.alloc(1);
-    CK(cudaMemsetAsync(d.map.p, 0xff, size_t(tg_[q]) * sizeof(u32), d.st));
-    CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), d.st));
-    k_nested<<<blocks_for(n_, 256), 256, 0, d.st>>>(d.tcodes[q].p, d.ccodes[c].p, n_, d.map.p, d.err.p);
-    d.launches++;
+    const cudaStream_t st = s.st.s;
+    s.map.alloc(tg_[q]);
+    s.err.alloc(1);
+    CK(cudaMemsetAsync(s.map.p, 0xff, size_t(tg_[q]) * sizeof(u32), st));
+    CK(cudaMemsetAsync(s.err.p, 0, sizeof(int), st));
+    k_nested<<<blocks_for(n_, 256), 256, 0, st>>>(d.tcodes[q].p, d.ccodes[c].p, n_, s.map.p, s.err.p);
+    s.launches++;
     int flag = 0;
-    CK(cudaMemcpyAsync(&flag, d.err.p, sizeof(int), cudaMemcpyDeviceToHost, d.st));
-    CK(cudaStreamSynchronize(d.st));
+    CK(cudaMemcpyAsync(&flag, s.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     return flag == 0;
+}
+
+// Starts the dof pass (dof.rs:64-180 does not depend on the data columns) on a host thread of
+// its own and its own low-priority stream, so that its union-finds overlap the column statistics
+// and the FE solve the caller issues on the session's stream; dof_end joins it. The pass waits
+// for the work already on the session's stream (the uploaded codes).
+std::future<GpuSession::Dof> GpuSession::dof_begin(bool clusters, bool firstpair, bool want_groupvar) {
+    SessionDev& d = *d_;
+    DofScratch& s = d.dof;
+    if (!s.st.s) {
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&s.st.s, cudaStreamNonBlocking, least));
+        CK(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
+    }
+    CK(cudaEventRecord(s.ready, d.st));
+    CK(cudaStreamWaitEvent(s.st.s, s.ready, 0));
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    cudaEvent_t ta = nullptr, tb = nullptr;
+    if (d.prof) {
+        ta = d.event();
+        tb = d.event();
+    }
+    s.ta = ta;
+    s.tb = tb;
+    return std::async(std::launch::async, [this, &s, dev, ta, tb, clusters, firstpair, want_groupvar]() {
+        CK(cudaSetDevice(dev));
+        AllocScope scope(s.st.s);
+        if (ta) CK(cudaEventRecord(ta, s.st.s));
+        Dof dof = dof_pass(clusters, firstpair, want_groupvar, s);
+        if (tb) CK(cudaEventRecord(tb, s.st.s));
+        return dof;
+    });
+}
+
+GpuSession::Dof GpuSession::dof_end(std::future<Dof>& job) {
+    SessionDev& d = *d_;
+    DofScratch& s = d.dof;
+    const cudaEvent_t ta = s.ta, tb = s.tb;
+    s.ta = s.tb = nullptr;
+    Dof dof;
+    try {
+        dof = job.get();
+    } catch (...) {
+        if (ta) d.pool.push_back(ta);
+        if (tb) d.pool.push_back(tb);
+        throw;
+    }
+    if (ta) d.open.push_back(SessionDev::Open{S_DOF, ta, tb});
+    d.launches += s.launches;
+    s.launches = 0;
+    return dof;
+}
+
+GpuSession::Dof GpuSession::estimate_dof(bool clusters, bool firstpair, bool want_groupvar) {
+    std::future<Dof> job = dof_begin(clusters, firstpair, want_groupvar);
+    return dof_end(job);
 }
 
 // dof.rs:64-180 estimate_dof (intercept-only terms, the default options: clusters and pairwise;
 // firstpair instead of both). Slot i: k levels, m redundant, exact, nested in a cluster.
-GpuSession::Dof GpuSession::estimate_dof(bool clusters, bool firstpair, bool want_groupvar) {
+GpuSession::Dof GpuSession::dof_pass(bool clusters, bool firstpair, bool want_groupvar, DofScratch& s) {
     Dof dof;
     const size_t nt = tg_.size();
     std::vector<bool> live(nt, true);
@@ -221,7 +282,7 @@ GpuSession::Dof GpuSession::estimate_dof(bool clusters, bool firstpair, bool wan
             if (std::none_of(live.begin(), live.end(), [](bool x) { return x; })) break;
             for (size_t q = 0; q < nt; q++) {
                 if (!live[q] || dof.slots[q].exact) continue;
-                if (nested_within(q, c)) {
+                if (nested_within(q, c, s)) {
                     dof.slots[q].m = dof.slots[q].k;
                     dof.slots[q].exact = dof.slots[q].nested = true;
                     dof.df_a_nested += dof.slots[q].k;
@@ -257,7 +318,7 @@ GpuSession::Dof GpuSession::estimate_dof(bool clusters, bool firstpair, bool wan
         for (size_t b = a + 1; b < idx.size(); b++) {
             pairs++;
             const bool save = pairs == 1 && want_groupvar;
-            const u64 m = mobility_groups(idx[a], idx[b], save);
+            const u64 m = mobility_groups(idx[a], idx[b], save, s);
             if (save) dof.has_groupvar = true;
             dof.slots[idx[b]].m = std::max(dof.slots[idx[b]].m, m);
             if (pairs == 1) dof.slots[idx[b]].exact = true;
@@ -431,10 +492,9 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     const bool has_intercept = true;  // intercept-only terms (or noabsorb) contain the constant
     const bool report_constant = has_intercept && !spec.noconstant;
 
-    int ph = d.begin(S_DOF);
-    const Dof dof = estimate_dof(vce == 2, spec.firstpair != 0, spec.want_groupvar != 0 && out.groupvar);
-    d.end(ph);
-    ph = d.begin(S_COLSTATS);
+    // the dof pass runs on its own stream beside the column statistics and the solve
+    std::future<Dof> dof_job = dof_begin(vce == 2, spec.firstpair != 0, spec.want_groupvar != 0 && out.groupvar);
+    int ph = d.begin(S_COLSTATS);
 
     // Pass A: column statistics of the raw rows (stats.rs:40), raw weights, in one device pass
     const ColStats cs = column_stats(rows, R);
@@ -553,6 +613,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     std::vector<double> b_full_s = b_s;
     if (report_constant) b_full_s.push_back(b0_s);
 
+    const Dof dof = dof_end(dof_job);
     const double df_a = double(dof.df_a), df_m = double(k);
     double df_r = bigN - df_a - df_m;
     double g_min = 0.0;
@@ -716,7 +777,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     if (out.groupvar) {
     if (dof.has_groupvar) {
         std::vector<u32> gv(n);
-        CK(cudaMemcpyAsync(gv.data(), d.gv.p, n * sizeof(u32), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(gv.data(), d.dof.gv.p, n * sizeof(u32), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         for (size_t i = 0; i < n; i++) out.groupvar[i] = double(gv[i]);
     } else {
@@ -762,10 +823,8 @@ void GpuSession::iv(double* rows_in, bool on_device, size_t nx, size_t ne, size_
     if (vce == 0 && kind == 3) vce = 1;  // pweights imply robust
     if (vce == 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg iv: cluster variance without clusters");
 
-    int ph = d.begin(S_DOF);
-    const Dof dof = estimate_dof(vce == 2, false, false);
-    d.end(ph);
-    ph = d.begin(S_COLSTATS);
+    std::future<Dof> dof_job = dof_begin(vce == 2, false, false);
+    int ph = d.begin(S_COLSTATS);
     const ColStats cs = column_stats(rows, R);
     d.end(ph);
     const SolveInfo info = ab_->residualize_device(rows, r, spec.tol, spec.maxiter, false, nullptr, nullptr, spec.prec);
@@ -862,6 +921,7 @@ void GpuSession::iv(double* rows_in, bool on_device, size_t nx, size_t ne, size_
     CK(cudaMemcpyAsync(&rss, d.sums.p, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
 
+    const Dof dof = dof_end(dof_job);
     const double sdof = std::max<double>(double(dof.df_a), 1.0);
     const double nk = bigN - double(k) - sdof;
     const double g_min = cg_.empty() ? 0.0 : double(*std::min_element(cg_.begin(), cg_.end()));

@@ -5,6 +5,7 @@
 // residuals and meats) and its K x K algebra on the host.
 #pragma once
 
+#include <future>
 #include <memory>
 #include <vector>
 
@@ -40,6 +41,7 @@ struct OlsOut {
 };
 
 struct SessionDev;
+struct DofScratch;
 
 class GpuSession {
    public:
@@ -148,7 +150,12 @@ class GpuSession {
         u64 df_a = 0, df_a_initial = 0, df_a_redundant = 0, df_a_nested = 0;
         bool has_groupvar = false;
     };
+    // The dof pass, joined at once.
     Dof estimate_dof(bool clusters, bool firstpair, bool want_groupvar);
+    // The same pass started on its own stream and host thread; dof_end joins it.
+    std::future<Dof> dof_begin(bool clusters, bool firstpair, bool want_groupvar);
+    Dof dof_end(std::future<Dof>& job);
+    Dof dof_pass(bool clusters, bool firstpair, bool want_groupvar, DofScratch& s);
     struct ColStats {
         std::vector<double> wmean, sumsq, wss_unc, sd, wss;
     };
@@ -167,8 +174,8 @@ class GpuSession {
         bool y_absorbed = false;
     };
     FitState fit_;
-    u64 mobility_groups(size_t qa, size_t qb, bool save);
-    bool nested_within(size_t q, size_t c);
+    u64 mobility_groups(size_t qa, size_t qb, bool save, DofScratch& s);
+    bool nested_within(size_t q, size_t c, DofScratch& s);
 };
 
 }  // namespace fereg

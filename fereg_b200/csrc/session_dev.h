@@ -8,8 +8,36 @@
 
 namespace fereg {
 
+// A CUDA stream owned by its holder.
+struct OwnedStream {
+    cudaStream_t s = nullptr;
+    OwnedStream() = default;
+    OwnedStream(const OwnedStream&) = delete;
+    OwnedStream& operator=(const OwnedStream&) = delete;
+    ~OwnedStream() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+// The degrees-of-freedom pass (nested checks and the union-finds of the FE pairs) runs on its own
+// low-priority stream from a host thread of its own, beside the session's stream; these are its
+// buffers. gv (the mobility groups of the first pair, row labels) is read on the session's
+// stream once the pass has been joined.
+struct DofScratch {
+    OwnedStream st;              // declared first: destroyed after the buffers allocated on it
+    cudaEvent_t ready = nullptr; // recorded on the session's stream before the pass starts
+    cudaEvent_t ta = nullptr, tb = nullptr;  // phase timing of the pass (when profiling)
+    DBuf<u32> uf, flags, scan, bsum, total, gv, map;
+    DBuf<int> err;
+    u64 launches = 0;
+    ~DofScratch() {
+        if (ready) cudaEventDestroy(ready);
+    }
+};
+
 // Device state of a session.
 struct SessionDev {
+    DofScratch dof;
     std::vector<DBuf<u32>> tcodes, ccodes;  // kept order
     struct Subset {
         DBuf<int> perm;  // rows (row order) grouped by cluster, stable
@@ -21,7 +49,7 @@ struct SessionDev {
     DBuf<double> w_raw, wv;  // row order
     DBuf<double> rows, part, sums, e, om, S, shift, beta;
     DBuf<int> col, err;
-    DBuf<u32> uf, flags, scan, bsum, total, gv, map;
+    DBuf<u32> map;
     DBuf<double> pstat;
     DBuf<double> colbuf;  // kept-order columns of a gather
     DBuf<u32> pi;         // row order -> kept position
