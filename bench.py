@@ -707,18 +707,42 @@ def workload_name(cfg_name):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: through NVML every 20 ms
+    (so that a timed region of a few tens of milliseconds still holds samples), else nvidia-smi
+    every 200 ms. Read-only queries; no GPU setting is changed."""
 
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
              "clocks_event_reasons.sw_power_cap"
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+        self.thread = None
         self.lines = []
+        self.samples = []  # (sm MHz, max MHz, set of reasons)
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            idx = torch.cuda._get_nvml_device_index(self.device)
+        except Exception:
+            idx = self.device
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+        except Exception:
+            self.nvml = None
+        if self.nvml:
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -729,11 +753,33 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv, h = self.nvml
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        while True:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(smax), {n for n, b in zip(self.NAMES, bits) if r & b}))
+            except Exception:
+                pass
+            if self.stop.wait(0.02):
+                break
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        if self.nvml:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -743,7 +789,10 @@ class ClockSampler:
 
     def summary(self):
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for a, b, rs in self.samples:
+            sm.append(a)
+            smax = b
+            reasons |= rs
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -753,11 +802,11 @@ class ClockSampler:
                 smax = float(parts[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            for nm, v in zip(self.NAMES, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def peaks():

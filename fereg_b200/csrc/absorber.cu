@@ -79,7 +79,6 @@ struct DevWarpTiles {
 
 // Dynamic shared memory of the warp-tile kernels for a chunk of Rc columns (per-warp parts, then
 // the lane-private small-coordinate slots and column partials).
-inline size_t wseg_smem(int Rc, size_t tsz, u32 ms_acc) { return WPB * (wseg_bytes(Rc, tsz) + size_t(ms_acc) * 32 * tsz); }
 inline size_t wrhs_smem(int Rc, u32 ms_acc) { return WPB * (wrhs_bytes(Rc) + size_t(ms_acc) * 32 * 8 + 2 * 32 * 8); }
 inline size_t wresid_smem(int Rc) { return WPB * wresid_bytes(Rc); }
 inline size_t wpull_smem() { return WPB * pull_bytes(); }
@@ -141,6 +140,7 @@ struct Scratch {
     DBuf<u32> seg_off, coord, cell_row, pl_off, pl_cell, pl_seg, pl_other;
     DevTiles seg_tiles, pull_tiles;      // CTA tiles of the long lists
     DevWarpTiles wseg, wpull;            // warp tiles of the short lists
+    DBuf<u32> wseg_segs;                 // the segments of the warp tiles, in order
     u32 ms_acc = 0, ns_acc = 0;  // small coordinates / blocks summed in the segment passes
     // weights
     DBuf<double> w_rows, cell_w, n1inv, nr, inv_diag, minv;
@@ -269,6 +269,10 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
         TileList ct;
         split_tiles(hs_.seg_off, &wgt, 0, hs_.g1, WT, WT, WSEG, TILE, wt, ct);
         d_->wseg.upload(wt, stream_);
+        std::vector<u32> segs;  // the short segments in order (one per lane group in k_gseg_apply)
+        for (size_t i = 0; i < wt.k0.size(); i++)
+            for (u32 s = wt.k0[i]; s < wt.k1[i]; s++) segs.push_back(s);
+        d_->wseg_segs.upload(segs, stream_);
         d_->seg_tiles.upload(ct, stream_);
         CK(cudaStreamSynchronize(stream_));
     }
@@ -855,12 +859,13 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
     if (d.wseg.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = wseg_smem(Rc, sizeof(T), S.ms_acc);
+            const size_t shm = size_t(WPB) * S.ms_acc * 32 * sizeof(T);
+            const u32 nsegs = u32(d.wseg_segs.n);
             with_rcp<1>(Rc, S.nb, [&](auto c, auto nbk) {
                 constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
-                allow_smem(k_wseg_apply<T, RCP, NBK>, shm);
-                k_wseg_apply<T, RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), P, R, j0, Rc, t,
-                                                                          acc ? small : nullptr);
+                allow_smem(k_gseg_apply<T, RCP, NBK>, shm);
+                k_gseg_apply<T, RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, nsegs, P, R, j0, Rc,
+                                                                          t, acc ? small : nullptr);
             });
             d.launches++;
         }

@@ -302,6 +302,112 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wseg_apply(DevStruct S, DevWeig
     if (acc) flush_wacc<RCP>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
 }
 
+// Operator pass 1 on the short segments, one segment per group of RCP lanes (lane = column):
+// t_s = n1inv_s sum_c W_c u_c with u_c = sum_b P[coord_b(c)], and the small coordinates take
+// sum_c W_c u_c - t_s sum_c W_c per small code in the lane's private slots. segs lists the short
+// segments in order; group q of the grid takes segs[q], segs[q + groups], ... so every lane's
+// sums have a fixed order.
+//
+// The group walks its segment in chunks of RCP cells: lane i of the group loads the block codes
+// and the weight of the chunk's cell i (one coalesced load per block), and the cells are then
+// taken in turn with the codes broadcast by shuffles, four cells' gathers in flight together.
+// The small codes are the first blocks' codes, already at hand. The second walk (t_s times the
+// weights) reloads the chunk's codes, which the first left in L1. The next segment's index is
+// fetched while the current one runs. The groups of a warp never wait on one another.
+template <class T, int RCP, int NBK>
+__global__ void __launch_bounds__(WPB * 32, 4) k_gseg_apply(DevStruct S, DevWeights W, const u32* __restrict__ segs,
+                                                            u32 nsegs, const T* __restrict__ P, int R, int j0, int Rc,
+                                                            T* __restrict__ t, T* __restrict__ cta_small) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int G = 32 / RCP;
+    constexpr int NL = NBK < WNB ? NBK : WNB;  // blocks whose codes the lanes hold
+    constexpr int U = 4;                       // cells whose gathers are in flight together
+    T* wacc_all = reinterpret_cast<T*>(smem_raw);
+    T* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 32;
+    const bool acc = cta_small != nullptr;
+    const bool weighted = W.cell_w != nullptr;
+    const u32 lane = wlane(), g = lane / RCP, j = lane % RCP;
+    const bool on = int(j) < Rc;
+    const unsigned gmask = RCP == 32 ? FULL : ((1u << RCP) - 1u) << (g * RCP);
+    const size_t Ru = size_t(R);
+    const u32 ns_acc = S.ns_acc;
+    if (acc)
+        for (u32 i = lane; i < S.ms_acc * 32; i += 32) wacc[i] = T(0);
+    const T* Pj = P + j0 + j;
+    const u32 groups = gridDim.x * WPB * G;
+    u32 q = (blockIdx.x * WPB + wid_in_cta()) * G + g;
+    u32 s = q < nsegs ? segs[q] : 0;
+    for (; q < nsegs; q += groups) {
+        const u32 c0 = S.seg_off[s], c1 = S.seg_off[s + 1];
+        const u32 qn = q + groups;
+        const u32 sn = qn < nsegs ? segs[qn] : 0;
+        T sum = T(0);
+        for (u32 cb = c0; cb < c1; cb += RCP) {
+            const u32 nc = min(c1 - cb, u32(RCP));
+            u32 code[NL];
+            double wl = 1.0;
+#pragma unroll
+            for (int b = 0; b < NL; b++) code[b] = j < nc ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
+            if (weighted && j < nc) wl = W.cell_w[cb + j];
+            for (u32 i0 = 0; i0 < nc; i0 += U) {
+                T v[U];
+                u32 k0[U];
+#pragma unroll
+                for (int k = 0; k < U; k++) {
+                    const u32 i = i0 + u32(k);
+                    T x = T(0);
+#pragma unroll
+                    for (int b = 0; b < NL; b++) {
+                        const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
+                        if (b == 0) k0[k] = cd;
+                        if (on && i < nc) x += Pj[size_t(cd) * Ru];
+                    }
+                    if constexpr (NBK == WNB)
+                        if (on && i < nc)
+                            for (u32 b = WNB; b < S.nb; b++)
+                                x += Pj[size_t(__ldg(S.coord + size_t(b) * S.M + cb + i)) * Ru];
+                    v[k] = x;
+                }
+#pragma unroll
+                for (int k = 0; k < U; k++) {
+                    const u32 i = i0 + u32(k);
+                    const T w = weighted ? T(__shfl_sync(gmask, wl, int(i), RCP)) : T(1);
+                    if (i < nc) {
+                        const T wv = w * v[k];
+                        sum += wv;
+                        if (acc && on) {
+                            wacc[k0[k] * 32 + lane] += wv;
+                            for (u32 b = 1; b < ns_acc; b++)
+                                wacc[__ldg(S.coord + size_t(b) * S.M + cb + i) * 32 + lane] += wv;
+                        }
+                    }
+                }
+            }
+        }
+        const T tv = sum * T(W.n1inv[s]);
+        if (on) t[size_t(s) * Ru + j0 + j] = tv;
+        if (acc)
+            for (u32 cb = c0; cb < c1; cb += RCP) {
+                const u32 nc = min(c1 - cb, u32(RCP));
+                u32 code[NL];
+#pragma unroll
+                for (int b = 0; b < NL; b++)
+                    code[b] = (b < int(ns_acc) && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
+                const double wl = (weighted && j < nc) ? W.cell_w[cb + j] : 1.0;
+                for (u32 i = 0; i < nc; i++) {
+                    const T w = weighted ? T(__shfl_sync(gmask, wl, int(i), RCP)) : T(1);
+#pragma unroll
+                    for (int b = 0; b < NL; b++) {
+                        const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
+                        if (on && b < int(ns_acc)) wacc[cd * 32 + lane] -= w * tv;
+                    }
+                }
+            }
+        s = sn;
+    }
+    if (acc) flush_wacc<RCP>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
+}
+
 // Staging of a coordinate-list tile: list ends and the entries' indices.
 struct PullStage {
     u32* kend;  // local end (entry) of each list (WLIST lists at most)
