@@ -79,7 +79,7 @@ struct DevWarpTiles {
 
 // Dynamic shared memory of the warp-tile kernels for a chunk of Rc columns (per-warp parts, then
 // the lane-private small-coordinate slots and column partials).
-inline size_t wrhs_smem(int Rc, u32 ms_acc) { return WPB * (wrhs_bytes(Rc) + size_t(ms_acc) * 32 * 8 + 2 * 32 * 8); }
+inline size_t grhs_smem(u32 ms_acc) { return WPB * (size_t(ms_acc) * 32 * 8 + 2 * 32 * 8); }
 inline size_t wresid_smem(int Rc) { return WPB * wresid_bytes(Rc); }
 inline size_t wpull_smem() { return WPB * pull_bytes(); }
 
@@ -985,12 +985,12 @@ void launch_rhs(Scratch& d, const DevStruct& S, const DevWeights& W, const doubl
     if (d.wseg.n) {
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = wrhs_smem(Rc, S.ms_acc);
+            const size_t shm = grhs_smem(S.ms_acc);
             with_rcp<WNB>(Rc, WNB, [&](auto c, auto) {
                 constexpr int RCP = decltype(c)::value;
-                allow_smem(k_wseg_rhs<RCP>, shm);
-                k_wseg_rhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, b1, d.cta2.p,
-                                                                acc ? small : nullptr);
+                allow_smem(k_grhs<RCP>, shm);
+                k_grhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, u32(d.wseg_segs.n), rows, R, j0, Rc,
+                                                            b1, d.cta2.p, acc ? small : nullptr);
             });
             d.launches++;
         }
@@ -1076,12 +1076,12 @@ void launch_rhs_scratch(Scratch& d, const DevStruct& S, const DevWeights& W, con
     if (d.wseg.n) {
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = wrhs_smem(Rc, S.ms_acc);
+            const size_t shm = grhs_smem(S.ms_acc);
             with_rcp<WNB>(Rc, WNB, [&](auto c, auto) {
                 constexpr int RCP = decltype(c)::value;
-                allow_smem(k_wseg_rhs<RCP>, shm);
-                k_wseg_rhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, b1, x.cta2,
-                                                                acc ? x.small : nullptr);
+                allow_smem(k_grhs<RCP>, shm);
+                k_grhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, u32(d.wseg_segs.n), rows, R, j0, Rc,
+                                                            b1, x.cta2, acc ? x.small : nullptr);
             });
             d.launches++;
         }

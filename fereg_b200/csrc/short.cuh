@@ -109,7 +109,6 @@ __device__ __forceinline__ SegStage seg_stage_at(unsigned char* p) {
 __host__ __device__ constexpr size_t wseg_bytes(int Rc, size_t tsz) {
     return al16(WT * Rc * tsz) + al16(WSEG * 32 * tsz) + segstage_bytes();
 }
-__host__ __device__ constexpr size_t wrhs_bytes(int Rc) { return wseg_bytes(Rc, 8); }
 __host__ __device__ constexpr size_t wresid_bytes(int Rc) { return wseg_bytes(Rc, 8) + al16(WSEG * Rc * 8); }
 
 // Stages the tile's per-segment scalars and the cells' weights, first `ncode` block coordinates
@@ -232,77 +231,7 @@ __device__ __forceinline__ void small_phase(const DevStruct& S, const SegStage& 
 }
 
 // ---------------------------------------------------------------------------------------------
-// Operator pass 1 (operator.rs:894-948) on short segments: t_s = sum_c W_c u_c / n1_s with
-// u_c = sum_b P[coord_b(c)]; small coordinates: sum of W_c (u_c - t_s) per small code.
-template <class T, int RCP, int NBK>
-__global__ void __launch_bounds__(WPB * 32, 4) k_wseg_apply(DevStruct S, DevWeights W, WarpTiles wt,
-                                                            const T* __restrict__ P, int R, int j0, int Rc,
-                                                            T* __restrict__ t, T* __restrict__ cta_small) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    using L_t = Lanes<RCP>;
-    constexpr int G = L_t::G;
-    unsigned char* mine = smem_raw + size_t(wid_in_cta()) * wseg_bytes(Rc, sizeof(T));
-    T* u = reinterpret_cast<T*>(mine);
-    T* ps = reinterpret_cast<T*>(mine + al16(WT * Rc * sizeof(T)));
-    const SegStage st = seg_stage_at(mine + al16(WT * Rc * sizeof(T)) + al16(WSEG * 32 * sizeof(T)));
-    T* wacc_all = reinterpret_cast<T*>(smem_raw + WPB * wseg_bytes(Rc, sizeof(T)));
-    T* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 32;
-    const bool acc = cta_small != nullptr;
-    const L_t L(Rc);
-    const u32 Ru = u32(R);
-    if (acc)
-        for (u32 i = L.lane; i < S.ms_acc * 32; i += 32) wacc[i] = T(0);
-    const T* Pj = P + j0 + L.j;
-    const u32 ncode = NBK < WNB ? u32(NBK) : u32(WNB);
-    const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
-    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
-    for (u32 tile = wid; tile < wt.n; tile += nw) {
-        const u32 s0 = tb.x, ns = tb.y - tb.x, c0 = tb.z, nc = tb.w - tb.z;
-        stage_cells(S, W, s0, tb.y, c0, tb.w, st, ncode, false);
-        if (tile + nw < wt.n) tb = wt.t[tile + nw];
-        __syncwarp();
-        stage_maps(nc, st, false);
-        __syncwarp();
-        if (L.on) {
-            SegRun<T> sr;
-            const u32* cg = st.code + L.g;
-#pragma unroll
-            for (int k0 = 0; k0 < L_t::KN; k0 += L_t::CH) {
-                T v[L_t::CH];
-#pragma unroll
-                for (int k = 0; k < L_t::CH; k++) {
-                    const u32 i = L.g + u32((k0 + k) * G);
-                    v[k] = i < nc ? gather_cell<NBK>(S, cg + (k0 + k) * G, Pj, Ru, c0 + i) : T(0);
-                }
-#pragma unroll
-                for (int k = 0; k < L_t::CH; k++) {
-                    const u32 i = L.g + u32((k0 + k) * G);
-                    if (i < nc) {
-                        const T w = T(st.cw[i]) * v[k];
-                        if (acc) u[i * Rc + L.j] = w;
-                        sr.add(st.segl[i], w, ps, L.lane);
-                    }
-                }
-            }
-            sr.finish(ns, ps, L.lane);
-        }
-        __syncwarp();
-        if (L.on)
-            for (u32 sl = L.g; sl < ns; sl += G) {
-                const T tv = seg_total<RCP>(ps, sl, L.j) * T(st.n1i[sl]);
-                t[size_t(s0 + sl) * Ru + j0 + L.j] = tv;
-                ps[sl * 32 + L.j] = tv;
-            }
-        if (acc) {
-            __syncwarp();
-            small_phase(S, st, L, nc, Rc, u, ps, wacc);
-        }
-        __syncwarp();
-    }
-    if (acc) flush_wacc<RCP>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
-}
-
-// Operator pass 1 on the short segments, one segment per group of RCP lanes (lane = column):
+// Operator pass 1 (operator.rs:894-948) on the short segments, one segment per group of RCP lanes (lane = column):
 // t_s = n1inv_s sum_c W_c u_c with u_c = sum_b P[coord_b(c)], and the small coordinates take
 // sum_c W_c u_c - t_s sum_c W_c per small code in the lane's private slots. segs lists the short
 // segments in order; group q of the grid takes segs[q], segs[q + groups], ... so every lane's
@@ -496,104 +425,129 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_apply(DevStruct S, DevWei
 }
 
 // ---------------------------------------------------------------------------------------------
-// Right-hand side pass 1 (operator.rs:969-1066) on short segments: s_c = sum over the rows of c of
-// w v, b1_s = sum_c s_c; per-CTA partials of [sum w v^2, sum w v] (cta_part[blockIdx][2R], this
-// chunk's columns); small coordinates' sums of s_c - W_c b1_s / n1_s into cta_small.
+// Right-hand side pass 1 (operator.rs:969-1066) on the short segments, one segment per group of
+// RCP lanes (lane = column), in the order of k_gseg_apply: b1_s = sum over the segment's rows of
+// w v; per-CTA partials of [sum w v^2, sum w v] (cta_part[blockIdx][2R], this chunk's columns);
+// the small coordinates take sum_c s_c - (b1_s / n1_s) sum_c W_c per small code (s_c: the sum over
+// the rows of cell c). The group streams its segment's rows (contiguous in the block): with one
+// row per cell, in chunks of RCP rows whose codes and weights lane i loads for row i, eight rows'
+// loads in flight; otherwise cell by cell over the cell's rows.
 template <int RCP>
-__global__ void __launch_bounds__(WPB * 32, 4) k_wseg_rhs(DevStruct S, DevWeights W, WarpTiles wt,
-                                                          const double* __restrict__ rows, int R, int j0, int Rc,
-                                                          double* __restrict__ b1, double* __restrict__ cta_part,
-                                                          double* __restrict__ cta_small) {
+__global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W, const u32* __restrict__ segs,
+                                                      u32 nsegs, const double* __restrict__ rows, int R, int j0,
+                                                      int Rc, double* __restrict__ b1, double* __restrict__ cta_part,
+                                                      double* __restrict__ cta_small) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using L_t = Lanes<RCP>;
-    constexpr int G = L_t::G;
-    unsigned char* mine = smem_raw + size_t(wid_in_cta()) * wrhs_bytes(Rc);
-    double* u = reinterpret_cast<double*>(mine);
-    double* ps = reinterpret_cast<double*>(mine + al16(WT * Rc * 8));
-    const SegStage st = seg_stage_at(mine + al16(WT * Rc * 8) + al16(WSEG * 32 * 8));
-    double* wacc_all = reinterpret_cast<double*>(smem_raw + WPB * wrhs_bytes(Rc));
+    constexpr int G = 32 / RCP;
+    constexpr int U = 8;  // rows whose loads are in flight together
+    double* wacc_all = reinterpret_cast<double*>(smem_raw);
     double* colsum = wacc_all + size_t(WPB) * S.ms_acc * 32;  // WPB x 2 x 32
     double* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 32;
     const bool acc = cta_small != nullptr;
     const bool trivial = S.cell_row == nullptr;
-    const L_t L(Rc);
-    const u32 Ru = u32(R);
+    const u32 lane = wlane(), g = lane / RCP, j = lane % RCP;
+    const bool on = int(j) < Rc;
+    const unsigned gmask = RCP == 32 ? FULL : ((1u << RCP) - 1u) << (g * RCP);
+    const size_t Ru = size_t(R);
+    const u32 ns_acc = acc ? S.ns_acc : 0u;
     if (acc)
-        for (u32 i = L.lane; i < S.ms_acc * 32; i += 32) wacc[i] = 0.0;
-    double q = 0.0, ws = 0.0;  // this lane's [sum w v^2, sum w v]
-    const double* vj = rows + j0 + L.j;
-    const u32 ncode = acc ? S.ns_acc : 0u;
-    const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
-    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
-    for (u32 tile = wid; tile < wt.n; tile += nw) {
-        const u32 s0 = tb.x, ns = tb.y - tb.x, c0 = tb.z, nc = tb.w - tb.z;
-        stage_cells(S, W, s0, tb.y, c0, tb.w, st, ncode, true);
-        if (tile + nw < wt.n) tb = wt.t[tile + nw];
-        __syncwarp();
-        stage_maps(nc, st, false);
-        __syncwarp();
-        if (L.on) {
-            SegRun<double> sr;
-            if (trivial) {  // one row per cell: row = cell
+        for (u32 i = lane; i < S.ms_acc * 32; i += 32) wacc[i] = 0.0;
+    double q2 = 0.0, ws = 0.0;  // this lane's [sum w v^2, sum w v]
+    const double* vj = rows + j0 + j;
+    const u32 groups = gridDim.x * WPB * G;
+    u32 q = (blockIdx.x * WPB + wid_in_cta()) * G + g;
+    u32 s = q < nsegs ? segs[q] : 0;
+    for (; q < nsegs; q += groups) {
+        const u32 c0 = S.seg_off[s], c1 = S.seg_off[s + 1];
+        const u32 qn = q + groups;
+        const u32 sn = qn < nsegs ? segs[qn] : 0;
+        double sum = 0.0;
+        for (u32 cb = c0; cb < c1; cb += RCP) {
+            const u32 nc = min(c1 - cb, u32(RCP));
+            u32 code[WNB];
 #pragma unroll
-                for (int k0 = 0; k0 < L_t::KN; k0 += L_t::CH) {
-                    double x[L_t::CH], w[L_t::CH];
+            for (int b = 0; b < WNB; b++)
+                code[b] = (b < int(ns_acc) && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
+            if (trivial) {
+                const double wl = (W.w_rows && j < nc) ? W.w_rows[cb + j] : 1.0;
+                for (u32 i0 = 0; i0 < nc; i0 += U) {
+                    double x[U];
 #pragma unroll
-                    for (int k = 0; k < L_t::CH; k++) {
-                        const u32 i = L.g + u32((k0 + k) * G);
-                        x[k] = i < nc ? __ldcs(vj + size_t(c0 + i) * Ru) : 0.0;
-                        w[k] = i < nc && W.w_rows ? W.w_rows[c0 + i] : 1.0;
+                    for (int k = 0; k < U; k++) {
+                        const u32 i = i0 + u32(k);
+                        x[k] = (on && i < nc) ? __ldcs(vj + size_t(cb + i) * Ru) : 0.0;
                     }
 #pragma unroll
-                    for (int k = 0; k < L_t::CH; k++) {
-                        const u32 i = L.g + u32((k0 + k) * G);
-                        if (i < nc) {
-                            const double wx = w[k] * x[k];
-                            q += wx * x[k];
-                            if (acc) u[i * Rc + L.j] = wx;
-                            sr.add(st.segl[i], wx, ps, L.lane);
+                    for (int k = 0; k < U; k++) {
+                        const u32 i = i0 + u32(k);
+                        const double w = W.w_rows ? __shfl_sync(gmask, wl, int(i), RCP) : 1.0;
+                        const double wx = w * x[k];
+                        q2 += wx * x[k];
+                        sum += wx;
+#pragma unroll
+                        for (int b = 0; b < WNB; b++) {
+                            const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
+                            if (on && i < nc && b < int(ns_acc)) wacc[cd * 32 + lane] += wx;
                         }
                     }
                 }
             } else {
-                for (u32 i = L.g; i < nc; i += G) {
+                const u32 rb = j < nc ? S.cell_row[cb + j] : 0u;  // lane i: first row of cell i
+                const u32 rend = S.cell_row[cb + nc];                // end of the chunk's last cell
+                for (u32 i = 0; i < nc; i++) {
+                    const u32 r0 = __shfl_sync(gmask, rb, int(i), RCP);
+                    const u32 rn = __shfl_sync(gmask, rb, int(i) + 1, RCP);
+                    const u32 r1 = i + 1 < nc ? rn : rend;
                     double sc = 0.0;
-                    for (u32 r = st.row0[i]; r < st.row0[i + 1]; r++) {
-                        const double x = __ldcs(vj + size_t(r) * Ru);
-                        const double wx = W.w_rows ? W.w_rows[r] * x : x;
-                        sc += wx;
-                        q += wx * x;
+                    if (on)
+                        for (u32 r = r0; r < r1; r++) {
+                            const double xv = __ldcs(vj + size_t(r) * Ru);
+                            const double wx = W.w_rows ? W.w_rows[r] * xv : xv;
+                            sc += wx;
+                            q2 += wx * xv;
+                        }
+                    sum += sc;
+#pragma unroll
+                    for (int b = 0; b < WNB; b++) {
+                        const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
+                        if (on && b < int(ns_acc)) wacc[cd * 32 + lane] += sc;
                     }
-                    if (acc) u[i * Rc + L.j] = sc;
-                    sr.add(st.segl[i], sc, ps, L.lane);
                 }
             }
-            sr.finish(ns, ps, L.lane);
         }
-        __syncwarp();
-        if (L.on)
-            for (u32 sl = L.g; sl < ns; sl += G) {
-                const double b = seg_total<RCP>(ps, sl, L.j);
-                ws += b;
-                b1[size_t(s0 + sl) * Ru + j0 + L.j] = b;
-                ps[sl * 32 + L.j] = b * st.n1i[sl];
-            }
+        ws += sum;
+        if (on) b1[size_t(s) * Ru + j0 + j] = sum;
         if (acc) {
-            __syncwarp();
-            small_phase(S, st, L, nc, Rc, u, ps, wacc);
+            const double tv = sum * W.n1inv[s];
+            for (u32 cb = c0; cb < c1; cb += RCP) {
+                const u32 nc = min(c1 - cb, u32(RCP));
+                u32 code[WNB];
+#pragma unroll
+                for (int b = 0; b < WNB; b++)
+                    code[b] = (b < int(ns_acc) && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
+                const double wl = j < nc ? cellw(W, cb + j) : 1.0;
+                for (u32 i = 0; i < nc; i++) {
+                    const double w = __shfl_sync(gmask, wl, int(i), RCP);
+#pragma unroll
+                    for (int b = 0; b < WNB; b++) {
+                        const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
+                        if (on && b < int(ns_acc)) wacc[cd * 32 + lane] -= w * tv;
+                    }
+                }
+            }
         }
-        __syncwarp();
+        s = sn;
     }
-    colsum[(size_t(wid_in_cta()) * 2) * 32 + L.lane] = L.on ? q : 0.0;
-    colsum[(size_t(wid_in_cta()) * 2 + 1) * 32 + L.lane] = L.on ? ws : 0.0;
+    colsum[(size_t(wid_in_cta()) * 2) * 32 + lane] = on ? q2 : 0.0;
+    colsum[(size_t(wid_in_cta()) * 2 + 1) * 32 + lane] = on ? ws : 0.0;
     __syncthreads();
     for (u32 i = threadIdx.x; i < 2 * u32(Rc); i += blockDim.x) {
-        const u32 half = i / u32(Rc), j = i % u32(Rc);
-        double s = 0.0;
+        const u32 half = i / u32(Rc), jj = i % u32(Rc);
+        double a = 0.0;
         for (int w = 0; w < WPB; w++)
 #pragma unroll
-            for (int g = 0; g < G; g++) s += colsum[(size_t(w) * 2 + half) * 32 + g * RCP + j];
-        cta_part[size_t(blockIdx.x) * 2 * R + half * R + j0 + j] = s;
+            for (int gg = 0; gg < G; gg++) a += colsum[(size_t(w) * 2 + half) * 32 + gg * RCP + jj];
+        cta_part[size_t(blockIdx.x) * 2 * R + half * R + j0 + jj] = a;
     }
     if (acc) flush_wacc<RCP>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
 }
