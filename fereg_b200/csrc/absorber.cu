@@ -79,7 +79,7 @@ struct DevWarpTiles {
 
 // Dynamic shared memory of the warp-tile kernels for a chunk of Rc columns (per-warp parts, then
 // the lane-private small-coordinate slots and column partials).
-inline size_t grhs_smem(u32 ms_acc) { return WPB * (size_t(ms_acc) * 32 * 8 + 2 * 32 * 8); }
+inline size_t grhs_smem(u32 ms_acc) { return WPB * (size_t(ms_acc) * 64 * 8 + 4 * 32 * 8); }
 inline size_t wresid_smem(int Rc) { return WPB * wresid_bytes(Rc); }
 inline size_t wpull_smem() { return WPB * pull_bytes(); }
 
@@ -94,6 +94,17 @@ void with_nbk(u32 nb, F&& f) {
         case 2: f(integral_constant<int, RCP>{}, integral_constant<int, 2>{}); break;
         case 3: f(integral_constant<int, RCP>{}, integral_constant<int, 3>{}); break;
         default: f(integral_constant<int, RCP>{}, integral_constant<int, WNB>{}); break;
+    }
+}
+// Lane groups of L = lanes_of(Rc) lanes, two columns per lane.
+template <int MIN_NBK = 0, class F>
+void with_lanes(int Rc, u32 nb, F&& f) {
+    switch (lanes_of(Rc)) {
+        case 1: with_nbk<1, MIN_NBK>(nb, f); break;
+        case 2: with_nbk<2, MIN_NBK>(nb, f); break;
+        case 4: with_nbk<4, MIN_NBK>(nb, f); break;
+        case 8: with_nbk<8, MIN_NBK>(nb, f); break;
+        default: with_nbk<16, MIN_NBK>(nb, f); break;
     }
 }
 template <int MIN_NBK = 0, class F>
@@ -859,9 +870,9 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
     if (d.wseg.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = size_t(WPB) * S.ms_acc * 32 * sizeof(T);
+            const size_t shm = size_t(WPB) * S.ms_acc * 64 * sizeof(T);
             const u32 nsegs = u32(d.wseg_segs.n);
-            with_rcp<1>(Rc, S.nb, [&](auto c, auto nbk) {
+            with_lanes<1>(Rc, S.nb, [&](auto c, auto nbk) {
                 constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
                 allow_smem(k_gseg_apply<T, RCP, NBK>, shm);
                 k_gseg_apply<T, RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, nsegs, P, R, j0, Rc,
@@ -986,7 +997,7 @@ void launch_rhs(Scratch& d, const DevStruct& S, const DevWeights& W, const doubl
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
             const size_t shm = grhs_smem(S.ms_acc);
-            with_rcp<WNB>(Rc, WNB, [&](auto c, auto) {
+            with_lanes<WNB>(Rc, WNB, [&](auto c, auto) {
                 constexpr int RCP = decltype(c)::value;
                 allow_smem(k_grhs<RCP>, shm);
                 k_grhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, u32(d.wseg_segs.n), rows, R, j0, Rc,
@@ -1077,7 +1088,7 @@ void launch_rhs_scratch(Scratch& d, const DevStruct& S, const DevWeights& W, con
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
             const size_t shm = grhs_smem(S.ms_acc);
-            with_rcp<WNB>(Rc, WNB, [&](auto c, auto) {
+            with_lanes<WNB>(Rc, WNB, [&](auto c, auto) {
                 constexpr int RCP = decltype(c)::value;
                 allow_smem(k_grhs<RCP>, shm);
                 k_grhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, u32(d.wseg_segs.n), rows, R, j0, Rc,

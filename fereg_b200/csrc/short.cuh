@@ -231,37 +231,58 @@ __device__ __forceinline__ void small_phase(const DevStruct& S, const SegStage& 
 }
 
 // ---------------------------------------------------------------------------------------------
-// Operator pass 1 (operator.rs:894-948) on the short segments, one segment per group of RCP lanes (lane = column):
+// Lane groups over the short segments: a group of L lanes takes one segment at a time, lane j of
+// the group holding columns j and j + L of the launch's column chunk (L = lanes_of(Rc): two
+// columns per lane, so 32 / L cells share every warp instruction). The small coordinates' sums
+// sit in lane-private shared slots, two per small code: slot(k, c) = (2k + c) * 32 + lane.
+__host__ __device__ constexpr int lanes_of(int Rc) { return rcp_of((Rc + 1) / 2); }
+
+// CTA end of the lane-group kernels: adds the lane-private small-coordinate slots of the warps and
+// groups, in that order, into the CTA's partial row (cta_small[blockIdx][k * R + j0 + col]).
+template <int L, class T>
+__device__ __forceinline__ void flush_pairs(const T* wacc_all, u32 ms_acc, int Rc, int j0, int R, T* cta_small) {
+    __syncthreads();
+    T* mine = cta_small + size_t(blockIdx.x) * ms_acc * R;
+    for (u32 i = threadIdx.x; i < ms_acc * u32(Rc); i += blockDim.x) {
+        const u32 k = i / u32(Rc), col = i % u32(Rc), c = col / u32(L), j = col % u32(L);
+        T s = T(0);
+        for (int w = 0; w < WPB; w++)
+#pragma unroll
+            for (int g = 0; g < 32 / L; g++) s += wacc_all[((size_t(w) * ms_acc + k) * 2 + c) * 32 + g * L + j];
+        mine[size_t(k) * R + j0 + col] = s;
+    }
+}
+
+// Operator pass 1 (operator.rs:894-948) on the short segments, one segment per lane group:
 // t_s = n1inv_s sum_c W_c u_c with u_c = sum_b P[coord_b(c)], and the small coordinates take
-// sum_c W_c u_c - t_s sum_c W_c per small code in the lane's private slots. segs lists the short
-// segments in order; group q of the grid takes segs[q], segs[q + groups], ... so every lane's
-// sums have a fixed order.
+// sum_c W_c u_c - t_s sum_c W_c per small code. segs lists the short segments in order; group q
+// of the grid takes segs[q], segs[q + groups], ... so every lane's sums have a fixed order.
 //
-// The group walks its segment in chunks of RCP cells: lane i of the group loads the block codes
+// The group walks its segment in chunks of L cells: lane i of the group loads the block codes
 // and the weight of the chunk's cell i (one coalesced load per block), and the cells are then
 // taken in turn with the codes broadcast by shuffles, four cells' gathers in flight together.
 // The small codes are the first blocks' codes, already at hand. The second walk (t_s times the
-// weights) reloads the chunk's codes, which the first left in L1. The next segment's index is
-// fetched while the current one runs. The groups of a warp never wait on one another.
-template <class T, int RCP, int NBK>
+// weights) reloads the chunk's small codes, which the first left in L1. The next segment's index
+// is fetched while the current one runs. The groups of a warp never wait on one another.
+template <class T, int L, int NBK>
 __global__ void __launch_bounds__(WPB * 32, 4) k_gseg_apply(DevStruct S, DevWeights W, const u32* __restrict__ segs,
                                                             u32 nsegs, const T* __restrict__ P, int R, int j0, int Rc,
                                                             T* __restrict__ t, T* __restrict__ cta_small) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int G = 32 / RCP;
+    constexpr int G = 32 / L;
     constexpr int NL = NBK < WNB ? NBK : WNB;  // blocks whose codes the lanes hold
     constexpr int U = 4;                       // cells whose gathers are in flight together
     T* wacc_all = reinterpret_cast<T*>(smem_raw);
-    T* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 32;
     const bool acc = cta_small != nullptr;
     const bool weighted = W.cell_w != nullptr;
-    const u32 lane = wlane(), g = lane / RCP, j = lane % RCP;
-    const bool on = int(j) < Rc;
-    const unsigned gmask = RCP == 32 ? FULL : ((1u << RCP) - 1u) << (g * RCP);
+    const u32 lane = wlane(), g = lane / L, j = lane % L;
+    const bool on0 = int(j) < Rc, on1 = int(j) + L < Rc;
+    const unsigned gmask = L == 32 ? FULL : ((1u << L) - 1u) << (g * L);
     const size_t Ru = size_t(R);
-    const u32 ns_acc = S.ns_acc;
+    const int ns_acc = acc ? int(S.ns_acc) : 0;
+    T* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 64 + lane;  // slot(k, c) at [(2k + c) * 32]
     if (acc)
-        for (u32 i = lane; i < S.ms_acc * 32; i += 32) wacc[i] = T(0);
+        for (u32 i = 0; i < S.ms_acc * 2; i++) wacc[i * 32] = T(0);
     const T* Pj = P + j0 + j;
     const u32 groups = gridDim.x * WPB * G;
     u32 q = (blockIdx.x * WPB + wid_in_cta()) * G + g;
@@ -270,71 +291,89 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_gseg_apply(DevStruct S, DevWeig
         const u32 c0 = S.seg_off[s], c1 = S.seg_off[s + 1];
         const u32 qn = q + groups;
         const u32 sn = qn < nsegs ? segs[qn] : 0;
-        T sum = T(0);
-        for (u32 cb = c0; cb < c1; cb += RCP) {
-            const u32 nc = min(c1 - cb, u32(RCP));
+        T sum0 = T(0), sum1 = T(0);
+        for (u32 cb = c0; cb < c1; cb += L) {
+            const u32 nc = min(c1 - cb, u32(L));
             u32 code[NL];
             double wl = 1.0;
 #pragma unroll
             for (int b = 0; b < NL; b++) code[b] = j < nc ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
             if (weighted && j < nc) wl = W.cell_w[cb + j];
             for (u32 i0 = 0; i0 < nc; i0 += U) {
-                T v[U];
+                T x0[U], x1[U];
                 u32 k0[U];
 #pragma unroll
                 for (int k = 0; k < U; k++) {
                     const u32 i = i0 + u32(k);
-                    T x = T(0);
+                    const bool live = i < nc;
+                    T a0 = T(0), a1 = T(0);
 #pragma unroll
                     for (int b = 0; b < NL; b++) {
-                        const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
+                        const u32 cd = __shfl_sync(gmask, code[b], int(i), L);
                         if (b == 0) k0[k] = cd;
-                        if (on && i < nc) x += Pj[size_t(cd) * Ru];
+                        const T* row = Pj + size_t(cd) * Ru;
+                        if (live && on0) a0 += row[0];
+                        if (live && on1) a1 += row[L];
                     }
                     if constexpr (NBK == WNB)
-                        if (on && i < nc)
-                            for (u32 b = WNB; b < S.nb; b++)
-                                x += Pj[size_t(__ldg(S.coord + size_t(b) * S.M + cb + i)) * Ru];
-                    v[k] = x;
+                        if (live)
+                            for (u32 b = WNB; b < S.nb; b++) {
+                                const T* row = Pj + size_t(__ldg(S.coord + size_t(b) * S.M + cb + i)) * Ru;
+                                if (on0) a0 += row[0];
+                                if (on1) a1 += row[L];
+                            }
+                    x0[k] = a0;
+                    x1[k] = a1;
                 }
 #pragma unroll
                 for (int k = 0; k < U; k++) {
                     const u32 i = i0 + u32(k);
-                    const T w = weighted ? T(__shfl_sync(gmask, wl, int(i), RCP)) : T(1);
+                    const T w = weighted ? T(__shfl_sync(gmask, wl, int(i), L)) : T(1);
                     if (i < nc) {
-                        const T wv = w * v[k];
-                        sum += wv;
-                        if (acc && on) {
-                            wacc[k0[k] * 32 + lane] += wv;
-                            for (u32 b = 1; b < ns_acc; b++)
-                                wacc[__ldg(S.coord + size_t(b) * S.M + cb + i) * 32 + lane] += wv;
+                        const T v0 = w * x0[k], v1 = w * x1[k];
+                        sum0 += v0;
+                        sum1 += v1;
+                        if (acc) {
+                            T* sl = wacc + k0[k] * 64;
+                            sl[0] += v0;
+                            sl[32] += v1;
+                            for (int b = 1; b < ns_acc; b++) {
+                                T* sb = wacc + __ldg(S.coord + size_t(b) * S.M + cb + i) * 64;
+                                sb[0] += v0;
+                                sb[32] += v1;
+                            }
                         }
                     }
                 }
             }
         }
-        const T tv = sum * T(W.n1inv[s]);
-        if (on) t[size_t(s) * Ru + j0 + j] = tv;
+        const T n1i = T(W.n1inv[s]);
+        const T tv0 = sum0 * n1i, tv1 = sum1 * n1i;
+        if (on0) t[size_t(s) * Ru + j0 + j] = tv0;
+        if (on1) t[size_t(s) * Ru + j0 + j + L] = tv1;
         if (acc)
-            for (u32 cb = c0; cb < c1; cb += RCP) {
-                const u32 nc = min(c1 - cb, u32(RCP));
-                u32 code[NL];
+            for (u32 cb = c0; cb < c1; cb += L) {
+                const u32 nc = min(c1 - cb, u32(L));
+                u32 code[WNB];
 #pragma unroll
-                for (int b = 0; b < NL; b++)
-                    code[b] = (b < int(ns_acc) && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
+                for (int b = 0; b < WNB; b++)
+                    code[b] = (b < ns_acc && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
                 const double wl = (weighted && j < nc) ? W.cell_w[cb + j] : 1.0;
                 for (u32 i = 0; i < nc; i++) {
-                    const T w = weighted ? T(__shfl_sync(gmask, wl, int(i), RCP)) : T(1);
+                    const T w = weighted ? T(__shfl_sync(gmask, wl, int(i), L)) : T(1);
+                    const T d0 = w * tv0, d1 = w * tv1;
 #pragma unroll
-                    for (int b = 0; b < NL; b++) {
-                        const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
-                        if (on && b < int(ns_acc)) wacc[cd * 32 + lane] -= w * tv;
-                    }
+                    for (int b = 0; b < WNB; b++)
+                        if (b < ns_acc) {
+                            T* sl = wacc + __shfl_sync(gmask, code[b], int(i), L) * 64;
+                            sl[0] -= d0;
+                            sl[32] -= d1;
+                        }
                 }
             }
         s = sn;
     }
-    if (acc) flush_wacc<RCP>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
+    if (acc) flush_pairs<L>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
 }
 
 // Staging of a coordinate-list tile: list ends and the entries' indices.
@@ -425,34 +464,34 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_apply(DevStruct S, DevWei
 }
 
 // ---------------------------------------------------------------------------------------------
-// Right-hand side pass 1 (operator.rs:969-1066) on the short segments, one segment per group of
-// RCP lanes (lane = column), in the order of k_gseg_apply: b1_s = sum over the segment's rows of
-// w v; per-CTA partials of [sum w v^2, sum w v] (cta_part[blockIdx][2R], this chunk's columns);
-// the small coordinates take sum_c s_c - (b1_s / n1_s) sum_c W_c per small code (s_c: the sum over
-// the rows of cell c). The group streams its segment's rows (contiguous in the block): with one
-// row per cell, in chunks of RCP rows whose codes and weights lane i loads for row i, eight rows'
-// loads in flight; otherwise cell by cell over the cell's rows.
-template <int RCP>
+// Right-hand side pass 1 (operator.rs:969-1066) on the short segments, one segment per lane group
+// in the order of k_gseg_apply: b1_s = sum over the segment's rows of w v; per-CTA partials of
+// [sum w v^2, sum w v] (cta_part[blockIdx][2R], this chunk's columns); the small coordinates take
+// sum_c s_c - (b1_s / n1_s) sum_c W_c per small code (s_c: the sum over the rows of cell c). The
+// group streams its segment's rows (contiguous in the block): with one row per cell, in chunks of
+// L rows whose small codes and weights lane i loads for row i, four rows' loads in flight;
+// otherwise cell by cell over the cell's rows.
+template <int L>
 __global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W, const u32* __restrict__ segs,
                                                       u32 nsegs, const double* __restrict__ rows, int R, int j0,
                                                       int Rc, double* __restrict__ b1, double* __restrict__ cta_part,
                                                       double* __restrict__ cta_small) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int G = 32 / RCP;
-    constexpr int U = 8;  // rows whose loads are in flight together
+    constexpr int G = 32 / L;
+    constexpr int U = 4;  // rows whose loads are in flight together (two columns each)
     double* wacc_all = reinterpret_cast<double*>(smem_raw);
-    double* colsum = wacc_all + size_t(WPB) * S.ms_acc * 32;  // WPB x 2 x 32
-    double* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 32;
+    double* colsum = wacc_all + size_t(WPB) * S.ms_acc * 64;  // WPB x 4 x 32: [q c0, q c1, ws c0, ws c1]
     const bool acc = cta_small != nullptr;
     const bool trivial = S.cell_row == nullptr;
-    const u32 lane = wlane(), g = lane / RCP, j = lane % RCP;
-    const bool on = int(j) < Rc;
-    const unsigned gmask = RCP == 32 ? FULL : ((1u << RCP) - 1u) << (g * RCP);
+    const u32 lane = wlane(), g = lane / L, j = lane % L;
+    const bool on0 = int(j) < Rc, on1 = int(j) + L < Rc;
+    const unsigned gmask = L == 32 ? FULL : ((1u << L) - 1u) << (g * L);
     const size_t Ru = size_t(R);
-    const u32 ns_acc = acc ? S.ns_acc : 0u;
+    const int ns_acc = acc ? int(S.ns_acc) : 0;
+    double* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 64 + lane;
     if (acc)
-        for (u32 i = lane; i < S.ms_acc * 32; i += 32) wacc[i] = 0.0;
-    double q2 = 0.0, ws = 0.0;  // this lane's [sum w v^2, sum w v]
+        for (u32 i = 0; i < S.ms_acc * 2; i++) wacc[i * 32] = 0.0;
+    double qa = 0.0, qb = 0.0, wa = 0.0, wb = 0.0;  // this lane's [sum w v^2, sum w v], both columns
     const double* vj = rows + j0 + j;
     const u32 groups = gridDim.x * WPB * G;
     u32 q = (blockIdx.x * WPB + wid_in_cta()) * G + g;
@@ -461,95 +500,118 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W,
         const u32 c0 = S.seg_off[s], c1 = S.seg_off[s + 1];
         const u32 qn = q + groups;
         const u32 sn = qn < nsegs ? segs[qn] : 0;
-        double sum = 0.0;
-        for (u32 cb = c0; cb < c1; cb += RCP) {
-            const u32 nc = min(c1 - cb, u32(RCP));
+        double sum0 = 0.0, sum1 = 0.0;
+        for (u32 cb = c0; cb < c1; cb += L) {
+            const u32 nc = min(c1 - cb, u32(L));
             u32 code[WNB];
 #pragma unroll
             for (int b = 0; b < WNB; b++)
-                code[b] = (b < int(ns_acc) && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
+                code[b] = (b < ns_acc && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
             if (trivial) {
                 const double wl = (W.w_rows && j < nc) ? W.w_rows[cb + j] : 1.0;
                 for (u32 i0 = 0; i0 < nc; i0 += U) {
-                    double x[U];
+                    double x0[U], x1[U];
 #pragma unroll
                     for (int k = 0; k < U; k++) {
                         const u32 i = i0 + u32(k);
-                        x[k] = (on && i < nc) ? __ldcs(vj + size_t(cb + i) * Ru) : 0.0;
+                        const double* row = vj + size_t(cb + i) * Ru;
+                        x0[k] = (on0 && i < nc) ? __ldcs(row) : 0.0;
+                        x1[k] = (on1 && i < nc) ? __ldcs(row + L) : 0.0;
                     }
 #pragma unroll
                     for (int k = 0; k < U; k++) {
                         const u32 i = i0 + u32(k);
-                        const double w = W.w_rows ? __shfl_sync(gmask, wl, int(i), RCP) : 1.0;
-                        const double wx = w * x[k];
-                        q2 += wx * x[k];
-                        sum += wx;
+                        const double w = W.w_rows ? __shfl_sync(gmask, wl, int(i), L) : 1.0;
+                        const double v0 = w * x0[k], v1 = w * x1[k];
+                        qa += v0 * x0[k];
+                        qb += v1 * x1[k];
+                        sum0 += v0;
+                        sum1 += v1;
 #pragma unroll
-                        for (int b = 0; b < WNB; b++) {
-                            const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
-                            if (on && i < nc && b < int(ns_acc)) wacc[cd * 32 + lane] += wx;
-                        }
+                        for (int b = 0; b < WNB; b++)
+                            if (b < ns_acc) {
+                                double* sl = wacc + __shfl_sync(gmask, code[b], int(i), L) * 64;
+                                if (i < nc) {
+                                    sl[0] += v0;
+                                    sl[32] += v1;
+                                }
+                            }
                     }
                 }
             } else {
                 const u32 rb = j < nc ? S.cell_row[cb + j] : 0u;  // lane i: first row of cell i
                 const u32 rend = S.cell_row[cb + nc];                // end of the chunk's last cell
                 for (u32 i = 0; i < nc; i++) {
-                    const u32 r0 = __shfl_sync(gmask, rb, int(i), RCP);
-                    const u32 rn = __shfl_sync(gmask, rb, int(i) + 1, RCP);
+                    const u32 r0 = __shfl_sync(gmask, rb, int(i), L);
+                    const u32 rn = __shfl_sync(gmask, rb, int(i) + 1, L);
                     const u32 r1 = i + 1 < nc ? rn : rend;
-                    double sc = 0.0;
-                    if (on)
-                        for (u32 r = r0; r < r1; r++) {
-                            const double xv = __ldcs(vj + size_t(r) * Ru);
-                            const double wx = W.w_rows ? W.w_rows[r] * xv : xv;
-                            sc += wx;
-                            q2 += wx * xv;
-                        }
-                    sum += sc;
-#pragma unroll
-                    for (int b = 0; b < WNB; b++) {
-                        const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
-                        if (on && b < int(ns_acc)) wacc[cd * 32 + lane] += sc;
+                    double s0 = 0.0, s1 = 0.0;
+                    for (u32 r = r0; r < r1; r++) {
+                        const double* row = vj + size_t(r) * Ru;
+                        const double a0 = on0 ? __ldcs(row) : 0.0, a1 = on1 ? __ldcs(row + L) : 0.0;
+                        const double w = W.w_rows ? W.w_rows[r] : 1.0;
+                        const double v0 = w * a0, v1 = w * a1;
+                        s0 += v0;
+                        s1 += v1;
+                        qa += v0 * a0;
+                        qb += v1 * a1;
                     }
+                    sum0 += s0;
+                    sum1 += s1;
+#pragma unroll
+                    for (int b = 0; b < WNB; b++)
+                        if (b < ns_acc) {
+                            double* sl = wacc + __shfl_sync(gmask, code[b], int(i), L) * 64;
+                            sl[0] += s0;
+                            sl[32] += s1;
+                        }
                 }
             }
         }
-        ws += sum;
-        if (on) b1[size_t(s) * Ru + j0 + j] = sum;
+        wa += sum0;
+        wb += sum1;
+        if (on0) b1[size_t(s) * Ru + j0 + j] = sum0;
+        if (on1) b1[size_t(s) * Ru + j0 + j + L] = sum1;
         if (acc) {
-            const double tv = sum * W.n1inv[s];
-            for (u32 cb = c0; cb < c1; cb += RCP) {
-                const u32 nc = min(c1 - cb, u32(RCP));
+            const double n1i = W.n1inv[s];
+            const double tv0 = sum0 * n1i, tv1 = sum1 * n1i;
+            for (u32 cb = c0; cb < c1; cb += L) {
+                const u32 nc = min(c1 - cb, u32(L));
                 u32 code[WNB];
 #pragma unroll
                 for (int b = 0; b < WNB; b++)
-                    code[b] = (b < int(ns_acc) && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
+                    code[b] = (b < ns_acc && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
                 const double wl = j < nc ? cellw(W, cb + j) : 1.0;
                 for (u32 i = 0; i < nc; i++) {
-                    const double w = __shfl_sync(gmask, wl, int(i), RCP);
+                    const double w = __shfl_sync(gmask, wl, int(i), L);
+                    const double d0 = w * tv0, d1 = w * tv1;
 #pragma unroll
-                    for (int b = 0; b < WNB; b++) {
-                        const u32 cd = __shfl_sync(gmask, code[b], int(i), RCP);
-                        if (on && b < int(ns_acc)) wacc[cd * 32 + lane] -= w * tv;
-                    }
+                    for (int b = 0; b < WNB; b++)
+                        if (b < ns_acc) {
+                            double* sl = wacc + __shfl_sync(gmask, code[b], int(i), L) * 64;
+                            sl[0] -= d0;
+                            sl[32] -= d1;
+                        }
                 }
             }
         }
         s = sn;
     }
-    colsum[(size_t(wid_in_cta()) * 2) * 32 + lane] = on ? q2 : 0.0;
-    colsum[(size_t(wid_in_cta()) * 2 + 1) * 32 + lane] = on ? ws : 0.0;
+    double* cs = colsum + size_t(wid_in_cta()) * 4 * 32 + lane;
+    cs[0] = on0 ? qa : 0.0;
+    cs[32] = on1 ? qb : 0.0;
+    cs[64] = on0 ? wa : 0.0;
+    cs[96] = on1 ? wb : 0.0;
     __syncthreads();
     for (u32 i = threadIdx.x; i < 2 * u32(Rc); i += blockDim.x) {
-        const u32 half = i / u32(Rc), jj = i % u32(Rc);
+        const u32 half = i / u32(Rc), col = i % u32(Rc), c = col / u32(L), jj = col % u32(L);
         double a = 0.0;
         for (int w = 0; w < WPB; w++)
 #pragma unroll
-            for (int gg = 0; gg < G; gg++) a += colsum[(size_t(w) * 2 + half) * 32 + gg * RCP + jj];
-        cta_part[size_t(blockIdx.x) * 2 * R + half * R + j0 + jj] = a;
+            for (int gg = 0; gg < G; gg++) a += colsum[(size_t(w) * 4 + half * 2 + c) * 32 + gg * L + jj];
+        cta_part[size_t(blockIdx.x) * 2 * R + half * R + j0 + col] = a;
     }
-    if (acc) flush_wacc<RCP>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
+    if (acc) flush_pairs<L>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
 }
 
 // Right-hand side pass 2 on short coordinate lists (k >= ms_acc): rhs[k] = sum over the cells c
