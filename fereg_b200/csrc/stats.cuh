@@ -491,14 +491,18 @@ __global__ void k_uf_init(u32* __restrict__ parent, u32 nv) {
 
 __device__ __forceinline__ u32 uf_find(u32* parent, u32 v) {
     // Path halving. Parents only decrease (a link sets parent[hi] = lo < hi; halving sets an
-    // ancestor), so the walk strictly descends and ends at a root. Reads bypass L1: parents
-    // change under concurrent links.
-    u32 p = __ldcg(parent + v);
+    // ancestor), so the walk strictly descends and ends at a vertex that was a root when its
+    // entry was read. The reads go through L1 and may be stale under concurrent links: a stale
+    // entry still names an ancestor, so two walks that end at the same vertex prove one
+    // component, and a link attempted on a vertex that is no longer a root fails its CAS (at L2)
+    // and retries from the parent the CAS returns. Caching keeps the root of a large component,
+    // which every walk ends at, out of a single hot L2 line.
+    u32 p = __ldca(parent + v);
     while (p != v) {
-        const u32 gp = __ldcg(parent + p);
+        const u32 gp = __ldca(parent + p);
         if (gp != p) parent[v] = gp;  // benign race: any ancestor is a valid parent
         v = p;
-        p = __ldcg(parent + v);
+        p = __ldca(parent + v);
     }
     return v;
 }
