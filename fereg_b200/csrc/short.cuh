@@ -1,24 +1,26 @@
-// Warp-tile kernels for the short lists: segments of at most WT cells (and WT rows) and
-// coordinate lists of at most PULL_WARP_MAX entries. Longer lists go to the CTA tiles
-// (tiles.cuh).
+// Kernels for the short lists: segments of at most WT cells (and WT rows) and coordinate lists
+// of at most PULL_WARP_MAX entries. Longer lists go to the CTA tiles (tiles.cuh).
 //
-// A warp takes one warp tile at a time: whole consecutive segments (at most WSEG segments, WT
-// cells and WT rows in all) or whole consecutive coordinate lists (at most PULL_WARP_MAX entries).
-// The tile's indices are staged first, one lane per cell, segment or entry, into the warp's
-// shared memory. Then every loop runs on all lanes as (group g, column j) pairs: a column chunk
-// of Rc columns is padded to RCP (a power of two, a template parameter), the warp holds
-// G = 32 / RCP groups, and cells and rows are dealt to the groups in turn (cell i to group
-// i mod G). Lanes of a group read consecutive columns of one row (coalesced); the per-cell loops
-// are unrolled with their loads batched in registers, so a tile's gathers are in flight together.
+// The operator's and the right-hand side's segment passes use lane groups: a group of L lanes
+// takes one segment at a time, lane j of the group holding columns j and j + L of the launch's
+// column chunk, so 32 / L segments share every warp instruction. The group loads the indices of
+// L cells at once, one per lane and coalesced, and takes the cells in turn with the indices
+// broadcast by shuffles, several cells' gathers in flight together.
 //
-// Segment sums: while a lane walks its cells (in order) it keeps a running sum of the current
-// segment and parks it in a lane-private slot when the segment ends; the segment's value is then
-// the sum of its G slots in group order. The small coordinates (when summed in the segment
-// passes) accumulate in lane-private slots as well; the CTA adds warps and groups in a fixed
-// order into its own partial row. All sums have a fixed order: results do not depend on timing.
+// The coordinate-list passes and the residualization use warp tiles: a warp takes whole
+// consecutive segments (at most WSEG segments, WT cells and WT rows in all) or whole consecutive
+// coordinate lists (at most PULL_WARP_MAX entries). The tile's indices are staged first, one lane
+// per cell, segment or entry, into the warp's shared memory. Then every loop runs on all lanes as
+// (group g, column j) pairs: a column chunk of Rc columns is padded to RCP (a power of two), the
+// warp holds G = 32 / RCP groups, and cells and rows are dealt to the groups in turn (cell i to
+// group i mod G). Segment sums: while a lane walks its cells (in order) it keeps a running sum of
+// the current segment and parks it in a lane-private slot when the segment ends; the segment's
+// value is then the sum of its G slots in group order.
 //
-// The number of blocks is a template parameter NBK (the exact count up to WNB - 1; WNB means
-// WNB or more, the ones past WNB read from global memory).
+// Every lane's sums run in a fixed order, and the small coordinates accumulate in lane-private
+// shared slots that the CTA adds in a fixed order: results do not depend on timing. The number of
+// blocks is a template parameter NBK (the exact count up to WNB - 1; WNB means WNB or more, the
+// ones past WNB read from global memory).
 #pragma once
 
 #include "tiles.cuh"
@@ -192,42 +194,6 @@ __device__ __forceinline__ T seg_total(const T* ps, u32 sl, u32 j) {
 #pragma unroll
     for (int g = 0; g < 32 / RCP; g++) s += ps[sl * 32 + g * RCP + j];
     return s;
-}
-
-// Lane-private small-coordinate slots: wacc[k * 32 + lane] for small code k.
-template <class T>
-__device__ __forceinline__ void small_add(const DevStruct& S, const SegStage& st, u32 i, T z, T* wacc, u32 lane) {
-    for (u32 b = 0; b < S.ns_acc; b++) wacc[st.code[b * WT + i] * 32 + lane] += z;
-}
-
-// CTA end: adds the lane-private small-coordinate slots (ms_acc x 32 per warp) of the warps and
-// groups, in that order, into the CTA's partial row (cta_small[blockIdx][k * R + j0 + j]).
-template <int RCP, class T>
-__device__ __forceinline__ void flush_wacc(const T* wacc_all, u32 ms_acc, int Rc, int j0, int R, T* cta_small) {
-    __syncthreads();
-    T* mine = cta_small + size_t(blockIdx.x) * ms_acc * R;
-    for (u32 i = threadIdx.x; i < ms_acc * u32(Rc); i += blockDim.x) {
-        const u32 k = i / u32(Rc), j = i % u32(Rc);
-        T s = T(0);
-        for (int w = 0; w < WPB; w++)
-#pragma unroll
-            for (int g = 0; g < 32 / RCP; g++) s += wacc_all[(size_t(w) * ms_acc + k) * 32 + g * RCP + j];
-        mine[size_t(k) * R + j0 + j] = s;
-    }
-}
-
-// Small-coordinate phase of a segment tile: every cell adds z_c = u_c - W_c sv_{s(c)} (sv: the
-// per-segment values parked in the group-0 slots of ps) to its small codes' slots.
-template <int RCP, class T>
-__device__ __forceinline__ void small_phase(const DevStruct& S, const SegStage& st, const Lanes<RCP>& L, u32 nc, int Rc,
-                                            const T* u, const T* ps, T* wacc) {
-    constexpr int G = Lanes<RCP>::G;
-    if (!L.on) return;
-#pragma unroll 4
-    for (int k = 0; k < Lanes<RCP>::KN; k++) {
-        const u32 i = L.g + u32(k * G);
-        if (i < nc) small_add(S, st, i, u[i * Rc + L.j] - T(st.cw[i]) * ps[st.segl[i] * 32 + L.j], wacc, L.lane);
-    }
 }
 
 // ---------------------------------------------------------------------------------------------
