@@ -368,7 +368,7 @@ std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, 
             case 3: k_outer_mma<3><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
             default: k_outer_mma<4><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
         }
-        k_sum_parts<<<(len + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
+        k_sum_parts<<<sum_parts_blocks(len), 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
         d.launches += 2;
         std::vector<double> h(len);
         CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
@@ -387,7 +387,7 @@ std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, 
         OpSpec s{src, nrows, srcR, d.col.p, shift ? d.shift.p : nullptr, k, cst ? 1 : 0, msz, om, perm, p0, np,
                  with_sq ? 1 : 0};
         k_outer<<<ST_GRID, ST_TB, 0, st>>>(s, d.part.p);
-        k_sum_parts<<<(len + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
+        k_sum_parts<<<sum_parts_blocks(len), 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
         d.launches += 2;
         std::vector<double> h(len);
         CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
@@ -444,7 +444,7 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
         }
         d.launches++;
     }
-    k_sum_parts<<<(R * 6 + 255) / 256, 256, 0, st>>>(d.part.p, ST_GRID, R * 6, d.sums.p);
+    k_sum_parts<<<sum_parts_blocks(R * 6), 256, 0, st>>>(d.part.p, ST_GRID, R * 6, d.sums.p);
     d.launches++;
     std::vector<double> s1(r * 6), c0(r);
     CK(cudaMemcpyAsync(s1.data(), d.sums.p, r * 6 * 8, cudaMemcpyDeviceToHost, st));

@@ -78,14 +78,20 @@ __global__ void __launch_bounds__(ST_TB) k_colstats(const double* __restrict__ r
     }
 }
 
-// Sum of `parts` rows of length len (fixed order), one thread per element.
+// Sum of `parts` rows of length len, one warp per element: lane l adds rows l, l + 32, ... in
+// order, then the lanes' sums are combined by a fixed butterfly (the same order every call).
 __global__ void k_sum_parts(const double* __restrict__ part, int parts, int len, double* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= len) return;
+    const int i = blockIdx.x * (blockDim.x / 32) + int(threadIdx.x / 32);
+    const int lane = int(threadIdx.x % 32);
+    if (i >= len) return;  // whole warps leave together
     double s = 0.0;
-    for (int p = 0; p < parts; p++) s += part[size_t(p) * len + i];
-    out[i] = s;
+    for (int p = lane; p < parts; p += 32) s += part[size_t(p) * len + i];
+#pragma unroll
+    for (int o = 16; o > 0; o /= 2) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[i] = s;
 }
+// Launch shape of k_sum_parts for len elements (8 warps per block).
+inline unsigned sum_parts_blocks(int len) { return unsigned((len + 7) / 8); }
 
 // Sum of the weights (sum w, and the count) over rows.
 __global__ void __launch_bounds__(ST_TB) k_sum_w(const double* __restrict__ w, size_t n, double* __restrict__ part) {
