@@ -38,6 +38,8 @@ constexpr size_t DENSE_SMALL_MAX = 1024;
 constexpr double REFINE_DROP = 1e-9;
 constexpr int REFINE_ROUNDS = 12;
 
+void dense_ldlt_inverse(double* a, double* d, int k, double* x, cudaStream_t st, u64& launches);
+
 inline int grid_for(size_t total) {
     size_t b = (total + THREADS - 1) / THREADS;
     return int(std::max<size_t>(1, std::min<size_t>(b, size_t(GRID_T) * 4)));
@@ -261,7 +263,14 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
     hs_ = build_structure(codes, g, n, SMALL_LIMIT);
     norm_fe1_ = fe1_index(g);
     ctx_.check();
-    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    {
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        const int above_least = std::max(greatest, least - 1);
+        const int prio = ctx_.priority_level < 0 ? above_least
+                                                 : std::min(above_least, greatest + ctx_.priority_level);
+        CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio));
+    }
     AllocScope alloc_scope(stream_);
     d_ = std::make_unique<Scratch>();
     CK(cudaHostAlloc(&d_->h_nactive, sizeof(int), cudaHostAllocDefault));
@@ -461,11 +470,10 @@ void GpuAbsorber::build_amg() {
             dx.alloc(k * k);
             dscale.upload(scale, stream_);
             dkeep.upload(keep, stream_);
-            k_ldlt_ground<<<1, 1024, 0, stream_>>>(da.p, dd.p, int(k));
-            k_ldlt_inverse<<<int((k + 127) / 128), 128, 0, stream_>>>(da.p, dd.p, int(k), dx.p);
+            dense_ldlt_inverse(da.p, dd.p, int(k), dx.p, stream_, d_->launches);
             k_expand_minv<<<grid_for(k * k), THREADS, 0, stream_>>>(dx.p, dkeep.p, dscale.p, int(k), nL, A.minv.p);
             CK(cudaGetLastError());
-            d_->launches += 3;
+            d_->launches++;
             CK(cudaStreamSynchronize(stream_));
         }
         d_->amg.push_back(std::move(A));
@@ -751,13 +759,10 @@ void GpuAbsorber::build_small_host() {
             dx.alloc(k * k);
             dscale.upload(scale, stream_);
             dkeep.upload(keep, stream_);
-            k_ldlt_ground<<<1, 1024, 0, stream_>>>(da.p, dd.p, int(k));
-            CK(cudaGetLastError());
-            k_ldlt_inverse<<<int((k + 127) / 128), 128, 0, stream_>>>(da.p, dd.p, int(k), dx.p);
-            CK(cudaGetLastError());
+            dense_ldlt_inverse(da.p, dd.p, int(k), dx.p, stream_, d_->launches);
             k_expand_minv<<<grid_for(k * k), THREADS, 0, stream_>>>(dx.p, dkeep.p, dscale.p, int(k), u32(ms), d_->minv.p);
             CK(cudaGetLastError());
-            d_->launches += 3;
+            d_->launches++;
         }
         CK(cudaStreamSynchronize(stream_));
         small_ok_ = true;
@@ -810,10 +815,9 @@ void GpuAbsorber::build_small_device() {
         dd.alloc(k);
         dx.alloc(k * k);
         k_small_gather<<<grid_for(k * k), THREADS, 0, stream_>>>(a.p, u32(ms), dkeep.p, dscale.p, int(k), ak.p);
-        k_ldlt_ground<<<1, 1024, 0, stream_>>>(ak.p, dd.p, int(k));
-        k_ldlt_inverse<<<int((k + 127) / 128), 128, 0, stream_>>>(ak.p, dd.p, int(k), dx.p);
+        dense_ldlt_inverse(ak.p, dd.p, int(k), dx.p, stream_, d.launches);
         k_expand_minv<<<grid_for(k * k), THREADS, 0, stream_>>>(dx.p, dkeep.p, dscale.p, int(k), u32(ms), d.minv.p);
-        d.launches += 4;
+        d.launches += 2;
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream_));
@@ -841,6 +845,33 @@ void allow_smem(K kernel, size_t bytes) {
     const int lim = optin - int(fa.sharedSizeBytes);
     if (bytes > size_t(lim)) throw Error(RC_INTERNAL, "fereg: a kernel needs more shared memory than a block can take");
     CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+}
+
+// Grounded LDL^T of the k x k row-major `a` (lower triangle read, overwritten) and its inverse
+// into x (k x k), on `st`: panels of NB columns (16 up to k = 1024, 8 beyond, so that a panel of
+// k rows fits the shared memory of one CTA), each followed by its trailing update.
+void dense_ldlt_inverse(double* a, double* d, int k, double* x, cudaStream_t st, u64& launches) {
+    if (k <= 0) return;
+    auto factor = [&](auto nbc) {
+        constexpr int NB = decltype(nbc)::value;
+        allow_smem(k_ldlt_panel<NB>, size_t(k) * NB * sizeof(double));
+        for (int jb = 0; jb < k; jb += NB) {
+            const int nb = std::min(NB, k - jb);
+            k_ldlt_panel<NB><<<1, 1024, size_t(k - jb) * NB * sizeof(double), st>>>(a, d, k, jb);
+            launches++;
+            const int T = (k - jb - nb + 31) / 32;  // trailing tiles per side
+            if (T > 0) {
+                k_ldlt_trail<NB><<<T * (T + 1) / 2, 256, 0, st>>>(a, d, k, jb, nb);
+                launches++;
+            }
+        }
+    };
+    if (k <= 1024) factor(std::integral_constant<int, 16>{});
+    else factor(std::integral_constant<int, 8>{});
+    allow_smem(k_ldlt_inverse, size_t(8) * k * sizeof(double));
+    k_ldlt_inverse<<<(k + 7) / 8, 256, size_t(8) * k * sizeof(double), st>>>(a, d, k, x);
+    launches++;
+    CK(cudaGetLastError());
 }
 
 // Per-CTA partial rows of the small coordinates: GRID_S rows of the short-segment kernels, then

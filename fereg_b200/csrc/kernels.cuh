@@ -267,41 +267,111 @@ __global__ void k_small_apply(const double* __restrict__ minv, u32 ms, const T* 
 
 // ---------------------------------------------------------------------------------------------
 // Grounded LDL^T of the unit-diagonal-scaled small block (precond/dense.rs:26-38, 79-100): a
-// pivot at or below PIVOT_TOL is replaced by GROUND. Right-looking, one block; `a` is k x k
-// row-major, its strict lower part becomes the unit-lower factor, `d` the pivots.
+// pivot at or below PIVOT_TOL is replaced by GROUND. `a` is k x k row-major and only its lower
+// triangle is read; its strict lower part becomes the unit-lower factor L, its strict upper part
+// L^T (for the inverse's backward pass), `d` the pivots. Blocked right-looking: a panel of NB
+// columns is factored by one CTA in shared memory (k_ldlt_panel), then every CTA of
+// k_ldlt_trail subtracts the panel's rank-NB update from one 32 x 32 tile of the trailing lower
+// triangle. Column by column the arithmetic is the unblocked one (a[i][l] -= a[i][j] a[l][j] / d_j
+// with the pivots taken in order); only the order of the trailing sums differs.
 constexpr double PIVOT_TOL = 1e-10;
 constexpr double GROUND = 1e30;
 
-__global__ void k_ldlt_ground(double* __restrict__ a, double* __restrict__ d, int k) {
-    for (int j = 0; j < k; j++) {
+template <int NB>
+__global__ void __launch_bounds__(1024) k_ldlt_panel(double* __restrict__ a, double* __restrict__ d, int k, int jb) {
+    extern __shared__ double P[];  // rows jb..k-1 of the panel columns jb..jb+NB-1, NB per row
+    const int nb = min(NB, k - jb), rows = k - jb;
+    for (int idx = threadIdx.x; idx < rows * NB; idx += blockDim.x) {
+        const int r = idx / NB, c = idx % NB;
+        P[idx] = (c < nb && r >= c) ? a[size_t(jb + r) * k + jb + c] : 0.0;
+    }
+    for (int jj = 0; jj < nb; jj++) {
         __syncthreads();
-        double dj = a[size_t(j) * k + j];
+        double dj = P[jj * NB + jj];
         if (dj <= PIVOT_TOL) dj = GROUND;
-        if (threadIdx.x == 0) d[j] = dj;
-        for (int i = j + 1; i < k; i++) {
-            const double f = a[size_t(i) * k + j] / dj;
-            for (int l = j + 1 + int(threadIdx.x); l <= i; l += int(blockDim.x)) a[size_t(i) * k + l] -= f * a[size_t(l) * k + j];
+        if (threadIdx.x == 0) d[jb + jj] = dj;
+        // the panel's later columns: P[r][l] -= P[r][jj] P[l][jj] / dj for jj < l <= r
+        for (int idx = threadIdx.x; idx < (rows - jj - 1) * NB; idx += blockDim.x) {
+            const int r = jj + 1 + idx / NB, l = idx % NB;
+            if (l > jj && l < nb && l <= r) P[r * NB + l] -= P[r * NB + jj] * P[l * NB + jj] / dj;
         }
         __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) a[size_t(i) * k + j] /= dj;
+        for (int r = jj + 1 + int(threadIdx.x); r < rows; r += blockDim.x) P[r * NB + jj] /= dj;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < rows * NB; idx += blockDim.x) {
+        const int r = idx / NB, c = idx % NB;
+        if (c < nb && r > c) {
+            a[size_t(jb + r) * k + jb + c] = P[idx];
+            a[size_t(jb + c) * k + jb + r] = P[idx];
+        }
     }
 }
 
-// X = L^-T D^-1 L^-1 column by column (one thread per identity column), into x (k x k row-major).
-__global__ void k_ldlt_inverse(const double* __restrict__ a, const double* __restrict__ d, int k, double* __restrict__ x) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= k) return;
-    for (int i = 0; i < k; i++) {
-        double v = i == col ? 1.0 : 0.0;
-        for (int p = col; p < i; p++) v -= a[size_t(i) * k + p] * x[size_t(p) * k + col];
-        x[size_t(i) * k + col] = v;
+// Tile (ti, tl), tl <= ti, of the trailing lower triangle (rows and columns from jb + nb): a[i][l]
+// -= sum over the panel's columns p of L[i][p] d_p L[l][p], for l <= i.
+template <int NB>
+__global__ void __launch_bounds__(256) k_ldlt_trail(double* __restrict__ a, const double* __restrict__ d, int k, int jb,
+                                                    int nb) {
+    __shared__ double Li[32][NB + 1], Ll[32][NB + 1];
+    const int t0 = jb + nb, b = int(blockIdx.x);
+    int ti = int((sqrt(8.0 * b + 1.0) - 1.0) / 2.0);
+    while ((ti + 1) * (ti + 2) / 2 <= b) ti++;
+    while (ti * (ti + 1) / 2 > b) ti--;
+    const int tl = b - ti * (ti + 1) / 2;
+    const int i0 = t0 + 32 * ti, l0 = t0 + 32 * tl;
+    for (int idx = threadIdx.x; idx < 32 * NB; idx += blockDim.x) {
+        const int r = idx / NB, p = idx % NB;
+        Li[r][p] = (i0 + r < k && p < nb) ? a[size_t(i0 + r) * k + jb + p] : 0.0;
+        Ll[r][p] = (l0 + r < k && p < nb) ? a[size_t(l0 + r) * k + jb + p] * d[jb + p] : 0.0;
     }
-    for (int i = 0; i < k; i++) x[size_t(i) * k + col] /= d[i];
-    for (int i = k - 1; i >= 0; i--) {
-        double v = x[size_t(i) * k + col];
-        for (int p = i + 1; p < k; p++) v -= a[size_t(p) * k + i] * x[size_t(p) * k + col];
-        x[size_t(i) * k + col] = v;
+    __syncthreads();
+    const int tx = int(threadIdx.x % 32), ty = int(threadIdx.x / 32);
+    const int l = l0 + tx;
+    for (int rr = ty; rr < 32; rr += int(blockDim.x / 32)) {
+        const int i = i0 + rr;
+        if (i < k && l < k && l <= i) {
+            double s = 0.0;
+#pragma unroll
+            for (int p = 0; p < NB; p++) s += Li[rr][p] * Ll[tx][p];
+            a[size_t(i) * k + l] -= s;
+        }
     }
+}
+
+// X = L^-T D^-1 L^-1, one warp per column of X (8 per block), the column held in shared memory:
+// forward over L's rows (strict lower part), the pivots, backward over L^T's rows (strict upper
+// part), each step a warp-wide dot product combined by a fixed butterfly.
+__global__ void __launch_bounds__(256) k_ldlt_inverse(const double* __restrict__ a, const double* __restrict__ d, int k,
+                                                      double* __restrict__ x) {
+    extern __shared__ double xs[];
+    const int w = int(threadIdx.x / 32), lane = int(threadIdx.x % 32);
+    const int col = int(blockIdx.x) * 8 + w;
+    if (col >= k) return;  // whole warps
+    double* v = xs + size_t(w) * k;
+    for (int i = lane; i < k; i += 32) v[i] = i == col ? 1.0 : 0.0;
+    __syncwarp();
+    for (int i = col + 1; i < k; i++) {
+        const double* Li = a + size_t(i) * k;
+        double s = 0.0;
+        for (int p = col + lane; p < i; p += 32) s += Li[p] * v[p];
+#pragma unroll
+        for (int o = 16; o > 0; o /= 2) s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0) v[i] = -s;
+        __syncwarp();
+    }
+    for (int i = lane; i < k; i += 32) v[i] /= d[i];
+    __syncwarp();
+    for (int i = k - 2; i >= 0; i--) {
+        const double* Ui = a + size_t(i) * k;
+        double s = 0.0;
+        for (int p = i + 1 + lane; p < k; p += 32) s += Ui[p] * v[p];
+#pragma unroll
+        for (int o = 16; o > 0; o /= 2) s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0) v[i] -= s;
+        __syncwarp();
+    }
+    for (int i = lane; i < k; i += 32) x[size_t(i) * k + col] = v[i];
 }
 
 // minv (ms x ms, zero outside the kept coordinates) = S^-1 X S^-1 scattered to the kept rows/cols.

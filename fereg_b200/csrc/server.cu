@@ -139,6 +139,16 @@ void Server::worker() {
     }
 }
 
+// Stream priority level of a request: 0 (highest) below 1e5 row-columns, one level lower per
+// decade above. A small request's solve is a long chain of short kernels and host round trips;
+// at equal priority each of its kernels queues behind the large requests' passes.
+static int priority_level(const ServeRequest& q) {
+    const double work = double(q.n) * double(std::max<size_t>(1, q.cols.size()));
+    int level = 0;
+    for (double b = 1e5; work >= b && level < 3; b *= 10.0) level++;
+    return level;
+}
+
 void Server::run(Entry& e) {
     const ServeRequest& q = e.req;
     ServeResult& res = e.res;
@@ -149,6 +159,7 @@ void Server::run(Entry& e) {
     }
     try {
         Ctx ctx;
+        ctx.priority_level = priority_level(q);
         const double t0 = now();
         GpuSession s(q.codes, q.g, q.cl_codes, q.cl_g, q.w, q.w ? q.weight_kind : 0, q.n, 0, ctx);
         double* rows = s.gather_columns(q.cols.data(), q.cols.size());

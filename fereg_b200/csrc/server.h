@@ -10,6 +10,10 @@
 //   session and CUDA stream (GpuSession owns a non-blocking stream; allocations are
 //   stream-ordered), so independent solves overlap on the GPU; a finished request frees its
 //   budget and its worker at once and the next request is admitted.
+// * Stream priorities by size: a request's stream takes a priority level by its rows x columns
+//   (the highest below 1e5, one level lower per decade above), so that small requests, whose
+//   solves are chains of short kernels and host round trips, are not queued behind the large
+//   requests' passes.
 // * Results do not depend on the mix: every kernel reduces in a fixed order and each request's
 //   work stays on its own stream, so a request gives the same bits alone and in the stream.
 // * dry_run: the scheduler without the GPU (each request sleeps dry_run_us), for host-side tests.

@@ -213,16 +213,18 @@ bool GpuSession::nested_within(size_t q, size_t c, DofScratch& s) {
 }
 
 // Starts the dof pass (dof.rs:64-180 does not depend on the data columns) on a host thread of
-// its own and its own low-priority stream, so that its union-finds overlap the column statistics
-// and the FE solve the caller issues on the session's stream; dof_end joins it. The pass waits
-// for the work already on the session's stream (the uploaded codes).
+// its own and its own stream, one priority step below the session's, so that its union-finds
+// overlap the column statistics and the FE solve the caller issues on the session's stream;
+// dof_end joins it. The pass waits for the work already on the session's stream (the uploaded
+// codes).
 std::future<GpuSession::Dof> GpuSession::dof_begin(bool clusters, bool firstpair, bool want_groupvar) {
     SessionDev& d = *d_;
     DofScratch& s = d.dof;
-    if (!s.st.s) {
-        int least = 0, greatest = 0;
+    if (!s.st.s) {  // one priority step below the session's stream
+        int least = 0, greatest = 0, own = 0;
         CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        CK(cudaStreamCreateWithPriority(&s.st.s, cudaStreamNonBlocking, least));
+        CK(cudaStreamGetPriority(d.st, &own));
+        CK(cudaStreamCreateWithPriority(&s.st.s, cudaStreamNonBlocking, std::min(least, own + 1)));
         CK(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
     }
     CK(cudaEventRecord(s.ready, d.st));

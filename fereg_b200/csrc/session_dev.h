@@ -20,7 +20,7 @@ struct OwnedStream {
 };
 
 // The degrees-of-freedom pass (nested checks and the union-finds of the FE pairs) runs on its own
-// low-priority stream from a host thread of its own, beside the session's stream; these are its
+// stream (one priority step below the session's) from a host thread of its own; these are its
 // buffers. gv (the mobility groups of the first pair, row labels) is read on the session's
 // stream once the pass has been joined.
 struct DofScratch {
