@@ -190,6 +190,69 @@ __global__ void k_small_assemble(const u32* __restrict__ seg_off, const u32* __r
     }
 }
 
+// The same S_SS by rows, for small super-blocks too large for per-thread partial matrices: one
+// warp per work item (row k, a run of k's coordinate-list entries that never splits a segment),
+// accumulating the item's dense partial row in shared memory. Per entry (cell c of segment s):
+// S[k][l] += W_c for the small codes l of c; once per segment of the run, with
+// c_{s,k} = sum over the segment's cells and small blocks of W [code == k] (a warp sum in fixed
+// order), S[k][l] -= c_{s,k} W_c' / n1_s for the small codes l of every cell c' of s. Lane 0
+// applies the updates in entry and cell order, so the row does not depend on timing;
+// k_small_rows_sum adds a row's items in item order.
+__global__ void __launch_bounds__(256) k_small_rows(const u32* __restrict__ seg_off, const u32* __restrict__ coord,
+                                                    u32 M, int ns, u32 ms, const double* __restrict__ cw,
+                                                    const double* __restrict__ n1inv, const u32* __restrict__ pl_cell,
+                                                    const u32* __restrict__ pl_seg, const u32* __restrict__ item_k,
+                                                    const u32* __restrict__ item_a, const u32* __restrict__ item_b,
+                                                    u32 nitems, double* __restrict__ part) {
+    extern __shared__ double rows_s[];
+    const u32 w = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const u32 it = blockIdx.x * 8 + w;
+    if (it >= nitems) return;  // whole warps
+    double* row = rows_s + size_t(w) * ms;
+    for (u32 l = lane; l < ms; l += 32) row[l] = 0.0;
+    __syncwarp();
+    const u32 k = item_k[it];
+    u32 prev = 0xffffffffu;
+    for (u32 e = item_a[it]; e < item_b[it]; e++) {
+        const u32 c = pl_cell[e], s = pl_seg[e];
+        if (lane == 0) {
+            const double wc = cw ? cw[c] : 1.0;
+            for (int b = 0; b < ns; b++) row[coord[size_t(b) * M + c]] += wc;
+        }
+        if (s != prev) {
+            prev = s;
+            const u32 c0 = seg_off[s], c1 = seg_off[s + 1];
+            double ck = 0.0;
+            for (u32 cc = c0 + lane; cc < c1; cc += 32) {
+                const double wc = cw ? cw[cc] : 1.0;
+                for (int b = 0; b < ns; b++)
+                    if (coord[size_t(b) * M + cc] == k) ck += wc;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o /= 2) ck += __shfl_xor_sync(FULL, ck, o);
+            const double f = ck * n1inv[s];
+            if (lane == 0)
+                for (u32 cc = c0; cc < c1; cc++) {
+                    const double v = f * (cw ? cw[cc] : 1.0);
+                    for (int b = 0; b < ns; b++) row[coord[size_t(b) * M + cc]] -= v;
+                }
+        }
+        __syncwarp();
+    }
+    for (u32 l = lane; l < ms; l += 32) part[size_t(it) * ms + l] = row[l];
+}
+
+// Row k of S_SS: the partial rows of k's items (first[k] .. first[k+1]) added in item order.
+__global__ void k_small_rows_sum(const double* __restrict__ part, const u32* __restrict__ first, u32 ms,
+                                 double* __restrict__ out) {
+    const u32 k = blockIdx.x;
+    for (u32 l = threadIdx.x; l < ms; l += blockDim.x) {
+        double v = 0.0;
+        for (u32 it = first[k]; it < first[k + 1]; it++) v += part[size_t(it) * ms + l];
+        out[size_t(k) * ms + l] = v;
+    }
+}
+
 __global__ void k_small_sum_parts(const double* __restrict__ part, int nparts, size_t len, double* __restrict__ out) {
     for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < len; e += size_t(gridDim.x) * blockDim.x) {
         double v = 0.0;
