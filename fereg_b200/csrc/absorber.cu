@@ -33,9 +33,6 @@ constexpr double REDUNDANT = 1e-12;  // operator.rs:21
 // Jacobi, as the reference does when the dense factor costs more than a few PCG iterations
 // (solve.rs:541-548 defer_small); the converged answer is the same within the tolerance.
 constexpr size_t DENSE_SMALL_MAX = 1024;
-// Above this many small coordinates the device assembly of the small block runs by rows
-// (k_small_rows): per-thread partial matrices of ms^2 would leave too few threads.
-constexpr size_t SMALL_ROWS_MIN = 128;
 // Refinement: an FP32 inner solve stops once its preconditioned residual fell by this factor
 // (squared), well above FP32 rounding; the FP64 true residual then restarts it.
 constexpr double REFINE_DROP = 1e-9;
@@ -329,7 +326,7 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
             d_->cw_e1.upload(e1, stream_);
             d_->cw_list_off.upload(loff, stream_);
         }
-        if (hs_.m_small > SMALL_ROWS_MIN && hs_.m_small <= DENSE_SMALL_MAX) {
+        if (hs_.m_small > 0 && hs_.m_small <= DENSE_SMALL_MAX) {
             // runs of each small coordinate's entries, at least `run` long, never splitting a segment
             const u32 es = pt.off[hs_.m_small];
             const u32 run = std::max<u32>(256, es / 4096);
@@ -802,7 +799,8 @@ void GpuAbsorber::build_small_host() {
 }
 
 // The dense small factor from the device assembly of S_SS (weights.cuh) for the device weight
-// state: per-thread partial matrices over segment ranges, summed in thread order.
+// state: by rows (k_small_rows over the work items built with the coordinate lists), each row's
+// items summed in item order.
 void GpuAbsorber::build_small_device() {
     const HostStructure& st = hs_;
     const size_t ms = st.m_small, M = st.ncells;
@@ -810,32 +808,17 @@ void GpuAbsorber::build_small_device() {
     int ns = 0;
     for (auto& b : st.blocks) ns += b.small;
     const size_t len = ms * ms;
-    DBuf<double> part, acc, a, ak, dd, dx, dscale;
-    DBuf<u32> touched, dkeep;
+    DBuf<double> part, a, ak, dd, dx, dscale;
+    DBuf<u32> dkeep;
     a.alloc(len);
-    if (d.sr_n > 0) {  // by rows
-        part.alloc(size_t(d.sr_n) * ms);
-        const size_t shm = size_t(8) * ms * sizeof(double);
-        allow_smem(k_small_rows, shm);
-        k_small_rows<<<(d.sr_n + 7) / 8, 256, shm, stream_>>>(d.seg_off.p, d.coord.p, u32(M), ns, u32(ms), d.cell_w.p,
-                                                               d.n1inv.p, d.pl_cell.p, d.pl_seg.p, d.sr_k.p, d.sr_a.p,
-                                                               d.sr_b.p, d.sr_n, part.p);
-        k_small_rows_sum<<<u32(ms), 256, 0, stream_>>>(part.p, d.sr_first.p, u32(ms), a.p);
-        d.launches += 2;
-    } else {  // per-thread partial matrices over segment ranges
-        const int nparts = int(std::max<size_t>(1, std::min<size_t>({size_t(GRID_V) * 4, size_t(st.g1),
-                                                                       (size_t(64) << 20) / (len * 8)})));
-        part.alloc(size_t(nparts) * len);
-        acc.alloc(size_t(nparts) * ms);
-        touched.alloc(size_t(nparts) * ms);
-        CK(cudaMemsetAsync(part.p, 0, size_t(nparts) * len * sizeof(double), stream_));
-        CK(cudaMemsetAsync(acc.p, 0, size_t(nparts) * ms * sizeof(double), stream_));
-        k_small_assemble<<<(nparts + 63) / 64, 64, 0, stream_>>>(d.seg_off.p, d.coord.p, st.g1, u32(M), ns,
-                                                                   u32(ms), nparts, d.cell_w.p, d.n1inv.p, part.p,
-                                                                   acc.p, touched.p);
-        k_small_sum_parts<<<grid_for(len), THREADS, 0, stream_>>>(part.p, nparts, len, a.p);
-        d.launches += 2;
-    }
+    part.alloc(size_t(d.sr_n) * ms);
+    const size_t shm = size_t(8) * ms * sizeof(double);
+    allow_smem(k_small_rows, shm);
+    k_small_rows<<<(d.sr_n + 7) / 8, 256, shm, stream_>>>(d.seg_off.p, d.coord.p, u32(M), ns, u32(ms), d.cell_w.p,
+                                                           d.n1inv.p, d.pl_cell.p, d.pl_seg.p, d.sr_k.p, d.sr_a.p,
+                                                           d.sr_b.p, d.sr_n, part.p);
+    k_small_rows_sum<<<u32(ms), 256, 0, stream_>>>(part.p, d.sr_first.p, u32(ms), a.p);
+    d.launches += 2;
     // kept coordinates (not redundant, positive diagonal) and their unit-diagonal scaling
     std::vector<double> diag(ms);
     std::vector<uint8_t> red(ms);

@@ -153,45 +153,8 @@ __global__ void k_coord_combine(const u32* __restrict__ list_chunk_off, u32 m, c
 
 // Dense small super-block S_SS (ms x ms, the first ms coordinates, ns small blocks) for the current
 // cell weights, on the device (operator.rs:1457-1523, as the host assembly of the dense factor):
-//   S_SS[k][l] = sum_c W_c [k in c][l in c] - sum_s c_{s,k} c_{s,l} / n1_s.
-// Thread t walks the segments of its contiguous range in order and accumulates into its own
-// partial matrix (no atomics); k_small_sum_parts adds the partials in thread order, so the
-// matrix is deterministic. acc / touched are the thread's sparse accumulator (ms entries each).
-__global__ void k_small_assemble(const u32* __restrict__ seg_off, const u32* __restrict__ coord, u32 g1, u32 M,
-                                 int ns, u32 ms, int nparts, const double* __restrict__ cw,
-                                 const double* __restrict__ n1inv, double* __restrict__ part,
-                                 double* __restrict__ acc_all, u32* __restrict__ touched_all) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nparts) return;
-    double* P = part + size_t(t) * ms * ms;
-    double* acc = acc_all + size_t(t) * ms;
-    u32* touched = touched_all + size_t(t) * ms;
-    const u32 s0 = u32((u64(g1) * u64(t)) / u64(nparts)), s1 = u32((u64(g1) * u64(t + 1)) / u64(nparts));
-    for (u32 s = s0; s < s1; s++) {
-        u32 cnt = 0;
-        for (u32 c = seg_off[s]; c < seg_off[s + 1]; c++) {
-            const double w = cw ? cw[c] : 1.0;
-            for (int b = 0; b < ns; b++) {
-                const u32 k = coord[size_t(b) * M + c];
-                if (acc[k] == 0.0) touched[cnt++] = k;
-                acc[k] += w;
-                P[size_t(k) * ms + k] += w;
-                for (int b2 = 0; b2 < ns; b2++)
-                    if (b2 != b) P[size_t(k) * ms + coord[size_t(b2) * M + c]] += w;
-            }
-        }
-        const double f = n1inv[s];
-        for (u32 i = 0; i < cnt; i++) {
-            const u32 k = touched[i];
-            const double ak = acc[k] * f;
-            for (u32 j = 0; j < cnt; j++) P[size_t(k) * ms + touched[j]] -= ak * acc[touched[j]];
-        }
-        for (u32 i = 0; i < cnt; i++) acc[touched[i]] = 0.0;
-    }
-}
-
-// The same S_SS by rows, for small super-blocks too large for per-thread partial matrices: one
-// warp per work item (row k, a run of k's coordinate-list entries that never splits a segment),
+//   S_SS[k][l] = sum_c W_c [k in c][l in c] - sum_s c_{s,k} c_{s,l} / n1_s,
+// by rows: one warp per work item (row k, a run of k's coordinate-list entries that never splits a segment),
 // accumulating the item's dense partial row in shared memory. Per entry (cell c of segment s):
 // S[k][l] += W_c for the small codes l of c; once per segment of the run, with
 // c_{s,k} = sum over the segment's cells and small blocks of W [code == k] (a warp sum in fixed
@@ -253,13 +216,6 @@ __global__ void k_small_rows_sum(const double* __restrict__ part, const u32* __r
     }
 }
 
-__global__ void k_small_sum_parts(const double* __restrict__ part, int nparts, size_t len, double* __restrict__ out) {
-    for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < len; e += size_t(gridDim.x) * blockDim.x) {
-        double v = 0.0;
-        for (int t = 0; t < nparts; t++) v += part[size_t(t) * len + e];
-        out[e] = v;
-    }
-}
 
 // ak (k x k) = the kept rows / columns of a (ms x ms), scaled to unit diagonal.
 __global__ void k_small_gather(const double* __restrict__ a, u32 ms, const u32* __restrict__ keep,

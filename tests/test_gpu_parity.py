@@ -208,9 +208,9 @@ def test_device_weights_match_oracle(pair):
 
 @pytest.mark.parametrize("case", ["dense_small", "small_firms", "two_fe", "repeated_cells"])
 def test_device_small_factor_matches_oracle(case):
-    """With weights set on the device, the dense small factor is assembled on the device (by
-    per-thread partial matrices, or by rows above 128 small coordinates: dense_small 910,
-    small_firms 310); the preconditioner matches the oracle's host assembly."""
+    """With weights set on the device, the dense small factor is assembled on the device by rows
+    (weights.cuh k_small_rows; dense_small: 910 small coordinates, small_firms 310, two_fe 10);
+    the preconditioner matches the oracle's host assembly."""
     import torch
 
     codes, g, w0, z = build(case)
