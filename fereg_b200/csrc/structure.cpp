@@ -7,6 +7,8 @@
 // is a stable LSD counting sort, so equal keys keep observation order; the result is unique and
 // therefore identical to the reference's (which sorts per segment in parallel).
 
+#include <omp.h>
+
 #include <algorithm>
 #include <numeric>
 
@@ -197,29 +199,59 @@ HostStructure build_structure(const std::vector<const u32*>& codes, const std::v
     return st;
 }
 
+// A stable parallel counting sort: thread t takes a contiguous range of cells, counts its
+// entries per coordinate, and writes them from its own offset in every list (the entries of
+// lower-ranked threads, hence of earlier cells, come first), so every list is in cell order
+// exactly as in one pass over the cells.
 PullTable build_pull_table(const HostStructure& st) {
     PullTable t;
-    const size_t nb = st.nb(), M = st.ncells;
-    const size_t E = M * nb;
-    t.off.assign(st.m + 1, 0);
-    for (size_t k = 0; k < nb; k++)
-        for (size_t c = 0; c < M; c++) t.off[st.coord[k * M + c] + 1]++;
-    for (size_t k = 0; k < st.m; k++) t.off[k + 1] += t.off[k];
+    const size_t nb = st.nb(), M = st.ncells, m = st.m;
+    const size_t E = M * nb, no = nb > 0 ? nb - 1 : 0;
+    t.off.assign(m + 1, 0);
     t.cell.resize(E);
     t.seg.resize(E);
-    t.other.resize(E * (nb > 0 ? nb - 1 : 0));
-    std::vector<u32> cur(t.off.begin(), t.off.end() - 1);
-    for (u32 s = 0; s < st.g1; s++)
-        for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++)
+    t.other.resize(E * no);
+    if (E == 0) return t;
+    std::vector<u32> cseg(M);  // segment of every cell
+#pragma omp parallel for schedule(static)
+    for (long long s = 0; s < (long long)st.g1; s++)
+        for (u32 c = st.seg_off[size_t(s)]; c < st.seg_off[size_t(s) + 1]; c++) cseg[c] = u32(s);
+    const size_t cap = std::max<size_t>(1, (size_t(128) << 20) / (4 * std::max<size_t>(1, m)));
+    const int T = E < (size_t(1) << 20) ? 1 : int(std::min<size_t>({16, size_t(omp_get_max_threads()), cap}));
+    std::vector<u32> pos(size_t(T) * m, 0);  // per thread: count, then first write position per list
+    auto lo = [&](int th) { return size_t(M * size_t(th) / size_t(T)); };
+#pragma omp parallel num_threads(T)
+    {
+        const int th = omp_get_thread_num();
+        u32* p = pos.data() + size_t(th) * m;
+        for (size_t c = lo(th); c < lo(th + 1); c++)
+            for (size_t k = 0; k < nb; k++) p[st.coord[k * M + c]]++;
+    }
+    for (size_t x = 0; x < m; x++) {
+        u32 acc = 0;
+        for (int th = 0; th < T; th++) {
+            const u32 v = pos[size_t(th) * m + x];
+            pos[size_t(th) * m + x] = acc;
+            acc += v;
+        }
+        t.off[x + 1] = acc;
+    }
+    for (size_t x = 0; x < m; x++) t.off[x + 1] += t.off[x];
+#pragma omp parallel num_threads(T)
+    {
+        const int th = omp_get_thread_num();
+        u32* p = pos.data() + size_t(th) * m;
+        for (size_t c = lo(th); c < lo(th + 1); c++)
             for (size_t k = 0; k < nb; k++) {
                 const u32 x = st.coord[k * M + c];
-                const u32 e = cur[x]++;
-                t.cell[e] = c;
-                t.seg[e] = s;
+                const u32 e = t.off[x] + p[x]++;
+                t.cell[e] = u32(c);
+                t.seg[e] = cseg[c];
                 size_t o = 0;
                 for (size_t k2 = 0; k2 < nb; k2++)
-                    if (k2 != k) t.other[size_t(e) * (nb - 1) + o++] = st.coord[k2 * M + c];
+                    if (k2 != k) t.other[size_t(e) * no + o++] = st.coord[k2 * M + c];
             }
+    }
     return t;
 }
 
