@@ -28,14 +28,36 @@ int fe1_index(const std::vector<u32>& g) {
     return best;
 }
 
-// Stable counting sort of `ids` by key(id) < g.
+// Stable counting sort of `ids` by key(id) < g. Above 2^18 ids it runs in parallel: thread t
+// counts its contiguous range, then writes it from its own offset in every bucket (after the
+// lower-ranked threads' ids), which keeps the order of one sequential pass.
 template <class Key>
 static void counting_pass(std::vector<u32>& ids, std::vector<u32>& tmp, u32 g, Key key) {
-    std::vector<u32> cnt(size_t(g) + 1, 0);
-    for (u32 i : ids) cnt[key(i) + 1]++;
-    for (u32 k = 0; k < g; k++) cnt[k + 1] += cnt[k];
-    tmp.resize(ids.size());
-    for (u32 i : ids) tmp[cnt[key(i)]++] = i;
+    const size_t n = ids.size();
+    const size_t cap = std::max<size_t>(1, (size_t(128) << 20) / (4 * (size_t(g) + 1)));
+    const int T = n < (size_t(1) << 18) ? 1 : int(std::min<size_t>({16, size_t(omp_get_max_threads()), cap}));
+    std::vector<u32> pos(size_t(T) * g, 0);
+    auto lo = [&](int th) { return size_t(n * size_t(th) / size_t(T)); };
+#pragma omp parallel num_threads(T)
+    {
+        const int th = omp_get_thread_num();
+        u32* p = pos.data() + size_t(th) * g;
+        for (size_t i = lo(th); i < lo(th + 1); i++) p[key(ids[i])]++;
+    }
+    u32 acc = 0;
+    for (u32 k = 0; k < g; k++)
+        for (int th = 0; th < T; th++) {
+            const u32 v = pos[size_t(th) * g + k];
+            pos[size_t(th) * g + k] = acc;
+            acc += v;
+        }
+    tmp.resize(n);
+#pragma omp parallel num_threads(T)
+    {
+        const int th = omp_get_thread_num();
+        u32* p = pos.data() + size_t(th) * g;
+        for (size_t i = lo(th); i < lo(th + 1); i++) tmp[p[key(ids[i])]++] = ids[i];
+    }
     ids.swap(tmp);
 }
 
@@ -130,11 +152,15 @@ HostStructure build_structure(const std::vector<const u32*>& codes, const std::v
         }
         return true;
     };
-    bool sorted = true;
-    for (size_t i = 1; i < n && sorted; i++) sorted = key_less_eq(u32(i - 1), u32(i));
+    const int T = n < (size_t(1) << 18) ? 1 : std::min(16, omp_get_max_threads());
+    auto lo = [&](int th) { return size_t(n * size_t(th) / size_t(T)); };
+    int unsorted = 0;
+#pragma omp parallel for num_threads(T) reduction(| : unsorted) schedule(static)
+    for (long long i = 1; i < (long long)n; i++)
+        if (!key_less_eq(u32(i - 1), u32(i))) unsorted = 1;
     st.pi.resize(n);
     std::iota(st.pi.begin(), st.pi.end(), 0u);
-    if (!sorted) {
+    if (unsorted) {
         std::vector<u32> tmp;
         for (size_t k = nb; k-- > 0;) {
             const u32* c = codes[st.blocks[k].term];
@@ -146,49 +172,73 @@ HostStructure build_structure(const std::vector<const u32*>& codes, const std::v
         }
     }
 
-    // Cells and segments in one pass.
-    st.seg_off.assign(size_t(st.g1) + 1, 0);
-    std::vector<u32> starts;
-    starts.reserve(n);
-    std::vector<std::vector<u32>> cc(nb);
-    for (auto& v : cc) v.reserve(n);
+    // Cells and segments: a row opens a cell when its key differs from the previous row's. Thread
+    // t cuts its own range of rows (the first compared with the row before the range), then
+    // writes its cells at the offset of the cells of the lower-ranked threads.
     const u32* c1 = st.fe1 >= 0 ? codes[size_t(st.fe1)] : nullptr;
-    for (size_t r = 0; r < n; r++) {
-        const u32 o = st.pi[r];
-        bool open = r == 0;
-        if (!open) {
-            const u32 p = st.pi[r - 1];
-            if (c1 && c1[o] != c1[p]) open = true;
-            for (size_t k = 0; k < nb && !open; k++) open = codes[st.blocks[k].term][o] != codes[st.blocks[k].term][p];
-        }
-        if (open) {
-            starts.push_back(u32(r));
-            st.seg_off[(c1 ? c1[o] : 0) + 1]++;
-            for (size_t k = 0; k < nb; k++) cc[k].push_back(st.blocks[k].off + codes[st.blocks[k].term][o]);
-        }
+    auto opens = [&](size_t r) {
+        if (r == 0) return true;
+        const u32 o = st.pi[r], p = st.pi[r - 1];
+        if (c1 && c1[o] != c1[p]) return true;
+        for (size_t k = 0; k < nb; k++)
+            if (codes[st.blocks[k].term][o] != codes[st.blocks[k].term][p]) return true;
+        return false;
+    };
+    std::vector<size_t> tcells(size_t(T) + 1, 0);
+#pragma omp parallel num_threads(T)
+    {
+        const int th = omp_get_thread_num();
+        size_t cnt = 0;
+        for (size_t r = lo(th); r < lo(th + 1); r++) cnt += opens(r) ? 1 : 0;
+        tcells[size_t(th) + 1] = cnt;
     }
+    for (int th = 0; th < T; th++) tcells[size_t(th) + 1] += tcells[size_t(th)];
+    st.ncells = tcells[size_t(T)];
+    const size_t M = st.ncells;
+    std::vector<u32> starts(M);
+    st.coord.resize(nb * M);
+    std::vector<u32> cseg(M);  // FE1 level of every cell
+#pragma omp parallel num_threads(T)
+    {
+        const int th = omp_get_thread_num();
+        size_t c = tcells[size_t(th)];
+        for (size_t r = lo(th); r < lo(th + 1); r++)
+            if (opens(r)) {
+                const u32 o = st.pi[r];
+                starts[c] = u32(r);
+                cseg[c] = c1 ? c1[o] : 0;
+                for (size_t k = 0; k < nb; k++) st.coord[k * M + c] = st.blocks[k].off + codes[st.blocks[k].term][o];
+                c++;
+            }
+    }
+    st.seg_off.assign(size_t(st.g1) + 1, 0);
+    for (size_t c = 0; c < M; c++) st.seg_off[size_t(cseg[c]) + 1]++;
     for (u32 s = 0; s < st.g1; s++) st.seg_off[s + 1] += st.seg_off[s];
-    st.ncells = starts.size();
-    if (st.ncells != n) {
+    if (M != n) {
         st.cell_row = std::move(starts);
         st.cell_row.push_back(u32(n));
     }
-    st.coord.resize(nb * st.ncells);
-    for (size_t k = 0; k < nb; k++) std::copy(cc[k].begin(), cc[k].end(), st.coord.begin() + k * st.ncells);
 
     // Dense small-block work sum_s (distinct small coordinates)^2 (structure.rs:521-525).
     if (st.m_small > 0) {
-        std::vector<u32> mark(st.m_small, 0);
         u64 work = 0;
-        for (u32 s = 0; s < st.g1; s++) {
-            u64 d = 0;
-            for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++)
-                for (size_t k = 0; k < nb; k++) {
-                    if (!st.blocks[k].small) continue;
-                    u32 x = st.coord[k * st.ncells + c];
-                    if (mark[x] != s + 1) { mark[x] = s + 1; d++; }
-                }
-            work += d * d;
+#pragma omp parallel num_threads(T) reduction(+ : work)
+        {
+            std::vector<u32> mark(st.m_small, 0);
+#pragma omp for schedule(static)
+            for (long long s = 0; s < (long long)st.g1; s++) {
+                u64 d = 0;
+                for (u32 c = st.seg_off[size_t(s)]; c < st.seg_off[size_t(s) + 1]; c++)
+                    for (size_t k = 0; k < nb; k++) {
+                        if (!st.blocks[k].small) continue;
+                        u32 x = st.coord[k * st.ncells + c];
+                        if (mark[x] != u32(s) + 1) {
+                            mark[x] = u32(s) + 1;
+                            d++;
+                        }
+                    }
+                work += d * d;
+            }
         }
         st.small_work = work;
         if (work > 64 * u64(st.ncells)) {
