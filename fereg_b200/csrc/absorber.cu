@@ -355,7 +355,7 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
         d_->pl_other.upload(pt.other, stream_);
         WarpTileList wt;
         TileList ct;
-        split_tiles(pt.off, nullptr, d_->ms_acc, u32(hs_.m), PULL_WARP_MAX, PULL_WARP_MAX, WLIST, TILE, wt, ct);
+        split_tiles(pt.off, nullptr, d_->ms_acc, u32(hs_.m), PULL_WARP_MAX, PULL_WARP_MAX, WLIST, PULL_SLICE, wt, ct);
         d_->wpull.upload(wt, stream_);
         d_->pull_tiles.upload(ct, stream_);
         CK(cudaStreamSynchronize(stream_));  // host tables die here

@@ -22,6 +22,7 @@ namespace fereg {
 
 constexpr int TB = 256;       // threads per tile CTA
 constexpr int TILE = 128;     // cells or entries per tile
+constexpr int PULL_SLICE = 2048;  // entries per coordinate-list tile
 constexpr int RC_MAX = 16;    // columns per chunk
 constexpr int SACC_MAX = 16;  // small coordinates summed in the segment passes
 constexpr int SACC_BLOCKS = 4;
@@ -221,13 +222,27 @@ __global__ void __launch_bounds__(TB) k_seg_small_slices(DevStruct S, DevWeights
     }
 }
 
+// Sum over the slots of a CTA of red[slot * Rc + col] into red[col] (slot 0), by a pairwise tree
+// over the slot indices: the same order every call. Every thread of the CTA calls it.
+template <class T>
+__device__ __forceinline__ void slot_tree(T* red, const ColMap& cm) {
+    for (int s = 1; s < cm.nslot; s *= 2) {
+        __syncthreads();
+        if (cm.on && cm.slot % (2 * s) == 0 && cm.slot + s < cm.nslot)
+            red[cm.slot * cm.Rc + cm.col] += red[(cm.slot + s) * cm.Rc + cm.col];
+    }
+    __syncthreads();
+}
+
 // Operator pass 2: Y[k] = nr_k P[k] + sum over the cells c of k of W_c (sum_{other b} P - t_{s(c)})
-// for the pulled coordinates.
+// for the pulled coordinates. A tile holds whole lists or a slice of one long list (its partial
+// goes to k_fix); per list, thread (slot, column) sums the entries slot, slot + nslot, ... in a
+// register and the slots are combined by slot_tree.
 template <class T>
 __global__ void __launch_bounds__(TB) k_pull_apply(DevStruct S, DevWeights W, const T* __restrict__ P,
                                                    const T* __restrict__ t, int R, T* __restrict__ Y,
                                                    T* __restrict__ part) {
-    __shared__ T vals[TILE * RC_MAX];
+    __shared__ T red[TB];
     const TileSet& ts = S.pull;
     const u32 no = S.nb - 1;
     for (u32 tile = blockIdx.x; tile < ts.n; tile += gridDim.x) {
@@ -235,28 +250,27 @@ __global__ void __launch_bounds__(TB) k_pull_apply(DevStruct S, DevWeights W, co
         const int pslot = ts.part[tile];
         for (int j0 = 0; j0 < R; j0 += RC_MAX) {
             const ColMap cm = colmap(R, j0);
-            if (cm.on) {
-#pragma unroll 4
-                for (u32 e = e0 + cm.slot; e < e1; e += cm.nslot) {
-                    T u = -__ldcg(t + size_t(__ldcs(S.pl_seg + e)) * R + j0 + cm.col);
-                    for (u32 o = 0; o < no; o++) u += P[size_t(__ldcs(S.pl_other + size_t(e) * no + o)) * R + j0 + cm.col];
-                    const T w = W.cell_w ? T(W.cell_w[__ldcs(S.pl_cell + e)]) : T(1);
-                    vals[(e - e0) * cm.Rc + cm.col] = w * u;
-                }
-            }
-            __syncthreads();
-            const u32 nk = (k1 - k0) * u32(cm.Rc);
-            for (u32 idx = threadIdx.x; idx < nk; idx += TB) {
-                const u32 k = k0 + idx / cm.Rc;
-                const int col = int(idx % cm.Rc);
+            for (u32 k = k0; k < k1; k++) {
                 const u32 a = max(S.pl_off[k], e0), b = min(S.pl_off[k + 1], e1);
                 T acc = T(0);
-                for (u32 e = a; e < b; e++) acc += vals[(e - e0) * cm.Rc + col];
-                const size_t o = size_t(k) * R + j0 + col;
-                if (pslot < 0) Y[o] = T(W.nr[k]) * P[o] + acc;
-                else part[size_t(pslot) * R + j0 + col] = acc;
+                if (cm.on) {
+#pragma unroll 4
+                    for (u32 e = a + cm.slot; e < b; e += cm.nslot) {
+                        T u = -__ldcg(t + size_t(__ldcs(S.pl_seg + e)) * R + j0 + cm.col);
+                        for (u32 o = 0; o < no; o++)
+                            u += P[size_t(__ldcs(S.pl_other + size_t(e) * no + o)) * R + j0 + cm.col];
+                        acc += W.cell_w ? T(W.cell_w[__ldcs(S.pl_cell + e)]) * u : u;
+                    }
+                    red[cm.slot * cm.Rc + cm.col] = acc;
+                }
+                slot_tree(red, cm);
+                if (cm.on && cm.slot == 0) {
+                    const size_t o = size_t(k) * R + j0 + cm.col;
+                    if (pslot < 0) Y[o] = T(W.nr[k]) * P[o] + red[cm.col];
+                    else part[size_t(pslot) * R + j0 + cm.col] = red[cm.col];
+                }
+                __syncthreads();
             }
-            __syncthreads();
         }
     }
 }
@@ -424,42 +438,41 @@ __global__ void __launch_bounds__(TB) k_rhs_small_slices(DevStruct S, DevWeights
 }
 
 // Right-hand side pass 2: rhs[k] = sum over the cells c of k of (s_c - W_c b1_{s(c)} / n1_{s(c)})
-// for the pulled coordinates.
+// for the pulled coordinates, with the tiles and the slot sums of k_pull_apply.
 __global__ void __launch_bounds__(TB) k_pull_rhs(DevStruct S, DevWeights W, const double* __restrict__ rows,
                                                  const double* __restrict__ b1, int R, double* __restrict__ Y,
                                                  double* __restrict__ part) {
-    __shared__ double vals[TILE * RC_MAX];
+    __shared__ double red[TB];
     const TileSet& ts = S.pull;
     for (u32 tile = blockIdx.x; tile < ts.n; tile += gridDim.x) {
         const u32 k0 = ts.k0[tile], k1 = ts.k1[tile], e0 = ts.e0[tile], e1 = ts.e1[tile];
         const int pslot = ts.part[tile];
         for (int j0 = 0; j0 < R; j0 += RC_MAX) {
             const ColMap cm = colmap(R, j0);
-            if (cm.on) {
-#pragma unroll 4
-                for (u32 e = e0 + cm.slot; e < e1; e += cm.nslot) {
-                    const u32 c = __ldcs(S.pl_cell + e), s = __ldcs(S.pl_seg + e);
-                    double sc = 0.0;
-                    const u32 r1 = row1_of(S, c);
-                    for (u32 row = row0_of(S, c); row < r1; row++) {
-                        const double v = __ldcs(rows + size_t(row) * R + j0 + cm.col);
-                        sc += W.w_rows ? W.w_rows[row] * v : v;
-                    }
-                    vals[(e - e0) * cm.Rc + cm.col] = sc - cellw(W, c) * __ldcg(b1 + size_t(s) * R + j0 + cm.col) * W.n1inv[s];
-                }
-            }
-            __syncthreads();
-            const u32 nk = (k1 - k0) * u32(cm.Rc);
-            for (u32 idx = threadIdx.x; idx < nk; idx += TB) {
-                const u32 k = k0 + idx / cm.Rc;
-                const int col = int(idx % cm.Rc);
+            for (u32 k = k0; k < k1; k++) {
                 const u32 a = max(S.pl_off[k], e0), b = min(S.pl_off[k + 1], e1);
                 double acc = 0.0;
-                for (u32 e = a; e < b; e++) acc += vals[(e - e0) * cm.Rc + col];
-                if (pslot < 0) Y[size_t(k) * R + j0 + col] = acc;
-                else part[size_t(pslot) * R + j0 + col] = acc;
+                if (cm.on) {
+#pragma unroll 4
+                    for (u32 e = a + cm.slot; e < b; e += cm.nslot) {
+                        const u32 c = __ldcs(S.pl_cell + e), s = __ldcs(S.pl_seg + e);
+                        double sc = 0.0;
+                        const u32 r1 = row1_of(S, c);
+                        for (u32 row = row0_of(S, c); row < r1; row++) {
+                            const double v = __ldcs(rows + size_t(row) * R + j0 + cm.col);
+                            sc += W.w_rows ? W.w_rows[row] * v : v;
+                        }
+                        acc += sc - cellw(W, c) * __ldcg(b1 + size_t(s) * R + j0 + cm.col) * W.n1inv[s];
+                    }
+                    red[cm.slot * cm.Rc + cm.col] = acc;
+                }
+                slot_tree(red, cm);
+                if (cm.on && cm.slot == 0) {
+                    if (pslot < 0) Y[size_t(k) * R + j0 + cm.col] = red[cm.col];
+                    else part[size_t(pslot) * R + j0 + cm.col] = red[cm.col];
+                }
+                __syncthreads();
             }
-            __syncthreads();
         }
     }
 }
