@@ -1026,7 +1026,7 @@ void launch_precond(Scratch& d, const DevStruct& S, bool small_ok, const T* r, T
         d.launches++;
     }
     if (ms > 0) {
-        k_small_apply<T><<<grid_for(size_t(ms) * R), THREADS, 0, st>>>(d.minv.p, ms, r, z, R);
+        k_small_apply<T><<<grid_for(size_t(ms) * R * 32), THREADS, 0, st>>>(d.minv.p, ms, r, z, R);
         d.launches++;
     }
     for (auto& a : d.amg) launch_amg<T>(d, a, r, z, R, st);  // escalated blocks replace their Jacobi values

@@ -252,16 +252,22 @@ __global__ void k_jacobi(const T* __restrict__ r, T* __restrict__ z, const doubl
 }
 
 // Small super-block: z[0..ms) = Minv r[0..ms) with the expanded, scaled generalized inverse.
+// z = minv r on the small coordinates (ms x R), one warp per output element: lane l adds the
+// products of entries l, l + 32, ... in order, combined by a fixed butterfly.
 template <class T>
 __global__ void k_small_apply(const double* __restrict__ minv, u32 ms, const T* __restrict__ r, T* __restrict__ z, int R) {
     const size_t total = size_t(ms) * R;
-    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+    const u32 lane = threadIdx.x % 32;
+    const size_t nw = size_t(gridDim.x) * blockDim.x / 32;
+    for (size_t i = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; i < total; i += nw) {
         const u32 row = u32(i / R);
         const int col = int(i % R);
-        double acc = 0.0;
         const double* mr = minv + size_t(row) * ms;
-        for (u32 l = 0; l < ms; l++) acc += mr[l] * double(r[size_t(l) * R + col]);
-        z[i] = T(acc);
+        double acc = 0.0;
+        for (u32 l = lane; l < ms; l += 32) acc += mr[l] * double(r[size_t(l) * R + col]);
+#pragma unroll
+        for (int o = 16; o > 0; o /= 2) acc += __shfl_xor_sync(FULL, acc, o);
+        if (lane == 0) z[i] = T(acc);
     }
 }
 
