@@ -957,9 +957,9 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
     if (d.wpull.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            with_rcp<1>(Rc, S.nb, [&](auto c, auto nbk) {
-                constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
-                k_wpull_apply<T, RCP, NBK><<<GRID_S, WPB * 32, wpull_smem(), st>>>(S, W, d.wpull.set(), P, t, R, j0,
+            with_lanes<1>(Rc, S.nb, [&](auto c, auto nbk) {
+                constexpr int L = decltype(c)::value, NBK = decltype(nbk)::value;
+                k_wpull_apply<T, L, NBK><<<GRID_S, WPB * 32, wpull_smem(), st>>>(S, W, d.wpull.set(), P, t, R, j0,
                                                                                     Rc, Y);
             });
             d.launches++;

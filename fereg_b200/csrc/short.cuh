@@ -13,7 +13,8 @@
 // per cell, segment or entry, into the warp's shared memory. Then every loop runs on all lanes as
 // (group g, column j) pairs: a column chunk of Rc columns is padded to RCP (a power of two), the
 // warp holds G = 32 / RCP groups, and cells and rows are dealt to the groups in turn (cell i to
-// group i mod G). Segment sums: while a lane walks its cells (in order) it keeps a running sum of
+// group i mod G). The operator's coordinate-list pass gives each lane two columns instead (groups
+// of L = lanes_of(Rc) lanes, as the lane groups do). Segment sums: while a lane walks its cells (in order) it keeps a running sum of
 // the current segment and parks it in a lane-private slot when the segment ends; the segment's
 // value is then the sum of its G slots in group order.
 //
@@ -380,22 +381,30 @@ __device__ __forceinline__ void stage_pull(const DevStruct& S, u32 k0, u32 k1, u
 }
 
 // Operator pass 2 on short coordinate lists (k >= ms_acc): Y[k] = nr_k P[k] + sum over the cells
-// c of k of W_c (sum_{other b} P[coord_b(c)] - t_{s(c)}).
-template <class T, int RCP, int NBK>
+// c of k of W_c (sum_{other b} P[coord_b(c)] - t_{s(c)}). Warp tiles of whole lists, staged; the
+// entries are dealt to groups of L lanes (L = lanes_of(Rc)), lane j of a group holding columns j
+// and j + L, and the groups' sums are added in group order.
+template <class T, int L, int NBK>
 __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_apply(DevStruct S, DevWeights W, WarpTiles wt,
                                                              const T* __restrict__ P, const T* __restrict__ t, int R,
                                                              int j0, int Rc, T* __restrict__ Y) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using L_t = Lanes<RCP>;
-    constexpr int G = L_t::G;
+    constexpr int G = 32 / L;
     constexpr int NO = NBK - 1;  // staged other blocks (all of them below WNB blocks)
     const PullStage st = pull_stage_at(smem_raw + size_t(wid_in_cta()) * pull_bytes());
-    const L_t L(Rc);
-    const u32 Ru = u32(R);
+    const u32 lane = wlane(), g = lane / L, j = lane % L;
+    const bool on0 = int(j) < Rc, on1 = int(j) + L < Rc;
+    const size_t Ru = size_t(R);
     const u32 no = S.nb - 1;
     const bool weighted = W.cell_w != nullptr;
-    const T* Pj = P + j0 + L.j;
-    const T* tj = t + j0 + L.j;
+    const T* Pj = P + j0 + j;
+    const T* tj = t + j0 + j;
+    auto total = [&](T v) {  // sum over the groups of the same column, in group order
+        T s = T(0);
+#pragma unroll
+        for (int gg = 0; gg < G; gg++) s += __shfl_sync(FULL, v, gg * L + int(j));
+        return s;
+    };
     const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
     uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
     for (u32 tile = wid; tile < wt.n; tile += nw) {
@@ -406,22 +415,34 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_apply(DevStruct S, DevWei
         u32 i0 = 0;
         for (u32 kl = 0; kl < k1 - k0; kl++) {
             const u32 ie = st.kend[kl];
-            T acc = T(0);
-            if (L.on) {
+            T acc0 = T(0), acc1 = T(0);
 #pragma unroll 8
-                for (u32 i = i0 + L.g; i < ie; i += G) {
-                    T v = -__ldcg(tj + size_t(st.seg[i]) * Ru);
+            for (u32 i = i0 + g; i < ie; i += G) {
+                const T* trow = tj + size_t(st.seg[i]) * Ru;
+                T v0 = on0 ? -__ldcg(trow) : T(0);
+                T v1 = on1 ? -__ldcg(trow + L) : T(0);
 #pragma unroll
-                    for (int o = 0; o < NO; o++) v += Pj[size_t(st.oth[o * PULL_WARP_MAX + i]) * Ru];
-                    if constexpr (NBK == WNB)
-                        for (u32 o = WNO; o < no; o++) v += Pj[size_t(S.pl_other[size_t(e0 + i) * no + o]) * Ru];
-                    acc += weighted ? T(W.cell_w[st.cell[i]]) * v : v;
+                for (int o = 0; o < NO; o++) {
+                    const T* row = Pj + size_t(st.oth[o * PULL_WARP_MAX + i]) * Ru;
+                    if (on0) v0 += row[0];
+                    if (on1) v1 += row[L];
                 }
+                if constexpr (NBK == WNB)
+                    for (u32 o = WNO; o < no; o++) {
+                        const T* row = Pj + size_t(S.pl_other[size_t(e0 + i) * no + o]) * Ru;
+                        if (on0) v0 += row[0];
+                        if (on1) v1 += row[L];
+                    }
+                const T w = weighted ? T(W.cell_w[st.cell[i]]) : T(1);
+                acc0 += w * v0;
+                acc1 += w * v1;
             }
-            acc = group_total(acc, L);
-            if (L.on && L.g == 0) {
-                const size_t o = size_t(k0 + kl) * Ru + j0 + L.j;
-                Y[o] = T(W.nr[k0 + kl]) * P[o] + acc;
+            acc0 = total(acc0);
+            acc1 = total(acc1);
+            if (g == 0) {
+                const size_t o = size_t(k0 + kl) * Ru + j0 + j;
+                if (on0) Y[o] = T(W.nr[k0 + kl]) * P[o] + acc0;
+                if (on1) Y[o + L] = T(W.nr[k0 + kl]) * P[o + L] + acc1;
             }
             i0 = ie;
         }
