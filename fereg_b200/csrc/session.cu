@@ -434,7 +434,29 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
     const double sumw = sumw_;
     d.part.alloc(size_t(ST_GRID) * r * 6);
     d.sums.alloc(r * 6);
-    for (int j0 = 0; j0 < R; j0 += 32) {
+    d.err.alloc(1);
+    CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), st));
+    // whole rows through shared memory by bulk copies when the block starts on a 16-byte boundary
+    const bool bulk = R <= 32 && reinterpret_cast<uintptr_t>(rows) % 16 == 0 && n >= size_t(CS_ROWS) * ST_GRID;
+    if (bulk) {
+        const size_t shm = size_t(CS_STAGES) * CS_ROWS * r * sizeof(double);
+        // the limit is a process-wide attribute: always the same value, the ring at R = 32
+        const int most = CS_STAGES * CS_ROWS * 32 * int(sizeof(double));
+        auto run = [&](auto kernel) {
+            CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+            kernel<<<ST_GRID, ST_TB, shm, st>>>(rows, n, R, wr, d.part.p, d.err.p);
+        };
+        switch (rcp_of(R)) {
+            case 1: run(k_colstats_bulk<1>); break;
+            case 2: run(k_colstats_bulk<2>); break;
+            case 4: run(k_colstats_bulk<4>); break;
+            case 8: run(k_colstats_bulk<8>); break;
+            case 16: run(k_colstats_bulk<16>); break;
+            default: run(k_colstats_bulk<32>); break;
+        }
+        d.launches++;
+    }
+    for (int j0 = 0; j0 < R && !bulk; j0 += 32) {
         const int Rc = std::min(32, R - j0);
         switch (rcp_of(Rc)) {
             case 1: k_colstats1<1><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
@@ -449,9 +471,12 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
     k_sum_parts<<<sum_parts_blocks(R * 6), 256, 0, st>>>(d.part.p, ST_GRID, R * 6, d.sums.p);
     d.launches++;
     std::vector<double> s1(r * 6), c0(r);
+    int late = 0;
     CK(cudaMemcpyAsync(s1.data(), d.sums.p, r * 6 * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(c0.data(), rows, r * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&late, d.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (late) throw Error(RC_INTERNAL, "fereg: a bulk copy of the column statistics did not complete");
     ColStats cs;
     cs.wmean.resize(r);
     cs.sumsq.resize(r);

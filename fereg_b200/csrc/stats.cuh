@@ -14,6 +14,7 @@
 
 #include <cstdint>
 
+#include "bulk.cuh"
 #include "device.cuh"
 #include "scan.cuh"
 
@@ -404,6 +405,95 @@ __global__ void __launch_bounds__(ST_TB, 4) k_colstats1(const double* __restrict
         for (int wp = 0; wp < ST_TB / 32; wp++)
             for (int gg = 0; gg < G; gg++) t += red[wp][gg * RCP + col][v];
         part[(size_t(blockIdx.x) * R + j0 + col) * NV + v] = t;
+    }
+}
+
+// The same statistics of all R <= 32 columns, the block streamed through shared memory by bulk
+// copies: CTA b takes the chunks of CS_ROWS whole rows b, b + grid, ... into a ring of CS_STAGES
+// buffers, thread 0 issuing the copies (one mbarrier per buffer, its phase expecting the chunk's
+// bytes) and every thread reading a buffer once its phase completes; lanes are (group, column)
+// pairs over the buffer's rows. CTA 0 reads the rows past the last whole chunk directly. A wait
+// that runs out (never expected) sets *err; the CTA then waits, bounded, for its copies in flight
+// and returns without writing its partial. The block must start on a 16-byte boundary (each chunk
+// is 1024 R bytes).
+constexpr int CS_ROWS = 128, CS_STAGES = 4;
+template <int RCP>
+__global__ void __launch_bounds__(ST_TB, 4) k_colstats_bulk(const double* __restrict__ rows, size_t n, int R,
+                                                          const double* __restrict__ w, double* __restrict__ part,
+                                                          int* __restrict__ err) {
+    constexpr int G = 32 / RCP, NV = 6, NWARP = ST_TB / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) u64 bar[CS_STAGES];
+    __shared__ double red[NWARP][32][NV];
+    double* buf = reinterpret_cast<double*>(smem_raw);  // CS_STAGES x CS_ROWS x R
+    const u32 chunk = u32(CS_ROWS) * u32(R);
+    const size_t nchunks = n / CS_ROWS;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / RCP, j = lane % RCP;
+    const bool on = j < R;
+    const double c = on ? rows[j] : 0.0;
+    double a[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) a[v] = 0.0;
+    auto add = [&](double x, double wv) {
+        const double d = x - c;
+        a[0] += d;
+        a[1] += d * d;
+        a[2] += wv * d;
+        a[3] += wv * d * d;
+        a[4] += x * x;
+        a[5] += wv * x * x;
+    };
+    const size_t mine = blockIdx.x < nchunks ? (nchunks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    auto issue = [&](size_t i) {  // thread 0: chunk i of this CTA into buffer i mod CS_STAGES
+        const int sb = int(i % CS_STAGES);
+        const size_t q = blockIdx.x + i * gridDim.x;
+        mbar_expect_tx(&bar[sb], chunk * 8u);
+        bulk_load(buf + size_t(sb) * chunk, rows + q * chunk, chunk * 8u, &bar[sb]);
+    };
+    if (threadIdx.x == 0) {
+        for (int sb = 0; sb < CS_STAGES; sb++) mbar_init(&bar[sb], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (size_t i = 0; i < mine && i < size_t(CS_STAGES); i++) issue(i);
+    size_t failed = mine;
+    for (size_t i = 0; i < mine; i++) {
+        const int sb = int(i % CS_STAGES);
+        const bool late = !mbar_wait(&bar[sb], u32((i / CS_STAGES) & 1), MBAR_WAIT_LIMIT);
+        if (__syncthreads_or(late)) {
+            failed = i;
+            break;
+        }
+        const double* cb = buf + size_t(sb) * chunk;
+        const size_t r0 = (blockIdx.x + i * gridDim.x) * CS_ROWS;
+        if (on)
+            for (int rr = warp * G + g; rr < CS_ROWS; rr += NWARP * G) add(cb[rr * R + j], w ? w[r0 + rr] : 1.0);
+        __syncthreads();  // every thread is done with buffer sb
+        if (threadIdx.x == 0 && i + CS_STAGES < mine) issue(i + CS_STAGES);
+    }
+    if (failed < mine) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            for (size_t i = failed; i < mine && i < failed + CS_STAGES; i++)
+                mbar_wait(&bar[i % CS_STAGES], u32((i / CS_STAGES) & 1), MBAR_WAIT_LIMIT);
+        }
+        __syncthreads();
+        return;
+    }
+    if (blockIdx.x == 0 && on)
+        for (size_t r = nchunks * CS_ROWS + size_t(warp * G + g); r < n; r += NWARP * G)
+            add(rows[r * R + j], w ? w[r] : 1.0);
+#pragma unroll
+    for (int v = 0; v < NV; v++) red[warp][lane][v] = on ? a[v] : 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < R * NV; i += ST_TB) {
+        const int col = i / NV, v = i % NV;
+        double t = 0.0;
+        for (int wp = 0; wp < NWARP; wp++)
+            for (int gg = 0; gg < G; gg++) t += red[wp][gg * RCP + col][v];
+        part[(size_t(blockIdx.x) * R + col) * NV + v] = t;
     }
 }
 
