@@ -364,17 +364,40 @@ std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, 
         d.sums.alloc(size_t(len));
         OpSpec sp{src, nrows, srcR, d.col.p, shift ? d.shift.p : nullptr, k, cst ? 1 : 0, msz, om, perm, 0, 0,
                   ssq ? 1 : 0};
-        switch ((msz + 7) / 8) {
-            case 1: k_outer_mma<1><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
-            case 2: k_outer_mma<2><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
-            case 3: k_outer_mma<3><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
-            default: k_outer_mma<4><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+        // a contiguous block on a 16-byte boundary streams through shared memory by bulk copies
+        const bool bulk = !perm && srcR <= 32 && reinterpret_cast<uintptr_t>(src) % 16 == 0 &&
+                          nrows >= size_t(CS_ROWS) * ST_GRID;
+        d.err.alloc(1);
+        if (bulk) {
+            CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), st));
+            const size_t shm = size_t(CS_STAGES) * CS_ROWS * size_t(srcR) * sizeof(double);
+            const int most = CS_STAGES * CS_ROWS * 32 * int(sizeof(double));  // process-wide: always the same
+            auto run = [&](auto kernel) {
+                CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+                kernel<<<ST_GRID, ST_TB, shm, st>>>(sp, d.part.p, d.err.p);
+            };
+            switch ((msz + 7) / 8) {
+                case 1: run(k_outer_mma_bulk<1>); break;
+                case 2: run(k_outer_mma_bulk<2>); break;
+                case 3: run(k_outer_mma_bulk<3>); break;
+                default: run(k_outer_mma_bulk<4>); break;
+            }
+        } else {
+            switch ((msz + 7) / 8) {
+                case 1: k_outer_mma<1><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+                case 2: k_outer_mma<2><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+                case 3: k_outer_mma<3><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+                default: k_outer_mma<4><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
+            }
         }
         k_sum_parts<<<sum_parts_blocks(len), 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
         d.launches += 2;
         std::vector<double> h(len);
+        int late = 0;
         CK(cudaMemcpyAsync(h.data(), d.sums.p, size_t(len) * 8, cudaMemcpyDeviceToHost, st));
+        if (bulk) CK(cudaMemcpyAsync(&late, d.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (late) throw Error(RC_INTERNAL, "fereg: a bulk copy of the outer products did not complete");
         for (int a = 0; a < msz; a++)
             for (int b = a; b < msz; b++) m[size_t(a) * msz + b] = m[size_t(b) * msz + a] = h[size_t(a) * msz + b];
         if (ss_out) *ss_out = std::vector<double>(h.begin() + msz * msz, h.end());

@@ -22,6 +22,8 @@ namespace fereg {
 
 constexpr int ST_TB = 256;          // threads per CTA of the stats passes
 constexpr int ST_GRID = 148 * 4;    // CTAs of the row passes (4 per SM: 32 warps)
+// Rows per chunk and chunks in flight per CTA of the passes that stream the block by bulk copies
+constexpr int CS_ROWS = 128, CS_STAGES = 4;
 constexpr int OP_ROWS = 32;         // rows staged per tile of the outer-product pass
 constexpr int OP_PPT = 8;           // pairs per thread of one outer-product launch
 constexpr int OP_MAXP = ST_TB * OP_PPT;  // pairs of one launch
@@ -358,6 +360,154 @@ __global__ void __launch_bounds__(ST_TB, NB <= 2 ? 4 : 2) k_outer_mma(OpSpec s, 
         part[size_t(blockIdx.x) * len + i] = i < mm ? red[(i / s.msz) * W + i % s.msz] : red[W * W + (i - mm)];
 }
 
+// k_outer_mma with the rows streamed through shared memory by bulk copies (the ring of
+// k_colstats_bulk, whose constants it uses): for a contiguous block (no permutation), R <= 32
+// columns, starting on a 16-byte boundary. A chunk of CS_ROWS rows is one MMA step of every warp
+// (16 rows each); CTA 0 takes the rows past the last whole chunk by direct loads. A wait that runs
+// out sets *err and the CTA returns after its copies in flight, without writing its partial.
+template <int NB>
+__global__ void __launch_bounds__(ST_TB, NB <= 2 ? 3 : 2) k_outer_mma_bulk(OpSpec s, double* __restrict__ part,
+                                                                          int* __restrict__ err) {
+    constexpr int NT = NB * (NB + 1) / 2, U = 4, W = 8 * NB, NWARP = ST_TB / 32;
+    static_assert(NWARP * U * 4 == CS_ROWS, "one MMA step of every warp per chunk");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) u64 bar[CS_STAGES];
+    __shared__ double red[W * W + W];
+    double* buf = reinterpret_cast<double*>(smem_raw);  // CS_STAGES x CS_ROWS x R
+    const int R = s.R;
+    const u32 chunk = u32(CS_ROWS) * u32(R);
+    const size_t nchunks = s.n / CS_ROWS;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int kr = lane & 3, cj = lane >> 2;
+    int csrc[NB];
+    double csh[NB];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        const int c = 8 * b + cj;
+        csrc[b] = c < s.k ? s.col[c] : (c < s.msz ? -1 : -2);
+        csh[b] = (c < s.k && s.shift) ? s.shift[c] : 0.0;
+    }
+    for (int i = threadIdx.x; i < W * W + W; i += ST_TB) red[i] = 0.0;
+    double acc[NT][2];
+#pragma unroll
+    for (int t = 0; t < NT; t++) acc[t][0] = acc[t][1] = 0.0;
+    double sq[NB];
+#pragma unroll
+    for (int b = 0; b < NB; b++) sq[b] = 0.0;
+    auto mma_step = [&](const double (&v)[U][NB], const double (&om)[U]) {
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (s.ssq) {
+#pragma unroll
+                for (int b = 0; b < NB; b++) {
+                    const double x = csrc[b] >= 0 ? v[u][b] - csh[b] : 0.0;
+                    sq[b] += x * x;
+                }
+            }
+            int t = 0;
+#pragma unroll
+            for (int bi = 0; bi < NB; bi++) {
+                const double a = om[u] * v[u][bi];
+#pragma unroll
+                for (int bj = bi; bj < NB; bj++, t++) dmma884(acc[t][0], acc[t][1], a, v[u][bj]);
+            }
+        }
+    };
+    const size_t mine = blockIdx.x < nchunks ? (nchunks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    auto issue = [&](size_t i) {  // thread 0: chunk i of this CTA into buffer i mod CS_STAGES
+        const int sb = int(i % CS_STAGES);
+        const size_t q = blockIdx.x + i * gridDim.x;
+        mbar_expect_tx(&bar[sb], chunk * 8u);
+        bulk_load(buf + size_t(sb) * chunk, s.rows + q * chunk, chunk * 8u, &bar[sb]);
+    };
+    if (threadIdx.x == 0) {
+        for (int sb = 0; sb < CS_STAGES; sb++) mbar_init(&bar[sb], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (size_t i = 0; i < mine && i < size_t(CS_STAGES); i++) issue(i);
+    size_t failed = mine;
+    for (size_t i = 0; i < mine; i++) {
+        const int sb = int(i % CS_STAGES);
+        const bool late = !mbar_wait(&bar[sb], u32((i / CS_STAGES) & 1), MBAR_WAIT_LIMIT);
+        if (__syncthreads_or(late)) {
+            failed = i;
+            break;
+        }
+        const double* cb = buf + size_t(sb) * chunk;
+        const size_t r0 = (blockIdx.x + i * gridDim.x) * CS_ROWS;
+        double v[U][NB], om[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int rr = warp * (U * 4) + u * 4 + kr;
+            om[u] = s.om ? s.om[r0 + rr] : 1.0;
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+                v[u][b] = csrc[b] >= 0 ? cb[rr * R + csrc[b]] + csh[b] : (csrc[b] == -1 ? 1.0 : 0.0);
+        }
+        mma_step(v, om);
+        __syncthreads();  // every thread is done with buffer sb
+        if (threadIdx.x == 0 && i + CS_STAGES < mine) issue(i + CS_STAGES);
+    }
+    if (failed < mine) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            for (size_t i = failed; i < mine && i < failed + CS_STAGES; i++)
+                mbar_wait(&bar[i % CS_STAGES], u32((i / CS_STAGES) & 1), MBAR_WAIT_LIMIT);
+        }
+        __syncthreads();
+        return;
+    }
+    if (blockIdx.x == 0)  // the rows past the last whole chunk (a whole warp per base: MMA is warp-wide)
+        for (size_t base = nchunks * CS_ROWS + size_t(warp) * U * 4; base < s.n; base += size_t(NWARP) * U * 4) {
+            double v[U][NB], om[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const size_t r = base + size_t(u) * 4 + kr;
+                om[u] = 0.0;
+#pragma unroll
+                for (int b = 0; b < NB; b++) v[u][b] = 0.0;
+                if (r < s.n) {
+                    om[u] = s.om ? s.om[r] : 1.0;
+#pragma unroll
+                    for (int b = 0; b < NB; b++)
+                        v[u][b] = csrc[b] >= 0 ? s.rows[r * R + csrc[b]] + csh[b] : (csrc[b] == -1 ? 1.0 : 0.0);
+                }
+            }
+            mma_step(v, om);
+        }
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        double q = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) q += __shfl_sync(FULL, sq[b], (cj << 2) + k);
+        sq[b] = q;
+    }
+    __syncthreads();
+    for (int w = 0; w < NWARP; w++) {
+        if (warp == w) {
+            int t = 0;
+#pragma unroll
+            for (int bi = 0; bi < NB; bi++)
+#pragma unroll
+                for (int bj = bi; bj < NB; bj++, t++) {
+                    const int rr = 8 * bi + cj, cc = 8 * bj + 2 * kr;
+                    red[rr * W + cc] += acc[t][0];
+                    red[rr * W + cc + 1] += acc[t][1];
+                }
+            if (kr == 0)
+#pragma unroll
+                for (int b = 0; b < NB; b++) red[W * W + 8 * b + cj] += sq[b];
+        }
+        __syncthreads();
+    }
+    const int mm = s.msz * s.msz;
+    const int len = mm + (s.ssq ? s.k : 0);
+    for (int i = threadIdx.x; i < len; i += ST_TB)
+        part[size_t(blockIdx.x) * len + i] = i < mm ? red[(i / s.msz) * W + i % s.msz] : red[W * W + (i - mm)];
+}
+
 // Column statistics in one pass, about a shift c per column (the column's first value):
 // [sum (x-c), sum (x-c)^2, sum w (x-c), sum w (x-c)^2, sum x^2, sum w x^2] per column; the means
 // and the sums of squares about them follow exactly up to rounding (m2 = S2 - S1^2 / n).
@@ -416,7 +566,6 @@ __global__ void __launch_bounds__(ST_TB, 4) k_colstats1(const double* __restrict
 // that runs out (never expected) sets *err; the CTA then waits, bounded, for its copies in flight
 // and returns without writing its partial. The block must start on a 16-byte boundary (each chunk
 // is 1024 R bytes).
-constexpr int CS_ROWS = 128, CS_STAGES = 4;
 template <int RCP>
 __global__ void __launch_bounds__(ST_TB, 4) k_colstats_bulk(const double* __restrict__ rows, size_t n, int R,
                                                           const double* __restrict__ w, double* __restrict__ part,
