@@ -269,12 +269,12 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
     hs_ = build_structure(codes, g, n, SMALL_LIMIT);
     norm_fe1_ = fe1_index(g);
     ctx_.check();
-    {
+    if (ctx_.priority_level < 0) {
+        CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    } else {
         int least = 0, greatest = 0;
         CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        const int above_least = std::max(greatest, least - 1);
-        const int prio = ctx_.priority_level < 0 ? above_least
-                                                 : std::min(above_least, greatest + ctx_.priority_level);
+        const int prio = std::min(std::max(greatest, least - 1), greatest + ctx_.priority_level);
         CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio));
     }
     AllocScope alloc_scope(stream_);
@@ -852,25 +852,13 @@ void GpuAbsorber::build_small_device() {
 
 namespace {
 
-// Lets `kernel` take `bytes` of dynamic shared memory (beyond the 48 KB default). The limit is a
-// per-kernel attribute shared by every thread and stream of the process, so it is always set to
-// the same value, the most the kernel can take (the per-block opt-in maximum less its static
-// shared memory): concurrent sessions that need different amounts then never lower the limit
-// under one another's launches.
+// Lets `kernel` take `bytes` of dynamic shared memory (static and dynamic together may pass the
+// 48 KB default) through smem_limit (device.cuh): set once per kernel, to the most it can take.
 template <class K>
 void allow_smem(K kernel, size_t bytes) {
-    if (bytes <= 48 * 1024) return;
-    static const int optin = [] {
-        int dev = 0, v = 0;
-        CK(cudaGetDevice(&dev));
-        CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        return v;
-    }();
-    cudaFuncAttributes fa;
-    CK(cudaFuncGetAttributes(&fa, kernel));
-    const int lim = optin - int(fa.sharedSizeBytes);
-    if (bytes > size_t(lim)) throw Error(RC_INTERNAL, "fereg: a kernel needs more shared memory than a block can take");
-    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    if (bytes == 0) return;
+    if (bytes > size_t(smem_limit(kernel)))
+        throw Error(RC_INTERNAL, "fereg: a kernel needs more shared memory than a block can take");
 }
 
 // Grounded LDL^T of the k x k row-major `a` (lower triangle read, overwritten) and its inverse

@@ -19,9 +19,9 @@ struct Ctx {
     void* log_data = nullptr;
     int verbose = 0;
     // Scheduling level of the absorber's stream: 0 the device's highest stream priority, each step
-    // one lower (clamped above the lowest, which side passes take); -1 the level just above the
-    // lowest. The serving engine gives small requests the high levels, so that their short kernels
-    // are not queued behind the large requests' passes.
+    // one lower (clamped above the lowest, which side passes take); -1 a stream of the default
+    // priority. The serving engine gives small requests the high levels, so that their short
+    // kernels are not queued behind the large requests' passes.
     int priority_level = -1;
     void check() const {
         if (interrupt && interrupt(interrupt_data)) throw Error(RC_INTERRUPTED, "--Break--");

@@ -1,6 +1,10 @@
 // Device helpers: error checks, buffers, warp lane layouts.
 #pragma once
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -89,6 +93,30 @@ struct DBuf {
     }
     void upload(const std::vector<T>& h, cudaStream_t st) { upload(h.data(), h.size(), st); }
 };
+
+// Raises a kernel's dynamic-shared-memory limit to the most a block can take (the per-block
+// opt-in maximum less the kernel's static shared memory), once per kernel and device, and
+// returns that limit. The limit is a process-wide attribute: it is always set to the same value,
+// so concurrent sessions never lower it under one another, and later calls cost no driver call.
+template <class K>
+inline int smem_limit(K kernel) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> lim;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = lim.find(key);
+    if (it != lim.end()) return it->second;
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, kernel));
+    const int v = optin - int(fa.sharedSizeBytes);
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, v));
+    lim.emplace(key, v);
+    return v;
+}
 
 constexpr unsigned FULL = 0xffffffffu;
 

@@ -371,9 +371,9 @@ std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, 
         if (bulk) {
             CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), st));
             const size_t shm = size_t(CS_STAGES) * CS_ROWS * size_t(srcR) * sizeof(double);
-            const int most = CS_STAGES * CS_ROWS * 32 * int(sizeof(double));  // process-wide: always the same
             auto run = [&](auto kernel) {
-                CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+                if (shm > size_t(smem_limit(kernel)))  // static + dynamic can pass 48 KB: always raise it
+                    throw Error(RC_INTERNAL, "fereg: the outer-product ring does not fit shared memory");
                 kernel<<<ST_GRID, ST_TB, shm, st>>>(sp, d.part.p, d.err.p);
             };
             switch ((msz + 7) / 8) {
@@ -463,10 +463,9 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
     const bool bulk = R <= 32 && reinterpret_cast<uintptr_t>(rows) % 16 == 0 && n >= size_t(CS_ROWS) * ST_GRID;
     if (bulk) {
         const size_t shm = size_t(CS_STAGES) * CS_ROWS * r * sizeof(double);
-        // the limit is a process-wide attribute: always the same value, the ring at R = 32
-        const int most = CS_STAGES * CS_ROWS * 32 * int(sizeof(double));
         auto run = [&](auto kernel) {
-            CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+            if (shm > size_t(smem_limit(kernel)))  // static + dynamic can pass 48 KB: always raise it
+                throw Error(RC_INTERNAL, "fereg: the column statistics ring does not fit shared memory");
             kernel<<<ST_GRID, ST_TB, shm, st>>>(rows, n, R, wr, d.part.p, d.err.p);
         };
         switch (rcp_of(R)) {
