@@ -857,8 +857,8 @@ def phase_bytes(info, n, R, weighted, s_v=8):
 
 
 PHASE_KERNEL = {"rhs_seg": "k_grhs", "rhs_pull": "k_wpull_rhs", "apply_seg": "k_gseg_apply",
-                "apply_pull": "k_wpull_apply", "residualize": "k_wresid", "colstats": "k_colstats1",
-                "gram": "k_outer_mma", "variance": "k_resid_e"}
+                "apply_pull": "k_wpull_apply", "residualize": "k_wresid", "colstats": "k_colstats_bulk",
+                "gram": "k_outer_mma_bulk", "variance": "k_resid_e"}
 
 
 def dist_setup():
