@@ -169,6 +169,7 @@ def _setup(L):
     L.fereg_session_iv.argtypes = [P, P, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(IvSpec),
                                    C.POINTER(IvOut)]
     L.fereg_amg_probe.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, C.c_int, u32p, u32p, u64p, f64p]
+    L.fereg_structure_digest.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, u64p]
     L.fereg_factorize.argtypes = [f64p, C.c_size_t, u32p, u32p]
     L.fereg_combine.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, u32p, u32p]
     L.fereg_drop_singletons.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, f64p, f64p, C.c_int, C.c_int,
@@ -660,6 +661,19 @@ def prepare(factors, absorb, fw=None, y=None, family=None, singletons=True):
         alive, s, f = np.ones(len(factors[0]), dtype=bool), 0, 0
     kept = [restrict(c, g, alive) for c, g in terms]
     return dict(alive=alive, num_singletons=s, fe_separated=f, terms=kept)
+
+
+def structure_digest(codes, g):
+    """Host-only test hook: counts of the cell structure a session would build (cells, segments,
+    reduced coordinates, small coordinates, blocks, FE1 index) and a digest of its arrays and
+    coordinate lists."""
+    arrs = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
+    ptrs = (u32p * len(arrs))(*[_p(a, u32p) for a in arrs])
+    garr = np.asarray(g, dtype=np.uint32)
+    out = np.zeros(7, dtype=np.uint64)
+    _check(lib().fereg_structure_digest(ptrs, _p(garr, u32p), len(arrs), len(arrs[0]), _p(out, u64p)))
+    keys = ["cells", "segments", "m", "m_small", "blocks", "fe1", "digest"]
+    return {k: int(v) for k, v in zip(keys, out)}
 
 
 def amg_probe(codes, g, max_levels=16):

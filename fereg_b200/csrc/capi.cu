@@ -610,6 +610,34 @@ int fereg_restrict(const uint32_t* codes, uint32_t g, const uint8_t* alive, size
     });
 }
 
+int fereg_structure_digest(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, uint64_t* out) {
+    return guard([&] {
+        if (!codes || !g || nterms < 1 || !out) throw Error(RC_INVALID_INPUT, "fereg_structure_digest: NULL argument");
+        std::vector<const u32*> c(codes, codes + nterms);
+        std::vector<u32> gg(g, g + nterms);
+        const HostStructure hs = build_structure(c, gg, n, SMALL_LIMIT);
+        const PullTable pt = build_pull_table(hs);
+        u64 h = 1469598103934665603ull;  // FNV-1a over the 32-bit words, array by array
+        auto mix = [&](const std::vector<u32>& v) {
+            for (u32 x : v) {
+                h ^= x;
+                h *= 1099511628211ull;
+            }
+            h ^= v.size();
+            h *= 1099511628211ull;
+        };
+        for (const auto* v : {&hs.pi, &hs.seg_off, &hs.cell_row, &hs.coord, &pt.off, &pt.cell, &pt.seg, &pt.other})
+            mix(*v);
+        out[0] = hs.ncells;
+        out[1] = hs.g1;
+        out[2] = hs.m;
+        out[3] = hs.m_small;
+        out[4] = hs.nb();
+        out[5] = u64(int64_t(hs.fe1));
+        out[6] = h;
+    });
+}
+
 int fereg_amg_probe(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, int max_levels,
                     uint32_t* levels, uint32_t* sizes, uint64_t* nnz, double* row_sum) {
     return guard([&] {

@@ -285,6 +285,13 @@ int fereg_session_poisson(fereg_session* s, double* rows, int rows_on_device, si
 int fereg_amg_probe(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, int max_levels,
                     uint32_t* levels, uint32_t* sizes, uint64_t* nnz, double* row_sum);
 
+/* Test hook, host only (no device): the cell structure (structure.rs:247-527) and coordinate lists
+ * that a session would build for the given terms, as counts (out[0..5]: cells, segments, reduced
+ * coordinates, small coordinates, blocks, FE1 index) and a 64-bit FNV-1a digest of the row order,
+ * segment offsets, first rows, cell coordinates and coordinate lists (out[6]). The host build is
+ * parallel; the digest shows it does not depend on the thread count. */
+int fereg_structure_digest(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, uint64_t* out);
+
 /* Sample preparation on the device (Session::prepare's FE-id compression and sample drops;
  * host arrays in and out). Bit-exact with the reference's definitions.
  * fereg_factorize: factor.rs:38, dense codes in ascending value order (-0 = +0; NaN: 198).
