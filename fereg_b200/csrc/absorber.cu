@@ -100,10 +100,10 @@ void with_nbk(u32 nb, F&& f) {
         default: f(integral_constant<int, RCP>{}, integral_constant<int, WNB>{}); break;
     }
 }
-// Lane groups of L = lanes_of(Rc) lanes, two columns per lane.
+// Lane groups of L lanes (lanes_of(Rc) by default: two columns per lane).
 template <int MIN_NBK = 0, class F>
-void with_lanes(int Rc, u32 nb, F&& f) {
-    switch (lanes_of(Rc)) {
+void with_lanes(int Rc, u32 nb, F&& f, int L = 0) {
+    switch (L > 0 ? L : lanes_of(Rc)) {
         case 1: with_nbk<1, MIN_NBK>(nb, f); break;
         case 2: with_nbk<2, MIN_NBK>(nb, f); break;
         case 4: with_nbk<4, MIN_NBK>(nb, f); break;
@@ -945,11 +945,16 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
     if (d.wpull.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            with_lanes<1>(Rc, S.nb, [&](auto c, auto nbk) {
-                constexpr int L = decltype(c)::value, NBK = decltype(nbk)::value;
-                k_wpull_apply<T, L, NBK><<<GRID_S, WPB * 32, wpull_smem(), st>>>(S, W, d.wpull.set(), P, t, R, j0,
-                                                                                    Rc, Y);
-            });
+            // up to 4 columns one column per lane (groups of rcp_of(Rc)): narrower groups of two
+            // columns measured slower there
+            with_lanes<1>(
+                Rc, S.nb,
+                [&](auto c, auto nbk) {
+                    constexpr int L = decltype(c)::value, NBK = decltype(nbk)::value;
+                    k_wpull_apply<T, L, NBK><<<GRID_S, WPB * 32, wpull_smem(), st>>>(S, W, d.wpull.set(), P, t, R,
+                                                                                        j0, Rc, Y);
+                },
+                Rc <= 4 ? rcp_of(Rc) : 0);
             d.launches++;
         }
     if (S.pull.n) {
