@@ -811,14 +811,18 @@ void GpuAbsorber::build_small_device() {
     DBuf<double> part, a, ak, dd, dx, dscale;
     DBuf<u32> dkeep;
     a.alloc(len);
-    part.alloc(size_t(d.sr_n) * ms);
-    const size_t shm = size_t(8) * ms * sizeof(double);
-    allow_smem(k_small_rows, shm);
-    k_small_rows<<<(d.sr_n + 7) / 8, 256, shm, stream_>>>(d.seg_off.p, d.coord.p, u32(M), ns, u32(ms), d.cell_w.p,
-                                                           d.n1inv.p, d.pl_cell.p, d.pl_seg.p, d.sr_k.p, d.sr_a.p,
-                                                           d.sr_b.p, d.sr_n, part.p);
-    k_small_rows_sum<<<u32(ms), 256, 0, stream_>>>(part.p, d.sr_first.p, u32(ms), a.p);
-    d.launches += 2;
+    if (d.sr_n > 0) {
+        part.alloc(size_t(d.sr_n) * ms);
+        const size_t shm = size_t(8) * ms * sizeof(double);
+        allow_smem(k_small_rows, shm);
+        k_small_rows<<<(d.sr_n + 7) / 8, 256, shm, stream_>>>(d.seg_off.p, d.coord.p, u32(M), ns, u32(ms),
+                                                               d.cell_w.p, d.n1inv.p, d.pl_cell.p, d.pl_seg.p,
+                                                               d.sr_k.p, d.sr_a.p, d.sr_b.p, d.sr_n, part.p);
+        k_small_rows_sum<<<u32(ms), 256, 0, stream_>>>(part.p, d.sr_first.p, u32(ms), a.p);
+        d.launches += 2;
+    } else {  // no small coordinate has a cell
+        CK(cudaMemsetAsync(a.p, 0, len * sizeof(double), stream_));
+    }
     // kept coordinates (not redundant, positive diagonal) and their unit-diagonal scaling
     std::vector<double> diag(ms);
     std::vector<uint8_t> red(ms);
