@@ -231,6 +231,11 @@ std::future<GpuSession::Dof> GpuSession::dof_begin(bool clusters, bool firstpair
     CK(cudaStreamWaitEvent(s.st.s, s.ready, 0));
     int dev = 0;
     CK(cudaGetDevice(&dev));
+    for (cudaEvent_t* e : {&s.ta, &s.tb})  // left by a call that threw before joining its pass
+        if (*e) {
+            d.pool.push_back(*e);
+            *e = nullptr;
+        }
     cudaEvent_t ta = nullptr, tb = nullptr;
     if (d.prof) {
         ta = d.event();
