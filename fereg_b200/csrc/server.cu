@@ -22,7 +22,20 @@ u64 request_bytes(const ServeRequest& r) {
     const u64 per_row = R * 8 * blocks + 4 * (3 * nt + 3 * nc + 6) + 8 * (r.model >= 2 ? 12 : 6);
     u64 levels = 0;
     for (u32 x : r.g) levels += x;
-    return n * per_row + levels * R * 8 * 10 + (32ull << 20);
+    // the dense small super-block (the smallest terms besides FE1 up to SMALL_LIMIT levels, when
+    // at most 1024 coordinates): factor, its work arrays and inverse (4 ms^2 doubles) and the
+    // partial rows of its assembly (at most 4096 + ms rows of ms doubles)
+    std::vector<u32> others(r.g.begin(), r.g.end());
+    const int f1 = fe1_index(r.g);
+    if (f1 >= 0) others.erase(others.begin() + f1);
+    std::sort(others.begin(), others.end());
+    u64 ms = 0;
+    for (u32 x : others) {
+        if (ms + x > SMALL_LIMIT) break;
+        ms += x;
+    }
+    const u64 dense = ms > 0 && ms <= 1024 ? (4 * ms * ms + (4096 + ms) * ms) * 8 : 0;
+    return n * per_row + levels * R * 8 * 10 + dense + (32ull << 20);
 }
 
 Server::Server(int workers, u64 budget, bool dry_run) : dry_(dry_run), t0_(std::chrono::steady_clock::now()) {
