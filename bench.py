@@ -707,9 +707,9 @@ def workload_name(cfg_name):
 
 
 class ClockSampler:
-    """SM clocks and throttle reasons sampled during the timed region: through NVML every 20 ms
-    (so that a timed region of a few tens of milliseconds still holds samples), else nvidia-smi
-    every 200 ms. Read-only queries; no GPU setting is changed."""
+    """SM clocks and throttle reasons sampled during the timed region: through NVML every 5 ms
+    (so that a timed region of a few tens of milliseconds still holds several samples), else
+    nvidia-smi every 200 ms. Read-only queries; no GPU setting is changed."""
 
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
@@ -765,7 +765,7 @@ class ClockSampler:
                 self.samples.append((float(sm), float(smax), {n for n, b in zip(self.NAMES, bits) if r & b}))
             except Exception:
                 pass
-            if self.stop.wait(0.02):
+            if self.stop.wait(0.005):
                 break
 
     def _read(self):
