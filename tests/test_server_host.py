@@ -87,3 +87,17 @@ def test_dry_run_needs_a_budget():
     with pytest.raises(fb.FeregError) as e:
         fb.Server(workers=1, hbm_budget=None, dry_run=True)
     assert e.value.rc == 198
+
+
+def test_estimate_counts_the_dense_small_block():
+    """A request whose small super-block gets the dense factor (900 coordinates <= 1024) is
+    estimated ~62 MB above one whose small block is too large for it (1100 coordinates): the
+    factor, its work arrays and inverse (4 ms^2 doubles) and the assembly rows ((4096 + ms) ms)."""
+    srv = fb.Server(workers=1, hbm_budget=1 << 40, dry_run=True)
+    est = {}
+    for levels in (900, 1100):
+        t = srv.submit("ols", CODES * 2, [5000, levels], COLS, 2, n=100_000, dry_run_us=0)
+        est[levels] = srv.wait(t)["bytes"]
+    srv.close()
+    dense = (4 * 900 * 900 + (4096 + 900) * 900) * 8
+    assert est[900] - est[1100] == dense - 200 * 3 * 8 * 10
