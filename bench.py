@@ -38,6 +38,10 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     # OLS y ~ x1..x10 | indiv + firm + year, n = 1e6 indiv x 10 years, firm = row mod 1e5.
     "c2": dict(n_ind=1_000_000, years=10, n_firm=100_000, k=10, seed=10**7 * 100 + 43),
+    # The same OLS on the connected "difficult" firm graph of the reference's benchmark DGP
+    # (bench/dgp.py:55,70): n_ind / 23 = 43,478 firms, firm = row mod 43,478. 43,478 is not a
+    # multiple of 10, so the individuals' runs of 10 consecutive firms wrap into one ring.
+    "c2d": dict(n_ind=1_000_000, years=10, n_firm=43_478, k=10, seed=10**7 * 100 + 47),
     # OLS y ~ x1 | indiv + year, n = 1e4 indiv x 10 years.
     "c1": dict(n_ind=10_000, years=10, n_firm=0, k=1, seed=10**5 * 100 + 42),
     # WCR11 wild cluster bootstrap of b_x1 (H0 true): y ~ x1 | indiv + year + firm, cluster firm,
@@ -146,13 +150,15 @@ GLM_METRIC = "sec/call (Poisson PML, n=9.95e6, exporter#year + importer#year + p
 
 
 def run_glm(args, cfg, rank, world, local, pg):
-    """C4: one PPML IRLS call per step (seconds per call)."""
+    """C4: one PPML IRLS call per step (seconds per call). Every call, timed or not, runs on a
+    fresh session (prepared outside the timed events), so no preconditioner, hierarchy or IRLS
+    state of an earlier call carries over."""
     codes, g, rows = make_gravity_data(cfg)
     n = rows.shape[0]
     if args.impl == "reference":
         if rank != 0:
             return
-        cpu = glm_cpu_sample(codes, g, rows, 12)
+        cpu, _ = glm_cpu_irls(codes, g, rows)
         v = cpu["value"]
         line = {"impl": "reference", "metric": GLM_METRIC, "value": v, "unit": "s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
@@ -170,59 +176,74 @@ def run_glm(args, cfg, rank, world, local, pg):
     t0 = time.perf_counter()
     sess = fb.Session(codes, g)
     prepare_s = time.perf_counter() - t0
-    rows = np.ascontiguousarray(rows[sess.row_order()])
+    order = sess.row_order()
+    info = sess.info()
+    sess.close()
+    rows = np.ascontiguousarray(rows[order])
     prec = fb.PREC_F64 if args.precision == "f64" else fb.PREC_F32_REFINED
-    stream = torch.cuda.ExternalStream(sess.stream(), device=device)
     src = torch.from_numpy(rows).to(device)
     pinned = torch.empty(rows.shape, dtype=torch.float64, pin_memory=True)
     host = pinned.numpy()
     np.copyto(host, rows)
+    phases, launches = {}, 0
 
-    def step(on_device):
+    def step(on_device, profile=False):
+        nonlocal launches
+        s = fb.Session(codes, g)  # fresh state (outside the events)
+        stream = torch.cuda.ExternalStream(s.stream(), device=device)
+        torch.cuda.synchronize(device)
+        if profile:
+            s.set_profiling(True)
+        l0 = s.launches()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        res = sess.poisson(src.data_ptr() if on_device else host, vce="robust", tol=1e-8, precision=prec,
-                           on_device=on_device, nx=2)
+        res = s.poisson(src.data_ptr() if on_device else host, vce="robust", tol=1e-8, precision=prec,
+                        on_device=on_device, nx=2)
         e1.record(stream)
         e1.synchronize()
+        if profile:
+            launches += s.launches() - l0
+            for k, (ms, c) in s.phase_times().items():
+                a = phases.get(k, (0.0, 0))
+                phases[k] = (a[0] + ms, a[1] + c)
+        s.close()
         return e0.elapsed_time(e1) / 1e3, res
 
     for _ in range(args.warmup):
         step(True)
     barrier(pg)
-    sess.set_profiling(True)
-    l0 = sess.launches()
     times = []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            dt, res = step(True)
+            dt, res = step(True, profile=True)
             times.append(dt)
-    launches = sess.launches() - l0
-    phases = sess.phase_times()
-    sess.set_profiling(False)
     step_s = max_over_ranks(float(np.mean(times)), pg, device)
     e2e = None
     if not args.no_e2e:
         e2e = max_over_ranks(float(np.mean([step(False)[0] for _ in range(2)])), pg, device) / world
     if rank == 0:
+        cpu = parity = None
+        if not args.no_cpu_baseline and world == 1:
+            cpu, ref = glm_cpu_irls(codes, g, make_gravity_data(cfg)[2])
+            parity = parity_of(res["b"], res["V"], ref[0], ref[1])
+            parity["oracle"] = "oracle/glm.py irls_absorbed at tol 1e-8, inner tolerance down to 1e-10"
         line = {"metric": GLM_METRIC, "value": step_s / world, "unit": "s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if prec == fb.PREC_F64 else "f32+f64", "data": "synthetic",
                 "config": {"workload": "c4", "n": n, "irls_iterations": res["iterations"],
                            "pcg_iterations": res["pcg_iterations"], "b_x1": float(res["b"][0]),
                            "status": [int(x) for x in res["status"]], "zero_share": float(np.mean(rows[:, 0] == 0)),
-                           "prepare_s": prepare_s, "precision": args.precision,
+                           "prepare_s": prepare_s, "precision": args.precision, "fresh_session_per_call": True,
                            "parallelism": f"replicas x{world}"},
                 "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
-                "roofline": roofline_of(sess, phases, n, 3, True, 8 if prec == fb.PREC_F64 else 4, "c4"),
-                "cpu_baseline": None if args.no_cpu_baseline or world > 1 else
-                glm_cpu_sample(codes, g, make_gravity_data(cfg)[2], res["iterations"]),
+                "roofline": roofline_of(info, phases, n, 3, True, 8 if prec == fb.PREC_F64 else 4, "c4"),
+                "cpu_baseline": cpu,
+                "parity": parity,
                 "clocks": clk.summary(),
                 "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": n * 3 * 8, "d2h_bytes_per_step": 96},
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
-    sess.close()
 
 
 SERVE_METRIC = "served p99 latency (s), mixed stream of 2,000 regressions (60% OLS / 20% IV / 20% logit)"
@@ -577,32 +598,27 @@ def boot_cpu_sample(codes, g, rows, rounds=2):
                       f"{len(times) - 1} timed rounds, C++ FP64 restatement, all host threads"}
 
 
-def glm_cpu_sample(codes, g, rows, iters):
-    """The CPU oracle's cost of one PPML call: one weighted FE solve of [z, x1, ldist] (the IRLS
-    iteration's dominant cost) times the iteration count, all host threads."""
+def glm_cpu_irls(codes, g, rows):
+    """The CPU oracle's PPML call: the full IRLS of oracle/glm.py (irls_absorbed: the reference's
+    loop with the FE solve on the C++ restatement, all host threads, the row work in numpy), robust
+    SEs. Returns the cpu_baseline record and (b, V)."""
+    from oracle import glm as oglm
     from oracle import oracle
 
-    ab = oracle.Absorber(codes, g)
-    rng = np.random.default_rng(1)
-    ab.set_weights(rng.uniform(0.5, 2.0, rows.shape[0]))
-    z = np.ascontiguousarray(rows[ab.row_order()])
-    ts = []
-    for _ in range(2):
-        zz = z.copy()
-        t0 = time.perf_counter()
-        ab.residualize(zz, tol=1e-8)
-        ts.append(time.perf_counter() - t0)
-    per_it = float(np.mean(ts))
-    return {"value": per_it * iters, "unit": "s", "cores": oracle.max_threads(), "kind": "port",
-            "sample": f"one weighted FE solve of [z, x1, ldist] ({per_it:.3f} s, C++ FP64 restatement, all host "
-                      f"threads) times {iters} IRLS iterations"}
+    t0 = time.perf_counter()
+    b, V, dev, ll, iters = oglm.irls_absorbed(codes, g, rows[:, 0], rows[:, 1:], "poisson", "robust", tol=1e-8)
+    v = time.perf_counter() - t0
+    return ({"value": v, "unit": "s", "cores": oracle.max_threads(), "kind": "port",
+             "sample": f"one full PPML IRLS call on the full workload ({iters} iterations; FE solves on the C++ "
+                       f"FP64 restatement with all host threads, row work in numpy)"}, (b, V))
 
 
 def roofline_of(sess, phases, n, R, weighted, s_v, workload):
     """Roofline of the dominant timed phase: algorithmic bytes of one call of it (phase_bytes with
-    R columns) over its average duration, against the measured copy bandwidth."""
+    R columns) over its average duration, against the measured copy bandwidth. `sess` is a
+    session or its info() dict."""
     hbm, peak_kind = peaks()
-    info = sess.info()
+    info = sess if isinstance(sess, dict) else sess.info()
     algo = phase_bytes(info, n, R, weighted, s_v)
     timed = {k: v for k, v in phases.items() if k in algo and v[1]}
     dom = max(timed, key=lambda k: timed[k][0])
@@ -703,7 +719,28 @@ def run_boot(args, cfg, rank, world, local, pg):
 def workload_name(cfg_name):
     if cfg_name == "c2":
         return "OLS y~x1..x10 | indiv(1e6)+firm(1e5, row mod 1e5)+year(10), n=1e7, iid SEs"
+    if cfg_name == "c2d":
+        return "OLS y~x1..x10 | indiv(1e6)+firm(43478, row mod 43478: connected ring)+year(10), n=1e7, iid SEs"
     return "OLS y~x1 | indiv(1e4)+year(10), n=1e5, iid SEs"
+
+
+PARITY_TOL = 1e-14  # the oracle's solver tolerance for the parity figures (the fixtures' tolerance)
+PARITY_TARGET = 1e-8
+
+
+def parity_of(b, V, b_ref, V_ref):
+    """Largest relative error of the coefficients and of the standard errors against the oracle's
+    (|b - b_oracle| / |b_oracle|, |se - se_oracle| / se_oracle)."""
+    b, b_ref = np.asarray(b), np.asarray(b_ref)
+    se = np.sqrt(np.maximum(np.diag(V), 0.0))
+    se_ref = np.sqrt(np.maximum(np.diag(V_ref), 0.0))
+    kept = np.flatnonzero(se_ref > 0)  # regressors the oracle omits (absorbed, collinear) have se 0
+    eb = float(np.max(np.abs(b[kept] - b_ref[kept]) / np.abs(b_ref[kept])))
+    es = float(np.max(np.abs(se[kept] - se_ref[kept]) / se_ref[kept]))
+    omitted_agree = bool(np.all(se[se_ref == 0] == 0))
+    return {"b_max_rel": eb, "se_max_rel": es, "target": PARITY_TARGET, "compared": int(len(kept)),
+            "omitted_agree": omitted_agree,
+            "ok": bool(eb <= PARITY_TARGET and es <= PARITY_TARGET and omitted_agree)}
 
 
 class ClockSampler:
@@ -950,6 +987,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=list(CONFIGS))
     ap.add_argument("--precision", default="f64", choices=["f64", "f32r"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity figures (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing (profiling runs)")
     ap.add_argument("--boot-tile", type=int, default=512, help="draws per block-PCG tile (c3)")
     ap.add_argument("--serve-workers", type=int, default=8, help="requests in flight (c5)")
@@ -1070,6 +1108,18 @@ def main():
         cpu = {"value": float(np.mean(ts)), "unit": "s", "cores": oracle.max_threads(), "kind": "port",
                "sample": "2 OLS calls on the full workload (C++ FP64 restatement of the reference's session OLS, "
                          f"OpenMP); its session prepare took {oprep:.3f} s"}
+    parity = None
+    if rank == 0 and world == 1 and not args.no_parity:
+        # the oracle's answer at the fixtures' tolerance on the same rows (untimed): the error of
+        # every coefficient and standard error of the last timed call
+        from oracle import oracle
+
+        osess, orows, _ = oracle_session(codes, g, make_data(cfg)[2])
+        ref = osess.ols(orows, tol=PARITY_TOL, maxiter=100000)
+        parity = parity_of(res["b"], res["V"], ref["b"], ref["V"])
+        parity["oracle_tol"] = PARITY_TOL
+        parity["k"] = len(ref["b"])
+        osess.close()
 
     if rank == 0:
         line = {
@@ -1086,6 +1136,7 @@ def main():
                          "algorithmic_bytes": algo[dom]},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clk.summary(),
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": n * R * 8, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,

@@ -4,7 +4,7 @@
  * (leoliu0/fereg, crates/fereg-core/src/absorber.rs:62-97) as implemented by `FeSolver`
  * (crates/fereg-core/src/solve.rs:351-1344), constructed where the reference calls
  * `solve::build` (solve.rs:338, selected by `build_absorber`, session.rs:606). A Rust shim
- * `impl Absorber for GpuAbsorber` binds them.
+ * `impl Absorber for GpuAbsorber` binds them from fereg-core.
  *
  * Conventions
  *   - Plain pointers and sizes. Row blocks are N x R row-major doubles in the absorber's row

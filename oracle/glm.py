@@ -97,7 +97,11 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
     and is tightened 10x when the deviance change falls below it, down to
     max(1e-12, min(itol, 0.1 tol)) (glm/mod.rs:826);
     convergence when the relative deviance change is below tol at the tightest inner tolerance.
-    Unweighted samples, no separation checks. Returns b, V, deviance, log-likelihood, iterations."""
+    A regressor that the fixed effects absorb (after the first iteration's solve, weighted
+    residual sum of squares <= min(1e-6, tol / 10) times its raw sum of squares, the stage-1 rule
+    of ols.rs:38) keeps being residualized but leaves the fit: its coefficient and its row and
+    column of V are 0. Unweighted samples, no separation checks. Returns b, V, deviance,
+    log-likelihood, iterations."""
     from oracle import oracle
 
     ab = oracle.Absorber(codes, g)
@@ -116,6 +120,8 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
     dev_old = np.nan
     warm = None
     eps, alt_tol, hist = np.nan, np.inf, []
+    sumsq = np.sum(X * X, axis=0)
+    keep = np.arange(k)
     for it in range(1, maxiter + 1):
         predicted = _predict_eps(hist, eps)
         if family == "poisson":
@@ -128,7 +134,10 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
         B = np.ascontiguousarray(np.column_stack([z, X]))
         out = ab.residualize(B, tol=tol_in, maxiter=100000, want_coefs=True, warm=warm)
         warm = out["coefs"]
-        Xt, zt = B[:, 1:], B[:, 0]
+        if it == 1:
+            ss = np.sum(w[:, None] * B[:, 1:] ** 2, axis=0)
+            keep = np.flatnonzero(ss > min(1e-6, tol / 10) * sumsq)
+        Xt, zt = B[:, 1 + keep], B[:, 0]
         A = np.linalg.inv(Xt.T @ (w[:, None] * Xt))
         b = A @ (Xt.T @ (w * zt))
         e = zt - Xt @ b
@@ -156,16 +165,20 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
         dev_old = dev
     s = (e * w)[:, None] * Xt
     if vce == "oim":
-        V = A
+        Vk = A
     elif vce == "robust":
-        V = A @ (s.T @ s) @ A * n / (n - 1)
+        Vk = A @ (s.T @ s) @ A * n / (n - 1)
     else:
         codes_c, G = cl
-        S = np.zeros((G, k))
+        S = np.zeros((G, len(keep)))
         np.add.at(S, np.asarray(codes_c)[pi], s)
-        V = A @ (S.T @ S) @ A * G / (G - 1)
+        Vk = A @ (S.T @ S) @ A * G / (G - 1)
     if family == "poisson":
         ll = np.sum(y * eta - mu - gammaln(y + 1))
     else:
         ll = np.sum(y * eta - np.logaddexp(0, eta))
-    return b, V, dev, ll, it
+    bf = np.zeros(k)
+    bf[keep] = b
+    V = np.zeros((k, k))
+    V[np.ix_(keep, keep)] = Vk
+    return bf, V, dev, ll, it

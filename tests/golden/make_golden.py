@@ -144,6 +144,8 @@ def main_iv_logit(ref):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+    ref = sys.argv[1]
     main(ref)
     main_iv_logit(ref)

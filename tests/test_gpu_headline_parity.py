@@ -1,0 +1,80 @@
+"""Coefficient and standard-error parity at the 1e-8 relative target on the benchmark's panels.
+
+The device OLS (fereg_session_ols, at the benchmark's solver tolerance) against the oracle's
+session OLS at tol 1e-14 (the tolerance of the reference's frozen fixtures) on the same seeded
+rows:
+
+- the 1e5-row panel of y ~ x1 | indiv + year (1e4 individuals x 10 years; x1 ~ N(0,1), the
+  individual effect ~ N(0,1), the year effect ~ N(0, 0.5) read as variance 0.5, y = x1 + effects
+  + N(0,1)), iid and CRV1 on the individual;
+- 1e6-row panels of y ~ x1..x10 | indiv + firm + year with the 1e7 panel's value distributions,
+  on the cyclic firm graph (firm = row mod 1e4: disconnected components of 10 firms) and on the
+  connected ring of the reference's "difficult" design (firm = row mod 4,348, i.e. n_ind / 23).
+
+Every coefficient b_j and standard error se_j must satisfy |x - x_oracle| / |x_oracle| <= 1e-8.
+"""
+
+import numpy as np
+import pytest
+
+import bench
+import fereg_b200 as fb
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+TARGET = 1e-8
+
+PANELS = {
+    "c1": dict(bench.CONFIGS["c1"]),
+    "cyclic_1e6": dict(n_ind=100_000, years=10, n_firm=10_000, k=10, seed=10**6 * 100 + 43),
+    "ring_1e6": dict(n_ind=100_000, years=10, n_firm=4_348, k=10, seed=10**6 * 100 + 47),
+}
+
+
+def rel_errors(a, b):
+    se_a = np.sqrt(np.diag(a["V"]))
+    se_b = np.sqrt(np.diag(b["V"]))
+    eb = float(np.max(np.abs(a["b"] - b["b"]) / np.abs(b["b"])))
+    es = float(np.max(np.abs(se_a - se_b) / se_b))
+    return eb, es
+
+
+_ORACLE = {}
+
+
+def oracle_ols(name, codes, g, clusters, cl_g, z, vce):
+    """The oracle's answer at tol 1e-14, computed once per panel and variance."""
+    if (name, vce) not in _ORACLE:
+        orc = oracle.Session(codes, g, clusters, cl_g)
+        _ORACLE[(name, vce)] = (orc.row_order(), orc.ols(z.copy(), vce=vce, tol=1e-14, maxiter=100000))
+        orc.close()
+    return _ORACLE[(name, vce)]
+
+
+_DATA = {}
+
+
+def panel(name):
+    if name not in _DATA:
+        _DATA[name] = bench.make_data(PANELS[name])
+    return _DATA[name]
+
+
+@pytest.mark.parametrize("name,vce", [("c1", "unadjusted"), ("c1", "cluster"), ("cyclic_1e6", "unadjusted"),
+                                      ("ring_1e6", "unadjusted")])
+@pytest.mark.parametrize("precision", [fb.PREC_F64, fb.PREC_F32_REFINED])
+def test_ols_within_target(name, vce, precision):
+    codes, g, rows = panel(name)
+    clusters, cl_g = ([codes[0]], [g[0]]) if vce == "cluster" else ([], [])
+    gpu = fb.Session(codes, g, clusters, cl_g)
+    ro = gpu.row_order()
+    z = np.ascontiguousarray(rows[ro])
+    a = gpu.ols(z, vce=vce, tol=bench.TOL, precision=precision)
+    gpu.close()
+    ro_orc, b = oracle_ols(name, codes, g, clusters, cl_g, z, vce)
+    assert np.array_equal(ro, ro_orc)
+    for k in ("N", "df_r", "df_a", "N_clust"):
+        assert a["scalars"][k] == b["scalars"][k], k
+    eb, es = rel_errors(a, b)
+    assert eb <= TARGET and es <= TARGET, (name, vce, precision, eb, es)
