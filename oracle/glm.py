@@ -17,7 +17,7 @@ from scipy.special import expit, gammaln
 
 
 def dense_glm(family, terms, y, X, vce="robust", cl=None, maxiter=200):
-    """terms: list of (codes, levels); cl: (codes, G) for vce="cluster". Returns b, V, deviance,
+    """terms: list of (codes, levels); cl: (codes, G), or a list of them, for vce="cluster". Returns b, V, deviance,
     log-likelihood."""
     n = len(y)
     D = np.concatenate([np.eye(g)[c] for c, g in terms], axis=1)
@@ -72,6 +72,33 @@ def dense_glm(family, terms, y, X, vce="robust", cl=None, maxiter=200):
     return b, V, dev, ll
 
 
+def cluster_sandwich(A, s, dims):
+    """A (sum over clusters of the score sums' outer products) A with reghdfe's multiway rule
+    (vcov.rs:480-560 multiway_meat): inclusion-exclusion over the intersections of the cluster
+    dimensions, the G/(G-1) factor of the smallest dimension, and the negative eigenvalues of a
+    multiway V clipped to 0. dims: (codes per row, G) in the rows' order."""
+    from itertools import combinations
+
+    k = s.shape[1]
+    meat = np.zeros((k, k))
+    for size in range(1, len(dims) + 1):
+        for sub in combinations(dims, size):
+            key = np.zeros(len(s), dtype=np.int64)
+            for c, G in sub:
+                key = key * G + c
+            _, inv = np.unique(key, return_inverse=True)
+            S = np.zeros((inv.max() + 1, k))
+            np.add.at(S, inv, s)
+            meat += (-1.0) ** (size + 1) * (S.T @ S)
+    gmin = min(G for _, G in dims)
+    V = A @ meat @ A * gmin / (gmin - 1)
+    if len(dims) > 1:
+        lam, Q = np.linalg.eigh(V)
+        if lam.min() < 0:
+            V = (Q * np.maximum(lam, 0)) @ Q.T
+    return V
+
+
 def _predict_eps(hist, eps):
     """ppmlhdfe predict_eps (glm/irls.rs:105-140): the cubic without a constant through the last
     three (i, ln eps_i), evaluated at i = 4; NaN until three values are known."""
@@ -89,7 +116,7 @@ def _predict_eps(hist, eps):
     return float(np.exp(4 * c[0] + 16 * c[1] + 64 * c[2]))
 
 
-def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=1e-10, maxiter=1000):
+def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=1e-10, maxiter=1000, state=None):
     """IRLS with the fixed effects absorbed by the oracle's FE solver (the reference's loop,
     glm/irls.rs:367-560): each iteration sets the family's weights on the absorber, residualizes
     [z, X] warm-started from the previous FE coefficients, fits the weighted regression on the
@@ -164,15 +191,14 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
                 tol_in *= 0.1
         dev_old = dev
     s = (e * w)[:, None] * Xt
+    if state is not None:  # the final iteration's quantities, in row order
+        state.update(w=w, e=e, Xt=Xt, X=X[:, keep], A=A, pi=pi, keep=keep)
     if vce == "oim":
         Vk = A
     elif vce == "robust":
         Vk = A @ (s.T @ s) @ A * n / (n - 1)
     else:
-        codes_c, G = cl
-        S = np.zeros((G, len(keep)))
-        np.add.at(S, np.asarray(codes_c)[pi], s)
-        Vk = A @ (S.T @ S) @ A * G / (G - 1)
+        Vk = cluster_sandwich(A, s, [(np.asarray(c)[pi], G) for c, G in (cl if isinstance(cl, list) else [cl])])
     if family == "poisson":
         ll = np.sum(y * eta - mu - gammaln(y + 1))
     else:

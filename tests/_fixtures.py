@@ -75,3 +75,57 @@ def prepare_iv(spec, data):
 def iv_block(spec, data, alive):
     cols = [spec["y"]] + spec["exog"] + spec["endog"] + spec["inst"]
     return np.ascontiguousarray(np.stack([data[c][alive] for c in cols], axis=1))
+
+
+def load_poisson():
+    """The committed ppmlhdfe fixtures and their data sets (tests/golden/make_golden.py)."""
+    data = {name: load_csv(f"glm_{name}.csv") for name in ("gravity", "auto", "problem1")}
+    return load_json("poisson_fixtures.json"), data
+
+
+def _interact(parts):
+    """Dense codes (ascending) of the interaction of factor codes, with the level count."""
+    key = np.zeros(len(parts[0][0]), dtype=np.uint64)
+    for codes, g in parts:
+        key = key * np.uint64(g) + codes.astype(np.uint64)
+    u, inv = np.unique(key, return_inverse=True)
+    return inv.astype(np.uint32), len(u)
+
+
+def prepare_poisson(spec, data):
+    """Sample preparation of a Poisson fixture as Session::prepare does it for ppmlhdfe: the
+    rows of the fixture's `if` condition, factorize, interactions, then cyclically the singleton
+    drops (unless singletons are kept) and the `fe` rule (sample.rs:74: rows of an FE group whose
+    y sums to 0) until neither changes the sample, then restrict. ppmlhdfe reports both kinds of
+    drops as singletons. Returns the kept mask over all input rows, the rows dropped, the kept
+    terms, the cluster dimensions and the kept n x (1 + k) block [y, x...] in kept order."""
+    from oracle import oracle
+
+    n_all = len(data[spec["y"]])
+    base = np.ones(n_all, dtype=bool)
+    base[[i - 1 for i in spec["exclude"]]] = False
+    names = sorted({f for t in spec["absorb"] for f in t} | {f for t in spec["cluster"] for f in t})
+    fac = {f: oracle.factorize(data[f][base]) for f in names}
+    terms = [_interact([fac[f] for f in t]) for t in spec["absorb"]]
+    y_all = data[spec["y"]][base]
+    alive = np.ones(int(base.sum()), dtype=bool)
+    while True:
+        before = int(alive.sum())
+        if not spec["keepsing"]:
+            idx = np.flatnonzero(alive)
+            a2, _ = oracle.drop_singletons([restrict(c, alive)[0] for c, _ in terms],
+                                           [restrict(c, alive)[1] for c, _ in terms], None)
+            alive[idx[~a2]] = False
+        for c, g in terms:
+            s = np.bincount(c[alive], weights=y_all[alive], minlength=g)
+            alive &= s[c] > 0
+        if int(alive.sum()) == before:
+            break
+    nsing = int(base.sum()) - int(alive.sum())
+    terms = [restrict(c, alive) for c, _ in terms]
+    cl = [restrict(_interact([fac[f] for f in t])[0], alive) for t in spec["cluster"]]
+    y = y_all[alive]
+    block = np.ascontiguousarray(np.column_stack([y] + [data[x][base][alive] for x in spec["x"]]))
+    keep = np.zeros(n_all, dtype=bool)
+    keep[np.flatnonzero(base)[alive]] = True
+    return keep, nsing, terms, cl, block

@@ -10,7 +10,9 @@ fixture's model specification as restated from the reference's harness
 It also extracts the IV fixtures (ivreghdfe 1.1.4 on an nlswork subset, iv_nls.csv +
 iv_nls_{a,b}_{unadj,robust,cl1,cl2}_{none,aw,fw,pw}.json; harness tests/iv.rs:216-248) and the
 logit fixtures (Stata `logit y x1 x2 i.fe1 i.fe2`, glm_logit.csv + glm_l_*.json; harness
-tests/glm.rs:319-325, 659-672): b, V, sample and the scalars compared here.
+tests/glm.rs:319-325, 659-672): b, V, sample and the scalars compared here; and the Poisson
+fixtures (ppmlhdfe 2.3.3, glm_p_*.json on glm_gravity.csv, glm_auto.csv and glm_problem1.csv;
+harness tests/glm.rs:432-480, 561-650) without separated observations.
 
 Run once in a container that has the reference mounted:
     python tests/golden/make_golden.py /path/to/reference
@@ -143,9 +145,63 @@ def main_iv_logit(ref):
     print("wrote the IV and logit fixtures")
 
 
+# tests/glm.rs:561-650: ppmlhdfe 2.3.3 fixtures with no separated observation, unweighted and
+# without offset (the scope of the device IRLS). Each spec restates the harness's: data set,
+# outcome, regressors, absorbed terms (interactions as lists), cluster dimensions, vce, whether
+# singletons are kept, the solver tolerance, and rows excluded before the call (`exclude`,
+# 1-based observation numbers of the fixture's `if` condition).
+POISSON_SPECS = [
+    dict(name="p_gravity", data="gravity", y="trade", x=["rta", "x2"],
+         absorb=[["exp", "year"], ["imp", "year"], ["exp", "imp"]], cluster=[["exp", "imp"]], vce="cluster",
+         keepsing=False, tol=1e-10, exclude=[]),
+    dict(name="p_twoway_robust", data="auto", y="price", x=["weight", "gear_ratio", "length"],
+         absorb=[["turn"], ["trunk"]], cluster=[], vce="robust", keepsing=True, tol=1e-12, exclude=[]),
+    # V not compared: ppmlhdfe's two-way cluster V is the eigenvalue-clipped bordered matrix with
+    # _cons on its internal standardized scale (glm/mod.rs:1054-1120); this path reports no
+    # _cons and clips the regressors' block. b, the sample, N and N_clust are compared.
+    dict(name="p_twoway_cluster2", data="auto", y="price", x=["weight", "gear_ratio", "length"],
+         absorb=[["turn"], ["trunk"]], cluster=[["turn"], ["trunk"]], vce="cluster", keepsing=True, tol=1e-12,
+         exclude=[], compare_v=False),
+    dict(name="p_twoway_cluster_turn", data="auto", y="price", x=["weight", "gear_ratio", "length"],
+         absorb=[["turn"], ["trunk"]], cluster=[["turn"]], vce="cluster", keepsing=False, tol=1e-12, exclude=[]),
+    dict(name="p_d_twoway", data="auto", y="price", x=["weight", "gear_ratio", "length"],
+         absorb=[["turn"], ["trunk"]], cluster=[], vce="robust", keepsing=False, tol=1e-12, exclude=[]),
+    dict(name="p_savefe", data="auto", y="price", x=["weight", "gear_ratio"], absorb=[["turn"], ["foreign"]],
+         cluster=[], vce="robust", keepsing=True, tol=1e-10, exclude=[]),
+    dict(name="p_guess_ols", data="auto", y="price", x=["weight", "gear_ratio", "length"], absorb=[["turn"]],
+         cluster=[], vce="robust", keepsing=False, tol=1e-10, exclude=[]),
+    dict(name="p_problem1", data="problem1", y="y", x=["x1", "x2"], absorb=[["i"], ["j"]], cluster=[],
+         vce="robust", keepsing=False, tol=1e-10, exclude=[5, 7, 8, 14, 15]),
+]
+POISSON_DATA = {
+    "gravity": ["trade", "rta", "x2", "exp", "imp", "year"],
+    "auto": ["price", "weight", "gear_ratio", "length", "turn", "trunk", "foreign"],
+    "problem1": ["y", "x1", "x2", "i", "j"],
+}
+POISSON_SCALARS = ["N", "num_separated", "num_singletons", "N_clust", "ll", "ll_0", "deviance", "chi2", "rank",
+                   "df_m"]
+
+
+def main_poisson(ref):
+    data_dir = os.path.join(ref, "crates", "fereg-core", "tests", "data")
+    for name, cols in POISSON_DATA.items():
+        copy_csv(os.path.join(data_dir, f"glm_{name}.csv"), os.path.join(HERE, f"glm_{name}.csv"), cols)
+    out = []
+    for spec in POISSON_SPECS:
+        with open(os.path.join(data_dir, f"glm_{spec['name']}.json")) as f:
+            j = json.load(f)
+        sc = {k: j["scalars"].get(k) for k in POISSON_SCALARS}
+        out.append(dict(spec=spec, cmdline=j["cmdline"], colnames=j["colnames"], b=j["b"], V=j["V"],
+                        sample=j["sample"], scalars=sc))
+    with open(os.path.join(HERE, "poisson_fixtures.json"), "w") as f:
+        json.dump(out, f)
+    print(f"wrote {len(out)} Poisson fixtures")
+
+
 if __name__ == "__main__":
     if len(sys.argv) != 2:
         sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
     ref = sys.argv[1]
     main(ref)
     main_iv_logit(ref)
+    main_poisson(ref)
