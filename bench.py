@@ -185,9 +185,9 @@ def run_glm(args, cfg, rank, world, local, pg):
     pinned = torch.empty(rows.shape, dtype=torch.float64, pin_memory=True)
     host = pinned.numpy()
     np.copyto(host, rows)
-    phases, launches = {}, 0
+    phases, launches, stats = {}, 0, {}
 
-    def step(on_device, profile=False):
+    def step(on_device, profile=False, count=False):
         nonlocal launches
         s = fb.Session(codes, g)  # fresh state (outside the events)
         stream = torch.cuda.ExternalStream(s.stream(), device=device)
@@ -202,8 +202,11 @@ def run_glm(args, cfg, rank, world, local, pg):
                         on_device=on_device, nx=2)
         e1.record(stream)
         e1.synchronize()
-        if profile:
+        if count:
             launches += s.launches() - l0
+            for k_, v_ in s.solver_stats().items():
+                stats[k_] = stats.get(k_, 0) + v_
+        if profile:
             for k, (ms, c) in s.phase_times().items():
                 a = phases.get(k, (0.0, 0))
                 phases[k] = (a[0] + ms, a[1] + c)
@@ -216,8 +219,10 @@ def run_glm(args, cfg, rank, world, local, pg):
     times = []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            dt, res = step(True, profile=True)
+            dt, res = step(True, count=True)
             times.append(dt)
+    for _ in range(args.prof_steps):
+        step(True, profile=True)
     step_s = max_over_ranks(float(np.mean(times)), pg, device)
     e2e = None
     if not args.no_e2e:
@@ -235,8 +240,9 @@ def run_glm(args, cfg, rank, world, local, pg):
                            "pcg_iterations": res["pcg_iterations"], "b_x1": float(res["b"][0]),
                            "status": [int(x) for x in res["status"]], "zero_share": float(np.mean(rows[:, 0] == 0)),
                            "prepare_s": prepare_s, "precision": args.precision, "fresh_session_per_call": True,
-                           "parallelism": f"replicas x{world}"},
-                "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
+                           "parallelism": f"replicas x{world}", "solver_stats_timed_calls": stats},
+                "phases_ms_per_step": {k: v[0] / args.prof_steps for k, v in phases.items() if v[1]},
+                "phases_note": PHASES_NOTE,
                 "roofline": roofline_of(info, phases, n, 3, True, 8 if prec == fb.PREC_F64 else 4, "c4"),
                 "cpu_baseline": cpu,
                 "parity": parity,
@@ -680,7 +686,6 @@ def run_boot(args, cfg, rank, world, local, pg):
     for _ in range(args.warmup):
         step(True)
     barrier(pg)
-    sess.set_profiling(True)
     l0 = sess.launches()
     times = []
     with ClockSampler(local) as clk:
@@ -688,8 +693,7 @@ def run_boot(args, cfg, rank, world, local, pg):
             dt, res = step(True)
             times.append(dt)
     launches = sess.launches() - l0
-    phases = sess.phase_times()
-    sess.set_profiling(False)
+    phases = profiled_phases(sess, lambda: step(True), args)
     step_s = max_over_ranks(float(np.mean(times)), pg, device)
     e2e = None
     if not args.no_e2e:
@@ -703,7 +707,8 @@ def run_boot(args, cfg, rank, world, local, pg):
                 "config": {"workload": "c3", "n": n, "reps": int(res["reps"]), "tile": args.boot_tile,
                            "precision": args.precision, "prepare_s": prepare_s, "stat": res["stat"],
                            "pvalue": res["pvalue"], "parallelism": f"replicas x{world}"},
-                "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
+                "phases_ms_per_step": {k: v[0] / args.prof_steps for k, v in phases.items() if v[1]},
+                "phases_note": PHASES_NOTE,
                 # per apply / residualize call of one draw tile (tile columns); the fit's 2-column
                 # solve is counted at the tile's width
                 "roofline": roofline_of(sess, phases, n, args.boot_tile, False, 8 if prec == fb.PREC_F64 else 4, "c3"),
@@ -714,6 +719,21 @@ def run_boot(args, cfg, rank, world, local, pg):
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     sess.close()
+
+
+PHASES_NOTE = ("per-phase CUDA events from --prof-steps extra calls after the timed ones, the same kernels "
+               "launched one by one (the timed calls run the PCG iterations as captured graphs)")
+
+
+def profiled_phases(sess, step, args):
+    """Phase times (ms, launches) of args.prof_steps calls with the session's per-phase CUDA events:
+    the same kernels, with the PCG iterations launched one by one instead of as graphs."""
+    sess.set_profiling(True)
+    for _ in range(args.prof_steps):
+        step()
+    phases = sess.phase_times()
+    sess.set_profiling(False)
+    return phases
 
 
 def workload_name(cfg_name):
@@ -988,6 +1008,7 @@ def main():
     ap.add_argument("--precision", default="f64", choices=["f64", "f32r"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity figures (profiling runs)")
+    ap.add_argument("--prof-steps", type=int, default=3, help="extra calls with per-phase timing (after the timed ones)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing (profiling runs)")
     ap.add_argument("--boot-tile", type=int, default=512, help="draws per block-PCG tile (c3)")
     ap.add_argument("--serve-workers", type=int, default=8, help="requests in flight (c5)")
@@ -1045,7 +1066,6 @@ def main():
         step_device()
     barrier(pg)
     torch.cuda.synchronize(device)
-    sess.set_profiling(True)
     l0 = sess.launches()
     times = []
     with ClockSampler(local) as clk:
@@ -1055,10 +1075,9 @@ def main():
     torch.cuda.synchronize(device)
     barrier(pg)
     launches = sess.launches() - l0
-    phases = sess.phase_times()
-    sess.set_profiling(False)
     step_s = max_over_ranks(float(np.mean(times)), pg, device)
     value = step_s / world
+    phases = profiled_phases(sess, step_device, args)
 
     # e2e: the same call through the C ABI with the block in pinned host memory
     pinned = torch.empty((n, R), dtype=torch.float64, pin_memory=True)
@@ -1130,11 +1149,12 @@ def main():
                        "m": info["m"], "g1": info["g1"], "pcg_iterations": int(res["scalars"]["ic"]), "tol": TOL,
                        "precision": args.precision, "l2": "inputs (880 MB) larger than L2, no flush",
                        "parallelism": f"replicas x{world}", "prepare_s": prepare_s,
-                       "b_x1": float(res["b"][0])},
+                       "b_x1": float(res["b"][0]), "solver_stats": sess.solver_stats()},
             "roofline": {"bound": "hbm", "kernel": kern, "phase": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes": algo[dom]},
-            "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]},
+            "phases_ms_per_step": {k: v[0] / args.prof_steps for k, v in phases.items() if v[1]},
+            "phases_note": PHASES_NOTE,
             "cpu_baseline": cpu,
             "parity": parity,
             "clocks": clk.summary(),

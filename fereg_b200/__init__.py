@@ -165,11 +165,14 @@ def _setup(L):
     L.fereg_session_stream.restype = P
     L.fereg_session_set_profiling.argtypes = [P, C.c_int]
     L.fereg_session_info.argtypes = [P, u64p]
+    L.fereg_session_solver_stats.argtypes = [P, u64p]
+    L.fereg_absorber_solver_stats.argtypes = [P, u64p]
     L.fereg_session_poisson.argtypes = [P, P, C.c_int, C.c_size_t, C.POINTER(GlmSpec), C.POINTER(GlmOut)]
     L.fereg_session_iv.argtypes = [P, P, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(IvSpec),
                                    C.POINTER(IvOut)]
     L.fereg_amg_probe.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, C.c_int, u32p, u32p, u64p, f64p]
     L.fereg_structure_digest.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, u64p]
+    L.fereg_structure_compare.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, u64p]
     L.fereg_factorize.argtypes = [f64p, C.c_size_t, u32p, u32p]
     L.fereg_combine.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, u32p, u32p]
     L.fereg_drop_singletons.argtypes = [C.POINTER(u32p), u32p, C.c_int, C.c_size_t, f64p, f64p, C.c_int, C.c_int,
@@ -313,6 +316,12 @@ class Absorber:
     def launches(self):
         return int(lib().fereg_absorber_launches(self.h))
 
+    def solver_stats(self):
+        """As Session.solver_stats for this absorber."""
+        v = np.zeros(4, dtype=np.uint64)
+        _check(lib().fereg_absorber_solver_stats(self.h, _p(v, u64p)))
+        return dict(zip(["graph_captures", "graph_launches", "graph_build_us", "fp64_finishes"], map(int, v)))
+
     def escalations(self):
         """Escalations so far (large blocks moved from Jacobi to the multigrid V-cycle)."""
         e = C.c_uint64()
@@ -403,6 +412,13 @@ class Session:
 
     def launches(self):
         return int(lib().fereg_session_launches(self.h))
+
+    def solver_stats(self):
+        """Counters of the device PCG loop: graphs captured, graph launches, host microseconds of
+        the captures, FP32-refined solves finished in FP64."""
+        v = np.zeros(4, dtype=np.uint64)
+        _check(lib().fereg_session_solver_stats(self.h, _p(v, u64p)))
+        return dict(zip(["graph_captures", "graph_launches", "graph_build_us", "fp64_finishes"], map(int, v)))
 
     PHASES = Absorber.PHASES + ["dof", "colstats", "gram", "variance", "weights"]
 
@@ -673,6 +689,18 @@ def structure_digest(codes, g):
     out = np.zeros(7, dtype=np.uint64)
     _check(lib().fereg_structure_digest(ptrs, _p(garr, u32p), len(arrs), len(arrs[0]), _p(out, u64p)))
     keys = ["cells", "segments", "m", "m_small", "blocks", "fe1", "digest"]
+    return {k: int(v) for k, v in zip(keys, out)}
+
+
+def structure_compare(codes, g):
+    """Test hook (device): differences between the cell structure built on the device and on the
+    host, per array (all 0 when they are identical)."""
+    arrs = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
+    ptrs = (u32p * len(arrs))(*[_p(a, u32p) for a in arrs])
+    garr = np.asarray(g, dtype=np.uint32)
+    out = np.zeros(9, dtype=np.uint64)
+    _check(lib().fereg_structure_compare(ptrs, _p(garr, u32p), len(arrs), len(arrs[0]), _p(out, u64p)))
+    keys = ["scalars", "pi", "seg_off", "cell_row", "coord", "pl_off", "pl_cell", "pl_seg", "pl_other"]
     return {k: int(v) for k, v in zip(keys, out)}
 
 

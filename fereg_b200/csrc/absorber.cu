@@ -18,7 +18,7 @@
 #include "absorber.h"
 #include "amg.cuh"
 #include "amg.h"
-#include "kernels.cuh"
+#include "pcg.cuh"
 #include "weights.cuh"
 
 namespace fereg {
@@ -36,7 +36,7 @@ constexpr size_t DENSE_SMALL_MAX = 1024;
 // Refinement: an FP32 inner solve stops once its preconditioned residual fell by this factor
 // (squared), well above FP32 rounding; the FP64 true residual then restarts it.
 constexpr double REFINE_DROP = 1e-9;
-constexpr int REFINE_ROUNDS = 12;
+constexpr int REFINE_ROUNDS = 30;
 
 void dense_ldlt_inverse(double* a, double* d, int k, double* x, cudaStream_t st, u64& launches);
 template <class K>
@@ -167,6 +167,12 @@ struct Scratch {
     // item of every row
     DBuf<u32> sr_k, sr_a, sr_b, sr_first;
     u32 sr_n = 0;
+    // dense rows of S on the small coordinates (srow, m x ms_acc, transposed) and the work items
+    // of their assembly: entry range of every run of a coordinate list, first item per coordinate
+    DBuf<double> srow;
+    DBuf<u32> si_a, si_b, si_first;
+    u32 si_n = 0;
+    bool srow_on = false;
     DBuf<uint8_t> red;
     DBuf<int> wflag;
     // solve (FP64)
@@ -175,7 +181,30 @@ struct Scratch {
     DBuf<float> fx, fb, fr, fz, fp, fq, ft, fpart, frhs, fx0, fsmall;
     DBuf<double> cg_rho, cg_rho_new, cg_pq, cg_gamma, cg_beta, cg_xb, cg_ss1, cg_floor, cg_ring, cg_xconst, cg_pfloor;
     DBuf<int> cg_active, cg_nactive;
-    int* h_nactive = nullptr;  // pinned
+    int* h_nactive = nullptr;  // pinned: the loop control words (CgLoop::ctl) read back
+    // PCG loop state on the device (pcg.cuh) and the captured iteration graphs, each keyed by
+    // every address its kernels read or write
+    DBuf<int> lp_ctl, lp_act;
+    DBuf<double> lp_tol;
+    DBuf<unsigned> lp_ticket;
+    DBuf<double> lp_rho_from, lp_rho_at;
+    struct PcgGraph {
+        std::vector<u64> key;
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        u64 body_launches = 0;  // kernels of one body
+    };
+    std::vector<PcgGraph> graphs;
+    u64 graph_launches = 0, graph_captures = 0;
+    u64 fp64_finishes = 0;  // FP32-refined solves finished in FP64
+    double graph_build_us = 0;  // host time of the captures and instantiations
+    void drop_graphs() {
+        for (auto& q : graphs) {
+            if (q.exec) cudaGraphExecDestroy(q.exec);
+            if (q.g) cudaGraphDestroy(q.g);
+        }
+        graphs.clear();
+    }
     // phase timing
     bool prof = false;
     std::vector<cudaEvent_t> ev;
@@ -250,6 +279,7 @@ struct Scratch {
         ev_slot.clear();
     }
     ~Scratch() {
+        drop_graphs();
         if (h_nactive) cudaFreeHost(h_nactive);
         for (auto e : ev)
             if (e) cudaEventDestroy(e);
@@ -279,7 +309,7 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
     }
     AllocScope alloc_scope(stream_);
     d_ = std::make_unique<Scratch>();
-    CK(cudaHostAlloc(&d_->h_nactive, sizeof(int), cudaHostAllocDefault));
+    CK(cudaHostAlloc(&d_->h_nactive, 8 * sizeof(int), cudaHostAllocDefault));
     d_->seg_off.upload(hs_.seg_off, stream_);
     d_->coord.upload(hs_.coord, stream_);
     if (!hs_.trivial()) d_->cell_row.upload(hs_.cell_row, stream_);
@@ -348,6 +378,27 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
             d_->sr_b.upload(ib, stream_);
             d_->sr_first.upload(first, stream_);
             d_->sr_n = u32(ik.size());
+        }
+        if (d_->ms_acc > 0) {
+            // work items of the dense small rows: runs of at least 256 entries of every list, never
+            // splitting a segment's run
+            std::vector<u32> ia, ib, first(hs_.m + 1, 0);
+            for (u32 f = 0; f < u32(hs_.m); f++) {
+                first[f] = u32(ia.size());
+                for (u32 a = pt.off[f]; a < pt.off[f + 1];) {
+                    u32 b = std::min(pt.off[f + 1], a + 256);
+                    while (b < pt.off[f + 1] && pt.seg[b] == pt.seg[b - 1]) b++;
+                    ia.push_back(a);
+                    ib.push_back(b);
+                    a = b;
+                }
+            }
+            first[hs_.m] = u32(ia.size());
+            d_->si_a.upload(ia, stream_);
+            d_->si_b.upload(ib, stream_);
+            d_->si_first.upload(first, stream_);
+            d_->si_n = u32(ia.size());
+            d_->srow_on = true;
         }
         d_->pl_off.upload(pt.off, stream_);
         d_->pl_cell.upload(pt.cell, stream_);
@@ -566,6 +617,7 @@ void GpuAbsorber::set_weights_device(const double* w_dev) {
     // probe asks for a stronger preconditioner (escalate).
     coord_stale_ = m > 0;
     refresh_coord();
+    build_srow();
     small_stale_ = small_ok_;
     pre_fresh_ = small_ok_;
     amg_stale_ = true;
@@ -687,7 +739,30 @@ void GpuAbsorber::upload_weights() {
     for (size_t s = 0; s < n1_.size(); s++) inv[s] = 1.0 / n1_[s];
     d_->n1inv.upload(inv, stream_);
     d_->nr.upload(nr_, stream_);
+    build_srow();
     CK(cudaStreamSynchronize(stream_));
+}
+
+// The dense rows of S on the small coordinates (weights.cuh) for the current cell weights: part
+// of the operator, so rebuilt with every weight state (unlike the preconditioners).
+void GpuAbsorber::build_srow() {
+    Scratch& d = *d_;
+    if (!d.srow_on || d.si_n == 0) return;
+    const HostStructure& st = hs_;
+    const u32 ms = d.ms_acc, M = u32(st.ncells), g1 = st.g1, m = u32(st.m);
+    const int ns = int(d.ns_acc);
+    const double* cw = d.cell_w.p;  // null: unit cell weights
+    DBuf<double> csk, part;
+    csk.alloc(size_t(g1) * ms);
+    part.alloc(size_t(d.si_n) * ms);
+    d.srow.alloc(size_t(m) * ms);
+    k_seg_small_w<<<grid_for(size_t(g1) * ms), THREADS, 0, stream_>>>(d.seg_off.p, d.coord.p, M, g1, ns, ms, cw,
+                                                                       csk.p);
+    k_srow_items<<<(d.si_n + 7) / 8, 256, 0, stream_>>>(d.coord.p, M, ns, ms, cw, d.n1inv.p, d.pl_cell.p, d.pl_seg.p,
+                                                        csk.p, d.si_a.p, d.si_b.p, d.si_n, part.p);
+    k_srow_sum<<<grid_for(size_t(m) * ms), THREADS, 0, stream_>>>(part.p, d.si_first.p, m, ms, d.srow.p);
+    d.launches += 3;
+    CK(cudaGetLastError());
 }
 
 void GpuAbsorber::set_weights(const double* w_rows) {
@@ -914,16 +989,19 @@ template <class T>
 void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* P, int R, T* Y, T* t, T* part,
                   T* small, cudaStream_t st) {
     int h = d.begin(GpuAbsorber::P_APPLY, st);
-    const bool acc = S.ms_acc > 0;
+    // small coordinates: from their dense rows of S (srow) when built, else summed per cell in
+    // the segment passes
+    const bool dense = S.ms_acc > 0 && d.srow_on;
+    const bool acc = S.ms_acc > 0 && !dense;
     const u32 len = S.ms_acc * u32(R);
     if (d.wseg.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = size_t(WPB) * S.ms_acc * 64 * sizeof(T);
+            const size_t shm = acc ? size_t(WPB) * S.ms_acc * 64 * sizeof(T) : 0;
             const u32 nsegs = u32(d.wseg_segs.n);
             with_lanes<1>(Rc, S.nb, [&](auto c, auto nbk) {
                 constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
-                allow_smem(k_gseg_apply<T, RCP, NBK>, shm);
+                if (shm) allow_smem(k_gseg_apply<T, RCP, NBK>, shm);
                 k_gseg_apply<T, RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, nsegs, P, R, j0, Rc,
                                                                           t, acc ? small : nullptr);
             });
@@ -969,33 +1047,51 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
             d.launches++;
         }
     }
-    if (acc) launch_small_reduce<T>(d, S, small, R, Y, st);
+    if (dense) {
+        const u32 grid = std::max<u32>(1, std::min<u32>(4 * GRID_V, (S.m + 31) / 32));
+        k_srow_apply<T><<<grid, THREADS, 0, st>>>(d.srow.p, S.m, S.ms_acc, P, R, small);
+        k_small_reduce<T><<<std::max<u32>(1, std::min<u32>((len + 7) / 8, GRID_V)), THREADS, 0, st>>>(
+            small, int(grid), nullptr, 0, nullptr, 0, len, Y);
+        d.launches += 2;
+    } else if (acc) {
+        launch_small_reduce<T>(d, S, small, R, Y, st);
+    }
     CK(cudaGetLastError());
     d.end(h, st);
+}
+
+// The V-cycle's work vectors of every level for R columns (allocated before a graph capture).
+template <class T>
+void amg_alloc(DevAmgBlock& A, int R) {
+    const size_t L = A.lv.size();
+    std::vector<DBuf<T>>& w = amg_work<T>(A);
+    if (w.size() != 3 * L) w.resize(3 * L);
+    for (size_t l = 0; l < L; l++) {
+        const size_t len = size_t(A.lv[l].n) * R;
+        if (l > 0) {
+            w[3 * l].alloc(len);
+            w[3 * l + 1].alloc(len);
+        }
+        if (l + 1 < L) w[3 * l + 2].alloc(len);
+    }
 }
 
 // One V(1,1) cycle (amg.cuh) on the block's slice of r into the same slice of z.
 template <class T>
 void launch_amg(Scratch& d, DevAmgBlock& A, const T* r, T* z, int R, cudaStream_t st) {
     const size_t L = A.lv.size();
+    amg_alloc<T>(A, R);
     std::vector<DBuf<T>>& w = amg_work<T>(A);
-    if (w.size() != 3 * L) w.resize(3 * L);
     std::vector<const T*> rin(L);
     std::vector<T*> zout(L), z1(L);
     rin[0] = r + size_t(A.off) * R;
     zout[0] = z + size_t(A.off) * R;
     for (size_t l = 0; l < L; l++) {
-        const size_t len = size_t(A.lv[l].n) * R;
         if (l > 0) {
-            w[3 * l].alloc(len);
-            w[3 * l + 1].alloc(len);
             rin[l] = w[3 * l].p;
             zout[l] = w[3 * l + 1].p;
         }
-        if (l + 1 < L) {
-            w[3 * l + 2].alloc(len);
-            z1[l] = w[3 * l + 2].p;
-        }
+        if (l + 1 < L) z1[l] = w[3 * l + 2].p;
     }
     for (size_t l = 0; l + 1 < L; l++) {
         const u32 nc = A.lv[l + 1].n;
@@ -1300,6 +1396,104 @@ SolveInfo GpuAbsorber::residualize_device(double* z_dev, size_t r, double tol, s
     return solve(z_dev, r, tol, maxiter, want_coefs, warm, coefs, prec);
 }
 
+constexpr int PROBE_FROM = 7, PROBE_AT = 12;
+constexpr double PROBE_RATIO = 0.6;
+
+// Iterations a graph launch may run at most before the host looks at the loop state again.
+constexpr int GRAPH_CAP = 64;
+
+// Every device address the iteration body reads or writes, with the body's shape: a captured
+// graph is reused only for an identical key.
+template <class T>
+std::vector<u64> body_key(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, const T* x,
+                          const T* rhs_true, const T* x0, const T* r, const T* z, const T* p, const T* q, const T* t,
+                          const T* part, const T* small, int R) {
+    std::vector<u64> k;
+    auto put = [&](const void* ptr) { k.push_back(u64(reinterpret_cast<uintptr_t>(ptr))); };
+    k.push_back(sizeof(T));
+    k.push_back(u64(R));
+    k.push_back(small_ok);
+    put(d.lp_tol.p);
+    for (const void* ptr : {(const void*)x, (const void*)rhs_true, (const void*)x0, (const void*)r, (const void*)z,
+                            (const void*)p, (const void*)q, (const void*)t, (const void*)part, (const void*)small})
+        put(ptr);
+    for (const void* ptr : {(const void*)W.w_rows, (const void*)W.cell_w, (const void*)W.n1inv, (const void*)W.nr,
+                            (const void*)d.inv_diag.p, (const void*)d.minv.p, (const void*)d.srow.p, (const void*)d.cta.p,
+                            (const void*)d.lp_ctl.p, (const void*)d.lp_ticket.p, (const void*)d.cg_rho.p,
+                            (const void*)d.cg_active.p, (const void*)d.cg_ring.p, (const void*)d.cg_xb.p,
+                            (const void*)d.cg_beta.p, (const void*)d.cg_gamma.p, (const void*)d.cg_pfloor.p,
+                            (const void*)d.cg_xconst.p, (const void*)d.cg_floor.p, (const void*)d.cg_ss1.p,
+                            (const void*)d.cg_pq.p, (const void*)d.cg_rho_new.p, (const void*)d.cg_nactive.p,
+                            (const void*)d.lp_rho_from.p, (const void*)d.lp_rho_at.p, (const void*)d.lp_act.p})
+        put(ptr);
+    k.push_back(d.amg.size());
+    for (auto& A : d.amg) {
+        put(A.minv.p);
+        for (auto& b : A.iu) put(b.p);
+        for (auto& b : A.dv) put(b.p);
+        for (auto& b : amg_work<T>(A)) put(b.p);
+    }
+    (void)S;
+    return k;
+}
+
+// The iteration body (cg.rs:207-290): q = S p, gamma, x and r (with the stopping rule's dot
+// products), z = M^-1 r, rho and the stopping rule, p. In a graph (use_cond) its last kernel sets
+// the WHILE condition.
+template <class T>
+void enqueue_iteration(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x, const T* rhs_true,
+                       const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small, int R, const CgState& cg,
+                       const CgLoop& lp, cudaGraphConditionalHandle cond, bool use_cond, cudaStream_t st) {
+    const u32 m = S.m;
+    const size_t tot = size_t(m) * R;
+    launch_apply<T>(d, S, W, p, R, q, t, part, small, st);
+    int h = d.begin(GpuAbsorber::P_VECTOR, st);
+    k_pq_gamma<T><<<GRID_V, THREADS, 0, st>>>(p, q, m, R, d.cta.p, cg, lp);
+    k_update_xr_sum<T><<<GRID_V, THREADS, 0, st>>>(x, r, p, q, rhs_true, x0, m, R, d.cta.p, cg, lp);
+    d.launches += 2;
+    d.end(h, st);
+    launch_precond<T>(d, S, small_ok, r, z, R, st);
+    h = d.begin(GpuAbsorber::P_VECTOR, st);
+    k_rz_stop<T><<<GRID_V, THREADS, 0, st>>>(r, z, m, R, d.cta.p, cg, lp, PROBE_FROM, PROBE_AT);
+    k_update_p_cond<T><<<grid_for(tot), THREADS, 0, st>>>(p, z, cg.beta, cg.active, m, R, lp, cond, use_cond ? 1 : 0);
+    d.launches += 2;
+    d.end(h, st);
+    CK(cudaGetLastError());
+}
+
+// The graph of one iteration body under a WHILE node, captured on `st` (the body kernels with
+// their current arguments).
+template <class T>
+Scratch::PcgGraph capture_iteration(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x,
+                                    const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small,
+                                    int R, const CgState& cg, const CgLoop& lp, cudaStream_t st,
+                                    std::vector<u64> key) {
+    const auto t0 = std::chrono::steady_clock::now();
+    Scratch::PcgGraph gr;
+    gr.key = std::move(key);
+    CK(cudaGraphCreate(&gr.g, 0));
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, gr.g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, gr.g, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    const u64 launches0 = d.launches;
+    CK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    enqueue_iteration<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part, small, R, cg, lp, cond, true, st);
+    CK(cudaStreamEndCapture(st, &body));
+    gr.body_launches = d.launches - launches0;
+    d.launches = launches0;  // counted when the graph runs
+    CK(cudaGraphInstantiate(&gr.exec, gr.g, 0));
+    d.graph_captures++;
+    d.graph_build_us += std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+    return gr;
+}
+
 // One PCG run (cg.rs:132-292) on the m x R system S d = b in precision T, from d = 0 unless
 // `x_is_start` (then d holds the start and b - S d is formed first). The stopping rule tests the
 // FP64 quantities of the full iterate x0 + d: ss_k = ss1 - (x0'rhs + d'rhs + x0'r + d'r), with
@@ -1310,9 +1504,10 @@ SolveInfo GpuAbsorber::residualize_device(double* z_dev, size_t r, double tol, s
 // rhohat = (rho_12 / rho_7)^(1/5) of the slowest active column is measured (cg.rs:24-37,
 // 254-279); above PROBE_RATIO the system escalates (when `escalate` can) and PCG restarts from
 // the current x.
-constexpr int PROBE_FROM = 7, PROBE_AT = 12;
-constexpr double PROBE_RATIO = 0.6;
-
+// The iterations run on the device: without phase timing, as launches of a captured graph whose
+// WHILE node repeats the body until every column stopped or the launch's cap is reached (the
+// host looks at the loop state only between launches: at the probe, at the cap, at the end);
+// with phase timing, one body at a time with the host reading the state after each.
 template <class T>
 static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x, const T* b,
                    const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small, int R, double tol,
@@ -1320,9 +1515,20 @@ static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool sma
                    const std::function<bool(double)>& escalate) {
     const size_t m = S.m, tot = m * size_t(R);
     CgState cg = d.cg();
+    d.lp_ctl.alloc(4);
+    d.lp_ticket.alloc(4);
+    d.lp_rho_from.alloc(size_t(R));
+    d.lp_rho_at.alloc(size_t(R));
+    d.lp_act.alloc(size_t(R));
+    d.lp_tol.alloc(1);
+    CK(cudaMemsetAsync(d.lp_ticket.p, 0, 4 * sizeof(unsigned), st));
+    std::memcpy(d.h_nactive + 6, &tol, sizeof(double));  // pinned words 6-7
+    CK(cudaMemcpyAsync(d.lp_tol.p, d.h_nactive + 6, sizeof(double), cudaMemcpyHostToDevice, st));
+    const CgLoop lp{d.lp_ctl.p, d.lp_tol.p, d.lp_ticket.p, d.lp_rho_from.p, d.lp_rho_at.p, d.lp_act.p};
     u64 it = 0;
     std::vector<double> rho_from(R), rho_at(R);
     std::vector<int> act(R);
+    int* hc = d.h_nactive;  // pinned [n_active, k, k of the launch, cap]
 restart:
     if (x_is_start) {
         launch_apply<T>(d, S, W, x, R, q, t, part, small, st);
@@ -1338,47 +1544,65 @@ restart:
     k_cg_start<<<1, THREADS, 0, st>>>(cg, R, drop);
     k_mask_copy<T><<<grid_for(tot), THREADS, 0, st>>>(p, z, d.cg_active.p, tot, R);
     d.launches += 3;
-    CK(cudaMemcpyAsync(d.h_nactive, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemsetAsync(d.lp_ctl.p, 0, 4 * sizeof(int), st));  // k = 0 since the (re)start
+    CK(cudaMemcpyAsync(hc, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     d.end(h, st);
     CK(cudaStreamSynchronize(st));
-    bool any_active = *d.h_nactive > 0;
+    bool any_active = hc[0] > 0;
     int k = 0;
+    bool probed = false;
     while (any_active) {
-        if (iters_done + it >= maxiter) {
+        ctx.check();
+        // iterations this launch may run: up to the probe, the cap and maxiter
+        long long cap = GRAPH_CAP;
+        if (escalate && !probed && k < PROBE_AT) cap = std::min<long long>(cap, PROBE_AT - k);
+        const long long left = (long long)maxiter - (long long)(iters_done + it);
+        if (left <= 0) {
             std::ostringstream os;
             os << "convergence not achieved in " << maxiter << " iterations";
             throw Error(RC_CONVERGENCE, os.str());
         }
-        ctx.check();
-        launch_apply<T>(d, S, W, p, R, q, t, part, small, st);
-        h = d.begin(GpuAbsorber::P_VECTOR, st);
-        k_dot<T><<<GRID_V, THREADS, 0, st>>>(p, q, u32(m), R, d.cta.p);
-        reduce_cols(d, d.cta.p, GRID_V, R, d.cg_pq.p, st);
-        k_cg_gamma<<<1, THREADS, 0, st>>>(cg, R);
-        k_update_xr<T><<<GRID_V, THREADS, 0, st>>>(x, r, p, q, rhs_true, x0, d.cg_gamma.p, u32(m), R, d.cta.p);
-        reduce_cols(d, d.cta.p, GRID_V, 3 * R, d.cg_xb.p, st);
-        d.launches += 3;
-        d.end(h, st);
-        launch_precond<T>(d, S, small_ok, r, z, R, st);
-        h = d.begin(GpuAbsorber::P_VECTOR, st);
-        k_dot<T><<<GRID_V, THREADS, 0, st>>>(r, z, u32(m), R, d.cta.p);
-        reduce_cols(d, d.cta.p, GRID_V, R, d.cg_rho_new.p, st);
-        it++;
-        k++;
-        k_cg_stop<<<1, THREADS, 0, st>>>(cg, R, k, tol);
-        k_update_p<T><<<grid_for(tot), THREADS, 0, st>>>(p, z, d.cg_beta.p, d.cg_active.p, u32(m), R);
-        d.launches += 3;
-        CK(cudaMemcpyAsync(d.h_nactive, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        if (escalate && (k == PROBE_FROM || k == PROBE_AT)) {
-            CK(cudaMemcpyAsync(k == PROBE_FROM ? rho_from.data() : rho_at.data(), d.cg_rho.p, R * sizeof(double),
-                               cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(act.data(), d.cg_active.p, R * sizeof(int), cudaMemcpyDeviceToHost, st));
+        cap = std::min(cap, left);
+        if (d.prof) cap = 1;  // phase timing: one body per launch, timed by events
+        hc[4] = 0;
+        hc[5] = int(cap);
+        CK(cudaMemcpyAsync(d.lp_ctl.p + 2, hc + 4, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+        const Scratch::PcgGraph* gr = nullptr;
+        if (!d.prof) {
+            for (auto& A : d.amg) amg_alloc<T>(A, R);
+            std::vector<u64> key = body_key<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part, small, R);
+            for (auto& q_ : d.graphs)
+                if (q_.key == key) gr = &q_;
+            if (!gr) {
+                // a new body: this batch runs one iteration by launches (first uses of its kernels
+                // set their attributes), and the body is captured for the next batches
+                enqueue_iteration<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part, small, R, cg, lp, 0, false,
+                                     st);
+                if (d.graphs.size() >= 8) d.drop_graphs();
+                d.graphs.push_back(capture_iteration<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part,
+                                                        small, R, cg, lp, st, std::move(key)));
+            } else {
+                CK(cudaGraphLaunch(gr->exec, st));
+                d.graph_launches++;
+            }
+        } else {
+            enqueue_iteration<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part, small, R, cg, lp, 0, false,
+                                 st);
         }
-        d.end(h, st);
+        CK(cudaMemcpyAsync(hc, d.lp_ctl.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(st));
-        any_active = *d.h_nactive > 0;
-        if (escalate && any_active && k == PROBE_AT) {
+        const int ran_now = hc[2];
+        it += u64(ran_now);
+        if (gr) d.launches += u64(ran_now) * gr->body_launches;
+        k = hc[1];
+        any_active = hc[0] > 0;
+        if (escalate && any_active && !probed && k >= PROBE_AT) {
+            probed = true;
+            CK(cudaMemcpyAsync(rho_from.data(), d.lp_rho_from.p, R * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(rho_at.data(), d.lp_rho_at.p, R * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(act.data(), d.lp_act.p, R * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
             double rho_hat = 0.0;
             for (int j = 0; j < R; j++)
                 if (act[j] == 1 && rho_from[j] > 0.0)
@@ -1510,14 +1734,18 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.rhs.p, d.frhs.p, tot);
             d.launches++;
             iterations = 0;
-            bool start_nonzero = warm != nullptr || have_last;
-            for (int round = 0; round < REFINE_ROUNDS; round++) {
-                // true residual b = rhs - S x in FP64, x'rhs, and the FP32 copies
-                if (start_nonzero) {
+            std::vector<double> rho64(r, 0.0), rho_prev(r, 0.0);
+            bool have_r = false;  // d.r holds the FP64 true residual of x
+            const bool start_nonzero = warm != nullptr || have_last;
+            bool accepted = false;
+            for (int round = 0; round < REFINE_ROUNDS && !accepted; round++) {
+                // true residual b = rhs - S x in FP64 (kept from the previous round's check), x'rhs,
+                // and the FP32 copies
+                if (!have_r && start_nonzero) {
                     launch_apply<double>(d, S, W, x, R, d.q.p, d.t.p, d.part.p, d.small.p, st);
                     k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhs.p, d.q.p, tot);
                     d.launches++;
-                } else {
+                } else if (!have_r) {
                     CK(cudaMemcpyAsync(d.r.p, d.rhs.p, tot * 8, cudaMemcpyDeviceToDevice, st));
                 }
                 k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.rhs.p, u32(m), R, d.cta.p);
@@ -1532,15 +1760,42 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
                                              REFINE_DROP, iterations, maxiter, false, ctx_, st, esc);
                 k_add_correction<<<grid_for(tot), THREADS, 0, st>>>(x, d.fx.p, tot);
                 d.launches++;
-                start_nonzero = true;
-                // columns stopped by the FP32 precision floor go another round
+                // the round's check in FP64: true residual, its preconditioned norm and ss_k
+                launch_apply<double>(d, S, W, x, R, d.q.p, d.t.p, d.part.p, d.small.p, st);
+                k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhs.p, d.q.p, tot);
+                launch_precond<double>(d, S, small_ok_, d.r.p, d.z.p, R, st);
+                k_dot<double><<<GRID_V, THREADS, 0, st>>>(d.r.p, d.z.p, u32(m), R, d.cta.p);
+                reduce_cols(d, d.cta.p, GRID_V, R, d.cg_rho.p, st);
+                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.rhs.p, u32(m), R, d.cta.p);
+                reduce_cols(d, d.cta.p, GRID_V, R, d.cg_xconst.p, st);
+                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.r.p, u32(m), R, d.cta.p);
+                reduce_cols(d, d.cta.p, GRID_V, R, d.cg_pq.p, st);
+                k_refine_accept<<<1, THREADS, 0, st>>>(d.cg(), R, tol);
+                d.launches += 5;
+                have_r = true;
+                CK(cudaMemcpyAsync(d.h_nactive, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(rho64.data(), d.cg_rho.p, r * sizeof(double), cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(act.data(), d.cg_active.p, r * sizeof(int), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
-                bool again = false;
-                for (size_t j = 0; j < r; j++) again |= act[j] == 2;
-                if (!again) break;
-                for (size_t j = 0; j < r; j++) act[j] = act[j] == 2 ? 1 : 0;
-                CK(cudaMemcpyAsync(d.cg_active.p, act.data(), r * sizeof(int), cudaMemcpyHostToDevice, st));
+                accepted = d.h_nactive[0] == 0;
+                // a round that cut no remaining column's FP64 residual norm tenfold is at the limit
+                // of FP32 (on an ill-conditioned graph S P of smooth vectors cancels below FP32
+                // precision): the remaining columns finish in FP64
+                bool progress = round == 0;
+                for (size_t j = 0; j < r && !progress; j++)
+                    progress = act[j] == 1 && rho64[j] <= 0.1 * rho_prev[j];
+                rho_prev = rho64;
+                if (!accepted && !progress) break;
+            }
+            if (!accepted) {
+                // FP64 PCG from the refined iterate on the columns not yet accepted, under the
+                // reference's stopping rule on the full iterate (x0 = 0, x'rhs in the rule)
+                CK(cudaMemsetAsync(d.cg_xconst.p, 0, r * 8, st));
+                CK(cudaMemsetAsync(d.cg_ring.p, 0, r * WINDOW * 8, st));
+                iterations += run_pcg<double>(d, S, W, small_ok_, x, d.rhs.p, d.rhs.p, nullptr, d.r.p, d.z.p, d.p.p,
+                                              d.q.p, d.t.p, d.part.p, d.small.p, R, tol, 0.0, iterations, maxiter, true,
+                                              ctx_, st, esc);
+                d.fp64_finishes++;
             }
             iterations = std::max<u64>(iterations, 1);
             exact = false;
@@ -1605,6 +1860,13 @@ void GpuAbsorber::phase_times(double* ms, u64* counts) const {
 }
 
 u64 GpuAbsorber::launches() const { return d_->launches; }
+
+void GpuAbsorber::solver_stats(u64* o) const {
+    o[0] = d_->graph_captures;
+    o[1] = d_->graph_launches;
+    o[2] = u64(d_->graph_build_us);
+    o[3] = d_->fp64_finishes;
+}
 
 void GpuAbsorber::fit_rows(const double* coefs, size_t r, size_t col, double* out) const {
     AllocScope alloc_scope(stream_);

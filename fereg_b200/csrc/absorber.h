@@ -102,6 +102,8 @@ class GpuAbsorber {
     void set_profiling(bool on);
     void phase_times(double* ms, u64* counts) const;
     u64 launches() const;
+    // [graphs captured, graph launches, host us of the captures, FP32-refined solves finished in FP64]
+    void solver_stats(u64* out4) const;
     // Large blocks currently preconditioned by a multigrid V-cycle, and the escalations so far.
     size_t escalated_blocks() const;
     u64 escalations() const;
@@ -152,6 +154,7 @@ class GpuAbsorber {
     void build_small_device();
 
     void refresh_weights(const double* w_kept);
+    void build_srow();
     void sync_host_weights() const;
     void upload_weights();
     void ensure_precond();

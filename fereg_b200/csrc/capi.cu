@@ -7,6 +7,7 @@
 #include "../../include/fereg_b200.h"
 #include "absorber.h"
 #include "amg.h"
+#include "dstruct.h"
 #include "prep.h"
 #include "server.h"
 #include "session.h"
@@ -237,6 +238,20 @@ int fereg_session_info(const fereg_session* s, uint64_t* o) {
     return guard([&] {
         if (!s || !o) throw Error(RC_INVALID_INPUT, "fereg_session_info: NULL argument");
         fill_info(s->s.absorber(), o);
+    });
+}
+
+int fereg_absorber_solver_stats(const fereg_absorber* h, uint64_t* o) {
+    return guard([&] {
+        if (!h || !o) throw Error(RC_INVALID_INPUT, "fereg_absorber_solver_stats: NULL argument");
+        h->a.solver_stats(o);
+    });
+}
+
+int fereg_session_solver_stats(const fereg_session* s, uint64_t* o) {
+    return guard([&] {
+        if (!s || !o) throw Error(RC_INVALID_INPUT, "fereg_session_solver_stats: NULL argument");
+        s->s.absorber().solver_stats(o);
     });
 }
 
@@ -635,6 +650,58 @@ int fereg_structure_digest(const uint32_t* const* codes, const uint32_t* g, int 
         out[4] = hs.nb();
         out[5] = u64(int64_t(hs.fe1));
         out[6] = h;
+    });
+}
+
+int fereg_structure_compare(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, uint64_t* out) {
+    return guard([&] {
+        if (!codes || !g || nterms < 1 || !out) throw Error(RC_INVALID_INPUT, "fereg_structure_compare: NULL argument");
+        std::vector<const u32*> c(codes, codes + nterms);
+        std::vector<u32> gg(g, g + nterms);
+        const HostStructure hs = build_structure(c, gg, n, SMALL_LIMIT);
+        const PullTable pt = build_pull_table(hs);
+        cudaStream_t st = nullptr;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamDestroy(s); }
+        } sg{st};
+        AllocScope alloc_scope(st);
+        std::vector<DBuf<u32>> dc(static_cast<size_t>(nterms));
+        std::vector<const u32*> dptr;
+        for (int q = 0; q < nterms; q++) {
+            dc[size_t(q)].upload(c[size_t(q)], n, st);
+            dptr.push_back(dc[size_t(q)].p);
+        }
+        HostStructure dh = plan_structure(c, gg, n, SMALL_LIMIT);
+        DeviceStructure ds;
+        std::vector<u32> poff, pseg;
+        build_structure_device(dptr, gg, dh, ds, poff, pseg, st);
+        auto fetch = [&](const DBuf<u32>& b, size_t count) {
+            std::vector<u32> h(count);
+            if (count) CK(cudaMemcpyAsync(h.data(), b.p, count * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            return h;
+        };
+        auto diff = [](const std::vector<u32>& a, const std::vector<u32>& b) {
+            if (a.size() != b.size()) return u64(1) << 40;
+            u64 k = 0;
+            for (size_t i = 0; i < a.size(); i++) k += a[i] != b[i];
+            return k;
+        };
+        const size_t M = dh.ncells, E = M * dh.nb();
+        out[0] = (dh.ncells != hs.ncells) + (dh.fe1 != hs.fe1) + (dh.m != hs.m) + (dh.m_small != hs.m_small) +
+                 (dh.small_work != hs.small_work) + (dh.g1 != hs.g1) + (dh.nb() != hs.nb());
+        for (size_t b = 0; b < std::min(dh.nb(), hs.nb()); b++)
+            out[0] += dh.blocks[b].small != hs.blocks[b].small || dh.blocks[b].off != hs.blocks[b].off;
+        out[1] = diff(dh.pi, hs.pi);
+        out[2] = diff(dh.seg_off, hs.seg_off);
+        out[3] = diff(dh.cell_row, hs.cell_row);
+        out[4] = diff(fetch(ds.coord, dh.nb() * M), hs.coord);
+        out[5] = diff(poff, pt.off);
+        out[6] = diff(fetch(ds.pl_cell, E), pt.cell);
+        out[7] = diff(pseg, pt.seg);
+        out[8] = diff(fetch(ds.pl_other, E * (dh.nb() > 0 ? dh.nb() - 1 : 0)), pt.other);
     });
 }
 

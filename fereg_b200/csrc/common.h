@@ -63,6 +63,10 @@ struct HostStructure {
 // structure.rs:23 SMALL_LIMIT.
 constexpr size_t SMALL_LIMIT = 4096;
 
+// The eliminated term, the blocks and their coordinate offsets (structure.rs:247-378), without the
+// per-row arrays.
+HostStructure plan_structure(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n,
+                             size_t small_limit);
 HostStructure build_structure(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n,
                               size_t small_limit);
 int fe1_index(const std::vector<u32>& g);

@@ -191,6 +191,30 @@ __global__ void k_cg_stop(CgState st, int R, int k, double tol) {
     if (threadIdx.x == 0) *st.n_active = cnt;
 }
 
+// End of an FP32 refinement round, on the FP64 quantities of the refined iterate x: rho = r'M^-1 r
+// of its true residual, xconst = x'rhs, pq = x'r. A column is accepted (state 0) only when
+// rho <= max(tol^2 ss_k, floor) with ss_k = ss1 - x'(rhs + r), whether the round ended it by the
+// FP32 window rule (whose recursive residual can fall below the true one) or at the FP32 floor;
+// otherwise it goes another round (state 1). Columns without variation (floor 0) stay stopped.
+__global__ void k_refine_accept(CgState st, int R, double tol) {
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    int local = 0;
+    for (int j = threadIdx.x; j < R; j += blockDim.x) {
+        if (st.floor_[j] > 0.0) {
+            const double ssk = st.ss1[j] - (st.xconst[j] + st.pq[j]);
+            const double thr = fmax(tol * tol * ssk, st.floor_[j]);
+            const bool ok = st.rho[j] <= thr;
+            st.active[j] = ok ? 0 : 1;
+        }
+        local += st.active[j] == 1;
+    }
+    atomicAdd(&cnt, local);  // integer count: order independent
+    __syncthreads();
+    if (threadIdx.x == 0) *st.n_active = cnt;
+}
+
 // p = z + beta p on the active columns, 0 on the others.
 template <class T>
 __global__ void k_update_p(T* __restrict__ p, const T* __restrict__ z, const double* __restrict__ beta,
@@ -239,6 +263,45 @@ template <class T>
 __global__ void k_add_active(T* __restrict__ x, const T* __restrict__ z, const int* __restrict__ active, size_t total, int R) {
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x)
         if (active[i % R] == 1) x[i] += z[i];
+}
+
+// The small coordinates' rows of Y = S P from the dense rows of S (srow, weights.cuh): CTA b
+// takes the coordinates f of its chunk; with at most TB (k, j) pairs the threads are (slot, pair)
+// and slot s adds srow[f][k] P[f][j] over the chunk's f = s, s + slots, ... (loads unrolled),
+// the slots' sums are then added in slot order into part[b][k * R + j]; with more pairs each
+// thread takes pairs in turn over the whole chunk. k_small_reduce adds the CTAs' partials in CTA
+// order.
+template <class T>
+__global__ void __launch_bounds__(TB) k_srow_apply(const double* __restrict__ srow, u32 m, u32 ms,
+                                                   const T* __restrict__ P, int R, T* __restrict__ part) {
+    __shared__ T red[TB];
+    const u32 npairs = ms * u32(R);
+    const u32 chunk = (m + gridDim.x - 1) / gridDim.x;
+    const u32 f0 = min(m, blockIdx.x * chunk), f1 = min(m, f0 + chunk);
+    if (npairs <= u32(TB)) {
+        const u32 nslot = u32(TB) / npairs, slot = threadIdx.x / npairs, pi = threadIdx.x % npairs;
+        const u32 k = pi / u32(R), j = pi % u32(R);
+        T acc = T(0);
+        if (slot < nslot) {
+#pragma unroll 4
+            for (u32 f = f0 + slot; f < f1; f += nslot) acc += T(srow[size_t(f) * ms + k]) * P[size_t(f) * R + j];
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        if (threadIdx.x < npairs) {
+            T sum = T(0);
+            for (u32 sl = 0; sl < nslot; sl++) sum += red[sl * npairs + threadIdx.x];
+            part[size_t(blockIdx.x) * npairs + threadIdx.x] = sum;
+        }
+        return;
+    }
+    for (u32 pi = threadIdx.x; pi < npairs; pi += blockDim.x) {
+        const u32 k = pi / u32(R), j = pi % u32(R);
+        T acc = T(0);
+#pragma unroll 4
+        for (u32 f = f0; f < f1; f++) acc += T(srow[size_t(f) * ms + k]) * P[size_t(f) * R + j];
+        part[size_t(blockIdx.x) * npairs + pi] = acc;
+    }
 }
 
 // Jacobi on coordinates [k0, m): z = inv_diag .* r (precond/jacobi.rs:12-42).

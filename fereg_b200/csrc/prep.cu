@@ -120,6 +120,30 @@ void check_codes(const u32* c, size_t n, u32 g, const char* what) {
 
 }  // namespace
 
+u32 device_excl_scan(const u32* in, size_t n, u32* out, cudaStream_t st) { return excl_scan(in, n, out, st); }
+
+void device_sort_pairs(u64*& keys, u32*& vals, u64* keys_alt, u32* vals_alt, size_t n, int bits, cudaStream_t st) {
+    if (n == 0 || bits <= 0) return;
+    DBuf<u32> hist, offs;
+    const u32 ntiles = u32((n + RS_TILE - 1) / RS_TILE);
+    hist.alloc(size_t(ntiles) * 256);
+    offs.alloc(size_t(ntiles) * 256);
+    u64* ka = keys;
+    u64* kb = keys_alt;
+    u32* va = vals;
+    u32* vb = vals_alt;
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_rs_hist<<<ntiles, RS_TB, 0, st>>>(ka, n, shift, ntiles, hist.p);
+        excl_scan(hist.p, size_t(ntiles) * 256, offs.p, st);
+        k_rs_scatter<<<ntiles, RS_TB, 0, st>>>(ka, va, n, shift, ntiles, offs.p, kb, vb);
+        CK(cudaGetLastError());
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    keys = ka;
+    vals = va;
+}
+
 u32 prep_factorize(const double* x, size_t n, u32* codes_out) {
     if (n == 0) return 0;
     Stream S;

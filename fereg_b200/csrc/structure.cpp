@@ -107,8 +107,8 @@ static int choose_elimination(const std::vector<const u32*>& codes, const std::v
     return int(best_f);
 }
 
-HostStructure build_structure(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n,
-                              size_t small_limit) {
+HostStructure plan_structure(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n,
+                             size_t small_limit) {
     HostStructure st;
     st.n = n;
     st.fe1 = choose_elimination(codes, g, n);
@@ -138,6 +138,12 @@ HostStructure build_structure(const std::vector<const u32*>& codes, const std::v
     st.m = off;
     for (auto& b : st.blocks)
         if (b.small) st.m_small += b.g;
+    return st;
+}
+
+HostStructure build_structure(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n,
+                              size_t small_limit) {
+    HostStructure st = plan_structure(codes, g, n, small_limit);
     const size_t nb = st.blocks.size();
 
     // Rows by (FE1, block codes, obs): check the order first (panels usually arrive sorted).

@@ -241,4 +241,72 @@ __global__ void __launch_bounds__(256) k_vec_sum(const double* __restrict__ v, s
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
+// ---------------------------------------------------------------------------------------------
+// The rows of S on the small coordinates, for the operator (operator.rs:894-948 restated as a
+// product): with at most SACC_MAX small coordinates (blocks 0..ns-1, coordinates 0..ms-1),
+//   S[k][f] = sum_{c containing k and f} W_c - sum_s c_{s,k} c_{s,f} / n1_s,
+// with c_{s,k} the weight of the cells of segment s that hold k. The operator then takes
+// Y[k] = sum_f S[k][f] P[f] for the small k from this dense ms x m block (stored transposed,
+// srow[f * ms + k], f over every coordinate) instead of accumulating per cell in the segment
+// pass. srow depends on the weights: it is rebuilt with every weight state.
+
+// c_{s,k} for every segment s and small coordinate k < ms: one thread per (segment, k), the
+// segment's cells in order.
+__global__ void k_seg_small_w(const u32* __restrict__ seg_off, const u32* __restrict__ coord, u32 M, u32 g1, int ns,
+                              u32 ms, const double* __restrict__ cw, double* __restrict__ csk) {
+    const size_t total = size_t(g1) * ms;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const u32 s = u32(i / ms), k = u32(i % ms);
+        double a = 0.0;
+        for (u32 c = seg_off[s]; c < seg_off[s + 1]; c++) {
+            const double w = cw ? cw[c] : 1.0;
+            for (int b = 0; b < ns; b++)
+                if (coord[size_t(b) * M + c] == k) a += w;
+        }
+        csk[i] = a;
+    }
+}
+
+// Partial rows of srow by work items: item i covers entries [item_a, item_b) of the coordinate
+// list of f = item_f (whole runs of equal segment). One warp per item, lane k < ms holding
+// S[k][f] over the item: for every entry (cell c of segment s) W_c when c holds k; at the end of
+// each run of segment s, - c_{s,k} c_{s,f} / n1_s with c_{s,f} the run's weight sum. Every lane
+// sums in entry order; k_srow_sum adds the items of a coordinate in item order.
+__global__ void __launch_bounds__(256) k_srow_items(const u32* __restrict__ coord, u32 M, int ns, u32 ms,
+                                                    const double* __restrict__ cw, const double* __restrict__ n1inv,
+                                                    const u32* __restrict__ pl_cell, const u32* __restrict__ pl_seg,
+                                                    const double* __restrict__ csk, const u32* __restrict__ item_a,
+                                                    const u32* __restrict__ item_b, u32 nitems,
+                                                    double* __restrict__ part) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (it >= nitems) return;  // whole warps
+    const u32 b = item_b[it];
+    double acc = 0.0, run = 0.0;
+    for (u32 e = item_a[it]; e < b; e++) {
+        const u32 c = pl_cell[e], s = pl_seg[e];
+        const double w = cw ? cw[c] : 1.0;
+        for (int bb = 0; bb < ns; bb++)
+            if (coord[size_t(bb) * M + c] == lane) acc += w;
+        run += w;
+        if (e + 1 == b || pl_seg[e + 1] != s) {
+            if (lane < ms) acc -= csk[size_t(s) * ms + lane] * run * n1inv[s];
+            run = 0.0;
+        }
+    }
+    if (lane < ms) part[size_t(it) * ms + lane] = acc;
+}
+
+// srow[f * ms + k] = the partial rows of f's items (first[f] .. first[f+1]) added in item order.
+__global__ void k_srow_sum(const double* __restrict__ part, const u32* __restrict__ first, u32 m, u32 ms,
+                           double* __restrict__ srow) {
+    const size_t total = size_t(m) * ms;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const u32 f = u32(i / ms), k = u32(i % ms);
+        double v = 0.0;
+        for (u32 it = first[f]; it < first[f + 1]; it++) v += part[size_t(it) * ms + k];
+        srow[i] = v;
+    }
+}
+
 }  // namespace fereg

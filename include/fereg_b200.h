@@ -291,6 +291,11 @@ int fereg_amg_probe(const uint32_t* const* codes, const uint32_t* g, int nterms,
  * segment offsets, first rows, cell coordinates and coordinate lists (out[6]). The host build is
  * parallel; the digest shows it does not depend on the thread count. */
 int fereg_structure_digest(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, uint64_t* out);
+/* Test hook (device): builds the cell structure and coordinate lists of the codes both on the host
+ * and on the device and counts the differences: out9 = [scalars and block flags, row order,
+ * seg_off, cell_row, coord, list offsets, list cells, list segments, list other-block
+ * coordinates]; all 0 when the device build is the host build element for element. */
+int fereg_structure_compare(const uint32_t* const* codes, const uint32_t* g, int nterms, size_t n, uint64_t* out9);
 
 /* Sample preparation on the device (Session::prepare's FE-id compression and sample drops;
  * host arrays in and out). Bit-exact with the reference's definitions.
@@ -388,6 +393,13 @@ int fereg_session_phase_times(const fereg_session* s, double* ms, uint64_t* coun
 
 /* fereg_absorber_info of the session's absorber (9 values). */
 int fereg_session_info(const fereg_session* s, uint64_t* out9);
+
+/* Counters of the device PCG loop since the handle was made (no counterpart in the reference):
+ * out4 = [iteration graphs captured, graph launches, host microseconds spent capturing and
+ * instantiating them, FP32-refined solves that finished in FP64]. */
+int fereg_absorber_solver_stats(const fereg_absorber* h, uint64_t* out4);
+/* fereg_absorber_solver_stats of the session's absorber. */
+int fereg_session_solver_stats(const fereg_session* s, uint64_t* out4);
 
 /* Kernel launches of the session so far (its passes and its absorber), and its CUDA stream. */
 uint64_t fereg_session_launches(const fereg_session* s);
