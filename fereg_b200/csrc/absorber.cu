@@ -18,6 +18,7 @@
 #include "absorber.h"
 #include "amg.cuh"
 #include "amg.h"
+#include "dstruct.h"
 #include "pcg.cuh"
 #include "weights.cuh"
 
@@ -28,6 +29,8 @@ constexpr int THREADS = TB;
 constexpr int GRID_T = 148 * 6;  // tile kernels: up to 6 resident CTAs per SM
 constexpr int GRID_V = 148 * 2;  // vector kernels with per-CTA partials
 constexpr int GRID_S = 148 * 4;  // warp-tile kernels (CTAs of WPB warps)
+constexpr size_t SMALL_STAGE_MAX = 16 * 1024;  // shared memory for the staged small rows of a chunk
+constexpr u32 VSEG_MAX = 256;  // longest segment (cells) a lane group walks in the operator's segment pass
 constexpr double REDUNDANT = 1e-12;  // operator.rs:21
 // Largest small super-block factored densely on the device. Beyond it the small coordinates keep
 // Jacobi, as the reference does when the dense factor costs more than a few PCG iterations
@@ -111,6 +114,18 @@ void with_lanes(int Rc, u32 nb, F&& f, int L = 0) {
         default: with_nbk<16, MIN_NBK>(nb, f); break;
     }
 }
+// Lane groups of the padded-vector passes: vlanes_of(Rc) lanes of 4 columns each (1 to 32).
+template <class F>
+void with_vlanes(int Rc, u32 nb, F&& f) {
+    switch (vlanes_of(Rc)) {
+        case 1: with_nbk<1, 1>(nb, f); break;
+        case 2: with_nbk<2, 1>(nb, f); break;
+        case 4: with_nbk<4, 1>(nb, f); break;
+        case 8: with_nbk<8, 1>(nb, f); break;
+        case 16: with_nbk<16, 1>(nb, f); break;
+        default: with_nbk<32, 1>(nb, f); break;
+    }
+}
 template <int MIN_NBK = 0, class F>
 void with_rcp(int Rc, u32 nb, F&& f) {
     switch (rcp_of(Rc)) {
@@ -156,10 +171,13 @@ struct Scratch {
     DevTiles seg_tiles, pull_tiles;      // CTA tiles of the long lists
     DevWarpTiles wseg, wpull;            // warp tiles of the short lists
     DBuf<u32> wseg_segs;                 // the segments of the warp tiles, in order
+    DBuf<u32> aseg_segs;                 // the operator's lane-group segments (at most VSEG_MAX cells)
+    DevTiles aseg_tiles;                 // the operator's CTA tiles (longer segments)
     u32 ms_acc = 0, ns_acc = 0;  // small coordinates / blocks summed in the segment passes
     // weights
     DBuf<double> w_rows, cell_w, n1inv, nr, inv_diag, minv;
     DBuf<double> n1, diag, wpart;  // device weight refresh
+    DBuf<u32> pi;                  // the row order (kept observation of each row)
     DBuf<u32> cw_e0, cw_e1, cw_list_off;  // chunks of the coordinate lists (weights.cuh)
     DBuf<double> cw_chunks;
     u32 cw_nchunks = 0;
@@ -177,6 +195,7 @@ struct Scratch {
     DBuf<int> wflag;
     // solve (FP64)
     DBuf<double> rows, rhs, b1, coefs, r, z, p, q, t, part, cta, cta2, colsum, along, small;
+    DBuf<double> rhsv, xv;  // the padded right-hand side and iterate of the PCG
     // inner FP32 buffers of the refined solve
     DBuf<float> fx, fb, fr, fz, fp, fq, ft, fpart, frhs, fx0, fsmall;
     DBuf<double> cg_rho, cg_rho_new, cg_pq, cg_gamma, cg_beta, cg_xb, cg_ss1, cg_floor, cg_ring, cg_xconst, cg_pfloor;
@@ -288,15 +307,11 @@ struct Scratch {
 };
 
 GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector<u32>& g, const double* w, size_t n,
-                         const Ctx& ctx)
+                         const Ctx& ctx, const std::vector<const u32*>* dev_codes)
     : g_(g), ctx_(ctx) {
-    for (size_t q = 0; q < codes.size(); q++)
-        for (size_t i = 0; i < n; i++)
-            if (codes[q][i] >= g[q]) throw Error(RC_INVALID_INPUT, "term code out of range of its level count");
-    if (w)
-        for (size_t i = 0; i < n; i++)
-            if (!(std::isfinite(w[i]) && w[i] > 0.0)) throw Error(RC_INVALID_INPUT, "weights must be positive and finite");
-    hs_ = build_structure(codes, g, n, SMALL_LIMIT);
+    check_codes_host(codes, g, n);
+    if (w) check_weights_host(w, n);
+    hs_ = plan_structure(codes, g, n, SMALL_LIMIT);
     norm_fe1_ = fe1_index(g);
     ctx_.check();
     if (ctx_.priority_level < 0) {
@@ -310,9 +325,32 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
     AllocScope alloc_scope(stream_);
     d_ = std::make_unique<Scratch>();
     CK(cudaHostAlloc(&d_->h_nactive, 8 * sizeof(int), cudaHostAllocDefault));
-    d_->seg_off.upload(hs_.seg_off, stream_);
-    d_->coord.upload(hs_.coord, stream_);
-    if (!hs_.trivial()) d_->cell_row.upload(hs_.cell_row, stream_);
+    // the cell structure and coordinate lists, built on the device from device codes
+    std::vector<u32> pl_off, pl_seg;
+    {
+        std::vector<DBuf<u32>> up;
+        std::vector<const u32*> dptr;
+        if (dev_codes) {
+            dptr = *dev_codes;
+        } else {
+            up.resize(codes.size());
+            for (size_t q = 0; q < codes.size(); q++) {
+                up[q].upload(codes[q], n, stream_);
+                dptr.push_back(up[q].p);
+            }
+        }
+        DeviceStructure ds;
+        build_structure_device(dptr, g, hs_, ds, pl_off, pl_seg, stream_);
+        d_->pi = std::move(ds.pi);
+        d_->seg_off = std::move(ds.seg_off);
+        d_->coord = std::move(ds.coord);
+        d_->cell_row = std::move(ds.cell_row);
+        d_->pl_off = std::move(ds.pl_off);
+        d_->pl_cell = std::move(ds.pl_cell);
+        d_->pl_seg = std::move(ds.pl_seg);
+        d_->pl_other = std::move(ds.pl_other);
+        CK(cudaStreamSynchronize(stream_));  // the uploaded codes die here
+    }
     {
         // segments weigh max(cells, rows): short ones go to warp tiles, the others to CTA tiles
         std::vector<u32> wgt(hs_.g1);
@@ -325,11 +363,18 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
         TileList ct;
         split_tiles(hs_.seg_off, &wgt, 0, hs_.g1, WT, WT, WSEG, TILE, wt, ct);
         d_->wseg.upload(wt, stream_);
-        std::vector<u32> segs;  // the short segments in order (one per lane group in k_gseg_apply)
+        std::vector<u32> segs;  // the short segments in order (one per lane group in k_vseg_apply)
         for (size_t i = 0; i < wt.k0.size(); i++)
             for (u32 s = wt.k0[i]; s < wt.k1[i]; s++) segs.push_back(s);
         d_->wseg_segs.upload(segs, stream_);
         d_->seg_tiles.upload(ct, stream_);
+        // the operator's segment pass: lane groups walk every segment of at most VSEG_MAX cells (in
+        // order), CTA tiles take the longer ones
+        std::vector<u32> asegs;
+        for (u32 s = 0; s < hs_.g1; s++)
+            if (hs_.seg_off[s + 1] - hs_.seg_off[s] <= VSEG_MAX) asegs.push_back(s);
+        d_->aseg_segs.upload(asegs, stream_);
+        d_->aseg_tiles.upload(build_tiles(hs_.seg_off, 0, hs_.g1, TILE, VSEG_MAX), stream_);
         CK(cudaStreamSynchronize(stream_));
     }
     {
@@ -341,13 +386,12 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
         }
     }
     if (hs_.m > 0) {
-        PullTable pt = build_pull_table(hs_);
         {  // chunks of the lists for the device weight refresh (weights.cuh)
             std::vector<u32> e0, e1, loff(hs_.m + 1, 0);
             for (size_t k = 0; k < hs_.m; k++) {
-                for (u32 a = pt.off[k]; a < pt.off[k + 1]; a += CW_CHUNK) {
+                for (u32 a = pl_off[k]; a < pl_off[k + 1]; a += CW_CHUNK) {
                     e0.push_back(a);
-                    e1.push_back(std::min<u32>(pt.off[k + 1], a + CW_CHUNK));
+                    e1.push_back(std::min<u32>(pl_off[k + 1], a + CW_CHUNK));
                 }
                 loff[k + 1] = u32(e0.size());
             }
@@ -358,14 +402,14 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
         }
         if (hs_.m_small > 0 && hs_.m_small <= DENSE_SMALL_MAX) {
             // runs of each small coordinate's entries, at least `run` long, never splitting a segment
-            const u32 es = pt.off[hs_.m_small];
+            const u32 es = pl_off[hs_.m_small];
             const u32 run = std::max<u32>(256, es / 4096);
             std::vector<u32> ik, ia, ib, first(hs_.m_small + 1, 0);
             for (u32 k = 0; k < u32(hs_.m_small); k++) {
                 first[k] = u32(ik.size());
-                for (u32 a = pt.off[k]; a < pt.off[k + 1];) {
-                    u32 b = std::min(pt.off[k + 1], a + run);
-                    while (b < pt.off[k + 1] && pt.seg[b] == pt.seg[b - 1]) b++;
+                for (u32 a = pl_off[k]; a < pl_off[k + 1];) {
+                    u32 b = std::min(pl_off[k + 1], a + run);
+                    while (b < pl_off[k + 1] && pl_seg[b] == pl_seg[b - 1]) b++;
                     ik.push_back(k);
                     ia.push_back(a);
                     ib.push_back(b);
@@ -385,9 +429,9 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
             std::vector<u32> ia, ib, first(hs_.m + 1, 0);
             for (u32 f = 0; f < u32(hs_.m); f++) {
                 first[f] = u32(ia.size());
-                for (u32 a = pt.off[f]; a < pt.off[f + 1];) {
-                    u32 b = std::min(pt.off[f + 1], a + 256);
-                    while (b < pt.off[f + 1] && pt.seg[b] == pt.seg[b - 1]) b++;
+                for (u32 a = pl_off[f]; a < pl_off[f + 1];) {
+                    u32 b = std::min(pl_off[f + 1], a + 256);
+                    while (b < pl_off[f + 1] && pl_seg[b] == pl_seg[b - 1]) b++;
                     ia.push_back(a);
                     ib.push_back(b);
                     a = b;
@@ -400,19 +444,66 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
             d_->si_n = u32(ia.size());
             d_->srow_on = true;
         }
-        d_->pl_off.upload(pt.off, stream_);
-        d_->pl_cell.upload(pt.cell, stream_);
-        d_->pl_seg.upload(pt.seg, stream_);
-        d_->pl_other.upload(pt.other, stream_);
         WarpTileList wt;
         TileList ct;
-        split_tiles(pt.off, nullptr, d_->ms_acc, u32(hs_.m), PULL_WARP_MAX, PULL_WARP_MAX, WLIST, PULL_SLICE, wt, ct);
+        split_tiles(pl_off, nullptr, d_->ms_acc, u32(hs_.m), PULL_WARP_MAX, PULL_WARP_MAX, WLIST, PULL_SLICE, wt, ct);
         d_->wpull.upload(wt, stream_);
         d_->pull_tiles.upload(ct, stream_);
         CK(cudaStreamSynchronize(stream_));  // host tables die here
     }
+    // the weight state, on the device: kept-order weights gathered into row order
+    if (w) {
+        DBuf<double> wk, wr;
+        wk.upload(w, n, stream_);
+        wr.alloc(n);
+        k_gather_rows_f64<<<grid_for(n), THREADS, 0, stream_>>>(wk.p, d_->pi.p, n, wr.p);
+        d_->launches++;
+        set_weights_device(wr.p);
+        CK(cudaStreamSynchronize(stream_));
+    } else {
+        unit_weights_device();
+    }
+}
+
+// The weight state of unit row weights on the device: cell weights are the cells' row counts
+// (none when every cell holds one row), n1 the segments' row counts.
+void GpuAbsorber::unit_weights_device() {
+    AllocScope alloc_scope(stream_);
+    Scratch& d = *d_;
+    const size_t M = hs_.ncells, g1 = hs_.g1;
+    d.w_rows.release();
+    if (hs_.trivial()) {
+        d.cell_w.release();
+    } else {
+        d.cell_w.alloc(M);
+        k_cell_counts<<<grid_for(M), THREADS, 0, stream_>>>(d.cell_row.p, u32(M), d.cell_w.p);
+        d.launches++;
+    }
+    d.n1.alloc(g1);
+    d.n1inv.alloc(g1);
+    k_seg_weights<<<grid_for(g1), THREADS, 0, stream_>>>(d.cell_w.p, d.seg_off.p, u32(g1), d.n1.p, d.n1inv.p);
+    d.launches++;
+    CK(cudaGetLastError());
+    sw_ = double(hs_.n);
+    weighted_ = false;
+    host_stale_ = true;
+    coord_stale_ = hs_.m > 0;
+    refresh_coord();
+    build_srow();
+    pre_fresh_ = false;
+    small_stale_ = false;
+    amg_stale_ = true;
     CK(cudaStreamSynchronize(stream_));
-    refresh_weights(w);
+}
+
+// The host copy of the cells' block coordinates, for the host readers of the structure (the
+// multigrid setup, fit_rows), fetched from the device the first time one needs it.
+void GpuAbsorber::ensure_host_coord() const {
+    const size_t len = hs_.nb() * hs_.ncells;
+    if (len == 0 || hs_.coord.size() == len) return;
+    hs_.coord.resize(len);
+    CK(cudaMemcpyAsync(hs_.coord.data(), d_->coord.p, len * sizeof(u32), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
 }
 
 // Escalation: the reference escalates once, when the probe finds slow contraction (cg.rs:24-37,
@@ -475,6 +566,7 @@ constexpr u32 AMG_DENSE_MAX = 2048;  // the largest coarsest level inverted dens
 void GpuAbsorber::build_amg() {
     AllocScope alloc_scope(stream_);
     sync_host_weights();
+    ensure_host_coord();
     d_->amg.clear();
     for (size_t b = 0; b < hs_.blocks.size(); b++) {
         const Block& B = hs_.blocks[b];
@@ -642,7 +734,6 @@ void GpuAbsorber::refresh_coord() const {
     d.launches += 2;
     CK(cudaGetLastError());
     coord_stale_ = false;
-    dev_jacobi_ = true;
 }
 
 // Copies the device weight state back into the host mirrors after set_weights_device.
@@ -653,14 +744,15 @@ void GpuAbsorber::sync_host_weights() const {
     const HostStructure& st = hs_;
     const size_t n = st.n, M = st.ncells, g1 = st.g1, m = st.m;
     Scratch& d = *d_;
-    w_rows_.resize(n);
-    cell_w_.resize(M);
+    // unweighted: no row weights; unit cells: no cell weights (both read as 1)
+    w_rows_.resize(d.w_rows.p ? n : 0);
+    cell_w_.resize(d.cell_w.p ? M : 0);
     n1_.resize(g1);
     nr_.resize(m);
     diag_.resize(m);
     red_.resize(m);
-    CK(cudaMemcpyAsync(w_rows_.data(), d.w_rows.p, n * 8, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(cell_w_.data(), d.cell_w.p, M * 8, cudaMemcpyDeviceToHost, stream_));
+    if (d.w_rows.p) CK(cudaMemcpyAsync(w_rows_.data(), d.w_rows.p, n * 8, cudaMemcpyDeviceToHost, stream_));
+    if (d.cell_w.p) CK(cudaMemcpyAsync(cell_w_.data(), d.cell_w.p, M * 8, cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(n1_.data(), d.n1.p, g1 * 8, cudaMemcpyDeviceToHost, stream_));
     if (m > 0) {
         CK(cudaMemcpyAsync(nr_.data(), d.nr.p, m * 8, cudaMemcpyDeviceToHost, stream_));
@@ -669,78 +761,6 @@ void GpuAbsorber::sync_host_weights() const {
     }
     CK(cudaStreamSynchronize(stream_));
     host_stale_ = false;
-}
-
-// operator.rs:211-338 refresh_weights + :344-570 level_weights (host form).
-void GpuAbsorber::refresh_weights(const double* w_kept) {
-    const HostStructure& st = hs_;
-    host_stale_ = false;
-    dev_jacobi_ = false;
-    coord_stale_ = false;
-    weighted_ = w_kept != nullptr;
-    w_rows_.clear();
-    cell_w_.clear();
-    if (w_kept) {
-        w_rows_.resize(st.n);
-        for (size_t r = 0; r < st.n; r++) w_rows_[r] = w_kept[st.pi[r]];
-    }
-    if (!st.trivial()) {
-        cell_w_.resize(st.ncells);
-        for (size_t c = 0; c < st.ncells; c++) {
-            double s = 0;
-            for (u32 r = st.cell_row[c]; r < st.cell_row[c + 1]; r++) s += w_kept ? w_rows_[r] : 1.0;
-            cell_w_[c] = s;
-        }
-    } else if (w_kept) {
-        cell_w_ = w_rows_;
-    }
-    auto cw = [&](size_t c) { return cell_w_.empty() ? 1.0 : cell_w_[c]; };
-    const size_t M = st.ncells, nb = st.nb(), m = st.m;
-    n1_.assign(st.g1, 0.0);
-    for (u32 s = 0; s < st.g1; s++) {
-        double a = 0;
-        for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++) a += cw(c);
-        n1_[s] = a;
-    }
-    sw_ = 0;
-    for (double v : n1_) sw_ += v;
-    nr_.assign(m, 0.0);
-    std::vector<double> dq(m, 0.0), cs(m, 0.0);
-    for (u32 s = 0; s < st.g1; s++) {
-        const u32 c0 = st.seg_off[s], c1 = st.seg_off[s + 1];
-        for (u32 c = c0; c < c1; c++)
-            for (size_t b = 0; b < nb; b++) cs[st.coord[b * M + c]] += cw(c);
-        for (u32 c = c0; c < c1; c++)
-            for (size_t b = 0; b < nb; b++) {
-                const u32 k = st.coord[b * M + c];
-                nr_[k] += cw(c);
-                dq[k] += cw(c) * cs[k] / n1_[s];
-            }
-        for (u32 c = c0; c < c1; c++)
-            for (size_t b = 0; b < nb; b++) cs[st.coord[b * M + c]] = 0.0;
-    }
-    diag_.resize(m);
-    red_.resize(m);
-    for (size_t k = 0; k < m; k++) {
-        diag_[k] = nr_[k] - dq[k];
-        red_[k] = diag_[k] <= REDUNDANT * nr_[k];
-    }
-    pre_fresh_ = false;
-    amg_stale_ = true;
-    upload_weights();
-}
-
-void GpuAbsorber::upload_weights() {
-    if (weighted_) d_->w_rows.upload(w_rows_, stream_);
-    else d_->w_rows.release();
-    if (!cell_w_.empty()) d_->cell_w.upload(cell_w_, stream_);
-    else d_->cell_w.release();
-    std::vector<double> inv(n1_.size());
-    for (size_t s = 0; s < n1_.size(); s++) inv[s] = 1.0 / n1_[s];
-    d_->n1inv.upload(inv, stream_);
-    d_->nr.upload(nr_, stream_);
-    build_srow();
-    CK(cudaStreamSynchronize(stream_));
 }
 
 // The dense rows of S on the small coordinates (weights.cuh) for the current cell weights: part
@@ -768,16 +788,14 @@ void GpuAbsorber::build_srow() {
 void GpuAbsorber::set_weights(const double* w_rows) {
     AllocScope alloc_scope(stream_);
     ctx_.check();
-    std::vector<double> kept;
-    if (w_rows) {
-        kept.resize(hs_.n);
-        for (size_t r = 0; r < hs_.n; r++) {
-            if (!(std::isfinite(w_rows[r]) && w_rows[r] > 0.0))
-                throw Error(RC_INVALID_INPUT, "weights must be positive and finite");
-            kept[hs_.pi[r]] = w_rows[r];
-        }
+    if (!w_rows) {
+        unit_weights_device();
+        return;
     }
-    refresh_weights(w_rows ? kept.data() : nullptr);
+    DBuf<double> wd;
+    wd.upload(w_rows, hs_.n, stream_);
+    set_weights_device(wd.p);
+    CK(cudaStreamSynchronize(stream_));
 }
 
 void GpuAbsorber::weight_state(double* n1, double* nr, double* diag, uint8_t* red, double* sw) const {
@@ -790,87 +808,16 @@ void GpuAbsorber::weight_state(double* n1, double* nr, double* diag, uint8_t* re
 }
 
 // Jacobi entries (precond/jacobi.rs:7) and the exact dense factor of the small super-block
-// (precond/dense.rs:79-160): S_SS assembled on the host (operator.rs:1457-1523), scaled to unit
-// diagonal over the kept coordinates, factored with grounding and inverted on the device.
+// (precond/dense.rs:79-160), both from the device weight state: the Jacobi factors come with the
+// coordinate weights (refresh_coord), S_SS is assembled on the device, scaled to unit diagonal
+// over the kept coordinates, factored with grounding and inverted.
 void GpuAbsorber::ensure_precond() {
     if (pre_fresh_) return;
-    const HostStructure& st = hs_;
-    const size_t m = st.m, ms = st.m_small;
-    const bool small = ms > 0 && ms <= DENSE_SMALL_MAX;
-    // weights held on the device (set_weights_device): the small block is assembled there too,
-    // without copying the weight state back
-    const bool dev = host_stale_;
-    if (dev) refresh_coord();
-    if (!dev_jacobi_) {  // after set_weights_device the Jacobi factors are already on the device
-        std::vector<double> inv(m);
-        for (size_t i = 0; i < m; i++) inv[i] = (red_[i] || !(diag_[i] > 0.0)) ? 0.0 : 1.0 / diag_[i];
-        d_->inv_diag.upload(inv, stream_);
-    }
+    const size_t ms = hs_.m_small;
+    refresh_coord();
     small_ok_ = false;
-    if (small && dev) {
-        build_small_device();
-    } else if (small) {
-        build_small_host();
-    }
+    if (ms > 0 && ms <= DENSE_SMALL_MAX) build_small_device();
     pre_fresh_ = true;
-}
-
-// The dense small factor from a host assembly of S_SS (host weight state).
-void GpuAbsorber::build_small_host() {
-    const HostStructure& st = hs_;
-    const size_t ms = st.m_small, M = st.ncells;
-    {
-        auto cw = [&](size_t c) { return cell_w_.empty() ? 1.0 : cell_w_[c]; };
-        size_t ns = 0;
-        for (auto& b : st.blocks) ns += b.small;
-        std::vector<double> a(ms * ms, 0.0), cs(ms, 0.0);
-        std::vector<u32> touched;
-        for (u32 s = 0; s < st.g1; s++) {
-            touched.clear();
-            for (u32 c = st.seg_off[s]; c < st.seg_off[s + 1]; c++) {
-                const double w = cw(c);
-                for (size_t b = 0; b < ns; b++) {
-                    const u32 k = st.coord[b * M + c];
-                    if (cs[k] == 0.0) touched.push_back(k);
-                    cs[k] += w;
-                    a[k * ms + k] += w;
-                    for (size_t b2 = 0; b2 < ns; b2++)
-                        if (b2 != b) a[k * ms + st.coord[b2 * M + c]] += w;
-                }
-            }
-            std::sort(touched.begin(), touched.end());
-            touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
-            const double inv1 = 1.0 / n1_[s];
-            for (u32 k : touched)
-                for (u32 l : touched) a[size_t(k) * ms + l] -= cs[k] * cs[l] * inv1;
-            for (u32 k : touched) cs[k] = 0.0;
-        }
-        std::vector<u32> keep;
-        for (size_t i = 0; i < ms; i++)
-            if (!red_[i] && a[i * ms + i] > 0.0) keep.push_back(u32(i));
-        const size_t k = keep.size();
-        std::vector<double> scale(k), ak(k * k);
-        for (size_t i = 0; i < k; i++) scale[i] = 1.0 / std::sqrt(a[size_t(keep[i]) * (ms + 1)]);
-        for (size_t i = 0; i < k; i++)
-            for (size_t j = 0; j < k; j++) ak[i * k + j] = a[size_t(keep[i]) * ms + keep[j]] * scale[i] * scale[j];
-        DBuf<double> da, dd, dx, dscale;
-        DBuf<u32> dkeep;
-        d_->minv.alloc(ms * ms);
-        CK(cudaMemsetAsync(d_->minv.p, 0, ms * ms * sizeof(double), stream_));
-        if (k > 0) {
-            da.upload(ak, stream_);
-            dd.alloc(k);
-            dx.alloc(k * k);
-            dscale.upload(scale, stream_);
-            dkeep.upload(keep, stream_);
-            dense_ldlt_inverse(da.p, dd.p, int(k), dx.p, stream_, d_->launches);
-            k_expand_minv<<<grid_for(k * k), THREADS, 0, stream_>>>(dx.p, dkeep.p, dscale.p, int(k), u32(ms), d_->minv.p);
-            CK(cudaGetLastError());
-            d_->launches++;
-        }
-        CK(cudaStreamSynchronize(stream_));
-        small_ok_ = true;
-    }
 }
 
 // The dense small factor from the device assembly of S_SS (weights.cuh) for the device weight
@@ -981,80 +928,82 @@ void launch_small_reduce(Scratch& d, const DevStruct& S, T* small, int R, T* Y, 
     d.launches++;
 }
 
-// Y = S P. Short segments: one thread per (segment, column) (t, small coordinates); long
-// segments: tiles (t; slices' partials completed by k_fix, then their small coordinates).
-// Short coordinate lists: one thread per (coordinate, column); long ones: tiles and k_fix.
-// The small coordinates' partial rows are summed last.
+// Y = S P on the PCG's padded vectors (Rv a multiple of 4). Short segments: one lane group per
+// segment (k_vseg_apply); long segments: CTA tiles, their slices' partials completed by k_fix.
+// Short coordinate lists: warp tiles (k_vpull_apply); long ones: CTA tiles and k_fix. The small
+// coordinates' rows (ms_acc > 0) come from the dense rows of S (k_srow_apply), their CTA
+// partials added by k_small_reduce.
 template <class T>
-void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* P, int R, T* Y, T* t, T* part,
+void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* P, int Rv, T* Y, T* t, T* part,
                   T* small, cudaStream_t st) {
+    if (Rv % 4 != 0) throw Error(RC_INTERNAL, "fereg: the operator takes padded vectors (a multiple of 4 columns)");
+    const bool weighted = W.cell_w != nullptr;
     int h = d.begin(GpuAbsorber::P_APPLY, st);
-    // small coordinates: from their dense rows of S (srow) when built, else summed per cell in
-    // the segment passes
-    const bool dense = S.ms_acc > 0 && d.srow_on;
-    const bool acc = S.ms_acc > 0 && !dense;
-    const u32 len = S.ms_acc * u32(R);
-    if (d.wseg.n)
-        for (int j0 = 0; j0 < R; j0 += WCOLS) {
-            const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = acc ? size_t(WPB) * S.ms_acc * 64 * sizeof(T) : 0;
-            const u32 nsegs = u32(d.wseg_segs.n);
-            with_lanes<1>(Rc, S.nb, [&](auto c, auto nbk) {
-                constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
-                if (shm) allow_smem(k_gseg_apply<T, RCP, NBK>, shm);
-                k_gseg_apply<T, RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, nsegs, P, R, j0, Rc,
-                                                                          t, acc ? small : nullptr);
+    DevStruct SA = S;  // the operator's segment tiles
+    SA.seg = d.aseg_tiles.set();
+    if (d.aseg_segs.n)
+        for (int j0 = 0; j0 < Rv; j0 += VCOLS) {
+            const int Rc = std::min(VCOLS, Rv - j0);
+            const u32 nsegs = u32(d.aseg_segs.n);
+            const size_t sm = small_stage_bytes<T>(S.ms_acc, Rc);
+            const int stage = S.ns_acc > 0 && sm <= SMALL_STAGE_MAX;
+            auto go = [&](auto lc, auto nbk, auto wc) {
+                constexpr int L = decltype(lc)::value, NBK = decltype(nbk)::value;
+                constexpr bool WT_ = decltype(wc)::value;
+                k_vseg_apply<T, L, NBK, WT_><<<GRID_S, WPB * 32, stage ? sm : 0, st>>>(S, W, d.aseg_segs.p, nsegs, P,
+                                                                                       Rv, j0, Rc, t, stage);
+            };
+            with_vlanes(Rc, S.nb, [&](auto lc, auto nbk) {
+                if (weighted) go(lc, nbk, std::true_type{});
+                else go(lc, nbk, std::false_type{});
             });
             d.launches++;
         }
-    else if (acc)
-        CK(cudaMemsetAsync(small, 0, size_t(GRID_S) * len * sizeof(T), st));
-    if (S.seg.n) {
-        T* sb = small + size_t(GRID_S) * len;
-        k_seg_apply<T><<<GRID_T, THREADS, 0, st>>>(S, W, P, R, t, part, false, acc ? sb : nullptr);
+    if (SA.seg.n) {
+        k_seg_apply<T><<<GRID_T, THREADS, 0, st>>>(SA, W, P, Rv, t, part, false, nullptr);
         d.launches++;
-        if (S.seg.nfix) {
-            k_fix<T><<<std::min<u32>(S.seg.nfix, GRID_T), THREADS, 0, st>>>(S.seg, W, P, part, R, 1, t);
+        if (SA.seg.nfix) {
+            k_fix<T><<<std::min<u32>(SA.seg.nfix, GRID_T), THREADS, 0, st>>>(SA.seg, W, P, part, Rv, 1, t);
             d.launches++;
-            if (acc) {
-                k_seg_small_slices<T><<<GRID_T, THREADS, 0, st>>>(S, W, P, t, R, sb + size_t(GRID_T) * len);
-                d.launches++;
-            }
         }
     }
     d.end(h, st);
     h = d.begin(GpuAbsorber::P_APPLY_PULL, st);
     if (d.wpull.n)
-        for (int j0 = 0; j0 < R; j0 += WCOLS) {
-            const int Rc = std::min(WCOLS, R - j0);
-            // up to 4 columns one column per lane (groups of rcp_of(Rc)): narrower groups of two
-            // columns measured slower there
-            with_lanes<1>(
-                Rc, S.nb,
-                [&](auto c, auto nbk) {
-                    constexpr int L = decltype(c)::value, NBK = decltype(nbk)::value;
-                    k_wpull_apply<T, L, NBK><<<GRID_S, WPB * 32, wpull_smem(), st>>>(S, W, d.wpull.set(), P, t, R,
-                                                                                        j0, Rc, Y);
-                },
-                Rc <= 4 ? rcp_of(Rc) : 0);
+        for (int j0 = 0; j0 < Rv; j0 += VCOLS) {
+            const int Rc = std::min(VCOLS, Rv - j0);
+            const size_t sm = small_stage_bytes<T>(S.ms_acc, Rc);
+            const int stage = S.ns_acc > 0 && sm <= SMALL_STAGE_MAX;
+            auto go = [&](auto lc, auto nbk, auto wc) {
+                constexpr int L = decltype(lc)::value, NBK = decltype(nbk)::value;
+                constexpr bool WT_ = decltype(wc)::value;
+                const size_t shm = wpull_smem() + (stage ? sm : 0);
+                allow_smem(k_vpull_apply<T, L, NBK, WT_>, shm);
+                k_vpull_apply<T, L, NBK, WT_><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wpull.set(), P, t, Rv, j0, Rc, Y,
+                                                                             stage);
+            };
+            with_vlanes(Rc, S.nb, [&](auto lc, auto nbk) {
+                if (weighted) go(lc, nbk, std::true_type{});
+                else go(lc, nbk, std::false_type{});
+            });
             d.launches++;
         }
     if (S.pull.n) {
-        k_pull_apply<T><<<GRID_T, THREADS, 0, st>>>(S, W, P, t, R, Y, part);
+        k_pull_apply<T><<<GRID_T, THREADS, 0, st>>>(S, W, P, t, Rv, Y, part);
         d.launches++;
         if (S.pull.nfix) {
-            k_fix<T><<<std::min<u32>(S.pull.nfix, GRID_T), THREADS, 0, st>>>(S.pull, W, P, part, R, 0, Y);
+            k_fix<T><<<std::min<u32>(S.pull.nfix, GRID_T), THREADS, 0, st>>>(S.pull, W, P, part, Rv, 0, Y);
             d.launches++;
         }
     }
-    if (dense) {
+    if (S.ms_acc > 0) {
+        if (!d.srow_on) throw Error(RC_INTERNAL, "fereg: the dense small rows are missing");
+        const u32 len = S.ms_acc * u32(Rv);
         const u32 grid = std::max<u32>(1, std::min<u32>(4 * GRID_V, (S.m + 31) / 32));
-        k_srow_apply<T><<<grid, THREADS, 0, st>>>(d.srow.p, S.m, S.ms_acc, P, R, small);
+        k_srow_apply<T><<<grid, THREADS, 0, st>>>(d.srow.p, S.m, S.ms_acc, P, Rv, small);
         k_small_reduce<T><<<std::max<u32>(1, std::min<u32>((len + 7) / 8, GRID_V)), THREADS, 0, st>>>(
             small, int(grid), nullptr, 0, nullptr, 0, len, Y);
         d.launches += 2;
-    } else if (acc) {
-        launch_small_reduce<T>(d, S, small, R, Y, st);
     }
     CK(cudaGetLastError());
     d.end(h, st);
@@ -1297,16 +1246,17 @@ void launch_rhs_scratch(Scratch& d, const DevStruct& S, const DevWeights& W, con
 
 void GpuAbsorber::apply_host(const double* p, size_t r, double* y) {
     AllocScope alloc_scope(stream_);
-    const size_t m = hs_.m;
+    const size_t m = hs_.m, rv = (r + 3) / 4 * 4;  // the PCG's padded layout
     const DevStruct S = d_->ds(hs_);
-    d_->p.alloc(m * r);
-    d_->q.alloc(m * r);
-    d_->t.alloc(size_t(hs_.g1) * r);
-    d_->part.alloc(std::max<size_t>(1, size_t(std::max(S.seg.nparts, S.pull.nparts)) * r));
-    d_->small.alloc(std::max<size_t>(1, small_rows() * d_->ms_acc * r));
-    CK(cudaMemcpyAsync(d_->p.p, p, m * r * 8, cudaMemcpyHostToDevice, stream_));
-    launch_apply<double>(*d_, S, d_->dw(), d_->p.p, int(r), d_->q.p, d_->t.p, d_->part.p, d_->small.p, stream_);
-    CK(cudaMemcpyAsync(y, d_->q.p, m * r * 8, cudaMemcpyDeviceToHost, stream_));
+    d_->p.alloc(m * rv);
+    d_->q.alloc(m * rv);
+    d_->t.alloc(size_t(hs_.g1) * rv);
+    d_->part.alloc(std::max<size_t>(1, size_t(std::max(S.seg.nparts, S.pull.nparts)) * rv));
+    d_->small.alloc(std::max<size_t>(1, small_rows() * d_->ms_acc * rv));
+    CK(cudaMemsetAsync(d_->p.p, 0, m * rv * 8, stream_));
+    CK(cudaMemcpy2DAsync(d_->p.p, rv * 8, p, r * 8, r * 8, m, cudaMemcpyHostToDevice, stream_));
+    launch_apply<double>(*d_, S, d_->dw(), d_->p.p, int(rv), d_->q.p, d_->t.p, d_->part.p, d_->small.p, stream_);
+    CK(cudaMemcpy2DAsync(y, r * 8, d_->q.p, rv * 8, r * 8, m, cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     d_->collect();
 }
@@ -1632,42 +1582,53 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     // the closed form x + M^-1 (rhs - S x) needs the current factor, not a stale one
     if (small_stale_ && small_ok_ && hs_.m_small == hs_.m) refresh_small();
     const int R = int(r);
+    // the PCG runs on padded vectors: row stride rv (a multiple of 4), columns r..rv-1 zero and
+    // inactive; the rows' passes keep r
+    const size_t rv = (r + 3) / 4 * 4;
+    const int RV = int(rv);
     const DevStruct S = d_->ds(hs_);
     const DevWeights W = d_->dw();
     cudaStream_t st = stream_;
     Scratch& d = *d_;
     const size_t nparts = std::max<size_t>(1, size_t(std::max(S.seg.nparts, S.pull.nparts)));
     d.rhs.alloc(std::max<size_t>(1, m * r));
+    d.rhsv.alloc(std::max<size_t>(1, m * rv));
+    d.xv.alloc(std::max<size_t>(1, m * rv));
     d.b1.alloc(g1 * r);
     d.coefs.alloc((m + g1) * r);
-    d.part.alloc(nparts * r);
-    d.cta.alloc(size_t(std::max(GRID_T, GRID_V)) * 3 * r);
+    d.part.alloc(nparts * rv);
+    d.cta.alloc(size_t(std::max(GRID_T, GRID_V)) * 3 * rv);
     d.colsum.alloc(3 * r);
-    d.t.alloc(g1 * r);
+    d.t.alloc(g1 * rv);
     d.cta2.alloc(size_t(GRID_S) * 2 * r);
-    d.small.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * r));
+    d.small.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * rv));
     launch_rhs(d, S, W, rows, R, d.b1.p, d.rhs.p, d.colsum.p, st);
     std::vector<double> cs(3 * r);
     CK(cudaMemcpyAsync(cs.data(), d.colsum.p, 3 * r * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     ctx_.check();
-    std::vector<double> ss0(r), ss1(r);
+    std::vector<double> ss0(rv, 0.0), ss1(rv, 0.0);
     for (size_t j = 0; j < r; j++) {  // solve.rs:1210-1217
         const double wsq = cs[j], wsum = cs[r + j], b1sq = cs[2 * r + j];
         const double s = wsq - wsum * wsum / sw_;
         ss0[j] = s > 1e-15 * wsq ? s : 0.0;
         ss1[j] = wsq - b1sq;
     }
-    double* x = d.coefs.p;
+    // the padded right-hand side
+    if (m > 0) {
+        CK(cudaMemsetAsync(d.rhsv.p, 0, m * rv * 8, st));
+        CK(cudaMemcpy2DAsync(d.rhsv.p, rv * 8, d.rhs.p, r * 8, r * 8, m, cudaMemcpyDeviceToDevice, st));
+    }
+    double* x = d.xv.p;  // the padded iterate
     const bool have_last = warm_last && last_r_ == r && m > 0;
     if (have_last) {  // the previous solution, already in place; zero the columns with ss0 = 0
-        std::vector<int> zc(r);
+        std::vector<int> zc(rv);
         bool any = false;
         for (size_t j = 0; j < r; j++) any |= (zc[j] = ss0[j] == 0.0) != 0;
         if (any) {
-            d.cg_active.alloc(r);
-            CK(cudaMemcpyAsync(d.cg_active.p, zc.data(), r * sizeof(int), cudaMemcpyHostToDevice, st));
-            k_zero_masked<<<grid_for(m * r), THREADS, 0, st>>>(x, d.cg_active.p, m * r, R);
+            d.cg_active.alloc(rv);
+            CK(cudaMemcpyAsync(d.cg_active.p, zc.data(), rv * sizeof(int), cudaMemcpyHostToDevice, st));
+            k_zero_masked<<<grid_for(m * rv), THREADS, 0, st>>>(x, d.cg_active.p, m * rv, RV);
             d.launches++;
         }
     } else if (warm) {
@@ -1675,66 +1636,69 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         for (size_t j = 0; j < r; j++)
             if (ss0[j] == 0.0)
                 for (size_t i = 0; i < m; i++) w0[i * r + j] = 0.0;
-        if (m > 0) CK(cudaMemcpyAsync(x, w0.data(), m * r * 8, cudaMemcpyHostToDevice, st));
+        if (m > 0) {
+            CK(cudaMemsetAsync(x, 0, m * rv * 8, st));
+            CK(cudaMemcpy2DAsync(x, rv * 8, w0.data(), r * 8, r * 8, m, cudaMemcpyHostToDevice, st));
+        }
     } else if (m > 0) {
-        CK(cudaMemsetAsync(x, 0, m * r * 8, st));
+        CK(cudaMemsetAsync(x, 0, m * rv * 8, st));
     }
     u64 iterations = 1;
     bool exact = true;
     if (m > 0) {
-        const size_t tot = m * r;
+        const size_t tot = m * rv;
         d.r.alloc(tot);
         d.z.alloc(tot);
         d.p.alloc(tot);
         d.q.alloc(tot);
         for (auto* b : {&d.cg_rho, &d.cg_rho_new, &d.cg_pq, &d.cg_gamma, &d.cg_beta, &d.cg_ss1, &d.cg_floor, &d.cg_xconst,
                         &d.cg_pfloor})
-            b->alloc(r);
-        d.cg_xb.alloc(3 * r);
-        d.cg_ring.alloc(r * WINDOW);
-        d.cg_active.alloc(r);
+            b->alloc(rv);
+        d.cg_xb.alloc(3 * rv);
+        d.cg_ring.alloc(rv * WINDOW);
+        d.cg_active.alloc(rv);
         d.cg_nactive.alloc(1);
-        std::vector<int> act(r);
-        std::vector<double> fl(r), zero(r, 0.0);
-        for (size_t j = 0; j < r; j++) {
+        std::vector<int> act(rv);
+        std::vector<double> fl(rv), zero(rv, 0.0);
+        for (size_t j = 0; j < rv; j++) {
             act[j] = ss0[j] > 0.0;
             fl[j] = 1e-26 * ss0[j];
         }
-        CK(cudaMemcpyAsync(d.cg_active.p, act.data(), r * sizeof(int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.cg_ss1.p, ss1.data(), r * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.cg_floor.p, fl.data(), r * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.cg_xconst.p, zero.data(), r * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemsetAsync(d.cg_ring.p, 0, r * WINDOW * 8, st));
+        CK(cudaMemcpyAsync(d.cg_active.p, act.data(), rv * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.cg_ss1.p, ss1.data(), rv * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.cg_floor.p, fl.data(), rv * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.cg_xconst.p, zero.data(), rv * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(d.cg_ring.p, 0, rv * WINDOW * 8, st));
         const bool exact_pre = small_ok_ && hs_.m_small == hs_.m;
         const std::function<bool(double)> esc = [this](double rho_hat) { return escalate(rho_hat); };
         if (exact_pre) {
             // x* = x + M^-1 (rhs - S x) (cg.rs:171-198)
             if (warm || have_last) {
-                launch_apply<double>(d, S, W, x, R, d.q.p, d.t.p, d.part.p, d.small.p, st);
-                k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhs.p, d.q.p, tot);
+                launch_apply<double>(d, S, W, x, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
+                k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhsv.p, d.q.p, tot);
                 d.launches++;
             } else {
-                CK(cudaMemcpyAsync(d.r.p, d.rhs.p, tot * 8, cudaMemcpyDeviceToDevice, st));
+                CK(cudaMemcpyAsync(d.r.p, d.rhsv.p, tot * 8, cudaMemcpyDeviceToDevice, st));
             }
-            launch_precond<double>(d, S, small_ok_, d.r.p, d.z.p, R, st);
-            k_add_active<double><<<grid_for(tot), THREADS, 0, st>>>(x, d.z.p, d.cg_active.p, tot, R);
+            launch_precond<double>(d, S, small_ok_, d.r.p, d.z.p, RV, st);
+            k_add_active<double><<<grid_for(tot), THREADS, 0, st>>>(x, d.z.p, d.cg_active.p, tot, RV);
             d.launches++;
             CK(cudaGetLastError());
         } else if (prec == Precision::F64) {
-            iterations = run_pcg<double>(d, S, W, small_ok_, x, d.rhs.p, d.rhs.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p,
-                                         d.t.p, d.part.p, d.small.p, R, tol, 0.0, 0, maxiter,
+            iterations = run_pcg<double>(d, S, W, small_ok_, x, d.rhsv.p, d.rhsv.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p,
+                                         d.t.p, d.part.p, d.small.p, RV, tol, 0.0, 0, maxiter,
                                          warm != nullptr || have_last, ctx_, st, esc);
             exact = false;
         } else {
             // FP32 inner PCG on the correction, FP64 true residual between rounds.
             for (auto* b : {&d.fx, &d.fb, &d.fr, &d.fz, &d.fp, &d.fq, &d.frhs, &d.fx0}) b->alloc(tot);
-            d.ft.alloc(g1 * r);
-            d.fpart.alloc(nparts * r);
-            d.fsmall.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * r));
-            k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.rhs.p, d.frhs.p, tot);
+            d.ft.alloc(g1 * rv);
+            d.fpart.alloc(nparts * rv);
+            d.fsmall.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * rv));
+            k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.rhsv.p, d.frhs.p, tot);
             d.launches++;
             iterations = 0;
-            std::vector<double> rho64(r, 0.0), rho_prev(r, 0.0);
+            std::vector<double> rho64(rv, 0.0), rho_prev(rv, 0.0);
             bool have_r = false;  // d.r holds the FP64 true residual of x
             const bool start_nonzero = warm != nullptr || have_last;
             bool accepted = false;
@@ -1742,47 +1706,47 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
                 // true residual b = rhs - S x in FP64 (kept from the previous round's check), x'rhs,
                 // and the FP32 copies
                 if (!have_r && start_nonzero) {
-                    launch_apply<double>(d, S, W, x, R, d.q.p, d.t.p, d.part.p, d.small.p, st);
-                    k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhs.p, d.q.p, tot);
+                    launch_apply<double>(d, S, W, x, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
+                    k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhsv.p, d.q.p, tot);
                     d.launches++;
                 } else if (!have_r) {
-                    CK(cudaMemcpyAsync(d.r.p, d.rhs.p, tot * 8, cudaMemcpyDeviceToDevice, st));
+                    CK(cudaMemcpyAsync(d.r.p, d.rhsv.p, tot * 8, cudaMemcpyDeviceToDevice, st));
                 }
-                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.rhs.p, u32(m), R, d.cta.p);
-                reduce_cols(d, d.cta.p, GRID_V, R, d.cg_xconst.p, st);
+                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.rhsv.p, u32(m), RV, d.cta.p);
+                reduce_cols(d, d.cta.p, GRID_V, RV, d.cg_xconst.p, st);
                 k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.fb.p, tot);
                 k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(x, d.fx0.p, tot);
                 CK(cudaMemsetAsync(d.fx.p, 0, tot * 4, st));
-                CK(cudaMemsetAsync(d.cg_ring.p, 0, r * WINDOW * 8, st));
+                CK(cudaMemsetAsync(d.cg_ring.p, 0, rv * WINDOW * 8, st));
                 d.launches += 3;
                 iterations += run_pcg<float>(d, S, W, small_ok_, d.fx.p, d.fb.p, d.frhs.p, d.fx0.p, d.fr.p, d.fz.p,
-                                             d.fp.p, d.fq.p, d.ft.p, d.fpart.p, d.fsmall.p, R, tol,
+                                             d.fp.p, d.fq.p, d.ft.p, d.fpart.p, d.fsmall.p, RV, tol,
                                              REFINE_DROP, iterations, maxiter, false, ctx_, st, esc);
                 k_add_correction<<<grid_for(tot), THREADS, 0, st>>>(x, d.fx.p, tot);
                 d.launches++;
                 // the round's check in FP64: true residual, its preconditioned norm and ss_k
-                launch_apply<double>(d, S, W, x, R, d.q.p, d.t.p, d.part.p, d.small.p, st);
-                k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhs.p, d.q.p, tot);
-                launch_precond<double>(d, S, small_ok_, d.r.p, d.z.p, R, st);
-                k_dot<double><<<GRID_V, THREADS, 0, st>>>(d.r.p, d.z.p, u32(m), R, d.cta.p);
-                reduce_cols(d, d.cta.p, GRID_V, R, d.cg_rho.p, st);
-                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.rhs.p, u32(m), R, d.cta.p);
-                reduce_cols(d, d.cta.p, GRID_V, R, d.cg_xconst.p, st);
-                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.r.p, u32(m), R, d.cta.p);
-                reduce_cols(d, d.cta.p, GRID_V, R, d.cg_pq.p, st);
-                k_refine_accept<<<1, THREADS, 0, st>>>(d.cg(), R, tol);
+                launch_apply<double>(d, S, W, x, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
+                k_sub<double><<<grid_for(tot), THREADS, 0, st>>>(d.r.p, d.rhsv.p, d.q.p, tot);
+                launch_precond<double>(d, S, small_ok_, d.r.p, d.z.p, RV, st);
+                k_dot<double><<<GRID_V, THREADS, 0, st>>>(d.r.p, d.z.p, u32(m), RV, d.cta.p);
+                reduce_cols(d, d.cta.p, GRID_V, RV, d.cg_rho.p, st);
+                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.rhsv.p, u32(m), RV, d.cta.p);
+                reduce_cols(d, d.cta.p, GRID_V, RV, d.cg_xconst.p, st);
+                k_dot<double><<<GRID_V, THREADS, 0, st>>>(x, d.r.p, u32(m), RV, d.cta.p);
+                reduce_cols(d, d.cta.p, GRID_V, RV, d.cg_pq.p, st);
+                k_refine_accept<<<1, THREADS, 0, st>>>(d.cg(), RV, tol);
                 d.launches += 5;
                 have_r = true;
                 CK(cudaMemcpyAsync(d.h_nactive, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(rho64.data(), d.cg_rho.p, r * sizeof(double), cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(act.data(), d.cg_active.p, r * sizeof(int), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(rho64.data(), d.cg_rho.p, rv * sizeof(double), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(act.data(), d.cg_active.p, rv * sizeof(int), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 accepted = d.h_nactive[0] == 0;
                 // a round that cut no remaining column's FP64 residual norm tenfold is at the limit
                 // of FP32 (on an ill-conditioned graph S P of smooth vectors cancels below FP32
                 // precision): the remaining columns finish in FP64
                 bool progress = round == 0;
-                for (size_t j = 0; j < r && !progress; j++)
+                for (size_t j = 0; j < rv && !progress; j++)
                     progress = act[j] == 1 && rho64[j] <= 0.1 * rho_prev[j];
                 rho_prev = rho64;
                 if (!accepted && !progress) break;
@@ -1790,10 +1754,10 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             if (!accepted) {
                 // FP64 PCG from the refined iterate on the columns not yet accepted, under the
                 // reference's stopping rule on the full iterate (x0 = 0, x'rhs in the rule)
-                CK(cudaMemsetAsync(d.cg_xconst.p, 0, r * 8, st));
-                CK(cudaMemsetAsync(d.cg_ring.p, 0, r * WINDOW * 8, st));
-                iterations += run_pcg<double>(d, S, W, small_ok_, x, d.rhs.p, d.rhs.p, nullptr, d.r.p, d.z.p, d.p.p,
-                                              d.q.p, d.t.p, d.part.p, d.small.p, R, tol, 0.0, iterations, maxiter, true,
+                CK(cudaMemsetAsync(d.cg_xconst.p, 0, rv * 8, st));
+                CK(cudaMemsetAsync(d.cg_ring.p, 0, rv * WINDOW * 8, st));
+                iterations += run_pcg<double>(d, S, W, small_ok_, x, d.rhsv.p, d.rhsv.p, nullptr, d.r.p, d.z.p, d.p.p,
+                                              d.q.p, d.t.p, d.part.p, d.small.p, RV, tol, 0.0, iterations, maxiter, true,
                                               ctx_, st, esc);
                 d.fp64_finishes++;
             }
@@ -1806,6 +1770,9 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             exact = all0;
         }
     }
+    // the unpadded solution [x; .] for the residualization and the caller
+    if (m > 0) CK(cudaMemcpy2DAsync(d.coefs.p, r * 8, d.xv.p, rv * 8, r * 8, m, cudaMemcpyDeviceToDevice, st));
+    x = d.coefs.p;
     ctx_.check();
     int h = d.begin(P_RESID, st);
     double* alpha = want_coefs ? x + m * r : nullptr;
@@ -1870,6 +1837,7 @@ void GpuAbsorber::solver_stats(u64* o) const {
 
 void GpuAbsorber::fit_rows(const double* coefs, size_t r, size_t col, double* out) const {
     AllocScope alloc_scope(stream_);
+    ensure_host_coord();
     const HostStructure& st = hs_;
     const size_t m = st.m, M = st.ncells, nb = st.nb();
     for (u32 s = 0; s < st.g1; s++)

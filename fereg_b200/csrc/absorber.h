@@ -46,7 +46,10 @@ struct Scratch;
 class GpuAbsorber {
    public:
     // `codes[q]` are the kept-order codes of term q (< g[q]); `w` kept-order weights or null.
-    GpuAbsorber(const std::vector<const u32*>& codes, const std::vector<u32>& g, const double* w, size_t n, const Ctx& ctx);
+    // The cell structure is built on the device; `dev_codes`, when given, are device copies of
+    // `codes` (the caller's session keeps them), otherwise the codes are uploaded for the build.
+    GpuAbsorber(const std::vector<const u32*>& codes, const std::vector<u32>& g, const double* w, size_t n, const Ctx& ctx,
+                const std::vector<const u32*>* dev_codes = nullptr);
     ~GpuAbsorber();
 
     size_t n() const { return hs_.n; }
@@ -124,7 +127,8 @@ class GpuAbsorber {
     void weight_state(double* n1, double* nr, double* diag, uint8_t* red, double* sw) const;
 
    private:
-    HostStructure hs_;
+    // the host copy: scalars, row order, seg_off, cell_row; coord fetched on demand (ensure_host_coord)
+    mutable HostStructure hs_;
     std::vector<u32> g_;
     int norm_fe1_ = -1;
     Ctx ctx_;
@@ -134,7 +138,6 @@ class GpuAbsorber {
     mutable std::vector<double> w_rows_, cell_w_, n1_, nr_, diag_;
     mutable std::vector<uint8_t> red_;
     mutable bool host_stale_ = false;
-    mutable bool dev_jacobi_ = false;   // inv_diag was computed on the device
     mutable bool coord_stale_ = false;  // nr / diag / Jacobi on the device are of earlier weights
     double sw_ = 0;
     bool weighted_ = false;
@@ -150,13 +153,12 @@ class GpuAbsorber {
     void build_amg();
     void refresh_small();
     void refresh_coord() const;
-    void build_small_host();
     void build_small_device();
 
-    void refresh_weights(const double* w_kept);
+    void unit_weights_device();
     void build_srow();
     void sync_host_weights() const;
-    void upload_weights();
+    void ensure_host_coord() const;
     void ensure_precond();
     SolveInfo solve(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
                     double* coefs, Precision prec, bool warm_last = false);

@@ -70,6 +70,9 @@ HostStructure plan_structure(const std::vector<const u32*>& codes, const std::ve
 HostStructure build_structure(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n,
                               size_t small_limit);
 int fe1_index(const std::vector<u32>& g);
+// Every code below its term's level count, every weight positive and finite (198 otherwise).
+void check_codes_host(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n);
+void check_weights_host(const double* w, size_t n);
 
 // Coordinate-sorted cell lists of every block (the transpose of the cell structure): for each
 // reduced coordinate k, the cells whose code in k's block is k, ascending. With the segment of

@@ -100,97 +100,6 @@ __global__ void k_cg_start(CgState st, int R, double drop) {
     if (threadIdx.x == 0) *st.n_active = cnt;
 }
 
-// gamma = rho / p'q for the active columns (a non-positive or non-finite p'q deactivates).
-__global__ void k_cg_gamma(CgState st, int R) {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < R; j += gridDim.x * blockDim.x) {
-        double g = 0.0;
-        if (st.active[j] == 1) {
-            const double pq = st.pq[j];
-            if (pq > 0.0 && isfinite(pq)) g = st.rho[j] / pq;
-            else st.active[j] = st.pfloor[j] > 0.0 ? 2 : 0;  // inner rounds: FP64 restart, not a stop
-        }
-        st.gamma[j] = g;
-    }
-}
-
-// x += gamma p, r -= gamma q, with per-CTA partials of x'rhs, x'r and x0'r (gridDim x 3R;
-// x0 null: 0).
-template <class T>
-__global__ void __launch_bounds__(TB) k_update_xr(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
-                                                  const T* __restrict__ q, const T* __restrict__ rhs,
-                                                  const T* __restrict__ x0, const double* __restrict__ gamma, u32 m,
-                                                  int R, double* __restrict__ cta_part) {
-    __shared__ double red[3 * TB];
-    for (int j0 = 0; j0 < R; j0 += RC_MAX) {
-        const ColMap cm = colmap(R, j0);
-        double xb = 0.0, xr = 0.0, x0r = 0.0;
-        if (cm.on) {
-            const T g = T(gamma[j0 + cm.col]);
-            for (u32 i = blockIdx.x * u32(cm.nslot) + u32(cm.slot); i < m; i += gridDim.x * u32(cm.nslot)) {
-                const size_t o = size_t(i) * R + j0 + cm.col;
-                const T xv = x[o] + g * p[o];
-                const T rv = r[o] - g * q[o];
-                x[o] = xv;
-                r[o] = rv;
-                xb += double(xv) * double(rhs[o]);
-                xr += double(xv) * double(rv);
-                if (x0) x0r += double(x0[o]) * double(rv);
-            }
-        }
-        red[threadIdx.x] = xb;
-        red[TB + threadIdx.x] = xr;
-        red[2 * TB + threadIdx.x] = x0r;
-        __syncthreads();
-        if (int(threadIdx.x) < cm.Rc) {
-            double a = 0.0, b = 0.0, c = 0.0;
-            for (int sl = 0; sl < cm.nslot; sl++) {
-                a += red[sl * cm.Rc + threadIdx.x];
-                b += red[TB + sl * cm.Rc + threadIdx.x];
-                c += red[2 * TB + sl * cm.Rc + threadIdx.x];
-            }
-            double* o = cta_part + size_t(blockIdx.x) * 3 * R + j0 + threadIdx.x;
-            o[0] = a;
-            o[R] = b;
-            o[2 * R] = c;
-        }
-        __syncthreads();
-    }
-}
-
-// Stopping rule (cg.rs:239-253) and beta; counts the active columns. Single block.
-__global__ void k_cg_stop(CgState st, int R, int k, double tol) {
-    __shared__ int cnt;
-    if (threadIdx.x == 0) cnt = 0;
-    __syncthreads();
-    int local = 0;
-    for (int j = threadIdx.x; j < R; j += blockDim.x) {
-        double beta = 0.0;
-        if (st.active[j] == 1) {
-            double* ring = st.ring + size_t(j) * WINDOW;
-            ring[(k - 1) % WINDOW] = st.gamma[j] * st.rho[j];
-            const double ssk = st.ss1[j] - (st.xconst[j] + st.xb[j] + st.xb[R + j] + st.xb[2 * R + j]);
-            const double thr = fmax(tol * tol * ssk, st.floor_[j]);
-            double sum = 0.0;
-            for (int w = 0; w < WINDOW; w++) sum += ring[w];
-            const double rn = st.rho_new[j];
-            const bool done = k >= WINDOW && sum <= thr;
-            const bool at_roundoff = rn <= st.floor_[j];
-            // In an FP32 round (pfloor > 0) a breakdown or the FP32 round-off floor ends the round
-            // with another FP64 restart (state 2); only the window rule stops the column.
-            if (done) st.active[j] = 0;
-            else if (at_roundoff || !(rn > 0.0)) st.active[j] = st.pfloor[j] > 0.0 ? 2 : 0;
-            else if (rn <= st.pfloor[j]) st.active[j] = 2;
-            else beta = rn / st.rho[j];
-        }
-        st.beta[j] = beta;
-        st.rho[j] = st.rho_new[j];
-        local += st.active[j] == 1;
-    }
-    atomicAdd(&cnt, local);  // integer count: order independent
-    __syncthreads();
-    if (threadIdx.x == 0) *st.n_active = cnt;
-}
-
 // End of an FP32 refinement round, on the FP64 quantities of the refined iterate x: rho = r'M^-1 r
 // of its true residual, xconst = x'rhs, pq = x'r. A column is accepted (state 0) only when
 // rho <= max(tol^2 ss_k, floor) with ss_k = ss1 - x'(rhs + r), whether the round ended it by the
@@ -213,17 +122,6 @@ __global__ void k_refine_accept(CgState st, int R, double tol) {
     atomicAdd(&cnt, local);  // integer count: order independent
     __syncthreads();
     if (threadIdx.x == 0) *st.n_active = cnt;
-}
-
-// p = z + beta p on the active columns, 0 on the others.
-template <class T>
-__global__ void k_update_p(T* __restrict__ p, const T* __restrict__ z, const double* __restrict__ beta,
-                           const int* __restrict__ active, u32 m, int R) {
-    const size_t total = size_t(m) * R;
-    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
-        const int j = int(i % R);
-        p[i] = active[j] == 1 ? z[i] + T(beta[j]) * p[i] : T(0);
-    }
 }
 
 template <class Src, class Dst>

@@ -35,9 +35,22 @@ __device__ __forceinline__ bool last_cta(unsigned* ticket) {
     return last;
 }
 
-// Column sums of [nparts x ncols] partials by one CTA in the order of k_reduce_cols: warp w takes
-// columns w, w + warps, ...; lane l adds parts l, l + 32, ...; then a fixed butterfly.
-__device__ __forceinline__ void cta_col_sums(const double* part, int nparts, int ncols, double* out) {
+// Above WIDE_R columns the vector kernels give each thread whole columns (coalesced across the
+// threads), and the last CTA sums a column's partials with one thread, in part order.
+constexpr int WIDE_R = 64;
+
+// Column sums of [nparts x ncols] partials by one CTA in a fixed order: up to WIDE_R columns (the
+// order of k_reduce_cols) warp w takes columns w, w + warps, ..., lane l adds parts l, l + 32, ...,
+// then a fixed butterfly; wider, thread t adds the parts of columns t, t + threads, ... in order.
+__device__ __forceinline__ void cta_col_sums(const double* part, int nparts, int ncols, int R, double* out) {
+    if (R > WIDE_R) {
+        for (int col = threadIdx.x; col < ncols; col += blockDim.x) {
+            double acc = 0.0;
+            for (int p = 0; p < nparts; p++) acc += __ldcg(part + size_t(p) * ncols + col);
+            out[col] = acc;
+        }
+        return;
+    }
     const int lane = int(threadIdx.x & 31), w = int(threadIdx.x >> 5), nw = int(blockDim.x >> 5);
     for (int col = w; col < ncols; col += nw) {
         double acc = 0.0;
@@ -47,10 +60,22 @@ __device__ __forceinline__ void cta_col_sums(const double* part, int nparts, int
     }
 }
 
-// Per-CTA partials of a'b per column (the layout of k_dot).
+// Per-CTA partials of a'b per column (the layout of k_dot); above WIDE_R columns thread t takes
+// columns t, t + threads, ... over the CTA's rows.
 template <class T>
 __device__ __forceinline__ void dot_partials(const T* __restrict__ a, const T* __restrict__ b, u32 m, int R,
                                              double* __restrict__ cta_part, double* red) {
+    if (R > WIDE_R) {
+        for (int c = threadIdx.x; c < R; c += blockDim.x) {
+            double acc = 0.0;
+            for (u32 i = blockIdx.x; i < m; i += gridDim.x) {
+                const size_t o = size_t(i) * R + c;
+                acc += double(a[o]) * double(b[o]);
+            }
+            cta_part[size_t(blockIdx.x) * R + c] = acc;
+        }
+        return;
+    }
     for (int j0 = 0; j0 < R; j0 += RC_MAX) {
         const ColMap cm = colmap(R, j0);
         double acc = 0.0;
@@ -70,14 +95,14 @@ __device__ __forceinline__ void dot_partials(const T* __restrict__ a, const T* _
     }
 }
 
-// p'q, then gamma = rho / p'q on the active columns (k_cg_gamma).
+// p'q, then gamma = rho / p'q on the active columns (a non-positive or non-finite p'q deactivates).
 template <class T>
 __global__ void __launch_bounds__(TB) k_pq_gamma(const T* __restrict__ p, const T* __restrict__ q, u32 m, int R,
                                                  double* __restrict__ cta_part, CgState st, CgLoop lp) {
     __shared__ double red[TB];
     dot_partials(p, q, m, R, cta_part, red);
     if (!last_cta(lp.ticket)) return;
-    cta_col_sums(cta_part, int(gridDim.x), R, st.pq);
+    cta_col_sums(cta_part, int(gridDim.x), R, R, st.pq);
     __syncthreads();
     for (int j = threadIdx.x; j < R; j += blockDim.x) {
         double g = 0.0;
@@ -91,13 +116,33 @@ __global__ void __launch_bounds__(TB) k_pq_gamma(const T* __restrict__ p, const 
     if (threadIdx.x == 0) lp.ticket[0] = 0;
 }
 
-// x += gamma p, r -= gamma q, and x'rhs, x'r, x0'r into st.xb (k_update_xr, reduced here).
+// x += gamma p, r -= gamma q, and x'rhs, x'r, x0'r (x0 null: 0) into st.xb.
 template <class T>
 __global__ void __launch_bounds__(TB) k_update_xr_sum(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
                                                       const T* __restrict__ q, const T* __restrict__ rhs,
                                                       const T* __restrict__ x0, u32 m, int R,
                                                       double* __restrict__ cta_part, CgState st, CgLoop lp) {
     __shared__ double red[3 * TB];
+    if (R > WIDE_R) {
+        for (int c = threadIdx.x; c < R; c += blockDim.x) {
+            const T g = T(st.gamma[c]);
+            double xb = 0.0, xr = 0.0, x0r = 0.0;
+            for (u32 i = blockIdx.x; i < m; i += gridDim.x) {
+                const size_t o = size_t(i) * R + c;
+                const T xv = x[o] + g * p[o];
+                const T rv = r[o] - g * q[o];
+                x[o] = xv;
+                r[o] = rv;
+                xb += double(xv) * double(rhs[o]);
+                xr += double(xv) * double(rv);
+                if (x0) x0r += double(x0[o]) * double(rv);
+            }
+            double* o = cta_part + size_t(blockIdx.x) * 3 * R + c;
+            o[0] = xb;
+            o[R] = xr;
+            o[2 * R] = x0r;
+        }
+    } else
     for (int j0 = 0; j0 < R; j0 += RC_MAX) {
         const ColMap cm = colmap(R, j0);
         double xb = 0.0, xr = 0.0, x0r = 0.0;
@@ -133,11 +178,11 @@ __global__ void __launch_bounds__(TB) k_update_xr_sum(T* __restrict__ x, T* __re
         __syncthreads();
     }
     if (!last_cta(lp.ticket + 1)) return;
-    cta_col_sums(cta_part, int(gridDim.x), 3 * R, st.xb);
+    cta_col_sums(cta_part, int(gridDim.x), 3 * R, R, st.xb);
     if (threadIdx.x == 0) lp.ticket[1] = 0;
 }
 
-// rho_new = r'z, then the stopping rule and beta (k_cg_stop) with the device iteration counter;
+// rho_new = r'z, then the stopping rule (cg.rs:239-253) and beta with the device iteration counter;
 // the probe's contraction inputs are recorded at PROBE_FROM and PROBE_AT.
 template <class T>
 __global__ void __launch_bounds__(TB) k_rz_stop(const T* __restrict__ r, const T* __restrict__ z, u32 m, int R,
@@ -147,7 +192,7 @@ __global__ void __launch_bounds__(TB) k_rz_stop(const T* __restrict__ r, const T
     __shared__ int cnt, kk;
     dot_partials(r, z, m, R, cta_part, red);
     if (!last_cta(lp.ticket + 2)) return;
-    cta_col_sums(cta_part, int(gridDim.x), R, st.rho_new);
+    cta_col_sums(cta_part, int(gridDim.x), R, R, st.rho_new);
     if (threadIdx.x == 0) {
         cnt = 0;
         kk = ++lp.ctl[1];

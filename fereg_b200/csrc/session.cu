@@ -82,15 +82,20 @@ GpuSession::GpuSession(const std::vector<const u32*>& codes, const std::vector<u
     } else {
         sumw_ = double(n);
     }
-    ab_ = std::make_unique<GpuAbsorber>(tptr, tg, w, n, ctx);
+    // the term codes on the device: the session's copies, from which the absorber also builds its
+    // cell structure
     d_ = std::make_unique<SessionDev>();
     SessionDev& d = *d_;
-    d.st = ab_->stream();
-    AllocScope alloc_scope(d.st);
+    std::vector<const u32*> dcodes;
     for (auto& c : tcodes_) {
         d.tcodes.emplace_back();
-        d.tcodes.back().upload(c, d.st);
+        d.tcodes.back().upload(c, nullptr);
+        dcodes.push_back(d.tcodes.back().p);
     }
+    CK(cudaStreamSynchronize(nullptr));
+    ab_ = std::make_unique<GpuAbsorber>(tptr, tg, w, n, ctx, &dcodes);
+    d.st = ab_->stream();
+    AllocScope alloc_scope(d.st);
     for (auto& c : ccodes_) {
         d.ccodes.emplace_back();
         d.ccodes.back().upload(c, d.st);
@@ -642,15 +647,30 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
     }
-    d.e.alloc(n);
-    d.part.alloc(ST_GRID);
-    d.sums.alloc(1);
-    k_resid_e<<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, d.col.p, d.beta.p, int(k), y_abs ? 1 : 0, wv, d.e.p, d.part.p);
-    k_sum_parts<<<1, 32, 0, st>>>(d.part.p, ST_GRID, 1, d.sums.p);
-    d.launches += 2;
+    // With the iid variance and no residuals asked for, rss comes from the Gram through the normal
+    // equations, rss = y'Wy - b'X'Wy, unless that difference cancels (rss below 1e-6 of y'Wy); the
+    // residual pass (which the other variances and the residual output need) otherwise.
     double rss = 0.0;
-    CK(cudaMemcpyAsync(&rss, d.sums.p, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    bool rss_done = false;
+    if (vce == 0 && !out.resid && !y_abs && g[0] > 0.0) {
+        double by = 0.0;
+        for (size_t a = 0; a < k; a++) by += beta[a] * g[kept[a] * r];
+        const double rg = g[0] - by;
+        if (rg > 1e-6 * g[0]) {
+            rss = rg;
+            rss_done = true;
+        }
+    }
+    if (!rss_done) {
+        d.e.alloc(n);
+        d.part.alloc(ST_GRID);
+        d.sums.alloc(1);
+        k_resid_e<<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, d.col.p, d.beta.p, int(k), y_abs ? 1 : 0, wv, d.e.p, d.part.p);
+        k_sum_parts<<<1, 32, 0, st>>>(d.part.p, ST_GRID, 1, d.sums.p);
+        d.launches += 2;
+        CK(cudaMemcpyAsync(&rss, d.sums.p, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
     const double rss_s = rss / (sd_y * sd_y);
 
     // bread: the standardized inverse, bordered by the constant (vcov.rs:220)

@@ -1,27 +1,31 @@
 // Kernels for the short lists: segments of at most WT cells (and WT rows) and coordinate lists
 // of at most PULL_WARP_MAX entries. Longer lists go to the CTA tiles (tiles.cuh).
 //
-// The operator's and the right-hand side's segment passes use lane groups: a group of L lanes
-// takes one segment at a time, lane j of the group holding columns j and j + L of the launch's
-// column chunk, so 32 / L segments share every warp instruction. The group loads the indices of
-// L cells at once, one per lane and coalesced, and takes the cells in turn with the indices
-// broadcast by shuffles, several cells' gathers in flight together.
+// The operator's passes (k_vseg_apply, k_vpull_apply) run on the PCG's padded vectors (a row
+// stride that is a multiple of 4): lane j of a group of L lanes holds 4 consecutive columns,
+// gathered with 16-byte loads. The segment pass gives each group one segment at a time and the
+// group walks its cells in order; the list pass deals a list's entries to the groups and adds
+// their sums in group order.
 //
-// The coordinate-list passes and the residualization use warp tiles: a warp takes whole
+// The right-hand side's segment pass (k_grhs) uses lane groups over the caller's rows: lane j of
+// a group holds columns j and j + L of the launch's column chunk; the group loads the indices of
+// L cells at once, one per lane and coalesced, and takes the cells in turn with the indices
+// broadcast by shuffles. The small coordinates accumulate in lane-private shared slots that the
+// CTA adds in a fixed order.
+//
+// The right-hand side's list pass and the residualization use warp tiles: a warp takes whole
 // consecutive segments (at most WSEG segments, WT cells and WT rows in all) or whole consecutive
 // coordinate lists (at most PULL_WARP_MAX entries). The tile's indices are staged first, one lane
 // per cell, segment or entry, into the warp's shared memory. Then every loop runs on all lanes as
 // (group g, column j) pairs: a column chunk of Rc columns is padded to RCP (a power of two), the
 // warp holds G = 32 / RCP groups, and cells and rows are dealt to the groups in turn (cell i to
-// group i mod G). The operator's coordinate-list pass gives each lane two columns instead (groups
-// of L = lanes_of(Rc) lanes, as the lane groups do). Segment sums: while a lane walks its cells (in order) it keeps a running sum of
+// group i mod G). Segment sums: while a lane walks its cells (in order) it keeps a running sum of
 // the current segment and parks it in a lane-private slot when the segment ends; the segment's
 // value is then the sum of its G slots in group order.
 //
-// Every lane's sums run in a fixed order, and the small coordinates accumulate in lane-private
-// shared slots that the CTA adds in a fixed order: results do not depend on timing. The number of
-// blocks is a template parameter NBK (the exact count up to WNB - 1; WNB means WNB or more, the
-// ones past WNB read from global memory).
+// Every lane's sums run in a fixed order: results do not depend on timing. The number of blocks
+// is a template parameter NBK (the exact count up to WNB - 1; WNB means WNB or more, the ones past
+// WNB read from global memory).
 #pragma once
 
 #include "tiles.cuh"
@@ -220,127 +224,160 @@ __device__ __forceinline__ void flush_pairs(const T* wacc_all, u32 ms_acc, int R
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The operator's passes on the PCG's padded vectors (row stride Rv, a multiple of 4, 16-byte
+// aligned rows): lane j of a group of L lanes holds the 4 consecutive columns j0 + 4j .. j0 + 4j + 3
+// of the launch's chunk, gathered with 16-byte loads (two per row in FP64, one in FP32).
+constexpr int VCOLS = 128;  // columns per launch of the padded-vector passes (32 lanes x 4)
+
+template <class T>
+struct V4 {
+    T a, b, c, d;
+};
+__device__ __forceinline__ V4<double> ld4(const double* p) {
+    const double2 x = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 y = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return V4<double>{x.x, x.y, y.x, y.y};
+}
+__device__ __forceinline__ V4<float> ld4(const float* p) {
+    const float4 x = __ldg(reinterpret_cast<const float4*>(p));
+    return V4<float>{x.x, x.y, x.z, x.w};
+}
+// L2-coherent load of values written earlier in the same pass sequence (t)
+__device__ __forceinline__ V4<double> ld4cg(const double* p) {
+    const double2 x = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 y = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    return V4<double>{x.x, x.y, y.x, y.y};
+}
+__device__ __forceinline__ V4<float> ld4cg(const float* p) {
+    const float4 x = __ldcg(reinterpret_cast<const float4*>(p));
+    return V4<float>{x.x, x.y, x.z, x.w};
+}
+__device__ __forceinline__ void st4(double* p, const V4<double>& v) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v.a, v.b);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v.c, v.d);
+}
+__device__ __forceinline__ void st4(float* p, const V4<float>& v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v.a, v.b, v.c, v.d);
+}
+template <class T>
+__device__ __forceinline__ void add4(V4<T>& s, const V4<T>& v) {
+    s.a += v.a;
+    s.b += v.b;
+    s.c += v.c;
+    s.d += v.d;
+}
+template <class T>
+__device__ __forceinline__ void sub4(V4<T>& s, const V4<T>& v) {
+    s.a -= v.a;
+    s.b -= v.b;
+    s.c -= v.c;
+    s.d -= v.d;
+}
+template <class T>
+__device__ __forceinline__ void fma4(V4<T>& s, T w, const V4<T>& v) {
+    s.a += w * v.a;
+    s.b += w * v.b;
+    s.c += w * v.c;
+    s.d += w * v.d;
+}
+// The rows of the small coordinates (0 .. ms_acc - 1, the first blocks) of the launch's column
+// chunk, staged in shared memory once per CTA: every cell holds one of them per small block, and a
+// gather from shared memory spares the L1 the tag and line work of a global gather.
+template <class T>
+__device__ __forceinline__ void stage_small(T* sp, const T* __restrict__ P, size_t Ru, int j0, int Rc, u32 ms) {
+    for (u32 i = threadIdx.x; i < ms * u32(Rc); i += blockDim.x)
+        sp[i] = P[size_t(i / u32(Rc)) * Ru + j0 + i % u32(Rc)];
+    __syncthreads();
+}
+__device__ __forceinline__ V4<double> ld4s(const double* p) {
+    const double2 x = reinterpret_cast<const double2*>(p)[0];
+    const double2 y = reinterpret_cast<const double2*>(p)[1];
+    return V4<double>{x.x, x.y, y.x, y.y};
+}
+__device__ __forceinline__ V4<float> ld4s(const float* p) {
+    const float4 x = *reinterpret_cast<const float4*>(p);
+    return V4<float>{x.x, x.y, x.z, x.w};
+}
+// Shared memory of the staged small rows for an Rc-column chunk (0: none staged).
+template <class T>
+__host__ __device__ constexpr size_t small_stage_bytes(u32 ms, int Rc) {
+    return al16(size_t(ms) * size_t(Rc) * sizeof(T));
+}
+
+// Lanes per group for an Rc-column chunk (Rc a multiple of 4).
+__host__ __device__ constexpr int vlanes_of(int Rc) { return rcp_of((Rc + 3) / 4); }
+
+// Sum over the blocks of the rows P[coord_b(c)] (this lane's 4 columns): the first NL blocks'
+// coordinates in `code`, the ones past WNB (NBK == WNB) read from the structure.
+template <int NBK, class T>
+__device__ __forceinline__ V4<T> gather4(const DevStruct& S, const u32* code, const T* __restrict__ Pj, size_t Ru,
+                                         u32 c, const T* spj, int nsm, int Rc) {
+    constexpr int NL = NBK < WNB ? NBK : WNB;
+    // the first nsm blocks are small, their rows staged at spj (stride Rc)
+    V4<T> u = nsm > 0 ? ld4s(spj + size_t(code[0]) * Rc) : ld4(Pj + size_t(code[0]) * Ru);
+#pragma unroll
+    for (int b = 1; b < NL; b++) add4(u, b < nsm ? ld4s(spj + size_t(code[b]) * Rc) : ld4(Pj + size_t(code[b]) * Ru));
+    if constexpr (NBK == WNB)
+        for (u32 b = WNB; b < S.nb; b++) add4(u, ld4(Pj + size_t(__ldg(S.coord + size_t(b) * S.M + c)) * Ru));
+    return u;
+}
+
 // Operator pass 1 (operator.rs:894-948) on the short segments, one segment per lane group:
-// t_s = n1inv_s sum_c W_c u_c with u_c = sum_b P[coord_b(c)], and the small coordinates take
-// sum_c W_c u_c - t_s sum_c W_c per small code. segs lists the short segments in order; group q
-// of the grid takes segs[q], segs[q + groups], ... so every lane's sums have a fixed order.
-//
-// The group walks its segment in chunks of L cells: lane i of the group loads the block codes
-// and the weight of the chunk's cell i (one coalesced load per block), and the cells are then
-// taken in turn with the codes broadcast by shuffles, four cells' gathers in flight together.
-// The small codes are the first blocks' codes, already at hand. The second walk (t_s times the
-// weights) reloads the chunk's small codes, which the first left in L1. The next segment's index
-// is fetched while the current one runs. The groups of a warp never wait on one another.
-template <class T, int L, int NBK>
-__global__ void __launch_bounds__(WPB * 32, 4) k_gseg_apply(DevStruct S, DevWeights W, const u32* __restrict__ segs,
-                                                            u32 nsegs, const T* __restrict__ P, int R, int j0, int Rc,
-                                                            T* __restrict__ t, T* __restrict__ cta_small) {
+// t_s = n1inv_s sum_c W_c u_c with u_c = sum_b P[coord_b(c)]. segs lists the short segments in
+// order; group q of the grid takes segs[q], segs[q + groups], ... Each group walks its segment's
+// cells in order, two cells' gathers in flight together, the lanes' sums in cell order.
+template <class T, int L, int NBK, bool WEIGHTED>
+__global__ void __launch_bounds__(WPB * 32, 4) k_vseg_apply(DevStruct S, DevWeights W, const u32* __restrict__ segs,
+                                                            u32 nsegs, const T* __restrict__ P, int Rv, int j0, int Rc,
+                                                            T* __restrict__ t, int stage) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int G = 32 / L;
-    constexpr int NL = NBK < WNB ? NBK : WNB;  // blocks whose codes the lanes hold
-    constexpr int U = 4;                       // cells whose gathers are in flight together
-    T* wacc_all = reinterpret_cast<T*>(smem_raw);
-    const bool acc = cta_small != nullptr;
-    const bool weighted = W.cell_w != nullptr;
+    constexpr int NL = NBK < WNB ? NBK : WNB;
     const u32 lane = wlane(), g = lane / L, j = lane % L;
-    const bool on0 = int(j) < Rc, on1 = int(j) + L < Rc;
-    const unsigned gmask = L == 32 ? FULL : ((1u << L) - 1u) << (g * L);
-    const size_t Ru = size_t(R);
-    const int ns_acc = acc ? int(S.ns_acc) : 0;
-    T* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 64 + lane;  // slot(k, c) at [(2k + c) * 32]
-    if (acc)
-        for (u32 i = 0; i < S.ms_acc * 2; i++) wacc[i * 32] = T(0);
-    const T* Pj = P + j0 + j;
+    const bool on = int(4 * j) < Rc;
+    const size_t Ru = size_t(Rv);
+    const T* Pj = P + j0 + 4 * j;
+    T* sp = reinterpret_cast<T*>(smem_raw);
+    const int nsm = stage ? int(S.ns_acc) : 0;
+    if (nsm) stage_small(sp, P, Ru, j0, Rc, S.ms_acc);
+    const T* spj = sp + 4 * j;
     const u32 groups = gridDim.x * WPB * G;
-    u32 q = (blockIdx.x * WPB + wid_in_cta()) * G + g;
-    u32 s = q < nsegs ? segs[q] : 0;
-    for (; q < nsegs; q += groups) {
+    for (u32 q = (blockIdx.x * WPB + wid_in_cta()) * G + g; q < nsegs; q += groups) {
+        const u32 s = segs[q];
         const u32 c0 = S.seg_off[s], c1 = S.seg_off[s + 1];
-        const u32 qn = q + groups;
-        const u32 sn = qn < nsegs ? segs[qn] : 0;
-        T sum0 = T(0), sum1 = T(0);
-        for (u32 cb = c0; cb < c1; cb += L) {
-            const u32 nc = min(c1 - cb, u32(L));
-            u32 code[NL];
-            double wl = 1.0;
+        V4<T> acc{T(0), T(0), T(0), T(0)};
+        if (on) {
+            u32 c = c0;
+            for (; c + 2 <= c1; c += 2) {
+                u32 k0[NL], k1[NL];
 #pragma unroll
-            for (int b = 0; b < NL; b++) code[b] = j < nc ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
-            if (weighted && j < nc) wl = W.cell_w[cb + j];
-            for (u32 i0 = 0; i0 < nc; i0 += U) {
-                T x0[U], x1[U];
-                u32 k0[U];
-#pragma unroll
-                for (int k = 0; k < U; k++) {
-                    const u32 i = i0 + u32(k);
-                    const bool live = i < nc;
-                    T a0 = T(0), a1 = T(0);
-#pragma unroll
-                    for (int b = 0; b < NL; b++) {
-                        const u32 cd = __shfl_sync(gmask, code[b], int(i), L);
-                        if (b == 0) k0[k] = cd;
-                        const T* row = Pj + size_t(cd) * Ru;
-                        if (live && on0) a0 += row[0];
-                        if (live && on1) a1 += row[L];
-                    }
-                    if constexpr (NBK == WNB)
-                        if (live)
-                            for (u32 b = WNB; b < S.nb; b++) {
-                                const T* row = Pj + size_t(__ldg(S.coord + size_t(b) * S.M + cb + i)) * Ru;
-                                if (on0) a0 += row[0];
-                                if (on1) a1 += row[L];
-                            }
-                    x0[k] = a0;
-                    x1[k] = a1;
+                for (int b = 0; b < NL; b++) {
+                    k0[b] = __ldg(S.coord + size_t(b) * S.M + c);
+                    k1[b] = __ldg(S.coord + size_t(b) * S.M + c + 1);
                 }
-#pragma unroll
-                for (int k = 0; k < U; k++) {
-                    const u32 i = i0 + u32(k);
-                    const T w = weighted ? T(__shfl_sync(gmask, wl, int(i), L)) : T(1);
-                    if (i < nc) {
-                        const T v0 = w * x0[k], v1 = w * x1[k];
-                        sum0 += v0;
-                        sum1 += v1;
-                        if (acc) {
-                            T* sl = wacc + k0[k] * 64;
-                            sl[0] += v0;
-                            sl[32] += v1;
-                            for (int b = 1; b < ns_acc; b++) {
-                                T* sb = wacc + __ldg(S.coord + size_t(b) * S.M + cb + i) * 64;
-                                sb[0] += v0;
-                                sb[32] += v1;
-                            }
-                        }
-                    }
+                const V4<T> u0 = gather4<NBK>(S, k0, Pj, Ru, c, spj, nsm, Rc);
+                const V4<T> u1 = gather4<NBK>(S, k1, Pj, Ru, c + 1, spj, nsm, Rc);
+                if constexpr (WEIGHTED) {
+                    fma4(acc, T(W.cell_w[c]), u0);
+                    fma4(acc, T(W.cell_w[c + 1]), u1);
+                } else {
+                    add4(acc, u0);
+                    add4(acc, u1);
                 }
             }
+            if (c < c1) {
+                u32 k0[NL];
+#pragma unroll
+                for (int b = 0; b < NL; b++) k0[b] = __ldg(S.coord + size_t(b) * S.M + c);
+                const V4<T> u0 = gather4<NBK>(S, k0, Pj, Ru, c, spj, nsm, Rc);
+                if constexpr (WEIGHTED) fma4(acc, T(W.cell_w[c]), u0);
+                else add4(acc, u0);
+            }
+            const T n1i = T(W.n1inv[s]);
+            st4(t + size_t(s) * Ru + j0 + 4 * j, V4<T>{acc.a * n1i, acc.b * n1i, acc.c * n1i, acc.d * n1i});
         }
-        const T n1i = T(W.n1inv[s]);
-        const T tv0 = sum0 * n1i, tv1 = sum1 * n1i;
-        if (on0) t[size_t(s) * Ru + j0 + j] = tv0;
-        if (on1) t[size_t(s) * Ru + j0 + j + L] = tv1;
-        if (acc)
-            for (u32 cb = c0; cb < c1; cb += L) {
-                const u32 nc = min(c1 - cb, u32(L));
-                u32 code[WNB];
-#pragma unroll
-                for (int b = 0; b < WNB; b++)
-                    code[b] = (b < ns_acc && j < nc) ? __ldg(S.coord + size_t(b) * S.M + cb + j) : 0u;
-                const double wl = (weighted && j < nc) ? W.cell_w[cb + j] : 1.0;
-                for (u32 i = 0; i < nc; i++) {
-                    const T w = weighted ? T(__shfl_sync(gmask, wl, int(i), L)) : T(1);
-                    const T d0 = w * tv0, d1 = w * tv1;
-#pragma unroll
-                    for (int b = 0; b < WNB; b++)
-                        if (b < ns_acc) {
-                            T* sl = wacc + __shfl_sync(gmask, code[b], int(i), L) * 64;
-                            sl[0] -= d0;
-                            sl[32] -= d1;
-                        }
-                }
-            }
-        s = sn;
     }
-    if (acc) flush_pairs<L>(wacc_all, S.ms_acc, Rc, j0, R, cta_small);
 }
 
 // Staging of a coordinate-list tile: list ends and the entries' indices.
@@ -380,69 +417,74 @@ __device__ __forceinline__ void stage_pull(const DevStruct& S, u32 k0, u32 k1, u
     }
 }
 
-// Operator pass 2 on short coordinate lists (k >= ms_acc): Y[k] = nr_k P[k] + sum over the cells
-// c of k of W_c (sum_{other b} P[coord_b(c)] - t_{s(c)}). Warp tiles of whole lists, staged; the
-// entries are dealt to groups of L lanes (L = lanes_of(Rc)), lane j of a group holding columns j
-// and j + L, and the groups' sums are added in group order.
-template <class T, int L, int NBK>
-__global__ void __launch_bounds__(WPB * 32, 4) k_wpull_apply(DevStruct S, DevWeights W, WarpTiles wt,
-                                                             const T* __restrict__ P, const T* __restrict__ t, int R,
-                                                             int j0, int Rc, T* __restrict__ Y) {
+// Operator pass 2 on short coordinate lists (k >= ms_acc) with the padded vectors:
+// Y[k] = nr_k P[k] + sum over the cells c of k of W_c (sum_{other b} P[coord_b(c)] - t_{s(c)}).
+// Warp tiles of whole lists, staged; the entries are dealt to groups of L lanes (lane j holding
+// 4 columns), and the groups' sums are added by a fixed xor butterfly.
+template <class T, int L, int NBK, bool WEIGHTED>
+__global__ void __launch_bounds__(WPB * 32, 4) k_vpull_apply(DevStruct S, DevWeights W, WarpTiles wt,
+                                                             const T* __restrict__ P, const T* __restrict__ t, int Rv,
+                                                             int j0, int Rc, T* __restrict__ Y, int stage) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int G = 32 / L;
     constexpr int NO = NBK - 1;  // staged other blocks (all of them below WNB blocks)
     const PullStage st = pull_stage_at(smem_raw + size_t(wid_in_cta()) * pull_bytes());
     const u32 lane = wlane(), g = lane / L, j = lane % L;
-    const bool on0 = int(j) < Rc, on1 = int(j) + L < Rc;
-    const size_t Ru = size_t(R);
+    const bool on = int(4 * j) < Rc;
+    const size_t Ru = size_t(Rv);
     const u32 no = S.nb - 1;
-    const bool weighted = W.cell_w != nullptr;
-    const T* Pj = P + j0 + j;
-    const T* tj = t + j0 + j;
-    auto total = [&](T v) {  // sum over the groups of the same column, in group order
-        T s = T(0);
+    const T* Pj = P + j0 + 4 * j;
+    const T* tj = t + j0 + 4 * j;
+    // the lists are of large coordinates: the small blocks come first among a cell's other blocks
+    T* sp = reinterpret_cast<T*>(smem_raw + size_t(WPB) * pull_bytes());
+    const int nsm = stage ? int(S.ns_acc) : 0;
+    if (nsm) stage_small(sp, P, Ru, j0, Rc, S.ms_acc);
+    const T* spj = sp + 4 * j;
+    auto total = [&](T v) {  // sum over the groups of the same lane slot, a fixed butterfly
 #pragma unroll
-        for (int gg = 0; gg < G; gg++) s += __shfl_sync(FULL, v, gg * L + int(j));
-        return s;
+        for (int o = L; o < 32; o <<= 1) v += __shfl_xor_sync(FULL, v, o);
+        return v;
     };
     const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
     uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
     for (u32 tile = wid; tile < wt.n; tile += nw) {
         const u32 k0 = tb.x, k1 = tb.y, e0 = tb.z;
-        stage_pull(S, k0, k1, e0, tb.w, st, weighted, u32(NO));
+        stage_pull(S, k0, k1, e0, tb.w, st, WEIGHTED, u32(NO));
         if (tile + nw < wt.n) tb = wt.t[tile + nw];
         __syncwarp();
         u32 i0 = 0;
         for (u32 kl = 0; kl < k1 - k0; kl++) {
             const u32 ie = st.kend[kl];
-            T acc0 = T(0), acc1 = T(0);
-#pragma unroll 8
-            for (u32 i = i0 + g; i < ie; i += G) {
-                const T* trow = tj + size_t(st.seg[i]) * Ru;
-                T v0 = on0 ? -__ldcg(trow) : T(0);
-                T v1 = on1 ? -__ldcg(trow + L) : T(0);
+            V4<T> acc{T(0), T(0), T(0), T(0)};
+            if (on) {
+#pragma unroll 2
+                for (u32 i = i0 + g; i < ie; i += G) {
+                    V4<T> v = ld4cg(tj + size_t(st.seg[i]) * Ru);
+                    v.a = -v.a;
+                    v.b = -v.b;
+                    v.c = -v.c;
+                    v.d = -v.d;
 #pragma unroll
-                for (int o = 0; o < NO; o++) {
-                    const T* row = Pj + size_t(st.oth[o * PULL_WARP_MAX + i]) * Ru;
-                    if (on0) v0 += row[0];
-                    if (on1) v1 += row[L];
-                }
-                if constexpr (NBK == WNB)
-                    for (u32 o = WNO; o < no; o++) {
-                        const T* row = Pj + size_t(S.pl_other[size_t(e0 + i) * no + o]) * Ru;
-                        if (on0) v0 += row[0];
-                        if (on1) v1 += row[L];
+                    for (int o = 0; o < NO; o++) {
+                        const u32 x = st.oth[o * PULL_WARP_MAX + i];
+                        add4(v, o < nsm ? ld4s(spj + size_t(x) * Rc) : ld4(Pj + size_t(x) * Ru));
                     }
-                const T w = weighted ? T(W.cell_w[st.cell[i]]) : T(1);
-                acc0 += w * v0;
-                acc1 += w * v1;
+                    if constexpr (NBK == WNB)
+                        for (u32 o = WNO; o < no; o++)
+                            add4(v, ld4(Pj + size_t(S.pl_other[size_t(e0 + i) * no + o]) * Ru));
+                    if constexpr (WEIGHTED) fma4(acc, T(W.cell_w[st.cell[i]]), v);
+                    else add4(acc, v);
+                }
             }
-            acc0 = total(acc0);
-            acc1 = total(acc1);
-            if (g == 0) {
-                const size_t o = size_t(k0 + kl) * Ru + j0 + j;
-                if (on0) Y[o] = T(W.nr[k0 + kl]) * P[o] + acc0;
-                if (on1) Y[o + L] = T(W.nr[k0 + kl]) * P[o + L] + acc1;
+            acc.a = total(acc.a);
+            acc.b = total(acc.b);
+            acc.c = total(acc.c);
+            acc.d = total(acc.d);
+            if (g == 0 && on) {
+                const size_t o = size_t(k0 + kl) * Ru + j0 + 4 * j;
+                const T nrk = T(W.nr[k0 + kl]);
+                const V4<T> pk = ld4(P + o);
+                st4(Y + o, V4<T>{nrk * pk.a + acc.a, nrk * pk.b + acc.b, nrk * pk.c + acc.c, nrk * pk.d + acc.d});
             }
             i0 = ie;
         }
@@ -452,7 +494,7 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_apply(DevStruct S, DevWei
 
 // ---------------------------------------------------------------------------------------------
 // Right-hand side pass 1 (operator.rs:969-1066) on the short segments, one segment per lane group
-// in the order of k_gseg_apply: b1_s = sum over the segment's rows of w v; per-CTA partials of
+// in the order of k_vseg_apply: b1_s = sum over the segment's rows of w v; per-CTA partials of
 // [sum w v^2, sum w v] (cta_part[blockIdx][2R], this chunk's columns); the small coordinates take
 // sum_c s_c - (b1_s / n1_s) sum_c W_c per small code (s_c: the sum over the rows of cell c). The
 // group streams its segment's rows (contiguous in the block): with one row per cell, in chunks of

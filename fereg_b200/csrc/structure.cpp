@@ -10,6 +10,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <cmath>
 #include <numeric>
 
 #include "common.h"
@@ -19,6 +20,24 @@ namespace fereg {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
+
+void check_codes_host(const std::vector<const u32*>& codes, const std::vector<u32>& g, size_t n) {
+    for (size_t q = 0; q < codes.size(); q++) {
+        const u32* c = codes[q];
+        const u32 gq = g[q];
+        int bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static) if (n > (size_t(1) << 20))
+        for (long long i = 0; i < (long long)n; i++) bad |= c[i] >= gq;
+        if (bad) throw Error(RC_INVALID_INPUT, "term code out of range of its level count");
+    }
+}
+
+void check_weights_host(const double* w, size_t n) {
+    int bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static) if (n > (size_t(1) << 20))
+    for (long long i = 0; i < (long long)n; i++) bad |= !(std::isfinite(w[i]) && w[i] > 0.0);
+    if (bad) throw Error(RC_INVALID_INPUT, "weights must be positive and finite");
+}
 
 // absorber.rs:100-108: the intercept-only term with the most levels, first on ties.
 int fe1_index(const std::vector<u32>& g) {

@@ -194,34 +194,6 @@ __global__ void __launch_bounds__(TB) k_seg_apply(DevStruct S, DevWeights W, con
     }
 }
 
-// Small coordinates of the slices of long segments, once t is complete: adds
-// sum W_c (u_c - t_s) over the slice's cells to the CTA rows of cta_small.
-template <class T>
-__global__ void __launch_bounds__(TB) k_seg_small_slices(DevStruct S, DevWeights W, const T* __restrict__ P,
-                                                         const T* __restrict__ t, int R, T* __restrict__ cta_small) {
-    __shared__ SegSmem<T> sm;
-    const TileSet& ts = S.seg;
-    zero_cta_row(cta_small, S.ms_acc * u32(R));
-    for (u32 tile = blockIdx.x; tile < ts.n; tile += gridDim.x) {
-        const u32 s0 = ts.k0[tile], c0 = ts.e0[tile], c1 = ts.e1[tile];
-        if (ts.part[tile] < 0) continue;
-        __syncthreads();
-        seg_maps(S, s0, s0 + 1, c0, c1, sm.cellseg, sm.scode);
-        for (int j0 = 0; j0 < R; j0 += RC_MAX) {
-            const ColMap cm = colmap(R, j0);
-            if (cm.on)
-                for (u32 c = c0 + cm.slot; c < c1; c += cm.nslot) {
-                    T u = -t[size_t(s0) * R + j0 + cm.col];
-                    for (u32 b = 0; b < S.nb; b++) u += P[size_t(S.coord[size_t(b) * S.M + c]) * R + j0 + cm.col];
-                    sm.vals[(c - c0) * cm.Rc + cm.col] = T(cellw(W, c)) * u;
-                }
-            __syncthreads();
-            small_accumulate(S, sm, c1 - c0, cm, j0, R, cta_small);
-            __syncthreads();
-        }
-    }
-}
-
 // Sum over the slots of a CTA of red[slot * Rc + col] into red[col] (slot 0), by a pairwise tree
 // over the slot indices: the same order every call. Every thread of the CTA calls it.
 template <class T>

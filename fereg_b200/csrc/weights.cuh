@@ -31,6 +31,19 @@ __global__ void k_cell_weights(const double* __restrict__ w, const u32* __restri
     }
 }
 
+// out[r] = in[pi[r]]: kept-order values in row order.
+__global__ void k_gather_rows_f64(const double* __restrict__ in, const u32* __restrict__ pi, size_t n,
+                                  double* __restrict__ out) {
+    for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += size_t(gridDim.x) * blockDim.x)
+        out[r] = in[pi[r]];
+}
+
+// W_c = the number of rows of cell c (unit row weights).
+__global__ void k_cell_counts(const u32* __restrict__ cell_row, u32 M, double* __restrict__ cw) {
+    for (u32 c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x)
+        cw[c] = double(cell_row[c + 1] - cell_row[c]);
+}
+
 // n1_s = sum of W_c over the segment's cells (cw null: 1 per cell); n1inv = 1 / n1.
 __global__ void k_seg_weights(const double* __restrict__ cw, const u32* __restrict__ seg_off, u32 g1,
                               double* __restrict__ n1, double* __restrict__ n1inv) {
