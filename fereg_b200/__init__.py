@@ -195,6 +195,36 @@ def _setup(L):
     L.fereg_absorber_launches.argtypes = [P]
     L.fereg_absorber_launches.restype = C.c_uint64
     L.fereg_absorber_escalations.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    ip = C.POINTER(C.c_int)
+    L.fereg_absorber_create_terms.argtypes = [C.POINTER(u32p), u32p, ip, ip, C.POINTER(f64p), C.c_int, f64p,
+                                              C.c_size_t, P, C.POINTER(P)]
+    L.fereg_absorber_has_slopes.argtypes = [P]
+    L.fereg_absorber_term_values_len.argtypes = [P]
+    L.fereg_absorber_term_values_len.restype = C.c_size_t
+    L.fereg_slope_weight_state.argtypes = [P, f64p, f64p, u8p]
+    L.fereg_slope_apply.argtypes = [P, f64p, C.c_size_t, f64p]
+    L.fereg_slope_precond.argtypes = [P, f64p, C.c_size_t, f64p]
+    L.fereg_slope_rhs.argtypes = [P, f64p, C.c_size_t, f64p, f64p]
+    L.fereg_slope_structure.argtypes = [P, u64p, u32p]
+    L.fereg_session_relu.argtypes = [P, P, C.c_int, C.c_size_t, C.c_double, C.c_size_t, u8p, f64p, u64p]
+    L.fereg_session_create_terms.argtypes = [C.POINTER(u32p), u32p, ip, ip, C.POINTER(f64p), C.c_int, C.POINTER(u32p),
+                                             u32p, C.c_int, f64p, C.c_int, C.c_size_t, C.c_uint64, P, C.POINTER(P)]
+
+
+def _term_shapes(ncodes, intercept, slopes, n):
+    """ctypes arrays of the terms' shapes: intercept flags, slope counts and the slope variables
+    (kept order) term after term; the arrays are returned to keep them alive."""
+    icpt = [1] * ncodes if intercept is None else [int(bool(v)) for v in intercept]
+    sl = [[] for _ in range(ncodes)] if slopes is None else [list(t) for t in slopes]
+    if len(icpt) != ncodes or len(sl) != ncodes:
+        raise ValueError("intercept and slopes need one entry per term")
+    keep = [np.ascontiguousarray(x, dtype=np.float64) for t in sl for x in t]
+    if any(len(x) != n for x in keep):
+        raise ValueError("slope variables need one value per row")
+    ia = (C.c_int * max(1, ncodes))(*icpt)
+    na = (C.c_int * max(1, ncodes))(*[len(t) for t in sl])
+    sa = (f64p * max(1, len(keep)))(*[_p(x, f64p) for x in keep])
+    return ia, na, sa, keep, any(not v for v in icpt) or any(sl)
 
 
 def declared_symbols():
@@ -217,20 +247,36 @@ def _check(rc):
 class Absorber:
     """Host mirror of the reference `Absorber` (absorber.rs:62-97) over the B200 solver."""
 
-    def __init__(self, codes, g, w=None):
+    def __init__(self, codes, g, w=None, intercept=None, slopes=None):
+        """intercept / slopes (solve.rs:338 build): per term its intercept flag and its slope
+        variables (kept order); a term with slopes or without an intercept makes the absorber
+        the heterogeneous-slope solver (slopes.rs SlopeSolver)."""
         self.n = len(codes[0]) if codes else 0
         self._codes = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
         self.g = np.asarray(g, dtype=np.uint32)
         ptrs = (u32p * max(1, len(self._codes)))(*[_p(a, u32p) for a in self._codes])
         wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
         h = P()
-        _check(lib().fereg_absorber_create(ptrs, _p(self.g, u32p), len(self._codes), _p(wa, f64p), self.n, None,
-                                           C.byref(h)))
+        if intercept is None and slopes is None:
+            _check(lib().fereg_absorber_create(ptrs, _p(self.g, u32p), len(self._codes), _p(wa, f64p), self.n, None,
+                                               C.byref(h)))
+        else:
+            ia, na, sa, self._slopes, _ = _term_shapes(len(self._codes), intercept, slopes, self.n)
+            _check(lib().fereg_absorber_create_terms(ptrs, _p(self.g, u32p), ia, na, sa, len(self._codes),
+                                                     _p(wa, f64p), self.n, None, C.byref(h)))
         self.h = h
+        self.has_slopes = bool(lib().fereg_absorber_has_slopes(self.h))
         info = np.zeros(9, dtype=np.uint64)
         _check(lib().fereg_absorber_info(self.h, _p(info, u64p)))
         self.m, self.g1, self.ncells, self.nb, self.m_small = (int(v) for v in info[1:6])
         self.fe1 = int(np.int64(info[6]))
+        self.coefs_len = int(lib().fereg_absorber_coefs_len(self.h))
+        self.term_values_len = int(lib().fereg_absorber_term_values_len(self.h))
+        self._slot_g = []  # levels of every term-values slot
+        icpt = [True] * len(self._codes) if intercept is None else [bool(v) for v in intercept]
+        sl = [[] for _ in self._codes] if slopes is None else slopes
+        for q, gq in enumerate(self.g):
+            self._slot_g += [int(gq)] * (int(icpt[q]) + len(sl[q]))
 
     def close(self):
         if getattr(self, "h", None):
@@ -262,7 +308,7 @@ class Absorber:
         """Residualizes the n x r row-major host block `z` (row order) in place."""
         assert z.dtype == np.float64 and z.flags.c_contiguous
         r = z.shape[1] if z.ndim == 2 else 1
-        coefs = np.empty((self.m + self.g1, r)) if want_coefs else None
+        coefs = np.empty((self.coefs_len, r)) if want_coefs else None
         wa = None if warm is None else np.ascontiguousarray(warm, dtype=np.float64)
         info = SolveInfo()
         _check(lib().fereg_absorber_residualize_ex(self.h, z.ctypes.data_as(P), 0, r, tol, maxiter, int(want_coefs),
@@ -273,7 +319,7 @@ class Absorber:
     def residualize_device(self, z_ptr, r, tol=1e-8, maxiter=16000, want_coefs=False, warm=None,
                            precision=PREC_F64):
         """Residualizes an n x r row-major block already in device memory (pointer `z_ptr`)."""
-        coefs = np.empty((self.m + self.g1, r)) if want_coefs else None
+        coefs = np.empty((self.coefs_len, r)) if want_coefs else None
         wa = None if warm is None else np.ascontiguousarray(warm, dtype=np.float64)
         info = SolveInfo()
         _check(lib().fereg_absorber_residualize_ex(self.h, P(z_ptr), 1, r, tol, maxiter, int(want_coefs),
@@ -289,13 +335,51 @@ class Absorber:
 
     def term_values(self, coefs, col):
         coefs = np.ascontiguousarray(coefs, dtype=np.float64)
-        out = np.zeros(int(self.g.sum()))
+        out = np.zeros(self.term_values_len)
         _check(lib().fereg_absorber_term_values(self.h, _p(coefs, f64p), coefs.shape[1], col, _p(out, f64p)))
         res, o = [], 0
-        for gq in self.g:
+        for gq in self._slot_g:  # per term its intercept, then its slopes
             res.append(out[o:o + gq].copy())
-            o += int(gq)
+            o += gq
         return res
+
+    # slope-solver parity hooks
+    def slope_structure(self):
+        v = np.zeros(9, dtype=np.uint64)
+        bt = np.zeros(max(1, len(self._codes)), dtype=np.uint32)
+        _check(lib().fereg_slope_structure(self.h, _p(v, u64p), _p(bt, u32p)))
+        keys = ["n", "m", "e", "ge", "be", "k", "nb", "nsmall", "m_small"]
+        out = {k: int(x) for k, x in zip(keys, v)}
+        out["block_terms"] = [int(x) for x in bt[:out["nb"]]]
+        return out
+
+    def slope_weight_state(self, jlen):
+        st = self.slope_structure()
+        minv = np.empty(st["ge"] * st["be"] ** 2)
+        jinv = np.empty(jlen)
+        red = np.empty(st["m"], dtype=np.uint8)
+        _check(lib().fereg_slope_weight_state(self.h, _p(minv, f64p), _p(jinv, f64p), _p(red, u8p)))
+        return dict(minv=minv, jinv=jinv, redundant=red.astype(bool))
+
+    def slope_apply(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        y = np.empty_like(p)
+        _check(lib().fereg_slope_apply(self.h, _p(p, f64p), p.shape[1], _p(y, f64p)))
+        return y
+
+    def slope_precond(self, r_):
+        r_ = np.ascontiguousarray(r_, dtype=np.float64)
+        z = np.empty_like(r_)
+        _check(lib().fereg_slope_precond(self.h, _p(r_, f64p), r_.shape[1], _p(z, f64p)))
+        return z
+
+    def slope_rhs(self, rows):
+        rows = np.ascontiguousarray(rows, dtype=np.float64)
+        r = rows.shape[1]
+        y = np.empty((self.m, r))
+        stats = np.empty((3, r))
+        _check(lib().fereg_slope_rhs(self.h, _p(rows, f64p), r, _p(y, f64p), _p(stats, f64p)))
+        return y, stats
 
     PHASES = ["rhs_seg", "rhs_pull", "apply_seg", "precond", "vector", "residualize", "h2d", "d2h", "apply_pull",
               "escalate"]
@@ -372,7 +456,10 @@ class Session:
     B200 absorber. codes / clusters: prepared kept-order codes; w: kept-order weights of
     weight_kind ("aweight", "fweight", "pweight") or None."""
 
-    def __init__(self, codes, g, clusters=(), cl_g=(), w=None, weight_kind=None, num_singletons=0):
+    def __init__(self, codes, g, clusters=(), cl_g=(), w=None, weight_kind=None, num_singletons=0, intercept=None,
+                 slopes=None):
+        """intercept / slopes: the terms' shapes as for Absorber (slope terms make the session's
+        absorber the slope solver and add one dof slot per slope)."""
         n = len(codes[0]) if len(codes) else len(clusters[0]) if len(clusters) else len(w)
         self._codes = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
         self._cl = [np.ascontiguousarray(c, dtype=np.uint32) for c in clusters]
@@ -382,9 +469,16 @@ class Session:
         clp = (u32p * max(1, len(self._cl)))(*[_p(c, u32p) for c in self._cl])
         wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
         h = P()
-        _check(lib().fereg_session_create(cp, _p(garr, u32p), len(self._codes), clp, _p(cgarr, u32p), len(self._cl),
-                                          _p(wa, f64p), WEIGHT_KIND[weight_kind if w is not None else None], n,
-                                          int(num_singletons), None, C.byref(h)))
+        wk = WEIGHT_KIND[weight_kind if w is not None else None]
+        if intercept is None and slopes is None:
+            _check(lib().fereg_session_create(cp, _p(garr, u32p), len(self._codes), clp, _p(cgarr, u32p),
+                                              len(self._cl), _p(wa, f64p), wk, n, int(num_singletons), None,
+                                              C.byref(h)))
+        else:
+            ia, na, sa, self._slopes, _ = _term_shapes(len(self._codes), intercept, slopes, n)
+            _check(lib().fereg_session_create_terms(cp, _p(garr, u32p), ia, na, sa, len(self._codes), clp,
+                                                    _p(cgarr, u32p), len(self._cl), _p(wa, f64p), wk, n,
+                                                    int(num_singletons), None, C.byref(h)))
         self.h = h
         self.n = n
 
@@ -524,6 +618,20 @@ class Session:
               on_device=False, nx=None, itol=1e-10):
         """Logit of column 0 (y in {0, 1}) on the other columns, as `poisson`."""
         return self.glm(rows, "logit", vce, tol, maxiter, inner_maxiter, precision, on_device, nx, itol)
+
+    def relu_separation(self, rows, itol=1e-10, inner_maxiter=16000):
+        """One ReLU separation check (glm/separation.rs:61) of the Poisson outcome in column 0
+        with the regressors in the other columns of the n x (1 + nx) host block (row order).
+        Returns the separated rows (bool, row order), the certificate, the ReLU and PCG
+        iterations and whether the check certified its result."""
+        assert rows.dtype == np.float64 and rows.flags.c_contiguous
+        sep = np.zeros(self.n, dtype=np.uint8)
+        cert = np.zeros(self.n)
+        o = np.zeros(4, dtype=np.uint64)
+        _check(lib().fereg_session_relu(self.h, P(rows.ctypes.data), 0, rows.shape[1] - 1, itol, inner_maxiter,
+                                        _p(sep, u8p), _p(cert, f64p), _p(o, u64p)))
+        return dict(separated=sep.astype(bool), certificate=cert, num_separated=int(o[0]), iterations=int(o[1]),
+                    pcg_iterations=int(o[2]), complete=bool(o[3]))
 
     def glm(self, rows, family, vce="robust", tol=1e-8, maxiter=10000, inner_maxiter=16000, precision=PREC_F64,
             on_device=False, nx=None, itol=1e-10):

@@ -16,9 +16,9 @@ LIB = os.path.join(HERE, "libfereg_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
+CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3,-fopenmp", "--expt-relaxed-constexpr",
                   "-ccbin", "/usr/bin/g++"]
-SOURCES = ["structure.cpp", "amg.cpp", "absorber.cu", "session.cu", "server.cu", "prep.cu", "dstruct.cu", "capi.cu"]
+SOURCES = ["structure.cpp", "amg.cpp", "absorber.cu", "session.cu", "server.cu", "prep.cu", "dstruct.cu", "slopes.cu", "capi.cu"]
 
 
 def _headers():

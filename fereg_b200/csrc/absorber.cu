@@ -20,6 +20,7 @@
 #include "amg.h"
 #include "dstruct.h"
 #include "pcg.cuh"
+#include "pcg_driver.h"
 #include "weights.cuh"
 
 namespace fereg {
@@ -88,6 +89,12 @@ struct DevWarpTiles {
 // the lane-private small-coordinate slots and column partials).
 inline size_t grhs_smem(u32 ms_acc) { return WPB * (size_t(ms_acc) * 64 * 8 + 4 * 32 * 8); }
 inline size_t wresid_smem(int Rc) { return WPB * wresid_bytes(Rc); }
+// Shared memory of k_wresid with the fused Gram: the tile parts and the chunk stages, at least
+// the final reduction.
+template <int RCP>
+size_t gram_wresid_smem(int Rc) {
+    return std::max(WPB * wresid_bytes(Rc) + WPB * GramShape<RCP>::stage_bytes, GramShape<RCP>::red_bytes);
+}
 inline size_t wpull_smem() { return WPB * pull_bytes(); }
 
 // Calls f(RCP, NBK) as integral constants: RCP the padded width of an Rc-column chunk, NBK the
@@ -195,6 +202,7 @@ struct Scratch {
     DBuf<int> wflag;
     // solve (FP64)
     DBuf<double> rows, rhs, b1, coefs, r, z, p, q, t, part, cta, cta2, colsum, along, small;
+    DBuf<double> gpart, gsum;  // the fused Gram: per-CTA partials, sums
     DBuf<double> rhsv, xv;  // the padded right-hand side and iterate of the PCG
     // inner FP32 buffers of the refined solve
     DBuf<float> fx, fb, fr, fz, fp, fq, ft, fpart, frhs, fx0, fsmall;
@@ -1341,9 +1349,10 @@ SolveInfo GpuAbsorber::residualize_device_warm_last(double* z_dev, size_t r, dou
 }
 
 SolveInfo GpuAbsorber::residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
-                                          const double* warm, double* coefs, Precision prec) {
+                                          const double* warm, double* coefs, Precision prec,
+                                          const GramRequest* gram) {
     AllocScope alloc_scope(stream_);
-    return solve(z_dev, r, tol, maxiter, want_coefs, warm, coefs, prec);
+    return solve(z_dev, r, tol, maxiter, want_coefs, warm, coefs, prec, false, gram);
 }
 
 constexpr int PROBE_FROM = 7, PROBE_AT = 12;
@@ -1352,57 +1361,80 @@ constexpr double PROBE_RATIO = 0.6;
 // Iterations a graph launch may run at most before the host looks at the loop state again.
 constexpr int GRAPH_CAP = 64;
 
+// The operator of a PCG run on the intercept-only structure: q = S p (launch_apply) and
+// z = M^-1 r (launch_precond), with the device addresses their launches touch.
+template <class T>
+struct FeOp {
+    Scratch& d;
+    const DevStruct& S;
+    const DevWeights& W;
+    bool small_ok;
+    T *t, *part, *small;
+    u32 m() const { return S.m; }
+    void apply(T* p, int R, T* q, cudaStream_t st) const { launch_apply<T>(d, S, W, p, R, q, t, part, small, st); }
+    void precond(T* r, T* z, int R, cudaStream_t st) const { launch_precond<T>(d, S, small_ok, r, z, R, st); }
+    void key(std::vector<u64>& k) const {
+        auto put = [&](const void* ptr) { k.push_back(u64(reinterpret_cast<uintptr_t>(ptr))); };
+        k.push_back(small_ok);
+        for (const void* ptr : {(const void*)t, (const void*)part, (const void*)small, (const void*)W.w_rows,
+                                (const void*)W.cell_w, (const void*)W.n1inv, (const void*)W.nr, (const void*)d.inv_diag.p,
+                                (const void*)d.minv.p, (const void*)d.srow.p})
+            put(ptr);
+        k.push_back(d.amg.size());
+        for (auto& A : d.amg) {
+            put(A.minv.p);
+            for (auto& b : A.iu) put(b.p);
+            for (auto& b : A.dv) put(b.p);
+            for (auto& b : amg_work<T>(A)) put(b.p);
+        }
+    }
+    void prepare(int R) const {
+        for (auto& A : d.amg) amg_alloc<T>(A, R);
+    }
+};
+
 // Every device address the iteration body reads or writes, with the body's shape: a captured
 // graph is reused only for an identical key.
-template <class T>
-std::vector<u64> body_key(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, const T* x,
-                          const T* rhs_true, const T* x0, const T* r, const T* z, const T* p, const T* q, const T* t,
-                          const T* part, const T* small, int R) {
+template <class T, class Op>
+std::vector<u64> body_key(Scratch& d, const Op& op, const T* x, const T* rhs_true, const T* x0, const T* r, const T* z,
+                          const T* p, const T* q, int R) {
     std::vector<u64> k;
     auto put = [&](const void* ptr) { k.push_back(u64(reinterpret_cast<uintptr_t>(ptr))); };
     k.push_back(sizeof(T));
     k.push_back(u64(R));
-    k.push_back(small_ok);
+    k.push_back(u64(op.m()));
     put(d.lp_tol.p);
     for (const void* ptr : {(const void*)x, (const void*)rhs_true, (const void*)x0, (const void*)r, (const void*)z,
-                            (const void*)p, (const void*)q, (const void*)t, (const void*)part, (const void*)small})
+                            (const void*)p, (const void*)q})
         put(ptr);
-    for (const void* ptr : {(const void*)W.w_rows, (const void*)W.cell_w, (const void*)W.n1inv, (const void*)W.nr,
-                            (const void*)d.inv_diag.p, (const void*)d.minv.p, (const void*)d.srow.p, (const void*)d.cta.p,
-                            (const void*)d.lp_ctl.p, (const void*)d.lp_ticket.p, (const void*)d.cg_rho.p,
-                            (const void*)d.cg_active.p, (const void*)d.cg_ring.p, (const void*)d.cg_xb.p,
-                            (const void*)d.cg_beta.p, (const void*)d.cg_gamma.p, (const void*)d.cg_pfloor.p,
-                            (const void*)d.cg_xconst.p, (const void*)d.cg_floor.p, (const void*)d.cg_ss1.p,
-                            (const void*)d.cg_pq.p, (const void*)d.cg_rho_new.p, (const void*)d.cg_nactive.p,
-                            (const void*)d.lp_rho_from.p, (const void*)d.lp_rho_at.p, (const void*)d.lp_act.p})
+    for (const void* ptr : {(const void*)d.cta.p, (const void*)d.lp_ctl.p, (const void*)d.lp_ticket.p,
+                            (const void*)d.cg_rho.p, (const void*)d.cg_active.p, (const void*)d.cg_ring.p,
+                            (const void*)d.cg_xb.p, (const void*)d.cg_beta.p, (const void*)d.cg_gamma.p,
+                            (const void*)d.cg_pfloor.p, (const void*)d.cg_xconst.p, (const void*)d.cg_floor.p,
+                            (const void*)d.cg_ss1.p, (const void*)d.cg_pq.p, (const void*)d.cg_rho_new.p,
+                            (const void*)d.cg_nactive.p, (const void*)d.lp_rho_from.p, (const void*)d.lp_rho_at.p,
+                            (const void*)d.lp_act.p})
         put(ptr);
-    k.push_back(d.amg.size());
-    for (auto& A : d.amg) {
-        put(A.minv.p);
-        for (auto& b : A.iu) put(b.p);
-        for (auto& b : A.dv) put(b.p);
-        for (auto& b : amg_work<T>(A)) put(b.p);
-    }
-    (void)S;
+    op.key(k);
     return k;
 }
 
 // The iteration body (cg.rs:207-290): q = S p, gamma, x and r (with the stopping rule's dot
 // products), z = M^-1 r, rho and the stopping rule, p. In a graph (use_cond) its last kernel sets
 // the WHILE condition.
-template <class T>
-void enqueue_iteration(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x, const T* rhs_true,
-                       const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small, int R, const CgState& cg,
-                       const CgLoop& lp, cudaGraphConditionalHandle cond, bool use_cond, cudaStream_t st) {
-    const u32 m = S.m;
+template <class T, class Op>
+void enqueue_iteration(Scratch& d, const Op& op, T* x, const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q, int R,
+                       const CgState& cg, const CgLoop& lp, cudaGraphConditionalHandle cond, bool use_cond,
+                       cudaStream_t st) {
+    const u32 m = op.m();
     const size_t tot = size_t(m) * R;
-    launch_apply<T>(d, S, W, p, R, q, t, part, small, st);
+    op.apply(p, R, q, st);
     int h = d.begin(GpuAbsorber::P_VECTOR, st);
     k_pq_gamma<T><<<GRID_V, THREADS, 0, st>>>(p, q, m, R, d.cta.p, cg, lp);
     k_update_xr_sum<T><<<GRID_V, THREADS, 0, st>>>(x, r, p, q, rhs_true, x0, m, R, d.cta.p, cg, lp);
     d.launches += 2;
     d.end(h, st);
-    launch_precond<T>(d, S, small_ok, r, z, R, st);
+    op.precond(r, z, R, st);
     h = d.begin(GpuAbsorber::P_VECTOR, st);
     k_rz_stop<T><<<GRID_V, THREADS, 0, st>>>(r, z, m, R, d.cta.p, cg, lp, PROBE_FROM, PROBE_AT);
     k_update_p_cond<T><<<grid_for(tot), THREADS, 0, st>>>(p, z, cg.beta, cg.active, m, R, lp, cond, use_cond ? 1 : 0);
@@ -1413,10 +1445,9 @@ void enqueue_iteration(Scratch& d, const DevStruct& S, const DevWeights& W, bool
 
 // The graph of one iteration body under a WHILE node, captured on `st` (the body kernels with
 // their current arguments).
-template <class T>
-Scratch::PcgGraph capture_iteration(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x,
-                                    const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small,
-                                    int R, const CgState& cg, const CgLoop& lp, cudaStream_t st,
+template <class T, class Op>
+Scratch::PcgGraph capture_iteration(Scratch& d, const Op& op, T* x, const T* rhs_true, const T* x0, T* r, T* z, T* p,
+                                    T* q, int R, const CgState& cg, const CgLoop& lp, cudaStream_t st,
                                     std::vector<u64> key) {
     const auto t0 = std::chrono::steady_clock::now();
     Scratch::PcgGraph gr;
@@ -1434,7 +1465,7 @@ Scratch::PcgGraph capture_iteration(Scratch& d, const DevStruct& S, const DevWei
     cudaGraph_t body = np.conditional.phGraph_out[0];
     const u64 launches0 = d.launches;
     CK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    enqueue_iteration<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part, small, R, cg, lp, cond, true, st);
+    enqueue_iteration<T>(d, op, x, rhs_true, x0, r, z, p, q, R, cg, lp, cond, true, st);
     CK(cudaStreamEndCapture(st, &body));
     gr.body_launches = d.launches - launches0;
     d.launches = launches0;  // counted when the graph runs
@@ -1458,12 +1489,11 @@ Scratch::PcgGraph capture_iteration(Scratch& d, const DevStruct& S, const DevWei
 // WHILE node repeats the body until every column stopped or the launch's cap is reached (the
 // host looks at the loop state only between launches: at the probe, at the cap, at the end);
 // with phase timing, one body at a time with the host reading the state after each.
-template <class T>
-static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool small_ok, T* x, const T* b,
-                   const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q, T* t, T* part, T* small, int R, double tol,
-                   double drop, u64 iters_done, size_t maxiter, bool x_is_start, const Ctx& ctx, cudaStream_t st,
-                   const std::function<bool(double)>& escalate) {
-    const size_t m = S.m, tot = m * size_t(R);
+template <class T, class Op>
+static u64 run_pcg(Scratch& d, const Op& op, T* x, const T* b, const T* rhs_true, const T* x0, T* r, T* z, T* p, T* q,
+                   int R, double tol, double drop, u64 iters_done, size_t maxiter, bool x_is_start, const Ctx& ctx,
+                   cudaStream_t st, const std::function<bool(double)>& escalate) {
+    const size_t m = op.m(), tot = m * size_t(R);
     CgState cg = d.cg();
     d.lp_ctl.alloc(4);
     d.lp_ticket.alloc(4);
@@ -1481,13 +1511,13 @@ static u64 run_pcg(Scratch& d, const DevStruct& S, const DevWeights& W, bool sma
     int* hc = d.h_nactive;  // pinned [n_active, k, k of the launch, cap]
 restart:
     if (x_is_start) {
-        launch_apply<T>(d, S, W, x, R, q, t, part, small, st);
+        op.apply(x, R, q, st);
         k_sub<T><<<grid_for(tot), THREADS, 0, st>>>(r, b, q, tot);
         d.launches++;
     } else {
         CK(cudaMemcpyAsync(r, b, tot * sizeof(T), cudaMemcpyDeviceToDevice, st));
     }
-    launch_precond<T>(d, S, small_ok, r, z, R, st);
+    op.precond(r, z, R, st);
     int h = d.begin(GpuAbsorber::P_VECTOR, st);
     k_dot<T><<<GRID_V, THREADS, 0, st>>>(r, z, u32(m), R, d.cta.p);
     reduce_cols(d, d.cta.p, GRID_V, R, d.cg_rho.p, st);
@@ -1519,25 +1549,22 @@ restart:
         CK(cudaMemcpyAsync(d.lp_ctl.p + 2, hc + 4, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
         const Scratch::PcgGraph* gr = nullptr;
         if (!d.prof) {
-            for (auto& A : d.amg) amg_alloc<T>(A, R);
-            std::vector<u64> key = body_key<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part, small, R);
+            op.prepare(R);
+            std::vector<u64> key = body_key<T>(d, op, x, rhs_true, x0, r, z, p, q, R);
             for (auto& q_ : d.graphs)
                 if (q_.key == key) gr = &q_;
             if (!gr) {
                 // a new body: this batch runs one iteration by launches (first uses of its kernels
                 // set their attributes), and the body is captured for the next batches
-                enqueue_iteration<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part, small, R, cg, lp, 0, false,
-                                     st);
+                enqueue_iteration<T>(d, op, x, rhs_true, x0, r, z, p, q, R, cg, lp, 0, false, st);
                 if (d.graphs.size() >= 8) d.drop_graphs();
-                d.graphs.push_back(capture_iteration<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part,
-                                                        small, R, cg, lp, st, std::move(key)));
+                d.graphs.push_back(capture_iteration<T>(d, op, x, rhs_true, x0, r, z, p, q, R, cg, lp, st, std::move(key)));
             } else {
                 CK(cudaGraphLaunch(gr->exec, st));
                 d.graph_launches++;
             }
         } else {
-            enqueue_iteration<T>(d, S, W, small_ok, x, rhs_true, x0, r, z, p, q, t, part, small, R, cg, lp, 0, false,
-                                 st);
+            enqueue_iteration<T>(d, op, x, rhs_true, x0, r, z, p, q, R, cg, lp, 0, false, st);
         }
         CK(cudaMemcpyAsync(hc, d.lp_ctl.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaGetLastError());
@@ -1569,7 +1596,7 @@ restart:
 
 // solve.rs:1141-1311 residualize.
 SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
-                             double* coefs, Precision prec, bool warm_last) {
+                             double* coefs, Precision prec, bool warm_last, const GramRequest* gram) {
     SolveInfo info;
     const size_t m = hs_.m, g1 = hs_.g1;
     if (r == 0) {
@@ -1671,6 +1698,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         CK(cudaMemsetAsync(d.cg_ring.p, 0, rv * WINDOW * 8, st));
         const bool exact_pre = small_ok_ && hs_.m_small == hs_.m;
         const std::function<bool(double)> esc = [this](double rho_hat) { return escalate(rho_hat); };
+        const FeOp<double> op64{d, S, W, small_ok_, d.t.p, d.part.p, d.small.p};
         if (exact_pre) {
             // x* = x + M^-1 (rhs - S x) (cg.rs:171-198)
             if (warm || have_last) {
@@ -1685,9 +1713,8 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             d.launches++;
             CK(cudaGetLastError());
         } else if (prec == Precision::F64) {
-            iterations = run_pcg<double>(d, S, W, small_ok_, x, d.rhsv.p, d.rhsv.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p,
-                                         d.t.p, d.part.p, d.small.p, RV, tol, 0.0, 0, maxiter,
-                                         warm != nullptr || have_last, ctx_, st, esc);
+            iterations = run_pcg<double>(d, op64, x, d.rhsv.p, d.rhsv.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p, RV, tol,
+                                         0.0, 0, maxiter, warm != nullptr || have_last, ctx_, st, esc);
             exact = false;
         } else {
             // FP32 inner PCG on the correction, FP64 true residual between rounds.
@@ -1719,9 +1746,9 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
                 CK(cudaMemsetAsync(d.fx.p, 0, tot * 4, st));
                 CK(cudaMemsetAsync(d.cg_ring.p, 0, rv * WINDOW * 8, st));
                 d.launches += 3;
-                iterations += run_pcg<float>(d, S, W, small_ok_, d.fx.p, d.fb.p, d.frhs.p, d.fx0.p, d.fr.p, d.fz.p,
-                                             d.fp.p, d.fq.p, d.ft.p, d.fpart.p, d.fsmall.p, RV, tol,
-                                             REFINE_DROP, iterations, maxiter, false, ctx_, st, esc);
+                const FeOp<float> op32{d, S, W, small_ok_, d.ft.p, d.fpart.p, d.fsmall.p};
+                iterations += run_pcg<float>(d, op32, d.fx.p, d.fb.p, d.frhs.p, d.fx0.p, d.fr.p, d.fz.p, d.fp.p, d.fq.p,
+                                             RV, tol, REFINE_DROP, iterations, maxiter, false, ctx_, st, esc);
                 k_add_correction<<<grid_for(tot), THREADS, 0, st>>>(x, d.fx.p, tot);
                 d.launches++;
                 // the round's check in FP64: true residual, its preconditioned norm and ss_k
@@ -1756,9 +1783,8 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
                 // reference's stopping rule on the full iterate (x0 = 0, x'rhs in the rule)
                 CK(cudaMemsetAsync(d.cg_xconst.p, 0, rv * 8, st));
                 CK(cudaMemsetAsync(d.cg_ring.p, 0, rv * WINDOW * 8, st));
-                iterations += run_pcg<double>(d, S, W, small_ok_, x, d.rhsv.p, d.rhsv.p, nullptr, d.r.p, d.z.p, d.p.p,
-                                              d.q.p, d.t.p, d.part.p, d.small.p, RV, tol, 0.0, iterations, maxiter, true,
-                                              ctx_, st, esc);
+                iterations += run_pcg<double>(d, op64, x, d.rhsv.p, d.rhsv.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p, RV,
+                                              tol, 0.0, iterations, maxiter, true, ctx_, st, esc);
                 d.fp64_finishes++;
             }
             iterations = std::max<u64>(iterations, 1);
@@ -1776,18 +1802,38 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     ctx_.check();
     int h = d.begin(P_RESID, st);
     double* alpha = want_coefs ? x + m * r : nullptr;
+    // the Gram in the same pass: every row in a short segment, every column in one launch
+    const bool fuse_gram = gram && gram->g && gram->ss && d.wseg.n && !S.seg.nfix && !S.seg.n && R <= 16;
+    const int glen = gram_len(R);
+    if (fuse_gram) {
+        d.gpart.alloc(size_t(GRID_S) * glen);
+        d.gsum.alloc(size_t(glen));
+    }
     if (d.wseg.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
-            const size_t shm = wresid_smem(Rc);
             with_rcp<0>(Rc, S.nb, [&](auto c, auto nbk) {
                 constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
-                allow_smem(k_wresid<RCP, NBK>, shm);
-                k_wresid<RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, x, d.b1.p,
-                                                                   alpha);
+                auto run = [&](auto kernel, size_t shm, GramFuse gf) {
+                    allow_smem(kernel, shm);
+                    kernel<<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, x, d.b1.p, alpha, gf);
+                };
+                if constexpr (RCP <= 16) {
+                    if (fuse_gram) {
+                        run(k_wresid<RCP, NBK, true>, gram_wresid_smem<RCP>(Rc), GramFuse{gram->w, d.gpart.p});
+                        return;
+                    }
+                }
+                run(k_wresid<RCP, NBK, false>, wresid_smem(Rc), GramFuse{nullptr, nullptr});
             });
             d.launches++;
         }
+    std::vector<double> gh(fuse_gram ? glen : 0);
+    if (fuse_gram) {
+        k_gram_sum<<<(glen + 7) / 8, 256, 0, st>>>(d.gpart.p, GRID_S, glen, d.gsum.p);
+        d.launches++;
+        CK(cudaMemcpyAsync(gh.data(), d.gsum.p, size_t(glen) * 8, cudaMemcpyDeviceToHost, st));
+    }
     if (S.seg.nfix) {
         d.along.alloc(size_t(S.seg.nfix) * r);
         k_seg_apply<double><<<GRID_T, THREADS, 0, st>>>(S, W, x, R, d.t.p, d.part.p, true, nullptr);
@@ -1802,6 +1848,11 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     CK(cudaGetLastError());
     if (want_coefs && coefs) CK(cudaMemcpyAsync(coefs, x, (m + g1) * r * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (fuse_gram) {
+        gram->g->assign(gh.begin(), gh.begin() + size_t(R) * R);
+        gram->ss->assign(gh.begin() + size_t(R) * R, gh.end());
+        info.gram = true;
+    }
     last_r_ = r;
     d.collect();
     info.iterations = iterations;
@@ -1849,6 +1900,12 @@ void GpuAbsorber::fit_rows(const double* coefs, size_t r, size_t col, double* ou
         }
 }
 
+size_t GpuAbsorber::term_values_len() const {
+    size_t t = 0;
+    for (u32 v : g_) t += v;
+    return t;
+}
+
 void GpuAbsorber::term_values(const double* coefs, size_t r, size_t col, double* out) const {
     AllocScope alloc_scope(stream_);
     sync_host_weights();
@@ -1882,6 +1939,73 @@ void GpuAbsorber::term_values(const double* coefs, size_t r, size_t col, double*
         std::copy(vals[t].begin(), vals[t].end(), out + o);
         o += g_[t];
     }
+}
+
+// The operator of a PcgDriver run, seen by the templated loop.
+struct VirtOp {
+    DevOperator& o;
+    u32 m() const { return o.m(); }
+    void apply(double* p, int R, double* q, cudaStream_t st) const { o.apply(p, R, q, st); }
+    void precond(double* r, double* z, int R, cudaStream_t st) const { o.precond(r, z, R, st); }
+    void key(std::vector<u64>& k) const { o.key(k); }
+    void prepare(int) const {}
+};
+
+PcgDriver::PcgDriver() : d_(std::make_unique<Scratch>()) {
+    CK(cudaHostAlloc(&d_->h_nactive, 8 * sizeof(int), cudaHostAllocDefault));
+}
+PcgDriver::~PcgDriver() = default;
+
+u64 PcgDriver::run(DevOperator& op, double* x, const double* b, int R, const std::vector<double>& ss0,
+                   const std::vector<double>& ss1, double tol, size_t maxiter, bool x_is_start, const Ctx& ctx,
+                   cudaStream_t st) {
+    Scratch& d = *d_;
+    const size_t m = op.m(), rv = size_t(R);
+    if (R % 4 != 0 || ss0.size() != rv || ss1.size() != rv) throw Error(RC_INTERNAL, "fereg: PCG driver shapes");
+    if (m == 0) return 0;
+    const size_t tot = m * rv;
+    d.r.alloc(tot);
+    d.z.alloc(tot);
+    d.p.alloc(tot);
+    d.q.alloc(tot);
+    d.cta.alloc(size_t(std::max(GRID_T, GRID_V)) * 3 * rv);
+    for (auto* buf : {&d.cg_rho, &d.cg_rho_new, &d.cg_pq, &d.cg_gamma, &d.cg_beta, &d.cg_ss1, &d.cg_floor, &d.cg_xconst,
+                      &d.cg_pfloor})
+        buf->alloc(rv);
+    d.cg_xb.alloc(3 * rv);
+    d.cg_ring.alloc(rv * WINDOW);
+    d.cg_active.alloc(rv);
+    d.cg_nactive.alloc(1);
+    std::vector<int> act(rv);
+    std::vector<double> fl(rv);
+    for (size_t j = 0; j < rv; j++) {
+        act[j] = ss0[j] > 0.0;
+        fl[j] = 1e-26 * ss0[j];
+    }
+    CK(cudaMemcpyAsync(d.cg_active.p, act.data(), rv * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d.cg_ss1.p, ss1.data(), rv * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d.cg_floor.p, fl.data(), rv * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(d.cg_xconst.p, 0, rv * 8, st));
+    CK(cudaMemsetAsync(d.cg_pfloor.p, 0, rv * 8, st));
+    CK(cudaMemsetAsync(d.cg_ring.p, 0, rv * WINDOW * 8, st));
+    const VirtOp vo{op};
+    const u64 it = run_pcg<double>(d, vo, x, b, b, nullptr, d.r.p, d.z.p, d.p.p, d.q.p, R, tol, 0.0, 0, maxiter,
+                                   x_is_start, ctx, st, std::function<bool(double)>());
+    CK(cudaStreamSynchronize(st));  // the host vectors above stay alive until the copies ran
+    return it;
+}
+
+void PcgDriver::col_sums(const double* part, int nparts, int ncols, double* out, cudaStream_t st) {
+    reduce_cols(*d_, part, nparts, ncols, out, st);
+}
+
+u64 PcgDriver::launches() const { return d_->launches; }
+
+void PcgDriver::stats(u64* o) const {
+    o[0] = d_->graph_captures;
+    o[1] = d_->graph_launches;
+    o[2] = u64(d_->graph_build_us);
+    o[3] = 0;
 }
 
 }  // namespace fereg

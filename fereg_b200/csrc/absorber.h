@@ -36,6 +36,18 @@ struct SolveInfo {
     u64 iterations = 0;
     bool escalated = false;
     bool exact = false;
+    bool gram = false;  // the residualization also summed the Gram (GramRequest)
+};
+
+// The weighted Gram of the residualized block (stats.rs:195) asked of residualize_device: when
+// the residualization runs as one pass of the short-segment kernel over all columns, that pass
+// also sums it, with row weights `w` (device memory, row order; null: 1), into `g` (R x R
+// row-major) and the plain sums of squares of the columns into `ss`. SolveInfo::gram says whether
+// it did.
+struct GramRequest {
+    const double* w = nullptr;
+    std::vector<double>* g = nullptr;
+    std::vector<double>* ss = nullptr;
 };
 
 // Precision of the inner PCG: FP64 throughout, or FP32 iterations inside FP64 refinement.
@@ -43,48 +55,86 @@ enum class Precision : int { F64 = 0, F32_REFINED = 1 };
 
 struct Scratch;
 
-class GpuAbsorber {
+// The device absorber behind a session and the C ABI (the reference's `Absorber` trait,
+// absorber.rs:62-97): the intercept-only solver (GpuAbsorber, solve.rs FeSolver) or the
+// heterogeneous-slope solver (GpuSlopeSolver, slopes.rs SlopeSolver), chosen as solve.rs:338
+// `build` chooses. Rows are in the absorber's row order; coefficient blocks are
+// coefs_len() x R row-major.
+class DeviceAbsorber {
+   public:
+    virtual ~DeviceAbsorber() = default;
+    virtual size_t n() const = 0;
+    virtual size_t coefs_len() const = 0;
+    // Values term_values writes: sum over terms of levels x (intercept + slopes).
+    virtual size_t term_values_len() const = 0;
+    virtual const std::vector<u32>& row_order() const = 0;
+    virtual bool weights(double* out) const = 0;
+    virtual void set_weights(const double* w_rows) = 0;
+    virtual void set_weights_device(const double* w_rows_dev) = 0;
+    virtual SolveInfo residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
+                                  double* coefs, Precision prec = Precision::F64) = 0;
+    virtual SolveInfo residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
+                                         const double* warm, double* coefs, Precision prec = Precision::F64,
+                                         const GramRequest* gram = nullptr) = 0;
+    virtual SolveInfo residualize_device_warm_last(double* z_dev, size_t r, double tol, size_t maxiter,
+                                                   Precision prec = Precision::F64) = 0;
+    virtual void fit_rows(const double* coefs, size_t r, size_t col, double* out) const = 0;
+    virtual void term_values(const double* coefs, size_t r, size_t col, double* out) const = 0;
+    virtual cudaStream_t stream() const = 0;
+    virtual void set_profiling(bool on) = 0;
+    virtual void phase_times(double* ms, u64* counts) const = 0;
+    virtual u64 launches() const = 0;
+    virtual void solver_stats(u64* out4) const = 0;
+    virtual const Ctx& ctx() const = 0;
+    virtual void set_ctx(const Ctx& c) = 0;
+    virtual size_t escalated_blocks() const { return 0; }
+    virtual u64 escalations() const { return 0; }
+};
+
+class GpuAbsorber : public DeviceAbsorber {
    public:
     // `codes[q]` are the kept-order codes of term q (< g[q]); `w` kept-order weights or null.
     // The cell structure is built on the device; `dev_codes`, when given, are device copies of
     // `codes` (the caller's session keeps them), otherwise the codes are uploaded for the build.
     GpuAbsorber(const std::vector<const u32*>& codes, const std::vector<u32>& g, const double* w, size_t n, const Ctx& ctx,
                 const std::vector<const u32*>* dev_codes = nullptr);
-    ~GpuAbsorber();
+    ~GpuAbsorber() override;
 
-    size_t n() const { return hs_.n; }
+    size_t n() const override { return hs_.n; }
     size_t m() const { return hs_.m; }
     size_t g1() const { return hs_.g1; }
-    size_t coefs_len() const { return hs_.m + hs_.g1; }
-    const std::vector<u32>& row_order() const { return hs_.pi; }
+    size_t coefs_len() const override { return hs_.m + hs_.g1; }
+    size_t term_values_len() const override;
+    const std::vector<u32>& row_order() const override { return hs_.pi; }
     const HostStructure& structure() const { return hs_; }
     // Row-order weights (false: all ones).
-    bool weights(double* out) const;
+    bool weights(double* out) const override;
     // Row-order weights (null = ones), strictly positive and finite (solve.rs:1010-1139).
-    void set_weights(const double* w_rows);
+    void set_weights(const double* w_rows) override;
     // The same for row-order weights in device memory; the weight state is computed on the
     // device (the host mirrors follow when a host-side reader needs them).
-    void set_weights_device(const double* w_rows_dev);
+    void set_weights_device(const double* w_rows_dev) override;
 
     // Residualizes the N x R row-major block `z` in place (rows in row order). `z` is host
     // memory for `residualize`, device memory for `residualize_device`. `warm` and `coefs` are
     // (m + g1) x R row-major host buffers ([x; alpha1], solve.rs:7-9) or null.
     SolveInfo residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
-                          double* coefs, Precision prec = Precision::F64);
+                          double* coefs, Precision prec = Precision::F64) override;
     SolveInfo residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
-                                 const double* warm, double* coefs, Precision prec = Precision::F64);
+                                 const double* warm, double* coefs, Precision prec = Precision::F64,
+                                 const GramRequest* gram = nullptr) override;
     // The same, warm-started from the reduced solution the previous solve left on the device
     // (the IRLS warm start without the host round trip); the previous solve must have had the
     // same column count.
     SolveInfo residualize_device_warm_last(double* z_dev, size_t r, double tol, size_t maxiter,
-                                           Precision prec = Precision::F64);
+                                           Precision prec = Precision::F64) override;
 
     // FE fit of coefficient column `col` per row (row order) (absorber.rs:88).
-    void fit_rows(const double* coefs, size_t r, size_t col, double* out) const;
+    void fit_rows(const double* coefs, size_t r, size_t col, double* out) const override;
     // Values per session term, normalized as solve.rs:1319-1343; `out` holds sum_q g_q values.
-    void term_values(const double* coefs, size_t r, size_t col, double* out) const;
+    void term_values(const double* coefs, size_t r, size_t col, double* out) const override;
 
-    cudaStream_t stream() const { return stream_; }
+    cudaStream_t stream() const override { return stream_; }
 
     // Phase timing with CUDA events on the solver's stream (the reference's PhaseTimer,
     // timing.rs): per-slot milliseconds and launch counts, accumulated while enabled.
@@ -102,16 +152,16 @@ class GpuAbsorber {
         P_ESCALATE,
         P_NSLOTS
     };
-    void set_profiling(bool on);
-    void phase_times(double* ms, u64* counts) const;
-    u64 launches() const;
+    void set_profiling(bool on) override;
+    void phase_times(double* ms, u64* counts) const override;
+    u64 launches() const override;
     // [graphs captured, graph launches, host us of the captures, FP32-refined solves finished in FP64]
-    void solver_stats(u64* out4) const;
+    void solver_stats(u64* out4) const override;
     // Large blocks currently preconditioned by a multigrid V-cycle, and the escalations so far.
-    size_t escalated_blocks() const;
-    u64 escalations() const;
-    void set_ctx(const Ctx& c) { ctx_ = c; }
-    const Ctx& ctx() const { return ctx_; }
+    size_t escalated_blocks() const override;
+    u64 escalations() const override;
+    void set_ctx(const Ctx& c) override { ctx_ = c; }
+    const Ctx& ctx() const override { return ctx_; }
 
     // Kernel-level entry points for the parity tests (device work, host buffers).
     void apply_host(const double* p, size_t r, double* y);
@@ -161,7 +211,7 @@ class GpuAbsorber {
     void ensure_host_coord() const;
     void ensure_precond();
     SolveInfo solve(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
-                    double* coefs, Precision prec, bool warm_last = false);
+                    double* coefs, Precision prec, bool warm_last = false, const GramRequest* gram = nullptr);
     size_t last_r_ = 0;        // column count of the solution left in the solve scratch
     bool small_stale_ = false;  // the dense small factor was built for earlier weights
 };

@@ -11,14 +11,31 @@
 #include "prep.h"
 #include "server.h"
 #include "session.h"
+#include "slopes.h"
 
 using namespace fereg;
 
 struct fereg_absorber {
-    GpuAbsorber a;
-    template <class... A>
-    explicit fereg_absorber(A&&... args) : a(std::forward<A>(args)...) {}
+    std::unique_ptr<DeviceAbsorber> a;
+    GpuAbsorber* fe = nullptr;     // the intercept-only solver, when it is the absorber
+    GpuSlopeSolver* sl = nullptr;  // the heterogeneous-slope solver, when it is
+    explicit fereg_absorber(std::unique_ptr<GpuAbsorber> f) : fe(f.get()) { a = std::move(f); }
+    explicit fereg_absorber(std::unique_ptr<GpuSlopeSolver> f) : sl(f.get()) { a = std::move(f); }
 };
+
+namespace {
+// The absorber of a handle as the intercept-only solver or as the slope solver (198 otherwise).
+fereg::GpuAbsorber& fe_of(const fereg_absorber* h, const char* what) {
+    if (!h) throw fereg::Error(fereg::RC_INVALID_INPUT, std::string(what) + ": NULL handle");
+    if (!h->fe) throw fereg::Error(fereg::RC_INVALID_INPUT, std::string(what) + ": the absorber has slope terms");
+    return *h->fe;
+}
+fereg::GpuSlopeSolver& sl_of(const fereg_absorber* h, const char* what) {
+    if (!h) throw fereg::Error(fereg::RC_INVALID_INPUT, std::string(what) + ": NULL handle");
+    if (!h->sl) throw fereg::Error(fereg::RC_INVALID_INPUT, std::string(what) + ": the absorber has no slope terms");
+    return *h->sl;
+}
+}  // namespace
 
 struct fereg_session {
     GpuSession s;
@@ -85,7 +102,26 @@ double* rhs_scratch_on_current_device() {
 }
 
 // fereg_absorber_info: n, m, g1, ncells, nb, m_small, fe1, small_work, small blocks.
-void fill_info(const GpuAbsorber& a, uint64_t* o) {
+// The terms of a *_create_terms call: intercept[q] (null: 1), nslopes[q] (null: 0) and the slope
+// variables of all terms, term after term (sum nslopes pointers).
+std::vector<SlopeTermIn> slope_terms(const uint32_t* const* codes, const uint32_t* g, const int* intercept,
+                                     const int* nslopes, const double* const* slopes, int nterms) {
+    std::vector<SlopeTermIn> t(static_cast<size_t>(nterms));
+    size_t k = 0;
+    for (int q = 0; q < nterms; q++) {
+        SlopeTermIn& x = t[size_t(q)];
+        x.codes = codes[q];
+        x.g = g[q];
+        x.intercept = intercept ? intercept[q] != 0 : true;
+        const int ns = nslopes ? nslopes[q] : 0;
+        if (ns < 0 || (ns > 0 && !slopes)) throw Error(RC_INVALID_INPUT, "fereg: bad slope variables");
+        for (int s = 0; s < ns; s++) x.slopes.push_back(slopes[k++]);
+        if (!x.codes || x.g == 0) throw Error(RC_INVALID_INPUT, "fereg: empty term");
+    }
+    return t;
+}
+
+void fill_info_fe(const GpuAbsorber& a, uint64_t* o) {
     const auto& st = a.structure();
     o[0] = st.n;
     o[1] = st.m;
@@ -98,6 +134,22 @@ void fill_info(const GpuAbsorber& a, uint64_t* o) {
     u64 ns = 0;
     for (const auto& b : st.blocks) ns += b.small ? 1 : 0;
     o[8] = ns;
+}
+
+// The same for either absorber; the slope solver reports n, m, G_E, n (every row its own cell),
+// the blocks, the small coordinates, E, 0 and the small blocks.
+void fill_info(const DeviceAbsorber& a, uint64_t* o) {
+    if (const auto* fe = dynamic_cast<const GpuAbsorber*>(&a)) return fill_info_fe(*fe, o);
+    const auto& st = dynamic_cast<const GpuSlopeSolver&>(a).structure();
+    o[0] = st.n;
+    o[1] = st.m;
+    o[2] = st.ge;
+    o[3] = st.n;
+    o[4] = st.blocks.size();
+    o[5] = st.m_small;
+    o[6] = st.e;
+    o[7] = 0;
+    o[8] = st.nsmall;
 }
 
 void fill(fereg_solve_info* info, const SolveInfo& s) {
@@ -125,20 +177,81 @@ int fereg_absorber_create(const uint32_t* const* codes, const uint32_t* g, int n
         std::vector<u32> gs(g, g + nterms);
         for (int q = 0; q < nterms; q++)
             if (!cs[size_t(q)] || gs[size_t(q)] == 0) throw Error(RC_INVALID_INPUT, "fereg_absorber_create: empty term");
-        *out = new fereg_absorber(cs, gs, w, n, to_ctx(ctx));
+        *out = new fereg_absorber(std::make_unique<GpuAbsorber>(cs, gs, w, n, to_ctx(ctx)));
+    });
+}
+
+int fereg_absorber_create_terms(const uint32_t* const* codes, const uint32_t* g, const int* intercept,
+                                const int* nslopes, const double* const* slopes, int nterms, const double* w, size_t n,
+                                const fereg_ctx* ctx, fereg_absorber** out) {
+    return guard([&] {
+        if (!out) throw Error(RC_INVALID_INPUT, "fereg_absorber_create_terms: out is NULL");
+        *out = nullptr;
+        if (nterms <= 0 || !codes || !g) throw Error(RC_INVALID_INPUT, "fereg_absorber_create_terms: bad terms");
+        if (n < 2) throw Error(RC_TOO_FEW_OBS, "insufficient observations");
+        if (n >= (size_t(1) << 32)) throw Error(RC_INVALID_INPUT, "more than 2^32 - 1 rows");
+        const std::vector<SlopeTermIn> terms = slope_terms(codes, g, intercept, nslopes, slopes, nterms);
+        bool plain = true;
+        for (const auto& t : terms) plain &= t.intercept && t.slopes.empty();
+        if (plain) {
+            std::vector<const u32*> cs(codes, codes + nterms);
+            std::vector<u32> gs(g, g + nterms);
+            *out = new fereg_absorber(std::make_unique<GpuAbsorber>(cs, gs, w, n, to_ctx(ctx)));
+        } else {
+            *out = new fereg_absorber(std::make_unique<GpuSlopeSolver>(terms, w, n, to_ctx(ctx)));
+        }
+    });
+}
+
+int fereg_absorber_has_slopes(const fereg_absorber* h) { return h && h->sl ? 1 : 0; }
+
+size_t fereg_absorber_term_values_len(const fereg_absorber* h) { return h ? h->a->term_values_len() : 0; }
+
+int fereg_slope_weight_state(const fereg_absorber* h, double* minv, double* jinv, uint8_t* redundant) {
+    return guard([&] { sl_of(h, "fereg_slope_weight_state").weight_state(minv, jinv, redundant); });
+}
+
+int fereg_slope_apply(fereg_absorber* h, const double* p, size_t r, double* y) {
+    return guard([&] { sl_of(h, "fereg_slope_apply").apply_host(p, r, y); });
+}
+
+int fereg_slope_precond(fereg_absorber* h, const double* rr, size_t r, double* z) {
+    return guard([&] { sl_of(h, "fereg_slope_precond").precond_host(rr, r, z); });
+}
+
+int fereg_slope_rhs(fereg_absorber* h, const double* rows, size_t r, double* y, double* stats) {
+    return guard([&] { sl_of(h, "fereg_slope_rhs").rhs_host(rows, r, y, stats); });
+}
+
+int fereg_slope_structure(const fereg_absorber* h, uint64_t* o, uint32_t* block_terms) {
+    return guard([&] {
+        const SlopeHost& st = sl_of(h, "fereg_slope_structure").structure();
+        if (o) {
+            o[0] = st.n;
+            o[1] = st.m;
+            o[2] = st.e;
+            o[3] = st.ge;
+            o[4] = st.be;
+            o[5] = st.k;
+            o[6] = st.blocks.size();
+            o[7] = st.nsmall;
+            o[8] = st.m_small;
+        }
+        if (block_terms)
+            for (size_t q = 0; q < st.blocks.size(); q++) block_terms[q] = uint32_t(st.blocks[q].term);
     });
 }
 
 void fereg_absorber_destroy(fereg_absorber* h) { delete h; }
 
-size_t fereg_absorber_n(const fereg_absorber* h) { return h ? h->a.n() : 0; }
+size_t fereg_absorber_n(const fereg_absorber* h) { return h ? h->a->n() : 0; }
 
-size_t fereg_absorber_coefs_len(const fereg_absorber* h) { return h ? h->a.coefs_len() : 0; }
+size_t fereg_absorber_coefs_len(const fereg_absorber* h) { return h ? h->a->coefs_len() : 0; }
 
 int fereg_absorber_row_order(const fereg_absorber* h, uint32_t* out) {
     return guard([&] {
         if (!h || !out) throw Error(RC_INVALID_INPUT, "fereg_absorber_row_order: NULL argument");
-        const auto& pi = h->a.row_order();
+        const auto& pi = h->a->row_order();
         std::copy(pi.begin(), pi.end(), out);
     });
 }
@@ -146,21 +259,21 @@ int fereg_absorber_row_order(const fereg_absorber* h, uint32_t* out) {
 int fereg_absorber_weights(const fereg_absorber* h, double* out, int* has) {
     return guard([&] {
         if (!h || !has) throw Error(RC_INVALID_INPUT, "fereg_absorber_weights: NULL argument");
-        *has = h->a.weights(out) ? 1 : 0;
+        *has = h->a->weights(out) ? 1 : 0;
     });
 }
 
 int fereg_absorber_set_weights(fereg_absorber* h, const double* w) {
     return guard([&] {
         if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_set_weights: NULL handle");
-        h->a.set_weights(w);
+        h->a->set_weights(w);
     });
 }
 
 int fereg_absorber_set_weights_device(fereg_absorber* h, const double* w_dev) {
     return guard([&] {
         if (!h || !w_dev) throw Error(RC_INVALID_INPUT, "fereg_absorber_set_weights_device: NULL argument");
-        h->a.set_weights_device(w_dev);
+        h->a->set_weights_device(w_dev);
     });
 }
 
@@ -179,8 +292,8 @@ int fereg_absorber_residualize_ex(fereg_absorber* h, double* z, int z_on_device,
         if (precision != FEREG_PREC_F64 && precision != FEREG_PREC_F32_REFINED)
             throw Error(RC_INVALID_INPUT, "residualize: unknown precision");
         const Precision p = Precision(precision);
-        SolveInfo s = z_on_device ? h->a.residualize_device(z, r, tol, maxiter, want_coefs != 0, warm, coefs_out, p)
-                                  : h->a.residualize(z, r, tol, maxiter, want_coefs != 0, warm, coefs_out, p);
+        SolveInfo s = z_on_device ? h->a->residualize_device(z, r, tol, maxiter, want_coefs != 0, warm, coefs_out, p)
+                                  : h->a->residualize(z, r, tol, maxiter, want_coefs != 0, warm, coefs_out, p);
         fill(info, s);
     });
 }
@@ -189,7 +302,7 @@ int fereg_absorber_fit_rows(const fereg_absorber* h, const double* coefs, size_t
     return guard([&] {
         if (!h || !coefs || !out) throw Error(RC_INVALID_INPUT, "fereg_absorber_fit_rows: NULL argument");
         if (col >= r) throw Error(RC_INVALID_INPUT, "fit_rows: column out of range");
-        h->a.fit_rows(coefs, r, col, out);
+        h->a->fit_rows(coefs, r, col, out);
     });
 }
 
@@ -197,40 +310,40 @@ int fereg_absorber_term_values(const fereg_absorber* h, const double* coefs, siz
     return guard([&] {
         if (!h || !coefs || !out) throw Error(RC_INVALID_INPUT, "fereg_absorber_term_values: NULL argument");
         if (col >= r) throw Error(RC_INVALID_INPUT, "term_values: column out of range");
-        h->a.term_values(coefs, r, col, out);
+        h->a->term_values(coefs, r, col, out);
     });
 }
 
-void* fereg_absorber_stream(const fereg_absorber* h) { return h ? static_cast<void*>(h->a.stream()) : nullptr; }
+void* fereg_absorber_stream(const fereg_absorber* h) { return h ? static_cast<void*>(h->a->stream()) : nullptr; }
 
 int fereg_absorber_set_profiling(fereg_absorber* h, int on) {
     return guard([&] {
         if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_set_profiling: NULL handle");
-        h->a.set_profiling(on != 0);
+        h->a->set_profiling(on != 0);
     });
 }
 
 int fereg_absorber_phase_times(const fereg_absorber* h, double* ms, uint64_t* counts) {
     return guard([&] {
         if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_phase_times: NULL handle");
-        h->a.phase_times(ms, counts);
+        h->a->phase_times(ms, counts);
     });
 }
 
-uint64_t fereg_absorber_launches(const fereg_absorber* h) { return h ? h->a.launches() : 0; }
+uint64_t fereg_absorber_launches(const fereg_absorber* h) { return h ? h->a->launches() : 0; }
 
 int fereg_absorber_escalations(const fereg_absorber* h, uint64_t* escalations, uint64_t* blocks) {
     return guard([&] {
         if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_escalations: NULL handle");
-        if (escalations) *escalations = h->a.escalations();
-        if (blocks) *blocks = h->a.escalated_blocks();
+        if (escalations) *escalations = h->a->escalations();
+        if (blocks) *blocks = h->a->escalated_blocks();
     });
 }
 
 int fereg_absorber_info(const fereg_absorber* h, uint64_t* o) {
     return guard([&] {
         if (!h || !o) throw Error(RC_INVALID_INPUT, "fereg_absorber_info: NULL argument");
-        fill_info(h->a, o);
+        fill_info(*h->a, o);
     });
 }
 
@@ -244,7 +357,7 @@ int fereg_session_info(const fereg_session* s, uint64_t* o) {
 int fereg_absorber_solver_stats(const fereg_absorber* h, uint64_t* o) {
     return guard([&] {
         if (!h || !o) throw Error(RC_INVALID_INPUT, "fereg_absorber_solver_stats: NULL argument");
-        h->a.solver_stats(o);
+        h->a->solver_stats(o);
     });
 }
 
@@ -256,11 +369,11 @@ int fereg_session_solver_stats(const fereg_session* s, uint64_t* o) {
 }
 
 int fereg_absorber_apply(fereg_absorber* h, const double* p, size_t r, double* y) {
-    return guard([&] { h->a.apply_host(p, r, y); });
+    return guard([&] { fe_of(h, "fereg_absorber_apply").apply_host(p, r, y); });
 }
 
 int fereg_absorber_rhs(fereg_absorber* h, const double* rows, size_t r, double* y, double* b1, double* wsq, double* wsum) {
-    return guard([&] { h->a.rhs_host(rows, r, y, b1, wsq, wsum); });
+    return guard([&] { fe_of(h, "fereg_absorber_rhs").rhs_host(rows, r, y, b1, wsq, wsum); });
 }
 
 int fereg_absorber_rhs_noalloc(fereg_absorber* h, const double* rows, size_t r, double* y, double* b1,
@@ -268,16 +381,16 @@ int fereg_absorber_rhs_noalloc(fereg_absorber* h, const double* rows, size_t r, 
     return guard([&] {
         if (!h) throw Error(RC_INVALID_INPUT, "fereg_absorber_rhs_noalloc: NULL handle");
         double* scratch = rhs_scratch_on_current_device();
-        h->a.rhs_device_scratch(rows, r, y, b1, colsum, scratch, NOALLOC_SCRATCH_BYTES / sizeof(double));
+        fe_of(h, "fereg_absorber_rhs_noalloc").rhs_device_scratch(rows, r, y, b1, colsum, scratch, NOALLOC_SCRATCH_BYTES / sizeof(double));
     });
 }
 
 int fereg_absorber_precond(fereg_absorber* h, const double* rr, size_t r, double* z) {
-    return guard([&] { h->a.precond_host(rr, r, z); });
+    return guard([&] { fe_of(h, "fereg_absorber_precond").precond_host(rr, r, z); });
 }
 
 int fereg_absorber_weight_state(const fereg_absorber* h, double* n1, double* nr, double* diag, uint8_t* redundant, double* sw) {
-    return guard([&] { h->a.weight_state(n1, nr, diag, redundant, sw); });
+    return guard([&] { fe_of(h, "fereg_absorber_weight_state").weight_state(n1, nr, diag, redundant, sw); });
 }
 
 
@@ -298,6 +411,32 @@ int fereg_session_create(const uint32_t* const* codes, const uint32_t* g, int nt
         for (int c = 0; c < ncl; c++)
             if (!cc[size_t(c)] || cgs[size_t(c)] == 0) throw Error(RC_INVALID_INPUT, "fereg_session_create: empty cluster");
         *out = new fereg_session(cs, gs, cc, cgs, w, weight_kind, n, num_singletons, to_ctx(ctx));
+    });
+}
+
+int fereg_session_create_terms(const uint32_t* const* codes, const uint32_t* g, const int* intercept,
+                               const int* nslopes, const double* const* slopes, int nterms,
+                               const uint32_t* const* cl_codes, const uint32_t* cl_g, int ncl, const double* w,
+                               int weight_kind, size_t n, uint64_t num_singletons, const fereg_ctx* ctx,
+                               fereg_session** out) {
+    return guard([&] {
+        if (!out) throw Error(RC_INVALID_INPUT, "fereg_session_create_terms: out is NULL");
+        *out = nullptr;
+        if (nterms <= 0 || ncl < 0 || !codes || !g || (ncl > 0 && (!cl_codes || !cl_g)))
+            throw Error(RC_INVALID_INPUT, "fereg_session_create_terms: bad terms or clusters");
+        if (n < 2) throw Error(RC_TOO_FEW_OBS, "insufficient observations");
+        if (n >= (size_t(1) << 31)) throw Error(RC_INVALID_INPUT, "more than 2^31 - 1 rows");
+        const std::vector<SlopeTermIn> terms = slope_terms(codes, g, intercept, nslopes, slopes, nterms);
+        std::vector<const u32*> cs(codes, codes + nterms), cc(cl_codes, cl_codes + ncl);
+        std::vector<u32> gs(g, g + nterms), cgs(cl_g, cl_g + ncl);
+        for (int c = 0; c < ncl; c++)
+            if (!cc[size_t(c)] || cgs[size_t(c)] == 0) throw Error(RC_INVALID_INPUT, "fereg_session_create: empty cluster");
+        std::vector<TermShape> shapes(terms.size());
+        for (size_t q = 0; q < terms.size(); q++) {
+            shapes[q].intercept = terms[q].intercept;
+            shapes[q].slopes = terms[q].slopes;
+        }
+        *out = new fereg_session(cs, gs, cc, cgs, w, weight_kind, n, num_singletons, to_ctx(ctx), &shapes);
     });
 }
 
@@ -471,6 +610,26 @@ static int session_glm(fereg_session* s, double* rows, int rows_on_device, size_
         out->iterations = go.iterations;
         out->pcg_iterations = go.pcg_iterations;
         out->converged = go.converged ? 1 : 0;
+    });
+}
+
+int fereg_session_relu(fereg_session* s, double* rows, int rows_on_device, size_t nx, double itol,
+                       size_t inner_maxiter, uint8_t* separated, double* certificate, uint64_t* out4) {
+    return guard([&] {
+        if (!s || !rows) throw Error(RC_INVALID_INPUT, "fereg_session_relu: NULL argument");
+        GpuSession::ReluSpec rs;
+        rs.itol = itol;
+        rs.inner_maxiter = inner_maxiter;
+        GpuSession::ReluOut o;
+        o.separated = separated;
+        o.certificate = certificate;
+        s->s.relu_separation(rows, rows_on_device != 0, nx, rs, o);
+        if (out4) {
+            out4[0] = o.num_separated;
+            out4[1] = o.iterations;
+            out4[2] = o.pcg_iterations;
+            out4[3] = o.complete ? 1 : 0;
+        }
     });
 }
 

@@ -17,8 +17,10 @@
 
 #include "linalg.h"
 #include "session.h"
+#include "slopes.h"
 #include "boot.cuh"
 #include "glm.cuh"
+#include "relu.cuh"
 #include "session_dev.h"
 #include "stats.cuh"
 
@@ -57,10 +59,38 @@ void combine_codes(const std::vector<const std::vector<u32>*>& dims, const std::
 
 }  // namespace
 
+namespace {
+
+// dof.rs:255-272 redundant_slope_levels: the variable scaled by its standard deviation
+// (stats.rs:187 stdev, at least 1e-3); a level is redundant when max - min <= 1e-6 (term with
+// intercept) or |min| + |max| <= 1e-6 (term without).
+u64 redundant_slope_levels(const u32* codes, u32 g, const double* x, size_t n, bool intercept) {
+    double mean = 0.0;
+    for (size_t i = 0; i < n; i++) mean += x[i];
+    mean /= double(n);
+    double m2 = 0.0;
+    for (size_t i = 0; i < n; i++) m2 += (x[i] - mean) * (x[i] - mean);
+    const double sd = std::max(std::sqrt(m2 / (double(n) - 1.0)), 1e-3);
+    std::vector<double> lo(g, INFINITY), hi(g, -INFINITY);
+    for (size_t i = 0; i < n; i++) {
+        const double v = x[i] / sd;
+        lo[codes[i]] = std::min(lo[codes[i]], v);
+        hi[codes[i]] = std::max(hi[codes[i]], v);
+    }
+    u64 cnt = 0;
+    for (u32 l = 0; l < g; l++)
+        cnt += intercept ? (hi[l] - lo[l] <= 1e-6) : (std::fabs(lo[l]) + std::fabs(hi[l]) <= 1e-6);
+    return cnt;
+}
+
+}  // namespace
+
 GpuSession::GpuSession(const std::vector<const u32*>& codes, const std::vector<u32>& g,
                        const std::vector<const u32*>& cl_codes, const std::vector<u32>& cl_g, const double* w,
-                       int weight_kind, size_t n, u64 num_singletons, const Ctx& ctx)
+                       int weight_kind, size_t n, u64 num_singletons, const Ctx& ctx,
+                       const std::vector<TermShape>* shapes)
     : n_(n), kind_(w ? weight_kind : 0), nsing_(num_singletons) {
+    if (shapes && shapes->size() != codes.size()) throw Error(RC_INVALID_INPUT, "fereg_session_create: term shapes");
     if (weight_kind < 0 || weight_kind > 3) throw Error(RC_INVALID_INPUT, "fereg_session_create: bad weight kind");
     if (w && weight_kind == 0) throw Error(RC_INVALID_INPUT, "fereg_session_create: weights need a weight kind");
     std::vector<const u32*> tptr = codes;
@@ -93,7 +123,30 @@ GpuSession::GpuSession(const std::vector<const u32*>& codes, const std::vector<u
         dcodes.push_back(d.tcodes.back().p);
     }
     CK(cudaStreamSynchronize(nullptr));
-    ab_ = std::make_unique<GpuAbsorber>(tptr, tg, w, n, ctx, &dcodes);
+    bool slopes = false;
+    for (size_t q = 0; q < tptr.size(); q++) {
+        const bool icpt = shapes ? (*shapes)[q].intercept : true;
+        t_icpt_.push_back(icpt);
+        slope_red_.emplace_back();
+        if (shapes)
+            for (const double* x : (*shapes)[q].slopes) {
+                if (!x) throw Error(RC_INVALID_INPUT, "fereg_session_create: missing slope variable");
+                slope_red_.back().push_back(redundant_slope_levels(tptr[q], tg[q], x, n, icpt));
+            }
+        slopes |= !icpt || !slope_red_.back().empty();
+    }
+    if (slopes) {
+        std::vector<SlopeTermIn> st(tptr.size());
+        for (size_t q = 0; q < tptr.size(); q++) {
+            st[q].codes = tptr[q];
+            st[q].g = tg[q];
+            st[q].intercept = t_icpt_[q];
+            st[q].slopes = (*shapes)[q].slopes;
+        }
+        ab_ = std::make_unique<GpuSlopeSolver>(st, w, n, ctx);
+    } else {
+        ab_ = std::make_unique<GpuAbsorber>(tptr, tg, w, n, ctx, &dcodes);
+    }
     d.st = ab_->stream();
     AllocScope alloc_scope(d.st);
     for (auto& c : ccodes_) {
@@ -282,55 +335,70 @@ GpuSession::Dof GpuSession::estimate_dof(bool clusters, bool firstpair, bool wan
     return dof_end(job);
 }
 
-// dof.rs:64-180 estimate_dof (intercept-only terms, the default options: clusters and pairwise;
-// firstpair instead of both). Slot i: k levels, m redundant, exact, nested in a cluster.
+// dof.rs:64-180 estimate_dof (the default options: clusters, pairwise and continuous; firstpair
+// instead of clusters and pairwise). Slots: per term its intercept (when it has one), then one
+// per slope; slot i: k levels, m redundant, exact, nested in a cluster.
 GpuSession::Dof GpuSession::dof_pass(bool clusters, bool firstpair, bool want_groupvar, DofScratch& s) {
     Dof dof;
     const size_t nt = tg_.size();
-    std::vector<bool> live(nt, true);
-    for (size_t q = 0; q < nt; q++) dof.slots.push_back(DofSlot{tg_[q], 0, false, false});
+    std::vector<int> icpt_term;  // per slot: the term of an intercept slot, -1 for a slope slot
+    std::vector<size_t> first_slope(nt, SIZE_MAX);
+    for (size_t q = 0; q < nt; q++) {
+        if (t_icpt_[q]) {
+            dof.slots.push_back(DofSlot{tg_[q], 0, false, false});
+            icpt_term.push_back(int(q));
+        }
+        if (!slope_red_[q].empty()) first_slope[q] = dof.slots.size();
+        for (size_t k = 0; k < slope_red_[q].size(); k++) {
+            dof.slots.push_back(DofSlot{tg_[q], 0, false, false});
+            icpt_term.push_back(-1);
+        }
+    }
+    const size_t ns = dof.slots.size();
+    std::vector<bool> live(ns);
+    for (size_t i = 0; i < ns; i++) live[i] = icpt_term[i] >= 0;
     if (clusters && !firstpair)
         for (size_t c = 0; c < ccodes_.size(); c++) {
             if (std::none_of(live.begin(), live.end(), [](bool x) { return x; })) break;
-            for (size_t q = 0; q < nt; q++) {
-                if (!live[q] || dof.slots[q].exact) continue;
-                if (nested_within(q, c, s)) {
-                    dof.slots[q].m = dof.slots[q].k;
-                    dof.slots[q].exact = dof.slots[q].nested = true;
-                    dof.df_a_nested += dof.slots[q].k;
-                    live[q] = false;
+            for (size_t i = 0; i < ns; i++) {
+                if (!live[i] || dof.slots[i].exact) continue;
+                if (nested_within(size_t(icpt_term[i]), c, s)) {
+                    dof.slots[i].m = dof.slots[i].k;
+                    dof.slots[i].exact = dof.slots[i].nested = true;
+                    dof.df_a_nested += dof.slots[i].k;
+                    live[i] = false;
                 }
             }
         }
     const size_t remaining = size_t(std::count(live.begin(), live.end(), true));
     if (remaining > 1 || (remaining > 0 && dof.df_a_nested > 0)) {
-        // each live term but the first keeps one redundant level (the constant), unless a term
-        // nested in a cluster already carries it
+        // each live intercept but the first keeps one redundant level (the constant), unless a
+        // term nested in a cluster already carries it
         bool skip = dof.df_a_nested == 0;
-        for (size_t q = 0; q < nt; q++) {
-            if (!live[q]) continue;
+        for (size_t i = 0; i < ns; i++) {
+            if (!live[i]) continue;
             if (skip) {
                 skip = false;
                 continue;
             }
-            dof.slots[q].m = 1;
+            dof.slots[i].m = 1;
         }
     }
-    for (size_t q = 0; q < nt; q++)
-        if (live[q]) {
-            dof.slots[q].exact = true;
+    for (size_t i = 0; i < ns; i++)
+        if (live[i]) {
+            dof.slots[i].exact = true;
             break;
         }
     std::vector<size_t> idx;
-    for (size_t q = 0; q < nt; q++)
-        if (live[q]) idx.push_back(q);
+    for (size_t i = 0; i < ns; i++)
+        if (live[i]) idx.push_back(i);
     int pairs = 0;
     for (size_t a = 0; a < idx.size(); a++) {
         bool stop = false;
         for (size_t b = a + 1; b < idx.size(); b++) {
             pairs++;
             const bool save = pairs == 1 && want_groupvar;
-            const u64 m = mobility_groups(idx[a], idx[b], save, s);
+            const u64 m = mobility_groups(size_t(icpt_term[idx[a]]), size_t(icpt_term[idx[b]]), save, s);
             if (save) dof.has_groupvar = true;
             dof.slots[idx[b]].m = std::max(dof.slots[idx[b]].m, m);
             if (pairs == 1) dof.slots[idx[b]].exact = true;
@@ -341,9 +409,13 @@ GpuSession::Dof GpuSession::dof_pass(bool clusters, bool firstpair, bool want_gr
         }
         if (stop) break;
     }
-    for (auto& s : dof.slots) {
-        dof.df_a_initial += s.k;
-        dof.df_a_redundant += s.m;
+    // slopes constant (term with intercept) or zero (term without) within a level
+    for (size_t q = 0; q < nt; q++)
+        for (size_t k = 0; k < slope_red_[q].size(); k++)
+            if (slope_red_[q][k] > 0) dof.slots[first_slope[q] + k].m = slope_red_[q][k];
+    for (auto& sl : dof.slots) {
+        dof.df_a_initial += sl.k;
+        dof.df_a_redundant += sl.m;
     }
     dof.df_a = dof.df_a_initial - dof.df_a_redundant;
     return dof;
@@ -529,6 +601,7 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
 
 void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out) {
     AllocScope alloc_scope(ab_->stream());
+    restore_weights();
     SessionDev& d = *d_;
     cudaStream_t st = d.st;
     const size_t n = n_, r = 1 + nx;
@@ -566,9 +639,13 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     const bool want_coefs = out.d != nullptr;
     const size_t p_len = ab_->coefs_len();
     std::vector<double> coefs(want_coefs ? p_len * r : 0);
+    // the Gram comes out of the residualization pass when that pass can sum it
+    const double* wv = weighted ? d.wv.p : nullptr;
+    std::vector<double> g, ss_res;
+    GramRequest greq{wv, &g, &ss_res};
     const SolveInfo info =
     ab_->residualize_device(rows, r, spec.tol, spec.maxiter, want_coefs, nullptr, want_coefs ? coefs.data() : nullptr,
-                            spec.prec);
+                            spec.prec, &greq);
 
     // Outer products over the block: sum om a a^T of columns `cols` shifted by `shift` (+ the
     // constant), optionally the plain sums of squares; returns the full msz x msz matrix.
@@ -578,14 +655,14 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     return outer_products(src, nrows, srcR, cols, shift, cst, om, perm, ssq, ss_out);
     };
 
-    // Pass B: weighted Gram of the residualized block (stats.rs:195)
-    ph = d.begin(S_GRAM);
-    const double* wv = weighted ? d.wv.p : nullptr;
-    std::vector<int> all_cols(r);
-    std::iota(all_cols.begin(), all_cols.end(), 0);
-    std::vector<double> ss_res;
-    std::vector<double> g = outer(rows, n, R, all_cols, nullptr, false, wv, nullptr, true, &ss_res);
-    d.end(ph);
+    // Pass B: weighted Gram of the residualized block (stats.rs:195), unless the solve summed it
+    if (!info.gram) {
+        ph = d.begin(S_GRAM);
+        std::vector<int> all_cols(r);
+        std::iota(all_cols.begin(), all_cols.end(), 0);
+        g = outer(rows, n, R, all_cols, nullptr, false, wv, nullptr, true, &ss_res);
+        d.end(ph);
+    }
 
     // Collinearity, stage 1 (ols.rs:38 stage1_absorbed): a column absorbed by the FE
     const double ctol = std::min(1e-6, spec.tol / 10.0);
@@ -877,6 +954,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
 void GpuSession::iv(double* rows_in, bool on_device, size_t nx, size_t ne, size_t ni, const IvSpec& spec,
                     IvOut& out) {
     AllocScope alloc_scope(ab_->stream());
+    restore_weights();
     SessionDev& d = *d_;
     cudaStream_t st = d.st;
     const size_t n = n_, r = 1 + nx + ne + ni;
@@ -1082,6 +1160,7 @@ void GpuSession::iv(double* rows_in, bool on_device, size_t nx, size_t ne, size_
 void GpuSession::wildboot(double* rows, bool on_device, size_t nx, const OlsSpec& ospec, const BootSpec& bs,
                           BootOut& out) {
     AllocScope alloc_scope(ab_->stream());
+    restore_weights();
     if (ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg wildboot: the session has no cluster dimension");
     if (bs.coef >= nx) throw Error(RC_INVALID_INPUT, "fereg wildboot: coefficient index out of range");
     if (bs.reps == 0 || bs.tile == 0) throw Error(RC_INVALID_INPUT, "fereg wildboot: reps and tile must be positive");
@@ -1515,5 +1594,211 @@ void GpuSession::glm(double* rows_in, bool on_device, size_t nx, const GlmSpec& 
     out.converged = converged;
     d.collect();
     CK(cudaGetLastError());
+    irls_weights_ = true;  // the absorber holds the last IRLS weights
 }
+
+// The absorber back on the session's weights after a GLM call left its IRLS weights there (the
+// GLM runs on unweighted sessions only).
+void GpuSession::restore_weights() {
+    if (!irls_weights_) return;
+    ab_->set_weights(nullptr);
+    irls_weights_ = false;
+}
+
+// glm/separation.rs:61-196 relu on the device: the method of weighting (M = ceil(eps^-1/2) on
+// y > 0, 1 on y = 0) of the ReLU working variable u (start 1[y = 0]) regressed on X / sd and the
+// fixed effects, until the prediction xbd = u - e is non-negative on the boundary (y = 0) or no
+// boundary residual is negative; past 100 iterations it continues while the negative predictions
+// keep shrinking (1% over 10 iterations), up to 2000. The regressors absorbed by the fixed
+// effects or collinear with the others (the first solve's Gram, ols.rs:38-46 rules) are left out.
+// The absorber's weights return to the session's afterwards.
+void GpuSession::relu_separation(double* rows_in, bool on_device, size_t nx, const ReluSpec& rs, ReluOut& out) {
+    AllocScope alloc_scope(ab_->stream());
+    if (!wk_.empty()) throw Error(RC_INVALID_INPUT, "fereg relu: weighted sessions are not supported");
+    if (1 + nx + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg relu: at most 62 regressors");
+    SessionDev& d = *d_;
+    const cudaStream_t st = d.st;
+    const size_t n = n_, r = 1 + nx, k = nx;
+    const int R = int(r);
+    const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+    constexpr double RELU_TOL = 1e-4, RELU_ZERO_TOL = 1e-8, RELU_STALL = 0.99;
+    constexpr size_t RELU_MAXITER = 100, RELU_HARD_MAXITER = 2000, RELU_STALL_SPAN = 10;
+    const double regtol = std::max(RELU_TOL * RELU_TOL, 1e-13);
+    const double big_m = std::ceil(std::pow(std::numeric_limits<double>::epsilon(), -0.5));
+    DBuf<double> raw, xs, w, u, B, resid, xbd, part, bdev;
+    DBuf<int> kdev;
+    raw.alloc(n * r);
+    CK(cudaMemcpyAsync(raw.p, rows_in, n * r * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    xs.alloc(std::max<size_t>(1, n * k));
+    w.alloc(n);
+    u.alloc(n);
+    B.alloc(n * r);
+    resid.alloc(n);
+    xbd.alloc(n);
+    part.alloc(size_t(blocks) * std::max<size_t>(RELU_PARTS, 2 * k));
+    auto parts = [&](size_t len) {
+        std::vector<double> h(size_t(blocks) * len);
+        CK(cudaMemcpyAsync(h.data(), part.p, h.size() * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return h;
+    };
+    // y must be a Poisson outcome
+    DBuf<int> flag;
+    flag.alloc(1);
+    CK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    k_glm_ysum<<<blocks, GLM_TB, 0, st>>>(raw.p, n, R, 0, part.p, flag.p);
+    int neg = 0;
+    CK(cudaMemcpyAsync(&neg, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (neg) throw Error(RC_INVALID_INPUT, "fereg relu: the dependent variable must be nonnegative");
+    // standardization: unweighted sd per regressor (stats.rs:187, floored at 1e-3)
+    std::vector<double> sd(std::max<size_t>(1, k), 1.0);
+    if (k) {
+        k_relu_colsums<<<blocks, GLM_TB, 0, st>>>(raw.p, n, R, part.p);
+        const std::vector<double> h = parts(2 * k);
+        for (size_t j = 0; j < k; j++) {
+            double s1 = 0.0, s2 = 0.0;
+            for (int b = 0; b < blocks; b++) {
+                s1 += h[size_t(b) * 2 * k + j];
+                s2 += h[size_t(b) * 2 * k + k + j];
+            }
+            const double mean = s1 / double(n);
+            const double m2 = std::max(0.0, s2 - double(n) * mean * mean);
+            sd[j] = std::max(std::sqrt(m2 / (double(n) - 1.0)), 1e-3);
+        }
+    }
+    DBuf<double> sdd;
+    sdd.upload(sd, st);
+    k_relu_init<<<blocks, GLM_TB, 0, st>>>(raw.p, n, R, sdd.p, big_m, xs.p, w.p, u.p, part.p);
+    d.launches += 4;
+    double ratio = 1.0;
+    if (k) {
+        const std::vector<double> h = parts(2 * k);
+        double nb = 0.0, bd = 0.0;
+        for (size_t j = 0; j < k; j++) {
+            double a = 0.0, c = 0.0;
+            for (int b = 0; b < blocks; b++) {
+                a += h[size_t(b) * 2 * k + j];
+                c += h[size_t(b) * 2 * k + k + j];
+            }
+            nb = std::max(nb, a);
+            bd = std::max(bd, c);
+        }
+        ratio = nb / bd;
+        ratio = std::isfinite(ratio) ? std::max(ratio, 1.0) : 1.0;
+    }
+    ab_->set_weights_device(w.p);
+    std::vector<int> all(r);
+    std::iota(all.begin(), all.end(), 0);
+    std::vector<double> sumsq;
+    std::vector<size_t> kept;
+    bool found = false, first = true;
+    u64 num_sep = 0, pcg = 0;
+    size_t iter = 0;
+    std::vector<double> hist;
+    for (;;) {
+        iter++;
+        ab_->ctx().check();
+        k_relu_block<<<blocks, GLM_TB, 0, st>>>(u.p, xs.p, n, R, B.p, part.p);
+        d.launches++;
+        double uu = 0.0;
+        for (double v : parts(1)) uu += v;
+        if (first && k) {
+            // the regressors' sums of squares before the solve (the collinearity reference)
+            outer_products(B.p, n, R, all, nullptr, false, nullptr, nullptr, true, &sumsq);
+        }
+        const SolveInfo si = first ? ab_->residualize_device(B.p, r, regtol, rs.inner_maxiter, false, nullptr, nullptr, rs.prec)
+                                   : ab_->residualize_device_warm_last(B.p, r, regtol, rs.inner_maxiter, rs.prec);
+        pcg += si.iterations;
+        std::vector<double> b;
+        if (k) {
+            std::vector<double> ss_res;
+            const std::vector<double> G = outer_products(B.p, n, R, all, nullptr, false, w.p, nullptr, true, &ss_res);
+            if (first) {
+                const double ctol = std::min(1e-6, rs.itol / 10.0);  // glm/mod.rs:7-8
+                std::vector<size_t> cand;
+                for (size_t j = 1; j < r; j++)
+                    if (!(ss_res[j] / sumsq[j] <= ctol)) cand.push_back(j);
+                const size_t kc = cand.size();
+                la::Mat gc(kc * kc);
+                for (size_t a = 0; a < kc; a++)
+                    for (size_t c = 0; c < kc; c++) gc[a * kc + c] = G[cand[a] * r + cand[c]];
+                std::vector<bool> dropped;
+                la::sweep_inverse(gc, kc, SWEEP_TOL, false, dropped);
+                for (size_t c = 0; c < kc; c++)
+                    if (!dropped[c]) kept.push_back(cand[c]);
+                out.dropped_collinear = int(k - kept.size());
+            }
+            const size_t kk = kept.size();
+            la::Mat gk(kk * kk);
+            for (size_t a = 0; a < kk; a++)
+                for (size_t c = 0; c < kk; c++) gk[a * kk + c] = G[kept[a] * r + kept[c]];
+            std::vector<bool> dk;
+            const la::Mat inv = la::sweep_inverse(gk, kk, SWEEP_TOL, false, dk);
+            b.assign(kk, 0.0);
+            for (size_t a = 0; a < kk; a++)
+                for (size_t c = 0; c < kk; c++) b[a] += inv[a * kk + c] * G[kept[c] * r];
+        }
+        first = false;
+        const int nk = int(b.size());
+        bdev.upload(b.empty() ? std::vector<double>{0.0} : b, st);
+        std::vector<int> kc(kept.begin(), kept.end());
+        kdev.upload(kc.empty() ? std::vector<int>{0} : kc, st);
+        // solve_lse's implied tolerance (ppmlhdfe_functions.mata, maxiter = 0)
+        const double epsilon = std::max(uu / big_m * ratio * ratio, 1e-8);
+        const double delta = epsilon + RELU_TOL;
+        k_relu_step<<<blocks, GLM_TB, 0, st>>>(raw.p, B.p, u.p, n, R, R, bdev.p, kdev.p, nk, delta, RELU_ZERO_TOL,
+                                                 resid.p, xbd.p, part.p);
+        d.launches++;
+        const std::vector<double> h = parts(RELU_PARTS);
+        double cneg = 0.0, cpos = 0.0, mn = INFINITY, negsum = 0.0;
+        for (int c = 0; c < blocks; c++) {
+            cneg += h[size_t(c) * RELU_PARTS];
+            cpos += h[size_t(c) * RELU_PARTS + 1];
+            mn = std::min(mn, h[size_t(c) * RELU_PARTS + 2]);
+            negsum += h[size_t(c) * RELU_PARTS + 3];
+        }
+        if (cneg == 0.0) {  // the prediction is non-negative on the boundary
+            num_sep = u64(cpos);
+            found = true;
+            break;
+        }
+        if (mn >= 0.0) {  // no negative boundary residual
+            k_relu_trim<<<blocks, GLM_TB, 0, st>>>(raw.p, n, R, resid.p, delta, xbd.p, part.p);
+            d.launches++;
+            double c2 = 0.0;
+            for (double v : parts(1)) c2 += v;
+            num_sep = u64(c2);
+            found = true;
+            break;
+        }
+        hist.push_back(negsum);
+        const size_t hn = hist.size();
+        const bool stalled = hn > RELU_STALL_SPAN && hist[hn - 1] > RELU_STALL * hist[hn - 1 - RELU_STALL_SPAN];
+        if (iter >= RELU_MAXITER && (stalled || iter >= RELU_HARD_MAXITER)) break;
+        k_relu_update<<<blocks, 256, 0, st>>>(raw.p, n, R, xbd.p, u.p);
+        d.launches++;
+    }
+    ab_->set_weights(nullptr);
+    out.iterations = iter;
+    out.pcg_iterations = pcg;
+    out.complete = found;
+    out.num_separated = found ? num_sep : 0;
+    DBuf<uint8_t> sep;
+    DBuf<double> cert;
+    sep.alloc(n);
+    cert.alloc(n);
+    if (found && num_sep > 0) {
+        k_relu_out<<<blocks, 256, 0, st>>>(raw.p, n, R, xbd.p, sep.p, cert.p);
+        d.launches++;
+    } else {
+        CK(cudaMemsetAsync(sep.p, 0, n, st));
+        CK(cudaMemsetAsync(cert.p, 0, n * 8, st));
+    }
+    if (out.separated) CK(cudaMemcpyAsync(out.separated, sep.p, n, cudaMemcpyDeviceToHost, st));
+    if (out.certificate) CK(cudaMemcpyAsync(out.certificate, cert.p, n * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+}
+
 }  // namespace fereg

@@ -43,19 +43,29 @@ struct OlsOut {
 struct SessionDev;
 struct DofScratch;
 
+// The shape of one absorb term beyond its codes: intercept flag and slope variables (kept order,
+// n values each).
+struct TermShape {
+    bool intercept = true;
+    std::vector<const double*> slopes;
+};
+
 class GpuSession {
    public:
     // codes[q]: kept-order codes of FE term q (< g[q]); no terms = the constant alone (noabsorb).
     // cl_codes[c]: kept-order codes of cluster dimension c. w: raw kept-order weights or null;
     // weight_kind 0 none, 1 aweight, 2 fweight, 3 pweight. num_singletons: rows the session's
     // preparation dropped as singletons (reported in N_full).
+    // shapes (null: every term intercept-only): per term its intercept flag and slope variables
+    // (kept order); a term with slopes or without an intercept makes the absorber the slope
+    // solver (solve.rs:338).
     GpuSession(const std::vector<const u32*>& codes, const std::vector<u32>& g,
                const std::vector<const u32*>& cl_codes, const std::vector<u32>& cl_g, const double* w, int weight_kind,
-               size_t n, u64 num_singletons, const Ctx& ctx);
+               size_t n, u64 num_singletons, const Ctx& ctx, const std::vector<TermShape>* shapes = nullptr);
     ~GpuSession();
 
-    GpuAbsorber& absorber() { return *ab_; }
-    const GpuAbsorber& absorber() const { return *ab_; }
+    DeviceAbsorber& absorber() { return *ab_; }
+    const DeviceAbsorber& absorber() const { return *ab_; }
     size_t n() const { return n_; }
     // Kernel launches of the session passes and its absorber so far.
     u64 launches() const;
@@ -130,6 +140,24 @@ class GpuSession {
     };
     void glm(double* rows, bool on_device, size_t nx, const GlmSpec& gs, GlmOut& out);
 
+    // One ReLU separation check (glm/separation.rs:61-196) of the Poisson outcome y (column 0)
+    // with the regressors (columns 1..nx) of the n x (1 + nx) block (row order; host or device
+    // memory), standardized by their standard deviations (glm/mod.rs:4-6): weighted FE solves of
+    // the ReLU working variable until the prediction is non-negative on the y = 0 rows.
+    struct ReluSpec {
+        double itol = 1e-10;  // the GLM's inner tolerance (its collinearity rule, glm/mod.rs:7-8)
+        size_t inner_maxiter = 16000;
+        Precision prec = Precision::F64;
+    };
+    struct ReluOut {
+        uint8_t* separated = nullptr;  // n, row order: 1 on the separated rows
+        double* certificate = nullptr; // n, row order: the certificate (positive on them, else 0)
+        u64 num_separated = 0, iterations = 0, pcg_iterations = 0;
+        bool complete = false;  // the check certified its result
+        int dropped_collinear = 0;
+    };
+    void relu_separation(double* rows, bool on_device, size_t nx, const ReluSpec& rs, ReluOut& out);
+
    private:
     size_t n_ = 0;
     int kind_ = 0;
@@ -138,8 +166,14 @@ class GpuSession {
     std::vector<std::vector<u32>> tcodes_, ccodes_;  // kept order (host)
     std::vector<double> wk_;                         // raw kept-order weights
     double sumw_ = 0;
-    std::unique_ptr<GpuAbsorber> ab_;
+    std::unique_ptr<DeviceAbsorber> ab_;
     std::unique_ptr<SessionDev> d_;
+    // per term: intercept flag, slope count, and per slope the levels on which it is redundant
+    // (dof.rs:165-176, reghdfe dof_update_cvars), fixed by the session's data
+    std::vector<bool> t_icpt_;
+    std::vector<std::vector<u64>> slope_red_;
+    bool irls_weights_ = false;  // a GLM call left its IRLS weights on the absorber
+    void restore_weights();
 
     struct DofSlot {
         u64 k = 0, m = 0;

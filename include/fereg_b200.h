@@ -58,6 +58,33 @@ const char* fereg_last_error(void);
 int fereg_absorber_create(const uint32_t* const* codes, const uint32_t* g, int nterms, const double* w, size_t n,
                           const fereg_ctx* ctx, fereg_absorber** out);
 
+/* solve.rs:338 build with the terms' shapes (session.rs:20-42 Term): term q has codes[q] below
+ * g[q], an intercept when intercept[q] != 0 (intercept NULL: every term), and nslopes[q] slope
+ * variables (nslopes NULL: none), kept order, n values each, given in `slopes` term after term.
+ * A term with slopes or without an intercept makes the absorber the heterogeneous-slope solver
+ * (slopes.rs:2183 SlopeSolver): coefficient blocks then hold m + G_E * b_E rows (the reduced
+ * coordinates, then E's level coefficients, slopes.rs:27-29) and term_values writes
+ * sum_q g_q * (intercept_q + nslopes_q) values. The kernel-level hooks fereg_absorber_apply,
+ * _rhs, _rhs_noalloc, _precond and _weight_state serve the intercept-only solver only (198). */
+int fereg_absorber_create_terms(const uint32_t* const* codes, const uint32_t* g, const int* intercept,
+                                const int* nslopes, const double* const* slopes, int nterms, const double* w, size_t n,
+                                const fereg_ctx* ctx, fereg_absorber** out);
+/* 1 when the absorber is the heterogeneous-slope solver. No counterpart in the reference. */
+int fereg_absorber_has_slopes(const fereg_absorber* h);
+/* Values fereg_absorber_term_values writes. */
+size_t fereg_absorber_term_values_len(const fereg_absorber* h);
+/* Test hooks of the slope solver (no counterpart in the reference): the weight state
+ * (slopes.rs:527-697: M_s^+ per level of E, G_E x b_E^2; the block-Jacobi inverses, b^2 per level
+ * of every block in block order; the redundant coordinates, m), one application of S and of the
+ * preconditioner to host m x r blocks, the right-hand side of a host n x r block with
+ * [sum w v^2; sum w v; sum w e^2] (3 x r), and the structure: n, m, E, G_E, b_E, slots per row,
+ * blocks, small blocks, small coordinates (9 values) with the session term of every block. */
+int fereg_slope_weight_state(const fereg_absorber* h, double* minv, double* jinv, uint8_t* redundant);
+int fereg_slope_apply(fereg_absorber* h, const double* p, size_t r, double* y);
+int fereg_slope_precond(fereg_absorber* h, const double* rr, size_t r, double* z);
+int fereg_slope_rhs(fereg_absorber* h, const double* rows, size_t r, double* y, double* stats);
+int fereg_slope_structure(const fereg_absorber* h, uint64_t* out9, uint32_t* block_terms);
+
 void fereg_absorber_destroy(fereg_absorber* h);
 
 /* Absorber::n (absorber.rs:64). */
@@ -177,6 +204,14 @@ typedef struct fereg_ols_out {
 int fereg_session_create(const uint32_t* const* codes, const uint32_t* g, int nterms, const uint32_t* const* cl_codes,
                          const uint32_t* cl_g, int ncl, const double* w, int weight_kind, size_t n,
                          uint64_t num_singletons, const fereg_ctx* ctx, fereg_session** out);
+/* fereg_session_create with the terms' shapes as fereg_absorber_create_terms: slope terms make
+ * the session's absorber the slope solver, and the dof slots (dof.rs:74-88) one per intercept
+ * and one per slope, with the slopes' redundant levels (dof.rs:165-176). */
+int fereg_session_create_terms(const uint32_t* const* codes, const uint32_t* g, const int* intercept,
+                               const int* nslopes, const double* const* slopes, int nterms,
+                               const uint32_t* const* cl_codes, const uint32_t* cl_g, int ncl, const double* w,
+                               int weight_kind, size_t n, uint64_t num_singletons, const fereg_ctx* ctx,
+                               fereg_session** out);
 void fereg_session_destroy(fereg_session* s);
 
 /* Session::row_order: the rows of an ols block (n values, kept-observation indices). */
@@ -271,6 +306,15 @@ typedef struct fereg_glm_out {
     int32_t converged;
 } fereg_glm_out;
 
+/* One ReLU separation check (glm/separation.rs:61-196, ppmlhdfe 2.3.3 relu_fix_separation) on
+ * the session's sample: column 0 of the n x (1 + nx) block (row order) is the Poisson outcome,
+ * columns 1..nx the regressors (standardized by their standard deviations inside). separated
+ * (n bytes) and certificate (n values) are row order and may be NULL; out4 receives [separated
+ * rows, ReLU iterations, PCG iterations, 1 when the check certified its result]. The rows it finds
+ * are dropped by the caller, who prepares the remaining sample again and repeats until a check
+ * finds none (glm/mod.rs:454-505 glm_separate). Unweighted sessions. */
+int fereg_session_relu(fereg_session* s, double* rows, int rows_on_device, size_t nx, double itol,
+                       size_t inner_maxiter, uint8_t* separated, double* certificate, uint64_t* out4);
 int fereg_session_glm(fereg_session* s, double* rows, int rows_on_device, size_t nx, const fereg_glm_spec* spec,
                       fereg_glm_out* out);
 /* fereg_session_glm with the Poisson family. */

@@ -163,7 +163,15 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
         warm = out["coefs"]
         if it == 1:
             ss = np.sum(w[:, None] * B[:, 1:] ** 2, axis=0)
-            keep = np.flatnonzero(ss > min(1e-6, tol / 10) * sumsq)
+            keep0 = np.flatnonzero(ss > min(1e-6, tol / 10) * sumsq)
+            # then the columns collinear with earlier kept ones (the sweep's pivot order)
+            sw = np.sqrt(w)
+            kk = []
+            for j in keep0:
+                M = B[:, [1 + q for q in kk + [j]]] * sw[:, None]
+                if np.linalg.matrix_rank(M, tol=1e-9 * np.linalg.norm(M)) == len(kk) + 1:
+                    kk.append(j)
+            keep = np.array(kk, dtype=int)
         Xt, zt = B[:, 1 + keep], B[:, 0]
         A = np.linalg.inv(Xt.T @ (w[:, None] * Xt))
         b = A @ (Xt.T @ (w * zt))
@@ -208,3 +216,81 @@ def irls_absorbed(codes, g, y, X, family, vce="robust", cl=None, tol=1e-8, itol=
     V = np.zeros((k, k))
     V[np.ix_(keep, keep)] = Vk
     return bf, V, dev, ll, it
+
+
+def relu_separation(codes, g, y, X, itol=1e-10):
+    """ReLU separation check (glm/separation.rs:61-196, ppmlhdfe 2.3.3 relu_fix_separation) on
+    the dense FE design: the method of weighting (M = ceil(eps^-1/2) on y > 0, 1 on y = 0) of the
+    working variable u (start 1[y = 0]) regressed on X / sd (unweighted sd floored at 1e-3,
+    glm/mod.rs:4-6) and the FE dummies; regressors absorbed by the FE (sum x~^2 / sum x^2 <=
+    min(1e-6, itol / 10)) or collinear with the others on the first solve leave the regression.
+    Each step: xbd = u - e, 0 off the boundary and within [-0.1 delta, delta] with delta =
+    max(u'u / M ratio^2, 1e-8) + 1e-4 (ratio: norm(X, 1) of the y > 0 rows over the y = 0 rows);
+    stop when xbd >= 0 on the boundary, or when no boundary residual (0 within 1e-8) is negative
+    (then rows with residual > delta leave); else u = max(xbd, 0) on the boundary. Past 100
+    steps it continues while the negative predictions fall by 1% over 10 steps (at most 2000).
+    Returns the separated rows (bool) and whether the check certified its result."""
+    y = np.asarray(y, dtype=float)
+    X = np.asarray(X, dtype=float).reshape(len(y), -1)
+    n, k = X.shape
+    bd = y == 0
+    if not bd.any():
+        return np.zeros(n, dtype=bool), True
+    D = np.concatenate([np.eye(gq)[c] for c, gq in zip(codes, g)], axis=1) if codes else np.ones((n, 1))
+    sd = np.maximum(X.std(axis=0, ddof=1), 1e-3) if k else np.ones(0)
+    Xs = X / sd if k else X
+    big_m = np.ceil(np.finfo(float).eps ** -0.5)
+    w = np.where(bd, 1.0, big_m)
+    sw = np.sqrt(w)
+    if k:
+        a = np.abs(Xs[~bd]).sum(axis=0).max() if (~bd).any() else 0.0
+        c = np.abs(Xs[bd]).sum(axis=0).max()
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = a / c
+        ratio = max(ratio, 1.0) if np.isfinite(ratio) else 1.0
+    else:
+        ratio = 1.0
+
+    def resid_on_d(B):
+        beta, *_ = np.linalg.lstsq(D * sw[:, None], B * sw[:, None], rcond=None)
+        return B - D @ beta
+
+    u = bd.astype(float)
+    keep = None
+    hist = []
+    it = 0
+    while True:
+        it += 1
+        B = np.column_stack([u, Xs])
+        Bt = resid_on_d(B)
+        if keep is None:
+            keep = []
+            if k:
+                ss = (w[:, None] * Bt[:, 1:] ** 2).sum(axis=0)
+                raw = (Xs ** 2).sum(axis=0)
+                cand = [j for j in range(k) if raw[j] > 0 and not ss[j] / raw[j] <= min(1e-6, itol / 10)]
+                for j in cand:  # sequential rank test (the sweep's pivot order)
+                    M = Bt[:, [1 + q for q in keep + [j]]] * sw[:, None]
+                    if np.linalg.matrix_rank(M, tol=1e-9 * np.linalg.norm(M)) == len(keep) + 1:
+                        keep.append(j)
+        if keep:
+            Xt = Bt[:, [1 + q for q in keep]]
+            b, *_ = np.linalg.lstsq(Xt * sw[:, None], Bt[:, 0] * sw, rcond=None)
+            e = Bt[:, 0] - Xt @ b
+        else:
+            e = Bt[:, 0].copy()
+        uu = float(u @ u)
+        delta = max(uu / big_m * ratio * ratio, 1e-8) + 1e-4
+        xbd = u - e
+        xbd[~bd | ((-0.1 * delta <= xbd) & (xbd <= delta))] = 0.0
+        if np.all(xbd[bd] >= 0):
+            return bd & (xbd > 0), True
+        e[np.abs(e) <= 1e-8] = 0.0
+        if e[bd].min() >= 0:
+            xbd[bd & (e > delta)] = 0.0
+            return bd & (xbd > 0), True
+        hist.append(float(-xbd[bd & (xbd < 0)].sum()))
+        stalled = len(hist) > 10 and hist[-1] > 0.99 * hist[-11]
+        if it >= 100 and (stalled or it >= 2000):
+            return np.zeros(n, dtype=bool), False
+        u[bd] = np.maximum(xbd[bd], 0.0)

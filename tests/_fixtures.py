@@ -129,3 +129,67 @@ def prepare_poisson(spec, data):
     keep = np.zeros(n_all, dtype=bool)
     keep[np.flatnonzero(base)[alive]] = True
     return keep, nsing, terms, cl, block
+
+
+def load_separation():
+    """The committed ppmlhdfe fixtures fitted with sep(fe relu) and their data sets."""
+    fx = load_json("separation_fixtures.json")
+    data = {f["spec"]["data"]: load_csv(f"glm_{f['spec']['data']}.csv") for f in fx}
+    return fx, data
+
+
+def prepare_separation(spec, data, check, drop=None):
+    """Session::glm_separate's rounds (glm/mod.rs:454-505) for a sep(fe relu) fixture: the rows
+    from `first_obs` on; per round the cyclic singleton drops (unless kept) and the `fe` rule
+    until stable (`drop(codes, g, y, keepsing) -> alive`, the oracle's by default), then the
+    separation check `check(terms, block) -> separated rows (kept order)` on the kept sample;
+    separated rows leave and the next round prepares the rest, until a check finds none. A
+    no-absorb fixture absorbs the constant (one term with one level). Returns the kept mask over
+    all rows, the separated and the singleton counts, the kept terms and the [y, x...] block."""
+    n_all = len(data[spec["y"]])
+    base = np.zeros(n_all, dtype=bool)
+    base[spec["first_obs"]:] = True
+    y_all = data[spec["y"]][base]
+    from oracle import oracle
+
+    if spec["absorb"]:
+        fac = {f: oracle.factorize(data[f][base]) for t in spec["absorb"] for f in t}
+        terms0 = [_interact([fac[f] for f in t]) if len(t) > 1 else fac[t[0]] for t in spec["absorb"]]
+    else:
+        terms0 = [(np.zeros(int(base.sum()), dtype=np.uint32), 1)]
+    X_all = np.column_stack([data[x][base] for x in spec["x"]]) if spec["x"] else np.zeros((int(base.sum()), 0))
+
+    def oracle_drop(codes, g, y, keepsing):
+        alive = np.ones(len(y), dtype=bool)
+        while True:
+            before = int(alive.sum())
+            if not keepsing:
+                idx = np.flatnonzero(alive)
+                a2, _ = oracle.drop_singletons([restrict(c, alive)[0] for c in codes],
+                                               [restrict(c, alive)[1] for c in codes], None)
+                alive[idx[~a2]] = False
+            for c, gq in zip(codes, g):
+                s = np.bincount(c[alive], weights=y[alive], minlength=gq)
+                alive &= s[c] > 0
+            if int(alive.sum()) == before:
+                return alive
+
+    drop = drop or oracle_drop
+    alive = np.ones(int(base.sum()), dtype=bool)
+    nsep = nsing = 0
+    while True:
+        idx = np.flatnonzero(alive)
+        a2 = drop([c[idx] for c, _ in terms0], [g for _, g in terms0], y_all[idx], spec["keepsing"])
+        nsing += int((~a2).sum())
+        alive[idx[~a2]] = False
+        idx = np.flatnonzero(alive)
+        terms = [restrict(c, alive) for c, _ in terms0]
+        block = np.ascontiguousarray(np.column_stack([y_all[idx], X_all[idx]]))
+        sep = check(terms, block)
+        if not sep.any():
+            break
+        nsep += int(sep.sum())
+        alive[idx[sep]] = False
+    keep = np.zeros(n_all, dtype=bool)
+    keep[np.flatnonzero(base)[alive]] = True
+    return keep, nsep, nsing, terms, block

@@ -38,7 +38,7 @@ def fx(name, x, absorb, **kw):
     return spec
 
 
-# tests/ols.rs:803-827 (s16 uses slopes, which this path does not cover).
+# tests/ols.rs:803-827 (s16, with slopes, in SLOPE_SPECS below).
 SPECS = [
     fx("s01_unadj", X3, IDYEAR),
     fx("s02_robust_3fe", X3, [["id"], ["year"], ["firm"]], robust=True),
@@ -60,6 +60,11 @@ SPECS = [
 ]
 
 COLUMNS = ["id", "year", "firm", "region", "c1", "c2", "x1", "x2", "x3", "x4", "xa", "xc", "w", "fw", "y", "y2"]
+
+# tests/ols.rs:827: reghdfe y x1 x2, absorb(id firm##c.x4), per term its intercept and slopes.
+SLOPE_SPECS = [
+    fx("s16_slopes", X2, [["id"], ["firm"]], intercept=[True, True], term_slopes=[[], ["x4"]]),
+]
 
 
 def main(ref):
@@ -85,6 +90,15 @@ def main(ref):
     with open(os.path.join(HERE, "ols_fixtures.json"), "w") as f:
         json.dump(out, f)
     print(f"wrote {len(out)} fixtures, {len(rows)} rows")
+    out = []
+    for spec in SLOPE_SPECS:
+        with open(os.path.join(data_dir, f"ols_{spec['name']}.json")) as f:
+            j = json.load(f)
+        out.append(dict(spec=spec, cmdline=j["cmdline"], colnames=j["colnames"], b=j["b"], V=j["V"],
+                        dof_table=j["dof_table"], sample=j["sample"], scalars=j["scalars"]))
+    with open(os.path.join(HERE, "ols_slopes_fixtures.json"), "w") as f:
+        json.dump(out, f)
+    print(f"wrote {len(out)} slope fixtures")
 
 
 IV_COLUMNS = ["idcode", "year", "ln_wage", "age", "tenure", "union", "south", "msp", "w", "fw"]
@@ -182,6 +196,67 @@ POISSON_SCALARS = ["N", "num_separated", "num_singletons", "N_clust", "ll", "ll_
                    "df_m"]
 
 
+# tests/glm.rs:549-590: ppmlhdfe 2.3.3 fixtures fitted with sep(fe relu) (the reference's
+# Session::glm_separate rounds), unweighted and without offset. `first_obs`: rows before it are
+# excluded (the fixture's `if _n > 2`); `counts`: the harness's (num_separated, num_singletons)
+# where they differ from the fixture's (p_problem1: ppmlhdfe's own check gave up on the full
+# data, so its fixture holds the sample its test expects).
+SEP_SPECS = [
+    dict(name="p_problem1", data="problem1", y="y", x=["x1", "x2"], absorb=[["i"], ["j"]], keepsing=False,
+         tol=1e-10, first_obs=0, counts=[4, 1], maxiter=10000),
+    dict(name="p_problem2", data="problem2", y="y", x=["x1", "x2"], absorb=[["i"], ["j"]], keepsing=False,
+         tol=1e-10, first_obs=0, counts=None, maxiter=10000),
+    dict(name="p_problem3", data="problem3", y="y", x=["x1", "x2", "x3"], absorb=[], keepsing=False, tol=1e-12,
+         first_obs=0, counts=None, maxiter=10000),
+    dict(name="p_problem4", data="problem4", y="y", x=["x1", "x2", "x3"], absorb=[], keepsing=False, tol=1e-12,
+         first_obs=0, counts=None, maxiter=200),
+    dict(name="p_problem5", data="problem5", y="y", x=["x1", "x2"], absorb=[["i"], ["j"]], keepsing=False,
+         tol=1e-12, first_obs=0, counts=None, maxiter=10000),
+    dict(name="p_problem6", data="problem6", y="y", x=["x"], absorb=[], keepsing=False, tol=1e-10, first_obs=0,
+         counts=None, maxiter=10000),
+    dict(name="p_hard1", data="hard1", y="y", x=[], absorb=[["id1"], ["id2"]], keepsing=False, tol=1e-10,
+         first_obs=0, counts=None, maxiter=10000),
+    dict(name="p_hard2_keepsing", data="hard2", y="FTA", x=[], absorb=[["ijk_fe"], ["jkt_fe"], ["ikt_fe"]],
+         keepsing=True, tol=1e-12, first_obs=0, counts=None, maxiter=10000),
+    dict(name="p_hard3", data="hard3", y="y", x=[], absorb=[["id1"], ["id2"]], keepsing=False, tol=1e-10,
+         first_obs=0, counts=None, maxiter=10000),
+    dict(name="p_hard5", data="hard5", y="y", x=["x1", "x2", "x3", "x4"], absorb=[], keepsing=False, tol=1e-10,
+         first_obs=0, counts=None, maxiter=10000),
+    dict(name="p_hard5b", data="hard5", y="y", x=["x2", "x3", "x4"], absorb=[], keepsing=False, tol=1e-10,
+         first_obs=0, counts=None, maxiter=10000),
+    dict(name="p_hard4", data="hard5", y="y", x=["x2", "x3", "x4"], absorb=[], keepsing=False, tol=1e-10,
+         first_obs=2, counts=None, maxiter=10000),
+]
+SEP_DATA = {
+    "problem1": ["y", "x1", "x2", "i", "j"],
+    "problem2": ["y", "x1", "x2", "i", "j"],
+    "problem3": ["y", "x1", "x2", "x3"],
+    "problem4": ["y", "x1", "x2", "x3"],
+    "problem5": ["y", "x1", "x2", "i", "j"],
+    "problem6": ["y", "x"],
+    "hard1": ["y", "id1", "id2"],
+    "hard2": ["FTA", "ikt_fe", "jkt_fe", "ijk_fe"],
+    "hard3": ["y", "id1", "id2"],
+    "hard5": ["y", "x1", "x2", "x3", "x4", "x5"],
+}
+
+
+def main_separation(ref):
+    data_dir = os.path.join(ref, "crates", "fereg-core", "tests", "data")
+    for name, cols in SEP_DATA.items():
+        copy_csv(os.path.join(data_dir, f"glm_{name}.csv"), os.path.join(HERE, f"glm_{name}.csv"), cols)
+    out = []
+    for spec in SEP_SPECS:
+        with open(os.path.join(data_dir, f"glm_{spec['name']}.json")) as f:
+            j = json.load(f)
+        sc = {k: j["scalars"].get(k) for k in POISSON_SCALARS}
+        out.append(dict(spec=spec, cmdline=j["cmdline"], colnames=j["colnames"], b=j["b"], V=j["V"],
+                        sample=j["sample"], scalars=sc))
+    with open(os.path.join(HERE, "separation_fixtures.json"), "w") as f:
+        json.dump(out, f)
+    print(f"wrote {len(out)} separation fixtures")
+
+
 def main_poisson(ref):
     data_dir = os.path.join(ref, "crates", "fereg-core", "tests", "data")
     for name, cols in POISSON_DATA.items():
@@ -205,3 +280,4 @@ if __name__ == "__main__":
     main(ref)
     main_iv_logit(ref)
     main_poisson(ref)
+    main_separation(ref)
