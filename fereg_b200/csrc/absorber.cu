@@ -89,12 +89,7 @@ struct DevWarpTiles {
 // the lane-private small-coordinate slots and column partials).
 inline size_t grhs_smem(u32 ms_acc) { return WPB * (size_t(ms_acc) * 64 * 8 + 4 * 32 * 8); }
 inline size_t wresid_smem(int Rc) { return WPB * wresid_bytes(Rc); }
-// Shared memory of k_wresid with the fused Gram: the tile parts and the chunk stages, at least
-// the final reduction.
-template <int RCP>
-size_t gram_wresid_smem(int Rc) {
-    return std::max(WPB * wresid_bytes(Rc) + WPB * GramShape<RCP>::stage_bytes, GramShape<RCP>::red_bytes);
-}
+
 inline size_t wpull_smem() { return WPB * pull_bytes(); }
 
 // Calls f(RCP, NBK) as integral constants: RCP the padded width of an Rc-column chunk, NBK the
@@ -202,7 +197,6 @@ struct Scratch {
     DBuf<int> wflag;
     // solve (FP64)
     DBuf<double> rows, rhs, b1, coefs, r, z, p, q, t, part, cta, cta2, colsum, along, small;
-    DBuf<double> gpart, gsum;  // the fused Gram: per-CTA partials, sums
     DBuf<double> rhsv, xv;  // the padded right-hand side and iterate of the PCG
     // inner FP32 buffers of the refined solve
     DBuf<float> fx, fb, fr, fz, fp, fq, ft, fpart, frhs, fx0, fsmall;
@@ -1349,10 +1343,9 @@ SolveInfo GpuAbsorber::residualize_device_warm_last(double* z_dev, size_t r, dou
 }
 
 SolveInfo GpuAbsorber::residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
-                                          const double* warm, double* coefs, Precision prec,
-                                          const GramRequest* gram) {
+                                          const double* warm, double* coefs, Precision prec) {
     AllocScope alloc_scope(stream_);
-    return solve(z_dev, r, tol, maxiter, want_coefs, warm, coefs, prec, false, gram);
+    return solve(z_dev, r, tol, maxiter, want_coefs, warm, coefs, prec);
 }
 
 constexpr int PROBE_FROM = 7, PROBE_AT = 12;
@@ -1596,7 +1589,7 @@ restart:
 
 // solve.rs:1141-1311 residualize.
 SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
-                             double* coefs, Precision prec, bool warm_last, const GramRequest* gram) {
+                             double* coefs, Precision prec, bool warm_last) {
     SolveInfo info;
     const size_t m = hs_.m, g1 = hs_.g1;
     if (r == 0) {
@@ -1802,38 +1795,18 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     ctx_.check();
     int h = d.begin(P_RESID, st);
     double* alpha = want_coefs ? x + m * r : nullptr;
-    // the Gram in the same pass: every row in a short segment, every column in one launch
-    const bool fuse_gram = gram && gram->g && gram->ss && d.wseg.n && !S.seg.nfix && !S.seg.n && R <= 16;
-    const int glen = gram_len(R);
-    if (fuse_gram) {
-        d.gpart.alloc(size_t(GRID_S) * glen);
-        d.gsum.alloc(size_t(glen));
-    }
     if (d.wseg.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
+            const size_t shm = wresid_smem(Rc);
             with_rcp<0>(Rc, S.nb, [&](auto c, auto nbk) {
                 constexpr int RCP = decltype(c)::value, NBK = decltype(nbk)::value;
-                auto run = [&](auto kernel, size_t shm, GramFuse gf) {
-                    allow_smem(kernel, shm);
-                    kernel<<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, x, d.b1.p, alpha, gf);
-                };
-                if constexpr (RCP <= 16) {
-                    if (fuse_gram) {
-                        run(k_wresid<RCP, NBK, true>, gram_wresid_smem<RCP>(Rc), GramFuse{gram->w, d.gpart.p});
-                        return;
-                    }
-                }
-                run(k_wresid<RCP, NBK, false>, wresid_smem(Rc), GramFuse{nullptr, nullptr});
+                allow_smem(k_wresid<RCP, NBK>, shm);
+                k_wresid<RCP, NBK><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, j0, Rc, x, d.b1.p,
+                                                                   alpha);
             });
             d.launches++;
         }
-    std::vector<double> gh(fuse_gram ? glen : 0);
-    if (fuse_gram) {
-        k_gram_sum<<<(glen + 7) / 8, 256, 0, st>>>(d.gpart.p, GRID_S, glen, d.gsum.p);
-        d.launches++;
-        CK(cudaMemcpyAsync(gh.data(), d.gsum.p, size_t(glen) * 8, cudaMemcpyDeviceToHost, st));
-    }
     if (S.seg.nfix) {
         d.along.alloc(size_t(S.seg.nfix) * r);
         k_seg_apply<double><<<GRID_T, THREADS, 0, st>>>(S, W, x, R, d.t.p, d.part.p, true, nullptr);
@@ -1848,11 +1821,6 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     CK(cudaGetLastError());
     if (want_coefs && coefs) CK(cudaMemcpyAsync(coefs, x, (m + g1) * r * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (fuse_gram) {
-        gram->g->assign(gh.begin(), gh.begin() + size_t(R) * R);
-        gram->ss->assign(gh.begin() + size_t(R) * R, gh.end());
-        info.gram = true;
-    }
     last_r_ = r;
     d.collect();
     info.iterations = iterations;

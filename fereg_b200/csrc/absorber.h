@@ -36,18 +36,6 @@ struct SolveInfo {
     u64 iterations = 0;
     bool escalated = false;
     bool exact = false;
-    bool gram = false;  // the residualization also summed the Gram (GramRequest)
-};
-
-// The weighted Gram of the residualized block (stats.rs:195) asked of residualize_device: when
-// the residualization runs as one pass of the short-segment kernel over all columns, that pass
-// also sums it, with row weights `w` (device memory, row order; null: 1), into `g` (R x R
-// row-major) and the plain sums of squares of the columns into `ss`. SolveInfo::gram says whether
-// it did.
-struct GramRequest {
-    const double* w = nullptr;
-    std::vector<double>* g = nullptr;
-    std::vector<double>* ss = nullptr;
 };
 
 // Precision of the inner PCG: FP64 throughout, or FP32 iterations inside FP64 refinement.
@@ -74,8 +62,7 @@ class DeviceAbsorber {
     virtual SolveInfo residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
                                   double* coefs, Precision prec = Precision::F64) = 0;
     virtual SolveInfo residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
-                                         const double* warm, double* coefs, Precision prec = Precision::F64,
-                                         const GramRequest* gram = nullptr) = 0;
+                                         const double* warm, double* coefs, Precision prec = Precision::F64) = 0;
     virtual SolveInfo residualize_device_warm_last(double* z_dev, size_t r, double tol, size_t maxiter,
                                                    Precision prec = Precision::F64) = 0;
     virtual void fit_rows(const double* coefs, size_t r, size_t col, double* out) const = 0;
@@ -121,8 +108,7 @@ class GpuAbsorber : public DeviceAbsorber {
     SolveInfo residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
                           double* coefs, Precision prec = Precision::F64) override;
     SolveInfo residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
-                                 const double* warm, double* coefs, Precision prec = Precision::F64,
-                                 const GramRequest* gram = nullptr) override;
+                                 const double* warm, double* coefs, Precision prec = Precision::F64) override;
     // The same, warm-started from the reduced solution the previous solve left on the device
     // (the IRLS warm start without the host round trip); the previous solve must have had the
     // same column count.
@@ -211,7 +197,7 @@ class GpuAbsorber : public DeviceAbsorber {
     void ensure_host_coord() const;
     void ensure_precond();
     SolveInfo solve(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
-                    double* coefs, Precision prec, bool warm_last = false, const GramRequest* gram = nullptr);
+                    double* coefs, Precision prec, bool warm_last = false);
     size_t last_r_ = 0;        // column count of the solution left in the solve scratch
     bool small_stale_ = false;  // the dense small factor was built for earlier weights
 };

@@ -639,13 +639,9 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     const bool want_coefs = out.d != nullptr;
     const size_t p_len = ab_->coefs_len();
     std::vector<double> coefs(want_coefs ? p_len * r : 0);
-    // the Gram comes out of the residualization pass when that pass can sum it
-    const double* wv = weighted ? d.wv.p : nullptr;
-    std::vector<double> g, ss_res;
-    GramRequest greq{wv, &g, &ss_res};
     const SolveInfo info =
     ab_->residualize_device(rows, r, spec.tol, spec.maxiter, want_coefs, nullptr, want_coefs ? coefs.data() : nullptr,
-                            spec.prec, &greq);
+                            spec.prec);
 
     // Outer products over the block: sum om a a^T of columns `cols` shifted by `shift` (+ the
     // constant), optionally the plain sums of squares; returns the full msz x msz matrix.
@@ -655,14 +651,14 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     return outer_products(src, nrows, srcR, cols, shift, cst, om, perm, ssq, ss_out);
     };
 
-    // Pass B: weighted Gram of the residualized block (stats.rs:195), unless the solve summed it
-    if (!info.gram) {
-        ph = d.begin(S_GRAM);
-        std::vector<int> all_cols(r);
-        std::iota(all_cols.begin(), all_cols.end(), 0);
-        g = outer(rows, n, R, all_cols, nullptr, false, wv, nullptr, true, &ss_res);
-        d.end(ph);
-    }
+    // Pass B: weighted Gram of the residualized block (stats.rs:195)
+    ph = d.begin(S_GRAM);
+    const double* wv = weighted ? d.wv.p : nullptr;
+    std::vector<int> all_cols(r);
+    std::iota(all_cols.begin(), all_cols.end(), 0);
+    std::vector<double> ss_res;
+    std::vector<double> g = outer(rows, n, R, all_cols, nullptr, false, wv, nullptr, true, &ss_res);
+    d.end(ph);
 
     // Collinearity, stage 1 (ols.rs:38 stage1_absorbed): a column absorbed by the FE
     const double ctol = std::min(1e-6, spec.tol / 10.0);

@@ -701,64 +701,15 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_rhs(DevStruct S, DevWeigh
     }
 }
 
-// The Gram of the residualized rows, fused into their pass (stats.rs:195), for one launch over
-// all columns (j0 = 0, Rc = R <= 16) on the FP64 tensor cores: after each chunk of rows the warp
-// stages the chunk (v and the row weights) in shared memory and adds G += (w v)' v over it by
-// mma.sync m8n8k4 f64 on the 8 x 8 blocks (I <= J) of the padded Gram; lane l holds row
-// 4 t + (l & 3), column 8 b + (l >> 2) of each block column b, which is its A fragment (times w)
-// and its B fragment. The plain sums of squares come from the lanes. Warps and CTAs add in a
-// fixed order.
-struct GramFuse {
-    const double* w;  // row weights of the Gram (null: 1)
-    double* part;     // per-CTA partials: R x R (row-major), then the R plain sums of squares
-};
-__host__ __device__ constexpr int gram_len(int R) { return R * R + R; }
-template <int RCP>
-struct GramShape {
-    static constexpr int G = 32 / RCP;
-    static constexpr int KN = WT / G;
-    static constexpr int CH = KN < 8 ? KN : 8;
-    static constexpr int CHR = CH > 4 ? 4 : CH;  // rows per group and chunk
-    static constexpr int ROWS = G * CHR;         // rows of a chunk (a multiple of 4)
-    static constexpr int NB8 = (RCP + 7) / 8;    // 8-column blocks
-    static constexpr int TS = NB8 * 8 + 1;       // staged row stride (doubles)
-    static constexpr int NBLK = NB8 * (NB8 + 1) / 2;
-    static constexpr size_t stage_bytes = al16(size_t(ROWS) * TS * 8) + al16(size_t(ROWS) * 8);
-    static constexpr size_t red_bytes = size_t(WPB) * (NBLK * 64 + 32) * 8;
-    static_assert(ROWS % 4 == 0, "chunks of whole MMA steps");
-};
-__device__ __forceinline__ void dmma884_acc(double& c0, double& c1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
-}
-// The sums of the fused Gram's per-CTA partials, one warp per element: lane l adds the partials
-// l, l + 32, ... in order, then a fixed butterfly (launch: 8 warps per CTA).
-__global__ void k_gram_sum(const double* __restrict__ part, int parts, int len, double* __restrict__ out) {
-    const int i = int(blockIdx.x) * 8 + int(threadIdx.x / 32);
-    const int lane = int(threadIdx.x % 32);
-    if (i >= len) return;  // whole warps leave together
-    double s = 0.0;
-    for (int p = lane; p < parts; p += 32) s += part[size_t(p) * len + i];
-#pragma unroll
-    for (int o = 16; o > 0; o /= 2) s += __shfl_xor_sync(FULL, s, o);
-    if (lane == 0) out[i] = s;
-}
-
 // Residualization of short segments (operator.rs:1107-1179): alpha_s = (b1_s - sum W_c u_c) / n1_s,
-// u_c = sum_b x[coord_b(c)]; every row of cell c loses alpha_s + u_c. With gf.part the Gram of
-// the residualized rows (above) comes out of the same pass.
-// GRAM: the Gram variant (RCP <= 16; its chunk stage follows the warps' tile parts).
-template <int RCP, int NBK, bool GRAM>
-__global__ void __launch_bounds__(WPB * 32, 4)
-    k_wresid(DevStruct S, DevWeights W, WarpTiles wt, double* __restrict__ rows, int R, int j0, int Rc,
-             const double* __restrict__ x, const double* __restrict__ b1, double* __restrict__ alpha, GramFuse gf) {
-    static_assert(!GRAM || RCP <= 16, "the fused Gram covers at most two 8-column blocks");
-    using L_t = Lanes<RCP>;
-    using GS = GramShape<RCP>;
-    constexpr int CHR = GRAM ? GS::CHR : L_t::CH;  // row loads in flight
-    constexpr int NBLK = GRAM ? GS::NBLK : 1;
+// u_c = sum_b x[coord_b(c)]; every row of cell c loses alpha_s + u_c.
+template <int RCP, int NBK>
+__global__ void __launch_bounds__(WPB * 32, 4) k_wresid(DevStruct S, DevWeights W, WarpTiles wt,
+                                                        double* __restrict__ rows, int R, int j0, int Rc,
+                                                        const double* __restrict__ x, const double* __restrict__ b1,
+                                                        double* __restrict__ alpha) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    using L_t = Lanes<RCP>;
     constexpr int G = L_t::G;
     constexpr int KS = (WSEG + G - 1) / G;  // tile segments per group
     unsigned char* mine = smem_raw + size_t(wid_in_cta()) * wresid_bytes(Rc);
@@ -772,18 +723,6 @@ __global__ void __launch_bounds__(WPB * 32, 4)
     const double* xj = x + j0 + L.j;
     double* vj = rows + j0 + L.j;
     const u32 ncode = NBK < WNB ? u32(NBK) : u32(WNB);
-    double gacc[NBLK][2], gss = 0.0;
-#pragma unroll
-    for (int q = 0; q < NBLK; q++) gacc[q][0] = gacc[q][1] = 0.0;
-    double* gT = nullptr;  // the chunk stage: ROWS x TS values, then ROWS row weights
-    double* gW = nullptr;
-    if constexpr (GRAM) {
-        unsigned char* gs = smem_raw + size_t(WPB) * wresid_bytes(Rc) + size_t(wid_in_cta()) * GS::stage_bytes;
-        gT = reinterpret_cast<double*>(gs);
-        gW = reinterpret_cast<double*>(gs + al16(size_t(GS::ROWS) * GS::TS * 8));
-        for (int q = int(wlane()); q < GS::ROWS * GS::TS; q += 32) gT[q] = 0.0;  // columns past RCP stay 0
-        __syncwarp();
-    }
     const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
     uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
     for (u32 tile = wid; tile < wt.n; tile += nw) {
@@ -836,89 +775,28 @@ __global__ void __launch_bounds__(WPB * 32, 4)
                 ps[sl * 32 + L.j] = al;
             }
         __syncwarp();
-        {
+        if (L.on) {
             const u32 r0 = trivial ? c0 : st.row0[0];
             const u32 nr = trivial ? nc : st.row0[nc] - r0;
 #pragma unroll
-            for (int k0 = 0; k0 < L_t::KN; k0 += CHR) {
-                double v[CHR];
+            for (int k0 = 0; k0 < L_t::KN; k0 += L_t::CH) {
+                double v[L_t::CH];
 #pragma unroll
-                for (int k = 0; k < CHR; k++) {
+                for (int k = 0; k < L_t::CH; k++) {
                     const u32 r = L.g + u32((k0 + k) * G);
-                    v[k] = (L.on && r < nr) ? __ldcs(vj + size_t(r0 + r) * Ru) : 0.0;
+                    v[k] = r < nr ? __ldcs(vj + size_t(r0 + r) * Ru) : 0.0;
                 }
 #pragma unroll
-                for (int k = 0; k < CHR; k++) {
+                for (int k = 0; k < L_t::CH; k++) {
                     const u32 r = L.g + u32((k0 + k) * G);
-                    double vn = 0.0;
-                    if (L.on && r < nr) {
+                    if (r < nr) {
                         const u32 i = trivial ? r : st.rcell[r];
-                        vn = v[k] - (ps[st.segl[i] * 32 + L.j] + u[i * Rc + L.j]);
-                        __stcs(vj + size_t(r0 + r) * Ru, vn);
+                        __stcs(vj + size_t(r0 + r) * Ru, v[k] - (ps[st.segl[i] * 32 + L.j] + u[i * Rc + L.j]));
                     }
-                    if constexpr (GRAM) {
-                        const int rr = k * G + int(L.g);
-                        gT[rr * GS::TS + int(L.j)] = vn;  // 0 on the inactive lanes and rows
-                        if (L.j == 0) gW[rr] = r < nr ? (gf.w ? gf.w[r0 + r] : 1.0) : 0.0;
-                        gss += vn * vn;
-                    }
-                }
-                if constexpr (GRAM) {
-                    __syncwarp();
-                    const int lr = int(wlane() & 3), lc = int(wlane() >> 2);
-#pragma unroll
-                    for (int ks = 0; ks < GS::ROWS / 4; ks++) {
-                        const int rr = ks * 4 + lr;
-                        const double wr = gW[rr];
-                        double bv[GS::NB8];
-#pragma unroll
-                        for (int bI = 0; bI < GS::NB8; bI++) bv[bI] = gT[rr * GS::TS + bI * 8 + lc];
-                        int q = 0;
-#pragma unroll
-                        for (int bI = 0; bI < GS::NB8; bI++)
-#pragma unroll
-                            for (int bJ = bI; bJ < GS::NB8; bJ++, q++) dmma884_acc(gacc[q][0], gacc[q][1], wr * bv[bI], bv[bJ]);
-                    }
-                    __syncwarp();
                 }
             }
         }
         __syncwarp();
-    }
-    if constexpr (GRAM) {
-        // the warps' blocks and the lanes' sums of squares in a fixed order (shared memory reused
-        // after the tiles)
-        __syncthreads();
-        constexpr int WS = NBLK * 64 + 32;
-        double* red = reinterpret_cast<double*>(smem_raw) + size_t(wid_in_cta()) * WS;
-        const int lane = int(wlane());
-#pragma unroll
-        for (int q = 0; q < NBLK; q++) {
-            red[q * 64 + (lane >> 2) * 8 + 2 * (lane & 3)] = gacc[q][0];
-            red[q * 64 + (lane >> 2) * 8 + 2 * (lane & 3) + 1] = gacc[q][1];
-        }
-        red[NBLK * 64 + lane] = gss;
-        __syncthreads();
-        const double* all = reinterpret_cast<const double*>(smem_raw);
-        for (int q = threadIdx.x; q < Rc * Rc + Rc; q += blockDim.x) {
-            double sum = 0.0;
-            if (q < Rc * Rc) {
-                int a = q / Rc, b = q % Rc;
-                if (a / 8 > b / 8) {
-                    const int t = a;
-                    a = b;
-                    b = t;
-                }
-                const int bI = a / 8, bJ = b / 8;
-                const int blk = bI * GS::NB8 - bI * (bI - 1) / 2 + (bJ - bI);
-                for (int w = 0; w < WPB; w++) sum += all[size_t(w) * WS + blk * 64 + (a % 8) * 8 + (b % 8)];
-            } else {
-                const int j = q - Rc * Rc;
-                for (int w = 0; w < WPB; w++)
-                    for (int g = 0; g < G; g++) sum += all[size_t(w) * WS + NBLK * 64 + g * RCP + j];
-            }
-            gf.part[size_t(blockIdx.x) * gram_len(Rc) + q] = sum;
-        }
     }
 }
 

@@ -482,7 +482,7 @@ SolveInfo GpuSlopeSolver::residualize(double* z, size_t r, double tol, size_t ma
 }
 
 SolveInfo GpuSlopeSolver::residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
-                                             const double* warm, double* coefs, Precision, const GramRequest*) {
+                                             const double* warm, double* coefs, Precision) {
     AllocScope alloc_scope(stream_);
     return solve(z_dev, r, tol, maxiter, want_coefs, warm, coefs, false);
 }

@@ -93,8 +93,7 @@ class GpuSlopeSolver : public DeviceAbsorber {
     SolveInfo residualize(double* z, size_t r, double tol, size_t maxiter, bool want_coefs, const double* warm,
                           double* coefs, Precision prec = Precision::F64) override;
     SolveInfo residualize_device(double* z_dev, size_t r, double tol, size_t maxiter, bool want_coefs,
-                                 const double* warm, double* coefs, Precision prec = Precision::F64,
-                                 const GramRequest* gram = nullptr) override;
+                                 const double* warm, double* coefs, Precision prec = Precision::F64) override;
     SolveInfo residualize_device_warm_last(double* z_dev, size_t r, double tol, size_t maxiter,
                                            Precision prec = Precision::F64) override;
     void fit_rows(const double* coefs, size_t r, size_t col, double* out) const override;
