@@ -43,7 +43,7 @@ OLS_SCALARS = ["N", "rank", "df_r", "df_m", "df_a", "df_a_initial", "df_a_redund
                "N_clustervars", "N_clust1", "N_clust2", "num_singletons", "N_full", "report_constant", "rss", "tss",
                "tss_within", "mss", "rmse", "r2", "r2_a", "r2_within", "r2_a_within", "ll", "ll_0", "F",
                "sumweights", "ic"]
-VCE = {"unadjusted": 0, "robust": 1, "cluster": 2}
+VCE = {"unadjusted": 0, "robust": 1, "cluster": 2, "crv3": 3, "hc2": 4, "hc3": 5}
 WEIGHT_KIND = {None: 0, "aweight": 1, "fweight": 2, "pweight": 3}
 
 
@@ -457,10 +457,12 @@ class Session:
     weight_kind ("aweight", "fweight", "pweight") or None."""
 
     def __init__(self, codes, g, clusters=(), cl_g=(), w=None, weight_kind=None, num_singletons=0, intercept=None,
-                 slopes=None):
+                 slopes=None, n=None):
         """intercept / slopes: the terms' shapes as for Absorber (slope terms make the session's
-        absorber the slope solver and add one dof slot per slope)."""
-        n = len(codes[0]) if len(codes) else len(clusters[0]) if len(clusters) else len(w)
+        absorber the slope solver and add one dof slot per slope); n: the rows, when neither terms,
+        clusters nor weights give it (no absorbed terms: the constant alone)."""
+        if n is None:
+            n = len(codes[0]) if len(codes) else len(clusters[0]) if len(clusters) else len(w)
         self._codes = [np.ascontiguousarray(c, dtype=np.uint32) for c in codes]
         self._cl = [np.ascontiguousarray(c, dtype=np.uint32) for c in clusters]
         garr = np.asarray(g, dtype=np.uint32)

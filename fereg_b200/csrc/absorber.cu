@@ -1847,6 +1847,21 @@ void GpuAbsorber::phase_times(double* ms, u64* counts) const {
 
 u64 GpuAbsorber::launches() const { return d_->launches; }
 
+void GpuAbsorber::fe_leverage_device(double* h_dev) {
+    AllocScope alloc_scope(stream_);
+    ensure_precond();
+    if (small_stale_ && small_ok_ && hs_.m_small == hs_.m) refresh_small();  // the current weights' factor
+    if (hs_.m > 0 && !(small_ok_ && hs_.m_small == hs_.m))
+        throw Error(RC_INVALID_INPUT,
+                    "fereg: the exact FE leverage (HC2/HC3) needs a reduced system of at most 1024 coordinates");
+    const DevStruct S = d_->ds(hs_);
+    k_fe_leverage<<<std::max(1u, std::min<u32>((hs_.g1 + 127) / 128, 148 * 8)), 128, 0, stream_>>>(
+        S, d_->dw(), hs_.m ? d_->minv.p : nullptr, h_dev);
+    d_->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+}
+
 void GpuAbsorber::solver_stats(u64* o) const {
     o[0] = d_->graph_captures;
     o[1] = d_->graph_launches;

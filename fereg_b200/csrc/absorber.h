@@ -76,6 +76,9 @@ class DeviceAbsorber {
     virtual void set_ctx(const Ctx& c) = 0;
     virtual size_t escalated_blocks() const { return 0; }
     virtual u64 escalations() const { return 0; }
+    // Exact leverage of the FE columns per row (leverage.rs:128 fe_hat), row order, into device
+    // memory (n values).
+    virtual void fe_leverage_device(double* h_dev) = 0;
 };
 
 class GpuAbsorber : public DeviceAbsorber {
@@ -159,6 +162,9 @@ class GpuAbsorber : public DeviceAbsorber {
     // aligned); a call that needs more is rejected (198).
     void rhs_device_scratch(const double* rows, size_t r, double* rhs, double* b1, double* colsum, double* scratch,
                             size_t cap);
+    // The reduced system must be held by the dense small factor (at most 1024 coordinates, or
+    // none); larger systems are rejected (198) rather than approximated.
+    void fe_leverage_device(double* h_dev) override;
     // Weight state (n1, nr, diag, redundant) as held for the kernels.
     void weight_state(double* n1, double* nr, double* diag, uint8_t* red, double* sw) const;
 

@@ -232,5 +232,51 @@ inline bool fix_psd(Mat& v, size_t k, bool constant) {
     return true;
 }
 
+// fixest's collinearity rule by Cholesky with exclusions (vcov.rs:124-200 chol_collin): column j
+// is excluded when its pivot a_jj - sum over the kept earlier columns of r_ij^2 is below tol
+// (or NaN); returns the inverse of the kept columns' block (kept x kept, in column order).
+inline Mat chol_collin(const Mat& a, size_t k, double tol, std::vector<bool>& excluded) {
+    Mat r(k * k, 0.0);
+    excluded.assign(k, false);
+    for (size_t j = 0; j < k; j++) {
+        double rjj = a[j * k + j];
+        for (size_t i = 0; i < j; i++)
+            if (!excluded[i]) rjj -= r[i * k + j] * r[i * k + j];
+        if (!(rjj >= tol)) {
+            excluded[j] = true;
+            continue;
+        }
+        const double d = std::sqrt(rjj);
+        r[j * k + j] = d;
+        for (size_t c = j + 1; c < k; c++) {
+            double v = a[c * k + j];
+            for (size_t i = 0; i < j; i++)
+                if (!excluded[i]) v -= r[i * k + c] * r[i * k + j];
+            r[j * k + c] = v / d;
+        }
+    }
+    std::vector<size_t> kept;
+    for (size_t j = 0; j < k; j++)
+        if (!excluded[j]) kept.push_back(j);
+    const size_t m = kept.size();
+    Mat ri(m * m, 0.0);
+    for (size_t c = 0; c < m; c++) {
+        ri[c * m + c] = 1.0 / r[kept[c] * k + kept[c]];
+        for (size_t row = c; row-- > 0;) {
+            double s = 0.0;
+            for (size_t l = row + 1; l <= c; l++) s += r[kept[row] * k + kept[l]] * ri[l * m + c];
+            ri[row * m + c] = -s / r[kept[row] * k + kept[row]];
+        }
+    }
+    Mat inv(m * m, 0.0);
+    for (size_t i = 0; i < m; i++)
+        for (size_t j = i; j < m; j++) {
+            double s = 0.0;
+            for (size_t l = j; l < m; l++) s += ri[i * m + l] * ri[j * m + l];
+            inv[i * m + j] = inv[j * m + i] = s;
+        }
+    return inv;
+}
+
 }  // namespace la
 }  // namespace fereg

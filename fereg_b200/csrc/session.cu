@@ -21,6 +21,7 @@
 #include "boot.cuh"
 #include "glm.cuh"
 #include "relu.cuh"
+#include "crv3.cuh"
 #include "session_dev.h"
 #include "stats.cuh"
 
@@ -189,6 +190,7 @@ GpuSession::GpuSession(const std::vector<const u32*>& codes, const std::vector<u
         s.coff.upload(coff, d.st);
         s.G = G;
         s.sign = dims.size() % 2 == 1 ? 1.0 : -1.0;
+        s.kc = std::move(kc);
     }
     CK(cudaStreamSynchronize(d.st));
 }
@@ -620,12 +622,24 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     const double bigN = kind == 2 ? sumw : double(n);
     int vce = spec.vce;
     if (vce == 0 && kind == 3) vce = 1;  // ols.rs:150 pweights imply robust
-    if (vce == 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg ols: cluster variance without clusters");
+    if (vce < 0 || vce > 5) throw Error(RC_INVALID_INPUT, "fereg ols: unknown variance");
+    if (vce == 5 && kind == 3) throw Error(RC_INVALID_INPUT, "pweights not allowed with option vce(hc3)");  // ols.rs:251
+    if (vce >= 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg ols: cluster variance without clusters");
+    if (vce == 3 && (kind == 2 || !dynamic_cast<GpuAbsorber*>(ab_.get())))
+        throw Error(RC_INVALID_INPUT, "fereg ols: CRV3 needs intercept-only terms and no fweights");
+    const bool clustered = vce >= 2;
     const bool has_intercept = true;  // intercept-only terms (or noabsorb) contain the constant
     const bool report_constant = has_intercept && !spec.noconstant;
+    // CRV3 refits start from the raw rows (row order)
+    std::vector<double> raw_h;
+    if (vce == 3) {
+        raw_h.resize(n * r);
+        CK(cudaMemcpyAsync(raw_h.data(), rows, n * r * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
 
     // the dof pass runs on its own stream beside the column statistics and the solve
-    std::future<Dof> dof_job = dof_begin(vce == 2, spec.firstpair != 0, spec.want_groupvar != 0 && out.groupvar);
+    std::future<Dof> dof_job = dof_begin(clustered, spec.firstpair != 0, spec.want_groupvar != 0 && out.groupvar);
     int ph = d.begin(S_COLSTATS);
 
     // Pass A: column statistics of the raw rows (stats.rs:40), raw weights, in one device pass
@@ -785,7 +799,23 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
         la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
         standardize(meat);
         v_s = la::sandwich(bread, meat, msz, bigN / (bigN - df_a - df_m));
-    } else {
+    } else if (vce == 4 || vce == 5) {
+        // ols.rs:450-474: the full design's leverage h = h_FE + w_v x~'(X~'WX~)^-1 x~, then the
+        // regress HC2 / HC3 multipliers (ols/stata_vce.rs:156-167) in the robust meat, no factor
+        d.h.alloc(n);
+        ab_->fe_leverage_device(d.h.p);
+        DBuf<double> ginv;
+        ginv.upload(fit_.A.empty() ? std::vector<double>{0.0} : fit_.A, st);
+        d.om.alloc(n);
+        if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+        k_hc_weights<<<blocks_for(n, 256), 256, 0, st>>>(rows, R, d.col.p, int(k), ginv.p, d.e.p, wv, d.h.p,
+                                                         kind == 2 ? 1 : 0, vce == 5 ? 1 : 0, n, d.om.p);
+        d.launches++;
+        const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+        la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
+        standardize(meat);
+        v_s = la::sandwich(bread, meat, msz, 1.0);
+    } else if (vce == 2) {
         d.om.alloc(n);
         k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 1, d.om.p);
         d.launches++;
@@ -813,11 +843,19 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
         fit_.ok = true;
         v_s = la::sandwich(bread, meat, msz, q_cluster);
         if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
+    } else {
+        const la::Mat meat = crv3_meat(rows, raw_h, R, kept, beta, wmean, report_constant, g);
+        const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
+        const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
+        for (size_t a = 0; a < msz; a++)
+            for (size_t b = 0; b < msz; b++)
+                v_s[a * msz + b] = q_cluster * meat[a * msz + b] * sc[a] * sc[b] / (sd_y * sd_y);
+        if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
     }
     }
     d.end(ph);
     d.collect();
-    if (vce == 2) df_r = std::min(df_r, g_min - 1.0);
+    if (clustered) df_r = std::min(df_r, g_min - 1.0);
     for (size_t i = 0; i < msz; i++)
     for (size_t j = 0; j < i; j++) v_s[j * msz + i] = v_s[i * msz + j];
 
@@ -872,10 +910,10 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     out.df_a_initial = double(dof.df_a_initial);
     out.df_a_redundant = double(dof.df_a_redundant);
     out.df_a_nested = double(dof.df_a_nested);
-    out.N_clust = vce == 2 ? g_min : nanv();
-    out.N_clustervars = vce == 2 ? double(ccodes_.size()) : nanv();
-    out.N_clust1 = vce == 2 && !cg_.empty() ? double(cg_[0]) : nanv();
-    out.N_clust2 = vce == 2 && cg_.size() > 1 ? double(cg_[1]) : nanv();
+    out.N_clust = clustered ? g_min : nanv();
+    out.N_clustervars = clustered ? double(ccodes_.size()) : nanv();
+    out.N_clust1 = clustered && !cg_.empty() ? double(cg_[0]) : nanv();
+    out.N_clust2 = clustered && cg_.size() > 1 ? double(cg_[1]) : nanv();
     out.num_singletons = double(nsing_);
     out.N_full = bigN + double(nsing_);
     out.report_constant = report_constant ? 1.0 : 0.0;
@@ -1795,6 +1833,171 @@ void GpuSession::relu_separation(double* rows_in, bool on_device, size_t nx, con
     if (out.certificate) CK(cudaMemcpyAsync(out.certificate, cert.p, n * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
+}
+
+// crv3.rs:84-426 for OLS on the device: beta_(-g) for every cluster g of every subset of the
+// cluster dimensions. Closed form when every FE term is nested in the subset's clusters (leaving g
+// out removes whole FE levels, so the residualized block restricted to the other rows is theirs):
+// the weighted Gram of all rows minus g's own (k_cluster_grams). Otherwise a refit: the rows
+// outside g with their FE levels renumbered, a device absorber built on them, the raw [y, x]
+// residualized and its Gram. Each solve is fixest's collinearity rule (vcov.rs:124 chol_collin,
+// tol 1e-9; a coefficient it removes is an error). With a reported constant every refit gets the
+// regression-through-the-means constant of its sample (ols/stata_vce.rs:572-600, raw weights).
+// The meat is sum_S sign_S sum_g (theta_(-g) - theta)(theta_(-g) - theta)'.
+std::vector<double> GpuSession::crv3_meat(const double* rows, const std::vector<double>& raw_h, int R,
+                                          const std::vector<size_t>& kept, const std::vector<double>& beta,
+                                          const std::vector<double>& wmean, bool report_constant,
+                                          const std::vector<double>& g) {
+    constexpr double COLLIN_TOL = 1e-9;  // fit/mod.rs:325
+    SessionDev& d = *d_;
+    const cudaStream_t st = d.st;
+    const size_t n = n_, r = size_t(R), k = kept.size(), k1 = 1 + k;
+    const std::vector<u32>& pi = ab_->row_order();
+    const size_t kt = k + (report_constant ? 1 : 0);
+    std::vector<double> theta(beta.begin(), beta.end());
+    if (report_constant) {
+        double b0 = wmean[0];
+        for (size_t a = 0; a < k; a++) b0 -= wmean[kept[a]] * beta[a];
+        theta.push_back(b0);
+    }
+    std::vector<int> cols(k1, 0);
+    for (size_t a = 0; a < k; a++) cols[1 + a] = int(kept[a]);
+    std::vector<double> wr(n, 1.0);  // raw weights, row order
+    if (!wk_.empty())
+        for (size_t i = 0; i < n; i++) wr[i] = wk_[pi[i]];
+    const double* wv = wk_.empty() ? nullptr : d.wv.p;
+    // beta from the Gram C of [y, x] (k1 x k1)
+    auto solve = [&](const std::vector<double>& C, u32 cluster) {
+        la::Mat cxx(k * k);
+        for (size_t a = 0; a < k; a++)
+            for (size_t b = 0; b < k; b++) cxx[a * k + b] = C[(1 + a) * k1 + 1 + b];
+        std::vector<bool> excl;
+        const la::Mat inv = la::chol_collin(cxx, k, COLLIN_TOL, excl);
+        for (size_t a = 0; a < k; a++)
+            if (excl[a]) {
+                std::ostringstream os;
+                os << "CRV3: regressor " << a << " is not estimable without cluster " << cluster;
+                throw Error(RC_INVALID_INPUT, os.str());
+            }
+        std::vector<double> b(k, 0.0);
+        for (size_t a = 0; a < k; a++)
+            for (size_t c = 0; c < k; c++) b[a] += inv[a * k + c] * C[(1 + c) * k1];
+        return b;
+    };
+    std::vector<double> meat(kt * kt, 0.0);
+    DBuf<int> dcol;
+    dcol.upload(cols, st);
+    for (auto& sub : d.subsets) {
+        const u32 G = sub.G;
+        std::vector<u32> cl(n);  // cluster of every row (row order)
+        for (size_t i = 0; i < n; i++) cl[i] = sub.kc[pi[i]];
+        bool nested_all = true;
+        for (size_t q = 0; q < tcodes_.size() && nested_all; q++) {
+            std::vector<u32> map(tg_[q], UINT32_MAX);
+            for (size_t i = 0; i < n && nested_all; i++) {
+                u32& m = map[tcodes_[q][i]];
+                if (m == UINT32_MAX) m = sub.kc[i];
+                else nested_all = m == sub.kc[i];
+            }
+        }
+        std::vector<double> betas(size_t(G) * k);
+        if (nested_all) {
+            d.cgram.alloc(std::max<size_t>(1, size_t(G) * k1 * k1));
+            k_cluster_grams<<<std::min<u32>(G, 148 * 8), 128, 0, st>>>(rows, R, dcol.p, int(k1), wv, sub.perm.p,
+                                                                      sub.coff.p, G, d.cgram.p);
+            d.launches++;
+            std::vector<double> cg(size_t(G) * k1 * k1);
+            CK(cudaMemcpyAsync(cg.data(), d.cgram.p, cg.size() * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            CK(cudaGetLastError());
+            std::vector<double> C(k1 * k1);
+            for (u32 gg = 0; gg < G; gg++) {
+                for (size_t a = 0; a < k1; a++)
+                    for (size_t b = 0; b < k1; b++)
+                        C[a * k1 + b] = g[size_t(cols[a]) * r + size_t(cols[b])] - cg[(size_t(gg) * k1 + a) * k1 + b];
+                const std::vector<double> b = solve(C, gg);
+                std::copy(b.begin(), b.end(), betas.begin() + size_t(gg) * k);
+            }
+        } else {
+            for (u32 gg = 0; gg < G; gg++) {
+                ab_->ctx().check();
+                std::vector<u32> idx;  // rows (row order) of the leave-out sample
+                for (size_t i = 0; i < n; i++)
+                    if (cl[i] != gg) idx.push_back(u32(i));
+                const size_t m = idx.size();
+                std::vector<std::vector<u32>> sc(tcodes_.size());
+                std::vector<const u32*> sp;
+                std::vector<u32> sg;
+                for (size_t q = 0; q < tcodes_.size(); q++) {
+                    std::vector<u32> map(tg_[q], UINT32_MAX);
+                    for (u32 i : idx) map[tcodes_[q][pi[i]]] = 0;
+                    u32 next = 0;
+                    for (auto& v : map)
+                        if (v == 0) v = next++;
+                    sc[q].resize(m);
+                    for (size_t j = 0; j < m; j++) sc[q][j] = map[tcodes_[q][pi[idx[j]]]];
+                    sp.push_back(sc[q].data());
+                    sg.push_back(next);
+                }
+                std::vector<double> ws;
+                if (!wk_.empty()) {
+                    ws.resize(m);
+                    for (size_t j = 0; j < m; j++) ws[j] = wk_[pi[idx[j]]];
+                }
+                GpuAbsorber sab(sp, sg, ws.empty() ? nullptr : ws.data(), m, ab_->ctx());
+                const std::vector<u32>& spi = sab.row_order();
+                std::vector<u32> gidx(m);
+                for (size_t t = 0; t < m; t++) gidx[t] = idx[spi[t]];
+                DBuf<u32> didx;
+                didx.upload(gidx, st);
+                d.jk.alloc(m * k1);
+                // the raw rows of the sample, from the host copy
+                std::vector<double> blk(m * k1);
+                for (size_t t = 0; t < m; t++)
+                    for (size_t a = 0; a < k1; a++) blk[t * k1 + a] = raw_h[size_t(gidx[t]) * r + size_t(cols[a])];
+                CK(cudaMemcpyAsync(d.jk.p, blk.data(), blk.size() * 8, cudaMemcpyHostToDevice, st));
+                CK(cudaStreamSynchronize(st));
+                sab.residualize_device(d.jk.p, k1, 1e-14, 100000, false, nullptr, nullptr);
+                DBuf<double> wsub;
+                if (!ws.empty()) {
+                    std::vector<double> wsr(m);
+                    for (size_t t = 0; t < m; t++) wsr[t] = ws[spi[t]];
+                    wsub.upload(wsr, st);
+                }
+                std::vector<int> all(k1);
+                std::iota(all.begin(), all.end(), 0);
+                const std::vector<double> C =
+                    outer_products(d.jk.p, m, int(k1), all, nullptr, false, ws.empty() ? nullptr : wsub.p, nullptr,
+                                   false, nullptr);
+                const std::vector<double> b = solve(C, gg);
+                std::copy(b.begin(), b.end(), betas.begin() + size_t(gg) * k);
+            }
+        }
+        // per-cluster raw sums for the refits' constants
+        std::vector<double> cs(size_t(G) * (1 + k1), 0.0), tot(1 + k1, 0.0);
+        for (size_t i = 0; i < n; i++) {
+            double* row = &cs[size_t(cl[i]) * (1 + k1)];
+            row[0] += wr[i];
+            for (size_t a = 0; a < k1; a++) row[1 + a] += wr[i] * raw_h[i * r + size_t(cols[a])];
+        }
+        for (u32 gg = 0; gg < G; gg++)
+            for (size_t a = 0; a <= k1; a++) tot[a] += cs[size_t(gg) * (1 + k1) + a];
+        std::vector<double> dv(kt);
+        for (u32 gg = 0; gg < G; gg++) {
+            const double* b = &betas[size_t(gg) * k];
+            for (size_t a = 0; a < k; a++) dv[a] = b[a] - theta[a];
+            if (report_constant) {
+                const double* row = &cs[size_t(gg) * (1 + k1)];
+                const double sw = tot[0] - row[0];
+                double b0 = (tot[1] - row[1]) / sw;
+                for (size_t a = 0; a < k; a++) b0 -= b[a] * (tot[2 + a] - row[2 + a]) / sw;
+                dv[k] = b0 - theta[k];
+            }
+            for (size_t a = 0; a < kt; a++)
+                for (size_t c = 0; c < kt; c++) meat[a * kt + c] += sub.sign * dv[a] * dv[c];
+        }
+    }
+    return meat;
 }
 
 }  // namespace fereg

@@ -174,6 +174,12 @@ class GpuSession {
     std::vector<std::vector<u64>> slope_red_;
     bool irls_weights_ = false;  // a GLM call left its IRLS weights on the absorber
     void restore_weights();
+    // CRV3 (crv3.rs, ols/stata_vce.rs:516-545): the jackknife meat of [b, _cons] over the cluster
+    // subsets; rows: the residualized block (device), raw_h: the raw rows (host, row order),
+    // g: the weighted Gram of the residualized block.
+    std::vector<double> crv3_meat(const double* rows, const std::vector<double>& raw_h, int R,
+                                  const std::vector<size_t>& kept, const std::vector<double>& beta,
+                                  const std::vector<double>& wmean, bool report_constant, const std::vector<double>& g);
 
     struct DofSlot {
         u64 k = 0, m = 0;

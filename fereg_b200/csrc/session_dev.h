@@ -44,6 +44,7 @@ struct SessionDev {
         DBuf<u32> coff;  // G + 1
         u32 G = 0;
         double sign = 1.0;
+        std::vector<u32> kc;  // host: the combined cluster code of every kept observation
     };
     std::vector<Subset> subsets;
     DBuf<double> w_raw, wv;  // row order
@@ -51,6 +52,8 @@ struct SessionDev {
     DBuf<int> col, err;
     DBuf<u32> map;
     DBuf<double> pstat;
+    DBuf<double> cgram, jk;  // CRV3: per-cluster Grams, a leave-out block
+    DBuf<double> h;          // HC2 / HC3: the FE leverage per row
     DBuf<double> colbuf;  // kept-order columns of a gather
     DBuf<u32> pi;         // row order -> kept position
     cudaStream_t st = nullptr;

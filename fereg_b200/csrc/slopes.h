@@ -105,6 +105,9 @@ class GpuSlopeSolver : public DeviceAbsorber {
     void solver_stats(u64* out4) const override;
     const Ctx& ctx() const override { return ctx_; }
     void set_ctx(const Ctx& c) override { ctx_ = c; }
+    void fe_leverage_device(double*) override {
+        throw Error(RC_INVALID_INPUT, "fereg: the exact FE leverage (HC2/HC3) of slope terms is not built");
+    }
 
     const SlopeHost& structure() const { return hs_; }
     // The weight state: M_s^+ of every level of E (ge x be^2), the block-Jacobi inverses and

@@ -322,4 +322,38 @@ __global__ void k_srow_sum(const double* __restrict__ part, const u32* __restric
     }
 }
 
+// Exact leverage of the fixed-effect columns per row (leverage.rs:128 fe_hat, by block
+// elimination of FE1): h_i = w_i (1 / W_s + v_c' G v_c) for row i of cell c in segment s, where
+// v_c = b_c - t_s, b_c the indicator of c's reduced coordinates, t_s = sum_{c' in s} W_c' b_c' / W_s
+// and G a generalized inverse of the reduced system S (any one: v_c lies in the range of
+// S = sum_c W_c v_c v_c'). G: the dense m x m inverse. One thread per segment, cells in order.
+__global__ void k_fe_leverage(DevStruct S, DevWeights W, const double* __restrict__ G, double* __restrict__ h) {
+    const u32 m = S.m, M = S.M;
+    for (u32 s = blockIdx.x * blockDim.x + threadIdx.x; s < S.g1; s += gridDim.x * blockDim.x) {
+        const u32 c0 = S.seg_off[s], c1 = S.seg_off[s + 1];
+        const double winv = W.n1inv[s];
+        // B(c, c') = b_c' G b_c'
+        auto B = [&](u32 c, u32 c2) {
+            double v = 0.0;
+            for (u32 k = 0; k < S.nb; k++)
+                for (u32 l = 0; l < S.nb; l++)
+                    v += G[size_t(S.coord[size_t(k) * M + c]) * m + S.coord[size_t(l) * M + c2]];
+            return v;
+        };
+        double tau = 0.0;  // t' G t
+        for (u32 c = c0; c < c1; c++) {
+            double row = 0.0;
+            for (u32 c2 = c0; c2 < c1; c2++) row += cellw(W, c2) * B(c, c2);
+            tau += cellw(W, c) * row;
+        }
+        tau *= winv * winv;
+        for (u32 c = c0; c < c1; c++) {
+            double gt = 0.0;  // b_c' G t
+            for (u32 c2 = c0; c2 < c1; c2++) gt += cellw(W, c2) * B(c, c2);
+            const double q = m ? B(c, c) - 2.0 * gt * winv + tau : 0.0;
+            for (u32 i = row0_of(S, c); i < row1_of(S, c); i++) h[i] = (W.w_rows ? W.w_rows[i] : 1.0) * (winv + q);
+        }
+    }
+}
+
 }  // namespace fereg

@@ -168,7 +168,10 @@ int fereg_absorber_weight_state(const fereg_absorber* h, double* n1, double* nr,
 typedef struct fereg_session fereg_session;
 
 /* ols.rs Spec: vce 0 unadjusted, 1 robust (HC1), 2 cluster (CRV1 over all the session's cluster
- * dimensions, multiway by inclusion-exclusion); firstpair: dof from the first FE pair only
+ * dimensions, multiway by inclusion-exclusion), 3 CRV3 (the leave-one-cluster-out jackknife,
+ * crv3.rs, over the same subsets; intercept-only terms, no fweights), 4 HC2, 5 HC3 (Stata regress
+ * with the exact leverage of the FE columns, leverage.rs:128 and ols.rs:450-474; the reduced
+ * system must fit the dense small factor, at most 1024 coordinates); firstpair: dof from the first FE pair only
  * (dof.rs DofOptions); want_groupvar: mobility groups of the first pair into out->groupvar. */
 typedef struct fereg_ols_spec {
     int vce;

@@ -257,6 +257,54 @@ def main_separation(ref):
     print(f"wrote {len(out)} separation fixtures")
 
 
+# tests/vce.rs:557-615: CRV3 fixtures of OLS on vce_cs.csv (do-file jackknife loops of reghdfe).
+CRV3_SPECS = [
+    dict(name="crv3_ols_nested", y="y", x=["x1", "x2"], absorb=["f1", "f2"], cluster=["c"], weight=None,
+         weight_kind=None),
+    dict(name="crv3_ols_aw", y="y", x=["x1", "x2"], absorb=["f1", "f2"], cluster=["c"], weight="w",
+         weight_kind="aweight"),
+    dict(name="crv3_ols_c2", y="y", x=["x1", "x2"], absorb=["f2"], cluster=["c2"], weight=None, weight_kind=None),
+    dict(name="crv3_ols_twoway", y="y", x=["x1", "x2"], absorb=["f2"], cluster=["c", "c2"], weight=None,
+         weight_kind=None),
+]
+VCE_CS_COLUMNS = ["f1", "f2", "c", "c2", "z1", "z2", "x1", "x2", "en", "y", "yp", "w", "fw"]
+
+
+# tests/vce.rs:509-550: Stata 19 `regress y x1 x2 i.f1 i.f2, vce(hc2|hc3)` on vce_cs.csv (the x
+# block compared with absorbed f1 f2; all of b and V without them).
+HC_SPECS = [dict(name=f"{hc}_{wt}", hc=hc, absorb=(wt != "noabsorb"),
+                 weight={"aw": "w", "pw": "w", "fw": "fw"}.get(wt),
+                 weight_kind={"aw": "aweight", "pw": "pweight", "fw": "fweight"}.get(wt))
+            for hc in ("hc2", "hc3") for wt in ("none", "aw", "fw", "noabsorb") + (("pw",) if hc == "hc2" else ())]
+
+
+def main_hc(ref):
+    data_dir = os.path.join(ref, "crates", "fereg-core", "tests", "data")
+    out = []
+    for spec in HC_SPECS:
+        with open(os.path.join(data_dir, f"vce_{spec['name']}.json")) as f:
+            j = json.load(f)
+        sc = {k: j["scalars"].get(k) for k in ("N", "df_r")}
+        out.append(dict(spec=spec, cmdline=j["cmdline"], b=j["b"], V=j["V"], sample=j["sample"], scalars=sc))
+    with open(os.path.join(HERE, "hc_fixtures.json"), "w") as f:
+        json.dump(out, f)
+    print(f"wrote {len(out)} HC2 / HC3 fixtures")
+
+
+def main_crv3(ref):
+    data_dir = os.path.join(ref, "crates", "fereg-core", "tests", "data")
+    copy_csv(os.path.join(data_dir, "vce_cs.csv"), os.path.join(HERE, "vce_cs.csv"), VCE_CS_COLUMNS)
+    out = []
+    for spec in CRV3_SPECS:
+        with open(os.path.join(data_dir, f"vce_{spec['name']}.json")) as f:
+            j = json.load(f)
+        sc = {k: j["scalars"].get(k) for k in ("N", "N_clust", "df_r", "df_a", "num_singletons")}
+        out.append(dict(spec=spec, cmdline=j["cmdline"], b=j["b"], V=j["V"], sample=j["sample"], scalars=sc))
+    with open(os.path.join(HERE, "crv3_fixtures.json"), "w") as f:
+        json.dump(out, f)
+    print(f"wrote {len(out)} CRV3 fixtures")
+
+
 def main_poisson(ref):
     data_dir = os.path.join(ref, "crates", "fereg-core", "tests", "data")
     for name, cols in POISSON_DATA.items():
@@ -281,3 +329,5 @@ if __name__ == "__main__":
     main_iv_logit(ref)
     main_poisson(ref)
     main_separation(ref)
+    main_crv3(ref)
+    main_hc(ref)
