@@ -42,6 +42,9 @@ CONFIGS = {
     # (bench/dgp.py:55,70): n_ind / 23 = 43,478 firms, firm = row mod 43,478. 43,478 is not a
     # multiple of 10, so the individuals' runs of 10 consecutive firms wrap into one ring.
     "c2d": dict(n_ind=1_000_000, years=10, n_firm=43_478, k=10, seed=10**7 * 100 + 47),
+    # The C2 shape at 3e6 rows (3e5 indiv x 10 years, firm = row mod 3e4; 264 MB of rows, above
+    # L2): the case of the full ncu captures, which must stay a few GB on the device.
+    "c2p": dict(n_ind=300_000, years=10, n_firm=30_000, k=10, seed=10**7 * 100 + 45),
     # OLS y ~ x1 | indiv + year, n = 1e4 indiv x 10 years.
     "c1": dict(n_ind=10_000, years=10, n_firm=0, k=1, seed=10**5 * 100 + 42),
     # WCR11 wild cluster bootstrap of b_x1 (H0 true): y ~ x1 | indiv + year + firm, cluster firm,
@@ -627,6 +630,8 @@ def roofline_of(sess, phases, n, R, weighted, s_v, workload):
     info = sess if isinstance(sess, dict) else sess.info()
     algo = phase_bytes(info, n, R, weighted, s_v)
     timed = {k: v for k, v in phases.items() if k in algo and v[1]}
+    if not timed:  # no profiled calls (--prof-steps 0)
+        return None
     dom = max(timed, key=lambda k: timed[k][0])
     ms, cnt = timed[dom]
     achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
@@ -741,6 +746,8 @@ def workload_name(cfg_name):
         return "OLS y~x1..x10 | indiv(1e6)+firm(1e5, row mod 1e5)+year(10), n=1e7, iid SEs"
     if cfg_name == "c2d":
         return "OLS y~x1..x10 | indiv(1e6)+firm(43478, row mod 43478: connected ring)+year(10), n=1e7, iid SEs"
+    if cfg_name == "c2p":
+        return "OLS y~x1..x10 | indiv(3e5)+firm(3e4, row mod 3e4)+year(10), n=3e6, iid SEs (profiling case)"
     return "OLS y~x1 | indiv(1e4)+year(10), n=1e5, iid SEs"
 
 
@@ -1113,11 +1120,12 @@ def main():
     hbm, peak_kind = peaks()
     algo = phase_bytes(info, n, R, False, 8 if prec == fb.PREC_F64 else 4)
     timed = {k: v for k, v in phases.items() if k in algo and v[1]}
-    dom = max(timed, key=lambda k: timed[k][0])
-    ms, cnt = timed[dom]
-    achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
-    kern = PHASE_KERNEL[dom]
-    traffic = traffic_from_profiles(kern, args.config)
+    dom = max(timed, key=lambda k: timed[k][0]) if timed else None  # none without profiled calls
+    if dom:
+        ms, cnt = timed[dom]
+        achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
+        kern = PHASE_KERNEL[dom]
+        traffic = traffic_from_profiles(kern, args.config)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1158,8 +1166,8 @@ def main():
                        "b_x1": float(res["b"][0]), "solver_stats": sess.solver_stats()},
             "roofline": {"bound": "hbm", "kernel": kern, "phase": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes": algo[dom]},
-            "phases_ms_per_step": {k: v[0] / args.prof_steps for k, v in phases.items() if v[1]},
+                         "algorithmic_bytes": algo[dom]} if dom else None,
+            "phases_ms_per_step": {k: v[0] / max(1, args.prof_steps) for k, v in phases.items() if v[1]},
             "phases_note": PHASES_NOTE,
             "cpu_baseline": cpu,
             "parity": parity,

@@ -12,6 +12,8 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <mutex>
 #include <sstream>
 #include <type_traits>
 
@@ -216,6 +218,12 @@ struct Scratch {
         u64 body_launches = 0;  // kernels of one body
     };
     std::vector<PcgGraph> graphs;
+    // grids of the S*P passes chosen by the autotuner, per (padded width, element size)
+    struct ApplyGrids {
+        int seg = 148 * 4, pull = 148 * 4;
+    };
+    std::map<std::pair<int, int>, ApplyGrids> grids;
+    double tune_us = 0;  // host time of the tuning runs
     u64 graph_launches = 0, graph_captures = 0;
     u64 fp64_finishes = 0;  // FP32-refined solves finished in FP64
     double graph_build_us = 0;  // host time of the captures and instantiations
@@ -940,6 +948,8 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
                   T* small, cudaStream_t st) {
     if (Rv % 4 != 0) throw Error(RC_INTERNAL, "fereg: the operator takes padded vectors (a multiple of 4 columns)");
     const bool weighted = W.cell_w != nullptr;
+    const auto gi = d.grids.find({Rv, int(sizeof(T))});
+    const Scratch::ApplyGrids grid = gi == d.grids.end() ? Scratch::ApplyGrids{} : gi->second;
     int h = d.begin(GpuAbsorber::P_APPLY, st);
     DevStruct SA = S;  // the operator's segment tiles
     SA.seg = d.aseg_tiles.set();
@@ -952,8 +962,8 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
             auto go = [&](auto lc, auto nbk, auto wc) {
                 constexpr int L = decltype(lc)::value, NBK = decltype(nbk)::value;
                 constexpr bool WT_ = decltype(wc)::value;
-                k_vseg_apply<T, L, NBK, WT_><<<GRID_S, WPB * 32, stage ? sm : 0, st>>>(S, W, d.aseg_segs.p, nsegs, P,
-                                                                                       Rv, j0, Rc, t, stage);
+                k_vseg_apply<T, L, NBK, WT_><<<grid.seg, WPB * 32, stage ? sm : 0, st>>>(S, W, d.aseg_segs.p, nsegs,
+                                                                                         P, Rv, j0, Rc, t, stage);
             };
             with_vlanes(Rc, S.nb, [&](auto lc, auto nbk) {
                 if (weighted) go(lc, nbk, std::true_type{});
@@ -981,8 +991,8 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
                 constexpr bool WT_ = decltype(wc)::value;
                 const size_t shm = wpull_smem() + (stage ? sm : 0);
                 allow_smem(k_vpull_apply<T, L, NBK, WT_>, shm);
-                k_vpull_apply<T, L, NBK, WT_><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wpull.set(), P, t, Rv, j0, Rc, Y,
-                                                                             stage);
+                k_vpull_apply<T, L, NBK, WT_><<<grid.pull, WPB * 32, shm, st>>>(S, W, d.wpull.set(), P, t, Rv, j0, Rc,
+                                                                                Y, stage);
             };
             with_vlanes(Rc, S.nb, [&](auto lc, auto nbk) {
                 if (weighted) go(lc, nbk, std::true_type{});
@@ -1009,6 +1019,75 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
     }
     CK(cudaGetLastError());
     d.end(h, st);
+}
+
+// The project's autotuner for the S*P passes: the grid of k_vseg_apply and of k_vpull_apply among
+// 1, 2, 4, 8 and 16 CTAs per SM (a grid only partitions the lane groups and list tiles, so every
+// choice gives the same bits), each timed with CUDA events on the solver's stream (one untimed
+// launch, then the shorter of two) on the solve's own vectors. The choice is kept for the process
+// under the structure's shape (cells, segments, coordinates, blocks, small coordinates, padded
+// width, element size, weighted), so later sessions of the same shape reuse it. FEREG_AUTOTUNE=0
+// turns it off (the default grid, 4 CTAs per SM). Passes under 2^20 cells are not tuned.
+std::mutex g_tune_mu;
+std::map<std::vector<u64>, Scratch::ApplyGrids> g_tuned;
+
+template <class T>
+void autotune_apply(Scratch& d, const DevStruct& S, const DevWeights& W, T* P, int Rv, T* Y, T* t, T* part, T* small,
+                    cudaStream_t st) {
+    const std::pair<int, int> key{Rv, int(sizeof(T))};
+    if (d.grids.count(key) || d.prof || S.M < (1u << 20)) return;
+    const char* env = std::getenv("FEREG_AUTOTUNE");
+    if (env && env[0] == '0') return;
+    const std::vector<u64> shape{S.M, S.g1, S.m, S.nb, S.ms_acc, u64(Rv), sizeof(T), W.cell_w != nullptr};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        const auto it = g_tuned.find(shape);
+        if (it != g_tuned.end()) {
+            d.grids[key] = it->second;
+            return;
+        }
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const int cand[] = {148, 296, 592, 1184, 2368};
+    Scratch::ApplyGrids best;
+    auto time_of = [&]() {
+        float mn = 1e30f;
+        for (int rep = 0; rep < 3; rep++) {
+            CK(cudaEventRecord(e0, st));
+            launch_apply<T>(d, S, W, P, Rv, Y, t, part, small, st);
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0) mn = std::min(mn, ms);
+        }
+        return mn;
+    };
+    // the segment pass's grid with the pull pass at its default, then the pull pass's
+    for (int pass = 0; pass < 2; pass++) {
+        float bt = 1e30f;
+        int bg = 148 * 4;
+        for (int g : cand) {
+            Scratch::ApplyGrids trial = best;
+            (pass == 0 ? trial.seg : trial.pull) = g;
+            d.grids[key] = trial;
+            const float ms = time_of();
+            if (ms < bt) {
+                bt = ms;
+                bg = g;
+            }
+        }
+        (pass == 0 ? best.seg : best.pull) = bg;
+    }
+    d.grids[key] = best;
+    CK(cudaEventDestroy(e0));
+    CK(cudaEventDestroy(e1));
+    d.tune_us += std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[shape] = best;
 }
 
 // The V-cycle's work vectors of every level for R columns (allocated before a graph capture).
@@ -1706,6 +1785,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             d.launches++;
             CK(cudaGetLastError());
         } else if (prec == Precision::F64) {
+            autotune_apply<double>(d, S, W, d.rhsv.p, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
             iterations = run_pcg<double>(d, op64, x, d.rhsv.p, d.rhsv.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p, RV, tol,
                                          0.0, 0, maxiter, warm != nullptr || have_last, ctx_, st, esc);
             exact = false;
@@ -1717,6 +1797,8 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             d.fsmall.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * rv));
             k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.rhsv.p, d.frhs.p, tot);
             d.launches++;
+            autotune_apply<float>(d, S, W, d.frhs.p, RV, d.fq.p, d.ft.p, d.fpart.p, d.fsmall.p, st);
+            autotune_apply<double>(d, S, W, d.rhsv.p, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
             iterations = 0;
             std::vector<double> rho64(rv, 0.0), rho_prev(rv, 0.0);
             bool have_r = false;  // d.r holds the FP64 true residual of x
