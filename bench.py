@@ -637,7 +637,8 @@ def roofline_of(sess, phases, n, R, weighted, s_v, workload):
     achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
     kern = PHASE_KERNEL[dom]
     return {"bound": "hbm", "kernel": kern, "phase": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": traffic_from_profiles(kern, workload), "peak_kind": peak_kind,
+            "frac": achieved / hbm, "traffic": traffic_from_profiles(kern, workload), "traffic_source": TRAFFIC_SOURCE,
+            "peak_kind": peak_kind,
             "algorithmic_bytes": algo[dom], "columns": R}
 
 
@@ -885,7 +886,8 @@ def peaks():
 
 def traffic_from_profiles(kernel, workload):
     """Per-launch DRAM bytes (read + write) of `kernel` on `workload` from the committed ncu
-    summary profiles/dram_traffic.txt (lines: kernel workload bytes)."""
+    summary profiles/dram_traffic.txt (lines: kernel workload bytes [capture note]): a figure of
+    the capture named there, not of this run. None when the kernel has no line."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     try:
         with open(path) as f:
@@ -896,6 +898,9 @@ def traffic_from_profiles(kernel, workload):
     except OSError:
         pass
     return None
+
+
+TRAFFIC_SOURCE = "profiles/dram_traffic.txt: one ncu capture per kernel (the file names the capture), not this run"
 
 
 def phase_bytes(info, n, R, weighted, s_v=8):
@@ -1165,7 +1170,8 @@ def main():
                        "parallelism": f"replicas x{world}", "prepare_s": prepare_s, "prepare_warm_s": prepare_warm_s,
                        "b_x1": float(res["b"][0]), "solver_stats": sess.solver_stats()},
             "roofline": {"bound": "hbm", "kernel": kern, "phase": dom, "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "traffic_source": TRAFFIC_SOURCE,
+                         "peak_kind": peak_kind,
                          "algorithmic_bytes": algo[dom]} if dom else None,
             "phases_ms_per_step": {k: v[0] / max(1, args.prof_steps) for k, v in phases.items() if v[1]},
             "phases_note": PHASES_NOTE,

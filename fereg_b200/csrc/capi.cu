@@ -464,7 +464,7 @@ int fereg_session_ols(fereg_session* s, double* rows, int rows_on_device, size_t
         sp.tol = spec->tol;
         sp.maxiter = spec->maxiter;
         sp.prec = spec->precision == FEREG_PREC_F32_REFINED ? Precision::F32_REFINED : Precision::F64;
-        if (sp.vce < 0 || sp.vce > 2) throw Error(RC_INVALID_INPUT, "fereg_session_ols: unknown vce");
+        if (sp.vce < 0 || sp.vce > 5) throw Error(RC_INVALID_INPUT, "fereg_session_ols: unknown vce");
         OlsOut o;
         o.b = out->b;
         o.V = out->V;

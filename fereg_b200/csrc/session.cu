@@ -624,10 +624,10 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     if (vce == 0 && kind == 3) vce = 1;  // ols.rs:150 pweights imply robust
     if (vce < 0 || vce > 5) throw Error(RC_INVALID_INPUT, "fereg ols: unknown variance");
     if (vce == 5 && kind == 3) throw Error(RC_INVALID_INPUT, "pweights not allowed with option vce(hc3)");  // ols.rs:251
-    if (vce >= 2 && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg ols: cluster variance without clusters");
+    const bool clustered = vce == 2 || vce == 3;
+    if (clustered && ccodes_.empty()) throw Error(RC_INVALID_INPUT, "fereg ols: cluster variance without clusters");
     if (vce == 3 && (kind == 2 || !dynamic_cast<GpuAbsorber*>(ab_.get())))
         throw Error(RC_INVALID_INPUT, "fereg ols: CRV3 needs intercept-only terms and no fweights");
-    const bool clustered = vce >= 2;
     const bool has_intercept = true;  // intercept-only terms (or noabsorb) contain the constant
     const bool report_constant = has_intercept && !spec.noconstant;
     // CRV3 refits start from the raw rows (row order)

@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_vpull_apply(DevStruct S, DevWei
             const u32 ie = st.kend[kl];
             V4<T> acc{T(0), T(0), T(0), T(0)};
             if (on) {
-#pragma unroll 2
+#pragma unroll 4
                 for (u32 i = i0 + g; i < ie; i += G) {
                     V4<T> v = ld4cg(tj + size_t(st.seg[i]) * Ru);
                     v.a = -v.a;
