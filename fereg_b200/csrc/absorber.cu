@@ -130,6 +130,18 @@ void with_vlanes(int Rc, u32 nb, F&& f) {
         default: with_nbk<32, 1>(nb, f); break;
     }
 }
+// Calls f(NSA) with the small blocks the segment passes sum (0 to WNB) as an integral constant.
+template <class F>
+void with_nsa(u32 ns, F&& f) {
+    using std::integral_constant;
+    switch (ns) {
+        case 0: f(integral_constant<int, 0>{}); break;
+        case 1: f(integral_constant<int, 1>{}); break;
+        case 2: f(integral_constant<int, 2>{}); break;
+        case 3: f(integral_constant<int, 3>{}); break;
+        default: f(integral_constant<int, WNB>{}); break;
+    }
+}
 template <int MIN_NBK = 0, class F>
 void with_rcp(int Rc, u32 nb, F&& f) {
     switch (rcp_of(Rc)) {
@@ -1179,9 +1191,12 @@ void launch_rhs(Scratch& d, const DevStruct& S, const DevWeights& W, const doubl
             const size_t shm = grhs_smem(S.ms_acc);
             with_lanes<WNB>(Rc, WNB, [&](auto c, auto) {
                 constexpr int RCP = decltype(c)::value;
-                allow_smem(k_grhs<RCP>, shm);
-                k_grhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, u32(d.wseg_segs.n), rows, R, j0, Rc,
-                                                            b1, d.cta2.p, acc ? small : nullptr);
+                with_nsa(acc ? S.ns_acc : 0u, [&](auto nsa) {
+                    constexpr int NSA = decltype(nsa)::value;
+                    allow_smem(k_grhs<RCP, NSA>, shm);
+                    k_grhs<RCP, NSA><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, u32(d.wseg_segs.n), rows, R,
+                                                                     j0, Rc, b1, d.cta2.p, acc ? small : nullptr);
+                });
             });
             d.launches++;
         }
@@ -1270,9 +1285,12 @@ void launch_rhs_scratch(Scratch& d, const DevStruct& S, const DevWeights& W, con
             const size_t shm = grhs_smem(S.ms_acc);
             with_lanes<WNB>(Rc, WNB, [&](auto c, auto) {
                 constexpr int RCP = decltype(c)::value;
-                allow_smem(k_grhs<RCP>, shm);
-                k_grhs<RCP><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, u32(d.wseg_segs.n), rows, R, j0, Rc,
-                                                            b1, x.cta2, acc ? x.small : nullptr);
+                with_nsa(acc ? S.ns_acc : 0u, [&](auto nsa) {
+                    constexpr int NSA = decltype(nsa)::value;
+                    allow_smem(k_grhs<RCP, NSA>, shm);
+                    k_grhs<RCP, NSA><<<GRID_S, WPB * 32, shm, st>>>(S, W, d.wseg_segs.p, u32(d.wseg_segs.n), rows, R,
+                                                                     j0, Rc, b1, x.cta2, acc ? x.small : nullptr);
+                });
             });
             d.launches++;
         }

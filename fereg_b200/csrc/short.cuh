@@ -500,7 +500,8 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_vpull_apply(DevStruct S, DevWei
 // group streams its segment's rows (contiguous in the block): with one row per cell, in chunks of
 // L rows whose small codes and weights lane i loads for row i, four rows' loads in flight;
 // otherwise cell by cell over the cell's rows.
-template <int L>
+// NSA: the small blocks summed (S.ns_acc when the small coordinates are accumulated, else 0).
+template <int L, int NSA>
 __global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W, const u32* __restrict__ segs,
                                                       u32 nsegs, const double* __restrict__ rows, int R, int j0,
                                                       int Rc, double* __restrict__ b1, double* __restrict__ cta_part,
@@ -510,13 +511,13 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W,
     constexpr int U = 4;  // rows whose loads are in flight together (two columns each)
     double* wacc_all = reinterpret_cast<double*>(smem_raw);
     double* colsum = wacc_all + size_t(WPB) * S.ms_acc * 64;  // WPB x 4 x 32: [q c0, q c1, ws c0, ws c1]
-    const bool acc = cta_small != nullptr;
+    constexpr bool acc = NSA > 0;
     const bool trivial = S.cell_row == nullptr;
     const u32 lane = wlane(), g = lane / L, j = lane % L;
     const bool on0 = int(j) < Rc, on1 = int(j) + L < Rc;
     const unsigned gmask = L == 32 ? FULL : ((1u << L) - 1u) << (g * L);
     const size_t Ru = size_t(R);
-    const int ns_acc = acc ? int(S.ns_acc) : 0;
+    constexpr int ns_acc = NSA;
     double* wacc = wacc_all + size_t(wid_in_cta()) * S.ms_acc * 64 + lane;
     if (acc)
         for (u32 i = 0; i < S.ms_acc * 2; i++) wacc[i * 32] = 0.0;
