@@ -636,6 +636,8 @@ def roofline_of(sess, phases, n, R, weighted, s_v, workload):
     ms, cnt = timed[dom]
     achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
     kern = PHASE_KERNEL[dom]
+    if dom == "residualize" and info["ncells"] == n:  # one row per cell: the row-major tile kernel
+        kern = "k_fresid"
     return {"bound": "hbm", "kernel": kern, "phase": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic_from_profiles(kern, workload), "traffic_source": TRAFFIC_SOURCE,
             "peak_kind": peak_kind,

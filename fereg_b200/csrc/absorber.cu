@@ -336,6 +336,7 @@ GpuAbsorber::GpuAbsorber(const std::vector<const u32*>& codes, const std::vector
     hs_ = plan_structure(codes, g, n, SMALL_LIMIT);
     norm_fe1_ = fe1_index(g);
     ctx_.check();
+    keep_pool_mapped();
     if (ctx_.priority_level < 0) {
         CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     } else {
@@ -1001,7 +1002,7 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
             auto go = [&](auto lc, auto nbk, auto wc) {
                 constexpr int L = decltype(lc)::value, NBK = decltype(nbk)::value;
                 constexpr bool WT_ = decltype(wc)::value;
-                const size_t shm = wpull_smem() + (stage ? sm : 0);
+                const size_t shm = WPB * 2 * vpull_buf_bytes<NBK - 1, WT_>() + (stage ? sm : 0);
                 allow_smem(k_vpull_apply<T, L, NBK, WT_>, shm);
                 k_vpull_apply<T, L, NBK, WT_><<<grid.pull, WPB * 32, shm, st>>>(S, W, d.wpull.set(), P, t, Rv, j0, Rc,
                                                                                 Y, stage);
@@ -1895,7 +1896,19 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     ctx_.check();
     int h = d.begin(P_RESID, st);
     double* alpha = want_coefs ? x + m * r : nullptr;
-    if (d.wseg.n)
+    if (d.wseg.n && !S.cell_row && R <= FR_MAXR) {  // one row per cell, narrow rows: pipelined tiles
+        const size_t shm = FR_WPB * fresid_bytes(R);
+        with_nbk<1, 0>(S.nb, [&](auto, auto nbk) {
+            constexpr int NBK = decltype(nbk)::value;
+            allow_smem(k_fresid<NBK>, shm);
+            int per_sm = 0;  // resident CTAs per SM at this width (shared memory bounds it)
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fresid<NBK>, FR_WPB * 32, shm));
+            const int grid = 148 * std::max(1, std::min(per_sm, 5));
+            k_fresid<NBK><<<grid, FR_WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, x, d.b1.p, alpha);
+        });
+        d.launches++;
+    }
+    else if (d.wseg.n)
         for (int j0 = 0; j0 < R; j0 += WCOLS) {
             const int Rc = std::min(WCOLS, R - j0);
             const size_t shm = wresid_smem(Rc);

@@ -1,8 +1,10 @@
 // Device helpers: error checks, buffers, warp lane layouts.
 #pragma once
 
+#include <algorithm>
 #include <map>
 #include <mutex>
+#include <set>
 #include <utility>
 
 #include <cuda_runtime.h>
@@ -38,6 +40,28 @@ struct AllocScope {
     AllocScope(const AllocScope&) = delete;
     AllocScope& operator=(const AllocScope&) = delete;
 };
+
+// Keeps memory released to the device's default pool mapped, up to 40% of the device memory (or
+// more, when the caller set more), once per device and process: the sessions' stream-ordered
+// allocations then reuse pool pages instead of mapping fresh ones at every call (the default
+// threshold of 0 returns the pool's memory at each synchronization). A per-process attribute of
+// the pool, not a device setting.
+inline void keep_pool_mapped() {
+    static std::mutex mu;
+    static std::set<int> done;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done.insert(dev).second) return;
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    u64 cur = 0;
+    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur));
+    u64 thr = std::max<u64>(cur, u64(0.4 * double(tot)));
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+}
 
 // Owned device allocation.
 template <class T>

@@ -28,6 +28,7 @@
 // WNB read from global memory).
 #pragma once
 
+#include "bulk.cuh"
 #include "tiles.cuh"
 
 namespace fereg {
@@ -417,10 +418,50 @@ __device__ __forceinline__ void stage_pull(const DevStruct& S, u32 k0, u32 k1, u
     }
 }
 
+// Per-warp buffer of the list pass's software pipeline: the tile's list ends (pl_off, global
+// entry indices), and per entry its segment, cell (weighted cells only) and NO other coordinates.
+template <int NO, bool WEIGHTED>
+__host__ __device__ constexpr size_t vpull_buf_bytes() {
+    return al16(WLIST * 4) + al16(PULL_WARP_MAX * 4) * (1 + (WEIGHTED ? 1 : 0) + NO);
+}
+struct VPullBuf {
+    u32* kend;
+    u32* seg;
+    u32* cell;
+    u32* oth;  // NO x PULL_WARP_MAX
+};
+template <int NO, bool WEIGHTED>
+__device__ __forceinline__ VPullBuf vpull_buf_at(unsigned char* p) {
+    VPullBuf b;
+    b.kend = reinterpret_cast<u32*>(p);
+    p += al16(WLIST * 4);
+    b.seg = reinterpret_cast<u32*>(p);
+    p += al16(PULL_WARP_MAX * 4);
+    b.cell = reinterpret_cast<u32*>(p);
+    if (WEIGHTED) p += al16(PULL_WARP_MAX * 4);
+    b.oth = reinterpret_cast<u32*>(p);
+    return b;
+}
+// Issues the copies of list tile tb into buffer b (the caller commits the group).
+template <int NO, bool WEIGHTED>
+__device__ __forceinline__ void vpull_prefetch(const DevStruct& S, const uint4& tb, const VPullBuf& b) {
+    const u32 lane = wlane(), k0 = tb.x, k1 = tb.y, e0 = tb.z, ne = tb.w - tb.z;
+    const u32 no = S.nb - 1;
+    if (lane < k1 - k0) cp_async4(b.kend + lane, S.pl_off + k0 + lane + 1);
+    for (u32 i = lane; i < ne; i += 32) {
+        cp_async4(b.seg + i, S.pl_seg + e0 + i);
+        if (WEIGHTED) cp_async4(b.cell + i, S.pl_cell + e0 + i);
+#pragma unroll
+        for (int o = 0; o < NO; o++) cp_async4(b.oth + o * PULL_WARP_MAX + i, S.pl_other + size_t(e0 + i) * no + o);
+    }
+}
+
 // Operator pass 2 on short coordinate lists (k >= ms_acc) with the padded vectors:
 // Y[k] = nr_k P[k] + sum over the cells c of k of W_c (sum_{other b} P[coord_b(c)] - t_{s(c)}).
-// Warp tiles of whole lists, staged; the entries are dealt to groups of L lanes (lane j holding
-// 4 columns), and the groups' sums are added by a fixed xor butterfly.
+// Warp tiles of whole lists; the entries are dealt to groups of L lanes (lane j holding 4
+// columns), and the groups' sums are added by a fixed xor butterfly. Software pipelined: while a
+// warp works on one tile, cp.async copies bring the next tile's list ends and entries' segments,
+// cells and other coordinates into the second of two shared buffers.
 template <class T, int L, int NBK, bool WEIGHTED>
 __global__ void __launch_bounds__(WPB * 32, 4) k_vpull_apply(DevStruct S, DevWeights W, WarpTiles wt,
                                                              const T* __restrict__ P, const T* __restrict__ t, int Rv,
@@ -428,7 +469,8 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_vpull_apply(DevStruct S, DevWei
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int G = 32 / L;
     constexpr int NO = NBK - 1;  // staged other blocks (all of them below WNB blocks)
-    const PullStage st = pull_stage_at(smem_raw + size_t(wid_in_cta()) * pull_bytes());
+    constexpr u32 BB = u32(vpull_buf_bytes<NO, WEIGHTED>());
+    unsigned char* mine = smem_raw + size_t(wid_in_cta()) * 2 * BB;
     const u32 lane = wlane(), g = lane / L, j = lane % L;
     const bool on = int(4 * j) < Rc;
     const size_t Ru = size_t(Rv);
@@ -436,7 +478,7 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_vpull_apply(DevStruct S, DevWei
     const T* Pj = P + j0 + 4 * j;
     const T* tj = t + j0 + 4 * j;
     // the lists are of large coordinates: the small blocks come first among a cell's other blocks
-    T* sp = reinterpret_cast<T*>(smem_raw + size_t(WPB) * pull_bytes());
+    T* sp = reinterpret_cast<T*>(smem_raw + size_t(WPB) * 2 * BB);
     const int nsm = stage ? int(S.ns_acc) : 0;
     if (nsm) stage_small(sp, P, Ru, j0, Rc, S.ms_acc);
     const T* spj = sp + 4 * j;
@@ -446,15 +488,24 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_vpull_apply(DevStruct S, DevWei
         return v;
     };
     const u32 wid = blockIdx.x * WPB + wid_in_cta(), nw = gridDim.x * WPB;
-    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);
-    for (u32 tile = wid; tile < wt.n; tile += nw) {
-        const u32 k0 = tb.x, k1 = tb.y, e0 = tb.z;
-        stage_pull(S, k0, k1, e0, tb.w, st, WEIGHTED, u32(NO));
-        if (tile + nw < wt.n) tb = wt.t[tile + nw];
+    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);            // this tile
+    uint4 tn = wid + nw < wt.n ? wt.t[wid + nw] : make_uint4(0, 0, 0, 0);  // the next
+    if (wid < wt.n) vpull_prefetch<NO, WEIGHTED>(S, tb, vpull_buf_at<NO, WEIGHTED>(mine));
+    cp_async_commit();
+    u32 it = 0;
+    for (u32 tile = wid; tile < wt.n; tile += nw, it++) {
+        const VPullBuf st = vpull_buf_at<NO, WEIGHTED>(mine + (it & 1) * BB);
+        if (tile + nw < wt.n) vpull_prefetch<NO, WEIGHTED>(S, tn, vpull_buf_at<NO, WEIGHTED>(mine + ((it + 1) & 1) * BB));
+        cp_async_commit();
+        const uint4 tc = tb;
+        tb = tn;
+        if (tile + 2 * nw < wt.n) tn = wt.t[tile + 2 * nw];
+        cp_async_wait_prior();  // this tile's copies
         __syncwarp();
+        const u32 k0 = tc.x, k1 = tc.y, e0 = tc.z;
         u32 i0 = 0;
         for (u32 kl = 0; kl < k1 - k0; kl++) {
-            const u32 ie = st.kend[kl];
+            const u32 ie = st.kend[kl] - e0;
             V4<T> acc{T(0), T(0), T(0), T(0)};
             if (on) {
 #pragma unroll 4
@@ -490,6 +541,7 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_vpull_apply(DevStruct S, DevWei
         }
         __syncwarp();
     }
+    cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -645,7 +697,8 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W,
 }
 
 // Right-hand side pass 2 on short coordinate lists (k >= ms_acc): rhs[k] = sum over the cells c
-// of k of (s_c - W_c b1_{s(c)} / n1_{s(c)}).
+// of k of (s_c - W_c b1_{s(c)} / n1_{s(c)}). The rows are gathered with the default cache policy:
+// a row shares its sectors with the rows of neighbouring coordinates, which nearby warps read.
 template <int RCP>
 __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_rhs(DevStruct S, DevWeights W, WarpTiles wt,
                                                            const double* __restrict__ rows,
@@ -676,7 +729,7 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_rhs(DevStruct S, DevWeigh
 #pragma unroll 8
                     for (u32 i = i0 + L.g; i < ie; i += G) {
                         const u32 c = st.cell[i], s = st.seg[i];
-                        const double x = __ldcs(vj + size_t(c) * Ru);
+                        const double x = __ldg(vj + size_t(c) * Ru);
                         const double sc = W.w_rows ? W.w_rows[c] * x : x;
                         acc += sc - cellw(W, c) * __ldcg(bj + size_t(s) * Ru) * W.n1inv[s];
                     }
@@ -687,7 +740,7 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_rhs(DevStruct S, DevWeigh
                         double sc = 0.0;
                         const u32 re = S.cell_row[c + 1];
                         for (u32 r = S.cell_row[c]; r < re; r++) {
-                            const double x = __ldcs(vj + size_t(r) * Ru);
+                            const double x = __ldg(vj + size_t(r) * Ru);
                             sc += W.w_rows ? W.w_rows[r] * x : x;
                         }
                         acc += sc - cellw(W, c) * __ldcg(bj + size_t(s) * Ru) * W.n1inv[s];
@@ -799,6 +852,169 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wresid(DevStruct S, DevWeights 
         }
         __syncwarp();
     }
+}
+
+// Residualization of the short segments when every cell holds one row and the rows have at most
+// FR_MAXR columns (operator.rs:1107-1179), per warp tile of whole segments (at most WT cells, WSEG
+// segments). The tile's rows are nc x R contiguous elements, dealt to the lanes in order (element e
+// to lane e mod 32), so the row copies and stores and the gathers of x run along the rows on all
+// 32 lanes. Software pipelined: while a warp works on one tile, cp.async copies bring the next
+// tile's rows, block coordinates, cell weights, segment offsets and 1/n1 into the other of two
+// shared buffers. For a tile:
+//  1. u(c, j) = sum_b x[coord_b(c), j] (blocks in order), every element's gathers in flight
+//     together, into the warp's shared memory U[e];
+//  2. alpha(s, j) = (b1(s, j) - sum_c W_c u(c, j)) / n1_s, one (segment, column) pair per lane,
+//     the segment's cells in order, into A;
+//  3. every element is written back as v - (alpha(s(c), j) + u(c, j)).
+constexpr int FR_MAXR = 16;  // widest rows k_fresid takes
+constexpr int FR_WPB = 4;    // warps per CTA of k_fresid
+constexpr int FR_NE = WT * FR_MAXR / 32;  // elements per lane of a tile, at most
+
+// Per-warp shared memory of k_fresid for R columns: two buffers of [rows, coordinates, cell
+// weights, segment offsets, 1/n1], then U, A and the cells' local segments.
+__host__ __device__ constexpr size_t fr_buf_bytes(int R) {
+    return al16(size_t(WT) * R * 8) + al16(size_t(WNB) * WT * 4) + al16(WT * 8) + al16((WSEG + 1) * 4) +
+           al16(WSEG * 8);
+}
+__host__ __device__ constexpr size_t fresid_bytes(int R) {
+    return 2 * fr_buf_bytes(R) + al16(size_t(WT) * R * 8) + al16(size_t(WSEG) * R * 8) + al16(WT * 4);
+}
+
+struct FrBuf {
+    double* v;    // the tile's rows (nc x R)
+    u32* code;    // block coordinates (WNB x WT)
+    double* cw;   // cell weights (weighted cells only)
+    u32* soff;    // seg_off[s0 .. s1]
+    double* n1i;  // 1/n1 of the tile's segments
+};
+__device__ __forceinline__ FrBuf fr_buf_at(unsigned char* p, int R) {
+    FrBuf b;
+    b.v = reinterpret_cast<double*>(p);
+    p += al16(size_t(WT) * R * 8);
+    b.code = reinterpret_cast<u32*>(p);
+    p += al16(size_t(WNB) * WT * 4);
+    b.cw = reinterpret_cast<double*>(p);
+    p += al16(WT * 8);
+    b.soff = reinterpret_cast<u32*>(p);
+    p += al16((WSEG + 1) * 4);
+    b.n1i = reinterpret_cast<double*>(p);
+    return b;
+}
+
+// Issues the copies of tile tb into buffer b (the caller commits the group).
+template <int NC>
+__device__ __forceinline__ void fr_prefetch(const DevStruct& S, const DevWeights& W, const double* rows, u32 R,
+                                            const uint4& tb, const FrBuf& b) {
+    const u32 lane = wlane(), s0 = tb.x, ns = tb.y - tb.x, c0 = tb.z, nc = tb.w - tb.z;
+    const double* src = rows + size_t(c0) * R;
+    for (u32 e = lane; e < nc * R; e += 32) cp_async8(b.v + e, src + e);
+    if (lane < nc) {
+#pragma unroll
+        for (int k = 0; k < NC; k++) cp_async4(b.code + k * WT + lane, S.coord + size_t(k) * S.M + c0 + lane);
+        if (W.cell_w) cp_async8(b.cw + lane, W.cell_w + c0 + lane);
+    }
+    if (lane <= ns) cp_async4(b.soff + lane, S.seg_off + s0 + lane);
+    if (lane < ns) cp_async8(b.n1i + lane, W.n1inv + s0 + lane);
+}
+
+// The (row, column) of element e = lane + 32 t of an R-column tile, advanced by 32 per step.
+struct ElemPos {
+    u32 r, c;
+    __device__ __forceinline__ void step(u32 q32, u32 r32, u32 R) {
+        r += q32;
+        c += r32;
+        if (c >= R) {
+            c -= R;
+            r++;
+        }
+    }
+};
+
+template <int NBK>
+__global__ void __launch_bounds__(FR_WPB * 32, 5) k_fresid(DevStruct S, DevWeights W, WarpTiles wt,
+                                                           double* __restrict__ rows, int R,
+                                                           const double* __restrict__ x,
+                                                           const double* __restrict__ b1, double* __restrict__ alpha) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NC = NBK < WNB ? NBK : WNB;  // blocks whose coordinates are staged
+    const u32 uR = u32(R);
+    unsigned char* mine = smem_raw + size_t(threadIdx.x >> 5) * fresid_bytes(R);
+    const u32 bbytes = u32(fr_buf_bytes(R));
+    double* U = reinterpret_cast<double*>(mine + 2 * bbytes);
+    double* A = U + size_t(WT) * R;
+    u32* segl = reinterpret_cast<u32*>(reinterpret_cast<unsigned char*>(A) + al16(size_t(WSEG) * R * 8));
+    const u32 lane = wlane();
+    const u32 q32 = 32u / uR, r32 = 32u % uR;
+    const ElemPos first{lane / uR, lane % uR};
+    const size_t Ru = size_t(R);
+    const u32 wid = blockIdx.x * FR_WPB + (threadIdx.x >> 5), nw = gridDim.x * FR_WPB;
+    uint4 tb = wid < wt.n ? wt.t[wid] : make_uint4(0, 0, 0, 0);            // this tile
+    uint4 tn = wid + nw < wt.n ? wt.t[wid + nw] : make_uint4(0, 0, 0, 0);  // the next
+    if (wid < wt.n) fr_prefetch<NC>(S, W, rows, uR, tb, fr_buf_at(mine, R));
+    cp_async_commit();
+    u32 it = 0;
+    for (u32 tile = wid; tile < wt.n; tile += nw, it++) {
+        const FrBuf cur = fr_buf_at(mine + (it & 1) * bbytes, R);
+        if (tile + nw < wt.n) fr_prefetch<NC>(S, W, rows, uR, tn, fr_buf_at(mine + ((it + 1) & 1) * bbytes, R));
+        cp_async_commit();
+        const uint4 tc = tb;
+        tb = tn;
+        if (tile + 2 * nw < wt.n) tn = wt.t[tile + 2 * nw];
+        cp_async_wait_prior();  // this tile's copies
+        __syncwarp();
+        const u32 s0 = tc.x, ns = tc.y - tc.x, c0 = tc.z, nc = tc.w - tc.z;
+        const u32 E = nc * uR;
+        if (lane < nc) {
+            u32 sl = 0;
+            while (cur.soff[sl + 1] - c0 <= lane) sl++;
+            segl[lane] = sl;
+        }
+        // 1. u of every element, all the lane's gathers in flight together
+        {
+            double g[FR_NE];
+            ElemPos p = first;
+#pragma unroll
+            for (int k = 0; k < FR_NE; k++) {
+                g[k] = 0.0;
+                if (p.r < nc) {
+#pragma unroll
+                    for (int b = 0; b < NC; b++) g[k] += __ldg(x + size_t(cur.code[b * WT + p.r]) * Ru + p.c);
+                    if constexpr (NBK == WNB)
+                        for (u32 b = WNB; b < S.nb; b++)
+                            g[k] += __ldg(x + size_t(__ldg(S.coord + size_t(b) * S.M + c0 + p.r)) * Ru + p.c);
+                }
+                p.step(q32, r32, uR);
+            }
+#pragma unroll
+            for (int k = 0; k < FR_NE; k++) {
+                const u32 e = lane + 32u * u32(k);
+                if (e < E) U[e] = g[k];
+            }
+        }
+        __syncwarp();
+        // 2. alpha of every (segment, column) pair
+        for (u32 pr = lane; pr < ns * uR; pr += 32) {
+            const u32 sl = pr / uR, c = pr % uR;
+            const u32 i0 = cur.soff[sl] - c0, i1 = cur.soff[sl + 1] - c0;
+            double a = 0.0;
+            for (u32 i = i0; i < i1; i++) a += (W.cell_w ? cur.cw[i] : 1.0) * U[i * uR + c];
+            const double al = (b1[size_t(s0 + sl) * Ru + c] - a) * cur.n1i[sl];
+            A[sl * uR + c] = al;
+            if (alpha) alpha[size_t(s0 + sl) * Ru + c] = al;
+        }
+        __syncwarp();
+        // 3. the rows
+        {
+            double* dst = rows + size_t(c0) * Ru;
+            ElemPos p = first;
+            for (u32 e = lane; e < E; e += 32) {
+                __stcs(dst + e, cur.v[e] - (A[segl[p.r] * uR + p.c] + U[e]));
+                p.step(q32, r32, uR);
+            }
+        }
+        __syncwarp();
+    }
+    cp_async_wait_all();
 }
 
 }  // namespace fereg

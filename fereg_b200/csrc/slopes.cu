@@ -271,6 +271,7 @@ GpuSlopeSolver::GpuSlopeSolver(const std::vector<SlopeTermIn>& terms, const doub
         if (terms[q].intercept && terms[q].slopes.empty() && (fe1_ < 0 || terms[q].g > terms[size_t(fe1_)].g))
             fe1_ = int(q);
     ctx_.check();
+    keep_pool_mapped();
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     AllocScope alloc_scope(stream_);
     d_ = std::make_unique<SlopeDevBufs>();

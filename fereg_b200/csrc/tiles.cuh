@@ -457,6 +457,7 @@ __global__ void __launch_bounds__(TB) k_b1sq(u32 g1, const double* __restrict__ 
         const ColMap cm = colmap(R, j0);
         double acc = 0.0;
         if (cm.on)
+#pragma unroll 8
             for (u32 s = blockIdx.x * u32(cm.nslot) + u32(cm.slot); s < g1; s += gridDim.x * u32(cm.nslot)) {
                 const double v = b1[size_t(s) * R + j0 + cm.col];
                 acc += v * v * n1inv[s];

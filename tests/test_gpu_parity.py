@@ -100,6 +100,32 @@ def test_residualize_matches_oracle(pair):
             assert rel(a, b) <= 1e-7
 
 
+@pytest.mark.parametrize("r", [1, 11, 17, 40])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_residualize_one_row_per_cell(r, weighted):
+    """One row per cell with FE1 segments of 1 to 40 cells: the lane-group residualization (its
+    register-held cells and the cells past them), the CTA tiles past 32 cells, and column chunks
+    of 1, 11, 16 + 1 and 16 + 16 + 8."""
+    rng = np.random.default_rng(40 + r + 100 * weighted)
+    n_ind = 2500
+    k = rng.integers(1, 41, n_ind)
+    ind = np.repeat(np.arange(n_ind), k).astype(np.uint32)
+    year = np.concatenate([rng.permutation(41)[:c] for c in k]).astype(np.uint32)
+    firm = rng.integers(0, 700, len(ind)).astype(np.uint32)
+    codes = [ind, firm, year]
+    g = [n_ind, 700, 41]
+    w = rng.uniform(0.2, 3.0, len(ind)) if weighted else None
+    gpu, orc = fb.Absorber(codes, g, w), oracle.Absorber(codes, g, w)
+    assert gpu.ncells == gpu.n
+    z = rng.standard_normal((gpu.n, r)) + 0.01 * ind[:, None]
+    z1, z2 = z.copy(), z.copy()
+    i1 = gpu.residualize(z1, tol=1e-12, maxiter=100000, want_coefs=True)
+    orc.residualize(z2, tol=1e-12, maxiter=100000)
+    for j in range(r):
+        assert rel(z1[:, j], z2[:, j]) <= 1e-9, j
+        assert rel(z[:, j] - gpu.fit_rows(i1["coefs"], j), z1[:, j]) <= 1e-9, j
+
+
 def test_residualize_is_deterministic(pair):
     _, gpu, _, z = pair
     z1, z2 = z.copy(), z.copy()
