@@ -1002,7 +1002,7 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
             auto go = [&](auto lc, auto nbk, auto wc) {
                 constexpr int L = decltype(lc)::value, NBK = decltype(nbk)::value;
                 constexpr bool WT_ = decltype(wc)::value;
-                const size_t shm = WPB * 2 * vpull_buf_bytes<NBK - 1, WT_>() + (stage ? sm : 0);
+                const size_t shm = WPB * vpull_warp_bytes<NBK - 1, WT_>() + (stage ? sm : 0);
                 allow_smem(k_vpull_apply<T, L, NBK, WT_>, shm);
                 k_vpull_apply<T, L, NBK, WT_><<<grid.pull, WPB * 32, shm, st>>>(S, W, d.wpull.set(), P, t, Rv, j0, Rc,
                                                                                 Y, stage);
