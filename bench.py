@@ -294,6 +294,12 @@ class ServePool:
         self.col["ybin"][:] = yb
 
 
+def serve_request_n(i, seed):
+    """The row count of request i of the C5 stream (the first draw of serve_request)."""
+    rng = np.random.default_rng(seed + i)
+    return int(np.exp(rng.uniform(np.log(1e4), np.log(SERVE_NMAX)))) // 10 * 10
+
+
 def serve_request(i, seed, pool):
     """Request i of the C5 stream (its own seed): n = exp(U(ln 1e4, ln 5e6)) rounded down to whole
     individuals, 1-4 FEs among indiv (n/10), year (10), firm (n/50 levels; random, or cyclic
@@ -374,7 +380,8 @@ def run_serve(args, cfg, rank, world, local, pg):
     """C5: a stream of 2,000 regressions with exponential inter-arrival times at ~70% of the
     measured capacity through the serving engine (fereg_server_*); value = p99 latency (submit to
     result) of the whole stream. The capacity is measured first (the warm-up) on 256 requests
-    generated and submitted back to back."""
+    generated and submitted back to back, in rows per second; the stream's request rate is 70% of
+    it over the stream's mean request size."""
     nreq = cfg["requests"]
     if args.impl == "reference":
         if rank != 0:
@@ -408,7 +415,10 @@ def run_serve(args, cfg, rank, world, local, pg):
     assert all(r["rc"] == 0 for r in res_b), [r["msg"] for r in res_b if r["rc"]]
     cap_rows = sum(r["n"] for r in burst) / burst_s
     cap_req = len(burst) / burst_s
-    rate = cfg["load"] * cap_req  # requests per second
+    # the offered load in rows per second: 70% of the burst's rows per second, spread over the
+    # stream's own request sizes (a request count would carry the burst sample's size mix over)
+    mean_rows = float(np.mean([serve_request_n(i, cfg["seed"]) for i in range(nreq)]))
+    rate = cfg["load"] * cap_rows / mean_rows  # requests per second
     arrivals = np.cumsum(np.random.default_rng(cfg["seed"] - 1).exponential(1.0 / rate, nreq))
     barrier(pg)
     results, tickets = [], []
@@ -477,7 +487,8 @@ def run_serve(args, cfg, rank, world, local, pg):
                 "warmup": 1, "ms_per_step": span * 1e3, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": "c5", "requests": nreq, "mix": mix, "rows_total": rows_total,
-                           "offered_rate_req_s": rate, "load": cfg["load"], "workers": args.serve_workers,
+                           "offered_rate_req_s": rate, "offered_rows_s": rate * mean_rows, "stream_mean_rows": mean_rows,
+                           "load": cfg["load"], "workers": args.serve_workers,
                            "tol": tol, "glm_tol": cfg["glm_tol"], "burst_requests": len(burst),
                            "burst_req_per_s": cap_req, "burst_rows_per_s": cap_rows, "late_submits": len(late),
                            "max_submit_lag_s": float(max(late)) if late else 0.0,
@@ -635,9 +646,7 @@ def roofline_of(sess, phases, n, R, weighted, s_v, workload):
     dom = max(timed, key=lambda k: timed[k][0])
     ms, cnt = timed[dom]
     achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
-    kern = PHASE_KERNEL[dom]
-    if dom == "residualize" and info["ncells"] == n:  # one row per cell: the row-major tile kernel
-        kern = "k_fresid"
+    kern = phase_kernel(dom, info, n, R)
     return {"bound": "hbm", "kernel": kern, "phase": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic_from_profiles(kern, workload), "traffic_source": TRAFFIC_SOURCE,
             "peak_kind": peak_kind,
@@ -932,6 +941,14 @@ PHASE_KERNEL = {"rhs_seg": "k_grhs", "rhs_pull": "k_wpull_rhs", "apply_seg": "k_
                 "gram": "k_outer_mma_bulk", "variance": "k_resid_e"}
 
 
+def phase_kernel(phase, info, n, R):
+    """The kernel of a phase: the residualization runs as k_fresid when every cell holds one row
+    and the rows have at most 16 columns (the absorber's FR_MAXR)."""
+    if phase == "residualize" and info["ncells"] == n and R <= 16:
+        return "k_fresid"
+    return PHASE_KERNEL[phase]
+
+
 def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1131,7 +1148,7 @@ def main():
     if dom:
         ms, cnt = timed[dom]
         achieved = algo[dom] / (ms / cnt / 1e3) / 1e9
-        kern = PHASE_KERNEL[dom]
+        kern = phase_kernel(dom, info, n, R)
         traffic = traffic_from_profiles(kern, args.config)
 
     cpu = None

@@ -1038,9 +1038,10 @@ void launch_apply(Scratch& d, const DevStruct& S, const DevWeights& W, const T* 
 // 1, 2, 4, 8 and 16 CTAs per SM (a grid only partitions the lane groups and list tiles, so every
 // choice gives the same bits), each timed with CUDA events on the solver's stream (one untimed
 // launch, then the shorter of two) on the solve's own vectors. The choice is kept for the process
-// under the structure's shape (cells, segments, coordinates, blocks, small coordinates, padded
-// width, element size, weighted), so later sessions of the same shape reuse it. FEREG_AUTOTUNE=0
-// turns it off (the default grid, 4 CTAs per SM). Passes under 2^20 cells are not tuned.
+// under the structure's shape (the powers of two of the cells, segments, coordinates and small
+// coordinates; blocks, padded width, element size, weighted), so later sessions of a similar shape
+// reuse it. FEREG_AUTOTUNE=0 turns it off (the default grid, 4 CTAs per SM). Passes under 2^20
+// cells are not tuned.
 std::mutex g_tune_mu;
 std::map<std::vector<u64>, Scratch::ApplyGrids> g_tuned;
 
@@ -1051,7 +1052,11 @@ void autotune_apply(Scratch& d, const DevStruct& S, const DevWeights& W, T* P, i
     if (d.grids.count(key) || d.prof || S.M < (1u << 20)) return;
     const char* env = std::getenv("FEREG_AUTOTUNE");
     if (env && env[0] == '0') return;
-    const std::vector<u64> shape{S.M, S.g1, S.m, S.nb, S.ms_acc, u64(Rv), sizeof(T), W.cell_w != nullptr};
+    // sizes by their power of two: structures of a similar size share a choice (a serving loop's
+    // requests each have their own exact sizes)
+    auto lg = [](u64 v) { return u64(v ? 64 - __builtin_clzll(v) : 0); };
+    const std::vector<u64> shape{lg(S.M), lg(S.g1), lg(S.m), S.nb, lg(S.ms_acc), u64(Rv), sizeof(T),
+                                 W.cell_w != nullptr};
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         const auto it = g_tuned.find(shape);
@@ -1691,6 +1696,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     SolveInfo info;
     const size_t m = hs_.m, g1 = hs_.g1;
     if (r == 0) {
+        wait_write_fence(stream_);
         info.iterations = 1;
         info.exact = true;
         return info;
@@ -1804,7 +1810,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             d.launches++;
             CK(cudaGetLastError());
         } else if (prec == Precision::F64) {
-            autotune_apply<double>(d, S, W, d.rhsv.p, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
+            if (ctx_.autotune) autotune_apply<double>(d, S, W, d.rhsv.p, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
             iterations = run_pcg<double>(d, op64, x, d.rhsv.p, d.rhsv.p, nullptr, d.r.p, d.z.p, d.p.p, d.q.p, RV, tol,
                                          0.0, 0, maxiter, warm != nullptr || have_last, ctx_, st, esc);
             exact = false;
@@ -1816,8 +1822,8 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             d.fsmall.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * rv));
             k_convert<double, float><<<grid_for(tot), THREADS, 0, st>>>(d.rhsv.p, d.frhs.p, tot);
             d.launches++;
-            autotune_apply<float>(d, S, W, d.frhs.p, RV, d.fq.p, d.ft.p, d.fpart.p, d.fsmall.p, st);
-            autotune_apply<double>(d, S, W, d.rhsv.p, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
+            if (ctx_.autotune) autotune_apply<float>(d, S, W, d.frhs.p, RV, d.fq.p, d.ft.p, d.fpart.p, d.fsmall.p, st);
+            if (ctx_.autotune) autotune_apply<double>(d, S, W, d.rhsv.p, RV, d.q.p, d.t.p, d.part.p, d.small.p, st);
             iterations = 0;
             std::vector<double> rho64(rv, 0.0), rho_prev(rv, 0.0);
             bool have_r = false;  // d.r holds the FP64 true residual of x
@@ -1894,6 +1900,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     if (m > 0) CK(cudaMemcpy2DAsync(d.coefs.p, r * 8, d.xv.p, rv * 8, r * 8, m, cudaMemcpyDeviceToDevice, st));
     x = d.coefs.p;
     ctx_.check();
+    wait_write_fence(st);
     int h = d.begin(P_RESID, st);
     double* alpha = want_coefs ? x + m * r : nullptr;
     if (d.wseg.n && !S.cell_row && R <= FR_MAXR) {  // one row per cell, narrow rows: pipelined tiles
@@ -1901,8 +1908,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
         with_nbk<1, 0>(S.nb, [&](auto, auto nbk) {
             constexpr int NBK = decltype(nbk)::value;
             allow_smem(k_fresid<NBK>, shm);
-            int per_sm = 0;  // resident CTAs per SM at this width (shared memory bounds it)
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fresid<NBK>, FR_WPB * 32, shm));
+            const int per_sm = resident_ctas(k_fresid<NBK>, FR_WPB * 32, shm);  // shared memory bounds it
             const int grid = 148 * std::max(1, std::min(per_sm, 5));
             k_fresid<NBK><<<grid, FR_WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, x, d.b1.p, alpha);
         });

@@ -23,6 +23,9 @@ struct Ctx {
     // priority. The serving engine gives small requests the high levels, so that their short
     // kernels are not queued behind the large requests' passes.
     int priority_level = -1;
+    // The S·P grid autotuner may time the passes (off in the serving engine: concurrent requests
+    // make the timings meaningless, and every grid gives the same bits).
+    bool autotune = true;
     void check() const {
         if (interrupt && interrupt(interrupt_data)) throw Error(RC_INTERRUPTED, "--Break--");
     }
@@ -79,6 +82,16 @@ class DeviceAbsorber {
     // Exact leverage of the FE columns per row (leverage.rs:128 fe_hat), row order, into device
     // memory (n values).
     virtual void fe_leverage_device(double* h_dev) = 0;
+    // The next residualize call makes its stream wait for `ev` (recorded on another stream) before
+    // it writes the rows, so that work still reading the raw rows runs beside the solve.
+    void set_write_fence(cudaEvent_t ev) { write_fence_ = ev; }
+
+   protected:
+    void wait_write_fence(cudaStream_t st) {
+        if (write_fence_) CK(cudaStreamWaitEvent(st, write_fence_, 0));
+        write_fence_ = nullptr;
+    }
+    cudaEvent_t write_fence_ = nullptr;
 };
 
 class GpuAbsorber : public DeviceAbsorber {

@@ -5,6 +5,7 @@
 #include <map>
 #include <mutex>
 #include <set>
+#include <tuple>
 #include <utility>
 
 #include <cuda_runtime.h>
@@ -40,6 +41,24 @@ struct AllocScope {
     AllocScope(const AllocScope&) = delete;
     AllocScope& operator=(const AllocScope&) = delete;
 };
+
+// CTAs of `kernel` resident on one SM at `threads` threads and `smem` dynamic shared memory, the
+// occupancy query cached per (kernel, threads, shared memory, device) for the process.
+template <class K>
+inline int resident_ctas(K kernel, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, size_t, int>, int> memo;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(reinterpret_cast<const void*>(kernel), threads, smem, dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    memo[key] = per_sm;
+    return per_sm;
+}
 
 // Keeps memory released to the device's default pool mapped, up to 40% of the device memory (or
 // more, when the caller set more), once per device and process: the sessions' stream-ordered

@@ -173,6 +173,7 @@ void Server::run(Entry& e) {
     try {
         Ctx ctx;
         ctx.priority_level = priority_level(q);
+        ctx.autotune = false;
         const double t0 = now();
         GpuSession s(q.codes, q.g, q.cl_codes, q.cl_g, q.w, q.w ? q.weight_kind : 0, q.n, 0, ctx);
         double* rows = s.gather_columns(q.cols.data(), q.cols.size());

@@ -452,13 +452,17 @@ std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, 
         const bool bulk = !perm && srcR <= 32 && reinterpret_cast<uintptr_t>(src) % 16 == 0 &&
                           nrows >= size_t(CS_ROWS) * ST_GRID;
         d.err.alloc(1);
+        int parts = ST_GRID;
         if (bulk) {
             CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), st));
             const size_t shm = size_t(CS_STAGES) * CS_ROWS * size_t(srcR) * sizeof(double);
             auto run = [&](auto kernel) {
                 if (shm > size_t(smem_limit(kernel)))  // static + dynamic can pass 48 KB: always raise it
                     throw Error(RC_INTERNAL, "fereg: the outer-product ring does not fit shared memory");
-                kernel<<<ST_GRID, ST_TB, shm, st>>>(sp, d.part.p, d.err.p);
+                // one wave: the CTAs resident at once (registers or the ring bound them), so that no
+                // second, partial wave runs the last chunks at a fraction of the occupancy
+                parts = std::max(1, std::min(ST_GRID, 148 * resident_ctas(kernel, ST_TB, shm)));
+                kernel<<<parts, ST_TB, shm, st>>>(sp, d.part.p, d.err.p);
             };
             switch ((msz + 7) / 8) {
                 case 1: run(k_outer_mma_bulk<1>); break;
@@ -474,7 +478,7 @@ std::vector<double> GpuSession::outer_products(const double* src, size_t nrows, 
                 default: k_outer_mma<4><<<ST_GRID, ST_TB, 0, st>>>(sp, d.part.p); break;
             }
         }
-        k_sum_parts<<<sum_parts_blocks(len), 256, 0, st>>>(d.part.p, ST_GRID, len, d.sums.p);
+        k_sum_parts<<<sum_parts_blocks(len), 256, 0, st>>>(d.part.p, parts, len, d.sums.p);
         d.launches += 2;
         std::vector<double> h(len);
         int late = 0;
@@ -532,25 +536,32 @@ double* GpuSession::gather_columns(const double* const* cols, size_t R) {
 
 // Column statistics of the raw rows (stats.rs:40) in one device pass about each column's first
 // value: sd (unweighted, floored at 1e-3), weighted mean, sum of squares, weighted centered and
-// uncentered sums of squares.
-GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
+// uncentered sums of squares. column_stats_alloc allocates the pass's buffers (on the session's
+// stream); column_stats_launch issues it on stream cs, the 6 R sums, the first row and the bulk
+// copies' error flag landing in host memory at s1, c0 and late once cs gets there.
+void GpuSession::column_stats_alloc(int R) {
     SessionDev& d = *d_;
-    cudaStream_t st = d.st;
+    d.part.alloc(size_t(ST_GRID) * size_t(R) * 6);
+    d.sums.alloc(size_t(R) * 6);
+    d.err.alloc(1);
+}
+
+void GpuSession::column_stats_launch(const double* rows, int R, cudaStream_t cs, double* s1, double* c0, int* late) {
+    SessionDev& d = *d_;
     const size_t n = n_, r = size_t(R);
     const double* wr = wk_.empty() ? nullptr : d.w_raw.p;
-    const double sumw = sumw_;
-    d.part.alloc(size_t(ST_GRID) * r * 6);
-    d.sums.alloc(r * 6);
-    d.err.alloc(1);
-    CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(d.err.p, 0, sizeof(int), cs));
     // whole rows through shared memory by bulk copies when the block starts on a 16-byte boundary
     const bool bulk = R <= 32 && reinterpret_cast<uintptr_t>(rows) % 16 == 0 && n >= size_t(CS_ROWS) * ST_GRID;
+    int parts = ST_GRID;
     if (bulk) {
         const size_t shm = size_t(CS_STAGES) * CS_ROWS * r * sizeof(double);
         auto run = [&](auto kernel) {
             if (shm > size_t(smem_limit(kernel)))  // static + dynamic can pass 48 KB: always raise it
                 throw Error(RC_INTERNAL, "fereg: the column statistics ring does not fit shared memory");
-            kernel<<<ST_GRID, ST_TB, shm, st>>>(rows, n, R, wr, d.part.p, d.err.p);
+            // one wave of resident CTAs (the ring and the reduction bound them)
+            parts = std::max(1, std::min(ST_GRID, 148 * resident_ctas(kernel, ST_TB, shm)));
+            kernel<<<parts, ST_TB, shm, cs>>>(rows, n, R, wr, d.part.p, d.err.p);
         };
         switch (rcp_of(R)) {
             case 1: run(k_colstats_bulk<1>); break;
@@ -565,24 +576,26 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
     for (int j0 = 0; j0 < R && !bulk; j0 += 32) {
         const int Rc = std::min(32, R - j0);
         switch (rcp_of(Rc)) {
-            case 1: k_colstats1<1><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            case 2: k_colstats1<2><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            case 4: k_colstats1<4><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            case 8: k_colstats1<8><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            case 16: k_colstats1<16><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
-            default: k_colstats1<32><<<ST_GRID, ST_TB, 0, st>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 1: k_colstats1<1><<<ST_GRID, ST_TB, 0, cs>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 2: k_colstats1<2><<<ST_GRID, ST_TB, 0, cs>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 4: k_colstats1<4><<<ST_GRID, ST_TB, 0, cs>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 8: k_colstats1<8><<<ST_GRID, ST_TB, 0, cs>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            case 16: k_colstats1<16><<<ST_GRID, ST_TB, 0, cs>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
+            default: k_colstats1<32><<<ST_GRID, ST_TB, 0, cs>>>(rows, n, R, j0, Rc, wr, d.part.p); break;
         }
         d.launches++;
     }
-    k_sum_parts<<<sum_parts_blocks(R * 6), 256, 0, st>>>(d.part.p, ST_GRID, R * 6, d.sums.p);
+    k_sum_parts<<<sum_parts_blocks(R * 6), 256, 0, cs>>>(d.part.p, parts, R * 6, d.sums.p);
     d.launches++;
-    std::vector<double> s1(r * 6), c0(r);
-    int late = 0;
-    CK(cudaMemcpyAsync(s1.data(), d.sums.p, r * 6 * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(c0.data(), rows, r * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&late, d.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpyAsync(s1, d.sums.p, r * 6 * 8, cudaMemcpyDeviceToHost, cs));
+    CK(cudaMemcpyAsync(c0, rows, r * 8, cudaMemcpyDeviceToHost, cs));
+    CK(cudaMemcpyAsync(late, d.err.p, sizeof(int), cudaMemcpyDeviceToHost, cs));
+}
+
+GpuSession::ColStats GpuSession::column_stats_finish(const double* s1, const double* c0, int late, int R) const {
     if (late) throw Error(RC_INTERNAL, "fereg: a bulk copy of the column statistics did not complete");
+    const size_t n = n_, r = size_t(R);
+    const double sumw = sumw_;
     ColStats cs;
     cs.wmean.resize(r);
     cs.sumsq.resize(r);
@@ -590,7 +603,7 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
     cs.sd.resize(r);
     cs.wss.resize(r);
     for (size_t j = 0; j < r; j++) {
-        const double* a = s1.data() + j * 6;
+        const double* a = s1 + j * 6;
         const double m2 = std::max(0.0, a[1] - a[0] * a[0] / double(n));
         cs.sd[j] = std::max(std::sqrt(m2 / (double(n) - 1.0)), 1e-3);
         cs.wmean[j] = c0[j] + a[2] / sumw;
@@ -599,6 +612,17 @@ GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
         cs.wss_unc[j] = a[5];
     }
     return cs;
+}
+
+GpuSession::ColStats GpuSession::column_stats(const double* rows, int R) {
+    SessionDev& d = *d_;
+    const size_t r = size_t(R);
+    column_stats_alloc(R);
+    std::vector<double> s1(r * 6), c0(r);
+    int late = 0;
+    column_stats_launch(rows, R, d.st, s1.data(), c0.data(), &late);
+    CK(cudaStreamSynchronize(d.st));
+    return column_stats_finish(s1.data(), c0.data(), late, R);
 }
 
 void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& spec, OlsOut& out) {
@@ -640,14 +664,38 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
 
     // the dof pass runs on its own stream beside the column statistics and the solve
     std::future<Dof> dof_job = dof_begin(clustered, spec.firstpair != 0, spec.want_groupvar != 0 && out.groupvar);
-    int ph = d.begin(S_COLSTATS);
 
-    // Pass A: column statistics of the raw rows (stats.rs:40), raw weights, in one device pass
-    const ColStats cs = column_stats(rows, R);
-    const std::vector<double>&wmean = cs.wmean, &sumsq = cs.sumsq, &wss_unc = cs.wss_unc, &sd = cs.sd, &wss = cs.wss;
-    const double tscale = (kind == 1 || kind == 3) ? double(n) / sumw : 1.0;
-    const double tss_y = (has_intercept ? wss[0] : wss_unc[0]) * tscale;
-    d.end(ph);
+    // Pass A: column statistics of the raw rows (stats.rs:40), raw weights, in one device pass. On
+    // the timed path it runs on the side stream beside the FE solve, which waits for it before it
+    // writes the rows; the phase-timed calls run it in place on the session's stream.
+    ColStatsSide& side = d.colstats_side();
+    ColStats cs;
+    bool side_pending = false;
+    if (d.prof) {
+        const int ph = d.begin(S_COLSTATS);
+        cs = column_stats(rows, R);
+        d.end(ph);
+    } else {
+        column_stats_alloc(R);
+        CK(cudaEventRecord(side.ready, st));
+        CK(cudaStreamWaitEvent(side.st.s, side.ready, 0));
+        column_stats_launch(rows, R, side.st.s, side.sums, side.c0, side.late);
+        CK(cudaEventRecord(side.done, side.st.s));
+        ab_->set_write_fence(side.done);
+        side_pending = true;
+    }
+    // a failed solve still waits for the side stream before the session's buffers are reused
+    struct SideJoin {
+        ColStatsSide& s;
+        bool& pending;
+        DeviceAbsorber* ab;
+        ~SideJoin() {
+            if (pending) {
+                cudaEventSynchronize(s.done);
+                ab->set_write_fence(nullptr);
+            }
+        }
+    } side_join{side, side_pending, ab_.get()};
 
     // The FE solve, in place
     const bool want_coefs = out.d != nullptr;
@@ -656,6 +704,14 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     const SolveInfo info =
     ab_->residualize_device(rows, r, spec.tol, spec.maxiter, want_coefs, nullptr, want_coefs ? coefs.data() : nullptr,
                             spec.prec);
+    if (side_pending) {
+        CK(cudaEventSynchronize(side.done));
+        side_pending = false;
+        cs = column_stats_finish(side.sums, side.c0, *side.late, R);
+    }
+    const std::vector<double>&wmean = cs.wmean, &sumsq = cs.sumsq, &wss_unc = cs.wss_unc, &sd = cs.sd, &wss = cs.wss;
+    const double tscale = (kind == 1 || kind == 3) ? double(n) / sumw : 1.0;
+    const double tss_y = (has_intercept ? wss[0] : wss_unc[0]) * tscale;
 
     // Outer products over the block: sum om a a^T of columns `cols` shifted by `shift` (+ the
     // constant), optionally the plain sums of squares; returns the full msz x msz matrix.
@@ -666,7 +722,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     };
 
     // Pass B: weighted Gram of the residualized block (stats.rs:195)
-    ph = d.begin(S_GRAM);
+    int ph = d.begin(S_GRAM);
     const double* wv = weighted ? d.wv.p : nullptr;
     std::vector<int> all_cols(r);
     std::iota(all_cols.begin(), all_cols.end(), 0);

@@ -200,6 +200,9 @@ class GpuSession {
         std::vector<double> wmean, sumsq, wss_unc, sd, wss;
     };
     ColStats column_stats(const double* rows, int R);
+    void column_stats_alloc(int R);
+    void column_stats_launch(const double* rows, int R, cudaStream_t cs, double* s1, double* c0, int* late);
+    ColStats column_stats_finish(const double* s1, const double* c0, int late, int R) const;
     std::vector<double> outer_products(const double* src, size_t nrows, int srcR, const std::vector<int>& cols,
                                        const std::vector<double>* shift, bool cst, const double* om, const int* perm,
                                        bool ssq, std::vector<double>* ss_out);

@@ -35,9 +35,29 @@ struct DofScratch {
     }
 };
 
+// The column statistics of an OLS call run on a side stream (one priority step below the
+// session's) beside the FE solve; their sums, first row and error flag come back into pinned host
+// memory (room for CS_MAXR columns, the most an OLS block has).
+constexpr int CS_MAXR = 64;
+struct ColStatsSide {
+    OwnedStream st;
+    cudaEvent_t ready = nullptr, done = nullptr;
+    double* sums = nullptr;  // 6 x CS_MAXR
+    double* c0 = nullptr;    // CS_MAXR
+    int* late = nullptr;
+    ~ColStatsSide() {
+        if (ready) cudaEventDestroy(ready);
+        if (done) cudaEventDestroy(done);
+        if (sums) cudaFreeHost(sums);
+        if (c0) cudaFreeHost(c0);
+        if (late) cudaFreeHost(late);
+    }
+};
+
 // Device state of a session.
 struct SessionDev {
     DofScratch dof;
+    ColStatsSide cside;
     std::vector<DBuf<u32>> tcodes, ccodes;  // kept order
     struct Subset {
         DBuf<int> perm;  // rows (row order) grouped by cluster, stable
@@ -68,6 +88,22 @@ struct SessionDev {
         cudaEvent_t a, b;
     };
     std::vector<Open> open;
+    // The side stream of the column statistics, created at first use.
+    ColStatsSide& colstats_side() {
+        ColStatsSide& c = cside;
+        if (!c.st.s) {
+            int least = 0, greatest = 0, own = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+            CK(cudaStreamGetPriority(st, &own));
+            CK(cudaStreamCreateWithPriority(&c.st.s, cudaStreamNonBlocking, std::min(least, own + 1)));
+            CK(cudaEventCreateWithFlags(&c.ready, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+            CK(cudaMallocHost(&c.sums, 6 * CS_MAXR * sizeof(double)));
+            CK(cudaMallocHost(&c.c0, CS_MAXR * sizeof(double)));
+            CK(cudaMallocHost(&c.late, sizeof(int)));
+        }
+        return c;
+    }
     cudaEvent_t event() {
         if (!pool.empty()) {
             cudaEvent_t e = pool.back();

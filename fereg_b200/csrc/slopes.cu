@@ -501,7 +501,10 @@ SolveInfo GpuSlopeSolver::solve(double* z, size_t r, double tol, size_t maxiter,
                                 double* coefs, bool warm_last) {
     SolveInfo info;
     info.iterations = 1;
-    if (r == 0) return info;
+    if (r == 0) {
+        wait_write_fence(stream_);
+        return info;
+    }
     ctx_.check();
     SlopeDevBufs& d = *d_;
     const SlopeHost& h = hs_;
@@ -568,6 +571,7 @@ SolveInfo GpuSlopeSolver::solve(double* z, size_t r, double tol, size_t maxiter,
     }
     // residualization: v <- d - h_E't with d = v - u(x), alpha_E = t
     double* alpha = want_coefs ? d.coefs.p + m * r : nullptr;
+    wait_write_fence(st);
     k_sl_seg<SL_RESID><<<sl_grid(size_t(h.ge) * r), SL_TB, 0, st>>>(D, z, R, R, m > 0 ? d.coefs.p : nullptr, R,
                                                                     nullptr, 0, z, alpha, R, nullptr);
     d.launches++;
