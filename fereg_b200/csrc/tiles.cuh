@@ -456,12 +456,25 @@ __global__ void __launch_bounds__(TB) k_b1sq(u32 g1, const double* __restrict__ 
     for (int j0 = 0; j0 < R; j0 += RC_MAX) {
         const ColMap cm = colmap(R, j0);
         double acc = 0.0;
-        if (cm.on)
-#pragma unroll 8
-            for (u32 s = blockIdx.x * u32(cm.nslot) + u32(cm.slot); s < g1; s += gridDim.x * u32(cm.nslot)) {
-                const double v = b1[size_t(s) * R + j0 + cm.col];
+        if (cm.on) {
+            // four segments' loads in flight together, the sum in segment order
+            const u32 step = gridDim.x * u32(cm.nslot);
+            u32 s = blockIdx.x * u32(cm.nslot) + u32(cm.slot);
+            const double* col = b1 + j0 + cm.col;
+            for (; size_t(s) + 3 * size_t(step) < g1; s += 4 * step) {
+                const double v0 = col[size_t(s) * R], v1 = col[size_t(s + step) * R];
+                const double v2 = col[size_t(s + 2 * step) * R], v3 = col[size_t(s + 3 * step) * R];
+                const double n0 = n1inv[s], n1 = n1inv[s + step], n2 = n1inv[s + 2 * step], n3 = n1inv[s + 3 * step];
+                acc += v0 * v0 * n0;
+                acc += v1 * v1 * n1;
+                acc += v2 * v2 * n2;
+                acc += v3 * v3 * n3;
+            }
+            for (; s < g1; s += step) {
+                const double v = col[size_t(s) * R];
                 acc += v * v * n1inv[s];
             }
+        }
         red[threadIdx.x] = acc;
         __syncthreads();
         if (int(threadIdx.x) < cm.Rc) {
