@@ -216,7 +216,10 @@ struct Scratch {
     DBuf<float> fx, fb, fr, fz, fp, fq, ft, fpart, frhs, fx0, fsmall;
     DBuf<double> cg_rho, cg_rho_new, cg_pq, cg_gamma, cg_beta, cg_xb, cg_ss1, cg_floor, cg_ring, cg_xconst, cg_pfloor;
     DBuf<int> cg_active, cg_nactive;
+    DBuf<double> cg_ss0;
     int* h_nactive = nullptr;  // pinned: the loop control words (CgLoop::ctl) read back
+    double* h_ss0 = nullptr;   // pinned: ss0 read back (h_ss0_n values)
+    size_t h_ss0_n = 0;
     // PCG loop state on the device (pcg.cuh) and the captured iteration graphs, each keyed by
     // every address its kernels read or write
     DBuf<int> lp_ctl, lp_act;
@@ -322,6 +325,7 @@ struct Scratch {
     ~Scratch() {
         drop_graphs();
         if (h_nactive) cudaFreeHost(h_nactive);
+        if (h_ss0) cudaFreeHost(h_ss0);
         for (auto e : ev)
             if (e) cudaEventDestroy(e);
         for (auto e : pool_) cudaEventDestroy(e);
@@ -1727,17 +1731,29 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     d.cta2.alloc(size_t(GRID_S) * 2 * r);
     d.small.alloc(std::max<size_t>(1, small_rows() * d.ms_acc * rv));
     launch_rhs(d, S, W, rows, R, d.b1.p, d.rhs.p, d.colsum.p, st);
-    std::vector<double> cs(3 * r);
-    CK(cudaMemcpyAsync(cs.data(), d.colsum.p, 3 * r * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
     ctx_.check();
-    std::vector<double> ss0(rv, 0.0), ss1(rv, 0.0);
-    for (size_t j = 0; j < r; j++) {  // solve.rs:1210-1217
-        const double wsq = cs[j], wsum = cs[r + j], b1sq = cs[2 * r + j];
-        const double s = wsq - wsum * wsum / sw_;
-        ss0[j] = s > 1e-15 * wsq ? s : 0.0;
-        ss1[j] = wsq - b1sq;
+    // ss0 and ss1 (solve.rs:1210-1217) and the PCG's start state on the device from the column sums;
+    // the host reads ss0 back only where it needs it (an explicit warm start; the exactness test
+    // after the PCG, whose launches synchronize the stream), with no round trip here
+    std::vector<double> ss0(rv, 0.0);
+    if (m > 0) {
+        for (auto* b : {&d.cg_ss0, &d.cg_ss1, &d.cg_floor, &d.cg_xconst}) b->alloc(rv);
+        d.cg_active.alloc(rv);
+        k_ss_prep<<<grid_for(rv), THREADS, 0, st>>>(d.colsum.p, R, RV, sw_, d.cg_ss0.p, d.cg_ss1.p, d.cg_active.p,
+                                                    d.cg_floor.p, d.cg_xconst.p);
+        d.launches++;
+        if (d.h_ss0_n < rv) {
+            if (d.h_ss0) CK(cudaFreeHost(d.h_ss0));
+            d.h_ss0 = nullptr;
+            d.h_ss0_n = 0;
+            CK(cudaHostAlloc(&d.h_ss0, rv * sizeof(double), cudaHostAllocDefault));
+            d.h_ss0_n = rv;
+        }
+        CK(cudaMemcpyAsync(d.h_ss0, d.cg_ss0.p, rv * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
+    auto read_ss0 = [&]() {  // once the stream has passed the copy above
+        if (m > 0) std::copy(d.h_ss0, d.h_ss0 + rv, ss0.begin());
+    };
     // the padded right-hand side
     if (m > 0) {
         CK(cudaMemsetAsync(d.rhsv.p, 0, m * rv * 8, st));
@@ -1746,16 +1762,11 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     double* x = d.xv.p;  // the padded iterate
     const bool have_last = warm_last && last_r_ == r && m > 0;
     if (have_last) {  // the previous solution, already in place; zero the columns with ss0 = 0
-        std::vector<int> zc(rv);
-        bool any = false;
-        for (size_t j = 0; j < r; j++) any |= (zc[j] = ss0[j] == 0.0) != 0;
-        if (any) {
-            d.cg_active.alloc(rv);
-            CK(cudaMemcpyAsync(d.cg_active.p, zc.data(), rv * sizeof(int), cudaMemcpyHostToDevice, st));
-            k_zero_masked<<<grid_for(m * rv), THREADS, 0, st>>>(x, d.cg_active.p, m * rv, RV);
-            d.launches++;
-        }
+        k_zero_ss0<<<grid_for(m * rv), THREADS, 0, st>>>(x, d.cg_ss0.p, m * rv, RV, R);
+        d.launches++;
     } else if (warm) {
+        CK(cudaStreamSynchronize(st));
+        read_ss0();
         std::vector<double> w0(warm, warm + m * r);
         for (size_t j = 0; j < r; j++)
             if (ss0[j] == 0.0)
@@ -1780,18 +1791,8 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             b->alloc(rv);
         d.cg_xb.alloc(3 * rv);
         d.cg_ring.alloc(rv * WINDOW);
-        d.cg_active.alloc(rv);
         d.cg_nactive.alloc(1);
         std::vector<int> act(rv);
-        std::vector<double> fl(rv), zero(rv, 0.0);
-        for (size_t j = 0; j < rv; j++) {
-            act[j] = ss0[j] > 0.0;
-            fl[j] = 1e-26 * ss0[j];
-        }
-        CK(cudaMemcpyAsync(d.cg_active.p, act.data(), rv * sizeof(int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.cg_ss1.p, ss1.data(), rv * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.cg_floor.p, fl.data(), rv * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.cg_xconst.p, zero.data(), rv * 8, cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(d.cg_ring.p, 0, rv * WINDOW * 8, st));
         const bool exact_pre = small_ok_ && hs_.m_small == hs_.m;
         const std::function<bool(double)> esc = [this](double rho_hat) { return escalate(rho_hat); };
@@ -1891,6 +1892,7 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
             exact = false;
         }
         if (!exact) {
+            read_ss0();
             bool all0 = true;
             for (double s : ss0) all0 &= s == 0.0;
             exact = all0;

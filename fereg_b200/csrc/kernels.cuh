@@ -156,6 +156,37 @@ __global__ void k_zero_masked(double* __restrict__ x, const int* __restrict__ ma
         if (mask[i % R]) x[i] = 0.0;
 }
 
+// The solve's column scalars from the rhs pass's column sums cs = [sum w v^2, sum w v, sum b1^2/n1]
+// (solve.rs:1210-1217): ss0 = the weighted centered sum of squares (0 below 1e-15 of the sum of
+// squares), ss1 = sum w v^2 - sum b1^2/n1, and the PCG's start state: active = ss0 > 0, the floor
+// 1e-26 ss0, x'rhs of the start 0. Columns r..rv-1 (padding) get zeros.
+__global__ void k_ss_prep(const double* __restrict__ cs, int r, int rv, double sw, double* __restrict__ ss0,
+                          double* __restrict__ ss1, int* __restrict__ active, double* __restrict__ floor_,
+                          double* __restrict__ xconst) {
+    for (int j = int(blockIdx.x * blockDim.x + threadIdx.x); j < rv; j += int(gridDim.x * blockDim.x)) {
+        double s0 = 0.0, s1 = 0.0;
+        if (j < r) {
+            const double wsq = cs[j], wsum = cs[r + j], b1sq = cs[2 * r + j];
+            const double s = wsq - wsum * wsum / sw;
+            s0 = s > 1e-15 * wsq ? s : 0.0;
+            s1 = wsq - b1sq;
+        }
+        ss0[j] = s0;
+        ss1[j] = s1;
+        active[j] = s0 > 0.0;
+        floor_[j] = 1e-26 * s0;
+        xconst[j] = 0.0;
+    }
+}
+
+// x = 0 on the columns j < r whose ss0 is 0 (a warm start of zero columns, solve.rs:1209-1217).
+__global__ void k_zero_ss0(double* __restrict__ x, const double* __restrict__ ss0, size_t total, int R, int r) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const int j = int(i % size_t(R));
+        if (j < r && ss0[j] == 0.0) x[i] = 0.0;
+    }
+}
+
 // x += z on the active columns (exact preconditioner, cg.rs:171-198).
 template <class T>
 __global__ void k_add_active(T* __restrict__ x, const T* __restrict__ z, const int* __restrict__ active, size_t total, int R) {

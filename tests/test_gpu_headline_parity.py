@@ -78,3 +78,24 @@ def test_ols_within_target(name, vce, precision):
         assert a["scalars"][k] == b["scalars"][k] or (np.isnan(a["scalars"][k]) and np.isnan(b["scalars"][k])), k
     eb, es = rel_errors(a, b)
     assert eb <= TARGET and es <= TARGET, (name, vce, precision, eb, es)
+
+
+@pytest.mark.parametrize("vce", ["unadjusted", "robust"])
+def test_side_stream_column_statistics_bit_equal(vce):
+    """The OLS call's column statistics run on a side stream beside the FE solve, which waits for
+    them before it writes the rows; phase-timed calls run them in place on the session's stream.
+    Both give the same bits (the same kernels on the same rows), and repeated calls agree."""
+    codes, g, rows = panel("cyclic_1e6")
+    gpu = fb.Session(codes, g)
+    z = np.ascontiguousarray(rows[gpu.row_order()])
+    out = []
+    for prof in (False, True, False):
+        gpu.set_profiling(prof)
+        out.append(gpu.ols(z.copy(), vce=vce, tol=bench.TOL))
+    gpu.set_profiling(False)
+    gpu.close()
+    for o in out[1:]:
+        assert np.array_equal(o["b"], out[0]["b"]) and np.array_equal(o["V"], out[0]["V"])
+        for k in ("r2", "rss", "tss"):
+            if k in o["scalars"]:
+                assert o["scalars"][k] == out[0]["scalars"][k] or np.isnan(o["scalars"][k]), k
