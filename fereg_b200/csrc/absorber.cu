@@ -1554,14 +1554,23 @@ Scratch::PcgGraph capture_iteration(Scratch& d, const Op& op, T* x, const T* rhs
     gr.key = std::move(key);
     CK(cudaGraphCreate(&gr.g, 0));
     cudaGraphConditionalHandle cond;
-    CK(cudaGraphConditionalHandleCreate(&cond, gr.g, 1, cudaGraphCondAssignDefault));
+    CK(cudaGraphConditionalHandleCreate(&cond, gr.g, 0, cudaGraphCondAssignDefault));
+    // a first node sets the condition from the active count and the launch's cap, so that a launch
+    // with no active column runs no iteration (the host need not look before launching)
+    CK(cudaStreamBeginCaptureToGraph(st, gr.g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    k_cond_first<<<1, 32, 0, st>>>(cond, cg.n_active, lp);
+    CK(cudaStreamEndCapture(st, &gr.g));
+    cudaGraphNode_t first = nullptr;
+    size_t nn = 1;
+    CK(cudaGraphGetNodes(gr.g, &first, &nn));
+    if (nn != 1) throw Error(RC_INTERNAL, "fereg: the PCG graph's first node");
     cudaGraphNodeParams np = {};
     np.type = cudaGraphNodeTypeConditional;
     np.conditional.handle = cond;
     np.conditional.type = cudaGraphCondTypeWhile;
     np.conditional.size = 1;
     cudaGraphNode_t node;
-    CK(cudaGraphAddNode(&node, gr.g, nullptr, 0, &np));
+    CK(cudaGraphAddNode(&node, gr.g, &first, 1, &np));
     cudaGraph_t body = np.conditional.phGraph_out[0];
     const u64 launches0 = d.launches;
     CK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
@@ -1627,8 +1636,18 @@ restart:
     CK(cudaMemsetAsync(d.lp_ctl.p, 0, 4 * sizeof(int), st));  // k = 0 since the (re)start
     CK(cudaMemcpyAsync(hc, d.cg_nactive.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     d.end(h, st);
-    CK(cudaStreamSynchronize(st));
-    bool any_active = hc[0] > 0;
+    // with the body's graph captured already, the graph's first node decides whether the first
+    // launch runs an iteration: the host launches it without reading the active count first
+    bool look = d.prof || maxiter <= iters_done + it;
+    if (!look) {
+        op.prepare(R);
+        const std::vector<u64> key0 = body_key<T>(d, op, x, rhs_true, x0, r, z, p, q, R);
+        look = true;
+        for (auto& q_ : d.graphs)
+            if (q_.key == key0) look = false;
+    }
+    if (look) CK(cudaStreamSynchronize(st));
+    bool any_active = look ? hc[0] > 0 : true;
     int k = 0;
     bool probed = false;
     while (any_active) {

@@ -238,6 +238,12 @@ __global__ void __launch_bounds__(TB) k_rz_stop(const T* __restrict__ r, const T
     }
 }
 
+// The first condition of a graph launch's WHILE node (a node before it): iterate while some
+// column is active and the launch's cap allows one iteration.
+__global__ void k_cond_first(cudaGraphConditionalHandle cond, const int* __restrict__ n_active, CgLoop lp) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, (*n_active > 0 && lp.ctl[3] > 0) ? 1u : 0u);
+}
+
 // p = z + beta p on the active columns, 0 on the others; then the iteration's end: the launch's
 // iteration count rises and, in a graph, the WHILE condition is set for the next iteration.
 template <class T>
