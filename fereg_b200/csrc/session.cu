@@ -635,9 +635,9 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     if (r + 1 > size_t(OP_MAXM)) throw Error(RC_INVALID_INPUT, "fereg ols: at most 62 regressors on the device path");
     double* rows = rows_in;
     if (!on_device) {
-    d.rows.alloc(n * r);
-    CK(cudaMemcpyAsync(d.rows.p, rows_in, n * r * 8, cudaMemcpyHostToDevice, st));
-    rows = d.rows.p;
+        d.rows.alloc(n * r);
+        CK(cudaMemcpyAsync(d.rows.p, rows_in, n * r * 8, cudaMemcpyHostToDevice, st));
+        rows = d.rows.p;
     }
     const std::vector<u32>& pi = ab_->row_order();
     const int kind = kind_;
@@ -718,7 +718,7 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     auto outer = [&](const double* src, size_t nrows, int srcR, const std::vector<int>& cols,
                  const std::vector<double>* shift, bool cst, const double* om, const int* perm, bool ssq,
                  std::vector<double>* ss_out) {
-    return outer_products(src, nrows, srcR, cols, shift, cst, om, perm, ssq, ss_out);
+        return outer_products(src, nrows, srcR, cols, shift, cst, om, perm, ssq, ss_out);
     };
 
     // Pass B: weighted Gram of the residualized block (stats.rs:195)
@@ -737,9 +737,9 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     for (size_t j = 0; j < r; j++) absorbed[j] = ss_res[j] / sumsq[j] <= ctol;
     const bool y_abs = nx >= 1 && absorbed[0];
     if (y_abs) {  // reghdfe zeroes the partialled-out depvar
-    k_zero_col<<<blocks_for(n, 256), 256, 0, st>>>(rows, n, R, 0);
-    d.launches++;
-    for (size_t j = 0; j < r; j++) g[j] = g[j * r] = 0.0;
+        k_zero_col<<<blocks_for(n, 256), 256, 0, st>>>(rows, n, R, 0);
+        d.launches++;
+        for (size_t j = 0; j < r; j++) g[j] = g[j * r] = 0.0;
     }
     for (size_t j = 1; j < r; j++)
     if (absorbed[j]) status[j - 1] = 2;
@@ -755,11 +755,11 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     const la::Mat inv_c = la::sweep_inverse(gs, kc, SWEEP_TOL, false, dropped);
     std::vector<size_t> keep_pos, kept;
     for (size_t c = 0; c < kc; c++) {
-    if (dropped[c]) status[cand[c] - 1] = 3;
-    else {
-        keep_pos.push_back(c);
-        kept.push_back(cand[c]);
-    }
+        if (dropped[c]) status[cand[c] - 1] = 3;
+        else {
+            keep_pos.push_back(c);
+            kept.push_back(cand[c]);
+        }
     }
     const size_t k = kept.size();
     la::Mat inv_s(k * k);
@@ -787,8 +787,8 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     d.col.alloc(k + 1);
     d.beta.alloc(k + 1);
     if (k) {
-    CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.beta.p, beta.data(), k * 8, cudaMemcpyHostToDevice, st));
     }
     // With the iid variance and no residuals asked for, rss comes from the Gram through the normal
     // equations, rss = y'Wy - b'X'Wy, unless that difference cancels (rss below 1e-6 of y'Wy); the
@@ -819,8 +819,8 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     // bread: the standardized inverse, bordered by the constant (vcov.rs:220)
     std::vector<double> means_s(k), xbar(k);
     for (size_t a = 0; a < k; a++) {
-    means_s[a] = wmean[kept[a]] / sd[kept[a]];
-    xbar[a] = wmean[kept[a]];
+        means_s[a] = wmean[kept[a]] / sd[kept[a]];
+        xbar[a] = wmean[kept[a]];
     }
     double b0_s = wmean[0] / sd_y;
     for (size_t a = 0; a < k; a++) b0_s -= means_s[a] * b_s[a];
@@ -839,75 +839,75 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     for (size_t a = 0; a < k; a++) sc[a] = sd[kept[a]];
     if (report_constant) sc[k] = 1.0;
     auto standardize = [&](la::Mat& mt) {
-    for (size_t a = 0; a < msz; a++)
-        for (size_t b = 0; b < msz; b++) mt[a * msz + b] /= sc[a] * sc[b] * sd_y * sd_y;
+        for (size_t a = 0; a < msz; a++)
+            for (size_t b = 0; b < msz; b++) mt[a * msz + b] /= sc[a] * sc[b] * sd_y * sd_y;
     };
     la::Mat v_s(msz * msz, 0.0);
     if (msz > 0) {
-    if (vce == 0) {
-        const double f = (rss_s / bigN) * (bigN / df_r);
-        for (size_t i = 0; i < msz * msz; i++) v_s[i] = f * bread[i];
-    } else if (vce == 1) {
-        d.om.alloc(n);
-        k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 0, d.om.p);
-        d.launches++;
-        const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
-        la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
-        standardize(meat);
-        v_s = la::sandwich(bread, meat, msz, bigN / (bigN - df_a - df_m));
-    } else if (vce == 4 || vce == 5) {
-        // ols.rs:450-474: the full design's leverage h = h_FE + w_v x~'(X~'WX~)^-1 x~, then the
-        // regress HC2 / HC3 multipliers (ols/stata_vce.rs:156-167) in the robust meat, no factor
-        d.h.alloc(n);
-        ab_->fe_leverage_device(d.h.p);
-        DBuf<double> ginv;
-        ginv.upload(fit_.A.empty() ? std::vector<double>{0.0} : fit_.A, st);
-        d.om.alloc(n);
-        if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
-        k_hc_weights<<<blocks_for(n, 256), 256, 0, st>>>(rows, R, d.col.p, int(k), ginv.p, d.e.p, wv, d.h.p,
-                                                         kind == 2 ? 1 : 0, vce == 5 ? 1 : 0, n, d.om.p);
-        d.launches++;
-        const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
-        la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
-        standardize(meat);
-        v_s = la::sandwich(bread, meat, msz, 1.0);
-    } else if (vce == 2) {
-        d.om.alloc(n);
-        k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 1, d.om.p);
-        d.launches++;
-        const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
-        if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
-        la::Mat meat(msz * msz, 0.0);
-        for (auto& sub : d.subsets) {
-            d.S.alloc(size_t(sub.G) * msz);
-            d.shift.alloc(k + 1);
-            if (k) CK(cudaMemcpyAsync(d.shift.p, shift.data(), k * 8, cudaMemcpyHostToDevice, st));
-            k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(rows, R, d.col.p, d.shift.p, int(k), report_constant ? 1 : 0,
-                                                       d.om.p, sub.perm.p, sub.coff.p, sub.G, d.S.p);
+        if (vce == 0) {
+            const double f = (rss_s / bigN) * (bigN / df_r);
+            for (size_t i = 0; i < msz * msz; i++) v_s[i] = f * bread[i];
+        } else if (vce == 1) {
+            d.om.alloc(n);
+            k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 0, d.om.p);
             d.launches++;
-            std::vector<int> scols(msz);
-            std::iota(scols.begin(), scols.end(), 0);
-            const la::Mat part = outer(d.S.p, sub.G, int(msz), scols, nullptr, false, nullptr, nullptr, false, nullptr);
-            for (size_t i = 0; i < msz * msz; i++) meat[i] += sub.sign * part[i];
-            // the next subset's scores need the kept columns again
+            const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+            la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
+            standardize(meat);
+            v_s = la::sandwich(bread, meat, msz, bigN / (bigN - df_a - df_m));
+        } else if (vce == 4 || vce == 5) {
+            // ols.rs:450-474: the full design's leverage h = h_FE + w_v x~'(X~'WX~)^-1 x~, then the
+            // regress HC2 / HC3 multipliers (ols/stata_vce.rs:156-167) in the robust meat, no factor
+            d.h.alloc(n);
+            ab_->fe_leverage_device(d.h.p);
+            DBuf<double> ginv;
+            ginv.upload(fit_.A.empty() ? std::vector<double>{0.0} : fit_.A, st);
+            d.om.alloc(n);
             if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+            k_hc_weights<<<blocks_for(n, 256), 256, 0, st>>>(rows, R, d.col.p, int(k), ginv.p, d.e.p, wv, d.h.p,
+                                                             kind == 2 ? 1 : 0, vce == 5 ? 1 : 0, n, d.om.p);
+            d.launches++;
+            const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+            la::Mat meat = outer(rows, n, R, kcols, &shift, report_constant, d.om.p, nullptr, false, nullptr);
+            standardize(meat);
+            v_s = la::sandwich(bread, meat, msz, 1.0);
+        } else if (vce == 2) {
+            d.om.alloc(n);
+            k_meat_weights<<<blocks_for(n, 256), 256, 0, st>>>(d.e.p, wv, n, kind, 1, d.om.p);
+            d.launches++;
+            const std::vector<double> shift = report_constant ? xbar : std::vector<double>(k, 0.0);
+            if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+            la::Mat meat(msz * msz, 0.0);
+            for (auto& sub : d.subsets) {
+                d.S.alloc(size_t(sub.G) * msz);
+                d.shift.alloc(k + 1);
+                if (k) CK(cudaMemcpyAsync(d.shift.p, shift.data(), k * 8, cudaMemcpyHostToDevice, st));
+                k_cluster_scores<<<ST_GRID, ST_TB, 0, st>>>(rows, R, d.col.p, d.shift.p, int(k), report_constant ? 1 : 0,
+                                                           d.om.p, sub.perm.p, sub.coff.p, sub.G, d.S.p);
+                d.launches++;
+                std::vector<int> scols(msz);
+                std::iota(scols.begin(), scols.end(), 0);
+                const la::Mat part = outer(d.S.p, sub.G, int(msz), scols, nullptr, false, nullptr, nullptr, false, nullptr);
+                for (size_t i = 0; i < msz * msz; i++) meat[i] += sub.sign * part[i];
+                // the next subset's scores need the kept columns again
+                if (k) CK(cudaMemcpyAsync(d.col.p, kcols.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+            }
+            standardize(meat);
+            const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
+            const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
+            fit_.crv1_scale = q_cluster;
+            fit_.ok = true;
+            v_s = la::sandwich(bread, meat, msz, q_cluster);
+            if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
+        } else {
+            const la::Mat meat = crv3_meat(rows, raw_h, R, kept, beta, wmean, report_constant, g);
+            const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
+            const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
+            for (size_t a = 0; a < msz; a++)
+                for (size_t b = 0; b < msz; b++)
+                    v_s[a * msz + b] = q_cluster * meat[a * msz + b] * sc[a] * sc[b] / (sd_y * sd_y);
+            if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
         }
-        standardize(meat);
-        const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
-        const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
-        fit_.crv1_scale = q_cluster;
-        fit_.ok = true;
-        v_s = la::sandwich(bread, meat, msz, q_cluster);
-        if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
-    } else {
-        const la::Mat meat = crv3_meat(rows, raw_h, R, kept, beta, wmean, report_constant, g);
-        const double nested_adj = dof.df_a_nested > 0 ? 1.0 : 0.0;
-        const double q_cluster = (bigN - 1.0) / (bigN - nested_adj - df_m - df_a) * g_min / (g_min - 1.0);
-        for (size_t a = 0; a < msz; a++)
-            for (size_t b = 0; b < msz; b++)
-                v_s[a * msz + b] = q_cluster * meat[a * msz + b] * sc[a] * sc[b] / (sd_y * sd_y);
-        if (ccodes_.size() > 1) la::fix_psd(v_s, msz, report_constant);
-    }
     }
     d.end(ph);
     d.collect();
@@ -918,17 +918,17 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     // Wald F of the slopes (greedy sweep of their variance)
     double f_stat = nanv();
     if (k > 0) {
-    la::Mat vkk(k * k);
-    for (size_t a = 0; a < k; a++)
-        for (size_t b = 0; b < k; b++) vkk[a * k + b] = v_s[a * msz + b];
-    std::vector<bool> dv;
-    const la::Mat iv = la::sweep_inverse(vkk, k, F_SWEEP_TOL, true, dv);
-    if (std::none_of(dv.begin(), dv.end(), [](bool x) { return x; })) {
-        double qf = 0.0;
+        la::Mat vkk(k * k);
         for (size_t a = 0; a < k; a++)
-            for (size_t b = 0; b < k; b++) qf += b_s[a] * iv[a * k + b] * b_s[b];
-        f_stat = finite_or_nan(qf / df_m);
-    }
+            for (size_t b = 0; b < k; b++) vkk[a * k + b] = v_s[a * msz + b];
+        std::vector<bool> dv;
+        const la::Mat iv = la::sweep_inverse(vkk, k, F_SWEEP_TOL, true, dv);
+        if (std::none_of(dv.begin(), dv.end(), [](bool x) { return x; })) {
+            double qf = 0.0;
+            for (size_t a = 0; a < k; a++)
+                for (size_t b = 0; b < k; b++) qf += b_s[a] * iv[a * k + b] * b_s[b];
+            f_stat = finite_or_nan(qf / df_m);
+        }
     }
     if (std::any_of(v_s.begin(), v_s.end(), [](double x) { return std::isnan(x); })) std::fill(v_s.begin(), v_s.end(), 0.0);
 
@@ -946,9 +946,9 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
     if (out.b) std::fill(out.b, out.b + k_all, 0.0);
     if (out.V) std::fill(out.V, out.V + k_all * k_all, 0.0);
     for (size_t a = 0; a < pos.size(); a++) {
-    if (out.b) out.b[pos[a]] = b_raw[a];
-    if (out.V)
-        for (size_t b = 0; b < pos.size(); b++) out.V[pos[a] * k_all + pos[b]] = v_raw[a * msz + b];
+        if (out.b) out.b[pos[a]] = b_raw[a];
+        if (out.V)
+            for (size_t b = 0; b < pos.size(); b++) out.V[pos[a] * k_all + pos[b]] = v_raw[a * msz + b];
     }
     if (out.status) std::copy(status.begin(), status.end(), out.status);
     out.k_all = int(k_all);
@@ -999,31 +999,31 @@ void GpuSession::ols(double* rows_in, bool on_device, size_t nx, const OlsSpec& 
         t[4] = s.nested ? 1.0 : 0.0;
     }
     if (out.resid) {
-    std::vector<double> e(n);
-    CK(cudaMemcpyAsync(e.data(), d.e.p, n * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (size_t i = 0; i < n; i++) out.resid[pi[i]] = e[i];
+        std::vector<double> e(n);
+        CK(cudaMemcpyAsync(e.data(), d.e.p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < n; i++) out.resid[pi[i]] = e[i];
     }
     if (out.d) {
-    // sum of the fixed effects: the FE fit of y minus the slopes' FE fits, less the constant
-    std::vector<double> comb(p_len, 0.0), fit(n);
-    for (size_t i = 0; i < p_len; i++) {
-        double v = coefs[i * r];
-        for (size_t a = 0; a < k; a++) v -= beta[a] * coefs[i * r + kept[a]];
-        comb[i] = v;
-    }
-    ab_->fit_rows(comb.data(), 1, 0, fit.data());
-    for (size_t i = 0; i < n; i++) out.d[pi[i]] = fit[i] - b0;
+        // sum of the fixed effects: the FE fit of y minus the slopes' FE fits, less the constant
+        std::vector<double> comb(p_len, 0.0), fit(n);
+        for (size_t i = 0; i < p_len; i++) {
+            double v = coefs[i * r];
+            for (size_t a = 0; a < k; a++) v -= beta[a] * coefs[i * r + kept[a]];
+            comb[i] = v;
+        }
+        ab_->fit_rows(comb.data(), 1, 0, fit.data());
+        for (size_t i = 0; i < n; i++) out.d[pi[i]] = fit[i] - b0;
     }
     if (out.groupvar) {
-    if (dof.has_groupvar) {
-        std::vector<u32> gv(n);
-        CK(cudaMemcpyAsync(gv.data(), d.dof.gv.p, n * sizeof(u32), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        for (size_t i = 0; i < n; i++) out.groupvar[i] = double(gv[i]);
-    } else {
-        std::fill(out.groupvar, out.groupvar + n, nanv());
-    }
+        if (dof.has_groupvar) {
+            std::vector<u32> gv(n);
+            CK(cudaMemcpyAsync(gv.data(), d.dof.gv.p, n * sizeof(u32), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (size_t i = 0; i < n; i++) out.groupvar[i] = double(gv[i]);
+        } else {
+            std::fill(out.groupvar, out.groupvar + n, nanv());
+        }
     }
     CK(cudaGetLastError());
 }
