@@ -639,9 +639,9 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W,
                         for (int b = 0; b < WNB; b++)
                             if (b < ns_acc) {
                                 double* sl = wacc + __shfl_sync(gmask, code[b], int(i), L) * 64;
-                                if (i < nc) {
-                                    sl[0] += v0;
-                                    sl[32] += v1;
+                                if (i < nc) {  // slots of columns past Rc are never read
+                                    if (on0) sl[0] += v0;
+                                    if (on1) sl[32] += v1;
                                 }
                             }
                     }
@@ -670,8 +670,8 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W,
                     for (int b = 0; b < WNB; b++)
                         if (b < ns_acc) {
                             double* sl = wacc + __shfl_sync(gmask, code[b], int(i), L) * 64;
-                            sl[0] += s0;
-                            sl[32] += s1;
+                            if (on0) sl[0] += s0;
+                            if (on1) sl[32] += s1;
                         }
                 }
             }
@@ -697,8 +697,8 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_grhs(DevStruct S, DevWeights W,
                     for (int b = 0; b < WNB; b++)
                         if (b < ns_acc) {
                             double* sl = wacc + __shfl_sync(gmask, code[b], int(i), L) * 64;
-                            sl[0] -= d0;
-                            sl[32] -= d1;
+                            if (on0) sl[0] -= d0;
+                            if (on1) sl[32] -= d1;
                         }
                 }
             }
