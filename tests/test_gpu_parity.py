@@ -103,9 +103,9 @@ def test_residualize_matches_oracle(pair):
 @pytest.mark.parametrize("r", [1, 11, 17, 40])
 @pytest.mark.parametrize("weighted", [False, True])
 def test_residualize_one_row_per_cell(r, weighted):
-    """One row per cell with FE1 segments of 1 to 40 cells: the lane-group residualization (its
-    register-held cells and the cells past them), the CTA tiles past 32 cells, and column chunks
-    of 1, 11, 16 + 1 and 16 + 16 + 8."""
+    """One row per cell with FE1 segments of 1 to 40 cells: the pipelined row-order tiles (R 1
+    and 11), the warp-tile kernel of wider rows (R 17 and 40, in column chunks), and the CTA tiles
+    past 32 cells."""
     rng = np.random.default_rng(40 + r + 100 * weighted)
     n_ind = 2500
     k = rng.integers(1, 41, n_ind)
