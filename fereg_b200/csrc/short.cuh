@@ -746,36 +746,52 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wpull_rhs(DevStruct S, DevWeigh
         stage_pull(S, k0, k1, tb.z, tb.w, st, true, 0u);
         if (tile + nw < wt.n) tb = wt.t[tile + nw];
         __syncwarp();
-        u32 i0 = 0;
-        for (u32 kl = 0; kl < k1 - k0; kl++) {
-            const u32 ie = st.kend[kl];
+        // this lane's column summed over the entries ib, ib + step, ... < ie of a list
+        auto list_sum = [&](u32 ib, u32 ie, u32 step) {
             double acc = 0.0;
-            if (L.on) {
-                if (trivial) {
+            if (trivial) {
 #pragma unroll 8
-                    for (u32 i = i0 + L.g; i < ie; i += G) {
-                        const u32 c = st.cell[i], s = st.seg[i];
-                        const double x = __ldg(vj + size_t(c) * Ru);
-                        const double sc = W.w_rows ? W.w_rows[c] * x : x;
-                        acc += sc - cellw(W, c) * __ldcg(bj + size_t(s) * Ru) * W.n1inv[s];
-                    }
-                } else {
+                for (u32 i = ib; i < ie; i += step) {
+                    const u32 c = st.cell[i], s = st.seg[i];
+                    const double x = __ldg(vj + size_t(c) * Ru);
+                    const double sc = W.w_rows ? W.w_rows[c] * x : x;
+                    acc += sc - cellw(W, c) * __ldcg(bj + size_t(s) * Ru) * W.n1inv[s];
+                }
+            } else {
 #pragma unroll 4
-                    for (u32 i = i0 + L.g; i < ie; i += G) {
-                        const u32 c = st.cell[i], s = st.seg[i];
-                        double sc = 0.0;
-                        const u32 re = S.cell_row[c + 1];
-                        for (u32 r = S.cell_row[c]; r < re; r++) {
-                            const double x = __ldg(vj + size_t(r) * Ru);
-                            sc += W.w_rows ? W.w_rows[r] * x : x;
-                        }
-                        acc += sc - cellw(W, c) * __ldcg(bj + size_t(s) * Ru) * W.n1inv[s];
+                for (u32 i = ib; i < ie; i += step) {
+                    const u32 c = st.cell[i], s = st.seg[i];
+                    double sc = 0.0;
+                    const u32 re = S.cell_row[c + 1];
+                    for (u32 r = S.cell_row[c]; r < re; r++) {
+                        const double x = __ldg(vj + size_t(r) * Ru);
+                        sc += W.w_rows ? W.w_rows[r] * x : x;
                     }
+                    acc += sc - cellw(W, c) * __ldcg(bj + size_t(s) * Ru) * W.n1inv[s];
                 }
             }
-            acc = group_total(acc, L);
-            if (L.on && L.g == 0) Y[size_t(k0 + kl) * Ru + j0 + L.j] = acc;
-            i0 = ie;
+            return acc;
+        };
+        const u32 nk = k1 - k0;
+        if (G <= 2 && nk >= u32(G)) {
+            // wide rows, two groups: group g takes the lists g, g + 2, ..., each list's entries in
+            // order, so that the groups' gathers at one step read the rows of neighbouring
+            // coordinates (neighbouring cells, sharing sectors)
+            for (u32 kb = 0; kb < nk; kb += G) {
+                const u32 kl = kb + L.g;
+                if (L.on && kl < nk)
+                    Y[size_t(k0 + kl) * Ru + j0 + L.j] = list_sum(kl ? st.kend[kl - 1] : 0u, st.kend[kl], 1u);
+            }
+        } else {
+            // the groups share each list's entries; their sums are added in group order
+            u32 i0 = 0;
+            for (u32 kl = 0; kl < nk; kl++) {
+                const u32 ie = st.kend[kl];
+                double acc = L.on ? list_sum(i0 + L.g, ie, u32(G)) : 0.0;
+                acc = group_total(acc, L);
+                if (L.on && L.g == 0) Y[size_t(k0 + kl) * Ru + j0 + L.j] = acc;
+                i0 = ie;
+            }
         }
         __syncwarp();
     }
