@@ -1926,13 +1926,23 @@ SolveInfo GpuAbsorber::solve(double* rows, size_t r, double tol, size_t maxiter,
     double* alpha = want_coefs ? x + m * r : nullptr;
     if (d.wseg.n && !S.cell_row && R <= FR_MAXR) {  // one row per cell, narrow rows: pipelined tiles
         const size_t shm = FR_WPB * fresid_bytes(R);
-        with_nbk<1, 0>(S.nb, [&](auto, auto nbk) {
-            constexpr int NBK = decltype(nbk)::value;
-            allow_smem(k_fresid<NBK>, shm);
-            const int per_sm = resident_ctas(k_fresid<NBK>, FR_WPB * 32, shm);  // shared memory bounds it
-            const int grid = 148 * std::max(1, std::min(per_sm, 5));
-            k_fresid<NBK><<<grid, FR_WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, x, d.b1.p, alpha);
-        });
+        auto run = [&](auto ne) {
+            constexpr int NE = decltype(ne)::value;
+            with_nbk<1, 0>(S.nb, [&](auto, auto nbk) {
+                constexpr int NBK = decltype(nbk)::value;
+                allow_smem(k_fresid<NBK, NE>, shm);
+                const int per_sm = resident_ctas(k_fresid<NBK, NE>, FR_WPB * 32, shm);  // shared memory bounds it
+                const int grid = 148 * std::max(1, std::min(per_sm, 5));
+                k_fresid<NBK, NE><<<grid, FR_WPB * 32, shm, st>>>(S, W, d.wseg.set(), rows, R, x, d.b1.p, alpha);
+            });
+        };
+        using std::integral_constant;
+        switch ((R + 3) / 4) {  // a tile holds at most WT R elements: R per lane
+            case 1: run(integral_constant<int, 4>{}); break;
+            case 2: run(integral_constant<int, 8>{}); break;
+            case 3: run(integral_constant<int, 12>{}); break;
+            default: run(integral_constant<int, 16>{}); break;
+        }
         d.launches++;
     }
     else if (d.wseg.n)

@@ -910,7 +910,6 @@ __global__ void __launch_bounds__(WPB * 32, 4) k_wresid(DevStruct S, DevWeights 
 //  3. every element is written back as v - (alpha(s(c), j) + u(c, j)).
 constexpr int FR_MAXR = 16;  // widest rows k_fresid takes
 constexpr int FR_WPB = 4;    // warps per CTA of k_fresid
-constexpr int FR_NE = WT * FR_MAXR / 32;  // elements per lane of a tile, at most
 
 // Per-warp shared memory of k_fresid for R columns: two buffers of [rows, coordinates, cell
 // weights, segment offsets, 1/n1], then U, A and the cells' local segments.
@@ -972,7 +971,8 @@ struct ElemPos {
     }
 };
 
-template <int NBK>
+// NE: elements per lane of a tile at most (WT R / 32 = R, rounded up to a multiple of 4).
+template <int NBK, int NE>
 __global__ void __launch_bounds__(FR_WPB * 32, 5) k_fresid(DevStruct S, DevWeights W, WarpTiles wt,
                                                            double* __restrict__ rows, int R,
                                                            const double* __restrict__ x,
@@ -1013,10 +1013,10 @@ __global__ void __launch_bounds__(FR_WPB * 32, 5) k_fresid(DevStruct S, DevWeigh
         }
         // 1. u of every element, all the lane's gathers in flight together
         {
-            double g[FR_NE];
+            double g[NE];
             ElemPos p = first;
 #pragma unroll
-            for (int k = 0; k < FR_NE; k++) {
+            for (int k = 0; k < NE; k++) {
                 g[k] = 0.0;
                 if (p.r < nc) {
 #pragma unroll
@@ -1028,7 +1028,7 @@ __global__ void __launch_bounds__(FR_WPB * 32, 5) k_fresid(DevStruct S, DevWeigh
                 p.step(q32, r32, uR);
             }
 #pragma unroll
-            for (int k = 0; k < FR_NE; k++) {
+            for (int k = 0; k < NE; k++) {
                 const u32 e = lane + 32u * u32(k);
                 if (e < E) U[e] = g[k];
             }
